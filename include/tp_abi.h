@@ -1,0 +1,278 @@
+/*
+ * tp_abi.h -- C ABI of the B200 particle-push library (libtpb200.so).
+ *
+ * The reference (TestParticle.jl v0.23.2) is pure Julia and has no FFI of its
+ * own; its hot path is entered through the ensemble-algorithm dispatch
+ *
+ *     TestParticle.solve(prob, alg, ensemblealg; dt, savestepinterval, ...)
+ *       -> _solve(::EnsembleAlg, prob::TraceProblem, alg::AbstractBoris, ...)
+ *                                        (src/boris/boris.jl:88-114,137-318)
+ *       -> _solve_adaptive(::EnsembleAlg, ...)   (src/boris/adaptive_boris.jl:21-139)
+ *       -> _solve(::EnsembleAlg, prob::TraceGCProblem, ...)
+ *                                        (src/gc/gc_solver.jl:59-161)
+ *
+ * A Julia package binds the entry points below with `ccall` from new
+ * `_solve(::EnsembleB200, ...)` methods, so a user call such as
+ * `TestParticle.solve(prob, Boris(), EnsembleB200(); dt, savestepinterval,
+ * trajectories)` returns the reference's EnsembleSolution layout.  Python
+ * binds the same symbols with ctypes.
+ *
+ * Conventions
+ *  - Every function returns an int status: TP_OK (0) or a negative TP_E_*.
+ *    TP_E_ARG corresponds to the reference's ArgumentError
+ *    (src/boris/boris.jl:349-356, src/types.jl:71-73); the others to
+ *    ErrorException.  The text of the last error of a context is returned by
+ *    tp_last_error().  No entry point aborts or traps.
+ *  - Input pointers are borrowed for the duration of the call.  Grid data is
+ *    copied to the device by tp_field_create().  Results are owned by a
+ *    tp_result until tp_result_destroy().
+ *  - Calls on one context are synchronous and must come from one thread at a
+ *    time.  Device entry points (suffix _device) are asynchronous on the
+ *    stream they are given.
+ *  - Particle state tables are 6 x N float64, column-major (Julia's layout of
+ *    a Matrix{Float64}(6, N)): element c of particle i is u0[6*i + c].
+ */
+#ifndef TP_ABI_H
+#define TP_ABI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TP_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    TP_OK = 0,
+    TP_E_ARG = -1,         /* invalid argument: reference ArgumentError     */
+    TP_E_CUDA = -2,        /* CUDA runtime error                             */
+    TP_E_TIMEOUT = -3,     /* device loop exceeded its wall-clock budget     */
+    TP_E_NOMEM = -4,       /* device or host allocation failed               */
+    TP_E_UNSUPPORTED = -5, /* field / algorithm combination not implemented  */
+    TP_E_OVERFLOW = -6     /* a particle produced more saves than slots      */
+};
+
+/* ---- per-trajectory return codes (SciMLBase.ReturnCode subset) --------- */
+enum {
+    TP_RET_DEFAULT = 0,
+    TP_RET_SUCCESS = 1,    /* ReturnCode.Success    */
+    TP_RET_TERMINATED = 2, /* ReturnCode.Terminated */
+    TP_RET_MAXITERS = 3    /* ReturnCode.MaxIters   */
+};
+
+/* ---- fields --------------------------------------------------------------
+ * The reference accepts any Julia callable F(x, t) as a field.  Callables
+ * cannot cross a C ABI, so a field is described by one of these kinds:
+ *   ZERO     ZeroField()                         (src/utility/zero.jl:35-51)
+ *   UNIFORM  F(x,t) = value
+ *   AFFINE   F(x,t) = value + jac * x + rate * t  (uniform, gradient and
+ *            linearly time-varying fields of the reference tests)
+ *   DIPOLE   F(x) = coef * (3 (m.rhat) rhat - m) / |x - center|^3
+ *            (the Magnetostatics.Dipole field of test/test_gc.jl:180)
+ *   GRID     trilinear interpolation of a (3, nx, ny, nz) column-major array
+ *            on a uniform Cartesian grid: build_interpolator(CartesianGrid,
+ *            A, x, y, z, 1, bc) (src/utility/interpolation.jl:217-235)     */
+enum {
+    TP_FIELD_ZERO = 0,
+    TP_FIELD_UNIFORM = 1,
+    TP_FIELD_AFFINE = 2,
+    TP_FIELD_DIPOLE = 3,
+    TP_FIELD_GRID = 4
+};
+
+/* grid boundary handling (FastInterpolations FillExtrap(NaN), ClampExtrap(),
+ * PeriodicBC(endpoint=:exclusive) / WrapExtrap() with period L = n * dx)   */
+enum {
+    TP_BC_FILL_NAN = 0,
+    TP_BC_CLAMP = 1,
+    TP_BC_PERIODIC = 2
+};
+
+enum { TP_DTYPE_F32 = 0, TP_DTYPE_F64 = 1 };
+
+typedef struct tp_field_desc {
+    int32_t kind;        /* TP_FIELD_*                                      */
+    int32_t bc;          /* GRID: TP_BC_*                                   */
+    int32_t dtype;       /* GRID: TP_DTYPE_* of data                        */
+    int32_t reserved;
+    double value[3];     /* UNIFORM value; AFFINE constant term             */
+    double jac[9];       /* AFFINE: d F_i / d x_j, row-major                */
+    double rate[3];      /* AFFINE: d F / d t                               */
+    double moment[3];    /* DIPOLE: magnetic moment [A m^2]                 */
+    double center[3];    /* DIPOLE: position of the dipole                  */
+    double coef;         /* DIPOLE: mu0 / 4pi                               */
+    int64_t n[3];        /* GRID: nodes along x, y, z (each >= 2)           */
+    double origin[3];    /* GRID: coordinate of node (0,0,0)                */
+    double spacing[3];   /* GRID: node spacing (> 0)                        */
+    const void* data;    /* GRID: host pointer, 3*nx*ny*nz values, (3,nx,ny,nz)
+                            column-major: component c of node (i,j,k) is at
+                            c + 3*(i + nx*(j + ny*k))                       */
+} tp_field_desc;
+
+/* ---- termination (the reference's `isoutside(u, p, t)` callback) --------
+ * A Julia closure cannot cross the ABI; the common predicates are flags.
+ * The predicate is evaluated where the reference calls isoutside:
+ * src/boris/boris.jl:459, src/boris/adaptive_boris.jl:227,
+ * src/gc/rk4_gc.jl:318, src/gc/rk45_gc.jl:128.                             */
+enum {
+    TP_TERM_SHELL = 1,   /* |x| < rmin or |x| > rmax                        */
+    TP_TERM_BOX = 2,     /* any x_c < lo_c or x_c > hi_c                    */
+    TP_TERM_NAN = 4,     /* any component of the state is NaN              */
+    TP_TERM_TIME = 8     /* t > tmax                                        */
+};
+
+typedef struct tp_term_desc {
+    int32_t flags;
+    int32_t reserved;
+    double rmin, rmax;
+    double lo[3], hi[3];
+    double tmax;
+} tp_term_desc;
+
+/* ---- full-orbit run ------------------------------------------------------ */
+enum {
+    TP_ALG_BORIS = 0,             /* Boris()                 boris.jl:480-557        */
+    TP_ALG_MULTISTEP = 1,         /* MultistepBoris{N}(n)    multistep_boris.jl:65-142 */
+    TP_ALG_ADAPTIVE = 2,          /* AdaptiveBoris(safety)   adaptive_boris.jl:145-266 */
+    TP_ALG_ADAPTIVE_MULTISTEP = 3 /* AdaptiveMultistepBoris{N}(n, safety)             */
+};
+
+enum {
+    TP_PREC_FP64 = 0,   /* plain float64, operation order of the reference   */
+    TP_PREC_FP32C = 1   /* float32 push, positions as compensated float pairs */
+};
+
+enum {
+    TP_SCHED_AUTO = 0,   /* library choice                                   */
+    TP_SCHED_STATIC = 1, /* one thread per particle                          */
+    TP_SCHED_QUEUE = 2   /* persistent kernel pulling particles from a queue */
+};
+
+typedef struct tp_run_desc {
+    int32_t alg;             /* TP_ALG_*                                    */
+    int32_t order;           /* multistep gyrophase order N: 2, 4 or 6      */
+    int32_t nsub;            /* multistep subcycles n >= 1                  */
+    int32_t precision;       /* TP_PREC_*                                   */
+    double safety;           /* adaptive safety factor                      */
+    double t0, t1;           /* tspan                                       */
+    double dt;               /* fixed-step dt                               */
+    double q2m, m;           /* p = (q2m, m, E, B, F) of prepare()          */
+    int64_t savestepinterval;
+    int64_t maxiters;        /* fixed step: nt > maxiters is TP_E_ARG       */
+    int32_t save_start, save_end, save_everystep, save_fields;
+    tp_term_desc term;
+    int64_t step_cap;        /* adaptive: steps per particle, 0 = no cap    */
+    int32_t schedule;        /* TP_SCHED_*                                  */
+    int32_t block;           /* threads per block, 0 = tuned / default      */
+    double budget_s;         /* device wall-clock budget, 0 = default 600 s */
+} tp_run_desc;
+
+/* ---- guiding-centre run ------------------------------------------------- */
+enum { TP_GC_RK4 = 0, TP_GC_RK45 = 1 };
+enum { TP_GC_PREC_FP64 = 0, TP_GC_PREC_FP32RHS = 1 };
+
+typedef struct tp_gc_desc {
+    int32_t alg;             /* TP_GC_RK4 (rk4_gc.jl) / TP_GC_RK45 (rk45_gc.jl)   */
+    int32_t precision;       /* TP_GC_PREC_*                                     */
+    double t0, t1;
+    double dt;               /* RK4 step / RK45 initial step                     */
+    int32_t dt_given;        /* 0: RK45 picks half a gyroperiod (rk45_gc.jl:82-99) */
+    int32_t reserved;
+    double q, q2m, mu;       /* p = (q, q2m, mu, E, B) of prepare_gc()          */
+    double abstol, reltol;
+    int64_t savestepinterval;
+    int64_t maxiters;
+    int32_t save_start, save_end, save_everystep, save_fields;
+    tp_term_desc term;
+    int32_t block;
+    int32_t reserved2;
+    double budget_s;
+} tp_gc_desc;
+
+typedef struct tp_ctx tp_ctx;
+typedef struct tp_field tp_field;
+typedef struct tp_result tp_result;
+
+/* ---- library and context ------------------------------------------------- */
+int tp_abi_version(void);
+int tp_ctx_create(int device, tp_ctx** out);
+void tp_ctx_destroy(tp_ctx* ctx);
+const char* tp_last_error(const tp_ctx* ctx);
+
+/* ---- fields --------------------------------------------------------------
+ * Replaces prepare_field / build_interpolator (src/prepare.jl:86-104,
+ * src/utility/interpolation.jl:217-235): the field is validated and any grid
+ * is uploaded once.                                                         */
+int tp_field_create(tp_ctx* ctx, const tp_field_desc* desc, tp_field** out);
+void tp_field_destroy(tp_field* field);
+
+/* ---- full-orbit solve (host buffers) --------------------------------------
+ * Replaces _solve(::EnsembleAlg, ::TraceProblem, ::AbstractBoris, ...)
+ * (src/boris/boris.jl:137-318) and _solve_adaptive (adaptive_boris.jl:40-139)
+ * for every trajectory i = 1..N:
+ *   u0     6 x N initial states (prob_func already applied on the host, as
+ *          src/boris/boris_kernel.jl:290-294 does)
+ *   dt_i   optional per-particle dt (fixed step), NULL = desc->dt
+ *   tend_i optional per-particle tspan[2], NULL = desc->t1
+ * The per-particle arrays are an extension: the reference shares one p, dt
+ * and tspan per solve (boris.jl:485).                                       */
+int tp_boris_run(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
+                 const tp_field* B, const double* u0, const double* dt_i,
+                 const double* tend_i, int64_t n, tp_result** out);
+
+/* Number of save slots per particle that a run needs (host arrays). */
+int tp_boris_slots(const tp_run_desc* desc, const double* dt_i,
+                   const double* tend_i, int64_t n, int64_t* nslots);
+
+/* Device-buffer variant: every pointer is device memory, the call is
+ * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * Outputs are slot-major structure-of-arrays:
+ *   t_out[k*n + i], u_out[(k*width + c)*n + i]  (width 6, or 12 with fields)
+ * nsaved[i] save count, retcode[i] TP_RET_*, nsteps[i] steps taken.
+ * status (device int32) receives a TP_E_* code from the kernel, or 0.      */
+int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* desc,
+                        const tp_field* E, const tp_field* B,
+                        const double* u0, const double* dt_i,
+                        const double* tend_i, int64_t n, int64_t nslots,
+                        double* t_out, double* u_out, int32_t* nsaved,
+                        int8_t* retcode, int64_t* nsteps, int32_t* status,
+                        void* stream);
+
+/* ---- guiding-centre solve -------------------------------------------------
+ * Replaces _solve(::EnsembleAlg, ::TraceGCProblem, ...) (gc_solver.jl:104-161)
+ * with _rk4! (rk4_gc.jl:27-130) or _rk45! (rk45_gc.jl:52-173).
+ *   y0  4 x N guiding-centre states (X, v_par)
+ *   q_i, q2m_i, mu_i  optional per-particle parameters (extension), NULL =
+ *   the shared values of desc
+ *   dt_i, tend_i      optional per-particle dt (RK4 step / RK45 initial step)
+ *                     and tspan[2] (extension), NULL = desc values.         */
+int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* desc, const tp_field* E,
+              const tp_field* B, const double* y0, const double* q_i,
+              const double* q2m_i, const double* mu_i, const double* dt_i,
+              const double* tend_i, int64_t n, tp_result** out);
+
+/* prepare_gc (src/gc/gc.jl:13-84) for N full-orbit states at time t:
+ * y0_out (4 x N) = (X, v_par), mu_out (N).  q, m shared by all particles.   */
+int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B,
+                  const double* xv, int64_t n, double q, double m, double t,
+                  double* y0_out, double* mu_out);
+
+/* ---- results ---------------------------------------------------------------
+ * Packed, per-trajectory layout of the reference solutions: trajectory i owns
+ * saves offset_i .. offset_i + nsaved_i - 1 with offset_i = sum_{j<i} nsaved_j;
+ * t_packed[s] is the save time and u_packed[s*width + c] the state of save s. */
+int tp_result_info(const tp_result* res, int64_t* n, int32_t* width,
+                   int64_t* total_saved);
+int tp_result_copy(const tp_result* res, int32_t* nsaved, int8_t* retcode,
+                   int64_t* nsteps, double* t_packed, double* u_packed);
+/* device time of the solve, milliseconds (CUDA events around the kernels) */
+int tp_result_elapsed_ms(const tp_result* res, double* ms);
+void tp_result_destroy(tp_result* res);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TP_ABI_H */

@@ -1,0 +1,297 @@
+"""ctypes wrapper of liboracle.so, the CPU restatement of the reference solver.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py to check and to time the CUDA library.  The
+product never imports it.
+
+Descriptors are the library's own (include/tp_abi.h via the package's _abi
+module), so the same run description drives both.  Fields and the
+termination predicate may also be Python callables (the reference tests'
+closures), passed as C callbacks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Callable, Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+FIELD_CB = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_void_p)
+JAC_CB = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_void_p)
+OUT_CB = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_void_p)
+
+
+class FieldCB(C.Structure):
+    _fields_ = [("f", FIELD_CB), ("j", JAC_CB), ("user", C.c_void_p)]
+
+
+class TermCB(C.Structure):
+    _fields_ = [("f", OUT_CB), ("user", C.c_void_p)]
+
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile liboracle.so with its Makefile (gcc; no GPU needed)."""
+    import subprocess
+    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        from_abi = _abi()
+        L = C.CDLL(str(LIB))
+        P = C.c_void_p
+        L.orc_boris_run.restype = C.c_int
+        L.orc_boris_run.argtypes = [C.POINTER(from_abi.RunDesc), C.POINTER(from_abi.FieldDesc),
+                                    C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), C.POINTER(FieldCB),
+                                    C.POINTER(TermCB), P, P, P, C.c_int64, C.c_int, C.c_int64, P, P, P, P, P]
+        L.orc_gc_run.restype = C.c_int
+        L.orc_gc_run.argtypes = [C.POINTER(from_abi.GCDesc), C.POINTER(from_abi.FieldDesc),
+                                 C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), C.POINTER(FieldCB),
+                                 C.POINTER(TermCB), P, P, P, P, P, P, C.c_int64, C.c_int, C.c_int64, P, P, P, P, P]
+        L.orc_gc_prepare.restype = C.c_int
+        L.orc_gc_prepare.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(from_abi.FieldDesc),
+                                     C.POINTER(FieldCB), C.POINTER(FieldCB), P, C.c_int64, C.c_double,
+                                     C.c_double, C.c_double, P, P]
+        L.orc_field_eval.restype = C.c_int
+        L.orc_field_eval.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), P, C.c_int64,
+                                     C.c_double, P, P]
+        L.orc_boris_counts.restype = C.c_int
+        L.orc_boris_counts.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64, C.c_int,
+                                       C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _abi():
+    import importlib.util
+    import sys
+    mod = sys.modules.get("testparticle_b200._abi")
+    if mod is not None:
+        return mod
+    p = HERE.parent / "testparticle.jl_b200" / "_abi.py"
+    spec = importlib.util.spec_from_file_location("_tp_oracle_abi", p)
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def field_callback(fn: Callable, jac: Optional[Callable] = None) -> FieldCB:
+    """Wrap fn(x: ndarray(3), t) -> 3-vector (and jac(x, t) -> 3x3) as C callbacks."""
+
+    def f(x, t, out, _u):
+        v = fn(np.array([x[0], x[1], x[2]]), t)
+        out[0], out[1], out[2] = float(v[0]), float(v[1]), float(v[2])
+
+    cb = FieldCB()
+    cb.f = FIELD_CB(f)
+    if jac is not None:
+        def j(x, t, out, _u):
+            J = np.asarray(jac(np.array([x[0], x[1], x[2]]), t), dtype=float).reshape(9)
+            for k in range(9):
+                out[k] = J[k]
+        cb.j = JAC_CB(j)
+    else:
+        cb.j = JAC_CB()
+    cb._keep = (cb.f, cb.j)
+    return cb
+
+
+def term_callback(fn: Callable) -> TermCB:
+    """Wrap isoutside(u: ndarray, t) -> bool as a C callback."""
+
+    def f(u, n, t, _u):
+        return 1 if fn(np.array([u[k] for k in range(n)]), t) else 0
+
+    cb = TermCB()
+    cb.f = OUT_CB(f)
+    cb._keep = cb.f
+    return cb
+
+
+@dataclass
+class OracleResult:
+    nsaved: np.ndarray
+    retcode: np.ndarray
+    nsteps: np.ndarray
+    t: np.ndarray      # packed
+    u: np.ndarray      # packed (total, width)
+
+    @property
+    def offsets(self):
+        o = np.zeros(self.nsaved.size + 1, dtype=np.int64)
+        np.cumsum(self.nsaved, out=o[1:])
+        return o
+
+    def traj(self, i):
+        o = self.offsets
+        return self.t[o[i]:o[i + 1]], self.u[o[i]:o[i + 1]]
+
+    def final_states(self):
+        o = self.offsets
+        return self.u[o[1:] - 1]
+
+
+def _pack(t_sm, u_sm, nsaved, W, n):
+    tot = int(nsaved.sum())
+    t = np.empty(tot)
+    u = np.empty((tot, W))
+    k = 0
+    for i in range(n):
+        m = int(nsaved[i])
+        t[k:k + m] = t_sm[:m, i]
+        u[k:k + m] = u_sm[:m, :, i]
+        k += m
+    return t, u
+
+
+def _field_arg(f):
+    """(descriptor, callback) for a package field object or a Python callable."""
+    if f is None:
+        return None, None
+    if callable(f) and not hasattr(f, "descriptor"):
+        return None, field_callback(f)
+    if isinstance(f, tuple) and len(f) == 2 and callable(f[0]):
+        return None, field_callback(f[0], f[1])
+    d = f.descriptor()
+    d._keep = f.keepalive()
+    return d, None
+
+
+def boris_run(desc, E, B, u0: np.ndarray, dt_i=None, tend_i=None, nthreads: int = 0,
+              isoutside: Optional[Callable] = None, nslots: int = 0) -> OracleResult:
+    """Ensemble solve on the CPU; E/B are package fields or Python callables."""
+    L = lib()
+    u0 = np.ascontiguousarray(u0, dtype=np.float64)
+    n = u0.shape[0]
+    W = 12 if desc.save_fields else 6
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    tcb = term_callback(isoutside) if isoutside is not None else None
+    dt_i = None if dt_i is None else np.ascontiguousarray(dt_i, dtype=np.float64)
+    tend_i = None if tend_i is None else np.ascontiguousarray(tend_i, dtype=np.float64)
+    if nthreads <= 0 and (Ecb is not None or Bcb is not None or tcb is not None):
+        nthreads = 1  # Python callbacks hold the GIL
+    if nslots <= 0:
+        nslots = 16
+    for _ in range(3):
+        t_sm = np.empty((nslots, n))
+        u_sm = np.empty((nslots, W, n))
+        nsaved = np.empty(n, dtype=np.int32)
+        rc = np.empty(n, dtype=np.int8)
+        nst = np.empty(n, dtype=np.int64)
+        code = L.orc_boris_run(C.byref(desc), C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None,
+                               C.byref(Ecb) if Ecb else None, C.byref(Bcb) if Bcb else None,
+                               C.byref(tcb) if tcb else None, _ptr(u0), _ptr(dt_i), _ptr(tend_i), n,
+                               int(nthreads), nslots, _ptr(t_sm), _ptr(u_sm), _ptr(nsaved), _ptr(rc),
+                               _ptr(nst))
+        if code == -6:  # overflow: grow and rerun
+            nslots = int(nsaved.max())
+            continue
+        if code == -1:
+            raise ValueError("oracle: ArgumentError")
+        if code != 0:
+            raise RuntimeError(f"oracle status {code}")
+        t, u = _pack(t_sm, u_sm, nsaved, W, n)
+        return OracleResult(nsaved, rc, nst, t, u)
+    raise RuntimeError("oracle: output sizing failed")
+
+
+def gc_run(desc, E, B, y0: np.ndarray, q_i=None, q2m_i=None, mu_i=None, nthreads: int = 0,
+           isoutside: Optional[Callable] = None, nslots: int = 0, dt_i=None, tend_i=None) -> OracleResult:
+    L = lib()
+    y0 = np.ascontiguousarray(y0, dtype=np.float64)
+    n = y0.shape[0]
+    W = 10 if desc.save_fields else 4
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    tcb = term_callback(isoutside) if isoutside is not None else None
+    conv = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+            for a in (q_i, q2m_i, mu_i, dt_i, tend_i)]
+    if nthreads <= 0 and (Ecb is not None or Bcb is not None or tcb is not None):
+        nthreads = 1
+    if nslots <= 0:
+        nslots = 64
+    for _ in range(3):
+        t_sm = np.empty((nslots, n))
+        u_sm = np.empty((nslots, W, n))
+        nsaved = np.empty(n, dtype=np.int32)
+        rc = np.empty(n, dtype=np.int8)
+        nst = np.empty(n, dtype=np.int64)
+        code = L.orc_gc_run(C.byref(desc), C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None,
+                            C.byref(Ecb) if Ecb else None, C.byref(Bcb) if Bcb else None,
+                            C.byref(tcb) if tcb else None, _ptr(y0), *[_ptr(a) for a in conv], n,
+                            int(nthreads), nslots, _ptr(t_sm), _ptr(u_sm), _ptr(nsaved), _ptr(rc), _ptr(nst))
+        if code == -6:
+            nslots = int(nsaved.max())
+            continue
+        if code == -1:
+            raise ValueError("oracle: ArgumentError")
+        if code != 0:
+            raise RuntimeError(f"oracle status {code}")
+        t, u = _pack(t_sm, u_sm, nsaved, W, n)
+        return OracleResult(nsaved, rc, nst, t, u)
+    raise RuntimeError("oracle: output sizing failed")
+
+
+def gc_prepare(E, B, xv: np.ndarray, q: float, m: float, t: float = 0.0):
+    L = lib()
+    xv = np.ascontiguousarray(np.atleast_2d(xv), dtype=np.float64)
+    n = xv.shape[0]
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    y0 = np.empty((n, 4))
+    mu = np.empty(n)
+    code = L.orc_gc_prepare(C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None,
+                            C.byref(Ecb) if Ecb else None, C.byref(Bcb) if Bcb else None, _ptr(xv), n,
+                            float(q), float(m), float(t), _ptr(y0), _ptr(mu))
+    if code != 0:
+        raise RuntimeError(f"oracle status {code}")
+    return y0, mu
+
+
+def field_eval(F, x: np.ndarray, t: float = 0.0, jacobian: bool = False):
+    L = lib()
+    x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+    n = x.shape[0]
+    d, cb = _field_arg(F)
+    out = np.empty((n, 3))
+    J = np.empty((n, 3, 3)) if jacobian else None
+    code = L.orc_field_eval(C.byref(d) if d else None, C.byref(cb) if cb else None, _ptr(x), n, float(t),
+                            _ptr(out), _ptr(J))
+    if code != 0:
+        raise RuntimeError(f"oracle status {code}")
+    return (out, J) if jacobian else out
+
+
+def boris_counts(t0, t1, dt, maxiters, ssi, save_start=True, save_end=True, save_everystep=True):
+    L = lib()
+    nt = C.c_int64()
+    nout = C.c_int64()
+    code = L.orc_boris_counts(t0, t1, dt, maxiters, ssi, int(save_start), int(save_end), int(save_everystep),
+                              C.byref(nt), C.byref(nout))
+    if code != 0:
+        raise ValueError("ArgumentError")
+    return nt.value, nout.value
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())

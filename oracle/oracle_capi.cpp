@@ -1,0 +1,341 @@
+// oracle_capi.cpp -- C entry points of the CPU oracle (liboracle.so).
+//
+// TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and the
+// cpu_baseline / --impl reference legs of bench.py, never by the product.
+//
+// The entry points take the same descriptors as the CUDA library
+// (include/tp_abi.h) and write the same slot-major output layout, so the two
+// can be compared element by element.  An OpenMP loop over particles stands
+// in for the reference's EnsembleThreads (src/boris/boris.jl:189-215:
+// Threads.@threads over index chunks).  Fields and the termination predicate
+// may instead be given as C callbacks, which is how the tests restate the
+// reference tests' Julia closures.
+#include <omp.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "tp_oracle.hpp"
+
+using namespace orc;
+
+extern "C" {
+
+typedef struct orc_field_cb {
+    field_cb f;
+    jac_cb j;
+    void* user;
+} orc_field_cb;
+
+typedef struct orc_term_cb {
+    outside_cb f;
+    void* user;
+} orc_term_cb;
+}
+
+namespace {
+
+std::unique_ptr<Field> make_field(const tp_field_desc* d, const orc_field_cb* cb) {
+    if (cb && cb->f) {
+        auto* f = new CallbackField();
+        f->f = cb->f;
+        f->jf = cb->j;
+        f->user = cb->user;
+        return std::unique_ptr<Field>(f);
+    }
+    if (!d || d->kind == TP_FIELD_ZERO) return std::unique_ptr<Field>(new ZeroField());
+    switch (d->kind) {
+        case TP_FIELD_UNIFORM:
+            return std::unique_ptr<Field>(new UniformField({d->value[0], d->value[1], d->value[2]}));
+        case TP_FIELD_AFFINE: {
+            auto* f = new AffineField();
+            f->f0 = {d->value[0], d->value[1], d->value[2]};
+            std::memcpy(f->Jm.a, d->jac, sizeof(f->Jm.a));
+            f->rate = {d->rate[0], d->rate[1], d->rate[2]};
+            return std::unique_ptr<Field>(f);
+        }
+        case TP_FIELD_DIPOLE: {
+            auto* f = new DipoleField();
+            f->m = {d->moment[0], d->moment[1], d->moment[2]};
+            f->c = {d->center[0], d->center[1], d->center[2]};
+            f->coef = d->coef;
+            return std::unique_ptr<Field>(f);
+        }
+        case TP_FIELD_GRID: {
+            if (d->dtype == TP_DTYPE_F32) {
+                auto* f = new GridField<float>();
+                for (int a = 0; a < 3; ++a) {
+                    f->n[a] = d->n[a];
+                    f->x0[a] = d->origin[a];
+                    f->inv_dx[a] = 1.0 / d->spacing[a];
+                }
+                f->bc = d->bc;
+                f->data = (const float*)d->data;
+                return std::unique_ptr<Field>(f);
+            } else {
+                auto* f = new GridField<double>();
+                for (int a = 0; a < 3; ++a) {
+                    f->n[a] = d->n[a];
+                    f->x0[a] = d->origin[a];
+                    f->inv_dx[a] = 1.0 / d->spacing[a];
+                }
+                f->bc = d->bc;
+                f->data = (const double*)d->data;
+                return std::unique_ptr<Field>(f);
+            }
+        }
+    }
+    return nullptr;
+}
+
+Term make_term(const tp_term_desc* d, const orc_term_cb* cb) {
+    Term t;
+    std::memset(&t.d, 0, sizeof(t.d));
+    if (d) t.d = *d;
+    if (cb && cb->f) {
+        t.cb = cb->f;
+        t.user = cb->user;
+    }
+    return t;
+}
+
+// Copy one trajectory into the slot-major output:
+//   t_out[k*n + i], u_out[(k*W + c)*n + i]
+bool store(const Traj& tr, int64_t i, int64_t n, int W, int64_t nslots, double* t_out,
+           double* u_out, int32_t* nsaved, int8_t* retcode, int64_t* nsteps) {
+    int64_t ns = (int64_t)tr.t.size();
+    if (nsaved) nsaved[i] = (int32_t)ns;
+    if (retcode) retcode[i] = (int8_t)tr.retcode;
+    if (nsteps) nsteps[i] = tr.nsteps;
+    int64_t m = ns < nslots ? ns : nslots;
+    for (int64_t k = 0; k < m; ++k) {
+        if (t_out) t_out[k * n + i] = tr.t[k];
+        if (u_out)
+            for (int c = 0; c < W; ++c) u_out[(k * W + c) * n + i] = tr.u[k * W + c];
+    }
+    return ns <= nslots;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_version(void) { return TP_ABI_VERSION; }
+
+int orc_max_threads(void) { return omp_get_max_threads(); }
+
+// nt and nout of _prepare_checks (src/boris/boris.jl:345-403).  Returns
+// TP_E_ARG for |dt| < 10 eps or nt > maxiters.
+int orc_boris_counts(double t0, double t1, double dt, int64_t maxiters, int64_t ssi,
+                     int save_start, int save_end, int save_everystep, int64_t* nt_out,
+                     int64_t* nout_out) {
+    if (std::fabs(dt) < 10.0 * 2.220446049250313e-16) return TP_E_ARG;
+    if (ssi < 1) return TP_E_ARG;
+    double ttotal = t1 - t0;
+    int64_t nt = jl_round(ttotal / dt);
+    if (nt < 0) nt = -nt;
+    if (nt > maxiters) return TP_E_ARG;
+    *nt_out = nt;
+    *nout_out = calculate_nout(nt, ssi, save_start != 0, save_end != 0, save_everystep != 0);
+    return TP_OK;
+}
+
+// Full-orbit ensemble (Boris, MultistepBoris, AdaptiveBoris, AdaptiveMultistepBoris).
+int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_desc* Bd,
+                  const orc_field_cb* Ecb, const orc_field_cb* Bcb, const orc_term_cb* tcb,
+                  const double* u0, const double* dt_i, const double* tend_i, int64_t n,
+                  int nthreads, int64_t nslots, double* t_out, double* u_out, int32_t* nsaved,
+                  int8_t* retcode, int64_t* nsteps) {
+    std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
+    if (!E || !B) return TP_E_ARG;
+    if (d->alg == TP_ALG_MULTISTEP || d->alg == TP_ALG_ADAPTIVE_MULTISTEP) {
+        if (d->order != 2 && d->order != 4 && d->order != 6) return TP_E_ARG;
+        if (d->nsub < 1) return TP_E_ARG;
+    }
+    if (d->savestepinterval < 1) return TP_E_ARG;
+    Term term = make_term(&d->term, tcb);
+    Params p{d->q2m, d->m, E.get(), B.get()};
+    const int W = d->save_fields ? 12 : 6;
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    const bool multistep = d->alg == TP_ALG_MULTISTEP || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+
+    // argument checks of every trajectory first (the reference throws before tracing)
+    if (!adaptive) {
+        for (int64_t i = 0; i < n; ++i) {
+            double dt = dt_i ? dt_i[i] : d->dt;
+            double t1 = tend_i ? tend_i[i] : d->t1;
+            int64_t nt, nout;
+            int st = orc_boris_counts(d->t0, t1, dt, d->maxiters, d->savestepinterval, d->save_start,
+                                      d->save_end, d->save_everystep, &nt, &nout);
+            if (st != TP_OK) return st;
+        }
+    }
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    int overflow = 0;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads) reduction(| : overflow)
+    for (int64_t i = 0; i < n; ++i) {
+        Traj tr;
+        double t1 = tend_i ? tend_i[i] : d->t1;
+        const double* ui = u0 + 6 * i;
+        if (!adaptive) {
+            FixedOpts o;
+            o.t0 = d->t0;
+            o.t1 = t1;
+            o.dt = dt_i ? dt_i[i] : d->dt;
+            int64_t nt, nout;
+            orc_boris_counts(d->t0, t1, o.dt, d->maxiters, d->savestepinterval, d->save_start,
+                             d->save_end, d->save_everystep, &nt, &nout);
+            o.nt = nt;
+            o.nout = nout;
+            o.ssi = d->savestepinterval;
+            o.save_start = d->save_start != 0;
+            o.save_end = d->save_end != 0;
+            o.save_everystep = d->save_everystep != 0;
+            o.save_fields = d->save_fields != 0;
+            if (multistep)
+                boris_single(MultistepUpdater{d->order, d->nsub}, p, o, term, ui, tr);
+            else
+                boris_single(BorisUpdater{}, p, o, term, ui, tr);
+        } else {
+            if (multistep)
+                adaptive_single(MultistepUpdater{d->order, d->nsub}, p, d->t0, t1, d->safety,
+                                d->savestepinterval, d->save_start, d->save_end,
+                                d->save_everystep, d->save_fields, d->step_cap, term, ui, tr);
+            else
+                adaptive_single(BorisUpdater{}, p, d->t0, t1, d->safety, d->savestepinterval,
+                                d->save_start, d->save_end, d->save_everystep, d->save_fields,
+                                d->step_cap, term, ui, tr);
+        }
+        if (!store(tr, i, n, W, nslots, t_out, u_out, nsaved, retcode, nsteps)) overflow |= 1;
+    }
+    return overflow ? TP_E_OVERFLOW : TP_OK;
+}
+
+// Guiding-centre ensemble (RK4 / RK45); per-particle q, q2m, mu optional.
+int orc_gc_run(const tp_gc_desc* d, const tp_field_desc* Ed, const tp_field_desc* Bd,
+               const orc_field_cb* Ecb, const orc_field_cb* Bcb, const orc_term_cb* tcb,
+               const double* y0, const double* q_i, const double* q2m_i, const double* mu_i,
+               const double* dt_i, const double* tend_i, int64_t n, int nthreads, int64_t nslots,
+               double* t_out, double* u_out, int32_t* nsaved, int8_t* retcode, int64_t* nsteps) {
+    std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
+    if (!E || !B) return TP_E_ARG;
+    Term term = make_term(&d->term, tcb);
+    const int W = d->save_fields ? 10 : 4;
+    // _prepare_gc, src/gc/gc_solver.jl:187-231
+    GCOpts o;
+    o.t0 = d->t0;
+    o.t1 = d->t1;
+    o.dt = d->dt;
+    o.dt_given = d->dt_given != 0;
+    o.ssi = d->savestepinterval;
+    o.maxiters = d->maxiters;
+    o.save_start = d->save_start != 0;
+    o.save_end = d->save_end != 0;
+    o.save_everystep = d->save_everystep != 0;
+    o.save_fields = d->save_fields != 0;
+    o.abstol = d->abstol;
+    o.reltol = d->reltol;
+    double ttotal = d->t1 - d->t0;
+    int64_t nt = 0;
+    if (!o.dt_given) {
+        if (d->alg == TP_GC_RK4) return TP_E_ARG;  // "dt must be provided for fixed step solver :rk4"
+    } else {
+        double sdt = (d->dt > 0) - (d->dt < 0), stt = (ttotal > 0) - (ttotal < 0);
+        if (d->alg == TP_GC_RK4 && sdt != stt && ttotal != 0) return TP_E_ARG;
+        nt = jl_round(ttotal / d->dt);
+        if (d->alg == TP_GC_RK4 && nt > d->maxiters) nt = d->maxiters;
+    }
+    if (d->alg == TP_GC_RK4 && o.ssi < 1) return TP_E_ARG;
+    int64_t nout = 0;
+    if (o.save_start) nout += 1;
+    if (d->alg == TP_GC_RK4 && o.save_everystep) {
+        int64_t steps = nt / o.ssi;
+        bool last_is_step = (nt > 0) && (nt % o.ssi == 0);
+        nout += steps;
+        if (!o.save_end && last_is_step) nout -= 1;
+        if (o.save_end && !last_is_step) nout += 1;
+    } else if (d->alg == TP_GC_RK4 && o.save_end) {
+        nout += 1;
+    }
+    o.nt = nt;
+    o.nout = nout;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    int overflow = 0;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads) reduction(| : overflow)
+    for (int64_t i = 0; i < n; ++i) {
+        GCParams p{q_i ? q_i[i] : d->q, q2m_i ? q2m_i[i] : d->q2m, mu_i ? mu_i[i] : d->mu, E.get(),
+                   B.get()};
+        GCOpts oi = o;  // per-particle dt / tspan[2] (extension): _prepare_gc per particle
+        if (dt_i || tend_i) {
+            oi.dt = dt_i ? dt_i[i] : d->dt;
+            oi.t1 = tend_i ? tend_i[i] : d->t1;
+            if (d->alg == TP_GC_RK4) {
+                int64_t nti = jl_round((oi.t1 - d->t0) / oi.dt);
+                if (nti > d->maxiters) nti = d->maxiters;
+                int64_t no = o.save_start ? 1 : 0;
+                if (o.save_everystep) {
+                    no += nti / o.ssi;
+                    bool last_is_step = (nti > 0) && (nti % o.ssi == 0);
+                    if (!o.save_end && last_is_step) no -= 1;
+                    if (o.save_end && !last_is_step) no += 1;
+                } else if (o.save_end) {
+                    no += 1;
+                }
+                oi.nt = nti;
+                oi.nout = no;
+            } else if (dt_i) {
+                oi.dt_given = true;
+            }
+        }
+        Traj tr;
+        if (d->alg == TP_GC_RK4)
+            rk4_single(p, oi, term, y0 + 4 * i, tr);
+        else
+            rk45_single(p, oi, term, y0 + 4 * i, tr);
+        if (!store(tr, i, n, W, nslots, t_out, u_out, nsaved, retcode, nsteps)) overflow |= 1;
+    }
+    return overflow ? TP_E_OVERFLOW : TP_OK;
+}
+
+// prepare_gc for n full-orbit states (src/gc/gc.jl:49-84)
+int orc_gc_prepare(const tp_field_desc* Ed, const tp_field_desc* Bd, const orc_field_cb* Ecb,
+                   const orc_field_cb* Bcb, const double* xv, int64_t n, double q, double m,
+                   double t, double* y0_out, double* mu_out) {
+    std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
+    if (!E || !B) return TP_E_ARG;
+    for (int64_t i = 0; i < n; ++i) {
+        gc_parameters(xv + 6 * i, *E, *B, q, m, t, y0_out + 4 * i, y0_out + 4 * i + 3,
+                      mu_out + i);
+    }
+    return TP_OK;
+}
+
+// Field values (and optionally Jacobians, row-major 9 per point) at n points.
+int orc_field_eval(const tp_field_desc* d, const orc_field_cb* cb, const double* x, int64_t n,
+                   double t, double* out, double* jac_out) {
+    std::unique_ptr<Field> F = make_field(d, cb);
+    if (!F) return TP_E_ARG;
+    for (int64_t i = 0; i < n; ++i) {
+        V3d r{x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+        if (jac_out) {
+            V3d v;
+            M3 J;
+            F->jac(r, t, v, J);
+            out[3 * i] = v.x;
+            out[3 * i + 1] = v.y;
+            out[3 * i + 2] = v.z;
+            std::memcpy(jac_out + 9 * i, J.a, sizeof(J.a));
+        } else {
+            V3d v = F->eval(r, t);
+            out[3 * i] = v.x;
+            out[3 * i + 1] = v.y;
+            out[3 * i + 2] = v.z;
+        }
+    }
+    return TP_OK;
+}
+
+}  // extern "C"

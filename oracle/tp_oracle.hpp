@@ -1,0 +1,855 @@
+// tp_oracle.hpp -- CPU restatement of TestParticle.jl's particle-push hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This header is the parity oracle: the tests, the
+// smoke check and the CPU-baseline leg of the benchmark link it (through
+// liboracle.so) to check and to time the CUDA library against it.  The
+// product library never includes, links or calls it.
+//
+// Scope (reference = TestParticle.jl v0.23.2, paths relative to its root):
+//   boris_velocity_update      src/boris/boris.jl:19-31
+//   update_velocity            src/boris/boris.jl:38-45
+//   update_velocity_multistep  src/boris/multistep_boris.jl:65-142
+//   _prepare_checks / nout     src/boris/boris.jl:345-403
+//   _boris_loop! / _boris_single  src/boris/boris.jl:445-557
+//   _adaptive_boris_single     src/boris/adaptive_boris.jl:145-266
+//   get_B_parameters           src/equations.jl:239-247
+//   get_gc_derivatives         src/equations.jl:329-360
+//   update_rk4 / _rk4!         src/gc/rk4_gc.jl:7-130
+//   update_dp5 / _rk45!        src/gc/rk45_gc.jl:7-173
+//   _prepare_gc                src/gc/gc_solver.jl:187-231
+//   _get_gc_parameters         src/gc/gc.jl:13-39
+//   get_perp_vector            src/utility/utility.jl:119-126
+//   fields: ZeroField (src/utility/zero.jl:66-73), trilinear FieldInterpolator
+//           (src/utility/interpolation.jl:21-27,217-235; the arithmetic of the
+//           third-party FastInterpolations.jl 0.4.11 linear_interp is restated
+//           from its published definition, see GridField below).
+//
+// Floating point.  Compile with -ffp-contract=off.  Julia evaluates these
+// expressions without contraction except where `@muladd` (or `@fastmath`)
+// rewrites a scalar `a*b + c`; those places call std::fma explicitly and say
+// so.  SVector arithmetic under `@muladd` is not fused (the generic muladd
+// fallback computes x*y + z), so vector updates are plain multiply-then-add.
+// The library's FP64 kernels follow the same order, which makes the two
+// bit-identical wherever only +, -, *, /, sqrt and fma are involved.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+#include <algorithm>
+
+#include "../include/tp_abi.h"
+
+namespace orc {
+
+// ---------------------------------------------------------------- vectors
+template <class T>
+struct V3 {
+    T x, y, z;
+};
+
+template <class T> inline V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> inline V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> inline V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> inline V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> inline V3<T> operator/(V3<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+// StaticArrays cross: (a2 b3 - a3 b2, a3 b1 - a1 b3, a1 b2 - a2 b1)
+template <class T> inline V3<T> cross(V3<T> a, V3<T> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// StaticArrays dot / sum(abs2, .): ((a1 b1 + a2 b2) + a3 b3)
+template <class T> inline T dot(V3<T> a, V3<T> b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+template <class T> inline T abs2sum(V3<T> a) { return (a.x * a.x + a.y * a.y) + a.z * a.z; }
+inline double norm(V3<double> a) { return std::sqrt(abs2sum(a)); }
+
+using V3d = V3<double>;
+
+// 3x3 matrix, row-major: J[i][j] = d F_i / d x_j
+struct M3 {
+    double a[9];
+    double operator()(int i, int j) const { return a[3 * i + j]; }
+};
+
+// ---------------------------------------------------------------- fields
+// Every field offers eval(r, t) and jac(r, t, B, J) (value and Jacobian, the
+// role ForwardDiff.jacobian plays in _get_B_jacobian, src/utility/utility.jl:386-392).
+
+struct Field {
+    virtual ~Field() {}
+    virtual V3d eval(V3d r, double t) const = 0;
+    virtual void jac(V3d r, double t, V3d& F, M3& J) const = 0;
+};
+
+struct ZeroField : Field {
+    V3d eval(V3d, double) const override { return {0.0, 0.0, 0.0}; }
+    void jac(V3d, double, V3d& F, M3& J) const override {
+        F = {0.0, 0.0, 0.0};
+        for (double& v : J.a) v = 0.0;
+    }
+};
+
+struct UniformField : Field {
+    V3d v;
+    explicit UniformField(V3d v_) : v(v_) {}
+    V3d eval(V3d, double) const override { return v; }
+    void jac(V3d, double, V3d& F, M3& J) const override {
+        F = v;
+        for (double& a : J.a) a = 0.0;
+    }
+};
+
+// F(x,t) = F0 + J x + rate t, evaluated as ((F0_i + ((J_i0 x + J_i1 y) + J_i2 z)) + rate_i t)
+struct AffineField : Field {
+    V3d f0;
+    M3 Jm;
+    V3d rate;
+    V3d eval(V3d r, double t) const override {
+        V3d F;
+        F.x = (f0.x + ((Jm(0, 0) * r.x + Jm(0, 1) * r.y) + Jm(0, 2) * r.z)) + rate.x * t;
+        F.y = (f0.y + ((Jm(1, 0) * r.x + Jm(1, 1) * r.y) + Jm(1, 2) * r.z)) + rate.y * t;
+        F.z = (f0.z + ((Jm(2, 0) * r.x + Jm(2, 1) * r.y) + Jm(2, 2) * r.z)) + rate.z * t;
+        return F;
+    }
+    void jac(V3d r, double t, V3d& F, M3& J) const override {
+        F = eval(r, t);
+        J = Jm;
+    }
+};
+
+// Point dipole B(x) = coef (3 (m.rhat) rhat - m) / d^3, d = |x - c|, evaluated
+// in the order of the textbook expression coef * (3*(m.rhat)*rhat - m) / d^3.
+struct DipoleField : Field {
+    V3d m, c;
+    double coef;
+    V3d eval(V3d r, double) const override {
+        V3d d = r - c;
+        double dm = norm(d);
+        V3d rh = d / dm;
+        double mr = dot(m, rh);
+        double d3 = (dm * dm) * dm;
+        V3d s = (3.0 * mr) * rh - m;
+        return (coef * s) / d3;
+    }
+    // Analytic Jacobian: B_i = coef (3 (m.d) d_i / |d|^5 - m_i / |d|^3)
+    // dB_i/dx_j = coef (3 (m_j d_i + (m.d) delta_ij + m_i d_j) / |d|^5
+    //                   - 15 (m.d) d_i d_j / |d|^7)
+    void jac(V3d r, double t, V3d& F, M3& J) const override {
+        F = eval(r, t);
+        V3d d = r - c;
+        double d2 = abs2sum(d);
+        double dm = std::sqrt(d2);
+        double inv5 = 1.0 / ((d2 * d2) * dm);
+        double inv7 = inv5 / d2;
+        double md = dot(m, d);
+        double dv[3] = {d.x, d.y, d.z}, mv[3] = {m.x, m.y, m.z};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double dij = (i == j) ? md : 0.0;
+                J.a[3 * i + j] = coef * (3.0 * ((mv[j] * dv[i] + dij) + mv[i] * dv[j]) * inv5 -
+                                         15.0 * md * dv[i] * dv[j] * inv7);
+            }
+    }
+};
+
+// Trilinear interpolation of a (3, nx, ny, nz) column-major array on a
+// uniform grid, the reference's FieldInterpolator over linear_interp
+// (src/utility/interpolation.jl:119-148,217-235).  Per axis:
+//   u = (x - origin) * inv_dx, with inv_dx = 1/dx computed once;
+//   FILL_NAN : u outside [0, n-1] -> NaN;  i = min(floor(u), n-2), f = u - i
+//   CLAMP    : u clamped to [0, n-1];     i = min(floor(u), n-2), f = u - i
+//   PERIODIC : i = floor(u), f = u - i, i = i mod n, i1 = (i+1) mod n
+//              (period L = n*dx, PeriodicBC(endpoint=:exclusive))
+// then lerp(a, b, f) = a + f*(b - a) along x, then y, then z.
+template <class D>
+struct GridField : Field {
+    int64_t n[3];
+    double x0[3], inv_dx[3];
+    int bc;
+    const D* data;  // (3, nx, ny, nz)
+
+    struct Axis {
+        int64_t i0, i1;
+        double f;
+        bool nan;
+    };
+    Axis axis(int a, double x) const {
+        Axis r{0, 0, 0.0, false};
+        double u = (x - x0[a]) * inv_dx[a];
+        int64_t na = n[a];
+        if (bc == TP_BC_PERIODIC) {
+            double fl = std::floor(u);
+            r.f = u - fl;
+            int64_t i = (int64_t)fl % na;
+            if (i < 0) i += na;
+            r.i0 = i;
+            r.i1 = (i + 1 == na) ? 0 : i + 1;
+            return r;
+        }
+        double umax = (double)(na - 1);
+        if (bc == TP_BC_CLAMP) {
+            u = std::min(std::max(u, 0.0), umax);
+        } else if (!(u >= 0.0 && u <= umax)) {
+            r.nan = true;
+            return r;
+        }
+        double fl = std::floor(u);
+        int64_t i = (int64_t)fl;
+        if (i > na - 2) i = na - 2;
+        r.i0 = i;
+        r.i1 = i + 1;
+        r.f = u - (double)i;
+        return r;
+    }
+    double at(int c, int64_t i, int64_t j, int64_t k) const {
+        return (double)data[c + 3 * (i + n[0] * (j + n[1] * k))];
+    }
+    static double lerp(double a, double b, double f) { return a + f * (b - a); }
+
+    V3d eval(V3d r, double) const override {
+        Axis ax = axis(0, r.x), ay = axis(1, r.y), az = axis(2, r.z);
+        if (ax.nan || ay.nan || az.nan) {
+            double q = std::numeric_limits<double>::quiet_NaN();
+            return {q, q, q};
+        }
+        double out[3];
+        for (int c = 0; c < 3; ++c) {
+            double c00 = lerp(at(c, ax.i0, ay.i0, az.i0), at(c, ax.i1, ay.i0, az.i0), ax.f);
+            double c10 = lerp(at(c, ax.i0, ay.i1, az.i0), at(c, ax.i1, ay.i1, az.i0), ax.f);
+            double c01 = lerp(at(c, ax.i0, ay.i0, az.i1), at(c, ax.i1, ay.i0, az.i1), ax.f);
+            double c11 = lerp(at(c, ax.i0, ay.i1, az.i1), at(c, ax.i1, ay.i1, az.i1), ax.f);
+            double c0 = lerp(c00, c10, ay.f);
+            double c1 = lerp(c01, c11, ay.f);
+            out[c] = lerp(c0, c1, az.f);
+        }
+        return {out[0], out[1], out[2]};
+    }
+    // Jacobian of the trilinear interpolant inside the cell (the derivative
+    // ForwardDiff takes through linear_interp); clamped axes outside the
+    // grid have zero derivative.
+    void jac(V3d r, double t, V3d& F, M3& J) const override {
+        F = eval(r, t);
+        Axis ax = axis(0, r.x), ay = axis(1, r.y), az = axis(2, r.z);
+        if (ax.nan || ay.nan || az.nan) {
+            for (double& a : J.a) a = std::numeric_limits<double>::quiet_NaN();
+            return;
+        }
+        double sx = inv_dx[0], sy = inv_dx[1], sz = inv_dx[2];
+        if (bc == TP_BC_CLAMP) {
+            double ux = (r.x - x0[0]) * inv_dx[0], uy = (r.y - x0[1]) * inv_dx[1],
+                   uz = (r.z - x0[2]) * inv_dx[2];
+            if (ux < 0.0 || ux > (double)(n[0] - 1)) sx = 0.0;
+            if (uy < 0.0 || uy > (double)(n[1] - 1)) sy = 0.0;
+            if (uz < 0.0 || uz > (double)(n[2] - 1)) sz = 0.0;
+        }
+        for (int c = 0; c < 3; ++c) {
+            double v000 = at(c, ax.i0, ay.i0, az.i0), v100 = at(c, ax.i1, ay.i0, az.i0);
+            double v010 = at(c, ax.i0, ay.i1, az.i0), v110 = at(c, ax.i1, ay.i1, az.i0);
+            double v001 = at(c, ax.i0, ay.i0, az.i1), v101 = at(c, ax.i1, ay.i0, az.i1);
+            double v011 = at(c, ax.i0, ay.i1, az.i1), v111 = at(c, ax.i1, ay.i1, az.i1);
+            double fx = ax.f, fy = ay.f, fz = az.f;
+            // d/dx
+            double dx00 = v100 - v000, dx10 = v110 - v010, dx01 = v101 - v001, dx11 = v111 - v011;
+            double dx0 = lerp(dx00, dx10, fy), dx1 = lerp(dx01, dx11, fy);
+            J.a[3 * c + 0] = lerp(dx0, dx1, fz) * sx;
+            // d/dy
+            double c00 = lerp(v000, v100, fx), c10 = lerp(v010, v110, fx);
+            double c01 = lerp(v001, v101, fx), c11 = lerp(v011, v111, fx);
+            J.a[3 * c + 1] = lerp(c10 - c00, c11 - c01, fz) * sy;
+            // d/dz
+            double c0 = lerp(c00, c10, fy), c1 = lerp(c01, c11, fy);
+            J.a[3 * c + 2] = (c1 - c0) * sz;
+        }
+    }
+};
+
+// A field given by C callbacks (the tests' Julia closures restated in Python).
+typedef void (*field_cb)(const double* x, double t, double* out, void* user);
+typedef void (*jac_cb)(const double* x, double t, double* out9, void* user);
+struct CallbackField : Field {
+    field_cb f;
+    jac_cb jf;
+    void* user;
+    V3d eval(V3d r, double t) const override {
+        double x[3] = {r.x, r.y, r.z}, o[3];
+        f(x, t, o, user);
+        return {o[0], o[1], o[2]};
+    }
+    void jac(V3d r, double t, V3d& F, M3& J) const override {
+        F = eval(r, t);
+        if (jf) {
+            double x[3] = {r.x, r.y, r.z};
+            jf(x, t, J.a, user);
+        } else {
+            for (double& a : J.a) a = 0.0;
+        }
+    }
+};
+
+// ---------------------------------------------------------------- termination
+typedef int (*outside_cb)(const double* u, int len, double t, void* user);
+struct Term {
+    tp_term_desc d;
+    outside_cb cb = nullptr;
+    void* user = nullptr;
+    bool any() const { return d.flags != 0 || cb != nullptr; }
+    // isoutside(u, p, t) with u = (r, v) (full orbit) or (X, v_par) (GC)
+    bool outside(const double* u, int len, double t) const {
+        if (cb) return cb(u, len, t, user) != 0;
+        int f = d.flags;
+        if (f & TP_TERM_NAN)
+            for (int k = 0; k < len; ++k)
+                if (std::isnan(u[k])) return true;
+        if (f & TP_TERM_SHELL) {
+            double r = std::sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+            if (r < d.rmin || r > d.rmax) return true;
+        }
+        if (f & TP_TERM_BOX)
+            for (int c = 0; c < 3; ++c)
+                if (u[c] < d.lo[c] || u[c] > d.hi[c]) return true;
+        if (f & TP_TERM_TIME)
+            if (t > d.tmax) return true;
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------- Boris core
+// boris_velocity_update, src/boris/boris.jl:19-31
+inline V3d boris_velocity_update(V3d v, V3d E, V3d B, double qdt_2m) {
+    V3d t_rotate = qdt_2m * B;
+    double t_mag2 = abs2sum(t_rotate);
+    V3d s_rotate = (2.0 * t_rotate) / (1.0 + t_mag2);
+    V3d vm = v + qdt_2m * E;
+    V3d vp_ = vm + cross(vm, t_rotate);
+    V3d vplus = vm + cross(vp_, s_rotate);
+    return vplus + qdt_2m * E;
+}
+
+struct Params {
+    double q2m, m;
+    const Field* E;
+    const Field* B;
+};
+
+// update_velocity, src/boris/boris.jl:38-45
+struct BorisUpdater {
+    V3d operator()(V3d v, V3d r, double dt, double t, const Params& p) const {
+        V3d E = p.E->eval(r, t);
+        V3d B = p.B->eval(r, t);
+        double qdt_2m = p.q2m * 0.5 * dt;
+        return boris_velocity_update(v, E, B, qdt_2m);
+    }
+};
+
+// update_velocity_multistep, src/boris/multistep_boris.jl:65-142
+// (@muladd fuses the scalar a*b+c forms: the Taylor coefficients and cos(2n alpha))
+struct MultistepUpdater {
+    int N;  // gyrophase correction order 2, 4, 6
+    int n;  // subcycles
+    V3d operator()(V3d v, V3d r, double dt, double t, const Params& p) const {
+        V3d E = p.E->eval(r, t);
+        V3d B = p.B->eval(r, t);
+        double factor = p.q2m * dt / (double)(2 * n);
+        V3d t_n = factor * B;
+        V3d e_n = factor * E;
+        if (N != 2) {
+            double t_mag2 = abs2sum(t_n);
+            double f_N, e_corr;
+            if (N == 4) {
+                f_N = 1.0 + t_mag2 / 3.0;
+                e_corr = -1.0 / 3.0;
+            } else {
+                f_N = (1.0 + t_mag2 / 3.0) + 2.0 * t_mag2 * t_mag2 / 15.0;
+                e_corr = -1.0 / 3.0 - 2.0 * t_mag2 / 15.0;
+            }
+            double e_dot_t = dot(e_n, t_n);
+            e_n = f_N * e_n + (e_corr * e_dot_t) * t_n;
+            t_n = f_N * t_n;
+        }
+        double t_n_mag2 = abs2sum(t_n);
+        double t_n_mag = std::sqrt(t_n_mag2);
+        double c1, c2, c3, c6;
+        double nd = (double)n;
+        if (t_n_mag < 1.0e-4) {  // TN_MAG_THRESHOLD, src/boris/boris.jl:3
+            c1 = std::fma(-(2.0 * nd * nd), t_n_mag2, 1.0);
+            double n_term1 = 2.0 * nd;
+            double n_term3 = 4.0 * nd * nd * nd;
+            c2 = std::fma(-((n_term1 + n_term3) / 3.0), t_n_mag2, n_term1);
+            c3 = std::fma(-((4.0 * nd * nd + 2.0 * nd * nd * nd * nd) / 3.0), t_n_mag2,
+                          2.0 * nd * nd);
+            c6 = (n_term1 + n_term3) / 3.0;
+        } else {
+            double alpha = std::atan(t_n_mag);
+            double na = nd * alpha;
+            double s = std::sin(na), c = std::cos(na);
+            double s2 = 2.0 * s * c;
+            double cc = std::fma(c, c, -(s * s));
+            c1 = cc;
+            c2 = s2 / t_n_mag;
+            c3 = 2.0 * s * s / t_n_mag2;
+            c6 = (2.0 * nd - c2) / t_n_mag2;
+        }
+        double c4 = c2, c5 = c3;
+        double v_dot_t = dot(v, t_n);
+        double e_dot_t = dot(e_n, t_n);
+        V3d v_cross_t = cross(v, t_n);
+        V3d e_cross_t = cross(e_n, t_n);
+        V3d out = c1 * v + c2 * v_cross_t;
+        out = out + (c3 * v_dot_t) * t_n;
+        out = out + c4 * e_n;
+        out = out + c5 * e_cross_t;
+        out = out + (c6 * e_dot_t) * t_n;
+        return out;
+    }
+};
+
+// Julia round(Int, x): round half to even
+inline int64_t jl_round(double x) { return (int64_t)std::nearbyint(x); }
+
+// _calculate_nout, src/boris/boris.jl:383-403
+inline int64_t calculate_nout(int64_t nt, int64_t ssi, bool save_start, bool save_end,
+                              bool save_everystep) {
+    int64_t nout = 0;
+    if (save_start) nout += 1;
+    if (save_everystep) {
+        int64_t steps = nt / ssi;
+        bool last_is_step = (nt > 0) && (nt % ssi == 0);
+        nout += steps;
+        if (!save_end && last_is_step) nout -= 1;
+        if (save_end && !last_is_step) nout += 1;
+    } else if (save_end) {
+        nout += 1;
+    }
+    return nout;
+}
+
+// One trajectory's output.
+struct Traj {
+    std::vector<double> t;
+    std::vector<double> u;  // width per save
+    int retcode = TP_RET_DEFAULT;
+    int64_t nsteps = 0;
+};
+
+inline void push_save(Traj& out, const Params& p, bool save_fields, V3d r, V3d v, double t) {
+    out.t.push_back(t);
+    double s[6] = {r.x, r.y, r.z, v.x, v.y, v.z};
+    out.u.insert(out.u.end(), s, s + 6);
+    if (save_fields) {  // _prepare_saved_data, src/boris/boris.jl:405-427
+        V3d E = p.E->eval(r, t), B = p.B->eval(r, t);
+        double f[6] = {E.x, E.y, E.z, B.x, B.y, B.z};
+        out.u.insert(out.u.end(), f, f + 6);
+    }
+}
+
+struct FixedOpts {
+    double t0, t1, dt;
+    int64_t nt, nout, ssi;
+    bool save_start, save_end, save_everystep, save_fields;
+};
+
+// _boris_single + _boris_loop!, src/boris/boris.jl:445-557
+template <class Upd>
+void boris_single(const Upd& upd, const Params& p, const FixedOpts& o, const Term& term,
+                  const double* u0, Traj& out) {
+    const double dt = o.dt;
+    int64_t iout = 0;
+    V3d r{u0[0], u0[1], u0[2]};
+    V3d v{u0[3], u0[4], u0[5]};
+    if (o.save_start) {
+        iout += 1;
+        push_save(out, p, o.save_fields, r, v, o.t0);
+    }
+    // push velocity back in time by 1/2 dt (boris.jl:514)
+    v = upd(v, r, -0.5 * dt, o.t0, p);
+
+    // _boris_loop! (boris.jl:445-478)
+    int64_t it = 1;
+    double t = o.t0 - 0.5 * dt;
+    bool terminated = false;
+    V3d v_prev = v;
+    while (it <= o.nt) {
+        v_prev = v;
+        t += dt;
+        v = upd(v, r, dt, t, p);
+        V3d r_next = r + v * dt;
+        double t_next = t + 0.5 * dt;
+        if (term.any()) {
+            double xv[6] = {r_next.x, r_next.y, r_next.z, v.x, v.y, v.z};
+            if (term.outside(xv, 6, t_next)) {
+                terminated = true;
+                break;
+            }
+        }
+        if (o.save_everystep && (it - 1) > 0 && (it - 1) % o.ssi == 0) {
+            iout += 1;
+            if (iout <= o.nout) {
+                double t_current = t - 0.5 * dt;
+                V3d v_save = upd(v_prev, r, 0.5 * dt, t_current, p);
+                push_save(out, p, o.save_fields, r, v_save, t_current);
+            }
+        }
+        r = r_next;
+        it += 1;
+    }
+    int64_t final_step = it - 1;
+    if (terminated) v = v_prev;  // return it - 1, iout, r, v_prev  (boris.jl:460)
+    out.nsteps = final_step;
+
+    bool should_save_final = false;
+    if (o.save_end)
+        should_save_final = true;
+    else if (o.save_everystep && final_step > 0 && final_step % o.ssi == 0)
+        should_save_final = true;
+
+    if (iout < o.nout && should_save_final) {
+        // @muladd: tspan[1] + final_step*dt and tspan[1] + (final_step - 0.5)*dt are fused
+        double t_final = (final_step == o.nt) ? o.t1 : std::fma((double)final_step, dt, o.t0);
+        if (iout == 0 || out.t.back() < t_final) {
+            iout += 1;
+            double dt_final = t_final - std::fma((double)final_step - 0.5, dt, o.t0);
+            V3d v_final = upd(v, r, dt_final, t_final, p);
+            push_save(out, p, o.save_fields, r, v_final, t_final);
+        }
+    }
+    out.retcode = (iout < o.nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS;
+}
+
+// _adaptive_boris_single, src/boris/adaptive_boris.jl:145-266
+// step_cap (extension): stop after that many steps with retcode MaxIters.
+template <class Upd>
+void adaptive_single(const Upd& upd, const Params& p, double t0, double t1, double safety,
+                     int64_t ssi, bool save_start, bool save_end, bool save_everystep,
+                     bool save_fields, int64_t step_cap, const Term& term, const double* u0,
+                     Traj& out) {
+    const double twopi = 6.283185307179586;  // Float64(2pi)
+    double sgn = (t1 - t0) > 0 ? 1.0 : ((t1 - t0) < 0 ? -1.0 : 0.0);
+    double C = (twopi * safety * sgn) / std::fabs(p.q2m);
+    V3d r{u0[0], u0[1], u0[2]};
+    V3d v{u0[3], u0[4], u0[5]};
+    double t = t0;
+    double ttotal = t1 - t0;
+    if (save_start) push_save(out, p, save_fields, r, v, t);
+    double Bmag = norm(p.B->eval(r, t));
+    double dt = C / Bmag;
+    v = upd(v, r, -0.5 * dt, t, p);
+    int64_t it = 1;
+    bool should_save_final = save_end;
+    int ret = TP_RET_SUCCESS;
+    int64_t steps = 0;
+    while (std::fabs(t - t0) < std::fabs(ttotal)) {
+        if (step_cap > 0 && steps >= step_cap) {
+            ret = TP_RET_MAXITERS;
+            break;
+        }
+        if (std::fabs(t + dt - t0) > std::fabs(ttotal)) {
+            double dt_step = t1 - t;
+            v = upd(v, r, 0.5 * dt, t, p);
+            v = upd(v, r, -0.5 * dt_step, t, p);
+            dt = dt_step;
+        }
+        if (save_everystep && (it - 1) > 0 && (it - 1) % ssi == 0) {
+            V3d v_save = upd(v, r, 0.5 * dt, t, p);
+            push_save(out, p, save_fields, r, v_save, t);
+        }
+        double t_mid = t + 0.5 * dt;
+        V3d v_new = upd(v, r, dt, t_mid, p);
+        V3d r_next = r + v_new * dt;
+        double t_next = t + dt;
+        if (term.any()) {
+            double xv[6] = {r_next.x, r_next.y, r_next.z, v_new.x, v_new.y, v_new.z};
+            if (term.outside(xv, 6, t_next)) {
+                should_save_final = true;
+                ret = TP_RET_TERMINATED;
+                break;
+            }
+        }
+        r = r_next;
+        t = t_next;
+        v = v_new;
+        steps += 1;
+        Bmag = norm(p.B->eval(r, t));
+        double dt_new = C / Bmag;
+        v = upd(v, r, 0.5 * dt, t, p);
+        v = upd(v, r, -0.5 * dt_new, t, p);
+        dt = dt_new;
+        it += 1;
+        if (save_everystep && (it - 1) % ssi == 0) should_save_final = true;
+    }
+    if (should_save_final && (out.t.empty() || out.t.back() != t)) {
+        V3d v_final = upd(v, r, 0.5 * dt, t, p);
+        push_save(out, p, save_fields, r, v_final, t);
+    }
+    out.retcode = ret;
+    out.nsteps = steps;
+}
+
+// ---------------------------------------------------------------- guiding centre
+struct GCParams {
+    double q, q2m, mu;
+    const Field* E;
+    const Field* B;
+};
+
+struct GCState {
+    double y[4];
+};
+
+// get_gc_derivatives, src/equations.jl:329-360 (with get_B_parameters, :239-247)
+inline GCState gc_rhs(const GCState& s, const GCParams& p, double t) {
+    V3d X{s.y[0], s.y[1], s.y[2]};
+    V3d E = p.E->eval(X, t);
+    V3d B;
+    M3 J;
+    p.B->jac(X, t, B, J);
+    double Bmag = norm(B);
+    V3d bh = B / Bmag;
+    // grad|B| = JB' * bhat
+    V3d gB{(J(0, 0) * bh.x + J(1, 0) * bh.y) + J(2, 0) * bh.z,
+           (J(0, 1) * bh.x + J(1, 1) * bh.y) + J(2, 1) * bh.z,
+           (J(0, 2) * bh.x + J(1, 2) * bh.y) + J(2, 2) * bh.z};
+    V3d curlB{J(2, 1) - J(1, 2), J(0, 2) - J(2, 0), J(1, 0) - J(0, 1)};
+    V3d curlb = (curlB + cross(bh, gB)) / Bmag;
+    V3d Bs = B + (s.y[3] / p.q2m) * curlb;
+    V3d Es = E - (p.mu / p.q) * gB;
+    double inv_Bpar = 1.0 / dot(bh, Bs);
+    V3d v = (s.y[3] * Bs + cross(Es, bh)) * inv_Bpar;
+    double du = dot((p.q2m * inv_Bpar) * Bs, Es);
+    return {{v.x, v.y, v.z, du}};
+}
+
+inline GCState gadd(const GCState& a, const GCState& b) {
+    return {{a.y[0] + b.y[0], a.y[1] + b.y[1], a.y[2] + b.y[2], a.y[3] + b.y[3]}};
+}
+inline GCState gscale(double s, const GCState& a) {
+    return {{s * a.y[0], s * a.y[1], s * a.y[2], s * a.y[3]}};
+}
+
+// update_rk4, src/gc/rk4_gc.jl:7-22
+inline GCState update_rk4(const GCState& y, const GCParams& p, double dt, double t) {
+    GCState k1 = gc_rhs(y, p, t);
+    GCState yt = gadd(y, gscale(0.5 * dt, k1));
+    GCState k2 = gc_rhs(yt, p, t + 0.5 * dt);
+    yt = gadd(y, gscale(0.5 * dt, k2));
+    GCState k3 = gc_rhs(yt, p, t + 0.5 * dt);
+    yt = gadd(y, gscale(dt, k3));
+    GCState k4 = gc_rhs(yt, p, t + dt);
+    GCState sum = gadd(gadd(gadd(k1, gscale(2.0, k2)), gscale(2.0, k3)), k4);
+    return gscale(dt / 6.0, sum);
+}
+
+inline void push_gc_save(Traj& out, const GCParams& p, bool save_fields, const GCState& s,
+                         double t) {
+    out.t.push_back(t);
+    out.u.insert(out.u.end(), s.y, s.y + 4);
+    if (save_fields) {  // _prepare_saved_data_gc, src/gc/gc_solver.jl:233-248
+        V3d X{s.y[0], s.y[1], s.y[2]};
+        V3d E = p.E->eval(X, t), B = p.B->eval(X, t);
+        double f[6] = {E.x, E.y, E.z, B.x, B.y, B.z};
+        out.u.insert(out.u.end(), f, f + 6);
+    }
+}
+
+struct GCOpts {
+    double t0, t1, dt;
+    bool dt_given;
+    int64_t nt, nout, ssi, maxiters;
+    bool save_start, save_end, save_everystep, save_fields;
+    double abstol, reltol;
+};
+
+// _rk4!, src/gc/rk4_gc.jl:27-130 (the @fastmath loop fuses t0 + (it-1)*dt)
+inline void rk4_single(const GCParams& p, const GCOpts& o, const Term& term, const double* y0,
+                       Traj& out) {
+    GCState xv{{y0[0], y0[1], y0[2], y0[3]}};
+    int64_t iout = 0;
+    if (o.save_start) {
+        iout += 1;
+        push_gc_save(out, p, o.save_fields, xv, o.t0);
+    }
+    int64_t it = 1;
+    const double dt = o.dt;
+    while (it <= o.nt && it <= o.maxiters) {
+        double t = std::fma((double)(it - 1), dt, o.t0);
+        GCState dx = update_rk4(xv, p, dt, t);
+        GCState xn = gadd(xv, dx);
+        if (term.any() && term.outside(xn.y, 4, t + dt)) break;
+        xv = xn;
+        if (o.save_everystep && (it % o.ssi == 0)) {
+            iout += 1;
+            if (iout <= o.nout) push_gc_save(out, p, o.save_fields, xv, t + dt);
+        }
+        it += 1;
+    }
+    int64_t final_step = it - 1;
+    bool should_save_final = false;
+    if (o.save_end)
+        should_save_final = true;
+    else if (o.save_everystep && final_step > 0 && final_step % o.ssi == 0)
+        should_save_final = true;
+    if (iout < o.nout && should_save_final) {
+        double t_final = (final_step == o.nt) ? o.t1 : std::fma((double)final_step, dt, o.t0);
+        if (iout == 0 || out.t.back() < t_final) {
+            iout += 1;
+            push_gc_save(out, p, o.save_fields, xv, t_final);
+        }
+    }
+    if (it <= o.nt && it <= o.maxiters)
+        out.retcode = TP_RET_TERMINATED;
+    else if (it > o.maxiters)
+        out.retcode = TP_RET_MAXITERS;
+    else
+        out.retcode = TP_RET_SUCCESS;
+    out.nsteps = final_step;
+}
+
+// Dormand-Prince 5(4) tableau, src/gc/rk45_gc.jl:9-20
+struct DP5 {
+    static constexpr double c2 = 1.0 / 5, c3 = 3.0 / 10, c4 = 4.0 / 5, c5 = 8.0 / 9, c6 = 1.0;
+    static constexpr double a21 = 1.0 / 5;
+    static constexpr double a31 = 3.0 / 40, a32 = 9.0 / 40;
+    static constexpr double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
+    static constexpr double a51 = 19372.0 / 6561, a52 = -25360.0 / 2187, a53 = 64448.0 / 6561,
+                            a54 = -212.0 / 729;
+    static constexpr double a61 = 9017.0 / 3168, a62 = -355.0 / 33, a63 = 46732.0 / 5247,
+                            a64 = 49.0 / 176, a65 = -5103.0 / 18656;
+    static constexpr double a71 = 35.0 / 384, a72 = 0.0, a73 = 500.0 / 1113, a74 = 125.0 / 192,
+                            a75 = -2187.0 / 6784, a76 = 11.0 / 84;
+    static constexpr double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192,
+                            b5 = -2187.0 / 6784, b6 = 11.0 / 84;
+    static constexpr double e1 = 71.0 / 57600, e3 = -71.0 / 16695, e4 = 71.0 / 1920,
+                            e5 = -17253.0 / 339200, e6 = 22.0 / 525, e7 = -1.0 / 40;
+};
+
+// update_dp5, src/gc/rk45_gc.jl:7-47.  Linear combinations are summed left to
+// right, each term a scalar times a vector, then scaled by dt; the stage times
+// t + c_k*dt are fused by @muladd.
+inline void update_dp5(const GCState& y, const GCParams& p, double dt, double t, GCState& dy,
+                       GCState& err) {
+    typedef DP5 D;
+    GCState k1 = gc_rhs(y, p, t);
+    GCState yt = gadd(y, gscale(dt, gscale(D::a21, k1)));
+    GCState k2 = gc_rhs(yt, p, std::fma(D::c2, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gscale(D::a31, k1), gscale(D::a32, k2))));
+    GCState k3 = gc_rhs(yt, p, std::fma(D::c3, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gscale(D::a41, k1), gscale(D::a42, k2)), gscale(D::a43, k3))));
+    GCState k4 = gc_rhs(yt, p, std::fma(D::c4, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gscale(D::a51, k1), gscale(D::a52, k2)),
+                                      gscale(D::a53, k3)),
+                                 gscale(D::a54, k4))));
+    GCState k5 = gc_rhs(yt, p, std::fma(D::c5, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gscale(D::a61, k1), gscale(D::a62, k2)),
+                                           gscale(D::a63, k3)),
+                                      gscale(D::a64, k4)),
+                                 gscale(D::a65, k5))));
+    GCState k6 = gc_rhs(yt, p, std::fma(D::c6, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(D::a71, k1), gscale(D::a72, k2)),
+                                                gscale(D::a73, k3)),
+                                           gscale(D::a74, k4)),
+                                      gscale(D::a75, k5)),
+                                 gscale(D::a76, k6))));
+    GCState k7 = gc_rhs(yt, p, t + dt);
+    dy = gscale(dt, gadd(gadd(gadd(gadd(gscale(D::b1, k1), gscale(D::b3, k3)), gscale(D::b4, k4)),
+                              gscale(D::b5, k5)),
+                         gscale(D::b6, k6)));
+    err = gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(D::e1, k1), gscale(D::e3, k3)),
+                                         gscale(D::e4, k4)),
+                                    gscale(D::e5, k5)),
+                               gscale(D::e6, k6)),
+                          gscale(D::e7, k7)));
+}
+
+// _rk45!, src/gc/rk45_gc.jl:52-173 (inside @fastmath: the error scale and the
+// sum of squares are fused multiply-adds)
+inline void rk45_single(const GCParams& p, const GCOpts& o, const Term& term, const double* y0,
+                        Traj& out) {
+    const double safety = 0.9, max_growth = 5.0, min_growth = 0.2;
+    GCState xv{{y0[0], y0[1], y0[2], y0[3]}};
+    double t = o.t0;
+    double dt;
+    if (!o.dt_given) {
+        V3d R{xv.y[0], xv.y[1], xv.y[2]};
+        double Bmag = norm(p.B->eval(R, t));
+        if (Bmag == 0.0 || p.q2m == 0.0) {
+            dt = 1.0e-6;
+        } else {
+            double omega = std::fabs(p.q2m * Bmag);
+            dt = 0.5 * 6.283185307179586 / omega;
+        }
+    } else {
+        dt = o.dt;
+    }
+    if (o.save_start) push_gc_save(out, p, o.save_fields, xv, t);
+    int64_t steps = 0;
+    int ret = TP_RET_SUCCESS;
+    while (t < o.t1 && steps < o.maxiters) {
+        if (t + dt > o.t1) dt = o.t1 - t;
+        GCState dx, E;
+        update_dp5(xv, p, dt, t, dx, E);
+        GCState yn = gadd(xv, dx);
+        double sum_sq = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            double sc = std::fma(std::max(std::fabs(xv.y[k]), std::fabs(yn.y[k])), o.reltol, o.abstol);
+            double q = E.y[k] / sc;
+            sum_sq = std::fma(q, q, sum_sq);
+        }
+        double error_ratio = 0.5 * std::sqrt(sum_sq);
+        // `error_ratio <= 1.0` inside @fastmath: the no-NaN comparison accepts a
+        // NaN ratio, after which isoutside sees the NaN state and terminates
+        // (the reference's test_boundary.jl:84-95 expects Terminated there).
+        if (!(error_ratio > 1.0)) {
+            if (term.any() && term.outside(yn.y, 4, t + dt)) {
+                ret = TP_RET_TERMINATED;
+                break;
+            }
+            t += dt;
+            xv = yn;
+            if (o.save_everystep) push_gc_save(out, p, o.save_fields, xv, t);
+            steps += 1;
+        }
+        double scale = (error_ratio == 0.0) ? max_growth : safety * std::pow(1.0 / error_ratio, 0.2);
+        scale = std::max(min_growth, std::min(scale, max_growth));
+        dt *= scale;
+        if (dt < 1.0e-14) break;
+    }
+    if (o.save_end && (out.t.empty() || out.t.back() != t)) push_gc_save(out, p, o.save_fields, xv, t);
+    out.retcode = ret;
+    out.nsteps = steps;
+}
+
+// get_perp_vector, src/utility/utility.jl:119-126
+inline void get_perp_vector(V3d b, V3d& e1, V3d& e2) {
+    V3d bh = b / norm(b);
+    V3d v = std::fabs(bh.z) < 0.9 ? V3d{0.0, 0.0, 1.0} : V3d{0.0, 1.0, 0.0};
+    V3d c = cross(v, bh);
+    e1 = c / norm(c);
+    e2 = cross(bh, e1);
+}
+
+// _get_gc_parameters, src/gc/gc.jl:13-39 -> (X, vpar, mu)
+inline void gc_parameters(const double* xv, const Field& E, const Field& B, double q, double m,
+                          double t, double* X_out, double* vpar_out, double* mu_out) {
+    V3d x{xv[0], xv[1], xv[2]}, v{xv[3], xv[4], xv[5]};
+    V3d bp = B.eval(x, t);
+    double Bmp = norm(bp);
+    V3d bhp = bp / Bmp;
+    V3d rho = cross(bhp, v) / (q / m * Bmp);
+    V3d X = x - rho;
+    V3d b = B.eval(X, t);
+    double Bmag = norm(b);
+    V3d bh = b / Bmag;
+    double vpar = dot(bh, v);
+    V3d vperp = v - vpar * bh;
+    V3d e = E.eval(X, t);
+    V3d vE = cross(e, bh) / Bmag;
+    V3d w = vperp - vE;
+    double mu = m * dot(w, w) / (2.0 * Bmag);
+    X_out[0] = X.x;
+    X_out[1] = X.y;
+    X_out[2] = X.z;
+    *vpar_out = vpar;
+    *mu_out = mu;
+}
+
+}  // namespace orc

@@ -1,0 +1,203 @@
+"""ctypes view of include/tp_abi.h and the loader of libtpb200.so.
+
+The structures mirror the C declarations field for field.  The library is
+loaded from this directory; a missing library raises ImportError -- there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libtpb200.so"
+
+TP_ABI_VERSION = 1
+
+TP_OK = 0
+TP_E_ARG = -1
+TP_E_CUDA = -2
+TP_E_TIMEOUT = -3
+TP_E_NOMEM = -4
+TP_E_UNSUPPORTED = -5
+TP_E_OVERFLOW = -6
+
+TP_RET_DEFAULT = 0
+TP_RET_SUCCESS = 1
+TP_RET_TERMINATED = 2
+TP_RET_MAXITERS = 3
+
+TP_FIELD_ZERO = 0
+TP_FIELD_UNIFORM = 1
+TP_FIELD_AFFINE = 2
+TP_FIELD_DIPOLE = 3
+TP_FIELD_GRID = 4
+
+TP_BC_FILL_NAN = 0
+TP_BC_CLAMP = 1
+TP_BC_PERIODIC = 2
+
+TP_DTYPE_F32 = 0
+TP_DTYPE_F64 = 1
+
+TP_TERM_SHELL = 1
+TP_TERM_BOX = 2
+TP_TERM_NAN = 4
+TP_TERM_TIME = 8
+
+TP_ALG_BORIS = 0
+TP_ALG_MULTISTEP = 1
+TP_ALG_ADAPTIVE = 2
+TP_ALG_ADAPTIVE_MULTISTEP = 3
+
+TP_PREC_FP64 = 0
+TP_PREC_FP32C = 1
+
+TP_SCHED_AUTO = 0
+TP_SCHED_STATIC = 1
+TP_SCHED_QUEUE = 2
+
+TP_GC_RK4 = 0
+TP_GC_RK45 = 1
+TP_GC_PREC_FP64 = 0
+TP_GC_PREC_FP32RHS = 1
+
+_D3 = C.c_double * 3
+_D9 = C.c_double * 9
+_I3 = C.c_int64 * 3
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("bc", C.c_int32),
+        ("dtype", C.c_int32),
+        ("reserved", C.c_int32),
+        ("value", _D3),
+        ("jac", _D9),
+        ("rate", _D3),
+        ("moment", _D3),
+        ("center", _D3),
+        ("coef", C.c_double),
+        ("n", _I3),
+        ("origin", _D3),
+        ("spacing", _D3),
+        ("data", C.c_void_p),
+    ]
+
+
+class TermDesc(C.Structure):
+    _fields_ = [
+        ("flags", C.c_int32),
+        ("reserved", C.c_int32),
+        ("rmin", C.c_double),
+        ("rmax", C.c_double),
+        ("lo", _D3),
+        ("hi", _D3),
+        ("tmax", C.c_double),
+    ]
+
+
+class RunDesc(C.Structure):
+    _fields_ = [
+        ("alg", C.c_int32),
+        ("order", C.c_int32),
+        ("nsub", C.c_int32),
+        ("precision", C.c_int32),
+        ("safety", C.c_double),
+        ("t0", C.c_double),
+        ("t1", C.c_double),
+        ("dt", C.c_double),
+        ("q2m", C.c_double),
+        ("m", C.c_double),
+        ("savestepinterval", C.c_int64),
+        ("maxiters", C.c_int64),
+        ("save_start", C.c_int32),
+        ("save_end", C.c_int32),
+        ("save_everystep", C.c_int32),
+        ("save_fields", C.c_int32),
+        ("term", TermDesc),
+        ("step_cap", C.c_int64),
+        ("schedule", C.c_int32),
+        ("block", C.c_int32),
+        ("budget_s", C.c_double),
+    ]
+
+
+class GCDesc(C.Structure):
+    _fields_ = [
+        ("alg", C.c_int32),
+        ("precision", C.c_int32),
+        ("t0", C.c_double),
+        ("t1", C.c_double),
+        ("dt", C.c_double),
+        ("dt_given", C.c_int32),
+        ("reserved", C.c_int32),
+        ("q", C.c_double),
+        ("q2m", C.c_double),
+        ("mu", C.c_double),
+        ("abstol", C.c_double),
+        ("reltol", C.c_double),
+        ("savestepinterval", C.c_int64),
+        ("maxiters", C.c_int64),
+        ("save_start", C.c_int32),
+        ("save_end", C.c_int32),
+        ("save_everystep", C.c_int32),
+        ("save_fields", C.c_int32),
+        ("term", TermDesc),
+        ("block", C.c_int32),
+        ("reserved2", C.c_int32),
+        ("budget_s", C.c_double),
+    ]
+
+
+_P = C.c_void_p
+_DP = C.POINTER(C.c_double)
+
+# (name, restype, argtypes) of every symbol include/tp_abi.h declares
+SIGNATURES = [
+    ("tp_abi_version", C.c_int, []),
+    ("tp_ctx_create", C.c_int, [C.c_int, C.POINTER(_P)]),
+    ("tp_ctx_destroy", None, [_P]),
+    ("tp_last_error", C.c_char_p, [_P]),
+    ("tp_field_create", C.c_int, [_P, C.POINTER(FieldDesc), C.POINTER(_P)]),
+    ("tp_field_destroy", None, [_P]),
+    ("tp_boris_run", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.POINTER(_P)]),
+    ("tp_boris_slots", C.c_int, [C.POINTER(RunDesc), _P, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    ("tp_boris_run_device", C.c_int,
+     [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
+    ("tp_gc_run", C.c_int, [_P, C.POINTER(GCDesc), _P, _P, _P, _P, _P, _P, _P, _P, C.c_int64, C.POINTER(_P)]),
+    ("tp_gc_prepare", C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_double, C.c_double, C.c_double, _P, _P]),
+    ("tp_result_info", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    ("tp_result_copy", C.c_int, [_P, _P, _P, _P, _P, _P]),
+    ("tp_result_elapsed_ms", C.c_int, [_P, _DP]),
+    ("tp_result_destroy", None, [_P]),
+]
+
+_lib = None
+
+
+def load_library(path: Path | None = None) -> C.CDLL:
+    """Load libtpb200.so (built in-tree by build_ext.py) and bind its symbols."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise ImportError(
+            f"{p} is missing: build it with `python testparticle.jl_b200/build_ext.py` "
+            "(the B200 library has no CPU fallback)")
+    lib = C.CDLL(str(p))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.tp_abi_version() != TP_ABI_VERSION:
+        raise ImportError("libtpb200.so ABI version mismatch")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    return [s[0] for s in SIGNATURES]

@@ -1,0 +1,675 @@
+// boris_fp32c.cu -- float32 push with compensated positions (TP_PREC_FP32C).
+//
+// Same algorithms and save semantics as boris_fp64.cu, with:
+//  * positions as unevaluated float pairs (hi, lo): every update x += v*dt is
+//    Knuth's TwoSum of hi and the increment followed by Dekker's Fast2Sum
+//    renormalisation, so the position carries ~48 significant bits;
+//  * on axes where every field is a periodic grid (and no spatial
+//    termination predicate is set) hi is kept inside [x0, x0 + L) with an
+//    integer wrap count, so the cell fraction is computed from a small
+//    number and stays exact to ~1e-8 cells even for drifting particles;
+//  * E, B, velocity and the rotation factors in float (rotation with correctly
+//    rounded division, no approximate reciprocals);
+//  * MultistepBoris in closed form without atan/sincos: with tau = |t_n|,
+//    (1 + i tau)^n = zr + i tau q gives cos/sin of n*atan(tau), and the
+//    coefficients of multistep_boris.jl:116-119 become
+//      c1 = (zr^2 - tau^2 q^2)/A, c2 = 2 zr q / A, c3 = 2 q^2 / A, c6 = 2 R / A
+//    with A = (1 + tau^2)^n and R = (n A - zr q) / tau^2 built by the
+//    recurrence R_{k+1} = R_k + (k+1) A_k + 2 q_k^2 + zr_k q_k, which is free
+//    of the cancellation the Taylor branch (multistep_boris.jl:99-108) guards;
+//  * time t, the adaptive step dt = C/|B| and the end-of-span clipping in
+//    float64 so that step decisions follow the float64 controller.
+#include "tp_device.cuh"
+#include "tp_launch.h"
+
+namespace tpb {
+
+namespace {
+
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Compensated position: x = hi + lo + w * L (w only on wrapped axes)
+struct CPos {
+    float hi[3], lo[3];
+    int w[3];
+};
+
+// TwoSum (Knuth) + Fast2Sum (Dekker): (hi, lo) += d
+__device__ __forceinline__ void cadd(float& hi, float& lo, float d) {
+    float s = __fadd_rn(hi, d);
+    float bb = __fsub_rn(s, hi);
+    float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(d, bb));
+    e = __fadd_rn(e, lo);
+    float h = __fadd_rn(s, e);
+    lo = __fsub_rn(e, __fsub_rn(h, s));
+    hi = h;
+}
+
+__device__ __forceinline__ double cpos_value(const BorisArgs& a, const CPos& p, int c) {
+    double x = (double)p.hi[c] + (double)p.lo[c];
+    if (a.wrap[c]) x += (double)p.w[c] * a.wrapL[c];
+    return x;
+}
+
+__device__ __forceinline__ void cpos_init(const BorisArgs& a, CPos& p, const double* x) {
+    for (int c = 0; c < 3; ++c) {
+        double v = x[c];
+        p.w[c] = 0;
+        if (a.wrap[c]) {
+            double k = floor((v - a.wrap0[c]) / a.wrapL[c]);
+            p.w[c] = (int)k;
+            v = v - k * a.wrapL[c];
+        }
+        p.hi[c] = (float)v;
+        p.lo[c] = (float)(v - (double)p.hi[c]);
+    }
+}
+
+__device__ __forceinline__ void cpos_push(const BorisArgs& a, CPos& p, F3 v, float dt) {
+    float d[3] = {v.x * dt, v.y * dt, v.z * dt};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        cadd(p.hi[c], p.lo[c], d[c]);
+        if (a.wrap[c]) {
+            float x0 = (float)a.wrap0[c];
+            float L = (float)a.wrapL[c];
+            if (p.hi[c] >= x0 + L) {
+                cadd(p.hi[c], p.lo[c], -L);
+                p.w[c] += 1;
+            } else if (p.hi[c] < x0) {
+                cadd(p.hi[c], p.lo[c], L);
+                p.w[c] -= 1;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fields
+struct AxF {
+    int i0, i1;
+    float f;
+};
+
+// cell index and fraction from the compensated coordinate
+__device__ __forceinline__ bool axis32(const DevField& g, int a, float hi, float lo, AxF& o) {
+    float d = hi - g.x0f[a];
+    float fl = floorf(d * g.idxf[a]);
+    float rem = fmaf(-fl, g.dxf[a], d) + lo;
+    float f = rem * g.idxf[a];
+    if (f < 0.0f) {
+        fl -= 1.0f;
+        f += 1.0f;
+    } else if (f >= 1.0f) {
+        fl += 1.0f;
+        f -= 1.0f;
+    }
+    int na = g.n[a];
+    if (g.bc == TP_BC_PERIODIC) {
+        int i = (int)fl % na;
+        if (i < 0) i += na;
+        o.i0 = i;
+        o.i1 = (i + 1 == na) ? 0 : i + 1;
+        o.f = f;
+        return true;
+    }
+    float u = fl + f;
+    float umax = (float)(na - 1);
+    if (g.bc == TP_BC_CLAMP) {
+        if (u < 0.0f) {
+            fl = 0.0f;
+            f = 0.0f;
+        } else if (u > umax) {
+            fl = umax;
+            f = 0.0f;
+        }
+    } else if (!(u >= 0.0f && u <= umax)) {
+        return false;
+    }
+    int i = (int)fl;
+    if (i > na - 2) {
+        f += (float)(i - (na - 2));
+        i = na - 2;
+    }
+    o.i0 = i;
+    o.i1 = i + 1;
+    o.f = f;
+    return true;
+}
+
+__device__ __forceinline__ float lerp32(float a, float b, float f) { return fmaf(f, b - a, a); }
+
+__device__ __forceinline__ F3 nanf3() {
+    float q = __int_as_float(0x7fc00000);
+    return {q, q, q};
+}
+
+__device__ __forceinline__ bool axes32(const DevField& g, const CPos& p, AxF& ax, AxF& ay, AxF& az) {
+    bool ok = axis32(g, 0, p.hi[0], p.lo[0], ax);
+    ok = axis32(g, 1, p.hi[1], p.lo[1], ay) && ok;
+    ok = axis32(g, 2, p.hi[2], p.lo[2], az) && ok;
+    return ok;
+}
+
+__device__ __forceinline__ F3 xyz(float4 q) { return {q.x, q.y, q.z}; }
+
+__device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, F3 v101, F3 v011,
+                                   F3 v111, const AxF& ax, const AxF& ay, const AxF& az) {
+    F3 o;
+#define TPB_TRI32(c)                                                       \
+    {                                                                      \
+        float c0 = lerp32(lerp32(v000.c, v100.c, ax.f), lerp32(v010.c, v110.c, ax.f), ay.f); \
+        float c1 = lerp32(lerp32(v001.c, v101.c, ax.f), lerp32(v011.c, v111.c, ax.f), ay.f); \
+        o.c = lerp32(c0, c1, az.f);                                        \
+    }
+    TPB_TRI32(x)
+    TPB_TRI32(y)
+    TPB_TRI32(z)
+#undef TPB_TRI32
+    return o;
+}
+
+__device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
+    AxF ax, ay, az;
+    if (!axes32(g, p, ax, ay, az)) return nanf3();
+    const float4* T = g.tab32;
+    const int nx = g.n[0], nxy = g.n[0] * g.n[1];
+    int j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+    F3 v000 = xyz(__ldg(T + ax.i0 + j0 + k0)), v100 = xyz(__ldg(T + ax.i1 + j0 + k0));
+    F3 v010 = xyz(__ldg(T + ax.i0 + j1 + k0)), v110 = xyz(__ldg(T + ax.i1 + j1 + k0));
+    F3 v001 = xyz(__ldg(T + ax.i0 + j0 + k1)), v101 = xyz(__ldg(T + ax.i1 + j0 + k1));
+    F3 v011 = xyz(__ldg(T + ax.i0 + j1 + k1)), v111 = xyz(__ldg(T + ax.i1 + j1 + k1));
+    return tri3(v000, v100, v010, v110, v001, v101, v011, v111, ax, ay, az);
+}
+
+__device__ __forceinline__ F3 analytic_eval32(const DevField& f, const CPos& p, double t) {
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            return {f.vf[0], f.vf[1], f.vf[2]};
+        case TP_FIELD_AFFINE: {
+            float x = p.hi[0], y = p.hi[1], z = p.hi[2], tf = (float)t;
+            return {f.vf[0] + f.Jf[0] * x + f.Jf[1] * y + f.Jf[2] * z + f.ratef[0] * tf,
+                    f.vf[1] + f.Jf[3] * x + f.Jf[4] * y + f.Jf[5] * z + f.ratef[1] * tf,
+                    f.vf[2] + f.Jf[6] * x + f.Jf[7] * y + f.Jf[8] * z + f.ratef[2] * tf};
+        }
+        case TP_FIELD_DIPOLE: {
+            F3 d{(p.hi[0] - f.cf[0]) + p.lo[0], (p.hi[1] - f.cf[1]) + p.lo[1],
+                 (p.hi[2] - f.cf[2]) + p.lo[2]};
+            F3 m{f.mf[0], f.mf[1], f.mf[2]};
+            float d2 = dot(d, d);
+            float inv = rsqrtf(d2);
+            float inv2 = 1.0f / d2;
+            float inv3 = inv * inv2;
+            float mr = dot(m, d) * inv2;  // (m.rhat)/|d|
+            float k = f.coeff * inv3;
+            return {k * (3.0f * mr * d.x - m.x), k * (3.0f * mr * d.y - m.y),
+                    k * (3.0f * mr * d.z - m.z)};
+        }
+        default:
+            return {0.0f, 0.0f, 0.0f};
+    }
+}
+
+template <bool PACKED_ONLY = false>
+__device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
+    if (PACKED_ONLY || F.eb32) {
+        AxF ax, ay, az;
+        if (!axes32(F.B, p, ax, ay, az)) {
+            E = nanf3();
+            B = E;
+            return;
+        }
+        const float4* T = F.eb32;
+        const int nx = F.B.n[0], nxy = F.B.n[0] * F.B.n[1];
+        int j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+        int n000 = 2 * (ax.i0 + j0 + k0), n100 = 2 * (ax.i1 + j0 + k0);
+        int n010 = 2 * (ax.i0 + j1 + k0), n110 = 2 * (ax.i1 + j1 + k0);
+        int n001 = 2 * (ax.i0 + j0 + k1), n101 = 2 * (ax.i1 + j0 + k1);
+        int n011 = 2 * (ax.i0 + j1 + k1), n111 = 2 * (ax.i1 + j1 + k1);
+        // all 16 loads issued before any use: 8 aligned 32-byte sectors
+        float4 e000 = __ldg(T + n000), b000 = __ldg(T + n000 + 1);
+        float4 e100 = __ldg(T + n100), b100 = __ldg(T + n100 + 1);
+        float4 e010 = __ldg(T + n010), b010 = __ldg(T + n010 + 1);
+        float4 e110 = __ldg(T + n110), b110 = __ldg(T + n110 + 1);
+        float4 e001 = __ldg(T + n001), b001 = __ldg(T + n001 + 1);
+        float4 e101 = __ldg(T + n101), b101 = __ldg(T + n101 + 1);
+        float4 e011 = __ldg(T + n011), b011 = __ldg(T + n011 + 1);
+        float4 e111 = __ldg(T + n111), b111 = __ldg(T + n111 + 1);
+        E = tri3(xyz(e000), xyz(e100), xyz(e010), xyz(e110), xyz(e001), xyz(e101), xyz(e011),
+                 xyz(e111), ax, ay, az);
+        B = tri3(xyz(b000), xyz(b100), xyz(b010), xyz(b110), xyz(b001), xyz(b101), xyz(b011),
+                 xyz(b111), ax, ay, az);
+        return;
+    }
+    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32(F.E, p) : analytic_eval32(F.E, p, t);
+    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32(F.B, p) : analytic_eval32(F.B, p, t);
+}
+
+template <int FK>
+__device__ __forceinline__ void eval_EB32t(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
+    if (FK == FK_ANALYTIC) {
+        E = analytic_eval32(F.E, p, t);
+        B = analytic_eval32(F.B, p, t);
+    } else if (FK == FK_EBGRID) {
+        eval_EB32<true>(F, p, t, E, B);
+    } else {
+        eval_EB32<false>(F, p, t, E, B);
+    }
+}
+
+__device__ __forceinline__ bool fields_static32(const DevFields& F) {
+    bool e = !(F.E.kind == TP_FIELD_AFFINE &&
+               (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
+    bool b = !(F.B.kind == TP_FIELD_AFFINE &&
+               (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
+    return e && b;
+}
+
+// ---------------------------------------------------------------- updates
+// Boris rotation (boris.jl:19-31) in float; h = q2m*dt/2
+__device__ __forceinline__ F3 boris_rot32(F3 v, F3 E, F3 B, float h) {
+    F3 t = h * B;
+    float tm2 = dot(t, t);
+    float sc = __fdiv_rn(2.0f, 1.0f + tm2);
+    F3 s = sc * t;
+    F3 he = h * E;
+    F3 vm = v + he;
+    F3 vp = vm + cross(vm, t);
+    F3 vpl = vm + cross(vp, s);
+    return vpl + he;
+}
+
+// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form; factor = q2m*dt/(2n)
+__device__ __forceinline__ F3 multistep_rot32(F3 v, F3 E, F3 B, float factor, int N, int n) {
+    F3 t_n = factor * B;
+    F3 e_n = factor * E;
+    if (N != 2) {
+        float tm2 = dot(t_n, t_n);
+        float f_N, e_corr;
+        if (N == 4) {
+            f_N = 1.0f + tm2 * (1.0f / 3.0f);
+            e_corr = -1.0f / 3.0f;
+        } else {
+            f_N = 1.0f + tm2 * (1.0f / 3.0f) + 2.0f * tm2 * tm2 * (1.0f / 15.0f);
+            e_corr = -1.0f / 3.0f - 2.0f * tm2 * (1.0f / 15.0f);
+        }
+        float edt = dot(e_n, t_n);
+        e_n = f_N * e_n + (e_corr * edt) * t_n;
+        t_n = f_N * t_n;
+    }
+    float s = dot(t_n, t_n);
+    float zr = 1.0f, q = 0.0f, A = 1.0f, R = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        R = R + (float)(k + 1) * A + 2.0f * q * q + zr * q;
+        float nzr = zr - s * q;
+        q = zr + q;
+        zr = nzr;
+        A = A * (1.0f + s);
+    }
+    float invA = __fdiv_rn(1.0f, A);
+    float c1 = (zr * zr - s * q * q) * invA;
+    float c2 = 2.0f * zr * q * invA;
+    float c3 = 2.0f * q * q * invA;
+    float c6 = 2.0f * R * invA;
+    float vdt = dot(v, t_n), edt = dot(e_n, t_n);
+    F3 vxt = cross(v, t_n), ext = cross(e_n, t_n);
+    return c1 * v + c2 * vxt + (c3 * vdt) * t_n + c2 * e_n + c3 * ext + (c6 * edt) * t_n;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ F3 vel32(F3 v, F3 E, F3 B, const BorisArgs& a, double dt) {
+    if (MULTI) return multistep_rot32(v, E, B, (float)(a.q2m * dt / (double)(2 * a.nsub)), a.order, a.nsub);
+    return boris_rot32(v, E, B, (float)(a.q2m * 0.5 * dt));
+}
+
+__device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, F3 v, double t) {
+    const DevTerm& T = a.term;
+    int f = T.flags;
+    if (f & TP_TERM_NAN)
+        if (isnan(p.hi[0]) || isnan(p.hi[1]) || isnan(p.hi[2]) || isnan(v.x) || isnan(v.y) ||
+            isnan(v.z))
+            return true;
+    if (f & (TP_TERM_SHELL | TP_TERM_BOX)) {
+        double x = cpos_value(a, p, 0), y = cpos_value(a, p, 1), z = cpos_value(a, p, 2);
+        if (f & TP_TERM_SHELL) {
+            double rr = sqrt((x * x + y * y) + z * z);
+            if (rr < T.rmin || rr > T.rmax) return true;
+        }
+        if (f & TP_TERM_BOX) {
+            if (x < T.lo[0] || x > T.hi[0] || y < T.lo[1] || y > T.hi[1] || z < T.lo[2] ||
+                z > T.hi[2])
+                return true;
+        }
+    }
+    if (f & TP_TERM_TIME)
+        if (t > T.tmax) return true;
+    return false;
+}
+
+template <int FK>
+struct Saver32 {
+    const BorisArgs& a;
+    int W;
+    __device__ Saver32(const BorisArgs& a_) : a(a_), W(a_.save_fields ? 12 : 6) {}
+    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, F3 v, double t) const {
+        if (k >= a.nslots) {
+            set_status(a.status, TP_E_OVERFLOW);
+            return;
+        }
+        const int64_t n = a.n;
+        a.t_out[k * n + i] = t;
+        double* u = a.u_out + (k * W) * n + i;
+        u[0 * n] = cpos_value(a, p, 0);
+        u[1 * n] = cpos_value(a, p, 1);
+        u[2 * n] = cpos_value(a, p, 2);
+        u[3 * n] = (double)v.x;
+        u[4 * n] = (double)v.y;
+        u[5 * n] = (double)v.z;
+        if (W == 12) {
+            F3 E, B;
+            eval_EB32t<FK>(a.f, p, t, E, B);
+            u[6 * n] = E.x;
+            u[7 * n] = E.y;
+            u[8 * n] = E.z;
+            u[9 * n] = B.x;
+            u[10 * n] = B.y;
+            u[11 * n] = B.z;
+        }
+    }
+};
+
+template <bool QUEUE>
+__device__ __forceinline__ int64_t next_particle32(const BorisArgs& a, int64_t& first) {
+    if (!QUEUE) {
+        int64_t g = first;
+        first = a.n;
+        return g;
+    }
+    return (int64_t)atomicAdd(a.queue, 1ULL);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- fixed step
+template <bool MULTI, bool QUEUE, int FK>
+__global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
+    const Saver32<FK> S(a);
+    const bool stat = fields_static32(a.f);
+    const uint64_t t_start = globaltimer_ns();
+    int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+
+    int64_t i = -1;
+    CPos p;
+    F3 v{0, 0, 0}, v_prev{0, 0, 0};
+    double dt = 0, t = 0, t1 = 0, t_last = 0;
+    float dtf = 0;
+    int64_t it = 0, nt = 0, nout = 0, iout = 0, csave = 0;
+    bool terminated = false;
+
+    for (;;) {
+        if (i < 0) {
+            i = next_particle32<QUEUE>(a, first);
+            if (i >= a.n) break;
+            dt = a.dt_i ? a.dt_i[i] : a.dt;
+            t1 = a.tend_i ? a.tend_i[i] : a.t1;
+            nt = (fabs(dt) < 10.0 * 2.220446049250313e-16) ? -1 : jl_round((t1 - a.t0) / dt);
+            if (nt < 0 && fabs(dt) >= 10.0 * 2.220446049250313e-16) nt = -nt;
+            if (nt < 0 || nt > a.maxiters) {
+                set_status(a.status, TP_E_ARG);
+                a.nsaved[i] = 0;
+                a.retcode[i] = TP_RET_DEFAULT;
+                a.nsteps[i] = 0;
+                i = -1;
+                continue;
+            }
+            dtf = (float)dt;
+            nout = calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
+            const double* u0 = a.u0 + 6 * i;
+            cpos_init(a, p, u0);
+            v = {(float)u0[3], (float)u0[4], (float)u0[5]};
+            iout = 0;
+            if (a.save_start) {
+                a.t_out[i] = a.t0;  // save_start writes u0 exactly (slot 0)
+                if (a.nslots > 0) {
+                    const int W = S.W;
+                    double* u = a.u_out + i;
+                    for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
+                    if (W == 12) {
+                        F3 E, B;
+                        eval_EB32t<FK>(a.f, p, a.t0, E, B);
+                        u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                        u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                    }
+                } else {
+                    set_status(a.status, TP_E_OVERFLOW);
+                }
+                t_last = a.t0;
+                iout = 1;
+            }
+            F3 E, B;
+            eval_EB32t<FK>(a.f, p, a.t0, E, B);
+            v = vel32<MULTI>(v, E, B, a, -0.5 * dt);
+            it = 1;
+            t = a.t0 - 0.5 * dt;
+            csave = 0;
+            terminated = false;
+        }
+
+        bool done = it > nt;
+        if (!done) {
+            v_prev = v;
+            t += dt;
+            F3 E, B;
+            eval_EB32t<FK>(a.f, p, t, E, B);
+            v = vel32<MULTI>(v, E, B, a, dt);
+            CPos pn = p;
+            cpos_push(a, pn, v, dtf);
+            if (a.term.flags && outside32(a, pn, v, t + 0.5 * dt)) {
+                terminated = true;
+                done = true;
+            } else {
+                if (a.save_everystep && it > 1 && csave == 0) {
+                    iout += 1;
+                    if (iout <= nout) {
+                        double t_cur = t - 0.5 * dt;
+                        if (!stat) eval_EB32t<FK>(a.f, p, t_cur, E, B);
+                        F3 vs = vel32<MULTI>(v_prev, E, B, a, 0.5 * dt);
+                        S.save(i, iout - 1, p, vs, t_cur);
+                        t_last = t_cur;
+                    }
+                }
+                p = pn;
+                it += 1;
+                csave += 1;
+                if (csave == a.ssi) csave = 0;
+                done = it > nt;
+                if ((it & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                    set_status(a.status, TP_E_TIMEOUT);
+                    done = true;
+                }
+            }
+        }
+        if (done) {
+            if (terminated) v = v_prev;
+            int64_t final_step = it - 1;
+            bool save_final = a.save_end ||
+                              (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
+            if (iout < nout && save_final) {
+                double t_final = (final_step == nt) ? t1 : fma((double)final_step, dt, a.t0);
+                if (iout == 0 || t_last < t_final) {
+                    double dt_final = t_final - fma((double)final_step - 0.5, dt, a.t0);
+                    F3 E, B;
+                    eval_EB32t<FK>(a.f, p, t_final, E, B);
+                    F3 vf = vel32<MULTI>(v, E, B, a, dt_final);
+                    S.save(i, iout, p, vf, t_final);
+                    iout += 1;
+                }
+            }
+            a.nsaved[i] = (int32_t)iout;
+            a.retcode[i] = (int8_t)((iout < nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
+            a.nsteps[i] = final_step;
+            i = -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- adaptive
+template <bool MULTI, bool QUEUE, int FK>
+__global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
+    const Saver32<FK> S(a);
+    const bool stat = fields_static32(a.f);
+    const uint64_t t_start = globaltimer_ns();
+    int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const double twopi = 6.283185307179586;
+
+    int64_t i = -1;
+    CPos p;
+    F3 v{0, 0, 0}, E{0, 0, 0}, B{0, 0, 0};
+    double t = 0, t1 = 0, dt = 0, C = 0, ttotal = 0, t_last = 0;
+    int64_t it = 0, iout = 0, steps = 0;
+    bool ssf = false;
+    int ret = TP_RET_SUCCESS;
+
+    for (;;) {
+        if (i < 0) {
+            i = next_particle32<QUEUE>(a, first);
+            if (i >= a.n) break;
+            t1 = a.tend_i ? a.tend_i[i] : a.t1;
+            double dtt = t1 - a.t0;
+            double sgn = dtt > 0 ? 1.0 : (dtt < 0 ? -1.0 : 0.0);
+            C = (twopi * a.safety * sgn) / fabs(a.q2m);
+            const double* u0 = a.u0 + 6 * i;
+            cpos_init(a, p, u0);
+            v = {(float)u0[3], (float)u0[4], (float)u0[5]};
+            t = a.t0;
+            ttotal = dtt;
+            iout = 0;
+            eval_EB32t<FK>(a.f, p, t, E, B);
+            if (a.save_start) {
+                if (a.nslots > 0) {
+                    a.t_out[i] = t;
+                    double* u = a.u_out + i;
+                    for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
+                    if (S.W == 12) {
+                        u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                        u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                    }
+                } else {
+                    set_status(a.status, TP_E_OVERFLOW);
+                }
+                t_last = t;
+                iout = 1;
+            }
+            dt = C / sqrt((double)dot(B, B));
+            v = vel32<MULTI>(v, E, B, a, -0.5 * dt);
+            it = 1;
+            steps = 0;
+            ssf = a.save_end;
+            ret = TP_RET_SUCCESS;
+        }
+
+        bool done = !(fabs(t - a.t0) < fabs(ttotal));
+        if (!done && a.step_cap > 0 && steps >= a.step_cap) {
+            ret = TP_RET_MAXITERS;
+            done = true;
+        }
+        if (!done) {
+            if (!stat) eval_EB32t<FK>(a.f, p, t, E, B);
+            if (fabs(t + dt - a.t0) > fabs(ttotal)) {
+                double dt_step = t1 - t;
+                v = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                v = vel32<MULTI>(v, E, B, a, -0.5 * dt_step);
+                dt = dt_step;
+            }
+            if (a.save_everystep && (it - 1) > 0 && (it - 1) % a.ssi == 0) {
+                F3 vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                S.save(i, iout, p, vs, t);
+                t_last = t;
+                iout += 1;
+            }
+            F3 Em = E, Bm = B;
+            if (!stat) eval_EB32t<FK>(a.f, p, t + 0.5 * dt, Em, Bm);
+            F3 v_new = vel32<MULTI>(v, Em, Bm, a, dt);
+            CPos pn = p;
+            cpos_push(a, pn, v_new, (float)dt);
+            double t_next = t + dt;
+            if (a.term.flags && outside32(a, pn, v_new, t_next)) {
+                ssf = true;
+                ret = TP_RET_TERMINATED;
+                done = true;
+            } else {
+                p = pn;
+                t = t_next;
+                v = v_new;
+                steps += 1;
+                eval_EB32t<FK>(a.f, p, t, E, B);
+                double dt_new = C / sqrt((double)dot(B, B));
+                v = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                v = vel32<MULTI>(v, E, B, a, -0.5 * dt_new);
+                dt = dt_new;
+                it += 1;
+                if (a.save_everystep && (it - 1) % a.ssi == 0) ssf = true;
+                if ((steps & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                    set_status(a.status, TP_E_TIMEOUT);
+                    ret = TP_RET_DEFAULT;
+                    done = true;
+                }
+            }
+        }
+        if (done) {
+            if (ssf && (iout == 0 || t_last != t)) {
+                if (!stat) eval_EB32t<FK>(a.f, p, t, E, B);
+                F3 vf = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                S.save(i, iout, p, vf, t);
+                iout += 1;
+            }
+            a.nsaved[i] = (int32_t)iout;
+            a.retcode[i] = (int8_t)ret;
+            a.nsteps[i] = steps;
+            i = -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+template <bool MULTI, bool QUEUE, int FK>
+static const void* kernel_ptr32(bool adaptive) {
+    return adaptive ? (const void*)k_adaptive32c<MULTI, QUEUE, FK> : (const void*)k_fixed32c<MULTI, QUEUE, FK>;
+}
+
+template <bool MULTI, bool QUEUE>
+static const void* pick_fk32(bool adaptive, int fk) {
+    if (fk == FK_ANALYTIC) return kernel_ptr32<MULTI, QUEUE, FK_ANALYTIC>(adaptive);
+    if (fk == FK_EBGRID) return kernel_ptr32<MULTI, QUEUE, FK_EBGRID>(adaptive);
+    return kernel_ptr32<MULTI, QUEUE, FK_GENERIC>(adaptive);
+}
+
+static const void* select_kernel32(const BorisArgs& a, bool queue) {
+    const bool multi = a.alg == TP_ALG_MULTISTEP || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    const bool adaptive = a.alg == TP_ALG_ADAPTIVE || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    int fk = field_config_of(a.f);
+    if (multi) return queue ? pick_fk32<true, true>(adaptive, fk) : pick_fk32<true, false>(adaptive, fk);
+    return queue ? pick_fk32<false, true>(adaptive, fk) : pick_fk32<false, false>(adaptive, fk);
+}
+
+cudaError_t launch_boris_fp32c(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s) {
+    const void* k = select_kernel32(a, a.use_queue != 0);
+    void* args[] = {const_cast<BorisArgs*>(&a)};
+    return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
+}
+
+int occupancy_boris_fp32c(const BorisArgs& a, int block) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, select_kernel32(a, true), block, 0);
+    return nb;
+}
+
+}  // namespace tpb

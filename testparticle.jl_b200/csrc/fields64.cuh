@@ -1,0 +1,301 @@
+// fields64.cuh -- float64 field evaluation and Boris / Multistep velocity
+// updates.  Included only by translation units compiled with -fmad=false:
+// the expressions follow the reference's operation order without contraction,
+// and the places where the reference fuses (@muladd on scalars) call fma()
+// explicitly, so results equal the CPU restatement bit for bit wherever only
+// +, -, *, /, sqrt and fma are involved.
+#pragma once
+
+#include "tp_device.cuh"
+
+namespace tpb {
+
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ D3 operator/(D3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double dot(D3 a, D3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ double abs2sum(D3 a) { return (a.x * a.x + a.y * a.y) + a.z * a.z; }
+__device__ __forceinline__ double norm(D3 a) { return sqrt(abs2sum(a)); }
+
+// ---------------------------------------------------------------- grid axis
+// Per-axis cell index and fraction of the trilinear interpolant (the
+// FieldInterpolator of src/utility/interpolation.jl:217-235, boundary rules
+// FillExtrap(NaN) / ClampExtrap() / PeriodicBC(endpoint=:exclusive)).
+struct Ax {
+    int32_t i0, i1;
+    double f;
+};
+
+__device__ __forceinline__ bool grid_axis(const DevField& g, int a, double x, Ax& o) {
+    double u = (x - g.x0[a]) * g.inv_dx[a];
+    int32_t na = g.n[a];
+    if (g.bc == TP_BC_PERIODIC) {
+        double fl = floor(u);
+        o.f = u - fl;
+        long long i = (long long)fl % (long long)na;
+        if (i < 0) i += na;
+        o.i0 = (int32_t)i;
+        o.i1 = (o.i0 + 1 == na) ? 0 : o.i0 + 1;
+        return true;
+    }
+    double umax = (double)(na - 1);
+    if (g.bc == TP_BC_CLAMP) {
+        u = (u < 0.0) ? 0.0 : u;
+        u = (umax < u) ? umax : u;
+    } else if (!(u >= 0.0 && u <= umax)) {
+        return false;
+    }
+    double fl = floor(u);
+    long long i = (long long)fl;
+    if (i > na - 2) i = na - 2;
+    o.i0 = (int32_t)i;
+    o.i1 = o.i0 + 1;
+    o.f = u - (double)i;
+    return true;
+}
+
+__device__ __forceinline__ double lerp64(double a, double b, double f) { return a + f * (b - a); }
+
+// Load node `node` of a table with `stride` 4-vectors per node, at offset `off`.
+__device__ __forceinline__ D3 load_node(const void* tab, bool f64, int64_t idx) {
+    if (f64) {
+        const double2* p = reinterpret_cast<const double2*>(tab) + 2 * idx;
+        double2 a = __ldg(p), b = __ldg(p + 1);
+        return {a.x, a.y, b.x};
+    }
+    float4 q = __ldg(reinterpret_cast<const float4*>(tab) + idx);
+    return {(double)q.x, (double)q.y, (double)q.z};
+}
+
+// Trilinear interpolation from precomputed axes; `stride`/`off` select a
+// field inside an interleaved table (stride 2: E at off 0, B at off 1).
+__device__ __forceinline__ D3 tri64(const DevField& g, const void* tab, bool f64, int stride,
+                                    int off, const Ax& ax, const Ax& ay, const Ax& az) {
+    const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
+    int64_t j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+    D3 v000 = load_node(tab, f64, (ax.i0 + j0 + k0) * stride + off);
+    D3 v100 = load_node(tab, f64, (ax.i1 + j0 + k0) * stride + off);
+    D3 v010 = load_node(tab, f64, (ax.i0 + j1 + k0) * stride + off);
+    D3 v110 = load_node(tab, f64, (ax.i1 + j1 + k0) * stride + off);
+    D3 v001 = load_node(tab, f64, (ax.i0 + j0 + k1) * stride + off);
+    D3 v101 = load_node(tab, f64, (ax.i1 + j0 + k1) * stride + off);
+    D3 v011 = load_node(tab, f64, (ax.i0 + j1 + k1) * stride + off);
+    D3 v111 = load_node(tab, f64, (ax.i1 + j1 + k1) * stride + off);
+    D3 o;
+#define TPB_TRI(c)                                              \
+    {                                                           \
+        double c00 = lerp64(v000.c, v100.c, ax.f);              \
+        double c10 = lerp64(v010.c, v110.c, ax.f);              \
+        double c01 = lerp64(v001.c, v101.c, ax.f);              \
+        double c11 = lerp64(v011.c, v111.c, ax.f);              \
+        double c0 = lerp64(c00, c10, ay.f);                     \
+        double c1 = lerp64(c01, c11, ay.f);                     \
+        o.c = lerp64(c0, c1, az.f);                             \
+    }
+    TPB_TRI(x)
+    TPB_TRI(y)
+    TPB_TRI(z)
+#undef TPB_TRI
+    return o;
+}
+
+__device__ __forceinline__ D3 nan3() {
+    double q = __longlong_as_double(0x7ff8000000000000ULL);
+    return {q, q, q};
+}
+
+__device__ __forceinline__ bool grid_axes64(const DevField& g, D3 r, Ax& ax, Ax& ay, Ax& az) {
+    bool ok = grid_axis(g, 0, r.x, ax);
+    ok = grid_axis(g, 1, r.y, ay) && ok;
+    ok = grid_axis(g, 2, r.z, az) && ok;
+    return ok;
+}
+
+__device__ __forceinline__ D3 grid_eval64(const DevField& g, D3 r) {
+    Ax ax, ay, az;
+    if (!grid_axes64(g, r, ax, ay, az)) return nan3();
+    return tri64(g, g.tab, g.f64 != 0, 1, 0, ax, ay, az);
+}
+
+// Analytic fields: ZERO, UNIFORM, AFFINE, DIPOLE (order of the oracle).
+__device__ __forceinline__ D3 analytic_eval64(const DevField& f, D3 r, double t) {
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            return {f.v[0], f.v[1], f.v[2]};
+        case TP_FIELD_AFFINE: {
+            D3 o;
+            o.x = (f.v[0] + ((f.J[0] * r.x + f.J[1] * r.y) + f.J[2] * r.z)) + f.rate[0] * t;
+            o.y = (f.v[1] + ((f.J[3] * r.x + f.J[4] * r.y) + f.J[5] * r.z)) + f.rate[1] * t;
+            o.z = (f.v[2] + ((f.J[6] * r.x + f.J[7] * r.y) + f.J[8] * r.z)) + f.rate[2] * t;
+            return o;
+        }
+        case TP_FIELD_DIPOLE: {
+            D3 d = r - D3{f.c[0], f.c[1], f.c[2]};
+            D3 m{f.m[0], f.m[1], f.m[2]};
+            double dm = norm(d);
+            D3 rh = d / dm;
+            double mr = dot(m, rh);
+            double d3 = (dm * dm) * dm;
+            D3 s = (3.0 * mr) * rh - m;
+            return (f.coef * s) / d3;
+        }
+        default:
+            return {0.0, 0.0, 0.0};
+    }
+}
+
+__device__ __forceinline__ D3 field_eval64(const DevField& f, D3 r, double t) {
+    if (f.kind == TP_FIELD_GRID) return grid_eval64(f, r);
+    return analytic_eval64(f, r, t);
+}
+
+// E and B at one point (one gather pass when the two grids are interleaved).
+__device__ __forceinline__ void eval_EB64(const DevFields& F, D3 r, double t, D3& E, D3& B) {
+    if (F.eb) {
+        // both grids on one geometry: one axis computation, one gather pass
+        Ax ax, ay, az;
+        if (!grid_axes64(F.B, r, ax, ay, az)) {
+            E = nan3();
+            B = E;
+            return;
+        }
+        bool f64 = F.eb_f64 != 0;
+        E = tri64(F.B, F.eb, f64, 2, 0, ax, ay, az);
+        B = tri64(F.B, F.eb, f64, 2, 1, ax, ay, az);
+        return;
+    }
+    E = field_eval64(F.E, r, t);
+    B = field_eval64(F.B, r, t);
+}
+
+template <int FK>
+__device__ __forceinline__ void eval_EB64t(const DevFields& F, D3 r, double t, D3& E, D3& B) {
+    if (FK == FK_ANALYTIC) {
+        E = analytic_eval64(F.E, r, t);
+        B = analytic_eval64(F.B, r, t);
+    } else if (FK == FK_EBGRID) {
+        Ax ax, ay, az;
+        if (!grid_axes64(F.B, r, ax, ay, az)) {
+            E = nan3();
+            B = E;
+            return;
+        }
+        bool f64 = F.eb_f64 != 0;
+        E = tri64(F.B, F.eb, f64, 2, 0, ax, ay, az);
+        B = tri64(F.B, F.eb, f64, 2, 1, ax, ay, az);
+    } else {
+        E = field_eval64(F.E, r, t);
+        B = field_eval64(F.B, r, t);
+    }
+}
+
+__device__ __forceinline__ bool fields_static(const DevFields& F) {
+    bool e = !(F.E.kind == TP_FIELD_AFFINE &&
+               (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
+    bool b = !(F.B.kind == TP_FIELD_AFFINE &&
+               (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
+    return e && b;
+}
+
+// ---------------------------------------------------------------- updates
+// boris_velocity_update, src/boris/boris.jl:19-31, with qdt_2m = q2m*0.5*dt
+// (update_velocity, boris.jl:38-45)
+__device__ __forceinline__ D3 boris_rot64(D3 v, D3 E, D3 B, double q2m, double dt) {
+    double qdt_2m = q2m * 0.5 * dt;
+    D3 t_rotate = qdt_2m * B;
+    double t_mag2 = abs2sum(t_rotate);
+    D3 s_rotate = (2.0 * t_rotate) / (1.0 + t_mag2);
+    D3 vm = v + qdt_2m * E;
+    D3 vp_ = vm + cross(vm, t_rotate);
+    D3 vplus = vm + cross(vp_, s_rotate);
+    return vplus + qdt_2m * E;
+}
+
+// update_velocity_multistep, src/boris/multistep_boris.jl:65-142
+__device__ __forceinline__ D3 multistep_rot64(D3 v, D3 E, D3 B, double q2m, double dt, int N,
+                                              int n) {
+    double factor = q2m * dt / (double)(2 * n);
+    D3 t_n = factor * B;
+    D3 e_n = factor * E;
+    if (N != 2) {
+        double t_mag2 = abs2sum(t_n);
+        double f_N, e_corr;
+        if (N == 4) {
+            f_N = 1.0 + t_mag2 / 3.0;
+            e_corr = -1.0 / 3.0;
+        } else {
+            f_N = (1.0 + t_mag2 / 3.0) + 2.0 * t_mag2 * t_mag2 / 15.0;
+            e_corr = -1.0 / 3.0 - 2.0 * t_mag2 / 15.0;
+        }
+        double e_dot_t = dot(e_n, t_n);
+        e_n = f_N * e_n + (e_corr * e_dot_t) * t_n;
+        t_n = f_N * t_n;
+    }
+    double t_n_mag2 = abs2sum(t_n);
+    double t_n_mag = sqrt(t_n_mag2);
+    double c1, c2, c3, c6;
+    double nd = (double)n;
+    if (t_n_mag < 1.0e-4) {
+        c1 = fma(-(2.0 * nd * nd), t_n_mag2, 1.0);
+        double n_term1 = 2.0 * nd;
+        double n_term3 = 4.0 * nd * nd * nd;
+        c2 = fma(-((n_term1 + n_term3) / 3.0), t_n_mag2, n_term1);
+        c3 = fma(-((4.0 * nd * nd + 2.0 * nd * nd * nd * nd) / 3.0), t_n_mag2, 2.0 * nd * nd);
+        c6 = (n_term1 + n_term3) / 3.0;
+    } else {
+        double alpha = atan(t_n_mag);
+        double s, c;
+        sincos(nd * alpha, &s, &c);
+        double s2 = 2.0 * s * c;
+        c1 = fma(c, c, -(s * s));
+        c2 = s2 / t_n_mag;
+        c3 = 2.0 * s * s / t_n_mag2;
+        c6 = (2.0 * nd - c2) / t_n_mag2;
+    }
+    double v_dot_t = dot(v, t_n);
+    double e_dot_t = dot(e_n, t_n);
+    D3 v_cross_t = cross(v, t_n);
+    D3 e_cross_t = cross(e_n, t_n);
+    D3 out = c1 * v + c2 * v_cross_t;
+    out = out + (c3 * v_dot_t) * t_n;
+    out = out + c2 * e_n;
+    out = out + c3 * e_cross_t;
+    out = out + (c6 * e_dot_t) * t_n;
+    return out;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ D3 vel_update64(D3 v, D3 E, D3 B, double q2m, double dt, int N, int n) {
+    if (MULTI) return multistep_rot64(v, E, B, q2m, dt, N, n);
+    return boris_rot64(v, E, B, q2m, dt);
+}
+
+// isoutside(u, p, t) restated for the flag predicates of tp_term_desc
+__device__ __forceinline__ bool outside64(const DevTerm& T, D3 r, D3 v, double t) {
+    int f = T.flags;
+    if (f & TP_TERM_NAN)
+        if (isnan(r.x) || isnan(r.y) || isnan(r.z) || isnan(v.x) || isnan(v.y) || isnan(v.z))
+            return true;
+    if (f & TP_TERM_SHELL) {
+        double rr = sqrt((r.x * r.x + r.y * r.y) + r.z * r.z);
+        if (rr < T.rmin || rr > T.rmax) return true;
+    }
+    if (f & TP_TERM_BOX) {
+        if (r.x < T.lo[0] || r.x > T.hi[0]) return true;
+        if (r.y < T.lo[1] || r.y > T.hi[1]) return true;
+        if (r.z < T.lo[2] || r.z > T.hi[2]) return true;
+    }
+    if (f & TP_TERM_TIME)
+        if (t > T.tmax) return true;
+    return false;
+}
+
+}  // namespace tpb

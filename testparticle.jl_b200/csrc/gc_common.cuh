@@ -1,0 +1,470 @@
+// gc_common.cuh -- guiding-centre RK4 / RK45 drivers, templated on the
+// right-hand side.  The state, the Runge-Kutta combinations, the error norm
+// and the step-size controller are float64 in every variant; the RHS
+// (get_gc_derivatives, src/equations.jl:329-360) is float64 (RHS64, the
+// drop-in) or float32 (RHS32).
+//
+//   k_rk4<RHS, QUEUE>   _rk4!  (src/gc/rk4_gc.jl:27-130)
+//   k_rk45<RHS, QUEUE>  _rk45! (src/gc/rk45_gc.jl:52-173)
+#pragma once
+
+#include "fields64.cuh"
+#include "tp_launch.h"
+
+namespace tpb {
+
+struct G4 {
+    double y[4];
+};
+__device__ __forceinline__ G4 gadd(const G4& a, const G4& b) {
+    return {{a.y[0] + b.y[0], a.y[1] + b.y[1], a.y[2] + b.y[2], a.y[3] + b.y[3]}};
+}
+__device__ __forceinline__ G4 gscale(double s, const G4& a) {
+    return {{s * a.y[0], s * a.y[1], s * a.y[2], s * a.y[3]}};
+}
+
+struct GCPar {
+    double q, q2m, mu;
+};
+
+// B and its Jacobian (row-major J[i][j] = dB_i/dx_j), float64, in the order
+// of the CPU restatement (the role of ForwardDiff in _get_B_jacobian,
+// src/utility/utility.jl:386-392)
+template <bool GRID>
+__device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
+    for (int k = 0; k < 9; ++k) J[k] = 0.0;
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            F = {f.v[0], f.v[1], f.v[2]};
+            return;
+        case TP_FIELD_AFFINE:
+            F = analytic_eval64(f, r, t);
+            for (int k = 0; k < 9; ++k) J[k] = f.J[k];
+            return;
+        case TP_FIELD_DIPOLE: {
+            F = analytic_eval64(f, r, t);
+            D3 d = r - D3{f.c[0], f.c[1], f.c[2]};
+            double d2 = abs2sum(d);
+            double dm = sqrt(d2);
+            double inv5 = 1.0 / ((d2 * d2) * dm);
+            double inv7 = inv5 / d2;
+            double md = dot(D3{f.m[0], f.m[1], f.m[2]}, d);
+            double dv[3] = {d.x, d.y, d.z};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double dij = (i == j) ? md : 0.0;
+                    J[3 * i + j] = f.coef * (3.0 * ((f.m[j] * dv[i] + dij) + f.m[i] * dv[j]) * inv5 -
+                                             15.0 * md * dv[i] * dv[j] * inv7);
+                }
+            return;
+        }
+        case TP_FIELD_GRID: {
+            if (!GRID) {
+                F = {0.0, 0.0, 0.0};
+                return;
+            }
+            Ax ax, ay, az;
+            if (!grid_axes64(f, r, ax, ay, az)) {
+                F = nan3();
+                for (int k = 0; k < 9; ++k) J[k] = F.x;
+                return;
+            }
+            F = tri64(f, f.tab, f.f64 != 0, 1, 0, ax, ay, az);
+            double sx = f.inv_dx[0], sy = f.inv_dx[1], sz = f.inv_dx[2];
+            if (f.bc == TP_BC_CLAMP) {
+                double ux = (r.x - f.x0[0]) * f.inv_dx[0], uy = (r.y - f.x0[1]) * f.inv_dx[1],
+                       uz = (r.z - f.x0[2]) * f.inv_dx[2];
+                if (ux < 0.0 || ux > (double)(f.n[0] - 1)) sx = 0.0;
+                if (uy < 0.0 || uy > (double)(f.n[1] - 1)) sy = 0.0;
+                if (uz < 0.0 || uz > (double)(f.n[2] - 1)) sz = 0.0;
+            }
+            const int64_t nx = f.n[0], nxy = (int64_t)f.n[0] * f.n[1];
+            int64_t j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+            bool f64 = f.f64 != 0;
+            D3 w000 = load_node(f.tab, f64, ax.i0 + j0 + k0), w100 = load_node(f.tab, f64, ax.i1 + j0 + k0);
+            D3 w010 = load_node(f.tab, f64, ax.i0 + j1 + k0), w110 = load_node(f.tab, f64, ax.i1 + j1 + k0);
+            D3 w001 = load_node(f.tab, f64, ax.i0 + j0 + k1), w101 = load_node(f.tab, f64, ax.i1 + j0 + k1);
+            D3 w011 = load_node(f.tab, f64, ax.i0 + j1 + k1), w111 = load_node(f.tab, f64, ax.i1 + j1 + k1);
+            double fx = ax.f, fy = ay.f, fz = az.f;
+#define TPB_GJ(c, row)                                                                  \
+    {                                                                                   \
+        double v000 = w000.c, v100 = w100.c, v010 = w010.c, v110 = w110.c;              \
+        double v001 = w001.c, v101 = w101.c, v011 = w011.c, v111 = w111.c;              \
+        double dx00 = v100 - v000, dx10 = v110 - v010, dx01 = v101 - v001, dx11 = v111 - v011; \
+        double dx0 = lerp64(dx00, dx10, fy), dx1 = lerp64(dx01, dx11, fy);              \
+        J[3 * row + 0] = lerp64(dx0, dx1, fz) * sx;                                     \
+        double c00 = lerp64(v000, v100, fx), c10 = lerp64(v010, v110, fx);              \
+        double c01 = lerp64(v001, v101, fx), c11 = lerp64(v011, v111, fx);              \
+        J[3 * row + 1] = lerp64(c10 - c00, c11 - c01, fz) * sy;                         \
+        double c0 = lerp64(c00, c10, fy), c1 = lerp64(c01, c11, fy);                    \
+        J[3 * row + 2] = (c1 - c0) * sz;                                                \
+    }
+            TPB_GJ(x, 0)
+            TPB_GJ(y, 1)
+            TPB_GJ(z, 2)
+#undef TPB_GJ
+            return;
+        }
+        default:
+            F = {0.0, 0.0, 0.0};
+            return;
+    }
+}
+
+template <bool GRID>
+__device__ __forceinline__ D3 field_val64(const DevField& f, D3 r, double t) {
+    if (GRID) return field_eval64(f, r, t);
+    return analytic_eval64(f, r, t);
+}
+
+// get_gc_derivatives (src/equations.jl:329-360), float64
+template <bool GRID>
+struct RHS64 {
+    static constexpr bool kGrid = GRID;
+    __device__ __forceinline__ G4 operator()(const DevFields& F, const G4& s, const GCPar& p,
+                                             double t) const {
+        D3 X{s.y[0], s.y[1], s.y[2]};
+        D3 E = field_val64<GRID>(F.E, X, t);
+        D3 B;
+        double J[9];
+        field_jac64<GRID>(F.B, X, t, B, J);
+        double Bmag = norm(B);
+        D3 bh = B / Bmag;
+        D3 gB{(J[0] * bh.x + J[3] * bh.y) + J[6] * bh.z, (J[1] * bh.x + J[4] * bh.y) + J[7] * bh.z,
+              (J[2] * bh.x + J[5] * bh.y) + J[8] * bh.z};
+        D3 curlB{J[7] - J[5], J[2] - J[6], J[3] - J[1]};
+        D3 curlb = (curlB + cross(bh, gB)) / Bmag;
+        D3 Bs = B + (s.y[3] / p.q2m) * curlb;
+        D3 Es = E - (p.mu / p.q) * gB;
+        double inv_Bpar = 1.0 / dot(bh, Bs);
+        D3 v = (s.y[3] * Bs + cross(Es, bh)) * inv_Bpar;
+        double du = dot((p.q2m * inv_Bpar) * Bs, Es);
+        return {{v.x, v.y, v.z, du}};
+    }
+};
+
+__device__ __forceinline__ bool outside_gc(const DevTerm& T, const G4& u, double t) {
+    int f = T.flags;
+    if (f & TP_TERM_NAN)
+        for (int k = 0; k < 4; ++k)
+            if (isnan(u.y[k])) return true;
+    if (f & TP_TERM_SHELL) {
+        double rr = sqrt((u.y[0] * u.y[0] + u.y[1] * u.y[1]) + u.y[2] * u.y[2]);
+        if (rr < T.rmin || rr > T.rmax) return true;
+    }
+    if (f & TP_TERM_BOX)
+        for (int c = 0; c < 3; ++c)
+            if (u.y[c] < T.lo[c] || u.y[c] > T.hi[c]) return true;
+    if (f & TP_TERM_TIME)
+        if (t > T.tmax) return true;
+    return false;
+}
+
+template <bool GRID>
+struct GCSaver {
+    const GCArgs& a;
+    int W;
+    __device__ GCSaver(const GCArgs& a_) : a(a_), W(a_.save_fields ? 10 : 4) {}
+    __device__ __forceinline__ void save(int64_t i, int64_t k, const G4& s, double t) const {
+        if (k >= a.nslots) {
+            set_status(a.status, TP_E_OVERFLOW);
+            return;
+        }
+        const int64_t n = a.n;
+        a.t_out[k * n + i] = t;
+        double* u = a.u_out + (k * W) * n + i;
+        for (int c = 0; c < 4; ++c) u[c * n] = s.y[c];
+        if (W == 10) {
+            D3 X{s.y[0], s.y[1], s.y[2]};
+            D3 E = field_val64<GRID>(a.f.E, X, t), B = field_val64<GRID>(a.f.B, X, t);
+            u[4 * n] = E.x;
+            u[5 * n] = E.y;
+            u[6 * n] = E.z;
+            u[7 * n] = B.x;
+            u[8 * n] = B.y;
+            u[9 * n] = B.z;
+        }
+    }
+};
+
+template <bool QUEUE>
+__device__ __forceinline__ int64_t gc_next(const GCArgs& a, int64_t& first) {
+    if (!QUEUE) {
+        int64_t g = first;
+        first = a.n;
+        return g;
+    }
+    return (int64_t)atomicAdd(a.queue, 1ULL);
+}
+
+__device__ __forceinline__ GCPar gc_par(const GCArgs& a, int64_t i) {
+    return {a.q_i ? a.q_i[i] : a.q, a.q2m_i ? a.q2m_i[i] : a.q2m, a.mu_i ? a.mu_i[i] : a.mu};
+}
+
+// update_rk4, src/gc/rk4_gc.jl:7-22
+template <class RHS>
+__device__ __forceinline__ G4 update_rk4(const RHS& f, const DevFields& F, const G4& y,
+                                         const GCPar& p, double dt, double t) {
+    G4 k1 = f(F, y, p, t);
+    G4 yt = gadd(y, gscale(0.5 * dt, k1));
+    G4 k2 = f(F, yt, p, t + 0.5 * dt);
+    yt = gadd(y, gscale(0.5 * dt, k2));
+    G4 k3 = f(F, yt, p, t + 0.5 * dt);
+    yt = gadd(y, gscale(dt, k3));
+    G4 k4 = f(F, yt, p, t + dt);
+    G4 sum = gadd(gadd(gadd(k1, gscale(2.0, k2)), gscale(2.0, k3)), k4);
+    return gscale(dt / 6.0, sum);
+}
+
+template <class RHS, bool QUEUE>
+__global__ void __launch_bounds__(256) k_rk4(GCArgs a) {
+    const RHS f;
+    const GCSaver<RHS::kGrid> S(a);
+    const uint64_t t_start = globaltimer_ns();
+    int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t i = -1, it = 0, iout = 0, nt = 0, nout = 0;
+    G4 xv;
+    GCPar p{0, 0, 0};
+    double t_last = 0, dt = 0, t1 = 0;
+    bool timed_out = false;
+    for (;;) {
+        if (i < 0) {
+            i = gc_next<QUEUE>(a, first);
+            if (i >= a.n) break;
+            p = gc_par(a, i);
+            const double* y0 = a.y0 + 4 * i;
+            xv = {{y0[0], y0[1], y0[2], y0[3]}};
+            dt = a.dt_i ? a.dt_i[i] : a.dt;
+            t1 = a.tend_i ? a.tend_i[i] : a.t1;
+            if (a.dt_i || a.tend_i) {
+                // _prepare_gc (gc_solver.jl:198-225) for this particle
+                nt = jl_round((t1 - a.t0) / dt);
+                if (nt > a.maxiters) nt = a.maxiters;
+                nout = (a.save_start ? 1 : 0);
+                if (a.save_everystep) {
+                    int64_t st = nt / a.ssi;
+                    bool last_is_step = (nt > 0) && (nt % a.ssi == 0);
+                    nout += st;
+                    if (!a.save_end && last_is_step) nout -= 1;
+                    if (a.save_end && !last_is_step) nout += 1;
+                } else if (a.save_end) {
+                    nout += 1;
+                }
+            } else {
+                nt = a.nt;
+                nout = a.nout;
+            }
+            iout = 0;
+            if (a.save_start) {
+                S.save(i, 0, xv, a.t0);
+                t_last = a.t0;
+                iout = 1;
+            }
+            it = 1;
+            timed_out = false;
+        }
+        bool done = !(it <= nt && it <= a.maxiters);
+        if (!done) {
+            double t = fma((double)(it - 1), dt, a.t0);
+            G4 dx = update_rk4(f, a.f, xv, p, dt, t);
+            G4 xn = gadd(xv, dx);
+            if (a.term.flags && outside_gc(a.term, xn, t + dt)) {
+                done = true;
+            } else {
+                xv = xn;
+                if (a.save_everystep && (it % a.ssi == 0)) {
+                    iout += 1;
+                    if (iout <= nout) {
+                        S.save(i, iout - 1, xv, t + dt);
+                        t_last = t + dt;
+                    }
+                }
+                it += 1;
+                done = !(it <= nt && it <= a.maxiters);
+                if ((it & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                    set_status(a.status, TP_E_TIMEOUT);
+                    timed_out = true;
+                    done = true;
+                }
+            }
+        }
+        if (done) {
+            int64_t final_step = it - 1;
+            bool sf = a.save_end || (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
+            if (iout < nout && sf) {
+                double t_final = (final_step == nt) ? t1 : fma((double)final_step, dt, a.t0);
+                if (iout == 0 || t_last < t_final) {
+                    S.save(i, iout, xv, t_final);
+                    iout += 1;
+                }
+            }
+            int ret;
+            if (timed_out)
+                ret = TP_RET_DEFAULT;
+            else if (it <= nt && it <= a.maxiters)
+                ret = TP_RET_TERMINATED;
+            else if (it > a.maxiters)
+                ret = TP_RET_MAXITERS;
+            else
+                ret = TP_RET_SUCCESS;
+            a.nsaved[i] = (int32_t)iout;
+            a.retcode[i] = (int8_t)ret;
+            a.nsteps[i] = final_step;
+            i = -1;
+        }
+    }
+}
+
+// update_dp5, src/gc/rk45_gc.jl:7-47 (tableau of rk45_gc.jl:9-20)
+template <class RHS>
+__device__ __forceinline__ void update_dp5(const RHS& f, const DevFields& F, const G4& y,
+                                           const GCPar& p, double dt, double t, G4& dy, G4& err) {
+    const double c2 = 1.0 / 5, c3 = 3.0 / 10, c4 = 4.0 / 5, c5 = 8.0 / 9;
+    const double a21 = 1.0 / 5;
+    const double a31 = 3.0 / 40, a32 = 9.0 / 40;
+    const double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
+    const double a51 = 19372.0 / 6561, a52 = -25360.0 / 2187, a53 = 64448.0 / 6561, a54 = -212.0 / 729;
+    const double a61 = 9017.0 / 3168, a62 = -355.0 / 33, a63 = 46732.0 / 5247, a64 = 49.0 / 176,
+                 a65 = -5103.0 / 18656;
+    const double a71 = 35.0 / 384, a72 = 0.0, a73 = 500.0 / 1113, a74 = 125.0 / 192,
+                 a75 = -2187.0 / 6784, a76 = 11.0 / 84;
+    const double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192, b5 = -2187.0 / 6784,
+                 b6 = 11.0 / 84;
+    const double e1 = 71.0 / 57600, e3 = -71.0 / 16695, e4 = 71.0 / 1920, e5 = -17253.0 / 339200,
+                 e6 = 22.0 / 525, e7 = -1.0 / 40;
+    G4 k1 = f(F, y, p, t);
+    G4 yt = gadd(y, gscale(dt, gscale(a21, k1)));
+    G4 k2 = f(F, yt, p, fma(c2, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gscale(a31, k1), gscale(a32, k2))));
+    G4 k3 = f(F, yt, p, fma(c3, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gscale(a41, k1), gscale(a42, k2)), gscale(a43, k3))));
+    G4 k4 = f(F, yt, p, fma(c4, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gscale(a51, k1), gscale(a52, k2)), gscale(a53, k3)),
+                                 gscale(a54, k4))));
+    G4 k5 = f(F, yt, p, fma(c5, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gscale(a61, k1), gscale(a62, k2)), gscale(a63, k3)),
+                                      gscale(a64, k4)),
+                                 gscale(a65, k5))));
+    G4 k6 = f(F, yt, p, fma(1.0, dt, t));
+    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(a71, k1), gscale(a72, k2)),
+                                                gscale(a73, k3)),
+                                           gscale(a74, k4)),
+                                      gscale(a75, k5)),
+                                 gscale(a76, k6))));
+    G4 k7 = f(F, yt, p, t + dt);
+    dy = gscale(dt, gadd(gadd(gadd(gadd(gscale(b1, k1), gscale(b3, k3)), gscale(b4, k4)),
+                              gscale(b5, k5)),
+                         gscale(b6, k6)));
+    err = gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(e1, k1), gscale(e3, k3)), gscale(e4, k4)),
+                                    gscale(e5, k5)),
+                               gscale(e6, k6)),
+                          gscale(e7, k7)));
+}
+
+template <class RHS, bool QUEUE>
+__global__ void __launch_bounds__(256) k_rk45(GCArgs a) {
+    const RHS f;
+    const GCSaver<RHS::kGrid> S(a);
+    const uint64_t t_start = globaltimer_ns();
+    int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const double safety = 0.9, max_growth = 5.0, min_growth = 0.2;
+    int64_t i = -1, iout = 0, steps = 0, attempts = 0;
+    G4 xv;
+    GCPar p{0, 0, 0};
+    double t = 0, dt = 0, t_last = 0, t1 = 0;
+    int ret = TP_RET_SUCCESS;
+    for (;;) {
+        if (i < 0) {
+            i = gc_next<QUEUE>(a, first);
+            if (i >= a.n) break;
+            p = gc_par(a, i);
+            const double* y0 = a.y0 + 4 * i;
+            xv = {{y0[0], y0[1], y0[2], y0[3]}};
+            t = a.t0;
+            t1 = a.tend_i ? a.tend_i[i] : a.t1;
+            if (a.dt_i) {
+                dt = a.dt_i[i];
+            } else if (!a.dt_given) {
+                D3 R{xv.y[0], xv.y[1], xv.y[2]};
+                double Bmag = norm(field_val64<RHS::kGrid>(a.f.B, R, t));
+                if (Bmag == 0.0 || p.q2m == 0.0) {
+                    dt = 1.0e-6;
+                } else {
+                    double omega = fabs(p.q2m * Bmag);
+                    dt = 0.5 * 6.283185307179586 / omega;
+                }
+            } else {
+                dt = a.dt;
+            }
+            iout = 0;
+            if (a.save_start) {
+                S.save(i, 0, xv, t);
+                t_last = t;
+                iout = 1;
+            }
+            steps = 0;
+            attempts = 0;
+            ret = TP_RET_SUCCESS;
+        }
+        bool done = !(t < t1 && steps < a.maxiters);
+        if (!done) {
+            if (t + dt > t1) dt = t1 - t;
+            G4 dx, E;
+            update_dp5(f, a.f, xv, p, dt, t, dx, E);
+            G4 yn = gadd(xv, dx);
+            double sum_sq = 0.0;
+            for (int k = 0; k < 4; ++k) {
+                double ax_ = fabs(xv.y[k]), ay_ = fabs(yn.y[k]);
+                double sc = fma((ax_ < ay_) ? ay_ : ax_, a.reltol, a.abstol);
+                double qk = E.y[k] / sc;
+                sum_sq = fma(qk, qk, sum_sq);
+            }
+            double error_ratio = 0.5 * sqrt(sum_sq);
+            bool stop = false;
+            // accept unless the ratio exceeds 1: a NaN ratio is accepted, as the
+            // reference's @fastmath comparison does (the NaN state then ends
+            // the trajectory through isoutside)
+            if (!(error_ratio > 1.0)) {
+                if (a.term.flags && outside_gc(a.term, yn, t + dt)) {
+                    ret = TP_RET_TERMINATED;
+                    stop = true;
+                } else {
+                    t += dt;
+                    xv = yn;
+                    if (a.save_everystep) {
+                        S.save(i, iout, xv, t);
+                        t_last = t;
+                        iout += 1;
+                    }
+                    steps += 1;
+                }
+            }
+            if (!stop) {
+                double scale = (error_ratio == 0.0) ? max_growth : safety * pow(1.0 / error_ratio, 0.2);
+                scale = (max_growth < scale) ? max_growth : scale;
+                scale = (min_growth < scale) ? scale : min_growth;
+                dt *= scale;
+                if (dt < 1.0e-14) stop = true;
+            }
+            attempts += 1;
+            if ((attempts & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                set_status(a.status, TP_E_TIMEOUT);
+                ret = TP_RET_DEFAULT;
+                stop = true;
+            }
+            done = stop || !(t < t1 && steps < a.maxiters);
+        }
+        if (done) {
+            if (a.save_end && (iout == 0 || t_last != t)) {
+                S.save(i, iout, xv, t);
+                iout += 1;
+            }
+            a.nsaved[i] = (int32_t)iout;
+            a.retcode[i] = (int8_t)ret;
+            a.nsteps[i] = steps;
+            i = -1;
+        }
+    }
+}
+
+}  // namespace tpb

@@ -1,0 +1,71 @@
+// gc_fp64.cu -- float64 guiding-centre kernels (the drop-in path) and the
+// prepare_gc kernel.  Compiled with -fmad=false (see fields64.cuh).
+#include "gc_common.cuh"
+
+namespace tpb {
+
+// _get_gc_parameters (src/gc/gc.jl:13-39) for one full-orbit state:
+// X = x - rho, v_par, mu in the E x B frame.
+__global__ void k_gc_prepare(GCPrepArgs a) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double* s = a.xv + 6 * i;
+    D3 x{s[0], s[1], s[2]}, v{s[3], s[4], s[5]};
+    D3 bp = field_eval64(a.f.B, x, a.t);
+    double Bmp = norm(bp);
+    D3 bhp = bp / Bmp;
+    D3 rho = cross(bhp, v) / (a.q / a.m * Bmp);
+    D3 X = x - rho;
+    D3 b = field_eval64(a.f.B, X, a.t);
+    double Bmag = norm(b);
+    D3 bh = b / Bmag;
+    double vpar = dot(bh, v);
+    D3 vperp = v - vpar * bh;
+    D3 e = field_eval64(a.f.E, X, a.t);
+    D3 vE = cross(e, bh) / Bmag;
+    D3 w = vperp - vE;
+    double mu = a.m * dot(w, w) / (2.0 * Bmag);
+    a.y0[4 * i + 0] = X.x;
+    a.y0[4 * i + 1] = X.y;
+    a.y0[4 * i + 2] = X.z;
+    a.y0[4 * i + 3] = vpar;
+    a.mu[i] = mu;
+}
+
+cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    int block = 256;
+    int64_t grid = (a.n + block - 1) / block;
+    k_gc_prepare<<<(unsigned)grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class R>
+static const void* gc_kernel(bool rk4, bool queue) {
+    if (rk4) return queue ? (const void*)k_rk4<R, true> : (const void*)k_rk4<R, false>;
+    return queue ? (const void*)k_rk45<R, true> : (const void*)k_rk45<R, false>;
+}
+
+const void* select_gc_kernel64(const GCArgs& a, bool queue) {
+    bool grid = a.f.E.kind == TP_FIELD_GRID || a.f.B.kind == TP_FIELD_GRID;
+    bool rk4 = a.alg == TP_GC_RK4;
+    return grid ? gc_kernel<RHS64<true>>(rk4, queue) : gc_kernel<RHS64<false>>(rk4, queue);
+}
+
+const void* select_gc_kernel32(const GCArgs& a, bool queue);
+
+int occupancy_gc(const GCArgs& a, int block) {
+    int nb = 0;
+    const void* f = a.precision == TP_GC_PREC_FP32RHS ? select_gc_kernel32(a, true) : select_gc_kernel64(a, true);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, block, 0);
+    return nb;
+}
+
+cudaError_t launch_gc(const GCArgs& a, const LaunchCfg& c, cudaStream_t s) {
+    const bool q = a.use_queue != 0;
+    const void* f = a.precision == TP_GC_PREC_FP32RHS ? select_gc_kernel32(a, q) : select_gc_kernel64(a, q);
+    void* args[] = {const_cast<GCArgs*>(&a)};
+    return cudaLaunchKernel(f, dim3(c.grid), dim3(c.block), args, 0, s);
+}
+
+}  // namespace tpb

@@ -1,0 +1,88 @@
+// pack.cu -- layout kernels: field node tables and result packing.
+#include <cub/device/device_scan.cuh>
+
+#include "tp_launch.h"
+
+namespace tpb {
+
+// (3, nx, ny, nz) column-major source -> 4-vector per node table, entry
+// node*stride + off (stride 2 interleaves E and B of one node in 32 bytes).
+template <class S, class D>
+__global__ void k_pack_nodes(const S* src, int64_t nodes, D* dst, int stride, int off) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nodes) return;
+    D* o = dst + 4 * (k * stride + off);
+    o[0] = (D)src[3 * k + 0];
+    o[1] = (D)src[3 * k + 1];
+    o[2] = (D)src[3 * k + 2];
+    o[3] = (D)0;
+}
+
+cudaError_t launch_pack_node_table(const void* src, int src_f64, int64_t nodes, void* dst,
+                                   int dst_f64, int stride, int off, cudaStream_t s) {
+    if (nodes <= 0) return cudaSuccess;
+    const int block = 256;
+    const unsigned grid = (unsigned)((nodes + block - 1) / block);
+    if (src_f64 && dst_f64)
+        k_pack_nodes<double, double><<<grid, block, 0, s>>>((const double*)src, nodes, (double*)dst, stride, off);
+    else if (src_f64)
+        k_pack_nodes<double, float><<<grid, block, 0, s>>>((const double*)src, nodes, (float*)dst, stride, off);
+    else if (dst_f64)
+        k_pack_nodes<float, double><<<grid, block, 0, s>>>((const float*)src, nodes, (double*)dst, stride, off);
+    else
+        k_pack_nodes<float, float><<<grid, block, 0, s>>>((const float*)src, nodes, (float*)dst, stride, off);
+    return cudaGetLastError();
+}
+
+// slot-major (t[k*n+i], u[(k*W+c)*n+i]) -> per-trajectory packed
+// (t_out[off_i + k], u_out[(off_i + k)*W + c]).  One warp per particle
+// group: threads stride over (particle, save) pairs.
+__global__ void k_pack_results(const double* t_in, const double* u_in, const int32_t* nsaved,
+                               const int64_t* offsets, int64_t n, int64_t nslots, int W,
+                               double* t_out, double* u_out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t ns = nsaved[i];
+    if (ns > nslots) ns = nslots;
+    int64_t o = offsets[i];
+    for (int64_t k = 0; k < ns; ++k) {
+        t_out[o + k] = t_in[k * n + i];
+        for (int c = 0; c < W; ++c) u_out[(o + k) * W + c] = u_in[(k * W + c) * n + i];
+    }
+}
+
+cudaError_t launch_pack_results(const double* t_in, const double* u_in, const int32_t* nsaved,
+                                const int64_t* offsets, int64_t n, int64_t nslots, int width,
+                                double* t_out, double* u_out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int block = 128;
+    const unsigned grid = (unsigned)((n + block - 1) / block);
+    k_pack_results<<<grid, block, 0, s>>>(t_in, u_in, nsaved, offsets, n, nslots, width, t_out, u_out);
+    return cudaGetLastError();
+}
+
+// nsaved (clamped to nslots) -> exclusive offsets, plus the total in offsets[n]
+__global__ void k_clamp_counts(const int32_t* nsaved, int64_t n, int64_t nslots, int64_t* cnt) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) {
+        cnt[n] = 0;
+        return;
+    }
+    int64_t v = nsaved[i];
+    cnt[i] = v > nslots ? nslots : v;
+}
+
+cudaError_t scan_offsets(const int32_t* nsaved, int64_t n, int64_t nslots, int64_t* cnt,
+                         int64_t* offsets, void* tmp, size_t* tmp_bytes, cudaStream_t s) {
+    if (!tmp) {
+        return cub::DeviceScan::ExclusiveSum(nullptr, *tmp_bytes, cnt, offsets, n + 1, s);
+    }
+    const int block = 256;
+    k_clamp_counts<<<(unsigned)((n + 1 + block - 1) / block), block, 0, s>>>(nsaved, n, nslots, cnt);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cub::DeviceScan::ExclusiveSum(tmp, *tmp_bytes, cnt, offsets, n + 1, s);
+}
+
+}  // namespace tpb

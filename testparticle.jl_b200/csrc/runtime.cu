@@ -1,0 +1,1026 @@
+// runtime.cu -- host side of the C ABI (include/tp_abi.h).
+//
+// Owns the device, one stream per context, field uploads (grid data is laid
+// out once as per-node 4-vectors; an E/B pair on one geometry is interleaved
+// so each corner is one 32-byte sector), argument validation that mirrors the
+// reference's ArgumentErrors, kernel launches, and result packing into the
+// reference's per-trajectory layout.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tp_launch.h"
+
+namespace tpb {
+cudaError_t scan_offsets(const int32_t* nsaved, int64_t n, int64_t nslots, int64_t* cnt,
+                         int64_t* offsets, void* tmp, size_t* tmp_bytes, cudaStream_t s);
+}
+
+using namespace tpb;
+
+struct tp_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // tuned launch shapes keyed by (alg, precision, field kinds, schedule)
+    std::map<std::string, int> tuned_block;
+};
+
+struct tp_field {
+    tp_ctx* ctx = nullptr;
+    uint64_t id = 0;
+    tp_field_desc desc{};
+    DevField dev{};
+    int64_t nodes = 0;
+    void* d_raw = nullptr;   // uploaded (3, nx, ny, nz) data
+    void* d_tab = nullptr;   // per-node table in the data's precision
+    void* d_tab32 = nullptr; // float per-node table (only for f64 data)
+    // interleaved E/B table built on first use with a partner field
+    uint64_t eb_partner = 0;
+    void* d_eb = nullptr;
+    void* d_eb32 = nullptr;
+};
+
+struct tp_result {
+    int64_t n = 0;
+    int32_t width = 0;
+    int64_t total = 0;
+    std::vector<int32_t> nsaved;
+    std::vector<int8_t> retcode;
+    std::vector<int64_t> nsteps;
+    std::vector<double> t;
+    std::vector<double> u;
+    double elapsed_ms = 0.0;
+};
+
+namespace {
+
+std::mutex g_id_mu;
+uint64_t g_next_id = 1;
+
+int fail(tp_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(tp_ctx* ctx, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();  // clear a sticky-free error
+    return fail(ctx, TP_E_CUDA, m);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// RAII device buffer
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t b) {
+        bytes = b;
+        if (b == 0) return cudaSuccess;
+        return cudaMalloc(&p, b);
+    }
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+const double kEps = 2.220446049250313e-16;
+
+int64_t jl_round_h(double x) { return (int64_t)std::nearbyint(x); }
+
+int64_t nout_h(int64_t nt, int64_t ssi, bool ss, bool se, bool sev) {
+    int64_t nout = 0;
+    if (ss) nout += 1;
+    if (sev) {
+        int64_t steps = nt / ssi;
+        bool last_is_step = (nt > 0) && (nt % ssi == 0);
+        nout += steps;
+        if (!se && last_is_step) nout -= 1;
+        if (se && !last_is_step) nout += 1;
+    } else if (se) {
+        nout += 1;
+    }
+    return nout;
+}
+
+void fill_float_copies(DevField& d) {
+    for (int a = 0; a < 3; ++a) {
+        d.vf[a] = (float)d.v[a];
+        d.ratef[a] = (float)d.rate[a];
+        d.mf[a] = (float)d.m[a];
+        d.cf[a] = (float)d.c[a];
+        d.x0f[a] = (float)d.x0[a];
+        d.dxf[a] = (float)(1.0 / d.inv_dx[a]);
+        d.idxf[a] = (float)d.inv_dx[a];
+    }
+    for (int k = 0; k < 9; ++k) d.Jf[k] = (float)d.J[k];
+    d.coeff = (float)d.coef;
+}
+
+bool same_geometry(const tp_field* a, const tp_field* b) {
+    if (a->desc.kind != TP_FIELD_GRID || b->desc.kind != TP_FIELD_GRID) return false;
+    if (a->desc.bc != b->desc.bc || a->desc.dtype != b->desc.dtype) return false;
+    for (int k = 0; k < 3; ++k) {
+        if (a->desc.n[k] != b->desc.n[k]) return false;
+        if (a->desc.origin[k] != b->desc.origin[k]) return false;
+        if (a->desc.spacing[k] != b->desc.spacing[k]) return false;
+    }
+    return true;
+}
+
+DevTerm dev_term(const tp_term_desc& t) {
+    DevTerm d{};
+    d.flags = t.flags;
+    d.rmin = t.rmin;
+    d.rmax = t.rmax;
+    for (int k = 0; k < 3; ++k) {
+        d.lo[k] = t.lo[k];
+        d.hi[k] = t.hi[k];
+    }
+    d.tmax = t.tmax;
+    return d;
+}
+
+// Build DevFields for a run; interleaves two grids on one geometry.
+int make_dev_fields(tp_ctx* ctx, const tp_field* E, tp_field* B, DevFields& F) {
+    std::memset(&F, 0, sizeof(F));
+    F.E = E->dev;
+    F.B = B->dev;
+    if (same_geometry(E, B)) {
+        if (B->eb_partner != E->id) {
+            if (B->d_eb) cudaFree(B->d_eb);
+            if (B->d_eb32) cudaFree(B->d_eb32);
+            B->d_eb = B->d_eb32 = nullptr;
+            bool f64 = B->desc.dtype == TP_DTYPE_F64;
+            size_t esz = f64 ? sizeof(double) : sizeof(float);
+            cudaError_t e = cudaMalloc(&B->d_eb, (size_t)B->nodes * 8 * esz);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "interleaved field table");
+            e = launch_pack_node_table(E->d_raw, f64, E->nodes, B->d_eb, f64, 2, 0, ctx->stream);
+            if (e == cudaSuccess)
+                e = launch_pack_node_table(B->d_raw, f64, B->nodes, B->d_eb, f64, 2, 1, ctx->stream);
+            if (e == cudaSuccess && f64) {
+                e = cudaMalloc(&B->d_eb32, (size_t)B->nodes * 8 * sizeof(float));
+                if (e == cudaSuccess)
+                    e = launch_pack_node_table(E->d_raw, 1, E->nodes, B->d_eb32, 0, 2, 0, ctx->stream);
+                if (e == cudaSuccess)
+                    e = launch_pack_node_table(B->d_raw, 1, B->nodes, B->d_eb32, 0, 2, 1, ctx->stream);
+            }
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "interleaved field table");
+            B->eb_partner = E->id;
+        }
+        F.eb = B->d_eb;
+        F.eb_f64 = B->desc.dtype == TP_DTYPE_F64;
+        F.eb32 = (const float4*)(B->d_eb32 ? B->d_eb32 : B->d_eb);
+    }
+    return TP_OK;
+}
+
+// Periodic wrapping of FP32C positions: only on axes where every
+// position-dependent field is a periodic grid with one period, and when no
+// spatial termination predicate reads absolute positions.
+void set_wrap(BorisArgs& a, const tp_field* E, const tp_field* B, const tp_term_desc& term) {
+    for (int c = 0; c < 3; ++c) a.wrap[c] = 0;
+    if (term.flags & (TP_TERM_SHELL | TP_TERM_BOX)) return;
+    const tp_field* f[2] = {E, B};
+    bool any_grid = false;
+    for (int c = 0; c < 3; ++c) {
+        bool ok = true;
+        double L = 0, x0 = 0;
+        bool have = false;
+        for (const tp_field* g : f) {
+            int k = g->desc.kind;
+            if (k == TP_FIELD_ZERO || k == TP_FIELD_UNIFORM) continue;
+            if (k == TP_FIELD_AFFINE) {
+                // translation-invariant only if it does not depend on this axis
+                for (int r = 0; r < 3; ++r)
+                    if (g->desc.jac[3 * r + c] != 0.0) ok = false;
+                continue;
+            }
+            if (k != TP_FIELD_GRID || g->desc.bc != TP_BC_PERIODIC) {
+                ok = false;
+                continue;
+            }
+            double Lg = (double)g->desc.n[c] * g->desc.spacing[c];
+            if (have && (Lg != L || g->desc.origin[c] != x0)) ok = false;
+            L = Lg;
+            x0 = g->desc.origin[c];
+            have = true;
+            any_grid = true;
+        }
+        if (ok && have) {
+            a.wrap[c] = 1;
+            a.wrapL[c] = L;
+            a.wrap0[c] = x0;
+        }
+    }
+    (void)any_grid;
+}
+
+int check_boris_desc(tp_ctx* ctx, const tp_run_desc* d) {
+    if (!d) return fail(ctx, TP_E_ARG, "null run descriptor");
+    if (d->alg < TP_ALG_BORIS || d->alg > TP_ALG_ADAPTIVE_MULTISTEP)
+        return fail(ctx, TP_E_UNSUPPORTED, "unknown algorithm");
+    bool multi = d->alg == TP_ALG_MULTISTEP || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (multi && d->order != 2 && d->order != 4 && d->order != 6)
+        return fail(ctx, TP_E_ARG, "Multistep Boris order N must be 2, 4, or 6.");
+    if (multi && d->nsub < 1) return fail(ctx, TP_E_ARG, "Multistep Boris subcycles n must be >= 1");
+    if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "savestepinterval must be >= 1");
+    if (d->precision != TP_PREC_FP64 && d->precision != TP_PREC_FP32C)
+        return fail(ctx, TP_E_UNSUPPORTED, "unknown precision");
+    if (d->block < 0 || d->block > 256 || (d->block % 32) != 0)
+        return fail(ctx, TP_E_ARG, "block must be 0 or a multiple of 32 up to 256");
+    return TP_OK;
+}
+
+// Static schedule: one thread per particle.  Queue schedule: a persistent
+// grid of (SMs x resident blocks) pulling particles from a device counter.
+int pick_launch(tp_ctx* ctx, int64_t n, int block_req, bool queue, int occ_blocks, LaunchCfg& cfg) {
+    int block = block_req > 0 ? block_req : 128;
+    int64_t need = (n + block - 1) / block;
+    if (need < 1) need = 1;
+    if (need > 0x7fffffff) return fail(ctx, TP_E_ARG, "too many particles for one launch");
+    cfg.block = block;
+    if (!queue) {
+        cfg.grid = (int)need;
+        return TP_OK;
+    }
+    int64_t resident = (int64_t)ctx->sms * std::max(occ_blocks, 1);
+    cfg.grid = (int)std::min<int64_t>(need, resident);
+    return TP_OK;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+int tp_abi_version(void) { return TP_ABI_VERSION; }
+
+int tp_ctx_create(int device, tp_ctx** out) {
+    if (!out) return TP_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return TP_E_CUDA;
+    }
+    if (device < 0 || device >= ndev) return TP_E_ARG;
+    DeviceGuard g(device);
+    tp_ctx* c = new tp_ctx();
+    c->device = device;
+    e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        cudaGetLastError();
+        return TP_E_CUDA;
+    }
+    *out = c;
+    return TP_OK;
+}
+
+void tp_ctx_destroy(tp_ctx* ctx) {
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* tp_last_error(const tp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
+    if (!ctx || !d || !out) return fail(ctx, TP_E_ARG, "null argument");
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    tp_field* f = new tp_field();
+    f->ctx = ctx;
+    {
+        std::lock_guard<std::mutex> lk(g_id_mu);
+        f->id = g_next_id++;
+    }
+    f->desc = *d;
+    f->desc.data = nullptr;
+    DevField& dv = f->dev;
+    std::memset(&dv, 0, sizeof(dv));
+    dv.kind = d->kind;
+    dv.bc = d->bc;
+    for (int k = 0; k < 3; ++k) {
+        dv.v[k] = d->value[k];
+        dv.rate[k] = d->rate[k];
+        dv.m[k] = d->moment[k];
+        dv.c[k] = d->center[k];
+    }
+    for (int k = 0; k < 9; ++k) dv.J[k] = d->jac[k];
+    dv.coef = d->coef;
+    switch (d->kind) {
+        case TP_FIELD_ZERO:
+        case TP_FIELD_UNIFORM:
+        case TP_FIELD_AFFINE:
+        case TP_FIELD_DIPOLE:
+            break;
+        case TP_FIELD_GRID: {
+            if (d->bc != TP_BC_FILL_NAN && d->bc != TP_BC_CLAMP && d->bc != TP_BC_PERIODIC) {
+                delete f;
+                return fail(ctx, TP_E_ARG, "unknown grid boundary condition");
+            }
+            if (d->dtype != TP_DTYPE_F32 && d->dtype != TP_DTYPE_F64) {
+                delete f;
+                return fail(ctx, TP_E_ARG, "grid dtype must be float32 or float64");
+            }
+            if (!d->data) {
+                delete f;
+                return fail(ctx, TP_E_ARG, "grid data pointer is null");
+            }
+            int64_t nodes = 1;
+            for (int k = 0; k < 3; ++k) {
+                if (d->n[k] < 2 || d->n[k] > (1 << 20)) {
+                    delete f;
+                    return fail(ctx, TP_E_ARG, "grid needs 2 .. 2^20 nodes per axis");
+                }
+                if (!(d->spacing[k] > 0.0) || !std::isfinite(d->spacing[k])) {
+                    delete f;
+                    return fail(ctx, TP_E_ARG, "grid spacing must be positive and finite");
+                }
+                nodes *= d->n[k];
+                dv.n[k] = (int32_t)d->n[k];
+                dv.x0[k] = d->origin[k];
+                dv.inv_dx[k] = 1.0 / d->spacing[k];
+                dv.L[k] = (double)d->n[k] * d->spacing[k];
+            }
+            if (nodes > ((int64_t)1 << 31) / 2) {
+                delete f;
+                return fail(ctx, TP_E_ARG, "grid too large (more than 2^30 nodes)");
+            }
+            f->nodes = nodes;
+            bool f64 = d->dtype == TP_DTYPE_F64;
+            size_t esz = f64 ? sizeof(double) : sizeof(float);
+            cudaError_t e = cudaMalloc(&f->d_raw, (size_t)nodes * 3 * esz);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(f->d_raw, d->data, (size_t)nodes * 3 * esz, cudaMemcpyHostToDevice,
+                                    ctx->stream);
+            if (e == cudaSuccess) e = cudaMalloc(&f->d_tab, (size_t)nodes * 4 * esz);
+            if (e == cudaSuccess)
+                e = launch_pack_node_table(f->d_raw, f64, nodes, f->d_tab, f64, 1, 0, ctx->stream);
+            if (e == cudaSuccess && f64) {
+                e = cudaMalloc(&f->d_tab32, (size_t)nodes * 4 * sizeof(float));
+                if (e == cudaSuccess)
+                    e = launch_pack_node_table(f->d_raw, 1, nodes, f->d_tab32, 0, 1, 0, ctx->stream);
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) {
+                int r = cuda_fail(ctx, e, "grid upload");
+                tp_field_destroy(f);
+                return r;
+            }
+            dv.f64 = f64;
+            dv.tab = f->d_tab;
+            dv.tab32 = (const float4*)(f64 ? f->d_tab32 : f->d_tab);
+            break;
+        }
+        default:
+            delete f;
+            return fail(ctx, TP_E_UNSUPPORTED, "field kind not supported by the B200 library");
+    }
+    fill_float_copies(dv);
+    *out = f;
+    return TP_OK;
+}
+
+void tp_field_destroy(tp_field* f) {
+    if (!f) return;
+    DeviceGuard g(f->ctx->device);
+    cudaStreamSynchronize(f->ctx->stream);
+    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32})
+        if (p) cudaFree(p);
+    delete f;
+}
+
+int tp_boris_slots(const tp_run_desc* d, const double* dt_i, const double* tend_i, int64_t n,
+                   int64_t* nslots) {
+    if (!d || !nslots || n < 0) return TP_E_ARG;
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (d->savestepinterval < 1) return TP_E_ARG;
+    if (adaptive) {
+        if (d->step_cap <= 0) {
+            *nslots = -1;  // unknown: the run grows its buffers
+            return TP_OK;
+        }
+        int64_t s = (d->save_start ? 1 : 0) + 1;
+        if (d->save_everystep) s += d->step_cap / d->savestepinterval + 1;
+        *nslots = s;
+        return TP_OK;
+    }
+    int64_t best = 0;
+    for (int64_t i = 0; i < std::max<int64_t>(n, 1); ++i) {
+        double dt = (dt_i && n > 0) ? dt_i[i] : d->dt;
+        double t1 = (tend_i && n > 0) ? tend_i[i] : d->t1;
+        if (std::fabs(dt) < 10.0 * kEps) return TP_E_ARG;
+        int64_t nt = jl_round_h((t1 - d->t0) / dt);
+        if (nt < 0) nt = -nt;
+        if (nt > d->maxiters) return TP_E_ARG;
+        best = std::max(best, nout_h(nt, d->savestepinterval, d->save_start, d->save_end,
+                                     d->save_everystep));
+        if (!dt_i && !tend_i) break;
+    }
+    *nslots = best;
+    return TP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Fill the launch block of a full-orbit run (device pointers set by caller).
+int prepare_boris_args(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, tp_field* B,
+                       BorisArgs& a) {
+    std::memset(&a, 0, sizeof(a));
+    int st = make_dev_fields(ctx, E, B, a.f);
+    if (st != TP_OK) return st;
+    a.term = dev_term(d->term);
+    a.alg = d->alg;
+    a.order = d->order;
+    a.nsub = d->nsub;
+    a.save_fields = d->save_fields;
+    a.save_start = d->save_start;
+    a.save_end = d->save_end;
+    a.save_everystep = d->save_everystep;
+    a.safety = d->safety;
+    a.t0 = d->t0;
+    a.t1 = d->t1;
+    a.dt = d->dt;
+    a.q2m = d->q2m;
+    a.m = d->m;
+    a.ssi = d->savestepinterval;
+    a.maxiters = d->maxiters;
+    a.step_cap = d->step_cap;
+    double budget = d->budget_s > 0 ? d->budget_s : 600.0;
+    a.budget_ns = (uint64_t)(budget * 1e9);
+    if (d->precision == TP_PREC_FP32C) set_wrap(a, E, B, d->term);
+    return TP_OK;
+}
+
+bool use_queue(const tp_run_desc* d) {
+    if (d->schedule == TP_SCHED_QUEUE) return true;
+    if (d->schedule == TP_SCHED_STATIC) return false;
+    // uneven lifetimes: adaptive steps or a termination predicate
+    return d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP || d->term.flags != 0;
+}
+
+int launch_boris(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, cudaStream_t s,
+                 unsigned long long* d_queue) {
+    bool q = use_queue(d);
+    a.use_queue = q;
+    a.queue = d_queue;
+    int block = d->block;
+    int occ = 0;
+    if (q) {
+        int b = block > 0 ? block : 128;
+        occ = d->precision == TP_PREC_FP32C ? occupancy_boris_fp32c(a, b) : occupancy_boris_fp64(a, b);
+    }
+    LaunchCfg cfg;
+    int st = pick_launch(ctx, a.n, block, q, occ, cfg);
+    if (st != TP_OK) return st;
+    if (q) {
+        cudaError_t e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "queue reset");
+    }
+    cudaError_t e = d->precision == TP_PREC_FP32C ? launch_boris_fp32c(a, cfg, s)
+                                                  : launch_boris_fp64(a, cfg, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "push kernel launch");
+    return TP_OK;
+}
+
+int status_to_error(tp_ctx* ctx, int32_t status) {
+    switch (status) {
+        case 0:
+            return TP_OK;
+        case TP_E_ARG:
+            return fail(ctx, TP_E_ARG, "invalid per-particle dt / tspan (|dt| < 10 eps or nt > maxiters)");
+        case TP_E_TIMEOUT:
+            return fail(ctx, TP_E_TIMEOUT, "device loop exceeded its wall-clock budget");
+        case TP_E_OVERFLOW:
+            return fail(ctx, TP_E_OVERFLOW, "a trajectory produced more saves than slots");
+        default:
+            return fail(ctx, TP_E_CUDA, "kernel reported status " + std::to_string(status));
+    }
+}
+
+// Copy slot-major device results into a packed host tp_result.
+int pack_to_host(tp_ctx* ctx, int64_t n, int64_t nslots, int W, const DBuf& t_d, const DBuf& u_d,
+                 const DBuf& ns_d, const DBuf& rc_d, const DBuf& st_d, tp_result* r) {
+    cudaStream_t s = ctx->stream;
+    r->n = n;
+    r->width = W;
+    r->nsaved.resize(n);
+    r->retcode.resize(n);
+    r->nsteps.resize(n);
+    if (n == 0) return TP_OK;
+    DBuf cnt, off, tmp;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cnt.alloc((size_t)(n + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = off.alloc((size_t)(n + 1) * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = scan_offsets(ns_d.as<int32_t>(), n, nslots, cnt.as<int64_t>(), off.as<int64_t>(), nullptr,
+                         &tmp_bytes, s);
+    if (e == cudaSuccess) e = tmp.alloc(tmp_bytes);
+    if (e == cudaSuccess)
+        e = scan_offsets(ns_d.as<int32_t>(), n, nslots, cnt.as<int64_t>(), off.as<int64_t>(), tmp.p,
+                         &tmp_bytes, s);
+    int64_t total = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&total, off.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result offsets");
+    r->total = total;
+    DBuf tp, up;
+    e = tp.alloc((size_t)std::max<int64_t>(total, 1) * sizeof(double));
+    if (e == cudaSuccess) e = up.alloc((size_t)std::max<int64_t>(total, 1) * W * sizeof(double));
+    if (e == cudaSuccess)
+        e = launch_pack_results(t_d.as<double>(), u_d.as<double>(), ns_d.as<int32_t>(), off.as<int64_t>(),
+                                n, nslots, W, tp.as<double>(), up.as<double>(), s);
+    r->t.resize(total);
+    r->u.resize((size_t)total * W);
+    if (e == cudaSuccess && total > 0)
+        e = cudaMemcpyAsync(r->t.data(), tp.p, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && total > 0)
+        e = cudaMemcpyAsync(r->u.data(), up.p, (size_t)total * W * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(r->nsaved.data(), ns_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(r->retcode.data(), rc_d.p, (size_t)n * sizeof(int8_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+    (void)st_d;
+    return TP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B,
+                        const double* u0, const double* dt_i, const double* tend_i, int64_t n,
+                        int64_t nslots, double* t_out, double* u_out, int32_t* nsaved,
+                        int8_t* retcode, int64_t* nsteps, int32_t* status, void* stream) {
+    if (!ctx) return TP_E_ARG;
+    int st = check_boris_desc(ctx, d);
+    if (st != TP_OK) return st;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (n < 0 || nslots < 0) return fail(ctx, TP_E_ARG, "negative size");
+    if (n == 0) return TP_OK;
+    if (!u0 || !nsaved || !retcode || !nsteps || !status || (nslots > 0 && (!t_out || !u_out)))
+        return fail(ctx, TP_E_ARG, "null device buffer");
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (!adaptive && !dt_i && std::fabs(d->dt) < 10.0 * kEps)
+        return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
+    DeviceGuard g(ctx->device);
+    BorisArgs a;
+    st = prepare_boris_args(ctx, d, E, const_cast<tp_field*>(B), a);
+    if (st != TP_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    // the interleaved table (if any) was built on the context stream
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "field table");
+    a.n = n;
+    a.nslots = nslots;
+    a.u0 = u0;
+    a.dt_i = dt_i;
+    a.tend_i = tend_i;
+    a.t_out = t_out;
+    a.u_out = u_out;
+    a.nsaved = nsaved;
+    a.retcode = retcode;
+    a.nsteps = nsteps;
+    a.status = status;
+    unsigned long long* q = nullptr;
+    if (use_queue(d)) {
+        e = cudaMallocAsync((void**)&q, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "queue counter");
+    }
+    st = launch_boris(ctx, d, a, s, q);
+    if (q) cudaFreeAsync(q, s);
+    return st;
+}
+
+int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B,
+                 const double* u0, const double* dt_i, const double* tend_i, int64_t n,
+                 tp_result** out) {
+    if (!ctx || !out) return TP_E_ARG;
+    *out = nullptr;
+    int st = check_boris_desc(ctx, d);
+    if (st != TP_OK) return st;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (n < 0 || (n > 0 && !u0)) return fail(ctx, TP_E_ARG, "bad particle table");
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    // the reference's ArgumentErrors (boris.jl:349-356) before any tracing
+    if (!adaptive) {
+        for (int64_t i = 0; i < std::max<int64_t>(n, 1); ++i) {
+            double dt = (dt_i && n > 0) ? dt_i[i] : d->dt;
+            double t1 = (tend_i && n > 0) ? tend_i[i] : d->t1;
+            if (std::fabs(dt) < 10.0 * kEps)
+                return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
+            int64_t nt = jl_round_h((t1 - d->t0) / dt);
+            if (nt < 0) nt = -nt;
+            if (nt > d->maxiters)
+                return fail(ctx, TP_E_ARG, "number of iterations nt (" + std::to_string(nt) +
+                                               ") exceeds maxiters (" + std::to_string(d->maxiters) + ")");
+            if (!dt_i && !tend_i) break;
+        }
+    }
+    int64_t nslots = 0;
+    st = tp_boris_slots(d, dt_i, tend_i, n, &nslots);
+    if (st != TP_OK) return fail(ctx, st, "cannot size the output");
+    if (nslots < 0) nslots = 64;  // adaptive without a cap: grown on overflow below
+    const int W = d->save_fields ? 12 : 6;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    tp_result* r = new tp_result();
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        DBuf u0_d, dt_d, te_d, t_d, u_d, ns_d, rc_d, nst_d, st_d, q_d;
+        cudaError_t e = u0_d.alloc((size_t)n * 6 * sizeof(double));
+        if (e == cudaSuccess && dt_i) e = dt_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && tend_i) e = te_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = t_d.alloc((size_t)nslots * n * sizeof(double));
+        if (e == cudaSuccess) e = u_d.alloc((size_t)nslots * W * n * sizeof(double));
+        if (e == cudaSuccess) e = ns_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = rc_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int8_t));
+        if (e == cudaSuccess) e = nst_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int64_t));
+        if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
+        if (e == cudaSuccess) e = q_d.alloc(sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            delete r;
+            return fail(ctx, TP_E_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+        }
+        if (n > 0) e = cudaMemcpyAsync(u0_d.p, u0, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && dt_i)
+            e = cudaMemcpyAsync(dt_d.p, dt_i, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && tend_i)
+            e = cudaMemcpyAsync(te_d.p, tend_i, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(st_d.p, 0, sizeof(int32_t), s);
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "input upload");
+        }
+        BorisArgs a;
+        st = prepare_boris_args(ctx, d, E, const_cast<tp_field*>(B), a);
+        if (st != TP_OK) {
+            delete r;
+            return st;
+        }
+        a.n = n;
+        a.nslots = nslots;
+        a.u0 = u0_d.as<double>();
+        a.dt_i = dt_i ? dt_d.as<double>() : nullptr;
+        a.tend_i = tend_i ? te_d.as<double>() : nullptr;
+        a.t_out = t_d.as<double>();
+        a.u_out = u_d.as<double>();
+        a.nsaved = ns_d.as<int32_t>();
+        a.retcode = rc_d.as<int8_t>();
+        a.nsteps = nst_d.as<int64_t>();
+        a.status = st_d.as<int32_t>();
+        cudaEvent_t ev0, ev1;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, s);
+        if (n > 0) {
+            st = launch_boris(ctx, d, a, s, q_d.as<unsigned long long>());
+            if (st != TP_OK) {
+                cudaEventDestroy(ev0);
+                cudaEventDestroy(ev1);
+                delete r;
+                return st;
+            }
+        }
+        cudaEventRecord(ev1, s);
+        int32_t status = 0;
+        e = cudaMemcpyAsync(&status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "push kernel");
+        }
+        r->elapsed_ms = ms;
+        if (status == TP_E_OVERFLOW && adaptive && attempt == 0) {
+            // saves of an adaptive run are unknown in advance: size exactly and rerun
+            std::vector<int32_t> ns(n);
+            e = cudaMemcpy(ns.data(), ns_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                delete r;
+                return cuda_fail(ctx, e, "save counts");
+            }
+            int64_t mx = 0;
+            for (int32_t v : ns) mx = std::max<int64_t>(mx, v);
+            nslots = mx;
+            continue;
+        }
+        if (status != 0) {
+            delete r;
+            return status_to_error(ctx, status);
+        }
+        st = pack_to_host(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, st_d, r);
+        if (st == TP_OK && n > 0) {
+            e = cudaMemcpy(r->nsteps.data(), nst_d.p, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = cuda_fail(ctx, e, "step counts");
+        }
+        if (st != TP_OK) {
+            delete r;
+            return st;
+        }
+        *out = r;
+        return TP_OK;
+    }
+    delete r;
+    return fail(ctx, TP_E_OVERFLOW, "save slots exceeded after resizing");
+}
+
+// ---------------------------------------------------------------- guiding centre
+int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B, const double* xv, int64_t n,
+                  double q, double m, double t, double* y0_out, double* mu_out) {
+    if (!ctx || !E || !B) return fail(ctx, TP_E_ARG, "null argument");
+    if (n < 0 || (n > 0 && (!xv || !y0_out || !mu_out))) return fail(ctx, TP_E_ARG, "bad buffers");
+    if (n == 0) return TP_OK;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    DBuf xv_d, y_d, mu_d;
+    cudaError_t e = xv_d.alloc((size_t)n * 6 * sizeof(double));
+    if (e == cudaSuccess) e = y_d.alloc((size_t)n * 4 * sizeof(double));
+    if (e == cudaSuccess) e = mu_d.alloc((size_t)n * sizeof(double));
+    if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, "device allocation");
+    e = cudaMemcpyAsync(xv_d.p, xv, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice, s);
+    GCPrepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.f.E = E->dev;
+    a.f.B = B->dev;
+    a.xv = xv_d.as<double>();
+    a.n = n;
+    a.q = q;
+    a.m = m;
+    a.t = t;
+    a.y0 = y_d.as<double>();
+    a.mu = mu_d.as<double>();
+    if (e == cudaSuccess) e = launch_gc_prepare(a, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(y0_out, y_d.p, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(mu_out, mu_d.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "prepare_gc");
+    return TP_OK;
+}
+
+int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_field* B,
+              const double* y0, const double* q_i, const double* q2m_i, const double* mu_i,
+              const double* dt_i, const double* tend_i, int64_t n, tp_result** out) {
+    if (!ctx || !out || !d) return fail(ctx, TP_E_ARG, "null argument");
+    *out = nullptr;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (n < 0 || (n > 0 && !y0)) return fail(ctx, TP_E_ARG, "bad particle table");
+    if (d->alg != TP_GC_RK4 && d->alg != TP_GC_RK45) return fail(ctx, TP_E_UNSUPPORTED, "unknown GC algorithm");
+    if (d->precision != TP_GC_PREC_FP64 && d->precision != TP_GC_PREC_FP32RHS)
+        return fail(ctx, TP_E_UNSUPPORTED, "unknown GC precision");
+    if (d->block < 0 || d->block > 256 || (d->block % 32) != 0)
+        return fail(ctx, TP_E_ARG, "block must be 0 or a multiple of 32 up to 256");
+    // _prepare_gc, src/gc/gc_solver.jl:187-231
+    double ttotal = d->t1 - d->t0;
+    int64_t nt = 0;
+    if (!d->dt_given) {
+        if (d->alg == TP_GC_RK4) return fail(ctx, TP_E_ARG, "dt must be provided for fixed step solver :rk4");
+    } else {
+        int sdt = (d->dt > 0) - (d->dt < 0), stt = (ttotal > 0) - (ttotal < 0);
+        if (d->alg == TP_GC_RK4 && sdt != stt && ttotal != 0)
+            return fail(ctx, TP_E_ARG, "dt must have the same sign as tspan[2] - tspan[1] for fixed step solver :rk4");
+        nt = jl_round_h(ttotal / d->dt);
+        if (d->alg == TP_GC_RK4 && nt > d->maxiters) nt = d->maxiters;
+    }
+    if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "savestepinterval must be >= 1");
+    int64_t nout = 0;
+    if (d->save_start) nout += 1;
+    if (d->alg == TP_GC_RK4 && d->save_everystep) {
+        int64_t steps = nt / d->savestepinterval;
+        bool last_is_step = (nt > 0) && (nt % d->savestepinterval == 0);
+        nout += steps;
+        if (!d->save_end && last_is_step) nout -= 1;
+        if (d->save_end && !last_is_step) nout += 1;
+    } else if (d->alg == TP_GC_RK4 && d->save_end) {
+        nout += 1;
+    }
+    if ((dt_i || tend_i) && d->alg == TP_GC_RK4) {
+        // per-particle dt / tspan (extension): the same checks and counts per particle
+        nout = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            double dti = dt_i ? dt_i[i] : d->dt;
+            double t1i = tend_i ? tend_i[i] : d->t1;
+            double tt = t1i - d->t0;
+            int sdt = (dti > 0) - (dti < 0), stt = (tt > 0) - (tt < 0);
+            if (sdt != stt && tt != 0)
+                return fail(ctx, TP_E_ARG, "dt must have the same sign as tspan[2] - tspan[1] for fixed step solver :rk4");
+            int64_t nti = jl_round_h(tt / dti);
+            if (nti > d->maxiters) nti = d->maxiters;
+            int64_t no = d->save_start ? 1 : 0;
+            if (d->save_everystep) {
+                int64_t steps = nti / d->savestepinterval;
+                bool last_is_step = (nti > 0) && (nti % d->savestepinterval == 0);
+                no += steps;
+                if (!d->save_end && last_is_step) no -= 1;
+                if (d->save_end && !last_is_step) no += 1;
+            } else if (d->save_end) {
+                no += 1;
+            }
+            nout = std::max(nout, no);
+        }
+    }
+    int64_t nslots = d->alg == TP_GC_RK4 ? std::max<int64_t>(nout, 0) : 64;
+    if (d->alg == TP_GC_RK45 && !d->save_everystep) nslots = 2;
+    const int W = d->save_fields ? 10 : 4;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    tp_result* r = new tp_result();
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        DBuf y_d, q_d, q2m_d, mu_d, dt_d, te_d, t_d, u_d, ns_d, rc_d, nst_d, st_d, qq_d;
+        cudaError_t e = y_d.alloc((size_t)n * 4 * sizeof(double));
+        if (e == cudaSuccess && dt_i) e = dt_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && tend_i) e = te_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && q_i) e = q_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && q2m_i) e = q2m_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && mu_i) e = mu_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = t_d.alloc((size_t)nslots * n * sizeof(double));
+        if (e == cudaSuccess) e = u_d.alloc((size_t)nslots * W * n * sizeof(double));
+        if (e == cudaSuccess) e = ns_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = rc_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int8_t));
+        if (e == cudaSuccess) e = nst_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int64_t));
+        if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
+        if (e == cudaSuccess) e = qq_d.alloc(sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            delete r;
+            return fail(ctx, TP_E_NOMEM, "device allocation");
+        }
+        if (n > 0) e = cudaMemcpyAsync(y_d.p, y0, (size_t)n * 4 * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && q_i) e = cudaMemcpyAsync(q_d.p, q_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && q2m_i) e = cudaMemcpyAsync(q2m_d.p, q2m_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && mu_i) e = cudaMemcpyAsync(mu_d.p, mu_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && dt_i) e = cudaMemcpyAsync(dt_d.p, dt_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && tend_i) e = cudaMemcpyAsync(te_d.p, tend_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(st_d.p, 0, sizeof(int32_t), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(qq_d.p, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "input upload");
+        }
+        GCArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.f.E = E->dev;
+        a.f.B = B->dev;
+        a.term = dev_term(d->term);
+        a.alg = d->alg;
+        a.precision = d->precision;
+        a.save_fields = d->save_fields;
+        a.dt_given = d->dt_given;
+        a.save_start = d->save_start;
+        a.save_end = d->save_end;
+        a.save_everystep = d->save_everystep;
+        a.t0 = d->t0;
+        a.t1 = d->t1;
+        a.dt = d->dt;
+        a.q = d->q;
+        a.q2m = d->q2m;
+        a.mu = d->mu;
+        a.abstol = d->abstol;
+        a.reltol = d->reltol;
+        a.ssi = d->savestepinterval;
+        a.maxiters = d->maxiters;
+        a.nt = nt;
+        a.nout = nout;
+        a.n = n;
+        a.nslots = nslots;
+        a.y0 = y_d.as<double>();
+        a.q_i = q_i ? q_d.as<double>() : nullptr;
+        a.q2m_i = q2m_i ? q2m_d.as<double>() : nullptr;
+        a.mu_i = mu_i ? mu_d.as<double>() : nullptr;
+        a.dt_i = dt_i ? dt_d.as<double>() : nullptr;
+        a.tend_i = tend_i ? te_d.as<double>() : nullptr;
+        a.t_out = t_d.as<double>();
+        a.u_out = u_d.as<double>();
+        a.nsaved = ns_d.as<int32_t>();
+        a.retcode = rc_d.as<int8_t>();
+        a.nsteps = nst_d.as<int64_t>();
+        a.status = st_d.as<int32_t>();
+        a.queue = qq_d.as<unsigned long long>();
+        a.use_queue = d->alg == TP_GC_RK45 || d->term.flags != 0;
+        double budget = d->budget_s > 0 ? d->budget_s : 600.0;
+        a.budget_ns = (uint64_t)(budget * 1e9);
+        int block = d->block > 0 ? d->block : 128;
+        LaunchCfg cfg;
+        int occ = a.use_queue ? occupancy_gc(a, block) : 0;
+        int st = pick_launch(ctx, n, block, a.use_queue, occ, cfg);
+        if (st != TP_OK) {
+            delete r;
+            return st;
+        }
+        cudaEvent_t ev0, ev1;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, s);
+        if (n > 0) e = launch_gc(a, cfg, s);
+        cudaEventRecord(ev1, s);
+        int32_t status = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "guiding-centre kernel");
+        }
+        r->elapsed_ms = ms;
+        if (status == TP_E_OVERFLOW && d->alg == TP_GC_RK45 && attempt == 0) {
+            std::vector<int32_t> ns(n);
+            e = cudaMemcpy(ns.data(), ns_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                delete r;
+                return cuda_fail(ctx, e, "save counts");
+            }
+            int64_t mx = 0;
+            for (int32_t v : ns) mx = std::max<int64_t>(mx, v);
+            nslots = mx;
+            continue;
+        }
+        if (status != 0) {
+            delete r;
+            return status_to_error(ctx, status);
+        }
+        st = pack_to_host(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, st_d, r);
+        if (st == TP_OK && n > 0) {
+            e = cudaMemcpy(r->nsteps.data(), nst_d.p, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = cuda_fail(ctx, e, "step counts");
+        }
+        if (st != TP_OK) {
+            delete r;
+            return st;
+        }
+        *out = r;
+        return TP_OK;
+    }
+    delete r;
+    return fail(ctx, TP_E_OVERFLOW, "save slots exceeded after resizing");
+}
+
+// ---------------------------------------------------------------- results
+int tp_result_info(const tp_result* r, int64_t* n, int32_t* width, int64_t* total) {
+    if (!r) return TP_E_ARG;
+    if (n) *n = r->n;
+    if (width) *width = r->width;
+    if (total) *total = r->total;
+    return TP_OK;
+}
+
+int tp_result_copy(const tp_result* r, int32_t* nsaved, int8_t* retcode, int64_t* nsteps,
+                   double* t_packed, double* u_packed) {
+    if (!r) return TP_E_ARG;
+    if (nsaved && r->n) std::memcpy(nsaved, r->nsaved.data(), r->n * sizeof(int32_t));
+    if (retcode && r->n) std::memcpy(retcode, r->retcode.data(), r->n * sizeof(int8_t));
+    if (nsteps && r->n) std::memcpy(nsteps, r->nsteps.data(), r->n * sizeof(int64_t));
+    if (t_packed && r->total) std::memcpy(t_packed, r->t.data(), r->total * sizeof(double));
+    if (u_packed && r->total) std::memcpy(u_packed, r->u.data(), (size_t)r->total * r->width * sizeof(double));
+    return TP_OK;
+}
+
+int tp_result_elapsed_ms(const tp_result* r, double* ms) {
+    if (!r || !ms) return TP_E_ARG;
+    *ms = r->elapsed_ms;
+    return TP_OK;
+}
+
+void tp_result_destroy(tp_result* r) { delete r; }
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// tp_device.cuh -- device-side types shared by the push kernels.
+//
+// Field evaluation for the kinds of include/tp_abi.h, the termination
+// predicate, and the launch argument block.  Everything here is plain CUDA C++
+// for sm_100a; there is no contraction (GEMM) anywhere in this path, so no
+// tensor-core code: the kernels are FP64/FP32-pipe or L2-gather bound.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/tp_abi.h"
+
+namespace tpb {
+
+// ------------------------------------------------------------------ fields
+// One field as the kernels see it.  Grid data lives in a per-node table
+// (4 values per node, the 4th is padding) so that a corner is one aligned
+// 16-byte (float) or 32-byte (double) load.  When E and B are grids on the
+// same geometry the runtime builds one interleaved table (E then B per node,
+// 32 bytes per node in float) so that each corner of a particle-step is a
+// single 32-byte sector.
+struct DevField {
+    int32_t kind;
+    int32_t bc;
+    int32_t f64;      // grid table holds doubles
+    int32_t pad0;
+    double v[3];      // uniform value / affine constant
+    double J[9];      // affine Jacobian (row-major)
+    double rate[3];   // affine d/dt
+    double m[3];      // dipole moment
+    double c[3];      // dipole centre
+    double coef;      // dipole mu0/4pi
+    int32_t n[3];
+    int32_t pad1;
+    double x0[3];
+    double inv_dx[3];
+    double L[3];      // periodic length n*dx
+    float x0f[3];     // float copies for the FP32C kernels
+    float dxf[3];
+    float idxf[3];
+    float vf[3];      // uniform value / affine constant (float)
+    float Jf[9];
+    float ratef[3];
+    float mf[3];
+    float cf[3];
+    float coeff;
+    const void* tab;  // per-node table: float4 / double4 per node (x,y,z,0)
+    const float4* tab32;  // float table for the FP32C kernels (same as tab for float data)
+};
+
+struct DevFields {
+    DevField E, B;
+    const void* eb;   // interleaved table (E xyz0, B xyz0) per node, or null
+    const float4* eb32;   // float interleaved table for the FP32C kernels
+    int32_t eb_f64;
+    int32_t pad;
+};
+
+// Termination predicate (the reference's isoutside, as flags).
+struct DevTerm {
+    int32_t flags;
+    int32_t pad;
+    double rmin, rmax;
+    double lo[3], hi[3];
+    double tmax;
+};
+
+// Field configurations a kernel is specialised for (keeps register use down):
+//   FK_ANALYTIC  E and B analytic (zero / uniform / affine / dipole)
+//   FK_EBGRID    E and B grids on one geometry, interleaved table
+//   FK_GENERIC   anything else (separate grids, grid + analytic)
+enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2 };
+
+__host__ __device__ __forceinline__ int field_config_of(const DevFields& f) {
+    if (f.eb) return FK_EBGRID;
+    if (f.E.kind != TP_FIELD_GRID && f.B.kind != TP_FIELD_GRID) return FK_ANALYTIC;
+    return FK_GENERIC;
+}
+
+// ------------------------------------------------------------------ launch
+struct BorisArgs {
+    DevFields f;
+    DevTerm term;
+    int32_t alg, order, nsub, save_fields;
+    int32_t save_start, save_end, save_everystep, use_queue;
+    double safety, t0, t1, dt, q2m, m;
+    int64_t ssi, maxiters, step_cap;
+    int64_t n, nslots;
+    const double* u0;     // 6 x n (column-major)
+    const double* dt_i;   // optional
+    const double* tend_i; // optional
+    double* t_out;        // nslots x n
+    double* u_out;        // nslots x W x n
+    int32_t* nsaved;
+    int8_t* retcode;
+    int64_t* nsteps;
+    int32_t* status;      // device: first error code
+    unsigned long long* queue;  // persistent-schedule work counter
+    uint64_t budget_ns;
+    // FP32C only: per axis, wrap positions into the periodic box
+    int32_t wrap[3];
+    int32_t pad2;
+    double wrapL[3], wrap0[3];
+};
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void set_status(int32_t* status, int32_t code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+// Julia round(Int, x): ties to even (rint in the default rounding mode)
+__device__ __forceinline__ int64_t jl_round(double x) { return (int64_t)rint(x); }
+
+// _calculate_nout, src/boris/boris.jl:383-403
+__device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, bool se, bool sev) {
+    int64_t nout = 0;
+    if (ss) nout += 1;
+    if (sev) {
+        int64_t steps = nt / ssi;
+        bool last_is_step = (nt > 0) && (nt % ssi == 0);
+        nout += steps;
+        if (!se && last_is_step) nout -= 1;
+        if (se && !last_is_step) nout += 1;
+    } else if (se) {
+        nout += 1;
+    }
+    return nout;
+}
+
+}  // namespace tpb

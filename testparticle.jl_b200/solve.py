@@ -1,0 +1,231 @@
+"""solve() -- the reference's entry point, routed to the B200 library.
+
+Mirrors TestParticle.solve for
+  * TraceProblem with Boris() / MultistepBoris{N}(n)       src/boris/boris.jl:88-114
+  * TraceProblem with AdaptiveBoris / AdaptiveMultistep    src/boris/adaptive_boris.jl:21-38
+  * TraceGCProblem with alg = :rk4 / :rk45                 src/gc/gc_solver.jl:59-102
+with the same keywords and defaults.  prob_func is applied on the host for
+every trajectory to build the (6, N) initial-state table, as the reference's
+GPU path does (src/boris/boris_kernel.jl:290-294); a (6, N) u0 can be passed
+instead.  Only EnsembleB200 runs here: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .fields import as_field
+from .problems import (Boris, EnsembleB200, EnsembleContext, MultistepBoris, TraceGCProblem,
+                       TraceProblem, as_term)
+from .runtime import Context
+from .solution import EnsembleSolution
+
+_PREC = {"fp64": _abi.TP_PREC_FP64, "fp32c": _abi.TP_PREC_FP32C}
+_SCHED = {"auto": _abi.TP_SCHED_AUTO, "static": _abi.TP_SCHED_STATIC, "queue": _abi.TP_SCHED_QUEUE}
+_GC_PREC = {"fp64": _abi.TP_GC_PREC_FP64, "fp32": _abi.TP_GC_PREC_FP32RHS, "fp32rhs": _abi.TP_GC_PREC_FP32RHS,
+            "fp32c": _abi.TP_GC_PREC_FP32RHS}
+
+
+def _initial_table(prob, trajectories: int, width: int) -> np.ndarray:
+    u0 = np.asarray(prob.u0, dtype=np.float64)
+    if u0.ndim == 2:
+        if u0.shape[0] != width:
+            raise ValueError(f"u0 table must be ({width}, N)")
+        if prob.prob_func is not None:
+            raise ValueError("pass either a (width, N) u0 table or a prob_func, not both")
+        if trajectories not in (1, u0.shape[1]):
+            raise ValueError("trajectories must equal the number of u0 columns")
+        return np.ascontiguousarray(u0.T)
+    if u0.shape != (width,):
+        raise ValueError(f"u0 must have {width} components")
+    if prob.prob_func is None:
+        return np.tile(u0, (trajectories, 1))
+    out = np.empty((trajectories, width))
+    for i in range(trajectories):
+        new = prob.prob_func(prob, EnsembleContext(i + 1))
+        out[i] = np.asarray(new.u0, dtype=np.float64)
+    return out
+
+
+@dataclass
+class BorisPlan:
+    """Everything a full-orbit solve hands to the library (also used by the tests)."""
+
+    desc: _abi.RunDesc
+    E: object
+    B: object
+    u0: np.ndarray          # (N, 6)
+    dt_i: Optional[np.ndarray]
+    tend_i: Optional[np.ndarray]
+    alg_name: str
+    device: int
+
+
+@dataclass
+class GCPlan:
+    desc: _abi.GCDesc
+    E: object
+    B: object
+    y0: np.ndarray          # (N, 4)
+    q_i: Optional[np.ndarray]
+    q2m_i: Optional[np.ndarray]
+    mu_i: Optional[np.ndarray]
+    dt_i: Optional[np.ndarray]
+    tend_i: Optional[np.ndarray]
+    alg_name: str
+    device: int
+
+
+def plan_boris(prob, balg, ens=None, *, trajectories=1, savestepinterval=1, dt=None, isoutside=None,
+               save_start=True, save_end=True, save_everystep=True, save_fields=False, save_work=False,
+               maxiters=None, step_cap=0, tend=None) -> BorisPlan:
+    ens = ens if ens is not None else EnsembleB200()
+    if not isinstance(ens, EnsembleB200):
+        raise NotImplementedError("this package runs ensembles on the B200 only: use EnsembleB200()")
+    if save_work:
+        raise NotImplementedError("save_work (work rates at save points) is not implemented on the B200 yet")
+    adaptive = getattr(balg, "adaptive", False)
+    if not adaptive and dt is None:
+        raise TypeError("solve() with a fixed-step Boris algorithm needs dt")
+    q2m, m, E, B, _F = prob.p
+    E, B = as_field(E), as_field(B)
+    desc = _abi.RunDesc()
+    if isinstance(balg, MultistepBoris):
+        desc.alg = _abi.TP_ALG_ADAPTIVE_MULTISTEP if adaptive else _abi.TP_ALG_MULTISTEP
+        desc.order = balg.N
+        desc.nsub = balg.n
+    elif isinstance(balg, Boris):
+        desc.alg = _abi.TP_ALG_ADAPTIVE if adaptive else _abi.TP_ALG_BORIS
+        desc.order, desc.nsub = 2, 1
+    else:
+        raise TypeError(f"unsupported algorithm {balg!r}")
+    desc.safety = float(balg.safety)
+    desc.precision = _PREC[ens.precision]
+    desc.t0, desc.t1 = float(prob.tspan[0]), float(prob.tspan[1])
+    dt_arr = None
+    if dt is not None and np.ndim(dt) > 0:
+        dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        desc.dt = float(dt_arr[0]) if dt_arr.size else 0.0
+    elif dt is not None:
+        desc.dt = float(dt)
+    desc.q2m, desc.m = float(q2m), float(m)
+    desc.savestepinterval = int(savestepinterval)
+    desc.maxiters = int(1_000_000 if maxiters is None else maxiters)
+    desc.save_start, desc.save_end = int(save_start), int(save_end)
+    desc.save_everystep, desc.save_fields = int(save_everystep), int(save_fields)
+    desc.term = as_term(isoutside).descriptor()
+    desc.step_cap = int(step_cap)
+    desc.schedule = _SCHED[ens.schedule]
+    desc.block = int(ens.block)
+    desc.budget_s = float(ens.budget_s)
+    u0 = _initial_table(prob, trajectories, 6)
+    tend_arr = None if tend is None else np.ascontiguousarray(tend, dtype=np.float64)
+    name = {_abi.TP_ALG_BORIS: "boris", _abi.TP_ALG_MULTISTEP: "multistep_boris",
+            _abi.TP_ALG_ADAPTIVE: "adaptive_boris",
+            _abi.TP_ALG_ADAPTIVE_MULTISTEP: "adaptive_multistep_boris"}[desc.alg]
+    return BorisPlan(desc, E, B, u0, dt_arr, tend_arr, name, ens.device)
+
+
+def plan_gc(prob, ens=None, *, trajectories=1, savestepinterval=1, dt=None, isoutside=None,
+            save_start=True, save_end=True, save_everystep=True, alg="rk4", abstol=1.0e-6,
+            reltol=1.0e-6, maxiters=10000, save_fields=False, save_work=False, tend=None) -> GCPlan:
+    ens = ens if ens is not None else EnsembleB200()
+    if not isinstance(ens, EnsembleB200):
+        raise NotImplementedError("this package runs ensembles on the B200 only: use EnsembleB200()")
+    if save_work:
+        raise NotImplementedError("save_work is not implemented on the B200 yet")
+    alg = str(alg).lstrip(":")
+    if alg not in ("rk4", "rk45"):
+        import warnings
+        warnings.warn("Only :rk4 and :rk45 are supported for native TraceGCProblem currently. Using :rk4.")
+        alg = "rk4"
+    q, q2m, mu, E, B = prob.p[:5]
+    desc = _abi.GCDesc()
+    desc.alg = _abi.TP_GC_RK4 if alg == "rk4" else _abi.TP_GC_RK45
+    desc.precision = _GC_PREC[ens.precision]
+    desc.t0, desc.t1 = float(prob.tspan[0]), float(prob.tspan[1])
+    desc.dt_given = int(dt is not None)
+    dt_arr = None
+    if dt is not None and np.ndim(dt) > 0:
+        dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        desc.dt = float(dt_arr[0]) if dt_arr.size else 0.0
+    else:
+        desc.dt = float(dt) if dt is not None else 0.0
+    tend_arr = None if tend is None else np.ascontiguousarray(tend, dtype=np.float64)
+    pp_mu = pp_q = pp_q2m = None
+    if np.ndim(mu) > 0:
+        pp_mu = np.ascontiguousarray(mu, dtype=np.float64)
+        desc.mu = 0.0
+    else:
+        desc.mu = float(mu)
+    if np.ndim(q) > 0:  # extension: per-particle charge / charge-to-mass arrays
+        pp_q = np.ascontiguousarray(q, dtype=np.float64)
+        pp_q2m = np.ascontiguousarray(q2m, dtype=np.float64)
+        desc.q, desc.q2m = 0.0, 0.0
+    else:
+        desc.q, desc.q2m = float(q), float(q2m)
+    desc.abstol, desc.reltol = float(abstol), float(reltol)
+    desc.savestepinterval = int(savestepinterval)
+    desc.maxiters = int(maxiters)
+    desc.save_start, desc.save_end = int(save_start), int(save_end)
+    desc.save_everystep, desc.save_fields = int(save_everystep), int(save_fields)
+    desc.term = as_term(isoutside).descriptor()
+    desc.block = int(ens.block)
+    desc.budget_s = float(ens.budget_s)
+    y0 = _initial_table(prob, trajectories, 4)
+    return GCPlan(desc, as_field(E), as_field(B), y0, pp_q, pp_q2m, pp_mu, dt_arr, tend_arr, alg, ens.device)
+
+
+def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None, isoutside=None,
+          save_start: bool = True, save_end: bool = True, save_everystep: bool = True,
+          save_fields: bool = False, save_work: bool = False, maxiters=None, alg=None,
+          abstol: float = 1.0e-6, reltol: float = 1.0e-6, step_cap: int = 0, tend=None,
+          batch_size=None, seed=None) -> EnsembleSolution:
+    """TestParticle.solve(prob, alg, ensemblealg=EnsembleB200(); kwargs...)."""
+    if isinstance(prob, TraceGCProblem):
+        p = plan_gc(prob, args[0] if args else None, trajectories=trajectories,
+                    savestepinterval=savestepinterval, dt=dt, isoutside=isoutside, save_start=save_start,
+                    save_end=save_end, save_everystep=save_everystep, alg=alg or "rk4", abstol=abstol,
+                    reltol=reltol, maxiters=10000 if maxiters is None else maxiters,
+                    save_fields=save_fields, save_work=save_work, tend=tend)
+        ctx = Context.get(p.device)
+        t0 = time.perf_counter()
+        r = ctx.gc_run(p.desc, p.E, p.B, p.y0, p.q_i, p.q2m_i, p.mu_i, p.dt_i, p.tend_i)
+        wall = time.perf_counter() - t0
+        return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall)
+    if not isinstance(prob, TraceProblem):
+        raise TypeError("prob must be a TraceProblem or TraceGCProblem")
+    if not args:
+        raise TypeError("solve(prob::TraceProblem, alg, [ensemblealg]; kwargs...)")
+    p = plan_boris(prob, args[0], args[1] if len(args) > 1 else None, trajectories=trajectories,
+                   savestepinterval=savestepinterval, dt=dt, isoutside=isoutside, save_start=save_start,
+                   save_end=save_end, save_everystep=save_everystep, save_fields=save_fields,
+                   save_work=save_work, maxiters=maxiters, step_cap=step_cap, tend=tend)
+    ctx = Context.get(p.device)
+    t0 = time.perf_counter()
+    r = ctx.boris_run(p.desc, p.E, p.B, p.u0, p.dt_i, p.tend_i)
+    wall = time.perf_counter() - t0
+    return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall)
+
+
+def prepare_gc(xv, E, B, *, species=None, q=None, m=None, t: float = 0.0, device: int = 0):
+    """prepare_gc(xv, E, B; species, q, m) -> (stateinit_gc, (q, q2m, mu, E, B)).
+
+    Computed on the device (src/gc/gc.jl:13-84).  Extension: xv may be a
+    (6, N) table; the result is then a (4, N) table and an array of mu.
+    """
+    from .constants import Proton
+    from .problems import _species
+    qq, mm = _species(species if species is not None else Proton, q, m)
+    E, B = as_field(E), as_field(B)
+    xv = np.asarray(xv, dtype=np.float64)
+    table = xv.ndim == 2
+    xs = xv.T if table else xv.reshape(1, 6)
+    y0, mu = Context.get(device).gc_prepare(E, B, xs, qq, mm, t)
+    if table:
+        return y0.T.copy(), (qq, qq / mm, mu, E, B)
+    return y0[0], (qq, qq / mm, float(mu[0]), E, B)

@@ -1,0 +1,329 @@
+"""GPU parity: the CUDA library against the CPU oracle on the same seeded inputs.
+
+Bars (per the reference's own kernel-vs-native test, test_boris_kernel.jl:92):
+  * FP64 Boris / adaptive Boris / GC, +-*/sqrt-only arithmetic: identical to
+    the oracle (both follow the reference's operation order, no contraction);
+    asserted as relative error <= 1e-13.
+  * FP64 MultistepBoris (CUDA vs glibc atan/sincos differ in the last bit):
+    relative error <= 1e-10 after the stated steps.
+  * FP32C: relative position error <= 1e-5 against the float64 oracle on
+    non-chaotic (uniform / dipole) cases, stated for gridded turbulence.
+All calls go through the C ABI (libtpb200.so) via the package's solve().
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import julia_isapprox
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    scale = np.maximum(np.abs(b), np.abs(b).max(axis=0, keepdims=True) * 1e-12 + 1e-300)
+    return float(np.max(np.abs(a - b) / scale)) if a.size else 0.0
+
+
+def _pos_rel(gpu_u, ref_u):
+    """max over saves of |x_gpu - x_ref| / |x_ref| (positions only)."""
+    d = np.linalg.norm(gpu_u[:, :3] - ref_u[:, :3], axis=1)
+    r = np.linalg.norm(ref_u[:, :3], axis=1)
+    return float(np.max(d / np.maximum(r, 1e-300)))
+
+
+def _both(tp, orc, prob, alg, ens=None, **kw):
+    ens = ens or tp.EnsembleB200()
+    sols = tp.solve(prob, alg, ens, **kw)
+    plan = tp.plan_boris(prob, alg, ens, **kw)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    return sols, ref
+
+
+def _check_same_layout(sols, ref):
+    assert np.array_equal(sols.nsaved, ref.nsaved)
+    assert np.array_equal(sols.retcodes, ref.retcode)
+    assert np.array_equal(sols.nsteps, ref.nsteps)
+
+
+# ------------------------------------------------------------------ config 1 (CPU-runnable)
+def test_config1_plain_boris_fp64_matches_oracle(tp, orc):
+    w = tp.workloads.config1()
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=tp.Proton))
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=w.dt, savestepinterval=w.savestepinterval)
+    _check_same_layout(sols, ref)
+    assert sols.nsaved[0] == 101
+    assert np.array_equal(sols.t_all, ref.t)
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+    # |v| conserved under pure-B rotation to float64 round-off
+    v0 = np.linalg.norm(w.u0[3:6].T, axis=1)
+    vend = np.linalg.norm(sols.final_states()[:, 3:6], axis=1)
+    assert np.max(np.abs(vend - v0) / v0) < 1e-12
+
+
+def test_reference_boris_kats_on_gpu(tp):
+    # test_boris.jl:40-61 through the B200 path
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param)
+    sol = tp.solve(prob, tp.Boris(), dt=3.0e-11, savestepinterval=10).u[0]
+    assert julia_isapprox(sol.u[-1], [-0.00010199137926394769, 3.46340469171306e-5, 0.0,
+                                      -60893.043824907196, -79322.36263335795, 0.0])
+    assert julia_isapprox(sol(1.5e-8), [-3.8587882024745045e-5, 5.3855907133664956e-5, 0.0,
+                                        -94689.58829601014, 32154.033469101283, 0.0])
+    assert sol.retcode == "Success" and len(sol.t) == 101
+
+    def pf(prob, ctx):
+        u = list(prob.u0)
+        u[4] = ctx.sim_id * 1.0e5
+        return tp.remake(prob, u0=u)
+
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param, prob_func=pf)
+    sols = tp.solve(prob, tp.Boris(), tp.EnsembleB200(), dt=3.0e-11, savestepinterval=1000, trajectories=4)
+    assert julia_isapprox(sum(s.u[-1][3] for s in sols.u), -608930.4382490724)
+
+
+@pytest.mark.parametrize("flags,n_expected", [
+    (dict(savestepinterval=10), 101),
+    (dict(savestepinterval=10, save_everystep=False, save_start=False, save_end=True), 1),
+    (dict(savestepinterval=10, save_everystep=False, save_start=True, save_end=True), 2),
+    (dict(savestepinterval=10, save_everystep=False, save_start=True, save_end=False), 1),
+    (dict(savestepinterval=10, save_everystep=True, save_start=False, save_end=False), 99),
+    (dict(savestepinterval=3, save_everystep=True, save_start=True, save_end=True), 335),
+])
+def test_saving_flags_gpu(tp, orc, flags, n_expected):
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param)
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=3.0e-11, **flags)
+    _check_same_layout(sols, ref)
+    assert sols.nsaved[0] == n_expected
+    assert np.array_equal(sols.t_all, ref.t)
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+def test_save_fields_gpu(tp, orc):
+    w = tp.workloads.config1(64)
+    prob = tp.TraceProblem(w.u0, (0.0, 500 * w.dt), tp.prepare(w.E, w.B))
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=w.dt, savestepinterval=50, save_fields=True)
+    assert sols.u_all.shape[1] == 12
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+def test_argument_errors_gpu(tp):
+    E = tp.UniformField((0.0, 1.0e5, 0.0))
+    B = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0], (0.0, 1.0e-9), tp.prepare(E, B, species=tp.Electron))
+    with pytest.raises(tp.ArgumentError):
+        tp.solve(prob, tp.Boris(), dt=1.0e-11, maxiters=50)
+    with pytest.raises(tp.ArgumentError):
+        tp.solve(prob, tp.Boris(), dt=np.finfo(float).eps)
+
+
+# ------------------------------------------------------------------ multistep / dipole
+@pytest.mark.parametrize("N,n", [(2, 1), (2, 2), (4, 2), (6, 2), (4, 1)])
+def test_multistep_dipole_fp64(tp, orc, N, n):
+    w = tp.workloads.config3(256, nt=2000, ssi=500)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=tp.Proton))
+    sols, ref = _both(tp, orc, prob, tp.MultistepBoris(N, n), dt=w.dt, tend=w.tend,
+                      savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+    _check_same_layout(sols, ref)
+    assert np.array_equal(sols.t_all, ref.t)
+    assert _rel(sols.u_all, ref.u) <= 1e-10
+
+
+def test_multistep_exb_and_gyration_gpu(tp):
+    # test_boris.jl:95-210 through the B200 path
+    param = (1.0, 1.0, tp.UniformField((0.0, 1.0, 0.0)), tp.UniformField((0.0, 0.0, 1.0)), tp.ZeroField())
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0.0, 10.0), param)
+    for alg in (tp.Boris(), tp.MultistepBoris(2, 2), tp.MultistepBoris(4, 2), tp.MultistepBoris(6, 2)):
+        end = tp.solve(prob, alg, dt=0.1).u[0].u[-1]
+        assert abs(end[0] - 10.0) <= 1e-6 and abs(end[3] - 1.0) <= 1e-6
+    param = (1.0, 1.0, tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0)), tp.ZeroField())
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0.0, 2 * math.pi), param)
+    for alg in (tp.Boris(), tp.MultistepBoris(2, 4), tp.MultistepBoris(4, 4), tp.MultistepBoris(6, 4)):
+        end = tp.solve(prob, alg, dt=0.1).u[0].u[-1]
+        assert math.hypot(*end[:3]) < 0.02 and abs(math.hypot(*end[3:6]) - 1.0) <= 2.0e-3
+
+
+# ------------------------------------------------------------------ adaptive
+@pytest.mark.parametrize("alg", ["adaptive", "adaptive_ms4"])
+def test_adaptive_dipole_fp64(tp, orc, alg):
+    w = tp.workloads.config3(256, nt=2000, ssi=50)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=tp.Proton))
+    a = tp.AdaptiveBoris(0.1) if alg == "adaptive" else tp.AdaptiveMultistepBoris(4, 2, 0.1)
+    sols, ref = _both(tp, orc, prob, a, tend=w.tend, savestepinterval=w.savestepinterval,
+                      isoutside=w.isoutside, step_cap=2000)
+    _check_same_layout(sols, ref)      # identical step decisions
+    assert np.array_equal(sols.t_all, ref.t) if alg == "adaptive" else _rel(sols.t_all, ref.t) <= 1e-10
+    assert _rel(sols.u_all, ref.u) <= (1e-13 if alg == "adaptive" else 1e-10)
+
+
+def test_adaptive_reference_kat_gpu(tp):
+    # test_boris.jl:212-248 through the B200 path (gradient B = AffineField)
+    tperiod = abs(tp.get_gyroperiod(0.01, q=tp.qe, m=tp.me))
+    E = tp.UniformField((0.0, 1.0e5, 0.0))
+    B = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 1.0e7, 0.0, 0.0], (0.0, 200 * tperiod),
+                           tp.prepare(E, B, species=tp.Electron))
+    sol = tp.solve(prob, tp.AdaptiveBoris(0.1)).u[0]
+    assert sol.t[-2] - sol.t[-3] < 0.8 * (sol.t[10] - sol.t[9])
+
+
+def test_termination_boris_gpu(tp, orc):
+    # test_boundary.jl:10-58 with the NaN region replaced by the shell predicate
+    p = (1.0, 1.0, tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0)), tp.ZeroField())
+    prob = tp.TraceProblem([0.9, 0.0, 0.0, 0.0, 1.0, 0.0], (0.0, 1.0), p)
+    out = tp.TerminateNaN() | tp.TerminateShell(rmax=1.0)
+    for alg, kw in ((tp.Boris(), dict(dt=0.2)), (tp.AdaptiveBoris(0.05), {})):
+        sols, ref = _both(tp, orc, prob, alg, isoutside=out, **kw)
+        _check_same_layout(sols, ref)
+        sol = sols.u[0]
+        assert sol.retcode == "Terminated" and np.linalg.norm(sol.u[-1][:3]) <= 1.0
+        assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+def test_queue_and_static_schedules_agree(tp):
+    w = tp.workloads.config3(512, nt=1000, ssi=250)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
+    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+    a = tp.solve(prob, tp.MultistepBoris(4, 2), tp.EnsembleB200(schedule="static"), **kw)
+    b = tp.solve(prob, tp.MultistepBoris(4, 2), tp.EnsembleB200(schedule="queue"), **kw)
+    assert np.array_equal(a.nsaved, b.nsaved) and np.array_equal(a.u_all, b.u_all)
+
+
+# ------------------------------------------------------------------ gridded fields
+def _small_grid_workload(tp, n=512, nx=32, nt=2000, ssi=500):
+    dx = 1.0e5
+    Ea, Ba, L = tp.workloads.turbulent_grid(nx, dx, 5.0e-9, nmodes=16)
+    E = tp.FieldInterpolator(Ea, (0.0, 0.0, 0.0), (dx,) * 3, tp.WrapExtrap())
+    B = tp.FieldInterpolator(Ba, (0.0, 0.0, 0.0), (dx,) * 3, tp.WrapExtrap())
+    rng = tp.workloads.SplitMix64(99)
+    u0 = np.empty((6, n))
+    u0[:3] = rng.uniform(3 * n, 0.0, L).reshape(3, n)
+    u0[3:] = rng.normal(3 * n, 2.0e5 / math.sqrt(2)).reshape(3, n)
+    dt = tp.get_gyroperiod(5.0e-9) / 50
+    return tp.TraceProblem(u0, (0.0, nt * dt), tp.prepare(E, B)), dt, ssi
+
+
+def test_grid_boris_fp64_matches_oracle(tp, orc):
+    prob, dt, ssi = _small_grid_workload(tp)
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=dt, savestepinterval=ssi)
+    _check_same_layout(sols, ref)
+    assert np.array_equal(sols.t_all, ref.t)
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+@pytest.mark.parametrize("bc", ["fill", "clamp"])
+def test_grid_boundaries_fp64(tp, orc, bc):
+    # separate E / B tables (E uniform), non-periodic boundary rules
+    dx = 1.0e5
+    _, Ba, L = tp.workloads.turbulent_grid(16, dx, 5.0e-9, nmodes=8)
+    b = tp.FillExtrap() if bc == "fill" else tp.ClampExtrap()
+    B = tp.FieldInterpolator(Ba, (0.0, 0.0, 0.0), (dx,) * 3, b)
+    rng = tp.workloads.SplitMix64(7)
+    n = 256
+    u0 = np.empty((6, n))
+    u0[:3] = rng.uniform(3 * n, 0.2 * L, 0.8 * L).reshape(3, n)
+    u0[3:] = rng.normal(3 * n, 1.0e5).reshape(3, n)
+    dt = tp.get_gyroperiod(5.0e-9) / 50
+    prob = tp.TraceProblem(u0, (0.0, 1000 * dt), tp.prepare(tp.UniformField((0.0, 1e-4, 0.0)), B))
+    out = tp.TerminateNaN() if bc == "fill" else None
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=dt, savestepinterval=100, isoutside=out)
+    _check_same_layout(sols, ref)
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+def test_grid_fp32c_error_stated(tp, orc):
+    prob, dt, ssi = _small_grid_workload(tp, nt=500, ssi=100)
+    sols = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=dt, savestepinterval=ssi)
+    plan = tp.plan_boris(prob, tp.Boris(), tp.EnsembleB200(), dt=dt, savestepinterval=ssi)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0)
+    assert np.array_equal(sols.nsaved, ref.nsaved)
+    # 500 steps (10 gyroperiods) of a turbulent field: float32 stays close
+    assert _pos_rel(sols.u_all, ref.u) <= 1e-5
+
+
+# ------------------------------------------------------------------ FP32C in analytic fields
+def test_fp32c_uniform_and_dipole(tp, orc):
+    w = tp.workloads.config1(1000)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
+    sols = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=w.dt,
+                    savestepinterval=w.savestepinterval)
+    plan = tp.plan_boris(prob, tp.Boris(), dt=w.dt, savestepinterval=w.savestepinterval)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0)
+    assert np.array_equal(sols.nsaved, ref.nsaved)
+    # positions are O(1 m) displacements around O(1e6 m) gyro-orbits: compare on the orbit scale
+    d = np.abs(sols.u_all[:, :3] - ref.u[:, :3]).max()
+    assert d <= 1e-5 * np.abs(ref.u[:, :3]).max()
+
+    w = tp.workloads.config3(1024, nt=10_000, ssi=1000)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
+    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+    sols = tp.solve(prob, tp.MultistepBoris(4, 2), tp.EnsembleB200(precision="fp32c"), **kw)
+    plan = tp.plan_boris(prob, tp.MultistepBoris(4, 2), **kw)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    both = (sols.retcodes == 1) & (ref.retcode == 1)
+    assert both.mean() > 0.95
+    fs, fr = sols.final_states()[both], ref.final_states()[both]
+    err = np.linalg.norm(fs[:, :3] - fr[:, :3], axis=1) / np.linalg.norm(fr[:, :3], axis=1)
+    # <= 1e-5 relative position error after 1e4 steps
+    assert np.median(err) <= 1e-5
+    assert np.quantile(err, 0.99) <= 1e-4
+
+
+# ------------------------------------------------------------------ guiding centre
+def _gc_dipole(tp, orc):
+    Ek = 5.0e7
+    v0 = tp.sph2cart(tp.energy2velocity(Ek), math.pi / 4, 0.0)
+    r0 = tp.sph2cart(2.5 * tp.Re, math.pi / 2, 0.0)
+    E, B = tp.ZeroField(), tp.DipoleField(tp.BMoment_Earth)
+    y0, p = tp.prepare_gc(np.concatenate([r0, v0]), E, B, species=tp.Proton)
+    y0o, muo = orc.gc_prepare(E, B, np.concatenate([r0, v0]), tp.qi, tp.mi)
+    assert _rel(y0, y0o[0]) <= 1e-14 and abs(p[2] - muo[0]) <= 1e-14 * muo[0]
+    return tp.TraceGCProblem(y0, (0.0, 1.0), p)
+
+
+def test_gc_reference_counts_gpu(tp, orc):
+    # test_gc.jl:190-251 through the B200 path
+    prob = _gc_dipole(tp, orc)
+    s = tp.solve(prob, dt=1.0e-4, alg="rk4").u[0]
+    assert len(s.t) == 10001 and s.retcode == "MaxIters"
+    assert len(tp.solve(prob, dt=1.0e-4, alg="rk4", save_everystep=False).u[0].t) == 2
+    assert len(tp.solve(prob, dt=1.0e-4, alg="rk4", isoutside=tp.TerminateTime(0.5)).u[0].t) == 5001
+    s = tp.solve(prob, dt=1.0e-4, alg="rk45").u[0]
+    assert len(s.t) == 61 and s.retcode == "Success"
+    s = tp.solve(prob, alg="rk45").u[0]
+    assert len(s.t) == 58 and s.retcode == "Success"
+
+
+@pytest.mark.parametrize("alg", ["rk4", "rk45"])
+def test_gc_fp64_matches_oracle(tp, orc, alg):
+    prob = _gc_dipole(tp, orc)
+    kw = dict(dt=1.0e-4, alg=alg)
+    sols = tp.solve(prob, **kw)
+    plan = tp.plan_gc(prob, **kw)
+    ref = orc.gc_run(plan.desc, plan.E, plan.B, plan.y0)
+    _check_same_layout(sols, ref)
+    assert np.array_equal(sols.t_all, ref.t)
+    assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+def test_gc_config4_subset(tp, orc):
+    w = tp.workloads.config4(512)
+    prob = tp.TraceGCProblem(w.y0, (0.0, 1.0), (w.q, w.q2m, w.mu, w.E, w.B))
+    dt = w.tau_b / 200
+    kw = dict(dt=dt, tend=5 * w.tau_b, alg="rk4", savestepinterval=100)
+    sols = tp.solve(prob, **kw)
+    plan = tp.plan_gc(prob, **kw)
+    ref = orc.gc_run(plan.desc, plan.E, plan.B, plan.y0, plan.q_i, plan.q2m_i, plan.mu_i,
+                     dt_i=plan.dt_i, tend_i=plan.tend_i)
+    _check_same_layout(sols, ref)
+    assert _rel(sols.u_all, ref.u) <= 1e-12
+    s32 = tp.solve(prob, tp.EnsembleB200(precision="fp32"), **kw)
+    assert np.array_equal(s32.nsaved, ref.nsaved)
+    err = np.linalg.norm(s32.final_states()[:, :3] - ref.final_states()[:, :3], axis=1) / \
+        np.linalg.norm(ref.final_states()[:, :3], axis=1)
+    assert np.median(err) <= 1e-4

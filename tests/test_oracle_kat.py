@@ -1,0 +1,355 @@
+"""Pin the CPU oracle to the reference's own known-answer tests.
+
+Every expected number below is quoted from the reference test suite
+(TestParticle.jl v0.23.2, test/...); the oracle restates the reference
+solver, so these checks are what makes it a trustworthy checker for the
+CUDA library.  Julia closures of those tests become Python callables passed
+to the oracle as C callbacks.  No GPU needed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import julia_isapprox
+
+
+def _solve(tp, orc, u0, tspan, param, alg, E=None, B=None, isoutside=None, trajectories=1,
+           prob_func=None, **kw):
+    """Oracle solve of a TraceProblem; E/B override the param fields with callables."""
+    q2m, m, Ep, Bp, F = param
+    place = (q2m, m, tp.ZeroField(), tp.ZeroField(), F)
+    prob = tp.TraceProblem(u0, tspan, place, prob_func=prob_func)
+    plan = tp.plan_boris(prob, alg, tp.EnsembleB200(), trajectories=trajectories, **kw)
+    return orc.boris_run(plan.desc, E if E is not None else Ep, B if B is not None else Bp, plan.u0,
+                         plan.dt_i, plan.tend_i, isoutside=isoutside)
+
+
+# ------------------------------------------------------------------ test/test_boris.jl
+def test_basic_boris_final_state_and_interpolation(tp, orc):
+    # test_boris.jl:40-61
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param, tp.Boris(),
+               dt=3.0e-11, savestepinterval=10)
+    t, u = r.traj(0)
+    assert julia_isapprox(u[-1], [-0.00010199137926394769, 3.46340469171306e-5, 0.0,
+                                  -60893.043824907196, -79322.36263335795, 0.0])
+    assert t.size == u.shape[0]
+    sol = tp.TraceSolution(t, u, "Success", "boris")
+    assert julia_isapprox(sol(3.0e-8 / 2), [-3.8587882024745045e-5, 5.3855907133664956e-5, 0.0,
+                                            -94689.58829601014, 32154.033469101283, 0.0])
+
+
+def test_basic_boris_ensembles(tp, orc):
+    # test_boris.jl:63-78 (prob_func sets vy = sim_id * 1e5)
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+
+    def pf(prob, ctx):
+        u = list(prob.u0)
+        u[4] = ctx.sim_id * 1.0e5
+        return tp.remake(prob, u0=u)
+
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param, tp.Boris(),
+               dt=3.0e-11, savestepinterval=1000, trajectories=4, prob_func=pf)
+    assert julia_isapprox(r.final_states()[:, 3].sum(), -608930.4382490724)
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param, tp.Boris(),
+               dt=3.0e-11, savestepinterval=1000, trajectories=2, prob_func=pf)
+    assert julia_isapprox(r.final_states().sum(), -420646.2195768674)
+
+
+def test_time_varying_field_accumulated_time(tp, orc):
+    # test_boris.jl:80-88: the field depends on t, which pins the accumulated-time rule
+    def B(x, t):
+        if x[0] > 100 * t:
+            bz = 1.0e-8
+        elif x[0] < -10.0:
+            bz = 1.0e-8
+        else:
+            bz = 0.0
+        return (0.0, 0.0, bz)
+
+    param = tp.prepare(tp.ZeroField(), tp.ZeroField(), species=tp.Electron)
+    r = _solve(tp, orc, [-1.0, 0.0, 0.0, 1.0e6, 0.0, 0.0], (0.0, 0.01), param, tp.Boris(), B=B,
+               dt=1.0e-4, savestepinterval=100)
+    assert julia_isapprox(r.final_states()[0, 0], -512.8807214528281)
+
+
+@pytest.mark.parametrize("alg", ["boris", "ms2n2", "h4n2", "h6n2", "h4n1"])
+def test_multistep_exb_drift(tp, orc, alg):
+    # test_boris.jl:95-125,162-188: E x B drift reaches x = 10 at t = 10
+    algs = {"boris": tp.Boris(), "ms2n2": tp.MultistepBoris(2, 2), "h4n2": tp.MultistepBoris(4, 2),
+            "h6n2": tp.MultistepBoris(6, 2), "h4n1": tp.MultistepBoris(4, 1)}
+    param = (1.0, 1.0, tp.UniformField((0.0, 1.0, 0.0)), tp.UniformField((0.0, 0.0, 1.0)), tp.ZeroField())
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0.0, 10.0), param, algs[alg], dt=0.1)
+    end = r.final_states()[0]
+    assert abs(end[0] - 10.0) <= 1e-6
+    assert abs(end[3] - 1.0) <= 1e-6
+
+
+@pytest.mark.parametrize("alg", ["boris", "ms2n2", "ms2n4", "h4n4", "h6n4"])
+def test_multistep_gyration_closes(tp, orc, alg):
+    # test_boris.jl:127-159,190-209
+    algs = {"boris": tp.Boris(), "ms2n2": tp.MultistepBoris(2, 2), "ms2n4": tp.MultistepBoris(2, 4),
+            "h4n4": tp.MultistepBoris(4, 4), "h6n4": tp.MultistepBoris(6, 4)}
+    param = (1.0, 1.0, tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0)), tp.ZeroField())
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0.0, 2 * math.pi), param, algs[alg], dt=0.1)
+    end = r.final_states()[0]
+    assert math.hypot(*end[:3]) < 0.02
+    assert abs(math.hypot(*end[3:6]) - 1.0) <= 2.0e-3
+
+
+def test_adaptive_boris_shrinks_dt_and_conserves_energy(tp, orc):
+    # test_boris.jl:212-248: B = (0, 0, 0.01 (1 + x)), E = (0, 1e5, 0), electron
+    tperiod = abs(tp.get_gyroperiod(0.01, q=tp.qe, m=tp.me))
+    E = tp.UniformField((0.0, 1.0e5, 0.0))
+    B = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    param = tp.prepare(E, B, species=tp.Electron)
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0e7, 0.0, 0.0], (0.0, 200 * tperiod), param,
+               tp.AdaptiveBoris(0.1))
+    t, u = r.traj(0)
+    dt_end = t[-2] - t[-3]
+    dt_start = t[10] - t[9]
+    assert dt_end < 0.8 * dt_start
+
+    def energy(s):
+        return 0.5 * tp.me * np.dot(s[3:6], s[3:6]) + tp.qe * (-1.0e5 * s[1])
+
+    assert abs(energy(u[-1]) - energy(u[0])) <= 1.0e-3 * max(abs(energy(u[0])), abs(energy(u[-1])))
+
+
+def test_nonzero_tspan_start(tp, orc):
+    # test_boris.jl:250-272: B exists only for t > 5; tspan starts at 10
+    def B(x, t):
+        return (0.0, 0.0, 0.01) if t > 5 else (0.0, 0.0, 0.0)
+
+    param = tp.prepare(tp.ZeroField(), tp.ZeroField())
+    u0 = [0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0]
+    r = _solve(tp, orc, u0, (10.0, 10.1), param, tp.Boris(), B=B, dt=0.001)
+    assert abs(r.final_states()[0, 3]) < 1.0e5 - 100
+    r = _solve(tp, orc, u0, (10.0, 10.1), param, tp.AdaptiveBoris(0.1), B=B)
+    assert abs(r.final_states()[0, 3]) < 1.0e5 - 100
+
+
+@pytest.mark.parametrize("flags,n_expected", [
+    (dict(savestepinterval=10), 101),
+    (dict(savestepinterval=10, save_everystep=False, save_start=False, save_end=True), 1),
+    (dict(savestepinterval=10, save_everystep=False, save_start=True, save_end=True), 2),
+    (dict(savestepinterval=10, save_everystep=False, save_start=True, save_end=False), 1),
+    (dict(savestepinterval=10, save_everystep=True, save_start=False, save_end=False), 99),
+    (dict(savestepinterval=3, save_everystep=True, save_start=True, save_end=True), 335),
+])
+def test_saving_flags(tp, orc, flags, n_expected):
+    # test_boris.jl:274-346
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+    dt = 3.0e-11
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0], (0.0, 3.0e-8), param, tp.Boris(), dt=dt, **flags)
+    t, u = r.traj(0)
+    assert t.size == n_expected
+    if flags.get("save_start", True):
+        assert t[0] == 0.0
+    if n_expected == 1 and not flags.get("save_start", True):
+        assert t[0] == 3.0e-8
+    if n_expected == 99:
+        assert math.isclose(t[0], 10 * dt) and math.isclose(t[-1], 990 * dt)
+    if n_expected == 335:
+        assert math.isclose(t[1], 3 * dt) and math.isclose(t[-2], 999 * dt) and t[-1] == 3.0e-8
+    if n_expected == 101:
+        assert t[-1] == 3.0e-8
+
+
+def test_saving_flags_multistep_and_fields(tp, orc):
+    # test_boris.jl:348-371
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), species=tp.Electron)
+    u0 = [0.0, 0.0, 0.0, 0.0, 1.0e5, 0.0]
+    r = _solve(tp, orc, u0, (0.0, 3.0e-8), param, tp.MultistepBoris(2, 2), dt=3.0e-11, savestepinterval=10,
+               save_everystep=False, save_start=True, save_end=True)
+    t, _ = r.traj(0)
+    assert t.size == 2 and t[0] == 0.0 and t[-1] == 3.0e-8
+    r = _solve(tp, orc, u0, (0.0, 3.0e-8), param, tp.Boris(), dt=3.0e-11, savestepinterval=10, save_fields=True)
+    _, u = r.traj(0)
+    assert u.shape[1] == 12
+    assert list(u[0, 6:9]) == [0.0, 0.0, 0.0] and list(u[0, 9:12]) == [0.0, 0.0, 0.01]
+    assert list(u[-1, 6:9]) == [0.0, 0.0, 0.0] and list(u[-1, 9:12]) == [0.0, 0.0, 0.01]
+
+
+def test_solver_limits(tp, orc):
+    # test_boris.jl:509-532
+    E = tp.UniformField((0.0, 1.0e5, 0.0))
+    B = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    param = tp.prepare(E, B, species=tp.Electron)
+    u0 = [0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0]
+    with pytest.raises(ValueError):
+        _solve(tp, orc, u0, (0.0, 1.0e-9), param, tp.Boris(), dt=1.0e-11, maxiters=50)
+    with pytest.raises(ValueError):
+        _solve(tp, orc, u0, (0.0, 1.0e-9), param, tp.Boris(), dt=np.finfo(float).eps)
+    with pytest.raises(ValueError):
+        tp.MultistepBoris(1)
+    with pytest.raises(ValueError):
+        tp.MultistepBoris(3, 2)
+
+
+# ------------------------------------------------------------------ test/test_boris_kernel.jl
+def test_energy_conservation_two_periods(tp, orc):
+    # test_boris_kernel.jl:95-116
+    B0 = 1.0e-8
+    T = 2 * math.pi / (tp.qi * B0 / tp.mi)
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, B0)), species=tp.Proton)
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0], (0.0, 2 * T), param, tp.Boris(), dt=T / 100,
+               savestepinterval=10)
+    v = r.final_states()[0, 3:6]
+    assert abs(np.linalg.norm(v) - 1.0e5) <= 1.0e-3 * 1.0e5
+
+
+# ------------------------------------------------------------------ test/test_adaptive_multistep_boris.jl
+def test_adaptive_multistep_n1_matches_adaptive_boris(tp, orc):
+    # test_adaptive_multistep_boris.jl:41-48
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0e-8)))
+    u0 = [1.0, 0.0, 0.0, 0.0, 1.0, 0.0]
+    a = _solve(tp, orc, u0, (0.0, 1.0), param, tp.AdaptiveBoris(0.1))
+    b = _solve(tp, orc, u0, (0.0, 1.0), param, tp.AdaptiveMultistepBoris(2, 1, 0.1))
+    assert julia_isapprox(a.t, b.t)
+    assert julia_isapprox(a.u, b.u)
+    assert a.retcode[0] == 1 and b.retcode[0] == 1
+
+
+# ------------------------------------------------------------------ test/test_boundary.jl
+def _nan_fields():
+    def E(r, t):
+        return (math.nan,) * 3 if np.linalg.norm(r) > 1.0 else (0.0, 0.0, 0.0)
+
+    def B(r, t):
+        return (math.nan,) * 3 if np.linalg.norm(r) > 1.0 else (0.0, 0.0, 1.0)
+
+    def isoutside(u, t):
+        return bool(np.any(np.isnan(u))) or np.linalg.norm(u[:3]) > 1.0
+
+    return E, B, isoutside
+
+
+def test_boundary_nan_boris_and_adaptive(tp, orc):
+    # test_boundary.jl:10-58
+    E, B, out = _nan_fields()
+    p = (1.0, 1.0, tp.ZeroField(), tp.ZeroField(), tp.ZeroField())
+    u0 = [0.9, 0.0, 0.0, 0.0, 1.0, 0.0]
+    for alg, kw in ((tp.Boris(), dict(dt=0.2)), (tp.AdaptiveBoris(0.05), {})):
+        r = _solve(tp, orc, u0, (0.0, 1.0), p, alg, E=E, B=B, isoutside=out, **kw)
+        end = r.final_states()[0]
+        assert not np.any(np.isnan(end))
+        assert np.linalg.norm(end[:3]) <= 1.0
+        assert r.retcode[0] == 2  # Terminated
+
+
+def _gc_solve(tp, orc, y0, tspan, p, E=None, B=None, isoutside=None, **kw):
+    q, q2m, mu, Ep, Bp = p
+    prob = tp.TraceGCProblem(y0, tspan, (q, q2m, mu, tp.ZeroField(), tp.ZeroField()))
+    plan = tp.plan_gc(prob, tp.EnsembleB200(), **kw)
+    return orc.gc_run(plan.desc, E if E is not None else Ep, B if B is not None else Bp, plan.y0,
+                      isoutside=isoutside)
+
+
+def test_boundary_nan_gc(tp, orc):
+    # test_boundary.jl:60-81
+    E, B, out = _nan_fields()
+    p = (1.0, 1.0, 0.0, None, None)
+    for kw in (dict(dt=0.2, alg="rk4"), dict(dt=0.01, alg="rk45")):
+        r = _gc_solve(tp, orc, [0.9, 0.0, 0.0, 1.0], (0.0, 1.0), p, E=E, B=B, isoutside=out, **kw)
+        end = r.final_states()[0]
+        assert not np.any(np.isnan(end))
+        assert np.linalg.norm(end[:3]) <= 1.0
+        assert r.retcode[0] == 2
+
+
+def test_boundary_spatial_and_time_rejection(tp, orc):
+    # test_boundary.jl:84-128
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((1.0, 0.0, 0.0)), species=tp.Proton)
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0], (0.0, 1.0e-5), param, tp.AdaptiveBoris(0.1),
+               isoutside=lambda u, t: u[0] > 0.5)
+    t, u = r.traj(0)
+    assert u[-1, 0] <= 0.5 and t[-1] < 1.0e-5 and r.retcode[0] == 2
+    # integer tspan
+    r = _solve(tp, orc, [0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0, 10), param, tp.Boris(), dt=1.0)
+    t, _ = r.traj(0)
+    assert t[-1] == 10 and r.retcode[0] == 1
+    # GC time rejection
+    Eg, Bg = tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0))
+    y0, mu = orc.gc_prepare(Eg, Bg, np.array([0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0]), tp.qi, tp.mi)
+    p = (tp.qi, tp.qi / tp.mi, mu[0], Eg, Bg)
+    r = _gc_solve(tp, orc, y0[0], (0.0, 1.0), p, dt=1.0e-4, alg="rk4", isoutside=lambda u, t: t > 0.5)
+    t, _ = r.traj(0)
+    assert math.isclose(t[-1], 0.5, rel_tol=1e-8) and r.retcode[0] == 2
+
+
+# ------------------------------------------------------------------ test/test_gc.jl
+def _gc_dipole_problem(tp, orc):
+    # test_gc.jl:166-186: 50 MeV proton at 2.5 R_E in the Earth dipole
+    Ek = 5.0e7
+    v0 = tp.sph2cart(tp.energy2velocity(Ek, m=tp.mi, q=tp.qi), math.pi / 4, 0.0)
+    r0 = tp.sph2cart(2.5 * tp.Re, math.pi / 2, 0.0)
+    E = tp.ZeroField()
+    B = tp.DipoleField(tp.BMoment_Earth)
+    y0, mu = orc.gc_prepare(E, B, np.concatenate([r0, v0]), tp.qi, tp.mi)
+    return y0[0], (tp.qi, tp.qi / tp.mi, mu[0], E, B)
+
+
+def test_gc_rk4_dipole_counts(tp, orc):
+    y0, p = _gc_dipole_problem(tp, orc)
+    r = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk4")
+    assert r.nsaved[0] == 10001 and r.retcode[0] == 3  # MaxIters
+    r = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk4", save_everystep=False)
+    assert r.nsaved[0] == 2
+    r = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk4", isoutside=lambda u, t: t > 0.5)
+    assert r.nsaved[0] == 5001
+
+
+def test_gc_rk45_dipole_counts(tp, orc):
+    y0, p = _gc_dipole_problem(tp, orc)
+    r = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk45")
+    assert r.nsaved[0] == 61 and r.retcode[0] == 1
+    tight = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk45", abstol=1e-8, reltol=1e-8)
+    assert tight.nsaved[0] > 61
+    rk4 = _gc_solve(tp, orc, y0, (0.0, 1.0), p, dt=1.0e-4, alg="rk4")
+    assert np.linalg.norm(tight.final_states()[0] - rk4.final_states()[0]) < 10.0
+    auto = _gc_solve(tp, orc, y0, (0.0, 1.0), p, alg="rk45")
+    assert auto.nsaved[0] == 58 and auto.retcode[0] == 1
+
+
+# ------------------------------------------------------------------ test/test_utility.jl
+def test_gyro_constants(tp):
+    # test_utility.jl:28-33
+    assert math.isclose(tp.get_gyroradius(440.0e3, 5.0e-9), 918692.2725070775, rel_tol=1.5e-8)
+    assert math.isclose(tp.get_gyroperiod(5.0e-9), 13.118894973717941, rel_tol=1.5e-8)
+
+
+def _scalar_grid(tp, bc):
+    # test_utility.jl:93-110: n[i,j,k] = i + j + k (1-based) on x(4), y(6), z(8) in [-10, 10]
+    x = np.linspace(-10, 10, 4)
+    y = np.linspace(-10, 10, 6)
+    z = np.linspace(-10, 10, 8)
+    i, j, k = np.meshgrid(np.arange(1, 5), np.arange(1, 7), np.arange(1, 9), indexing="ij")
+    A = np.zeros((3, 4, 6, 8), dtype=np.float32)
+    A[0] = (i + j + k).astype(np.float32)
+    return tp.build_interpolator(A, x, y, z, 1, bc)
+
+
+def test_interpolation_kats(tp, orc):
+    f = _scalar_grid(tp, tp.FillExtrap())
+    assert math.isclose(orc.field_eval(f, [9.0, 0.0, 0.0])[0, 0], 11.85, rel_tol=1e-12)
+    assert np.all(np.isnan(orc.field_eval(f, [20.0, 0.0, 0.0])))
+    f = _scalar_grid(tp, tp.PeriodicBC("exclusive"))
+    assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 9.5, rel_tol=1e-12)
+    f = _scalar_grid(tp, tp.ClampExtrap())
+    assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 12.0, rel_tol=1e-12)
+
+
+def test_dipole_jacobian_matches_finite_differences(tp, orc):
+    B = tp.DipoleField(tp.BMoment_Earth)
+    x = np.array([2.1 * tp.Re, 0.7 * tp.Re, 0.4 * tp.Re])
+    _, J = orc.field_eval(B, x, jacobian=True)
+    h = 1.0
+    for jdx in range(3):
+        e = np.zeros(3)
+        e[jdx] = h
+        fd = (orc.field_eval(B, x + e) - orc.field_eval(B, x - e))[0] / (2 * h)
+        assert np.allclose(J[0][:, jdx], fd, rtol=1e-6, atol=1e-20)
