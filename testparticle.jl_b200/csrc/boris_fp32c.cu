@@ -201,17 +201,16 @@ __device__ __forceinline__ F3 analytic_eval32(const DevField& f, const CPos& p, 
                     f.vf[2] + f.Jf[6] * x + f.Jf[7] * y + f.Jf[8] * z + f.ratef[2] * tf};
         }
         case TP_FIELD_DIPOLE: {
+            // unit-vector form keeps float intermediates normal:
+            // B = K/r^3 (3 (mh.rh) rh - mh), K = coef |m|
             F3 d{(p.hi[0] - f.cf[0]) + p.lo[0], (p.hi[1] - f.cf[1]) + p.lo[1],
                  (p.hi[2] - f.cf[2]) + p.lo[2]};
-            F3 m{f.mf[0], f.mf[1], f.mf[2]};
-            float d2 = dot(d, d);
-            float inv = rsqrtf(d2);
-            float inv2 = 1.0f / d2;
-            float inv3 = inv * inv2;
-            float mr = dot(m, d) * inv2;  // (m.rhat)/|d|
-            float k = f.coeff * inv3;
-            return {k * (3.0f * mr * d.x - m.x), k * (3.0f * mr * d.y - m.y),
-                    k * (3.0f * mr * d.z - m.z)};
+            F3 mh{f.mhatf[0], f.mhatf[1], f.mhatf[2]};
+            float ir = __frsqrt_rn(dot(d, d));  // correctly rounded: |rh| = 1 to 1 ulp
+            F3 rh = ir * d;
+            float mr = dot(mh, rh);
+            float k = f.Kf * ir * ir * ir;
+            return {k * (3.0f * mr * rh.x - mh.x), k * (3.0f * mr * rh.y - mh.y), k * (3.0f * mr * rh.z - mh.z)};
         }
         default:
             return {0.0f, 0.0f, 0.0f};
@@ -274,63 +273,110 @@ __device__ __forceinline__ bool fields_static32(const DevFields& F) {
 }
 
 // ---------------------------------------------------------------- updates
-// Boris rotation (boris.jl:19-31) in float; h = q2m*dt/2
-__device__ __forceinline__ F3 boris_rot32(F3 v, F3 E, F3 B, float h) {
+// Velocity as a compensated float pair, v = h + l, advanced in "delta form":
+// the kernels compute the change dv = v_new - v in float (|dv| ~ the
+// rotation angle times |v|, so its rounding is ~1e-8 |v|) and add it with
+// TwoSum.  The scalar rotation coefficients -- the only quantities whose
+// float rounding would bias the gyrophase every step -- are formed in
+// float64 from the float rotation vector; 1/(1+|t|^2) and 1/A use a float
+// reciprocal refined by one float64 Newton step.
+struct CV {
+    F3 h, l;
+};
+
+__device__ __forceinline__ void cv_add(CV& v, F3 d) {
+    cadd(v.h.x, v.l.x, d.x);
+    cadd(v.h.y, v.l.y, d.y);
+    cadd(v.h.z, v.l.z, d.z);
+}
+
+__device__ __forceinline__ CV cv_from(const double* u) {
+    CV v;
+    v.h = {(float)u[0], (float)u[1], (float)u[2]};
+    v.l = {(float)(u[0] - (double)v.h.x), (float)(u[1] - (double)v.h.y), (float)(u[2] - (double)v.h.z)};
+    return v;
+}
+
+__device__ __forceinline__ double dot64(F3 a, F3 b) {
+    return fma((double)a.x, (double)b.x, fma((double)a.y, (double)b.y, (double)a.z * (double)b.z));
+}
+
+// 1/d for d >= 1 (float64): float reciprocal + one Newton step
+__device__ __forceinline__ double recip64(double d) {
+    double r = (double)__frcp_rn((float)d);
+    return fma(r, fma(-d, r, 1.0), r);
+}
+
+// Boris (boris.jl:19-31): dv = 2 h E + (v- + v- x t) x s,  h = q2m*dt/2
+__device__ __forceinline__ F3 boris_delta32(F3 v, F3 E, F3 B, double hd) {
+    float h = (float)hd;
     F3 t = h * B;
-    float tm2 = dot(t, t);
-    float sc = __fdiv_rn(2.0f, 1.0f + tm2);
-    F3 s = sc * t;
+    float sc = (float)(2.0 * recip64(1.0 + dot64(t, t)));
     F3 he = h * E;
     F3 vm = v + he;
     F3 vp = vm + cross(vm, t);
-    F3 vpl = vm + cross(vp, s);
-    return vpl + he;
+    F3 d = cross(vp, sc * t);
+    return d + (2.0f * he);
 }
 
-// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form; factor = q2m*dt/(2n)
-__device__ __forceinline__ F3 multistep_rot32(F3 v, F3 E, F3 B, float factor, int N, int n) {
-    F3 t_n = factor * B;
-    F3 e_n = factor * E;
+// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form:
+// dv = (c1 - 1) v + c2 v x t + c3 (v.t) t + c2 e + c3 e x t + c6 (e.t) t
+__device__ __forceinline__ F3 multistep_delta32(F3 v, F3 E, F3 B, double facd, int N, int n) {
+    float fac = (float)facd;
+    F3 t_n = fac * B;
+    F3 e_n = fac * E;
+    double s = dot64(t_n, t_n);
     if (N != 2) {
-        float tm2 = dot(t_n, t_n);
-        float f_N, e_corr;
+        double f_N, e_corr;
         if (N == 4) {
-            f_N = 1.0f + tm2 * (1.0f / 3.0f);
-            e_corr = -1.0f / 3.0f;
+            f_N = 1.0 + s * (1.0 / 3.0);
+            e_corr = -1.0 / 3.0;
         } else {
-            f_N = 1.0f + tm2 * (1.0f / 3.0f) + 2.0f * tm2 * tm2 * (1.0f / 15.0f);
-            e_corr = -1.0f / 3.0f - 2.0f * tm2 * (1.0f / 15.0f);
+            f_N = 1.0 + s * (1.0 / 3.0) + 2.0 * s * s * (1.0 / 15.0);
+            e_corr = -1.0 / 3.0 - 2.0 * s * (1.0 / 15.0);
         }
         float edt = dot(e_n, t_n);
-        e_n = f_N * e_n + (e_corr * edt) * t_n;
-        t_n = f_N * t_n;
+        float fN = (float)f_N;
+        e_n = fN * e_n + ((float)e_corr * edt) * t_n;
+        t_n = fN * t_n;
+        s = s * f_N * f_N;
     }
-    float s = dot(t_n, t_n);
-    float zr = 1.0f, q = 0.0f, A = 1.0f, R = 0.0f;
+    double zr = 1.0, q = 0.0, A = 1.0, R = 0.0;
     for (int k = 0; k < n; ++k) {
-        R = R + (float)(k + 1) * A + 2.0f * q * q + zr * q;
-        float nzr = zr - s * q;
+        R = R + (double)(k + 1) * A + 2.0 * q * q + zr * q;
+        double nzr = zr - s * q;
         q = zr + q;
         zr = nzr;
-        A = A * (1.0f + s);
+        A = A * (1.0 + s);
     }
-    float invA = __fdiv_rn(1.0f, A);
-    float c1 = (zr * zr - s * q * q) * invA;
-    float c2 = 2.0f * zr * q * invA;
-    float c3 = 2.0f * q * q * invA;
-    float c6 = 2.0f * R * invA;
+    double invA = recip64(A);
+    float c1m1 = (float)((zr * zr - s * q * q - A) * invA);
+    float c2 = (float)(2.0 * zr * q * invA);
+    float c3 = (float)(2.0 * q * q * invA);
+    float c6 = (float)(2.0 * R * invA);
     float vdt = dot(v, t_n), edt = dot(e_n, t_n);
     F3 vxt = cross(v, t_n), ext = cross(e_n, t_n);
-    return c1 * v + c2 * vxt + (c3 * vdt) * t_n + c2 * e_n + c3 * ext + (c6 * edt) * t_n;
+    return c1m1 * v + c2 * vxt + (c3 * vdt) * t_n + c2 * e_n + c3 * ext + (c6 * edt) * t_n;
 }
 
+// v advanced by one velocity update of length dt with fields (E, B)
 template <bool MULTI>
-__device__ __forceinline__ F3 vel32(F3 v, F3 E, F3 B, const BorisArgs& a, double dt) {
-    if (MULTI) return multistep_rot32(v, E, B, (float)(a.q2m * dt / (double)(2 * a.nsub)), a.order, a.nsub);
-    return boris_rot32(v, E, B, (float)(a.q2m * 0.5 * dt));
+__device__ __forceinline__ CV vel32(CV v, F3 E, F3 B, const BorisArgs& a, double dt) {
+    F3 d = MULTI ? multistep_delta32(v.h, E, B, a.q2m * dt / (double)(2 * a.nsub), a.order, a.nsub)
+                 : boris_delta32(v.h, E, B, a.q2m * 0.5 * dt);
+    cv_add(v, d);
+    return v;
 }
 
-__device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, F3 v, double t) {
+// position push x += v dt with dt = dth + dtl (float pair)
+__device__ __forceinline__ void cpos_push_cv(const BorisArgs& a, CPos& p, const CV& v, float dth, float dtl) {
+    F3 d{fmaf(v.h.x, dth, fmaf(v.h.x, dtl, v.l.x * dth)), fmaf(v.h.y, dth, fmaf(v.h.y, dtl, v.l.y * dth)),
+         fmaf(v.h.z, dth, fmaf(v.h.z, dtl, v.l.z * dth))};
+    cpos_push(a, p, d, 1.0f);
+}
+
+__device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, const CV& vc, double t) {
+    const F3 v = vc.h;
     const DevTerm& T = a.term;
     int f = T.flags;
     if (f & TP_TERM_NAN)
@@ -359,7 +405,7 @@ struct Saver32 {
     const BorisArgs& a;
     int W;
     __device__ Saver32(const BorisArgs& a_) : a(a_), W(a_.save_fields ? 12 : 6) {}
-    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, F3 v, double t) const {
+    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, const CV& v, double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
             return;
@@ -370,9 +416,9 @@ struct Saver32 {
         u[0 * n] = cpos_value(a, p, 0);
         u[1 * n] = cpos_value(a, p, 1);
         u[2 * n] = cpos_value(a, p, 2);
-        u[3 * n] = (double)v.x;
-        u[4 * n] = (double)v.y;
-        u[5 * n] = (double)v.z;
+        u[3 * n] = (double)v.h.x + (double)v.l.x;
+        u[4 * n] = (double)v.h.y + (double)v.l.y;
+        u[5 * n] = (double)v.h.z + (double)v.l.z;
         if (W == 12) {
             F3 E, B;
             eval_EB32t<FK>(a.f, p, t, E, B);
@@ -408,9 +454,9 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
 
     int64_t i = -1;
     CPos p;
-    F3 v{0, 0, 0}, v_prev{0, 0, 0};
+    CV v{}, v_prev{};
     double dt = 0, t = 0, t1 = 0, t_last = 0;
-    float dtf = 0;
+    float dth = 0, dtl = 0;
     int64_t it = 0, nt = 0, nout = 0, iout = 0, csave = 0;
     bool terminated = false;
 
@@ -430,11 +476,12 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
                 i = -1;
                 continue;
             }
-            dtf = (float)dt;
+            dth = (float)dt;
+            dtl = (float)(dt - (double)dth);
             nout = calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
             const double* u0 = a.u0 + 6 * i;
             cpos_init(a, p, u0);
-            v = {(float)u0[3], (float)u0[4], (float)u0[5]};
+            v = cv_from(u0 + 3);
             iout = 0;
             if (a.save_start) {
                 a.t_out[i] = a.t0;  // save_start writes u0 exactly (slot 0)
@@ -471,7 +518,7 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
             eval_EB32t<FK>(a.f, p, t, E, B);
             v = vel32<MULTI>(v, E, B, a, dt);
             CPos pn = p;
-            cpos_push(a, pn, v, dtf);
+            cpos_push_cv(a, pn, v, dth, dtl);
             if (a.term.flags && outside32(a, pn, v, t + 0.5 * dt)) {
                 terminated = true;
                 done = true;
@@ -481,7 +528,7 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
                     if (iout <= nout) {
                         double t_cur = t - 0.5 * dt;
                         if (!stat) eval_EB32t<FK>(a.f, p, t_cur, E, B);
-                        F3 vs = vel32<MULTI>(v_prev, E, B, a, 0.5 * dt);
+                        CV vs = vel32<MULTI>(v_prev, E, B, a, 0.5 * dt);
                         S.save(i, iout - 1, p, vs, t_cur);
                         t_last = t_cur;
                     }
@@ -508,7 +555,7 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
                     double dt_final = t_final - fma((double)final_step - 0.5, dt, a.t0);
                     F3 E, B;
                     eval_EB32t<FK>(a.f, p, t_final, E, B);
-                    F3 vf = vel32<MULTI>(v, E, B, a, dt_final);
+                    CV vf = vel32<MULTI>(v, E, B, a, dt_final);
                     S.save(i, iout, p, vf, t_final);
                     iout += 1;
                 }
@@ -532,7 +579,8 @@ __global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
 
     int64_t i = -1;
     CPos p;
-    F3 v{0, 0, 0}, E{0, 0, 0}, B{0, 0, 0};
+    CV v{};
+    F3 E{0, 0, 0}, B{0, 0, 0};
     double t = 0, t1 = 0, dt = 0, C = 0, ttotal = 0, t_last = 0;
     int64_t it = 0, iout = 0, steps = 0;
     bool ssf = false;
@@ -548,7 +596,7 @@ __global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
             C = (twopi * a.safety * sgn) / fabs(a.q2m);
             const double* u0 = a.u0 + 6 * i;
             cpos_init(a, p, u0);
-            v = {(float)u0[3], (float)u0[4], (float)u0[5]};
+            v = cv_from(u0 + 3);
             t = a.t0;
             ttotal = dtt;
             iout = 0;
@@ -590,16 +638,17 @@ __global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
                 dt = dt_step;
             }
             if (a.save_everystep && (it - 1) > 0 && (it - 1) % a.ssi == 0) {
-                F3 vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                CV vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
                 S.save(i, iout, p, vs, t);
                 t_last = t;
                 iout += 1;
             }
             F3 Em = E, Bm = B;
             if (!stat) eval_EB32t<FK>(a.f, p, t + 0.5 * dt, Em, Bm);
-            F3 v_new = vel32<MULTI>(v, Em, Bm, a, dt);
+            CV v_new = vel32<MULTI>(v, Em, Bm, a, dt);
             CPos pn = p;
-            cpos_push(a, pn, v_new, (float)dt);
+            float dh = (float)dt;
+            cpos_push_cv(a, pn, v_new, dh, (float)(dt - (double)dh));
             double t_next = t + dt;
             if (a.term.flags && outside32(a, pn, v_new, t_next)) {
                 ssf = true;
@@ -627,7 +676,7 @@ __global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
         if (done) {
             if (ssf && (iout == 0 || t_last != t)) {
                 if (!stat) eval_EB32t<FK>(a.f, p, t, E, B);
-                F3 vf = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                CV vf = vel32<MULTI>(v, E, B, a, 0.5 * dt);
                 S.save(i, iout, p, vf, t);
                 iout += 1;
             }

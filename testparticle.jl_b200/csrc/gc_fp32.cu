@@ -30,13 +30,12 @@ __device__ __forceinline__ V3f field32(const DevField& f, V3f r, float t) {
                     f.vf[2] + f.Jf[6] * r.x + f.Jf[7] * r.y + f.Jf[8] * r.z + f.ratef[2] * t};
         case TP_FIELD_DIPOLE: {
             V3f d{r.x - f.cf[0], r.y - f.cf[1], r.z - f.cf[2]};
-            V3f m{f.mf[0], f.mf[1], f.mf[2]};
-            float d2 = dotf(d, d);
-            float inv2 = 1.0f / d2;
-            float inv3 = rsqrtf(d2) * inv2;
-            float md = dotf(m, d) * inv2;
-            float k = f.coeff * inv3;
-            return {k * (3.0f * md * d.x - m.x), k * (3.0f * md * d.y - m.y), k * (3.0f * md * d.z - m.z)};
+            V3f mh{f.mhatf[0], f.mhatf[1], f.mhatf[2]};
+            float ir = rsqrtf(dotf(d, d));
+            V3f rh = ir * d;
+            float mr = dotf(mh, rh);
+            float k3 = f.Kf * ir * ir * ir;  // coef |m| / r^3
+            return {k3 * (3.0f * mr * rh.x - mh.x), k3 * (3.0f * mr * rh.y - mh.y), k3 * (3.0f * mr * rh.z - mh.z)};
         }
         default:
             return {0.0f, 0.0f, 0.0f};
@@ -52,23 +51,20 @@ __device__ __forceinline__ void field_jac32(const DevField& f, V3f r, float t, V
         return;
     }
     if (f.kind == TP_FIELD_DIPOLE) {
+        // unit-vector form: B = K/r^3 (3 (mh.rh) rh - mh),
+        // dB_i/dx_j = K/r^4 (3 (mh_j rh_i + (mh.rh) delta_ij + mh_i rh_j) - 15 (mh.rh) rh_i rh_j)
         V3f d{r.x - f.cf[0], r.y - f.cf[1], r.z - f.cf[2]};
-        float mv[3] = {f.mf[0], f.mf[1], f.mf[2]};
-        float d2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        float inv2 = 1.0f / d2;
-        float inv3 = rsqrtf(d2) * inv2;
-        float inv5 = inv3 * inv2;
-        float md = mv[0] * d.x + mv[1] * d.y + mv[2] * d.z;
-        float dv[3] = {d.x, d.y, d.z};
-        float k3 = f.coeff * inv3, k5 = 3.0f * f.coeff * inv5;
-        float bv[3];
-        for (int i = 0; i < 3; ++i) bv[i] = k5 * md * dv[i] - k3 * mv[i];
-        B = {bv[0], bv[1], bv[2]};
-        float k7 = 5.0f * md * inv2;
+        float ir = rsqrtf(dotf(d, d));
+        float rh[3] = {ir * d.x, ir * d.y, ir * d.z};
+        float mh[3] = {f.mhatf[0], f.mhatf[1], f.mhatf[2]};
+        float mr = mh[0] * rh[0] + mh[1] * rh[1] + mh[2] * rh[2];
+        float k3 = f.Kf * ir * ir * ir;
+        float k4 = k3 * ir;
+        B = {k3 * (3.0f * mr * rh[0] - mh[0]), k3 * (3.0f * mr * rh[1] - mh[1]), k3 * (3.0f * mr * rh[2] - mh[2])};
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) {
-                float dij = (i == j) ? md : 0.0f;
-                J[3 * i + j] = k5 * (mv[j] * dv[i] + dij + mv[i] * dv[j] - k7 * dv[i] * dv[j]);
+                float dij = (i == j) ? mr : 0.0f;
+                J[3 * i + j] = k4 * (3.0f * (mh[j] * rh[i] + dij + mh[i] * rh[j]) - 15.0f * mr * rh[i] * rh[j]);
             }
         return;
     }

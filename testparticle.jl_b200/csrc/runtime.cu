@@ -139,6 +139,9 @@ void fill_float_copies(DevField& d) {
     }
     for (int k = 0; k < 9; ++k) d.Jf[k] = (float)d.J[k];
     d.coeff = (float)d.coef;
+    double mm = std::sqrt(d.m[0] * d.m[0] + d.m[1] * d.m[1] + d.m[2] * d.m[2]);
+    for (int a = 0; a < 3; ++a) d.mhatf[a] = mm > 0 ? (float)(d.m[a] / mm) : 0.0f;
+    d.Kf = (float)(d.coef * mm);
 }
 
 bool same_geometry(const tp_field* a, const tp_field* b) {

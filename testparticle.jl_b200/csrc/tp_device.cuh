@@ -45,6 +45,8 @@ struct DevField {
     float mf[3];
     float cf[3];
     float coeff;
+    float mhatf[3];   // dipole: unit moment and K = coef * |m| (keeps float
+    float Kf;         //   intermediates normal: coef / r^5 alone underflows)
     const void* tab;  // per-node table: float4 / double4 per node (x,y,z,0)
     const float4* tab32;  // float table for the FP32C kernels (same as tab for float data)
 };
