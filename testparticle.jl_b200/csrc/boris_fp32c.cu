@@ -100,41 +100,64 @@ struct AxF {
 };
 
 // cell index and fraction from the compensated coordinate
+// The cell index comes from rounding u = d/dx to the nearest integer with
+// the float "magic number" 1.5*2^23 (two float adds and an integer subtract
+// on the FP32/ALU pipes instead of floor + float-to-int conversions on the
+// XU pipe); the fraction is then corrected into [0, 1).  Valid for |u| <
+// 2^22, i.e. positions kept within the periodic box or a grid of < 4M cells;
+// larger |u| takes the floorf path.
 __device__ __forceinline__ bool axis32(const DevField& g, int a, float hi, float lo, AxF& o) {
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23
     float d = hi - g.x0f[a];
-    float fl = floorf(d * g.idxf[a]);
+    float u = d * g.idxf[a];
+    float fl;
+    int i;
+    if (fabsf(u) < 4194304.0f) {
+        float tr = u + kMagic;
+        i = __float_as_int(tr) - __float_as_int(kMagic);
+        fl = tr - kMagic;
+    } else {
+        fl = floorf(u);
+        i = (int)fl;
+    }
     float rem = fmaf(-fl, g.dxf[a], d) + lo;
     float f = rem * g.idxf[a];
     if (f < 0.0f) {
         fl -= 1.0f;
+        i -= 1;
         f += 1.0f;
     } else if (f >= 1.0f) {
         fl += 1.0f;
+        i += 1;
         f -= 1.0f;
     }
     int na = g.n[a];
     if (g.bc == TP_BC_PERIODIC) {
-        int i = (int)fl % na;
+        if (i >= na) i -= na;
         if (i < 0) i += na;
+        if (i < 0 || i >= na) {  // far outside the box (positions not wrapped)
+            i %= na;
+            if (i < 0) i += na;
+        }
         o.i0 = i;
         o.i1 = (i + 1 == na) ? 0 : i + 1;
         o.f = f;
         return true;
     }
-    float u = fl + f;
+    float uc = fl + f;
     float umax = (float)(na - 1);
     if (g.bc == TP_BC_CLAMP) {
-        if (u < 0.0f) {
+        if (uc < 0.0f) {
             fl = 0.0f;
             f = 0.0f;
-        } else if (u > umax) {
+        } else if (uc > umax) {
             fl = umax;
             f = 0.0f;
         }
-    } else if (!(u >= 0.0f && u <= umax)) {
+    } else if (!(uc >= 0.0f && uc <= umax)) {
         return false;
     }
-    int i = (int)fl;
+    i = (int)fl;
     if (i > na - 2) {
         f += (float)(i - (na - 2));
         i = na - 2;
@@ -160,6 +183,14 @@ __device__ __forceinline__ bool axes32(const DevField& g, const CPos& p, AxF& ax
 }
 
 __device__ __forceinline__ F3 xyz(float4 q) { return {q.x, q.y, q.z}; }
+
+// One 32-byte, 32-byte-aligned node record of the interleaved E/B table in a
+// single 256-bit read-only load (sm_100 ld.global.nc.v8).
+__device__ __forceinline__ void ldg_node8(const float4* p, float4& e, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
 
 __device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, F3 v101, F3 v011,
                                    F3 v111, const AxF& ax, const AxF& ay, const AxF& az) {
@@ -233,15 +264,18 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
         int n010 = 2 * (ax.i0 + j1 + k0), n110 = 2 * (ax.i1 + j1 + k0);
         int n001 = 2 * (ax.i0 + j0 + k1), n101 = 2 * (ax.i1 + j0 + k1);
         int n011 = 2 * (ax.i0 + j1 + k1), n111 = 2 * (ax.i1 + j1 + k1);
-        // all 16 loads issued before any use: 8 aligned 32-byte sectors
-        float4 e000 = __ldg(T + n000), b000 = __ldg(T + n000 + 1);
-        float4 e100 = __ldg(T + n100), b100 = __ldg(T + n100 + 1);
-        float4 e010 = __ldg(T + n010), b010 = __ldg(T + n010 + 1);
-        float4 e110 = __ldg(T + n110), b110 = __ldg(T + n110 + 1);
-        float4 e001 = __ldg(T + n001), b001 = __ldg(T + n001 + 1);
-        float4 e101 = __ldg(T + n101), b101 = __ldg(T + n101 + 1);
-        float4 e011 = __ldg(T + n011), b011 = __ldg(T + n011 + 1);
-        float4 e111 = __ldg(T + n111), b111 = __ldg(T + n111 + 1);
+        // 8 corners, each one aligned 32-byte sector (E xyz0, B xyz0) read by
+        // one 256-bit load; all issued before any use
+        float4 e000, b000, e100, b100, e010, b010, e110, b110;
+        float4 e001, b001, e101, b101, e011, b011, e111, b111;
+        ldg_node8(T + n000, e000, b000);
+        ldg_node8(T + n100, e100, b100);
+        ldg_node8(T + n010, e010, b010);
+        ldg_node8(T + n110, e110, b110);
+        ldg_node8(T + n001, e001, b001);
+        ldg_node8(T + n101, e101, b101);
+        ldg_node8(T + n011, e011, b011);
+        ldg_node8(T + n111, e111, b111);
         E = tri3(xyz(e000), xyz(e100), xyz(e010), xyz(e110), xyz(e001), xyz(e101), xyz(e011),
                  xyz(e111), ax, ay, az);
         B = tri3(xyz(b000), xyz(b100), xyz(b010), xyz(b110), xyz(b001), xyz(b101), xyz(b011),
@@ -297,21 +331,11 @@ __device__ __forceinline__ CV cv_from(const double* u) {
     return v;
 }
 
-__device__ __forceinline__ double dot64(F3 a, F3 b) {
-    return fma((double)a.x, (double)b.x, fma((double)a.y, (double)b.y, (double)a.z * (double)b.z));
-}
-
-// 1/d for d >= 1 (float64): float reciprocal + one Newton step
-__device__ __forceinline__ double recip64(double d) {
-    double r = (double)__frcp_rn((float)d);
-    return fma(r, fma(-d, r, 1.0), r);
-}
-
-// Boris (boris.jl:19-31): dv = 2 h E + (v- + v- x t) x s,  h = q2m*dt/2
-__device__ __forceinline__ F3 boris_delta32(F3 v, F3 E, F3 B, double hd) {
-    float h = (float)hd;
+// Boris (boris.jl:19-31): dv = 2 h E + (v- + v- x t) x s,  h = q2m*dt/2,
+// s = 2 t / (1 + |t|^2) with a correctly rounded reciprocal
+__device__ __forceinline__ F3 boris_delta32(F3 v, F3 E, F3 B, float h) {
     F3 t = h * B;
-    float sc = (float)(2.0 * recip64(1.0 + dot64(t, t)));
+    float sc = 2.0f * __frcp_rn(1.0f + dot(t, t));
     F3 he = h * E;
     F3 vm = v + he;
     F3 vp = vm + cross(vm, t);
@@ -319,53 +343,65 @@ __device__ __forceinline__ F3 boris_delta32(F3 v, F3 E, F3 B, double hd) {
     return d + (2.0f * he);
 }
 
-// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form:
-// dv = (c1 - 1) v + c2 v x t + c3 (v.t) t + c2 e + c3 e x t + c6 (e.t) t
-__device__ __forceinline__ F3 multistep_delta32(F3 v, F3 E, F3 B, double facd, int N, int n) {
-    float fac = (float)facd;
+// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form,
+// fac = q2m*dt/(2n):
+//   dv = (c1 - 1) v + c2 v x t + c3 (v.t) t + c2 e + c3 e x t + c6 (e.t) t
+// with c1 - 1 = -2 s q^2 / A = -s c3 (because zr^2 + s q^2 = |1 + i tau|^(2n) = A),
+// so no coefficient is formed by cancellation.
+__device__ __forceinline__ F3 multistep_delta32(F3 v, F3 E, F3 B, float fac, int N, int n) {
     F3 t_n = fac * B;
     F3 e_n = fac * E;
-    double s = dot64(t_n, t_n);
+    float s = dot(t_n, t_n);
     if (N != 2) {
-        double f_N, e_corr;
+        float f_N, e_corr;
         if (N == 4) {
-            f_N = 1.0 + s * (1.0 / 3.0);
-            e_corr = -1.0 / 3.0;
+            f_N = 1.0f + s * (1.0f / 3.0f);
+            e_corr = -1.0f / 3.0f;
         } else {
-            f_N = 1.0 + s * (1.0 / 3.0) + 2.0 * s * s * (1.0 / 15.0);
-            e_corr = -1.0 / 3.0 - 2.0 * s * (1.0 / 15.0);
+            f_N = 1.0f + s * (1.0f / 3.0f) + 2.0f * s * s * (1.0f / 15.0f);
+            e_corr = -1.0f / 3.0f - 2.0f * s * (1.0f / 15.0f);
         }
         float edt = dot(e_n, t_n);
-        float fN = (float)f_N;
-        e_n = fN * e_n + ((float)e_corr * edt) * t_n;
-        t_n = fN * t_n;
-        s = s * f_N * f_N;
+        e_n = f_N * e_n + (e_corr * edt) * t_n;
+        t_n = f_N * t_n;
+        s = dot(t_n, t_n);
     }
-    double zr = 1.0, q = 0.0, A = 1.0, R = 0.0;
+    float zr = 1.0f, q = 0.0f, A = 1.0f, R = 0.0f;
     for (int k = 0; k < n; ++k) {
-        R = R + (double)(k + 1) * A + 2.0 * q * q + zr * q;
-        double nzr = zr - s * q;
+        R = R + (float)(k + 1) * A + 2.0f * q * q + zr * q;
+        float nzr = zr - s * q;
         q = zr + q;
         zr = nzr;
-        A = A * (1.0 + s);
+        A = A * (1.0f + s);
     }
-    double invA = recip64(A);
-    float c1m1 = (float)((zr * zr - s * q * q - A) * invA);
-    float c2 = (float)(2.0 * zr * q * invA);
-    float c3 = (float)(2.0 * q * q * invA);
-    float c6 = (float)(2.0 * R * invA);
+    float invA = __frcp_rn(A);
+    float c2 = 2.0f * zr * q * invA;
+    float c3 = 2.0f * q * q * invA;
+    float c6 = 2.0f * R * invA;
+    float c1m1 = -s * c3;
     float vdt = dot(v, t_n), edt = dot(e_n, t_n);
     F3 vxt = cross(v, t_n), ext = cross(e_n, t_n);
     return c1m1 * v + c2 * vxt + (c3 * vdt) * t_n + c2 * e_n + c3 * ext + (c6 * edt) * t_n;
 }
 
-// v advanced by one velocity update of length dt with fields (E, B)
+// the float factor of a velocity update of length dt: q2m*dt/2 (Boris) or
+// q2m*dt/(2n) (Multistep), rounded once from float64
 template <bool MULTI>
-__device__ __forceinline__ CV vel32(CV v, F3 E, F3 B, const BorisArgs& a, double dt) {
-    F3 d = MULTI ? multistep_delta32(v.h, E, B, a.q2m * dt / (double)(2 * a.nsub), a.order, a.nsub)
-                 : boris_delta32(v.h, E, B, a.q2m * 0.5 * dt);
+__device__ __forceinline__ float vfac(const BorisArgs& a, double dt) {
+    return MULTI ? (float)(a.q2m * dt / (double)(2 * a.nsub)) : (float)(a.q2m * 0.5 * dt);
+}
+
+// v advanced by one velocity update with factor h (see vfac) and fields (E, B)
+template <bool MULTI>
+__device__ __forceinline__ CV vel32h(CV v, F3 E, F3 B, const BorisArgs& a, float h) {
+    F3 d = MULTI ? multistep_delta32(v.h, E, B, h, a.order, a.nsub) : boris_delta32(v.h, E, B, h);
     cv_add(v, d);
     return v;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ CV vel32(CV v, F3 E, F3 B, const BorisArgs& a, double dt) {
+    return vel32h<MULTI>(v, E, B, a, vfac<MULTI>(a, dt));
 }
 
 // position push x += v dt with dt = dth + dtl (float pair)
@@ -446,7 +482,7 @@ __device__ __forceinline__ int64_t next_particle32(const BorisArgs& a, int64_t& 
 
 // ---------------------------------------------------------------- fixed step
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
     const Saver32<FK> S(a);
     const bool stat = fields_static32(a.f);
     const uint64_t t_start = globaltimer_ns();
@@ -454,11 +490,11 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
 
     int64_t i = -1;
     CPos p;
-    CV v{}, v_prev{};
+    CV v{};
     double dt = 0, t = 0, t1 = 0, t_last = 0;
-    float dth = 0, dtl = 0;
-    int64_t it = 0, nt = 0, nout = 0, iout = 0, csave = 0;
-    bool terminated = false;
+    float dth = 0, dtl = 0, hstep = 0;
+    int64_t it = 0, nt = 0;
+    int32_t nout = 0, iout = 0, csave = 0;
 
     for (;;) {
         if (i < 0) {
@@ -478,7 +514,8 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
             }
             dth = (float)dt;
             dtl = (float)(dt - (double)dth);
-            nout = calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
+            hstep = vfac<MULTI>(a, dt);
+            nout = (int32_t)calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
             const double* u0 = a.u0 + 6 * i;
             cpos_init(a, p, u0);
             v = cv_from(u0 + 3);
@@ -507,20 +544,20 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
             it = 1;
             t = a.t0 - 0.5 * dt;
             csave = 0;
-            terminated = false;
         }
 
         bool done = it > nt;
         if (!done) {
-            v_prev = v;
+            // v is v_{it-1/2} until the step is accepted: the save of r_{it-1}
+            // and the termination rollback (the reference returns v_prev,
+            // boris.jl:460) both use it, so no copy of it is kept
             t += dt;
             F3 E, B;
             eval_EB32t<FK>(a.f, p, t, E, B);
-            v = vel32<MULTI>(v, E, B, a, dt);
+            CV vn = vel32h<MULTI>(v, E, B, a, hstep);
             CPos pn = p;
-            cpos_push_cv(a, pn, v, dth, dtl);
-            if (a.term.flags && outside32(a, pn, v, t + 0.5 * dt)) {
-                terminated = true;
+            cpos_push_cv(a, pn, vn, dth, dtl);
+            if (a.term.flags && outside32(a, pn, vn, t + 0.5 * dt)) {
                 done = true;
             } else {
                 if (a.save_everystep && it > 1 && csave == 0) {
@@ -528,12 +565,13 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
                     if (iout <= nout) {
                         double t_cur = t - 0.5 * dt;
                         if (!stat) eval_EB32t<FK>(a.f, p, t_cur, E, B);
-                        CV vs = vel32<MULTI>(v_prev, E, B, a, 0.5 * dt);
+                        CV vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
                         S.save(i, iout - 1, p, vs, t_cur);
                         t_last = t_cur;
                     }
                 }
                 p = pn;
+                v = vn;
                 it += 1;
                 csave += 1;
                 if (csave == a.ssi) csave = 0;
@@ -545,7 +583,6 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
             }
         }
         if (done) {
-            if (terminated) v = v_prev;
             int64_t final_step = it - 1;
             bool save_final = a.save_end ||
                               (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
@@ -570,7 +607,7 @@ __global__ void __launch_bounds__(256) k_fixed32c(BorisArgs a) {
 
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(256) k_adaptive32c(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
     const Saver32<FK> S(a);
     const bool stat = fields_static32(a.f);
     const uint64_t t_start = globaltimer_ns();

@@ -72,7 +72,7 @@ __device__ __forceinline__ int64_t next_particle(const BorisArgs& a, int64_t& fi
 
 // ---------------------------------------------------------------- fixed step
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
     const Saver64<FK> S(a);
     const bool stat = fields_static(a.f);
     const uint64_t t_start = globaltimer_ns();
@@ -80,10 +80,10 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
 
     // per-particle state
     int64_t i = -1;
-    D3 r{0, 0, 0}, v{0, 0, 0}, v_prev{0, 0, 0};
+    D3 r{0, 0, 0}, v{0, 0, 0};
     double dt = 0, t = 0, t1 = 0, t_last = 0;
-    int64_t it = 0, nt = 0, nout = 0, iout = 0, csave = 0;
-    bool terminated = false;
+    int64_t it = 0, nt = 0;
+    int32_t nout = 0, iout = 0, csave = 0;
 
     for (;;) {
         if (i < 0) {
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
                 i = -1;
                 continue;
             }
-            nout = calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
+            nout = (int32_t)calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
             const double* u0 = a.u0 + 6 * i;
             r = {u0[0], u0[1], u0[2]};
             v = {u0[3], u0[4], u0[5]};
@@ -126,21 +126,20 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
             it = 1;
             t = a.t0 - 0.5 * dt;
             csave = 0;  // (it - 1) % ssi
-            terminated = false;
         }
 
         bool done = it > nt;
         if (!done) {
-            // ---- one step of _boris_loop! (boris.jl:452-476)
-            v_prev = v;
+            // ---- one step of _boris_loop! (boris.jl:452-476); v stays the
+            // pre-step velocity (the reference's v_prev) until the step is
+            // accepted, which serves both the save and the termination rollback
             t += dt;
             D3 E, B;
             eval_EB64t<FK>(a.f, r, t, E, B);
-            v = vel_update64<MULTI>(v, E, B, a.q2m, dt, a.order, a.nsub);
-            D3 r_next = r + v * dt;
+            D3 vn = vel_update64<MULTI>(v, E, B, a.q2m, dt, a.order, a.nsub);
+            D3 r_next = r + vn * dt;
             double t_next = t + 0.5 * dt;
-            if (a.term.flags && outside64(a.term, r_next, v, t_next)) {
-                terminated = true;
+            if (a.term.flags && outside64(a.term, r_next, vn, t_next)) {
                 done = true;
             } else {
                 if (a.save_everystep && it > 1 && csave == 0) {
@@ -148,12 +147,13 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
                     if (iout <= nout) {
                         double t_cur = t - 0.5 * dt;
                         if (!stat) eval_EB64t<FK>(a.f, r, t_cur, E, B);
-                        D3 v_save = vel_update64<MULTI>(v_prev, E, B, a.q2m, 0.5 * dt, a.order, a.nsub);
+                        D3 v_save = vel_update64<MULTI>(v, E, B, a.q2m, 0.5 * dt, a.order, a.nsub);
                         S.save(i, iout - 1, r, v_save, t_cur);
                         t_last = t_cur;
                     }
                 }
                 r = r_next;
+                v = vn;
                 it += 1;
                 csave += 1;
                 if (csave == a.ssi) csave = 0;
@@ -166,7 +166,6 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
         }
         if (done) {
             // ---- final save and retcode (boris.jl:522-551)
-            if (terminated) v = v_prev;
             int64_t final_step = it - 1;
             bool save_final = a.save_end ||
                               (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
@@ -191,7 +190,7 @@ __global__ void __launch_bounds__(256) k_fixed64(BorisArgs a) {
 
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(256) k_adaptive64(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive64(BorisArgs a) {
     const Saver64<FK> S(a);
     const bool stat = fields_static(a.f);
     const uint64_t t_start = globaltimer_ns();

@@ -176,21 +176,62 @@ __device__ __forceinline__ void eval_EB64(const DevFields& F, D3 r, double t, D3
     B = field_eval64(F.B, r, t);
 }
 
+// One 32-byte node record (E xyz0, B xyz0) of the float interleaved table in
+// a single 256-bit read-only load (sm_100 ld.global.nc.v8).
+__device__ __forceinline__ void ldg_node8_64(const float4* p, float4& e, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
+// E and B from the float interleaved table, interpolated in float64 in the
+// order of tri64 (the values are exact float -> double conversions)
+__device__ __forceinline__ void eb_eval64_f32(const DevFields& F, D3 r, D3& E, D3& B) {
+    Ax ax, ay, az;
+    if (!grid_axes64(F.B, r, ax, ay, az)) {
+        E = nan3();
+        B = E;
+        return;
+    }
+    const float4* T = F.eb32;
+    const int64_t nx = F.B.n[0], nxy = (int64_t)F.B.n[0] * F.B.n[1];
+    int64_t j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+    float4 e000, b000, e100, b100, e010, b010, e110, b110;
+    float4 e001, b001, e101, b101, e011, b011, e111, b111;
+    ldg_node8_64(T + 2 * (ax.i0 + j0 + k0), e000, b000);
+    ldg_node8_64(T + 2 * (ax.i1 + j0 + k0), e100, b100);
+    ldg_node8_64(T + 2 * (ax.i0 + j1 + k0), e010, b010);
+    ldg_node8_64(T + 2 * (ax.i1 + j1 + k0), e110, b110);
+    ldg_node8_64(T + 2 * (ax.i0 + j0 + k1), e001, b001);
+    ldg_node8_64(T + 2 * (ax.i1 + j0 + k1), e101, b101);
+    ldg_node8_64(T + 2 * (ax.i0 + j1 + k1), e011, b011);
+    ldg_node8_64(T + 2 * (ax.i1 + j1 + k1), e111, b111);
+#define TPB_TRI64F(dst, q, c)                                                                  \
+    {                                                                                          \
+        double c00 = lerp64((double)(q##000).c, (double)(q##100).c, ax.f);                         \
+        double c10 = lerp64((double)(q##010).c, (double)(q##110).c, ax.f);                         \
+        double c01 = lerp64((double)(q##001).c, (double)(q##101).c, ax.f);                         \
+        double c11 = lerp64((double)(q##011).c, (double)(q##111).c, ax.f);                         \
+        double c0 = lerp64(c00, c10, ay.f);                                                    \
+        double c1 = lerp64(c01, c11, ay.f);                                                    \
+        dst.c = lerp64(c0, c1, az.f);                                                          \
+    }
+    TPB_TRI64F(E, e, x)
+    TPB_TRI64F(E, e, y)
+    TPB_TRI64F(E, e, z)
+    TPB_TRI64F(B, b, x)
+    TPB_TRI64F(B, b, y)
+    TPB_TRI64F(B, b, z)
+#undef TPB_TRI64F
+}
+
 template <int FK>
 __device__ __forceinline__ void eval_EB64t(const DevFields& F, D3 r, double t, D3& E, D3& B) {
     if (FK == FK_ANALYTIC) {
         E = analytic_eval64(F.E, r, t);
         B = analytic_eval64(F.B, r, t);
     } else if (FK == FK_EBGRID) {
-        Ax ax, ay, az;
-        if (!grid_axes64(F.B, r, ax, ay, az)) {
-            E = nan3();
-            B = E;
-            return;
-        }
-        bool f64 = F.eb_f64 != 0;
-        E = tri64(F.B, F.eb, f64, 2, 0, ax, ay, az);
-        B = tri64(F.B, F.eb, f64, 2, 1, ax, ay, az);
+        eb_eval64_f32(F, r, E, B);
     } else {
         E = field_eval64(F.E, r, t);
         B = field_eval64(F.B, r, t);

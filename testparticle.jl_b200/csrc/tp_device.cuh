@@ -75,7 +75,7 @@ struct DevTerm {
 enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2 };
 
 __host__ __device__ __forceinline__ int field_config_of(const DevFields& f) {
-    if (f.eb) return FK_EBGRID;
+    if (f.eb && !f.eb_f64) return FK_EBGRID;  // float interleaved table
     if (f.E.kind != TP_FIELD_GRID && f.B.kind != TP_FIELD_GRID) return FK_ANALYTIC;
     return FK_GENERIC;
 }
@@ -136,3 +136,9 @@ __device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, b
 }
 
 }  // namespace tpb
+
+// Largest block a push kernel is compiled for, per field configuration: it
+// caps the register allocation at 65536 / TPB_MAXT(FK) per thread.  The
+// interleaved-grid kernels are gather-latency bound, so they take 384 (<= 170
+// registers: three 128-thread blocks per SM); the others 256.
+#define TPB_MAXT(FK) ((FK) == FK_EBGRID ? 384 : 256)

@@ -1,0 +1,319 @@
+"""
+    TestParticleB200
+
+Drop-in B200 ensemble algorithm for TestParticle.jl: `EnsembleB200()` routes
+`TestParticle.solve(prob, Boris() | MultistepBoris{N}(; n) | AdaptiveBoris(; safety),
+EnsembleB200(); dt, savestepinterval, trajectories, ...)` and
+`TestParticle.solve(prob::TraceGCProblem, EnsembleB200(); alg = :rk4 | :rk45, ...)`
+to libtpb200.so through `ccall`, and returns the reference's `EnsembleSolution`
+(one `ODESolution` per trajectory, `LinearInterpolation`, retcodes).
+
+It adds methods to the reference's own dispatch points
+(`_solve(::EnsembleAlg, ::TraceProblem, ...)`, src/boris/boris.jl:137-318;
+`_solve_adaptive(::EnsembleAlg, ...)`, src/boris/adaptive_boris.jl:40-139;
+`_solve(::EnsembleAlg, ::TraceGCProblem, ...)`, src/gc/gc_solver.jl:104-161).
+
+Fields must be one of the device-evaluable types below (closures cannot run on
+the device); they are ordinary callables, so the reference CPU solver runs on
+the same objects for a like-for-like comparison.  `isoutside` must be a
+`Terminate` predicate.
+"""
+module TestParticleB200
+
+using TestParticle
+import TestParticle: _solve, _solve_adaptive, TraceProblem, TraceGCProblem, Boris, MultistepBoris,
+    ZeroField, Field
+using SciMLBase: BasicEnsembleAlgorithm, EnsembleSolution, EnsembleContext, ReturnCode,
+    LinearInterpolation, build_solution
+using StaticArrays: SVector
+
+export EnsembleB200, UniformField, AffineField, DipoleField, B200Grid, Terminate
+
+const libtpb200 = get(ENV, "TPB200_LIB", joinpath(@__DIR__, "..", "..", "..", "libtpb200.so"))
+
+# ------------------------------------------------------------------ ensemble
+"""
+    EnsembleB200(; device = 0, precision = :fp64, schedule = :auto)
+
+`precision = :fp64` is the drop-in path (reference operation order);
+`:fp32c` the float32 push with compensated positions and velocities.
+"""
+struct EnsembleB200 <: BasicEnsembleAlgorithm
+    device::Int
+    precision::Symbol
+    schedule::Symbol
+end
+EnsembleB200(; device = 0, precision = :fp64, schedule = :auto) = EnsembleB200(device, precision, schedule)
+
+# ------------------------------------------------------------------ fields
+"Uniform field F(x) = v."
+struct UniformField{T} <: Function
+    v::SVector{3, T}
+end
+(f::UniformField)(x) = f.v
+
+"Affine field F(x, t) = v + J x + rate t."
+struct AffineField{T} <: Function
+    v::SVector{3, T}
+    J::NTuple{9, T}       # row-major
+    rate::SVector{3, T}
+end
+function (f::AffineField)(x, t)
+    J = f.J
+    return f.v + SVector(J[1] * x[1] + J[2] * x[2] + J[3] * x[3],
+        J[4] * x[1] + J[5] * x[2] + J[6] * x[3],
+        J[7] * x[1] + J[8] * x[2] + J[9] * x[3]) + f.rate * t
+end
+
+"Point dipole B = coef (3 (m.rhat) rhat - m) / |x - c|^3."
+struct DipoleField{T} <: Function
+    m::SVector{3, T}
+    c::SVector{3, T}
+    coef::T
+end
+DipoleField(m; c = SVector(0.0, 0.0, 0.0), coef = TestParticle.μ₀ / (4π)) =
+    DipoleField(SVector{3}(Float64.(m)), SVector{3}(Float64.(c)), Float64(coef))
+function (f::DipoleField)(x)
+    d = x - f.c
+    r = sqrt(d[1]^2 + d[2]^2 + d[3]^2)
+    rh = d / r
+    return f.coef * (3 * (f.m' * rh) * rh - f.m) / r^3
+end
+
+"""
+    B200Grid(A, x, y, z; bc = :fill_nan | :clamp | :periodic)
+
+Trilinear interpolator of a (3, nx, ny, nz) Float32/Float64 array on uniform
+ranges, evaluated identically on the CPU (this callable) and on the device.
+"""
+struct B200Grid{T} <: Function
+    A::Array{T, 4}
+    origin::NTuple{3, Float64}
+    spacing::NTuple{3, Float64}
+    bc::Int32
+end
+function B200Grid(A::Array{T, 4}, x::AbstractRange, y::AbstractRange, z::AbstractRange; bc = :fill_nan) where {T}
+    code = bc === :fill_nan ? Int32(0) : bc === :clamp ? Int32(1) : bc === :periodic ? Int32(2) :
+        throw(ArgumentError("bc must be :fill_nan, :clamp or :periodic"))
+    return B200Grid{T}(A, (first(x), first(y), first(z)), (step(x), step(y), step(z)), code)
+end
+function (g::B200Grid)(x)
+    idx = ntuple(3) do a
+        n = size(g.A, a + 1)
+        u = (x[a] - g.origin[a]) * (1 / g.spacing[a])
+        if g.bc == 2
+            fl = floor(u); i = mod(Int(fl), n)
+            (i, i + 1 == n ? 0 : i + 1, u - fl)
+        else
+            g.bc == 1 && (u = clamp(u, 0.0, n - 1.0))
+            (g.bc == 0 && !(0 <= u <= n - 1)) && return nothing
+            i = min(Int(floor(u)), n - 2)
+            (i, i + 1, u - i)
+        end
+    end
+    any(isnothing, idx) && return SVector(NaN, NaN, NaN)
+    (i0, i1, fx), (j0, j1, fy), (k0, k1, fz) = idx
+    lerp(a, b, f) = a + f * (b - a)
+    c(v, i, j, k) = Float64(g.A[v, i + 1, j + 1, k + 1])
+    return SVector(ntuple(v -> lerp(lerp(lerp(c(v, i0, j0, k0), c(v, i1, j0, k0), fx),
+        lerp(c(v, i0, j1, k0), c(v, i1, j1, k0), fx), fy),
+        lerp(lerp(c(v, i0, j0, k1), c(v, i1, j0, k1), fx),
+            lerp(c(v, i0, j1, k1), c(v, i1, j1, k1), fx), fy), fz), 3))
+end
+
+# ------------------------------------------------------------------ termination
+"isoutside(u, p, t) as flags: shell rmin/rmax, box lo/hi, NaN, t > tmax."
+Base.@kwdef struct Terminate <: Function
+    flags::Int32 = 0
+    rmin::Float64 = -Inf
+    rmax::Float64 = Inf
+    lo::NTuple{3, Float64} = (-Inf, -Inf, -Inf)
+    hi::NTuple{3, Float64} = (Inf, Inf, Inf)
+    tmax::Float64 = Inf
+end
+function (T::Terminate)(u, p, t)
+    (T.flags & 4 != 0) && any(isnan, u) && return true
+    if T.flags & 1 != 0
+        r = sqrt(u[1]^2 + u[2]^2 + u[3]^2)
+        (r < T.rmin || r > T.rmax) && return true
+    end
+    (T.flags & 2 != 0) && any(c -> u[c] < T.lo[c] || u[c] > T.hi[c], 1:3) && return true
+    (T.flags & 8 != 0) && t > T.tmax && return true
+    return false
+end
+
+# ------------------------------------------------------------------ C descriptors (include/tp_abi.h)
+struct TpFieldDesc
+    kind::Int32; bc::Int32; dtype::Int32; reserved::Int32
+    value::NTuple{3, Float64}; jac::NTuple{9, Float64}; rate::NTuple{3, Float64}
+    moment::NTuple{3, Float64}; center::NTuple{3, Float64}; coef::Float64
+    n::NTuple{3, Int64}; origin::NTuple{3, Float64}; spacing::NTuple{3, Float64}
+    data::Ptr{Cvoid}
+end
+struct TpTermDesc
+    flags::Int32; reserved::Int32; rmin::Float64; rmax::Float64
+    lo::NTuple{3, Float64}; hi::NTuple{3, Float64}; tmax::Float64
+end
+struct TpRunDesc
+    alg::Int32; order::Int32; nsub::Int32; precision::Int32
+    safety::Float64; t0::Float64; t1::Float64; dt::Float64; q2m::Float64; m::Float64
+    savestepinterval::Int64; maxiters::Int64
+    save_start::Int32; save_end::Int32; save_everystep::Int32; save_fields::Int32
+    term::TpTermDesc; step_cap::Int64; schedule::Int32; block::Int32; budget_s::Float64
+end
+struct TpGCDesc
+    alg::Int32; precision::Int32; t0::Float64; t1::Float64; dt::Float64
+    dt_given::Int32; reserved::Int32; q::Float64; q2m::Float64; mu::Float64
+    abstol::Float64; reltol::Float64; savestepinterval::Int64; maxiters::Int64
+    save_start::Int32; save_end::Int32; save_everystep::Int32; save_fields::Int32
+    term::TpTermDesc; block::Int32; reserved2::Int32; budget_s::Float64
+end
+
+const Z3 = (0.0, 0.0, 0.0)
+const Z9 = ntuple(_ -> 0.0, 9)
+unwrap(f::Field) = f.field_function
+unwrap(f) = f
+fdesc(::ZeroField) = TpFieldDesc(0, 0, 0, 0, Z3, Z9, Z3, Z3, Z3, 0.0, (0, 0, 0), Z3, Z3, C_NULL)
+fdesc(f::UniformField) = TpFieldDesc(1, 0, 0, 0, Tuple(Float64.(f.v)), Z9, Z3, Z3, Z3, 0.0, (0, 0, 0), Z3, Z3, C_NULL)
+fdesc(f::AffineField) = TpFieldDesc(2, 0, 0, 0, Tuple(Float64.(f.v)), Float64.(f.J), Tuple(Float64.(f.rate)),
+    Z3, Z3, 0.0, (0, 0, 0), Z3, Z3, C_NULL)
+fdesc(f::DipoleField) = TpFieldDesc(3, 0, 0, 0, Z3, Z9, Z3, Tuple(f.m), Tuple(f.c), f.coef, (0, 0, 0), Z3, Z3, C_NULL)
+fdesc(g::B200Grid{T}) where {T} = TpFieldDesc(4, g.bc, T === Float32 ? 0 : 1, 0, Z3, Z9, Z3, Z3, Z3, 0.0,
+    Int64.(size(g.A)[2:4]), g.origin, g.spacing, pointer(g.A))
+fdesc(f) = throw(ArgumentError("field not supported by EnsembleB200: $(typeof(f)); use ZeroField, " *
+    "UniformField, AffineField, DipoleField or B200Grid"))
+
+termdesc(::typeof(TestParticle.ODE_DEFAULT_ISOUTOFDOMAIN)) = TpTermDesc(0, 0, -Inf, Inf, (-Inf, -Inf, -Inf), (Inf, Inf, Inf), Inf)
+termdesc(T::Terminate) = TpTermDesc(T.flags, 0, T.rmin, T.rmax, T.lo, T.hi, T.tmax)
+termdesc(f) = throw(ArgumentError("isoutside must be a TestParticleB200.Terminate predicate on the B200"))
+
+# ------------------------------------------------------------------ library calls
+const CTX = Dict{Int, Ptr{Cvoid}}()
+function context(dev::Int)
+    get!(CTX, dev) do
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        st = ccall((:tp_ctx_create, libtpb200), Cint, (Cint, Ref{Ptr{Cvoid}}), dev, r)
+        st == 0 || error("tp_ctx_create failed ($st)")
+        r[]
+    end
+end
+function check(ctx, st, what)
+    st == 0 && return
+    msg = unsafe_string(ccall((:tp_last_error, libtpb200), Cstring, (Ptr{Cvoid},), ctx))
+    st == -1 ? throw(ArgumentError("$what: $msg")) : error("$what: $msg (status $st)")
+end
+function field_handle(ctx, f)
+    d = Ref(fdesc(f))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve f check(ctx, ccall((:tp_field_create, libtpb200), Cint,
+        (Ptr{Cvoid}, Ref{TpFieldDesc}, Ref{Ptr{Cvoid}}), ctx, d, h), "tp_field_create")
+    return h[]
+end
+free_field(h) = ccall((:tp_field_destroy, libtpb200), Cvoid, (Ptr{Cvoid},), h)
+
+# the (6, N) initial-state table: prob_func applied on the host (boris_kernel.jl:290-294)
+function initial_table(prob, trajectories, seed)
+    U = Matrix{Float64}(undef, length(prob.u0), trajectories)
+    for i in 1:trajectories
+        rng = isnothing(seed) ? TestParticle.default_rng() : TestParticle.Xoshiro(TestParticle._rng_seed(seed, i))
+        U[:, i] .= prob.prob_func(prob, EnsembleContext(i, 1, 0, nothing, rng, seed)).u0
+    end
+    return U
+end
+
+const RETCODES = Dict(1 => ReturnCode.Success, 2 => ReturnCode.Terminated, 3 => ReturnCode.MaxIters,
+    0 => ReturnCode.Default)
+
+function collect_result(ctx, res, prob, alg_name, T)
+    n = Ref{Int64}(0); w = Ref{Int32}(0); tot = Ref{Int64}(0)
+    ccall((:tp_result_info, libtpb200), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int32}, Ref{Int64}), res, n, w, tot)
+    ns = Vector{Int32}(undef, n[]); rc = Vector{Int8}(undef, n[]); st = Vector{Int64}(undef, n[])
+    t = Vector{Float64}(undef, tot[]); u = Matrix{Float64}(undef, w[], tot[])
+    ccall((:tp_result_copy, libtpb200), Cint, (Ptr{Cvoid}, Ptr{Int32}, Ptr{Int8}, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}),
+        res, ns, rc, st, t, u)
+    ms = Ref{Float64}(0.0)
+    ccall((:tp_result_elapsed_ms, libtpb200), Cint, (Ptr{Cvoid}, Ref{Float64}), res, ms)
+    ccall((:tp_result_destroy, libtpb200), Cvoid, (Ptr{Cvoid},), res)
+    W = Int(w[])
+    sols = Vector{Any}(undef, n[])
+    off = 0
+    for i in 1:n[]
+        r = (off + 1):(off + ns[i])
+        ti = t[r]
+        ui = [SVector{W, T}(view(u, :, k)) for k in r]
+        sols[i] = build_solution(prob, alg_name, ti, ui; interp = LinearInterpolation(ti, ui),
+            retcode = RETCODES[Int(rc[i])], stats = nothing)
+        off += ns[i]
+    end
+    return EnsembleSolution([s for s in sols], ms[] * 1e-3, true)
+end
+
+function boris_run(ens::EnsembleB200, prob::TraceProblem, alg, adaptive, trajectories, dt, savestepinterval,
+        isoutside, save_start, save_end, save_everystep, save_fields, maxiters, seed, alg_name)
+    ctx = context(ens.device)
+    q2m, m, E, B, _ = prob.p
+    hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
+    try
+        multi = alg isa MultistepBoris
+        N = multi ? typeof(alg).parameters[1] : 2
+        desc = Ref(TpRunDesc(adaptive ? (multi ? 3 : 2) : (multi ? 1 : 0), N, multi ? alg.n : 1,
+            ens.precision === :fp32c ? 1 : 0, alg.safety, prob.tspan[1], prob.tspan[2],
+            isnothing(dt) ? 0.0 : dt, q2m, m, savestepinterval, maxiters,
+            save_start, save_end, save_everystep, save_fields, termdesc(isoutside), 0,
+            ens.schedule === :static ? 1 : ens.schedule === :queue ? 2 : 0, 0, 0.0))
+        U = initial_table(prob, trajectories, seed)
+        res = Ref{Ptr{Cvoid}}(C_NULL)
+        st = ccall((:tp_boris_run, libtpb200), Cint,
+            (Ptr{Cvoid}, Ref{TpRunDesc}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
+                Ref{Ptr{Cvoid}}), ctx, desc, hE, hB, U, C_NULL, C_NULL, trajectories, res)
+        check(ctx, st, "tp_boris_run")
+        return collect_result(ctx, res[], prob, alg_name, eltype(prob.u0))
+    finally
+        free_field(hE); free_field(hB)
+    end
+end
+
+# ------------------------------------------------------------------ drop-in methods
+function _solve(ens::EnsembleB200, prob::TraceProblem, alg::TestParticle.AbstractBoris, trajectories, dt,
+        savestepinterval, isoutside, save_start, save_end, save_everystep,
+        ::Val{SaveFields}, ::Val{SaveWork}, maxiters, batch_size, seed) where {SaveFields, SaveWork}
+    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
+    name = alg isa MultistepBoris ? :multistep_boris : :boris
+    return boris_run(ens, prob, alg, false, trajectories, dt, savestepinterval, isoutside, save_start,
+        save_end, save_everystep, SaveFields, maxiters, seed, name)
+end
+
+function _solve_adaptive(ens::EnsembleB200, prob, trajectories, alg::TestParticle.AbstractBoris, savestepinterval,
+        isoutside, save_start, save_end, save_everystep, ::Val{SaveFields}, ::Val{SaveWork},
+        batch_size) where {SaveFields, SaveWork}
+    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
+    name = alg isa Boris ? :adaptive_boris : :adaptive_multistep_boris
+    return boris_run(ens, prob, alg, true, trajectories, nothing, savestepinterval, isoutside, save_start,
+        save_end, save_everystep, SaveFields, typemax(Int64), nothing, name)
+end
+
+function _solve(ens::EnsembleB200, prob::TraceGCProblem, trajectories, dt, savestepinterval, isoutside,
+        save_start, save_end, save_everystep, alg, abstol, reltol, maxiters,
+        ::Val{SaveFields}, ::Val{SaveWork}, seed) where {SaveFields, SaveWork}
+    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
+    ctx = context(ens.device)
+    q, q2m, μ, E, B = prob.p
+    hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
+    try
+        desc = Ref(TpGCDesc(alg == :rk45 ? 1 : 0, ens.precision === :fp64 ? 0 : 1, prob.tspan[1], prob.tspan[2],
+            isnothing(dt) ? 0.0 : dt, isnothing(dt) ? 0 : 1, 0, q, q2m, μ, abstol, reltol, savestepinterval,
+            maxiters, save_start, save_end, save_everystep, SaveFields, termdesc(isoutside), 0, 0, 0.0))
+        Y = initial_table(prob, trajectories, seed)
+        res = Ref{Ptr{Cvoid}}(C_NULL)
+        st = ccall((:tp_gc_run, libtpb200), Cint,
+            (Ptr{Cvoid}, Ref{TpGCDesc}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Ref{Ptr{Cvoid}}),
+            ctx, desc, hE, hB, Y, C_NULL, C_NULL, C_NULL, C_NULL, C_NULL, trajectories, res)
+        check(ctx, st, "tp_gc_run")
+        return collect_result(ctx, res[], prob, alg == :rk45 ? :rk45 : :rk4, eltype(prob.u0))
+    finally
+        free_field(hE); free_field(hB)
+    end
+end
+
+end # module
