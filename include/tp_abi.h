@@ -271,6 +271,26 @@ int tp_result_copy(const tp_result* res, int32_t* nsaved, int8_t* retcode,
 int tp_result_elapsed_ms(const tp_result* res, double* ms);
 void tp_result_destroy(tp_result* res);
 
+/* ---- packing without allocation ---------------------------------------------
+ * No counterpart in the reference: an addition of this library for callers
+ * that must not let a library allocate device memory (their own memory pool
+ * owns every buffer, or allocation is off-limits on their latency path).
+ * Packs the slot-major output of tp_boris_run_device (or a guiding-centre run
+ * written the same way) into the per-trajectory layout of tp_result_copy, on
+ * `stream`, using a static device scratch array instead of cudaMalloc:
+ *   t_in[k*n + i], u_in[(k*width + c)*n + i], nsaved[i]  (device, as written)
+ *   t_out, u_out  device buffers of at least total saves (n * nslots is safe)
+ *   total_out     device int64 receiving the number of packed saves
+ * n may not exceed TP_NOALLOC_MAX_TRAJECTORIES (else TP_E_ARG).  Calls share
+ * the scratch: calls that overlap on the GPU race.  The first call on a
+ * device performs a one-time set-up; make it before any stream capture.    */
+#define TP_NOALLOC_MAX_TRAJECTORIES 1048576
+int tp_pack_results_device_noalloc(tp_ctx* ctx, const double* t_in,
+                                   const double* u_in, const int32_t* nsaved,
+                                   int64_t n, int64_t nslots, int32_t width,
+                                   double* t_out, double* u_out,
+                                   int64_t* total_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

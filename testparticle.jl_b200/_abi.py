@@ -172,7 +172,12 @@ SIGNATURES = [
     ("tp_result_copy", C.c_int, [_P, _P, _P, _P, _P, _P]),
     ("tp_result_elapsed_ms", C.c_int, [_P, _DP]),
     ("tp_result_destroy", None, [_P]),
+    ("tp_pack_results_device_noalloc", C.c_int,
+     [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
 ]
+
+# static scratch limit of tp_pack_results_device_noalloc (include/tp_abi.h)
+TP_NOALLOC_MAX_TRAJECTORIES = 1048576
 
 _lib = None
 

@@ -1027,3 +1027,11 @@ int tp_result_elapsed_ms(const tp_result* r, double* ms) {
 void tp_result_destroy(tp_result* r) { delete r; }
 
 }  // extern "C"
+
+namespace tpb {
+int ctx_device(const tp_ctx* ctx) { return ctx->device; }
+int ctx_fail(tp_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+}  // namespace tpb

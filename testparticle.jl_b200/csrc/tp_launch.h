@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "tp_device.cuh"
 
 namespace tpb {
@@ -58,6 +60,16 @@ cudaError_t launch_gc(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_gc_fp32(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 int occupancy_gc(const GCArgs& a, int block);
 cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
+
+// context accessors for translation units outside runtime.cu
+int ctx_device(const tp_ctx* ctx);
+int ctx_fail(tp_ctx* ctx, int code, const std::string& msg);
+
+// static-scratch packing (noalloc.cu)
+int noalloc_scratch(int device, int64_t** out);
+cudaError_t launch_noalloc_pack(int64_t* scratch, const double* t_in, const double* u_in,
+                                const int32_t* nsaved, int64_t n, int64_t nslots, int width,
+                                double* t_out, double* u_out, int64_t* total_out, cudaStream_t s);
 
 // packing helpers (pack.cu)
 cudaError_t launch_pack_node_table(const void* src, int src_f64, int64_t nodes, void* dst,
