@@ -22,7 +22,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -38,6 +37,9 @@ sys.path.insert(0, str(ROOT))
 import __graft_entry__ as ge  # noqa: E402
 
 BYTES_PER_PARTICLE_STEP = 192  # 8 trilinear corners x (E, B) x 3 float32
+# DRAM bytes per particle-step of k_fixed32c on this workload, from an ncu
+# capture (profiles/k_fixed32c_config2_gridded.md): 1.683 GB / 2e8 particle-steps
+TRAFFIC_PER_PARTICLE_STEP = 8.4
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -172,6 +174,137 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+class DeviceRun:
+    """Device buffers of one full-orbit workload, launched through tp_boris_run_device."""
+
+    def __init__(self, tp, torch, ctx, plan, dev, stream):
+        self.tp, self.torch, self.ctx = tp, torch, ctx
+        self.n = n = plan.u0.shape[0]
+        self.nslots = ctx.slots(plan.desc, n, plan.dt_i, plan.tend_i)
+        if self.nslots < 0:
+            raise SystemExit("bench runs need a bounded number of saves (set step_cap for adaptive runs)")
+        W = 12 if plan.desc.save_fields else 6
+        f = lambda a: None if a is None else torch.from_numpy(a).to(dev)  # noqa: E731
+        self.u0, self.dt_i, self.tend_i = f(plan.u0), f(plan.dt_i), f(plan.tend_i)
+        self.t_out = torch.empty((self.nslots, n), dtype=torch.float64, device=dev)
+        self.u_out = torch.empty((self.nslots, W, n), dtype=torch.float64, device=dev)
+        self.nsaved = torch.empty(n, dtype=torch.int32, device=dev)
+        self.retc = torch.empty(n, dtype=torch.int8, device=dev)
+        self.nsteps = torch.empty(n, dtype=torch.int64, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.stream = stream
+
+    def launch(self, plan):
+        p = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        self.ctx.boris_run_device(plan.desc, plan.E, plan.B, p(self.u0), p(self.dt_i), p(self.tend_i), self.n,
+                                  self.nslots, p(self.t_out), p(self.u_out), p(self.nsaved), p(self.retc),
+                                  p(self.nsteps), p(self.status), self.stream.cuda_stream)
+
+    def check(self):
+        st = int(self.status.item())
+        if st != 0:
+            raise SystemExit(f"kernel status {st}")
+
+    def final_states(self):
+        ns = self.nsaved.to("cpu").numpy().astype(np.int64)
+        u = self.u_out.to("cpu").numpy()
+        idx = np.clip(ns - 1, 0, u.shape[0] - 1)
+        return u[idx, :, np.arange(self.n)]
+
+    def particle_steps(self):
+        return float(self.nsteps.sum().item())
+
+
+def timed(torch, dist, dev, run, plan, k, warm, flush):
+    """k launches bracketed by barrier + synchronize; device time (ms), max over ranks."""
+    for _ in range(warm):
+        run.launch(plan)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(k):
+        flush.zero_()  # L2 flush between timed iterations (outside the events)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(run.stream)
+        run.launch(plan)
+        b.record(run.stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    tot = torch.tensor([sum(a.elapsed_time(b) for a, b in evs)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    run.check()
+    return float(tot.item())
+
+
+def _plan(tp, w, alg, prec, device, step_cap=0):
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    return tp.plan_boris(prob, alg, tp.EnsembleB200(device=device, precision=prec), dt=w.dt, tend=w.tend,
+                         savestepinterval=w.savestepinterval, isoutside=w.isoutside, step_cap=step_cap)
+
+
+def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
+    """Dipole ensemble (config 3): MultistepBoris4(n=2) and AdaptiveBoris(0.1), FP32C vs FP64."""
+    w = tp.workloads.config3(n=n, nt=nt, ssi=min(1000, nt))
+    out = {"workload": w.name, "particles": n, "time_steps": nt}
+    for name, alg, cap in (("multistep4_n2", tp.MultistepBoris4(2), 0), ("adaptive_0.1", tp.AdaptiveBoris(0.1), nt)):
+        p32, p64 = _plan(tp, w, alg, "fp32c", ctx.device, cap), _plan(tp, w, alg, "fp64", ctx.device, cap)
+        run = DeviceRun(tp, torch, ctx, p32, dev, stream)
+        ms32 = timed(torch, dist, dev, run, p32, 1, 1, flush)
+        ps32 = run.particle_steps()
+        fs32, rc32 = run.final_states(), run.retc.cpu().numpy()
+        ms64 = timed(torch, dist, dev, run, p64, 1, 1, flush)
+        ps64 = run.particle_steps()
+        fs64, rc64 = run.final_states(), run.retc.cpu().numpy()
+        # float64 started 1 ulp away: the orbits' own sensitivity
+        u0_saved = run.u0.clone()
+        run.u0.mul_(1.0 + 2.0 ** -52)
+        run.launch(p64)
+        torch.cuda.synchronize()
+        fs64b, rc64b = run.final_states(), run.retc.cpu().numpy()
+        run.u0.copy_(u0_saved)
+        ok = (rc32 == 1) & (rc64 == 1)
+        okb = (rc64b == 1) & (rc64 == 1)
+        v32, v64 = world * ps32 / (ms32 * 1e-3), world * ps64 / (ms64 * 1e-3)
+        out[name] = {"fp32c": v32, "fp64": v64, "speedup_fp32c_over_fp64": v32 / v64,
+                     "unit": "particle-steps/s", "fp32c_error_vs_fp64": _err_summary(_rel_err(fs32[ok], fs64[ok])),
+                     "fp64_vs_fp64_1ulp_start": _err_summary(_rel_err(fs64b[okb], fs64[okb])),
+                     "both_success_fraction": float(ok.mean())}
+    return out
+
+
+def leg_gc(tp, n):
+    """Guiding centres in the dipole (config 4): RK4 over 5 bounce periods, RK45, FP64 vs float32 RHS."""
+    w = tp.workloads.config4(n)
+    prob = tp.TraceGCProblem(w.y0, (0.0, 1.0), (w.q, w.q2m, w.mu, w.E, w.B))
+    out = {"workload": w.name, "particles": n}
+    res = {}
+    for prec in ("fp64", "fp32"):
+        for alg, kw in (("rk4", dict(dt=w.tau_b / 200)), ("rk45", dict(abstol=1e-9, reltol=1e-6))):
+            s = tp.solve(prob, tp.EnsembleB200(precision=prec), alg=alg, tend=5 * w.tau_b, savestepinterval=100000,
+                         maxiters=1_000_000, **kw)
+            res[(prec, alg)] = s
+            out[f"{alg}_{prec}"] = {"value": s.particle_steps() / s.elapsedTime, "unit": "particle-steps/s",
+                                    "device_s": s.elapsedTime}
+    # energy 1/2 m v_par^2 + mu |B| at the end, float32 RHS against float64 (same algorithm)
+    for alg in ("rk4", "rk45"):
+        a, b = res[("fp32", alg)].final_states(), res[("fp64", alg)].final_states()
+        def energy(s):
+            B = np.linalg.norm(tp.workloads.dipole_B(s[:, :3], (0.0, 0.0, -8.0e22)), axis=1)
+            return 0.5 * w.m * s[:, 3] ** 2 + w.mu * B
+        e0 = energy(w.y0.T)
+        e64, e32 = energy(b), energy(a)
+        out[f"{alg}_energy_drift_fp64_median"] = float(np.median(np.abs(e64 - e0) / e0))
+        out[f"{alg}_fp32rhs_vs_fp64"] = {"energy_rel_median": float(np.median(np.abs(e32 - e64) / e64)),
+                                         "position": _err_summary(_rel_err(a, b))}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -184,6 +317,7 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="skip the dipole / guiding-centre legs")
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -201,101 +335,51 @@ def main():
     ctx = tp.Context.get(local)
     w = _workload(tp, args.workload, args.particles, args.nt)
     alg = _alg(tp, args.workload)
-    n = w.n
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    sptr = stream.cuda_stream
-
-    def plan(prec):
-        prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
-        return tp.plan_boris(prob, alg, tp.EnsembleB200(device=local, precision=prec), dt=w.dt, tend=w.tend,
-                             savestepinterval=w.savestepinterval, isoutside=w.isoutside)
-
-    p32, p64 = plan("fp32c"), plan("fp64")
-    nslots = ctx.slots(p32.desc, n, p32.dt_i, p32.tend_i)
-    W = 6
-    u0_d = torch.from_numpy(p32.u0).to(dev)
-    dti_d = None if p32.dt_i is None else torch.from_numpy(p32.dt_i).to(dev)
-    tend_d = None if p32.tend_i is None else torch.from_numpy(p32.tend_i).to(dev)
-    t_out = torch.empty((nslots, n), dtype=torch.float64, device=dev)
-    u_out = torch.empty((nslots, W, n), dtype=torch.float64, device=dev)
-    nsaved = torch.empty(n, dtype=torch.int32, device=dev)
-    retc = torch.empty(n, dtype=torch.int8, device=dev)
-    nsteps = torch.empty(n, dtype=torch.int64, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
-    def ptr(t):
-        return None if t is None else t.data_ptr()
-
-    def launch(p):
-        ctx.boris_run_device(p.desc, p.E, p.B, ptr(u0_d), ptr(dti_d), ptr(tend_d), n, nslots, ptr(t_out),
-                             ptr(u_out), ptr(nsaved), ptr(retc), ptr(nsteps), ptr(status), sptr)
-
-    def timed(p, k, warm):
-        for _ in range(warm):
-            launch(p)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        evs = []
-        for _ in range(k):
-            flush.zero_()  # L2 flush between timed iterations (outside the events)
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            launch(p)
-            b.record(stream)
-            evs.append((a, b))
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        ms = [a.elapsed_time(b) for a, b in evs]
-        tot = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-        if int(status.item()) != 0:
-            raise SystemExit(f"kernel status {int(status.item())}")
-        return float(tot.item()), ms
+    p32, p64 = _plan(tp, w, alg, "fp32c", local), _plan(tp, w, alg, "fp64", local)
+    run = DeviceRun(tp, torch, ctx, p32, dev, stream)
 
     # ---- FP32C (headline), clocks sampled during the timed region
     sampler = ClockSampler(local)
-    status.zero_()
-    launch(p32)  # first call builds the interleaved field table
+    run.launch(p32)  # first call builds the interleaved field table
     torch.cuda.synchronize()
     sampler.start()
-    tot32, ms32 = timed(p32, args.steps, args.warmup)
+    tot32 = timed(torch, dist, dev, run, p32, args.steps, args.warmup, flush)
     clocks = sampler.stop()
-    ps_step = float(nsteps.sum().item())
-    fs32 = _final_states(tp, t_out, u_out, nsaved, n)
+    ps_step = run.particle_steps()
+    fs32 = run.final_states()
 
     # ---- FP64 drop-in path on the same workload
-    status.zero_()
-    tot64, ms64 = timed(p64, max(args.fp64_steps, 1), 1)
-    ps64 = float(nsteps.sum().item())
-    fs64 = _final_states(tp, t_out, u_out, nsaved, n)
+    k64 = max(args.fp64_steps, 1)
+    tot64 = timed(torch, dist, dev, run, p64, k64, 1, flush)
+    ps64 = run.particle_steps()
+    fs64 = run.final_states()
     err = _rel_err(fs32, fs64)
     # the same float64 solve started 1 ulp away: how fast neighbouring orbits
     # separate in this field (chaotic flows separate at any precision)
-    u0_saved = u0_d.clone()
-    u0_d.mul_(1.0 + 2.0 ** -52)
-    launch(p64)
+    u0_saved = run.u0.clone()
+    run.u0.mul_(1.0 + 2.0 ** -52)
+    run.launch(p64)
     torch.cuda.synchronize()
-    fs64b = _final_states(tp, t_out, u_out, nsaved, n)
-    u0_d.copy_(u0_saved)
-    chaos = _rel_err(fs64b, fs64)
+    chaos = _rel_err(run.final_states(), fs64)
+    run.u0.copy_(u0_saved)
 
     value = world * ps_step * args.steps / (tot32 * 1e-3)
-    value64 = world * ps64 * max(args.fp64_steps, 1) / (tot64 * 1e-3)
+    value64 = world * ps64 * k64 / (tot64 * 1e-3)
     kernel_s = tot32 * 1e-3 / args.steps
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_PARTICLE_STEP * ps_step / kernel_s / 1e9
+    sm_clock = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    l1_ceiling = 148 * sm_clock / 8  # one L1 wavefront per SM clock, 8 corner lines per particle-step
 
     # ---- end to end through the public API (host arrays in, packed host results out)
     prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
     e2e_t = []
     h2d = d2h = 0
+    sol = None
     for k in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -315,8 +399,14 @@ def main():
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             e2e_time = float(tt.item())
         e2e_value = world * float(sol.nsteps.sum()) / e2e_time
+    del sol
 
-    line = None
+    legs = {}
+    if not args.no_legs:
+        legs["dipole_config3"] = leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, 1_000_000, args.nt)
+        if rank == 0:
+            legs["guiding_centre_config4"] = leg_gc(tp, 1 << 20)
+
     if rank == 0:
         cpu = None
         if not args.no_cpu:
@@ -330,23 +420,28 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot32 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+compensated",
             "data": "synthetic (seeded SplitMix64)",
-            "config": {"workload": w.name, "particles": n, "time_steps": w.nt,
+            "config": {"workload": w.name, "particles": run.n, "time_steps": w.nt,
                        "savestepinterval": w.savestepinterval, "precision": "fp32c",
                        "inputs_in_hbm": True, "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}"},
-            "fp64": {"value": value64, "unit": "particle-steps/s", "ms_per_step": tot64 / args.fp64_steps,
+            "fp64": {"value": value64, "unit": "particle-steps/s", "ms_per_step": tot64 / k64,
                      "speedup_fp32c_over_fp64": value / value64},
             "fp32c_error_vs_fp64": _err_summary(err),
             "fp64_vs_fp64_1ulp_start": _err_summary(chaos),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": TRAFFIC_PER_PARTICLE_STEP * ps_step,
                          "note": f"{BYTES_PER_PARTICLE_STEP} algorithmic B/particle-step; peak {peak_kind}; "
-                                 "the 50 MB field table is L2-resident, so frac > 1 is possible"},
+                                 "the field table is L2-resident (DRAM traffic from an ncu capture, "
+                                 f"{TRAFFIC_PER_PARTICLE_STEP} B/particle-step), so frac > 1 is possible"},
+            "l1_wavefront_ceiling": {"value": l1_ceiling, "unit": "particle-steps/s",
+                                     "frac": value / world / l1_ceiling,
+                                     "note": "148 SMs x SM clock / 8 corner lines per particle-step"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps,
             "clocks": clocks,
+            "legs": legs,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -365,13 +460,6 @@ def _err_summary(e):
         return None
     return {"final_position_rel_median": float(np.median(e)), "p90": float(np.quantile(e, 0.9)),
             "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
-
-
-def _final_states(tp, t_out, u_out, nsaved, n):
-    ns = nsaved.to("cpu").numpy().astype(np.int64)
-    u = u_out.to("cpu").numpy()
-    idx = np.clip(ns - 1, 0, u.shape[0] - 1)
-    return u[idx, :, np.arange(n)]
 
 
 if __name__ == "__main__":

@@ -760,6 +760,33 @@ inline void update_dp5(const GCState& y, const GCParams& p, double dt, double t,
                           gscale(D::e7, k7)));
 }
 
+// x^0.2 rounded to nearest, the step-size factor of rk45_gc.jl:151
+// (`(1.0 / error_ratio)^0.2`, a Float64 `^`).  Julia's `^` and the C library's
+// pow are accurate to about half an ulp but, within a small fraction of an
+// ulp of a rounding tie, round either way; a one-ulp difference in the factor
+// shifts every later step.  Both the oracle and the CUDA kernels therefore use
+// this function: one Newton step for the real fifth root z = x^(1/5) from the
+// library pow z0, with the residual z0^5 - x evaluated in double-double
+// arithmetic (Dekker's exact product by fma; z0^5 - x is exact by Sterbenz's
+// lemma), then the exponent correction x^(0.2 - 1/5) = 1 + d ln x for the
+// float64 constant 0.2 = 1/5 + d, d = 2^-54 / 5.  The result is the correctly
+// rounded x^0.2 unless x^0.2 lies within ~1e-30 relative of a tie.  Outside
+// [1e-30, 1e30] (where the controller clamps the factor anyway) it returns z0.
+inline double pow02_rn(double x) {
+    double z0 = std::pow(x, 0.2);
+    if (!(x >= 1.0e-30 && x <= 1.0e30) || !(z0 > 0.0) || std::isinf(z0)) return z0;
+    double a = z0 * z0;
+    double ae = std::fma(z0, z0, -a);
+    double b = a * a;
+    double be = std::fma(a, a, -b) + (2.0 * a) * ae;
+    double c = b * z0;
+    double ce = std::fma(b, z0, -c) + be * z0;
+    double r = (c - x) + ce;
+    double corr = -r / (5.0 * b);
+    double t = (0.2 * 0x1p-54) * std::log(x);
+    return z0 + (corr + z0 * t);
+}
+
 // _rk45!, src/gc/rk45_gc.jl:52-173 (inside @fastmath: the error scale and the
 // sum of squares are fused multiply-adds)
 inline void rk45_single(const GCParams& p, const GCOpts& o, const Term& term, const double* y0,
@@ -808,7 +835,7 @@ inline void rk45_single(const GCParams& p, const GCOpts& o, const Term& term, co
             if (o.save_everystep) push_gc_save(out, p, o.save_fields, xv, t);
             steps += 1;
         }
-        double scale = (error_ratio == 0.0) ? max_growth : safety * std::pow(1.0 / error_ratio, 0.2);
+        double scale = (error_ratio == 0.0) ? max_growth : safety * pow02_rn(1.0 / error_ratio);
         scale = std::max(min_growth, std::min(scale, max_growth));
         dt *= scale;
         if (dt < 1.0e-14) break;

@@ -1,0 +1,401 @@
+// fp32c_common.cuh -- float32 compensated-position arithmetic shared by the
+// FP32C push kernels (boris_fp32c.cu) and the discrete adjoint (adjoint.cu):
+// compensated positions and velocities, the float cell index, trilinear
+// gathers from the interleaved E/B table, analytic fields, and the Boris and
+// Multistep velocity updates in delta form.
+#pragma once
+
+#include "tp_device.cuh"
+
+namespace tpb {
+
+namespace {
+
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Compensated position: x = hi + lo + w * L (w only on wrapped axes)
+struct CPos {
+    float hi[3], lo[3];
+    int w[3];
+};
+
+// TwoSum (Knuth) + Fast2Sum (Dekker): (hi, lo) += d
+__device__ __forceinline__ void cadd(float& hi, float& lo, float d) {
+    float s = __fadd_rn(hi, d);
+    float bb = __fsub_rn(s, hi);
+    float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(d, bb));
+    e = __fadd_rn(e, lo);
+    float h = __fadd_rn(s, e);
+    lo = __fsub_rn(e, __fsub_rn(h, s));
+    hi = h;
+}
+
+__device__ __forceinline__ double cpos_value(const BorisArgs& a, const CPos& p, int c) {
+    double x = (double)p.hi[c] + (double)p.lo[c];
+    if (a.wrap[c]) x += (double)p.w[c] * a.wrapL[c];
+    return x;
+}
+
+__device__ __forceinline__ void cpos_init(const BorisArgs& a, CPos& p, const double* x) {
+    for (int c = 0; c < 3; ++c) {
+        double v = x[c];
+        p.w[c] = 0;
+        if (a.wrap[c]) {
+            double k = floor((v - a.wrap0[c]) / a.wrapL[c]);
+            p.w[c] = (int)k;
+            v = v - k * a.wrapL[c];
+        }
+        p.hi[c] = (float)v;
+        p.lo[c] = (float)(v - (double)p.hi[c]);
+    }
+}
+
+__device__ __forceinline__ void cpos_push(const BorisArgs& a, CPos& p, F3 v, float dt) {
+    float d[3] = {v.x * dt, v.y * dt, v.z * dt};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        cadd(p.hi[c], p.lo[c], d[c]);
+        if (a.wrap[c]) {
+            float x0 = (float)a.wrap0[c];
+            float L = (float)a.wrapL[c];
+            if (p.hi[c] >= x0 + L) {
+                cadd(p.hi[c], p.lo[c], -L);
+                p.w[c] += 1;
+            } else if (p.hi[c] < x0) {
+                cadd(p.hi[c], p.lo[c], L);
+                p.w[c] -= 1;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fields
+struct AxF {
+    int i0, i1;
+    float f;
+};
+
+// cell index and fraction from the compensated coordinate
+// The cell index comes from rounding u = d/dx to the nearest integer with
+// the float "magic number" 1.5*2^23 (two float adds and an integer subtract
+// on the FP32/ALU pipes instead of floor + float-to-int conversions on the
+// XU pipe); the fraction is then corrected into [0, 1).  Valid for |u| <
+// 2^22, i.e. positions kept within the periodic box or a grid of < 4M cells;
+// larger |u| takes the floorf path.
+__device__ __forceinline__ bool axis32(const DevField& g, int a, float hi, float lo, AxF& o) {
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23
+    float d = hi - g.x0f[a];
+    float u = d * g.idxf[a];
+    float fl;
+    int i;
+    if (fabsf(u) < 4194304.0f) {
+        float tr = u + kMagic;
+        i = __float_as_int(tr) - __float_as_int(kMagic);
+        fl = tr - kMagic;
+    } else {
+        fl = floorf(u);
+        i = (int)fl;
+    }
+    float rem = fmaf(-fl, g.dxf[a], d) + lo;
+    float f = rem * g.idxf[a];
+    if (f < 0.0f) {
+        fl -= 1.0f;
+        i -= 1;
+        f += 1.0f;
+    } else if (f >= 1.0f) {
+        fl += 1.0f;
+        i += 1;
+        f -= 1.0f;
+    }
+    int na = g.n[a];
+    if (g.bc == TP_BC_PERIODIC) {
+        if (i >= na) i -= na;
+        if (i < 0) i += na;
+        if (i < 0 || i >= na) {  // far outside the box (positions not wrapped)
+            i %= na;
+            if (i < 0) i += na;
+        }
+        o.i0 = i;
+        o.i1 = (i + 1 == na) ? 0 : i + 1;
+        o.f = f;
+        return true;
+    }
+    float uc = fl + f;
+    float umax = (float)(na - 1);
+    if (g.bc == TP_BC_CLAMP) {
+        if (uc < 0.0f) {
+            fl = 0.0f;
+            f = 0.0f;
+        } else if (uc > umax) {
+            fl = umax;
+            f = 0.0f;
+        }
+    } else if (!(uc >= 0.0f && uc <= umax)) {
+        return false;
+    }
+    i = (int)fl;
+    if (i > na - 2) {
+        f += (float)(i - (na - 2));
+        i = na - 2;
+    }
+    o.i0 = i;
+    o.i1 = i + 1;
+    o.f = f;
+    return true;
+}
+
+__device__ __forceinline__ float lerp32(float a, float b, float f) { return fmaf(f, b - a, a); }
+
+__device__ __forceinline__ F3 nanf3() {
+    float q = __int_as_float(0x7fc00000);
+    return {q, q, q};
+}
+
+__device__ __forceinline__ bool axes32(const DevField& g, const CPos& p, AxF& ax, AxF& ay, AxF& az) {
+    bool ok = axis32(g, 0, p.hi[0], p.lo[0], ax);
+    ok = axis32(g, 1, p.hi[1], p.lo[1], ay) && ok;
+    ok = axis32(g, 2, p.hi[2], p.lo[2], az) && ok;
+    return ok;
+}
+
+__device__ __forceinline__ F3 xyz(float4 q) { return {q.x, q.y, q.z}; }
+
+// One 32-byte, 32-byte-aligned node record of the interleaved E/B table in a
+// single 256-bit read-only load (sm_100 ld.global.nc.v8).
+__device__ __forceinline__ void ldg_node8(const float4* p, float4& e, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
+__device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, F3 v101, F3 v011,
+                                   F3 v111, const AxF& ax, const AxF& ay, const AxF& az) {
+    F3 o;
+#define TPB_TRI32(c)                                                       \
+    {                                                                      \
+        float c0 = lerp32(lerp32(v000.c, v100.c, ax.f), lerp32(v010.c, v110.c, ax.f), ay.f); \
+        float c1 = lerp32(lerp32(v001.c, v101.c, ax.f), lerp32(v011.c, v111.c, ax.f), ay.f); \
+        o.c = lerp32(c0, c1, az.f);                                        \
+    }
+    TPB_TRI32(x)
+    TPB_TRI32(y)
+    TPB_TRI32(z)
+#undef TPB_TRI32
+    return o;
+}
+
+__device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
+    AxF ax, ay, az;
+    if (!axes32(g, p, ax, ay, az)) return nanf3();
+    const float4* T = g.tab32;
+    const int nx = g.n[0], nxy = g.n[0] * g.n[1];
+    int j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+    F3 v000 = xyz(__ldg(T + ax.i0 + j0 + k0)), v100 = xyz(__ldg(T + ax.i1 + j0 + k0));
+    F3 v010 = xyz(__ldg(T + ax.i0 + j1 + k0)), v110 = xyz(__ldg(T + ax.i1 + j1 + k0));
+    F3 v001 = xyz(__ldg(T + ax.i0 + j0 + k1)), v101 = xyz(__ldg(T + ax.i1 + j0 + k1));
+    F3 v011 = xyz(__ldg(T + ax.i0 + j1 + k1)), v111 = xyz(__ldg(T + ax.i1 + j1 + k1));
+    return tri3(v000, v100, v010, v110, v001, v101, v011, v111, ax, ay, az);
+}
+
+__device__ __forceinline__ F3 analytic_eval32(const DevField& f, const CPos& p, double t) {
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            return {f.vf[0], f.vf[1], f.vf[2]};
+        case TP_FIELD_AFFINE: {
+            float x = p.hi[0], y = p.hi[1], z = p.hi[2], tf = (float)t;
+            return {f.vf[0] + f.Jf[0] * x + f.Jf[1] * y + f.Jf[2] * z + f.ratef[0] * tf,
+                    f.vf[1] + f.Jf[3] * x + f.Jf[4] * y + f.Jf[5] * z + f.ratef[1] * tf,
+                    f.vf[2] + f.Jf[6] * x + f.Jf[7] * y + f.Jf[8] * z + f.ratef[2] * tf};
+        }
+        case TP_FIELD_DIPOLE: {
+            // unit-vector form keeps float intermediates normal:
+            // B = K/r^3 (3 (mh.rh) rh - mh), K = coef |m|
+            F3 d{(p.hi[0] - f.cf[0]) + p.lo[0], (p.hi[1] - f.cf[1]) + p.lo[1],
+                 (p.hi[2] - f.cf[2]) + p.lo[2]};
+            F3 mh{f.mhatf[0], f.mhatf[1], f.mhatf[2]};
+            float ir = __frsqrt_rn(dot(d, d));  // correctly rounded: |rh| = 1 to 1 ulp
+            F3 rh = ir * d;
+            float mr = dot(mh, rh);
+            float k = f.Kf * ir * ir * ir;
+            return {k * (3.0f * mr * rh.x - mh.x), k * (3.0f * mr * rh.y - mh.y), k * (3.0f * mr * rh.z - mh.z)};
+        }
+        default:
+            return {0.0f, 0.0f, 0.0f};
+    }
+}
+
+template <bool PACKED_ONLY = false>
+__device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
+    if (PACKED_ONLY || F.eb32) {
+        AxF ax, ay, az;
+        if (!axes32(F.B, p, ax, ay, az)) {
+            E = nanf3();
+            B = E;
+            return;
+        }
+        const float4* T = F.eb32;
+        const int nx = F.B.n[0], nxy = F.B.n[0] * F.B.n[1];
+        int j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+        int n000 = 2 * (ax.i0 + j0 + k0), n100 = 2 * (ax.i1 + j0 + k0);
+        int n010 = 2 * (ax.i0 + j1 + k0), n110 = 2 * (ax.i1 + j1 + k0);
+        int n001 = 2 * (ax.i0 + j0 + k1), n101 = 2 * (ax.i1 + j0 + k1);
+        int n011 = 2 * (ax.i0 + j1 + k1), n111 = 2 * (ax.i1 + j1 + k1);
+        // 8 corners, each one aligned 32-byte sector (E xyz0, B xyz0) read by
+        // one 256-bit load; all issued before any use
+        float4 e000, b000, e100, b100, e010, b010, e110, b110;
+        float4 e001, b001, e101, b101, e011, b011, e111, b111;
+        ldg_node8(T + n000, e000, b000);
+        ldg_node8(T + n100, e100, b100);
+        ldg_node8(T + n010, e010, b010);
+        ldg_node8(T + n110, e110, b110);
+        ldg_node8(T + n001, e001, b001);
+        ldg_node8(T + n101, e101, b101);
+        ldg_node8(T + n011, e011, b011);
+        ldg_node8(T + n111, e111, b111);
+        E = tri3(xyz(e000), xyz(e100), xyz(e010), xyz(e110), xyz(e001), xyz(e101), xyz(e011),
+                 xyz(e111), ax, ay, az);
+        B = tri3(xyz(b000), xyz(b100), xyz(b010), xyz(b110), xyz(b001), xyz(b101), xyz(b011),
+                 xyz(b111), ax, ay, az);
+        return;
+    }
+    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32(F.E, p) : analytic_eval32(F.E, p, t);
+    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32(F.B, p) : analytic_eval32(F.B, p, t);
+}
+
+template <int FK>
+__device__ __forceinline__ void eval_EB32t(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
+    if (FK == FK_ANALYTIC) {
+        E = analytic_eval32(F.E, p, t);
+        B = analytic_eval32(F.B, p, t);
+    } else if (FK == FK_EBGRID) {
+        eval_EB32<true>(F, p, t, E, B);
+    } else {
+        eval_EB32<false>(F, p, t, E, B);
+    }
+}
+
+__device__ __forceinline__ bool fields_static32(const DevFields& F) {
+    bool e = !(F.E.kind == TP_FIELD_AFFINE &&
+               (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
+    bool b = !(F.B.kind == TP_FIELD_AFFINE &&
+               (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
+    return e && b;
+}
+
+// ---------------------------------------------------------------- updates
+// Velocity as a compensated float pair, v = h + l, advanced in "delta form":
+// the kernels compute the change dv = v_new - v in float (|dv| ~ the
+// rotation angle times |v|, so its rounding is ~1e-8 |v|) and add it with
+// TwoSum.  The scalar rotation coefficients -- the only quantities whose
+// float rounding would bias the gyrophase every step -- are formed in
+// float64 from the float rotation vector; 1/(1+|t|^2) and 1/A use a float
+// reciprocal refined by one float64 Newton step.
+struct CV {
+    F3 h, l;
+};
+
+__device__ __forceinline__ void cv_add(CV& v, F3 d) {
+    cadd(v.h.x, v.l.x, d.x);
+    cadd(v.h.y, v.l.y, d.y);
+    cadd(v.h.z, v.l.z, d.z);
+}
+
+__device__ __forceinline__ CV cv_from(const double* u) {
+    CV v;
+    v.h = {(float)u[0], (float)u[1], (float)u[2]};
+    v.l = {(float)(u[0] - (double)v.h.x), (float)(u[1] - (double)v.h.y), (float)(u[2] - (double)v.h.z)};
+    return v;
+}
+
+// Boris (boris.jl:19-31): dv = 2 h E + (v- + v- x t) x s,  h = q2m*dt/2,
+// s = 2 t / (1 + |t|^2) with a correctly rounded reciprocal
+__device__ __forceinline__ F3 boris_delta32(F3 v, F3 E, F3 B, float h) {
+    F3 t = h * B;
+    float sc = 2.0f * __frcp_rn(1.0f + dot(t, t));
+    F3 he = h * E;
+    F3 vm = v + he;
+    F3 vp = vm + cross(vm, t);
+    F3 d = cross(vp, sc * t);
+    return d + (2.0f * he);
+}
+
+// Multistep / Hyper Boris (multistep_boris.jl:65-142) in closed form,
+// fac = q2m*dt/(2n):
+//   dv = (c1 - 1) v + c2 v x t + c3 (v.t) t + c2 e + c3 e x t + c6 (e.t) t
+// with c1 - 1 = -2 s q^2 / A = -s c3 (because zr^2 + s q^2 = |1 + i tau|^(2n) = A),
+// so no coefficient is formed by cancellation.
+__device__ __forceinline__ F3 multistep_delta32(F3 v, F3 E, F3 B, float fac, int N, int n) {
+    F3 t_n = fac * B;
+    F3 e_n = fac * E;
+    float s = dot(t_n, t_n);
+    if (N != 2) {
+        float f_N, e_corr;
+        if (N == 4) {
+            f_N = 1.0f + s * (1.0f / 3.0f);
+            e_corr = -1.0f / 3.0f;
+        } else {
+            f_N = 1.0f + s * (1.0f / 3.0f) + 2.0f * s * s * (1.0f / 15.0f);
+            e_corr = -1.0f / 3.0f - 2.0f * s * (1.0f / 15.0f);
+        }
+        float edt = dot(e_n, t_n);
+        e_n = f_N * e_n + (e_corr * edt) * t_n;
+        t_n = f_N * t_n;
+        s = dot(t_n, t_n);
+    }
+    float zr = 1.0f, q = 0.0f, A = 1.0f, R = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        R = R + (float)(k + 1) * A + 2.0f * q * q + zr * q;
+        float nzr = zr - s * q;
+        q = zr + q;
+        zr = nzr;
+        A = A * (1.0f + s);
+    }
+    float invA = __frcp_rn(A);
+    float c2 = 2.0f * zr * q * invA;
+    float c3 = 2.0f * q * q * invA;
+    float c6 = 2.0f * R * invA;
+    float c1m1 = -s * c3;
+    float vdt = dot(v, t_n), edt = dot(e_n, t_n);
+    F3 vxt = cross(v, t_n), ext = cross(e_n, t_n);
+    return c1m1 * v + c2 * vxt + (c3 * vdt) * t_n + c2 * e_n + c3 * ext + (c6 * edt) * t_n;
+}
+
+// the float factor of a velocity update of length dt: q2m*dt/2 (Boris) or
+// q2m*dt/(2n) (Multistep), rounded once from float64
+template <bool MULTI>
+__device__ __forceinline__ float vfac(const BorisArgs& a, double dt) {
+    return MULTI ? (float)(a.q2m * dt / (double)(2 * a.nsub)) : (float)(a.q2m * 0.5 * dt);
+}
+
+// v advanced by one velocity update with factor h (see vfac) and fields (E, B)
+template <bool MULTI>
+__device__ __forceinline__ CV vel32h(CV v, F3 E, F3 B, const BorisArgs& a, float h) {
+    F3 d = MULTI ? multistep_delta32(v.h, E, B, h, a.order, a.nsub) : boris_delta32(v.h, E, B, h);
+    cv_add(v, d);
+    return v;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ CV vel32(CV v, F3 E, F3 B, const BorisArgs& a, double dt) {
+    return vel32h<MULTI>(v, E, B, a, vfac<MULTI>(a, dt));
+}
+
+// position push x += v dt with dt = dth + dtl (float pair)
+__device__ __forceinline__ void cpos_push_cv(const BorisArgs& a, CPos& p, const CV& v, float dth, float dtl) {
+    F3 d{fmaf(v.h.x, dth, fmaf(v.h.x, dtl, v.l.x * dth)), fmaf(v.h.y, dth, fmaf(v.h.y, dtl, v.l.y * dth)),
+         fmaf(v.h.z, dth, fmaf(v.h.z, dtl, v.l.z * dth))};
+    cpos_push(a, p, d, 1.0f);
+}
+
+}  // namespace
+
+}  // namespace tpb

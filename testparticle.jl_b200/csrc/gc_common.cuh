@@ -315,6 +315,32 @@ __global__ void __launch_bounds__(256) k_rk4(GCArgs a) {
     }
 }
 
+// x^0.2 rounded to nearest: the step-size factor (1.0 / error_ratio)^0.2 of
+// rk45_gc.jl:151.  CUDA's pow is accurate to 2 ulp, and a one-ulp change of
+// the factor moves every later step, so the factor is refined to the
+// correctly rounded value, which is also what the oracle computes: one
+// Newton step for the real fifth root from z0 = pow(x, 0.2), with the
+// residual z0^5 - x in double-double arithmetic (Dekker's exact product by
+// fma; z0^5 - x is exact by Sterbenz's lemma), then the exponent correction
+// x^(0.2 - 1/5) = 1 + d ln x for the float64 constant 0.2 = 1/5 + d,
+// d = 2^-54 / 5.  Explicit _rn operations keep the sequence free of
+// contraction in every translation unit.  Outside [1e-30, 1e30], where the
+// controller clamps the factor anyway, z0 is returned.
+__device__ __forceinline__ double pow02_rn(double x) {
+    double z0 = pow(x, 0.2);
+    if (!(x >= 1.0e-30 && x <= 1.0e30) || !(z0 > 0.0) || isinf(z0)) return z0;
+    double a = __dmul_rn(z0, z0);
+    double ae = fma(z0, z0, -a);
+    double b = __dmul_rn(a, a);
+    double be = __dadd_rn(fma(a, a, -b), __dmul_rn(__dmul_rn(2.0, a), ae));
+    double c = __dmul_rn(b, z0);
+    double ce = __dadd_rn(fma(b, z0, -c), __dmul_rn(be, z0));
+    double r = __dadd_rn(__dsub_rn(c, x), ce);
+    double corr = __ddiv_rn(-r, __dmul_rn(5.0, b));
+    double t = __dmul_rn(0.2 * 0x1p-54, log(x));
+    return __dadd_rn(z0, __dadd_rn(corr, __dmul_rn(z0, t)));
+}
+
 // update_dp5, src/gc/rk45_gc.jl:7-47 (tableau of rk45_gc.jl:9-20)
 template <class RHS>
 __device__ __forceinline__ void update_dp5(const RHS& f, const DevFields& F, const G4& y,
@@ -440,7 +466,7 @@ __global__ void __launch_bounds__(256) k_rk45(GCArgs a) {
                 }
             }
             if (!stop) {
-                double scale = (error_ratio == 0.0) ? max_growth : safety * pow(1.0 / error_ratio, 0.2);
+                double scale = (error_ratio == 0.0) ? max_growth : safety * pow02_rn(1.0 / error_ratio);
                 scale = (max_growth < scale) ? max_growth : scale;
                 scale = (min_growth < scale) ? scale : min_growth;
                 dt *= scale;
