@@ -278,6 +278,79 @@ def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
     return out
 
 
+def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, reps=3):
+    """Discrete adjoint of Boris in the gridded field (config 5): forward with
+    checkpoints, backward (recompute + reverse + node scatter), and the plain
+    FP32C push of the same workload, each timed on the device."""
+    w = tp.workloads.config5(n=n, nt=nt)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    # targets: the float64 endpoints (library FP64 path) plus seeded offsets
+    sol64 = tp.solve(prob, tp.Boris(), tp.EnsembleB200(device=ctx.device, precision="fp64"), dt=w.dt,
+                     savestepinterval=10 ** 9, save_start=False)
+    x_target = torch.from_numpy(sol64.final_states()[:, :3] + w.extra["target_offset"]).to(dev)
+    del sol64
+    plan = tp.plan_adjoint(prob, tp.EnsembleB200(device=ctx.device, precision="fp32c"), dt=w.dt,
+                           checkpoint_every=K)
+    u0 = torch.from_numpy(plan.u0).to(dev)
+    uf = torch.empty_like(u0)
+    s = stream.cuda_stream
+    tape = ctx.adjoint_forward_device(plan.desc, plan.E, plan.B, u0.data_ptr(), n, uf.data_ptr(), s)
+    nodes = int(np.prod(w.B.data.shape[1:]))
+    gE = torch.empty(3 * nodes, dtype=torch.float32, device=dev)
+    gB = torch.empty_like(gE)
+    gp = torch.empty(6, dtype=torch.float64, device=dev)
+    gu = torch.empty_like(u0)
+
+    def grad_final():
+        g = torch.zeros_like(uf)
+        g[:, :3] = 2.0 * (uf[:, :3] - x_target) / n
+        return g
+
+    def fwd():
+        tape.rerun_device(u0.data_ptr(), uf.data_ptr(), s)
+
+    def bwd(g):
+        tape.backward_device(g.data_ptr(), gu.data_ptr(), gE.data_ptr(), gB.data_ptr(), gp.data_ptr(), s)
+
+    def device_ms(fn, *args):
+        fn(*args)  # warm-up (first backward allocates the records and tables)
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn(*args)
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+
+    torch.cuda.synchronize()
+    ms_f = device_ms(fwd)
+    g = grad_final()
+    loss = float(((uf[:, :3] - x_target) ** 2).sum().item() / n)
+    ms_b = device_ms(bwd, g)
+    # the plain FP32C push of the same workload (no checkpoints, final save only)
+    pp = tp.plan_boris(prob, tp.Boris(), tp.EnsembleB200(device=ctx.device, precision="fp32c"), dt=w.dt,
+                       savestepinterval=10 ** 9, save_start=False)
+    run = DeviceRun(tp, torch, ctx, pp, dev, stream)
+    ms_p = device_ms(run.launch, pp)
+    run.check()
+    ps = float(n) * nt
+    gnorm = float(torch.linalg.vector_norm(gu[:, :3]).item())
+    dLdB0 = 4.0e5 * float(gp[1].item()) + float(gp[5].item())
+    bytes_, _ = tape.info()
+    tape.close()
+    return {"workload": w.name, "particles": n, "time_steps": nt, "checkpoint_every": K,
+            "forward_ms": ms_f, "backward_ms": ms_b, "plain_fp32c_push_ms": ms_p,
+            "forward": {"value": ps / (ms_f * 1e-3), "unit": "particle-steps/s"},
+            "backward": {"value": ps / (ms_b * 1e-3), "unit": "particle-steps/s"},
+            "adjoint_over_forward": ms_b / ms_f, "adjoint_over_plain_push": ms_b / ms_p,
+            "tape_device_bytes": bytes_, "loss": loss, "grad_x0_norm": gnorm, "dL_dB0": dLdB0}
+
+
 def leg_gc(tp, n):
     """Guiding centres in the dipole (config 4): RK4 over 5 bounce periods, RK45, FP64 vs float32 RHS."""
     w = tp.workloads.config4(n)
@@ -319,6 +392,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-legs", action="store_true", help="skip the dipole / guiding-centre legs")
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
+    ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (profiling)")
+    ap.add_argument("--adj-n", type=int, default=1 << 18)
+    ap.add_argument("--adj-nt", type=int, default=4096)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -333,6 +409,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     tp = ge.load_package()
     ctx = tp.Context.get(local)
+    if args.adjoint_only:
+        dev = torch.device("cuda", local)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+        leg = leg_adjoint(tp, torch, ctx, dev, torch.cuda.current_stream(), flush, n=args.adj_n, nt=args.adj_nt)
+        if rank == 0:
+            print(json.dumps({"adjoint_only": leg}), flush=True)
+        return
     w = _workload(tp, args.workload, args.particles, args.nt)
     alg = _alg(tp, args.workload)
     dev = torch.device("cuda", local)
@@ -406,6 +489,7 @@ def main():
         legs["dipole_config3"] = leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, 1_000_000, args.nt)
         if rank == 0:
             legs["guiding_centre_config4"] = leg_gc(tp, 1 << 20)
+        legs["adjoint_config5"] = leg_adjoint(tp, torch, ctx, dev, stream, flush)
 
     if rank == 0:
         cpu = None

@@ -23,9 +23,9 @@
  *    (src/boris/boris.jl:349-356, src/types.jl:71-73); the others to
  *    ErrorException.  The text of the last error of a context is returned by
  *    tp_last_error().  No entry point aborts or traps.
- *  - Input pointers are borrowed for the duration of the call.  Grid data is
- *    copied to the device by tp_field_create().  Results are owned by a
- *    tp_result until tp_result_destroy().
+ *  - Input pointers are borrowed for the duration of the call.  Grid data
+ *    (host or device memory) is copied to the device by tp_field_create().
+ *    Results are owned by a tp_result until tp_result_destroy().
  *  - Calls on one context are synchronous and must come from one thread at a
  *    time.  Device entry points (suffix _device) are asynchronous on the
  *    stream they are given.
@@ -207,6 +207,12 @@ const char* tp_last_error(const tp_ctx* ctx);
  * is uploaded once.                                                         */
 int tp_field_create(tp_ctx* ctx, const tp_field_desc* desc, tp_field** out);
 void tp_field_destroy(tp_field* field);
+/* Replace the node values of a grid field in place (same geometry and dtype;
+ * `data` is host or device memory of the field's size).  The next solve sees
+ * the new values; tapes recorded before the update must not be reused.  An
+ * addition for optimisation loops over gridded fields (the reference rebuilds
+ * the interpolator).                                                        */
+int tp_field_update(tp_field* field, const void* data);
 
 /* ---- full-orbit solve (host buffers) --------------------------------------
  * Replaces _solve(::EnsembleAlg, ::TraceProblem, ::AbstractBoris, ...)
@@ -290,6 +296,60 @@ int tp_pack_results_device_noalloc(tp_ctx* ctx, const double* t_in,
                                    int64_t n, int64_t nslots, int32_t width,
                                    double* t_out, double* u_out,
                                    int64_t* total_out, void* stream);
+
+/* ---- discrete adjoint of the Boris map ------------------------------------
+ * No entry point of the reference: there, gradients of a trajectory come from
+ * ForwardDiff through the CPU solver.  The map differentiated is the
+ * fixed-step Boris solve of tp_boris_run (boris.jl:445-557) from the initial
+ * state to the final save:
+ *   v_{-1/2} = U(v_0, x_0, -dt/2);  for k = 0..N-1:
+ *   v_{k+1/2} = U(v_{k-1/2}, x_k, dt),  x_{k+1} = x_k + dt v_{k+1/2};
+ *   v_N = U(v_{N-1/2}, x_N, dt_final)                     (final save)
+ * with U the velocity update of boris.jl:19-45, N = round((t1 - t0)/dt), in
+ * the FP32C arithmetic of the push kernels, static fields, no termination.
+ * tp_adjoint_forward returns (x_N, v_N) and a tape holding the state every
+ * `checkpoint_every` steps; tp_adjoint_backward takes dL/d(x_N, v_N) and
+ * recomputes each segment from its checkpoint before running it backwards.
+ * Gradients:
+ *   grad_u0      dL/du0, N x 6 (float64)
+ *   grad_E/B     for grid fields: dL/d(node values), laid out like the
+ *                field's data (component fastest), float32; NULL to skip
+ *   grad_param   6 float64: for E then B, dL/dtheta with theta = the dipole
+ *                moment for a dipole field, else a uniform offset added to
+ *                the field (for a grid: the sum of the node gradients)
+ * The fields must outlive the tape and must not be updated in between.     */
+typedef struct tp_adj_desc {
+    tp_run_desc run;           /* alg TP_ALG_BORIS, precision TP_PREC_FP32C,
+                                  term.flags 0; t0, t1, dt, q2m, block     */
+    int64_t checkpoint_every;  /* K >= 1 steps per checkpoint segment     */
+} tp_adj_desc;
+
+typedef struct tp_tape tp_tape;
+
+/* host buffers: u0 and u_final N x 6 */
+int tp_adjoint_forward(tp_ctx* ctx, const tp_adj_desc* desc, const tp_field* E,
+                       const tp_field* B, const double* u0, int64_t n,
+                       double* u_final, tp_tape** tape);
+int tp_adjoint_backward(tp_tape* tape, const double* grad_final,
+                        double* grad_u0, float* grad_E, float* grad_B,
+                        double* grad_param);
+/* device buffers, asynchronous on `stream` (a cudaStream_t) */
+int tp_adjoint_forward_device(tp_ctx* ctx, const tp_adj_desc* desc,
+                              const tp_field* E, const tp_field* B,
+                              const double* u0, int64_t n, double* u_final,
+                              tp_tape** tape, void* stream);
+int tp_adjoint_backward_device(tp_tape* tape, const double* grad_final,
+                               double* grad_u0, float* grad_E, float* grad_B,
+                               double* grad_param, void* stream);
+/* Re-record an existing tape for new initial states (same N), reusing its
+ * device memory; fields updated with tp_field_update since are picked up.
+ * For optimisation loops: rerun, then backward, without reallocation.     */
+int tp_tape_rerun_device(tp_tape* tape, const double* u0, double* u_final,
+                         void* stream);
+/* device bytes a tape holds (checkpoints, and after the first backward pass
+ * the segment records and gradient tables), and its step count N */
+int tp_tape_info(const tp_tape* tape, int64_t* device_bytes, int64_t* nsteps);
+void tp_tape_destroy(tp_tape* tape);
 
 #ifdef __cplusplus
 }

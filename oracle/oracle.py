@@ -73,6 +73,9 @@ def lib() -> C.CDLL:
         L.orc_boris_counts.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64, C.c_int,
                                        C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.orc_max_threads.restype = C.c_int
+        L.orc_boris_jvp.restype = C.c_int
+        L.orc_boris_jvp.argtypes = [C.POINTER(from_abi.RunDesc), C.POINTER(from_abi.FieldDesc),
+                                    C.POINTER(from_abi.FieldDesc), P, P, P, P, P, C.c_int64, C.c_int, P, P]
         _lib = L
     return _lib
 
@@ -213,6 +216,41 @@ def boris_run(desc, E, B, u0: np.ndarray, dt_i=None, tend_i=None, nthreads: int 
         t, u = _pack(t_sm, u_sm, nsaved, W, n)
         return OracleResult(nsaved, rc, nst, t, u)
     raise RuntimeError("oracle: output sizing failed")
+
+
+def boris_jvp(desc, E, B, u0: np.ndarray, du0=None, dE_nodes=None, dB_nodes=None, dparam=None,
+              nthreads: int = 0):
+    """Final save (x_N, v_N) of the fixed-step Boris solve and its directional
+    derivative along (du0, node-value tangents of grid fields, parameter
+    tangents [E then B: dipole moment, else uniform offset]).  E/B are
+    package field objects (analytic kinds or grids).  Returns (uN, duN), N x 6.
+    """
+    L = lib()
+    u0 = np.ascontiguousarray(u0, dtype=np.float64)
+    n = u0.shape[0]
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    if Ecb is not None or Bcb is not None:
+        raise TypeError("boris_jvp needs package field objects, not callables")
+
+    def arr(a, shape=None):
+        if a is None:
+            return None
+        a = np.asarray(a, dtype=np.float64)
+        if a.ndim == 4:  # (3, nx, ny, nz) grid tangent: the field's column-major layout
+            a = np.asfortranarray(a).ravel(order="F")
+        return np.ascontiguousarray(a)
+
+    du0, dEn, dBn, dp = arr(du0), arr(dE_nodes), arr(dB_nodes), arr(dparam)
+    uN = np.empty((n, 6))
+    duN = np.empty((n, 6))
+    code = L.orc_boris_jvp(C.byref(desc), C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None, _ptr(u0),
+                           _ptr(du0), _ptr(dEn), _ptr(dBn), _ptr(dp), n, int(nthreads), _ptr(uN), _ptr(duN))
+    if code == -1:
+        raise ValueError("oracle: ArgumentError")
+    if code != 0:
+        raise RuntimeError(f"oracle status {code}")
+    return uN, duN
 
 
 def gc_run(desc, E, B, y0: np.ndarray, q_i=None, q2m_i=None, mu_i=None, nthreads: int = 0,

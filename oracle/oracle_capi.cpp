@@ -143,6 +143,133 @@ int orc_boris_counts(double t0, double t1, double dt, int64_t maxiters, int64_t 
     return TP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// ---- forward-mode tangent of the fixed-step Boris map -------------------
+// Stands in for ForwardDiff through the reference solver (Julia is absent):
+// the primal is the oracle's own Boris update in the reference's order, and
+// the tangent follows it operation by operation.
+
+// Field tangent at r along a direction: J(r) rdot plus the direction field
+// (node-value and parameter perturbations) at r.
+V3d field_tangent(const Field& f, const Field* dgrid, const Field* dpar, V3d r, V3d rdot, double t) {
+    V3d F;
+    M3 J;
+    f.jac(r, t, F, J);
+    V3d o{(J(0, 0) * rdot.x + J(0, 1) * rdot.y) + J(0, 2) * rdot.z,
+          (J(1, 0) * rdot.x + J(1, 1) * rdot.y) + J(1, 2) * rdot.z,
+          (J(2, 0) * rdot.x + J(2, 1) * rdot.y) + J(2, 2) * rdot.z};
+    if (dgrid) o = o + dgrid->eval(r, t);
+    if (dpar) o = o + dpar->eval(r, t);
+    return o;
+}
+
+// boris_velocity_update (boris.jl:19-31) and its derivative:
+//   t = hB, s = 2t/(1+|t|^2), vm = v + hE, vp = vm + vm x t,
+//   v+ = vm + vp x s, v_new = v+ + hE
+void boris_update_tangent(V3d v, V3d vd, V3d E, V3d Ed, V3d B, V3d Bd, double h, V3d& vn, V3d& vnd) {
+    vn = boris_velocity_update(v, E, B, h);
+    V3d t = h * B, td = h * Bd;
+    double den = 1.0 + abs2sum(t);
+    double dden = 2.0 * dot(t, td);
+    V3d s = (2.0 * t) / den;
+    V3d sd = (2.0 / den) * td - ((2.0 * dden) / (den * den)) * t;
+    V3d vm = v + h * E, vmd = vd + h * Ed;
+    V3d vp = vm + cross(vm, t);
+    V3d vpd = (vmd + cross(vmd, t)) + cross(vm, td);
+    V3d vplusd = (vmd + cross(vpd, s)) + cross(vp, sd);
+    vnd = vplusd + h * Ed;
+}
+
+// The direction field of a parameter perturbation: the dipole's moment, or
+// a uniform offset for every other kind.
+std::unique_ptr<Field> param_direction(const tp_field_desc* d, const double* dp) {
+    if (!dp || (dp[0] == 0.0 && dp[1] == 0.0 && dp[2] == 0.0)) return nullptr;
+    if (d && d->kind == TP_FIELD_DIPOLE) {
+        auto* f = new DipoleField();
+        f->m = {dp[0], dp[1], dp[2]};
+        f->c = {d->center[0], d->center[1], d->center[2]};
+        f->coef = d->coef;
+        return std::unique_ptr<Field>(f);
+    }
+    return std::unique_ptr<Field>(new UniformField({dp[0], dp[1], dp[2]}));
+}
+
+// The direction field of node-value perturbations of a grid field.
+std::unique_ptr<Field> grid_direction(const tp_field_desc* d, const double* nodes) {
+    if (!nodes || !d || d->kind != TP_FIELD_GRID) return nullptr;
+    tp_field_desc g = *d;
+    g.dtype = TP_DTYPE_F64;
+    g.data = nodes;
+    return make_field(&g, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Final save (x_N, v_N) of the fixed-step Boris solve of orc_boris_run
+// (boris.jl:445-557 with save_end, no termination, static fields) and its
+// directional derivative along (du0, dE_nodes, dB_nodes, dparam):
+//   du0       N x 6 tangent of the initial states (NULL = 0)
+//   dE_nodes, dB_nodes  tangents of a grid field's node values, float64 in
+//             the field's data layout (NULL = 0)
+//   dparam    6: tangent of (E, B) parameters -- the dipole moment for a
+//             dipole, else a uniform offset (NULL = 0)
+// uN, duN: N x 6.
+int orc_boris_jvp(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_desc* Bd,
+                  const double* u0, const double* du0, const double* dE_nodes, const double* dB_nodes,
+                  const double* dparam, int64_t n, int nthreads, double* uN, double* duN) {
+    std::unique_ptr<Field> E = make_field(Ed, nullptr), B = make_field(Bd, nullptr);
+    if (!E || !B) return TP_E_ARG;
+    if (d->alg != TP_ALG_BORIS) return TP_E_UNSUPPORTED;
+    int64_t nt, nout;
+    int st = orc_boris_counts(d->t0, d->t1, d->dt, d->maxiters, 1, 0, 1, 0, &nt, &nout);
+    if (st != TP_OK) return st;
+    std::unique_ptr<Field> gE = grid_direction(Ed, dE_nodes), gB = grid_direction(Bd, dB_nodes);
+    std::unique_ptr<Field> pE = param_direction(Ed, dparam), pB = param_direction(Bd, dparam ? dparam + 3 : nullptr);
+    const double dt = d->dt, t0 = d->t0, h_loop = d->q2m * 0.5 * dt;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int64_t i = 0; i < n; ++i) {
+        const double* ui = u0 + 6 * i;
+        V3d r{ui[0], ui[1], ui[2]}, v{ui[3], ui[4], ui[5]};
+        V3d rd{0, 0, 0}, vd{0, 0, 0};
+        if (du0) {
+            const double* q = du0 + 6 * i;
+            rd = {q[0], q[1], q[2]};
+            vd = {q[3], q[4], q[5]};
+        }
+        auto update = [&](double h, double t) {
+            V3d Ev = E->eval(r, t), Bv = B->eval(r, t);
+            V3d Et = field_tangent(*E, gE.get(), pE.get(), r, rd, t);
+            V3d Bt = field_tangent(*B, gB.get(), pB.get(), r, rd, t);
+            V3d vn, vnd;
+            boris_update_tangent(v, vd, Ev, Et, Bv, Bt, h, vn, vnd);
+            v = vn;
+            vd = vnd;
+        };
+        update(d->q2m * 0.5 * (-0.5 * dt), t0);  // v_{-1/2}
+        double t = t0 - 0.5 * dt;
+        for (int64_t it = 1; it <= nt; ++it) {
+            t += dt;
+            update(h_loop, t);
+            r = r + v * dt;
+            rd = rd + vd * dt;
+        }
+        double t_final = d->t1;
+        double dt_final = t_final - std::fma((double)nt - 0.5, dt, t0);
+        update(d->q2m * 0.5 * dt_final, t_final);
+        double* o = uN + 6 * i;
+        double* od = duN + 6 * i;
+        o[0] = r.x; o[1] = r.y; o[2] = r.z; o[3] = v.x; o[4] = v.y; o[5] = v.z;
+        od[0] = rd.x; od[1] = rd.y; od[2] = rd.z; od[3] = vd.x; od[4] = vd.y; od[5] = vd.z;
+    }
+    return TP_OK;
+}
+
 // Full-orbit ensemble (Boris, MultistepBoris, AdaptiveBoris, AdaptiveMultistepBoris).
 int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_desc* Bd,
                   const orc_field_cb* Ecb, const orc_field_cb* Bcb, const orc_term_cb* tcb,

@@ -18,9 +18,10 @@ from .problems import (AdaptiveBoris, AdaptiveMultistepBoris, Boris, EnsembleB20
                        MultistepBoris, MultistepBoris2, MultistepBoris4, MultistepBoris6, Terminate,
                        TerminateBox, TerminateNaN, TerminateShell, TerminateTime, TraceGCProblem,
                        TraceProblem, prepare, remake)
-from .runtime import ArgumentError, Context, DeviceError
+from .runtime import AdjointGrads, ArgumentError, Context, DeviceError, Tape
 from .solution import EnsembleSolution, TraceSolution
-from .solve import BorisPlan, GCPlan, plan_boris, plan_gc, prepare_gc, solve
+from .solve import (AdjointPlan, BorisPlan, GCPlan, adjoint_solve, plan_adjoint, plan_boris, plan_gc,
+                    prepare_gc, solve)
 from .utility import energy2velocity, get_gyrofrequency, get_gyroperiod, get_gyroradius, get_perp_vector, sph2cart
 
 __version__ = "0.1.0"

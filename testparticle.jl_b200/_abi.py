@@ -151,6 +151,13 @@ class GCDesc(C.Structure):
     ]
 
 
+class AdjDesc(C.Structure):
+    _fields_ = [
+        ("run", RunDesc),
+        ("checkpoint_every", C.c_int64),
+    ]
+
+
 _P = C.c_void_p
 _DP = C.POINTER(C.c_double)
 
@@ -174,6 +181,15 @@ SIGNATURES = [
     ("tp_result_destroy", None, [_P]),
     ("tp_pack_results_device_noalloc", C.c_int,
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    ("tp_field_update", C.c_int, [_P, _P]),
+    ("tp_adjoint_forward", C.c_int, [_P, C.POINTER(AdjDesc), _P, _P, _P, C.c_int64, _P, C.POINTER(_P)]),
+    ("tp_adjoint_backward", C.c_int, [_P, _P, _P, _P, _P, _P]),
+    ("tp_adjoint_forward_device", C.c_int,
+     [_P, C.POINTER(AdjDesc), _P, _P, _P, C.c_int64, _P, C.POINTER(_P), _P]),
+    ("tp_adjoint_backward_device", C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    ("tp_tape_rerun_device", C.c_int, [_P, _P, _P, _P]),
+    ("tp_tape_info", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("tp_tape_destroy", None, [_P]),
 ]
 
 # static scratch limit of tp_pack_results_device_noalloc (include/tp_abi.h)

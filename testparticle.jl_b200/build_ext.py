@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
 NO_FMAD = {"boris_fp64.cu", "gc_fp64.cu"}
-SOURCES = ["runtime.cu", "pack.cu", "boris_fp64.cu", "boris_fp32c.cu", "gc_fp64.cu", "gc_fp32.cu",
+SOURCES = ["runtime.cu", "pack.cu", "boris_fp64.cu", "boris_fp32c.cu", "gc_fp64.cu", "gc_fp32.cu", "adjoint.cu",
            "noalloc.cu"]
 
 

@@ -1,0 +1,562 @@
+// adjoint.cu -- discrete adjoint of the fixed-step Boris map, in the FP32C
+// arithmetic of boris_fp32c.cu (compensated positions and velocities).
+//
+// The map (boris.jl:445-557 without saves or termination):
+//   v_{-1/2} = U(v_0, x_0, -dt/2);  for k = 0..N-1:
+//   v_{k+1/2} = U(v_{k-1/2}, x_k, dt),  x_{k+1} = x_k + dt v_{k+1/2};
+//   v_N = U(v_{N-1/2}, x_N, dt_final)
+// with U the Boris velocity update (boris.jl:19-45), in delta form
+//   U(v) = v + 2hE + vp x s,  vm = v + hE,  vp = vm + vm x t,  t = hB,
+//   s = sc t,  sc = 2 / (1 + |t|^2),  h = q2m * dt_u / 2.
+//
+// Forward (k_adj_forward): the push of k_fixed32c, writing the compensated
+// state every K steps to the tape and the final save to u_final.
+//
+// Backward (k_adj_backward): one thread per particle walks the checkpoint
+// segments from last to first.  Each segment is recomputed from its
+// checkpoint with the forward's own arithmetic (so the recomputed states are
+// the forward's bit for bit), each step's input state going to a record
+// buffer, and then the records are run backwards through the adjoint of one
+// step: with lo the cotangent of v_{k+1/2} including the position update
+// (lo = lv + dt lx), the adjoint of U is (c = a x b gives la += b x lc,
+// lb += lc x a)
+//   ls = lo x vp,  lvp = s x lo,  lvm = lvp + t x lvp,
+//   lt = lvp x vm + sc ls - sc^2 (t . ls) t,
+//   lv_in = lo + lvm,  lE = h (2 lo + lvm),  lB = h lt.
+// E and B depend on x and on the node values through the trilinear weights
+// w_c(x): node c receives w_c lE and w_c lB (red.global.add.v4.f32 into a
+// gradient table laid out like the field table), and
+// lx += sum_c grad w_c(x) (E_c . lE + B_c . lB).
+// Analytic fields contribute J^T l to lx (J the field's Jacobian) and their
+// parameter gradient (uniform offset, or dipole moment) to g_param.
+#include "fp32c_common.cuh"
+#include "tp_device.cuh"
+#include "tp_launch.h"
+
+namespace tpb {
+
+namespace {
+
+constexpr int kCk = 15;   // checkpoint words per particle
+constexpr int kRec = 9;   // record words per particle-step
+
+__device__ __forceinline__ F3 nanf3_() { return nanf3(); }
+
+__device__ __forceinline__ void store_ck(const AdjArgs& A, int64_t s, int64_t i, const CPos& p, const CV& v) {
+    const int64_t n = A.a.n;
+    float* c = A.ckpt + s * kCk * n + i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        c[(0 + k) * n] = p.hi[k];
+        c[(3 + k) * n] = p.lo[k];
+        c[(6 + k) * n] = __int_as_float(p.w[k]);
+    }
+    c[9 * n] = v.h.x;
+    c[10 * n] = v.h.y;
+    c[11 * n] = v.h.z;
+    c[12 * n] = v.l.x;
+    c[13 * n] = v.l.y;
+    c[14 * n] = v.l.z;
+}
+
+__device__ __forceinline__ void load_ck(const AdjArgs& A, int64_t s, int64_t i, CPos& p, CV& v) {
+    const int64_t n = A.a.n;
+    const float* c = A.ckpt + s * kCk * n + i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p.hi[k] = c[(0 + k) * n];
+        p.lo[k] = c[(3 + k) * n];
+        p.w[k] = __float_as_int(c[(6 + k) * n]);
+    }
+    v.h = {c[9 * n], c[10 * n], c[11 * n]};
+    v.l = {c[12 * n], c[13 * n], c[14 * n]};
+}
+
+__device__ __forceinline__ void store_rec(const AdjArgs& A, int j, int64_t i, const CPos& p, F3 v) {
+    const int64_t n = A.a.n;
+    float* r = A.rec + (int64_t)j * kRec * n + i;
+    r[0] = p.hi[0];
+    r[n] = p.hi[1];
+    r[2 * n] = p.hi[2];
+    r[3 * n] = p.lo[0];
+    r[4 * n] = p.lo[1];
+    r[5 * n] = p.lo[2];
+    r[6 * n] = v.x;
+    r[7 * n] = v.y;
+    r[8 * n] = v.z;
+}
+
+// the wrap counts are not needed to evaluate a field (wrapped axes are
+// periodic in every field), so records leave them out
+__device__ __forceinline__ void load_rec(const AdjArgs& A, int j, int64_t i, CPos& p, F3& v) {
+    const int64_t n = A.a.n;
+    const float* r = A.rec + (int64_t)j * kRec * n + i;
+    p.hi[0] = r[0];
+    p.hi[1] = r[n];
+    p.hi[2] = r[2 * n];
+    p.lo[0] = r[3 * n];
+    p.lo[1] = r[4 * n];
+    p.lo[2] = r[5 * n];
+    p.w[0] = p.w[1] = p.w[2] = 0;
+    v = {r[6 * n], r[7 * n], r[8 * n]};
+}
+
+// ------------------------------------------------------------ adjoint of U
+struct UAdj {
+    F3 lv, lE, lB;
+};
+
+__device__ __forceinline__ UAdj u_adjoint(F3 v, F3 E, F3 B, float h, F3 lo) {
+    F3 t = h * B;
+    float sc = 2.0f * __frcp_rn(1.0f + dot(t, t));
+    F3 he = h * E;
+    F3 vm = v + he;
+    F3 vp = vm + cross(vm, t);
+    F3 s = sc * t;
+    F3 ls = cross(lo, vp);
+    F3 lvp = cross(s, lo);
+    F3 lvm = lvp + cross(t, lvp);
+    F3 lt = cross(lvp, vm) + sc * ls - (sc * sc * dot(t, ls)) * t;
+    UAdj r;
+    r.lv = lo + lvm;
+    r.lE = h * ((2.0f * lo) + lvm);
+    r.lB = h * lt;
+    return r;
+}
+
+// ------------------------------------------------------- trilinear stencil
+// corners in the order 000, 100, 010, 110, 001, 101, 011, 111 (x fastest)
+__device__ __forceinline__ void tri_nodes(const DevField& g, const AxF& ax, const AxF& ay, const AxF& az,
+                                          int* nd) {
+    const int nx = g.n[0], nxy = g.n[0] * g.n[1];
+    const int j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+    nd[0] = ax.i0 + j0 + k0;
+    nd[1] = ax.i1 + j0 + k0;
+    nd[2] = ax.i0 + j1 + k0;
+    nd[3] = ax.i1 + j1 + k0;
+    nd[4] = ax.i0 + j0 + k1;
+    nd[5] = ax.i1 + j0 + k1;
+    nd[6] = ax.i0 + j1 + k1;
+    nd[7] = ax.i1 + j1 + k1;
+}
+
+__device__ __forceinline__ void tri_weights(const AxF& ax, const AxF& ay, const AxF& az, float* w) {
+    const float x0 = 1.0f - ax.f, x1 = ax.f, y0 = 1.0f - ay.f, y1 = ay.f, z0 = 1.0f - az.f, z1 = az.f;
+    const float a00 = y0 * z0, a10 = y1 * z0, a01 = y0 * z1, a11 = y1 * z1;
+    w[0] = x0 * a00;
+    w[1] = x1 * a00;
+    w[2] = x0 * a10;
+    w[3] = x1 * a10;
+    w[4] = x0 * a01;
+    w[5] = x1 * a01;
+    w[6] = x0 * a11;
+    w[7] = x1 * a11;
+}
+
+// gradient in x of sum_c w_c(x) g_c
+__device__ __forceinline__ F3 tri_grad(const float* g, const AxF& ax, const AxF& ay, const AxF& az) {
+    const float fx = ax.f, fy = ay.f, fz = az.f;
+    float dx = lerp32(lerp32(g[1] - g[0], g[3] - g[2], fy), lerp32(g[5] - g[4], g[7] - g[6], fy), fz);
+    float dy = lerp32(lerp32(g[2] - g[0], g[3] - g[1], fx), lerp32(g[6] - g[4], g[7] - g[5], fx), fz);
+    float dz = lerp32(lerp32(g[4] - g[0], g[5] - g[1], fx), lerp32(g[6] - g[2], g[7] - g[3], fx), fy);
+    return {dx * ax.ds, dy * ay.ds, dz * az.ds};
+}
+
+__device__ __forceinline__ void red_add3(float4* p, float a, float b, float c) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(0.0f)
+                 : "memory");
+}
+
+// Scatter w_c * la (and w_c * lb when NV == 2) to the 8 corner nodes of a
+// gradient table with NV float4 entries per node.  Warp aggregation: lanes
+// whose particles sit in the same cell update the same 8 nodes, so
+//  * when no two lanes share a cell (the usual case) every lane adds its own;
+//  * when the whole warp shares one cell, a butterfly sum leaves one
+//    red.global.add per node and vector;
+//  * for groups of 4 or more lanes the group's lowest lane pulls the others'
+//    contributions by shuffles and adds the group sum;
+//  * small groups add individually (the adds are atomic either way).
+template <int NV>
+__device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w, F3 la, F3 lb) {
+    const unsigned act = __activemask();
+    const unsigned me = 1u << (threadIdx.x & 31);
+    const unsigned peers = __match_any_sync(act, nd[0]);
+    const int gsize = __popc(peers);
+    const int gmax = __reduce_max_sync(act, (unsigned)gsize);
+    if (gmax == 1) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            red_add3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
+            if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
+        }
+        return;
+    }
+    if (act == 0xffffffffu && gsize == 32) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float q[6] = {w[c] * la.x, w[c] * la.y, w[c] * la.z, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z};
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int k = 0; k < 3 * NV; ++k) q[k] += __shfl_xor_sync(0xffffffffu, q[k], o);
+            if (me == 1u) {
+                red_add3(G + (int64_t)NV * nd[c], q[0], q[1], q[2]);
+                if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, q[3], q[4], q[5]);
+            }
+        }
+        return;
+    }
+    if (gmax >= 4) {
+        const bool leader = (peers & (0u - peers)) == me;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float q[6] = {w[c] * la.x, w[c] * la.y, w[c] * la.z, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z};
+            float acc[6] = {q[0], q[1], q[2], q[3], q[4], q[5]};
+            unsigned rest = peers & (peers - 1u);  // the group without its lowest lane
+            for (int r = 1; r < gmax; ++r) {
+                const bool have = rest != 0u;
+                const int src = have ? __ffs(rest) - 1 : (int)(threadIdx.x & 31);
+                rest &= rest - 1u;
+#pragma unroll
+                for (int k = 0; k < 3 * NV; ++k) {
+                    float x = __shfl_sync(act, q[k], src);
+                    if (have) acc[k] += x;
+                }
+            }
+            if (leader) {
+                red_add3(G + (int64_t)NV * nd[c], acc[0], acc[1], acc[2]);
+                if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, acc[3], acc[4], acc[5]);
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        red_add3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
+        if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
+    }
+}
+
+// --------------------------------------------- one step, interleaved E/B grid
+// Returns the cotangent of the update's input velocity; adds the position
+// cotangent to lx and scatters the node gradients.
+__device__ __forceinline__ F3 adj_step_eb(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx) {
+    const DevFields& F = A.a.f;
+    AxF ax, ay, az;
+    if (!axes32(F.B, p, ax, ay, az)) {  // outside a FillExtrap(NaN) grid: NaN, as the forward
+        lx = nanf3_();
+        return nanf3_();
+    }
+    int nd[8];
+    tri_nodes(F.B, ax, ay, az, nd);
+    const float4* T = F.eb32;
+    float4 e[8], b[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ldg_node8(T + 2 * (int64_t)nd[c], e[c], b[c]);
+    F3 E = tri3(xyz(e[0]), xyz(e[1]), xyz(e[2]), xyz(e[3]), xyz(e[4]), xyz(e[5]), xyz(e[6]), xyz(e[7]), ax, ay,
+                az);
+    F3 B = tri3(xyz(b[0]), xyz(b[1]), xyz(b[2]), xyz(b[3]), xyz(b[4]), xyz(b[5]), xyz(b[6]), xyz(b[7]), ax, ay,
+                az);
+    UAdj u = u_adjoint(v, E, B, h, lo);
+    float g[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) g[c] = dot(xyz(e[c]), u.lE) + dot(xyz(b[c]), u.lB);
+    lx = lx + tri_grad(g, ax, ay, az);
+    float w[8];
+    tri_weights(ax, ay, az, w);
+    scatter<2>(A.g_eb, nd, w, u.lE, u.lB);
+    return u.lv;
+}
+
+// ------------------------------------------------ one step, generic fields
+struct GridKeep {
+    AxF ax, ay, az;
+    int nd[8];
+    float4 c[8];
+    bool ok;
+};
+
+// the arithmetic of grid_eval32, keeping the stencil
+__device__ __forceinline__ F3 grid_eval_keep(const DevField& g, const CPos& p, GridKeep& k) {
+    k.ok = axes32(g, p, k.ax, k.ay, k.az);
+    if (!k.ok) return nanf3_();
+    tri_nodes(g, k.ax, k.ay, k.az, k.nd);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) k.c[c] = __ldg(g.tab32 + k.nd[c]);
+    return tri3(xyz(k.c[0]), xyz(k.c[1]), xyz(k.c[2]), xyz(k.c[3]), xyz(k.c[4]), xyz(k.c[5]), xyz(k.c[6]),
+                xyz(k.c[7]), k.ax, k.ay, k.az);
+}
+
+// field f evaluated to lam's cotangent: lx += J^T lam, parameter gradient
+// to th (analytic kinds), node gradients to G (grids)
+__device__ __forceinline__ void field_adj(const DevField& f, const CPos& p, const GridKeep& k, F3 lam, float4* G,
+                                          F3& lx, double* th) {
+    switch (f.kind) {
+        case TP_FIELD_GRID: {
+            if (!k.ok) {
+                lx = nanf3_();
+                return;
+            }
+            float g[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) g[c] = dot(xyz(k.c[c]), lam);
+            lx = lx + tri_grad(g, k.ax, k.ay, k.az);
+            float w[8];
+            tri_weights(k.ax, k.ay, k.az, w);
+            scatter<1>(G, k.nd, w, lam, lam);
+            return;
+        }
+        case TP_FIELD_AFFINE: {
+            // F = v + J x (static): d/dx = J, d/d(offset) = I
+            const float* J = f.Jf;
+            lx = lx + F3{J[0] * lam.x + J[3] * lam.y + J[6] * lam.z, J[1] * lam.x + J[4] * lam.y + J[7] * lam.z,
+                         J[2] * lam.x + J[5] * lam.y + J[8] * lam.z};
+            th[0] += lam.x;
+            th[1] += lam.y;
+            th[2] += lam.z;
+            return;
+        }
+        case TP_FIELD_DIPOLE: {
+            // B = K/r^3 (3 (mh.rh) rh - mh), K = coef |m|; the Jacobian is
+            // symmetric: J^T l = K/r^4 (3 mh (rh.l) + 3 (mh.rh) l
+            //                   + 3 (mh.l) rh - 15 (mh.rh)(rh.l) rh)
+            // and dB/dm = coef/r^3 (3 rh rh^T - I)
+            F3 d{(p.hi[0] - f.cf[0]) + p.lo[0], (p.hi[1] - f.cf[1]) + p.lo[1], (p.hi[2] - f.cf[2]) + p.lo[2]};
+            F3 mh{f.mhatf[0], f.mhatf[1], f.mhatf[2]};
+            float ir = __frsqrt_rn(dot(d, d));
+            F3 rh = ir * d;
+            float mr = dot(mh, rh), rl = dot(rh, lam), ml = dot(mh, lam);
+            float k4 = (f.Kf * ir) * ir * ir * ir;
+            lx = lx + k4 * ((3.0f * rl) * mh + (3.0f * mr) * lam + (3.0f * ml - 15.0f * mr * rl) * rh);
+            double k3 = f.coef * (double)ir * (double)ir * (double)ir;
+            th[0] += k3 * (3.0 * (double)rl * (double)rh.x - (double)lam.x);
+            th[1] += k3 * (3.0 * (double)rl * (double)rh.y - (double)lam.y);
+            th[2] += k3 * (3.0 * (double)rl * (double)rh.z - (double)lam.z);
+            return;
+        }
+        default:  // zero / uniform: gradient of a uniform offset
+            th[0] += lam.x;
+            th[1] += lam.y;
+            th[2] += lam.z;
+            return;
+    }
+}
+
+template <int FK>
+__device__ __forceinline__ F3 adj_step_gen(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx,
+                                           double* thE, double* thB) {
+    const DevFields& F = A.a.f;
+    GridKeep kE, kB;
+    kE.ok = kB.ok = true;
+    F3 E = (FK == FK_GENERIC && F.E.kind == TP_FIELD_GRID) ? grid_eval_keep(F.E, p, kE)
+                                                            : analytic_eval32(F.E, p, A.a.t0);
+    F3 B = (FK == FK_GENERIC && F.B.kind == TP_FIELD_GRID) ? grid_eval_keep(F.B, p, kB)
+                                                            : analytic_eval32(F.B, p, A.a.t0);
+    UAdj u = u_adjoint(v, E, B, h, lo);
+    field_adj(F.E, p, kE, u.lE, A.g_E, lx, thE);
+    field_adj(F.B, p, kB, u.lB, A.g_B, lx, thB);
+    return u.lv;
+}
+
+template <int FK>
+__device__ __forceinline__ F3 adj_step(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx,
+                                       double* thE, double* thB) {
+    if (FK == FK_EBGRID) return adj_step_eb(A, p, v, h, lo, lx);
+    return adj_step_gen<FK>(A, p, v, h, lo, lx, thE, thB);
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ kernels
+template <int FK>
+__global__ void __launch_bounds__(256) k_adj_forward(AdjArgs A) {
+    const BorisArgs& a = A.a;
+    const double dt = a.dt;
+    const float dth = (float)dt, dtl = (float)(dt - (double)dth);
+    const float h = vfac<false>(a, dt);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double* u0 = a.u0 + 6 * i;
+        CPos p;
+        cpos_init(a, p, u0);
+        CV v = cv_from(u0 + 3);
+        F3 E, B;
+        eval_EB32t<FK>(a.f, p, a.t0, E, B);
+        v = vel32<false>(v, E, B, a, -0.5 * dt);
+        int64_t s = 0, left = 0;
+        for (int64_t k = 0; k < A.nt; ++k) {
+            if (left == 0) {
+                store_ck(A, s, i, p, v);
+                ++s;
+                left = A.K;
+            }
+            --left;
+            eval_EB32t<FK>(a.f, p, a.t0, E, B);
+            v = vel32h<false>(v, E, B, a, h);
+            cpos_push_cv(a, p, v, dth, dtl);
+        }
+        if (A.nt == 0) store_ck(A, 0, i, p, v);
+        eval_EB32t<FK>(a.f, p, a.t0, E, B);
+        CV vf = vel32<false>(v, E, B, a, A.dt_final);
+        double* uo = A.u_final + 6 * i;
+        uo[0] = cpos_value(a, p, 0);
+        uo[1] = cpos_value(a, p, 1);
+        uo[2] = cpos_value(a, p, 2);
+        uo[3] = (double)vf.h.x + (double)vf.l.x;
+        uo[4] = (double)vf.h.y + (double)vf.l.y;
+        uo[5] = (double)vf.h.z + (double)vf.l.z;
+    }
+}
+
+template <int FK>
+__global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
+    const BorisArgs& a = A.a;
+    const double dt = a.dt;
+    const float dtf = (float)dt;
+    const float dth = dtf, dtl = (float)(dt - (double)dth);
+    const float h = vfac<false>(a, dt);
+    const float h_fin = vfac<false>(a, A.dt_final);
+    const float h_ini = vfac<false>(a, -0.5 * dt);
+    double thE[3] = {0.0, 0.0, 0.0}, thB[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double* gf = A.g_final + 6 * i;
+        F3 lx{(float)gf[0], (float)gf[1], (float)gf[2]};
+        F3 lv{(float)gf[3], (float)gf[4], (float)gf[5]};
+        for (int64_t s = A.S - 1; s >= 0; --s) {
+            CPos p;
+            CV v;
+            load_ck(A, s, i, p, v);
+            const int64_t k0 = s * A.K;
+            const int m = (int)((A.nt - k0 < A.K) ? A.nt - k0 : A.K);
+            for (int j = 0; j < m; ++j) {
+                store_rec(A, j, i, p, v.h);
+                F3 E, B;
+                eval_EB32t<FK>(a.f, p, a.t0, E, B);
+                v = vel32h<false>(v, E, B, a, h);
+                cpos_push_cv(a, p, v, dth, dtl);
+            }
+            if (s == A.S - 1) lv = adj_step<FK>(A, p, v.h, h_fin, lv, lx, thE, thB);  // final save
+            for (int j = m - 1; j >= 0; --j) {
+                CPos q;
+                F3 vh;
+                load_rec(A, j, i, q, vh);
+                F3 lo = lv + dtf * lx;
+                lv = adj_step<FK>(A, q, vh, h, lo, lx, thE, thB);
+            }
+        }
+        // initial half step back
+        const double* u0 = a.u0 + 6 * i;
+        CPos p0;
+        cpos_init(a, p0, u0);
+        CV v0 = cv_from(u0 + 3);
+        lv = adj_step<FK>(A, p0, v0.h, h_ini, lv, lx, thE, thB);
+        double* go = A.g_u0 + 6 * i;
+        go[0] = lx.x;
+        go[1] = lx.y;
+        go[2] = lx.z;
+        go[3] = lv.x;
+        go[4] = lv.y;
+        go[5] = lv.z;
+    }
+    if (FK != FK_EBGRID) {
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            thE[k] = warp_sum(thE[k]);
+            thB[k] = warp_sum(thB[k]);
+            any = any || thE[k] != 0.0 || thB[k] != 0.0;
+        }
+        if ((threadIdx.x & 31) == 0 && any) {
+            for (int k = 0; k < 3; ++k) {
+                atomicAdd(A.g_param + k, thE[k]);
+                atomicAdd(A.g_param + 3 + k, thB[k]);
+            }
+        }
+    }
+}
+
+__global__ void k_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nodes;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        float4 q = tab[k * stride + off];
+        sx += q.x;
+        sy += q.y;
+        sz += q.z;
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    __shared__ double part[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        part[0][wid] = sx;
+        part[1][wid] = sy;
+        part[2][wid] = sz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += part[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, s);
+    }
+}
+
+__global__ void k_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nodes) return;
+    float4 q = tab[k * stride + off];
+    out[3 * k + 0] = q.x;
+    out[3 * k + 1] = q.y;
+    out[3 * k + 2] = q.z;
+}
+
+// ---------------------------------------------------------------- launchers
+int adjoint_field_config(const DevFields& f) {
+    if (f.eb32) return FK_EBGRID;
+    if (f.E.kind != TP_FIELD_GRID && f.B.kind != TP_FIELD_GRID) return FK_ANALYTIC;
+    return FK_GENERIC;
+}
+
+cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
+    const void* k = fk == FK_EBGRID    ? (const void*)k_adj_forward<FK_EBGRID>
+                    : fk == FK_ANALYTIC ? (const void*)k_adj_forward<FK_ANALYTIC>
+                                        : (const void*)k_adj_forward<FK_GENERIC>;
+    void* args[] = {const_cast<AdjArgs*>(&a)};
+    return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
+}
+
+cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
+    const void* k = fk == FK_EBGRID    ? (const void*)k_adj_backward<FK_EBGRID>
+                    : fk == FK_ANALYTIC ? (const void*)k_adj_backward<FK_ANALYTIC>
+                                        : (const void*)k_adj_backward<FK_GENERIC>;
+    void* args[] = {const_cast<AdjArgs*>(&a)};
+    return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
+}
+
+cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out,
+                             cudaStream_t s) {
+    if (nodes <= 0) return cudaSuccess;
+    const int block = 256;
+    int64_t g = (nodes + block - 1) / block;
+    if (g > 148 * 8) g = 148 * 8;
+    k_table_sum<<<(unsigned)g, block, 0, s>>>(tab, nodes, stride, off, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out,
+                                cudaStream_t s) {
+    if (nodes <= 0) return cudaSuccess;
+    const int block = 256;
+    k_table_unpack<<<(unsigned)((nodes + block - 1) / block), block, 0, s>>>(tab, nodes, stride, off, out);
+    return cudaGetLastError();
+}
+
+}  // namespace tpb

@@ -82,6 +82,7 @@ __device__ __forceinline__ void cpos_push(const BorisArgs& a, CPos& p, F3 v, flo
 struct AxF {
     int i0, i1;
     float f;
+    float ds;  // d f / d x: 1/dx, or 0 where the axis is clamped (adjoint only)
 };
 
 // cell index and fraction from the compensated coordinate
@@ -127,17 +128,21 @@ __device__ __forceinline__ bool axis32(const DevField& g, int a, float hi, float
         o.i0 = i;
         o.i1 = (i + 1 == na) ? 0 : i + 1;
         o.f = f;
+        o.ds = g.idxf[a];
         return true;
     }
     float uc = fl + f;
     float umax = (float)(na - 1);
+    o.ds = g.idxf[a];
     if (g.bc == TP_BC_CLAMP) {
         if (uc < 0.0f) {
             fl = 0.0f;
             f = 0.0f;
+            o.ds = 0.0f;
         } else if (uc > umax) {
             fl = umax;
             f = 0.0f;
+            o.ds = 0.0f;
         }
     } else if (!(uc >= 0.0f && uc <= umax)) {
         return false;

@@ -384,7 +384,7 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
             size_t esz = f64 ? sizeof(double) : sizeof(float);
             cudaError_t e = cudaMalloc(&f->d_raw, (size_t)nodes * 3 * esz);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(f->d_raw, d->data, (size_t)nodes * 3 * esz, cudaMemcpyHostToDevice,
+                e = cudaMemcpyAsync(f->d_raw, d->data, (size_t)nodes * 3 * esz, cudaMemcpyDefault,
                                     ctx->stream);
             if (e == cudaSuccess) e = cudaMalloc(&f->d_tab, (size_t)nodes * 4 * esz);
             if (e == cudaSuccess)
@@ -411,6 +411,29 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
     }
     fill_float_copies(dv);
     *out = f;
+    return TP_OK;
+}
+
+int tp_field_update(tp_field* f, const void* data) {
+    if (!f) return TP_E_ARG;
+    tp_ctx* ctx = f->ctx;
+    if (f->desc.kind != TP_FIELD_GRID) return fail(ctx, TP_E_ARG, "tp_field_update needs a grid field");
+    if (!data) return fail(ctx, TP_E_ARG, "grid data pointer is null");
+    DeviceGuard g(ctx->device);
+    bool f64 = f->desc.dtype == TP_DTYPE_F64;
+    size_t esz = f64 ? sizeof(double) : sizeof(float);
+    cudaError_t e = cudaMemcpyAsync(f->d_raw, data, (size_t)f->nodes * 3 * esz, cudaMemcpyDefault, ctx->stream);
+    if (e == cudaSuccess) e = launch_pack_node_table(f->d_raw, f64, f->nodes, f->d_tab, f64, 1, 0, ctx->stream);
+    if (e == cudaSuccess && f64)
+        e = launch_pack_node_table(f->d_raw, 1, f->nodes, f->d_tab32, 0, 1, 0, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid update");
+    // new identity: interleaved tables built with the old values are rebuilt
+    {
+        std::lock_guard<std::mutex> lk(g_id_mu);
+        f->id = g_next_id++;
+    }
+    f->eb_partner = 0;
     return TP_OK;
 }
 
@@ -1025,6 +1048,299 @@ int tp_result_elapsed_ms(const tp_result* r, double* ms) {
 }
 
 void tp_result_destroy(tp_result* r) { delete r; }
+
+}  // extern "C"
+
+// ============================================================ adjoint
+struct tp_tape {
+    tp_ctx* ctx = nullptr;
+    const tp_field* E = nullptr;
+    const tp_field* B = nullptr;
+    uint64_t E_id = 0, B_id = 0;
+    AdjArgs A{};
+    int fk = 0;
+    LaunchCfg cfg{};
+    int64_t nodes_E = 0, nodes_B = 0;
+    float* d_ckpt = nullptr;
+    double* d_u0 = nullptr;
+    float* d_rec = nullptr;
+    float4* d_geb = nullptr;
+    float4* d_gE = nullptr;
+    float4* d_gB = nullptr;
+    double* d_gparam = nullptr;
+    int64_t bytes = 0;
+    ~tp_tape() {
+        for (void* q : {(void*)d_ckpt, (void*)d_u0, (void*)d_rec, (void*)d_geb, (void*)d_gE, (void*)d_gB,
+                        (void*)d_gparam})
+            if (q) cudaFree(q);
+    }
+};
+
+namespace {
+
+bool field_static(const tp_field* f) {
+    if (f->desc.kind != TP_FIELD_AFFINE) return true;
+    return f->desc.rate[0] == 0.0 && f->desc.rate[1] == 0.0 && f->desc.rate[2] == 0.0;
+}
+
+template <class T>
+cudaError_t tape_alloc(tp_tape* t, T** p, size_t bytes) {
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e == cudaSuccess) t->bytes += (int64_t)bytes;
+    return e;
+}
+
+// Validate, build the launch block and allocate the checkpoint tape.
+int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const tp_field* B, int64_t n,
+                    tp_tape** out) {
+    if (!ctx || !d || !E || !B || !out) return fail(ctx, TP_E_ARG, "null argument");
+    *out = nullptr;
+    const tp_run_desc* r = &d->run;
+    int st = check_boris_desc(ctx, r);
+    if (st != TP_OK) return st;
+    if (r->alg != TP_ALG_BORIS) return fail(ctx, TP_E_UNSUPPORTED, "the adjoint covers the fixed-step Boris map");
+    if (r->precision != TP_PREC_FP32C)
+        return fail(ctx, TP_E_UNSUPPORTED, "the adjoint runs in TP_PREC_FP32C arithmetic");
+    if (r->term.flags != 0) return fail(ctx, TP_E_UNSUPPORTED, "the adjoint takes no termination predicate");
+    if (!field_static(E) || !field_static(B))
+        return fail(ctx, TP_E_UNSUPPORTED, "the adjoint needs static fields");
+    if (d->checkpoint_every < 1) return fail(ctx, TP_E_ARG, "checkpoint_every must be >= 1");
+    if (n < 0) return fail(ctx, TP_E_ARG, "negative particle count");
+    if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");
+    double dt = r->dt;
+    if (!(std::fabs(dt) >= 10.0 * kEps) || !std::isfinite(dt))
+        return fail(ctx, TP_E_ARG, "dt is too small (|dt| < 10 eps)");
+    int64_t nt = jl_round_h((r->t1 - r->t0) / dt);
+    if (nt < 0) return fail(ctx, TP_E_ARG, "the adjoint needs (t1 - t0) / dt >= 0");
+    if (nt > r->maxiters) return fail(ctx, TP_E_ARG, "nt exceeds maxiters");
+    DeviceGuard g(ctx->device);
+    auto* t = new tp_tape();
+    t->ctx = ctx;
+    t->E = E;
+    t->B = B;
+    t->E_id = E->id;
+    t->B_id = B->id;
+    AdjArgs& A = t->A;
+    st = prepare_boris_args(ctx, r, E, const_cast<tp_field*>(B), A.a);
+    if (st != TP_OK) {
+        delete t;
+        return st;
+    }
+    A.a.n = n;
+    A.nt = nt;
+    A.K = d->checkpoint_every < nt ? d->checkpoint_every : (nt > 0 ? nt : 1);
+    A.S = nt > 0 ? (nt + A.K - 1) / A.K : 1;
+    // final save of _boris_loop! at it = nt: t_final = t1, dt_final = t1 - (t0 + (nt - 1/2) dt)
+    A.dt_final = r->t1 - std::fma((double)nt - 0.5, dt, r->t0);
+    t->fk = adjoint_field_config(A.a.f);
+    t->nodes_E = E->nodes;
+    t->nodes_B = B->nodes;
+    st = pick_launch(ctx, n, r->block, false, 0, t->cfg);
+    if (st != TP_OK) {
+        delete t;
+        return st;
+    }
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        e = tape_alloc(t, &t->d_ckpt, (size_t)A.S * 15 * (size_t)n * sizeof(float));
+        if (e == cudaSuccess) e = tape_alloc(t, &t->d_u0, (size_t)n * 6 * sizeof(double));
+    }
+    if (e == cudaSuccess) e = tape_alloc(t, &t->d_gparam, 6 * sizeof(double));
+    if (e != cudaSuccess) {
+        delete t;
+        return cuda_fail(ctx, e, "adjoint tape");
+    }
+    A.ckpt = t->d_ckpt;
+    A.a.u0 = t->d_u0;
+    A.g_param = t->d_gparam;
+    *out = t;
+    return TP_OK;
+}
+
+int adjoint_forward_on(tp_tape* t, const double* u0_dev, double* ufinal_dev, cudaStream_t s) {
+    tp_ctx* ctx = t->ctx;
+    AdjArgs& A = t->A;
+    if (A.a.n == 0) return TP_OK;
+    cudaError_t e = cudaMemcpyAsync(t->d_u0, u0_dev, (size_t)A.a.n * 6 * sizeof(double), cudaMemcpyDefault, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint initial states");
+    A.u_final = ufinal_dev;
+    e = launch_adjoint_forward(A, t->fk, t->cfg, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint forward launch");
+    return TP_OK;
+}
+
+int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, float* gE_dev, float* gB_dev,
+                        double* gparam_dev, cudaStream_t s) {
+    tp_ctx* ctx = t->ctx;
+    AdjArgs& A = t->A;
+    if (t->E->id != t->E_id || t->B->id != t->B_id)
+        return fail(ctx, TP_E_ARG, "a field was updated after the tape was recorded");
+    const int64_t n = A.a.n;
+    cudaError_t e = cudaSuccess;
+    // segment records and node-gradient tables: allocated on first use, kept
+    if (!t->d_rec && n > 0) e = tape_alloc(t, &t->d_rec, (size_t)A.K * 9 * (size_t)n * sizeof(float));
+    const bool eb = t->fk == FK_EBGRID;
+    const bool gridE = !eb && t->E->desc.kind == TP_FIELD_GRID;
+    const bool gridB = !eb && t->B->desc.kind == TP_FIELD_GRID;
+    if (e == cudaSuccess && eb && !t->d_geb) e = tape_alloc(t, &t->d_geb, (size_t)t->nodes_B * 2 * sizeof(float4));
+    if (e == cudaSuccess && gridE && !t->d_gE) e = tape_alloc(t, &t->d_gE, (size_t)t->nodes_E * sizeof(float4));
+    if (e == cudaSuccess && gridB && !t->d_gB) e = tape_alloc(t, &t->d_gB, (size_t)t->nodes_B * sizeof(float4));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint scratch");
+    A.rec = t->d_rec;
+    A.g_eb = t->d_geb;
+    A.g_E = t->d_gE;
+    A.g_B = t->d_gB;
+    A.g_final = gfinal_dev;
+    A.g_u0 = gu0_dev;
+    if (eb) e = cudaMemsetAsync(t->d_geb, 0, (size_t)t->nodes_B * 2 * sizeof(float4), s);
+    if (e == cudaSuccess && gridE) e = cudaMemsetAsync(t->d_gE, 0, (size_t)t->nodes_E * sizeof(float4), s);
+    if (e == cudaSuccess && gridB) e = cudaMemsetAsync(t->d_gB, 0, (size_t)t->nodes_B * sizeof(float4), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->d_gparam, 0, 6 * sizeof(double), s);
+    if (e == cudaSuccess && n > 0) e = launch_adjoint_backward(A, t->fk, t->cfg, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint backward launch");
+    // grid parameter (uniform offset) gradients are the node-gradient sums
+    if (eb) {
+        e = launch_table_sum(t->d_geb, t->nodes_B, 2, 0, t->d_gparam, s);
+        if (e == cudaSuccess) e = launch_table_sum(t->d_geb, t->nodes_B, 2, 1, t->d_gparam + 3, s);
+        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 0, gE_dev, s);
+        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 1, gB_dev, s);
+    }
+    if (e == cudaSuccess && gridE) {
+        e = launch_table_sum(t->d_gE, t->nodes_E, 1, 0, t->d_gparam, s);
+        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_gE, t->nodes_E, 1, 0, gE_dev, s);
+    }
+    if (e == cudaSuccess && gridB) {
+        e = launch_table_sum(t->d_gB, t->nodes_B, 1, 0, t->d_gparam + 3, s);
+        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_gB, t->nodes_B, 1, 0, gB_dev, s);
+    }
+    if (e == cudaSuccess && gparam_dev)
+        e = cudaMemcpyAsync(gparam_dev, t->d_gparam, 6 * sizeof(double), cudaMemcpyDefault, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint gradient reduction");
+    return TP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tp_adjoint_forward_device(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const tp_field* B,
+                              const double* u0, int64_t n, double* u_final, tp_tape** tape, void* stream) {
+    if (!tape) return fail(ctx, TP_E_ARG, "null tape pointer");
+    *tape = nullptr;
+    if (n > 0 && (!u0 || !u_final)) return fail(ctx, TP_E_ARG, "null state buffer");
+    tp_tape* t = nullptr;
+    int st = adjoint_prepare(ctx, d, E, B, n, &t);
+    if (st != TP_OK) return st;
+    DeviceGuard g(ctx->device);
+    st = adjoint_forward_on(t, u0, u_final, (cudaStream_t)stream);
+    if (st != TP_OK) {
+        delete t;
+        return st;
+    }
+    *tape = t;
+    return TP_OK;
+}
+
+int tp_adjoint_backward_device(tp_tape* t, const double* grad_final, double* grad_u0, float* grad_E,
+                               float* grad_B, double* grad_param, void* stream) {
+    if (!t) return TP_E_ARG;
+    if (t->A.a.n > 0 && (!grad_final || !grad_u0)) return fail(t->ctx, TP_E_ARG, "null gradient buffer");
+    DeviceGuard g(t->ctx->device);
+    return adjoint_backward_on(t, grad_final, grad_u0, grad_E, grad_B, grad_param, (cudaStream_t)stream);
+}
+
+int tp_adjoint_forward(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const tp_field* B,
+                       const double* u0, int64_t n, double* u_final, tp_tape** tape) {
+    if (!tape) return fail(ctx, TP_E_ARG, "null tape pointer");
+    *tape = nullptr;
+    if (n > 0 && (!u0 || !u_final)) return fail(ctx, TP_E_ARG, "null state buffer");
+    tp_tape* t = nullptr;
+    int st = adjoint_prepare(ctx, d, E, B, n, &t);
+    if (st != TP_OK) return st;
+    DeviceGuard g(ctx->device);
+    DBuf uf;
+    cudaError_t e = uf.alloc((size_t)n * 6 * sizeof(double));
+    if (e != cudaSuccess) {
+        delete t;
+        return cuda_fail(ctx, e, "adjoint final states");
+    }
+    st = adjoint_forward_on(t, u0, uf.as<double>(), ctx->stream);
+    if (st == TP_OK && n > 0) {
+        e = cudaMemcpyAsync(u_final, uf.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "adjoint forward");
+    }
+    if (st != TP_OK) {
+        delete t;
+        return st;
+    }
+    *tape = t;
+    return TP_OK;
+}
+
+int tp_adjoint_backward(tp_tape* t, const double* grad_final, double* grad_u0, float* grad_E, float* grad_B,
+                        double* grad_param) {
+    if (!t) return TP_E_ARG;
+    tp_ctx* ctx = t->ctx;
+    const int64_t n = t->A.a.n;
+    if (n > 0 && (!grad_final || !grad_u0)) return fail(ctx, TP_E_ARG, "null gradient buffer");
+    DeviceGuard g(ctx->device);
+    const bool eb = t->fk == FK_EBGRID;
+    const int64_t nE = (eb || t->E->desc.kind == TP_FIELD_GRID) ? t->nodes_E : 0;
+    const int64_t nB = (eb || t->B->desc.kind == TP_FIELD_GRID) ? t->nodes_B : 0;
+    DBuf gf, gu, ge, gb, gp;
+    cudaError_t e = gf.alloc((size_t)n * 6 * sizeof(double));
+    if (e == cudaSuccess) e = gu.alloc((size_t)n * 6 * sizeof(double));
+    if (e == cudaSuccess && grad_E && nE) e = ge.alloc((size_t)nE * 3 * sizeof(float));
+    if (e == cudaSuccess && grad_B && nB) e = gb.alloc((size_t)nB * 3 * sizeof(float));
+    if (e == cudaSuccess) e = gp.alloc(6 * sizeof(double));
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpyAsync(gf.p, grad_final, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint buffers");
+    int st = adjoint_backward_on(t, gf.as<double>(), gu.as<double>(), ge.as<float>(), gb.as<float>(),
+                                 gp.as<double>(), ctx->stream);
+    if (st != TP_OK) return st;
+    if (n > 0) e = cudaMemcpyAsync(grad_u0, gu.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && ge.p)
+        e = cudaMemcpyAsync(grad_E, ge.p, (size_t)nE * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && gb.p)
+        e = cudaMemcpyAsync(grad_B, gb.p, (size_t)nB * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && grad_param)
+        e = cudaMemcpyAsync(grad_param, gp.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint backward");
+    return TP_OK;
+}
+
+int tp_tape_rerun_device(tp_tape* t, const double* u0, double* u_final, void* stream) {
+    if (!t) return TP_E_ARG;
+    tp_ctx* ctx = t->ctx;
+    if (t->A.a.n > 0 && (!u0 || !u_final)) return fail(ctx, TP_E_ARG, "null state buffer");
+    DeviceGuard g(ctx->device);
+    // refresh the field tables: a field may have been updated since the recording
+    DevFields f;
+    int st = make_dev_fields(ctx, t->E, const_cast<tp_field*>(t->B), f);
+    if (st != TP_OK) return st;
+    t->A.a.f = f;
+    t->E_id = t->E->id;
+    t->B_id = t->B->id;
+    return adjoint_forward_on(t, u0, u_final, (cudaStream_t)stream);
+}
+
+int tp_tape_info(const tp_tape* t, int64_t* device_bytes, int64_t* nsteps) {
+    if (!t) return TP_E_ARG;
+    if (device_bytes) *device_bytes = t->bytes;
+    if (nsteps) *nsteps = t->A.nt;
+    return TP_OK;
+}
+
+void tp_tape_destroy(tp_tape* t) {
+    if (!t) return;
+    DeviceGuard g(t->ctx->device);
+    cudaStreamSynchronize(t->ctx->stream);
+    cudaDeviceSynchronize();
+    delete t;
+}
 
 }  // extern "C"
 

@@ -51,6 +51,35 @@ struct GCPrepArgs {
     double* mu;
 };
 
+// discrete adjoint of the fixed-step Boris map (adjoint.cu)
+struct AdjArgs {
+    BorisArgs a;           // fields, q2m, t0, dt, FP32C wrap data, n, u0 (device, n x 6)
+    int64_t nt;            // steps N
+    int64_t K;             // steps per checkpoint segment
+    int64_t S;             // checkpoints: max(1, ceil(N / K))
+    double dt_final;       // dt of the final save's half update
+    float* ckpt;           // [S][15][n]: hi xyz, lo xyz, wrap xyz (int bits), v.h xyz, v.l xyz
+    double* u_final;       // n x 6
+    const double* g_final; // n x 6: dL/d(x_N, v_N)
+    double* g_u0;          // n x 6
+    float* rec;            // [K][9][n]: per step of a segment, hi xyz, lo xyz, v xyz
+    float4* g_eb;          // interleaved node-gradient table (2 float4 per node) or null
+    float4* g_E;           // per-field node-gradient tables (1 float4 per node) or null
+    float4* g_B;
+    double* g_param;       // 6: analytic-field parameter gradients (E then B)
+};
+
+// field configuration of an adjoint run (FK_ANALYTIC / FK_EBGRID / FK_GENERIC)
+int adjoint_field_config(const DevFields& f);
+cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
+cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
+// sum of a node-gradient table into out[0..2] (+=), entries k*stride + off
+cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out,
+                             cudaStream_t s);
+// node-gradient table -> user layout out[3*k + c] (float32)
+cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out,
+                                cudaStream_t s);
+
 cudaError_t launch_boris_fp64(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_boris_fp32c(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s);
 int occupancy_boris_fp64(const BorisArgs& a, int block);

@@ -26,8 +26,9 @@ import TestParticle: _solve, _solve_adaptive, TraceProblem, TraceGCProblem, Bori
 using SciMLBase: BasicEnsembleAlgorithm, EnsembleSolution, EnsembleContext, ReturnCode,
     LinearInterpolation, build_solution
 using StaticArrays: SVector
+import ChainRulesCore
 
-export EnsembleB200, UniformField, AffineField, DipoleField, B200Grid, Terminate
+export EnsembleB200, UniformField, AffineField, DipoleField, B200Grid, Terminate, boris_final_state
 
 const libtpb200 = get(ENV, "TPB200_LIB", joinpath(@__DIR__, "..", "..", "..", "libtpb200.so"))
 
@@ -314,6 +315,94 @@ function _solve(ens::EnsembleB200, prob::TraceGCProblem, trajectories, dt, saves
     finally
         free_field(hE); free_field(hB)
     end
+end
+
+# ------------------------------------------------------------------ adjoint (tp_adjoint_*)
+# Final save (x_N, v_N) of the fixed-step Boris solve as a differentiable
+# function of the initial states and of the fields: forward
+# tp_adjoint_forward (FP32C push, checkpoints every K steps), pullback
+# tp_adjoint_backward.  Field cotangents are Tangent{B200Grid}(A = dA) for
+# grids, Tangent{UniformField}(v = ...) and Tangent{DipoleField}(m = ...).
+struct TpAdjDesc
+    run::TpRunDesc
+    checkpoint_every::Int64
+end
+
+function adj_desc(q2m, m, dt, tspan, K)
+    nt = round(Int, abs((tspan[2] - tspan[1]) / dt))
+    TpAdjDesc(TpRunDesc(0, 2, 1, 1, 0.0, tspan[1], tspan[2], dt, q2m, m, 1, max(1_000_000, nt),
+        0, 1, 0, 0, termdesc(TestParticle.ODE_DEFAULT_ISOUTOFDOMAIN), 0, 0, 0, 0.0), K)
+end
+
+# tape and field handles of one recorded forward pass, released by the GC
+mutable struct AdjointTape
+    ctx::Ptr{Cvoid}; tape::Ptr{Cvoid}; hE::Ptr{Cvoid}; hB::Ptr{Cvoid}; n::Int
+    function AdjointTape(ctx, tape, hE, hB, n)
+        t = new(ctx, tape, hE, hB, n)
+        finalizer(release!, t)
+    end
+end
+function release!(t::AdjointTape)
+    t.tape != C_NULL && ccall((:tp_tape_destroy, libtpb200), Cvoid, (Ptr{Cvoid},), t.tape)
+    t.hE != C_NULL && free_field(t.hE)
+    t.hB != C_NULL && free_field(t.hB)
+    t.tape = t.hE = t.hB = C_NULL
+    return nothing
+end
+
+function adjoint_forward(U0::Matrix{Float64}, E, B; q2m, m = 1.0, dt, tspan, checkpoint_every = 64, device = 0)
+    size(U0, 1) == 6 || throw(ArgumentError("U0 must be a (6, N) matrix"))
+    ctx = context(device)
+    hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
+    n = size(U0, 2)
+    UN = Matrix{Float64}(undef, 6, n)
+    tape = Ref{Ptr{Cvoid}}(C_NULL)
+    d = Ref(adj_desc(q2m, m, dt, tspan, checkpoint_every))
+    st = ccall((:tp_adjoint_forward, libtpb200), Cint,
+        (Ptr{Cvoid}, Ref{TpAdjDesc}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Float64}, Ref{Ptr{Cvoid}}),
+        ctx, d, hE, hB, U0, n, UN, tape)
+    t = AdjointTape(ctx, tape[], hE, hB, n)
+    if st != 0
+        release!(t)
+        check(ctx, st, "tp_adjoint_forward")
+    end
+    return UN, t
+end
+
+"""
+    boris_final_state(U0, E, B; q2m, m, dt, tspan, checkpoint_every = 64, device = 0)
+
+(6, N) final saves of `solve(TraceProblem(u0, tspan, (q2m, m, E, B, ...)), Boris(); dt)` for the
+columns of `U0`, in the FP32C arithmetic of `EnsembleB200(; precision = :fp32c)`.  Differentiable
+through its `ChainRulesCore.rrule` (discrete adjoint on the B200).
+"""
+function boris_final_state(U0::Matrix{Float64}, E, B; kw...)
+    UN, t = adjoint_forward(U0, E, B; kw...)
+    release!(t)
+    return UN
+end
+
+field_cotangent(f::B200Grid, g, _) = ChainRulesCore.Tangent{typeof(f)}(; A = g)
+field_cotangent(f::UniformField, _, p) = ChainRulesCore.Tangent{typeof(f)}(; v = SVector{3}(p))
+field_cotangent(f::DipoleField, _, p) = ChainRulesCore.Tangent{typeof(f)}(; m = SVector{3}(p))
+field_cotangent(f, _, _) = ChainRulesCore.NoTangent()
+
+function ChainRulesCore.rrule(::typeof(boris_final_state), U0::Matrix{Float64}, E, B; kw...)
+    UN, t = adjoint_forward(U0, E, B; kw...)
+    function boris_final_state_pullback(dUN)
+        G = Matrix{Float64}(ChainRulesCore.unthunk(dUN))
+        dU0 = Matrix{Float64}(undef, 6, t.n)
+        gE = unwrap(E) isa B200Grid ? Array{Float32}(undef, size(unwrap(E).A)) : nothing
+        gB = unwrap(B) isa B200Grid ? Array{Float32}(undef, size(unwrap(B).A)) : nothing
+        gp = Vector{Float64}(undef, 6)
+        st = ccall((:tp_adjoint_backward, libtpb200), Cint,
+            (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float32}, Ptr{Float32}, Ptr{Float64}),
+            t.tape, G, dU0, isnothing(gE) ? C_NULL : gE, isnothing(gB) ? C_NULL : gB, gp)
+        check(t.ctx, st, "tp_adjoint_backward")
+        return (ChainRulesCore.NoTangent(), dU0, field_cotangent(unwrap(E), gE, gp[1:3]),
+            field_cotangent(unwrap(B), gB, gp[4:6]))
+    end
+    return UN, boris_final_state_pullback
 end
 
 end # module

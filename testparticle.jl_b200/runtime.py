@@ -135,6 +135,45 @@ class Context:
                                             nsteps, status, stream)
         _check(self.lib, self.handle, code, "tp_boris_run_device")
 
+    def field_update(self, f, data) -> None:
+        """Replace the node values of a grid field already on the device (tp_field_update).
+
+        `data` is a (3, nx, ny, nz) array in the field's dtype, or an int
+        device pointer to the same layout (component fastest).
+        """
+        h = self.field(f)
+        if isinstance(data, int):
+            ptr = C.c_void_p(data)
+        else:
+            a = np.asfortranarray(np.asarray(data, dtype=f.data.dtype))
+            if a.shape != f.data.shape:
+                raise ValueError("field_update: shape differs from the field's grid")
+            f.data = a
+            ptr = a.ctypes.data_as(C.c_void_p)
+        _check(self.lib, self.handle, self.lib.tp_field_update(h, ptr), "tp_field_update")
+
+    # ------------------------------------------------------------ adjoint
+    def adjoint_forward(self, desc: _abi.AdjDesc, E, B, u0: np.ndarray):
+        """Final save (x_N, v_N) (N x 6) of a fixed-step Boris solve and the tape of its adjoint."""
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        n = u0.shape[0]
+        assert u0.shape == (n, 6)
+        uf = np.empty((n, 6))
+        h = C.c_void_p()
+        code = self.lib.tp_adjoint_forward(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0), n,
+                                           _ptr(uf), C.byref(h))
+        _check(self.lib, self.handle, code, "tp_adjoint_forward")
+        return uf, Tape(self, h, n, E, B)
+
+    def adjoint_forward_device(self, desc: _abi.AdjDesc, E, B, u0: int, n: int, u_final: int,
+                               stream: int = 0) -> "Tape":
+        """Device-buffer forward: u0 and u_final are device pointers (N x 6 float64)."""
+        h = C.c_void_p()
+        code = self.lib.tp_adjoint_forward_device(self.handle, C.byref(desc), self.field(E), self.field(B), u0,
+                                                  int(n), u_final, C.byref(h), stream)
+        _check(self.lib, self.handle, code, "tp_adjoint_forward_device")
+        return Tape(self, h, n, E, B)
+
     def gc_prepare(self, E, B, xv: np.ndarray, q: float, m: float, t: float = 0.0):
         xv = np.ascontiguousarray(xv, dtype=np.float64)
         n = xv.shape[0]
@@ -179,3 +218,61 @@ class RunResult:
         o = np.zeros(self.nsaved.size + 1, dtype=np.int64)
         np.cumsum(self.nsaved, out=o[1:])
         return o
+
+
+def _grid_nodes(f) -> int:
+    d = getattr(f, "data", None)
+    return int(np.prod(d.shape[1:])) if d is not None and getattr(d, "ndim", 0) == 4 else 0
+
+
+@dataclass
+class AdjointGrads:
+    u0: np.ndarray                 # dL/du0, N x 6
+    E: object                      # dL/d(E node values), (3, nx, ny, nz) float32, or None
+    B: object
+    param: np.ndarray              # 6: (E, B) dipole moment or uniform-offset gradients
+
+
+class Tape:
+    """Checkpoints of one adjoint forward pass (tp_tape); backward() may run more than once."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, n: int, E, B):
+        self.ctx, self.handle, self.n = ctx, handle, int(n)
+        self.E, self.B = E, B  # the fields must outlive the tape
+        self._fin = weakref.finalize(self, ctx.lib.tp_tape_destroy, handle)
+
+    def backward(self, grad_final: np.ndarray, fields: bool = True) -> AdjointGrads:
+        lib = self.ctx.lib
+        g = np.ascontiguousarray(grad_final, dtype=np.float64)
+        assert g.shape == (self.n, 6)
+        gu = np.empty((self.n, 6))
+        gp = np.empty(6)
+        out = []
+        for f in (self.E, self.B):
+            nodes = _grid_nodes(f) if fields else 0
+            out.append(np.empty(3 * nodes, dtype=np.float32) if nodes else None)
+        code = lib.tp_adjoint_backward(self.handle, _ptr(g), _ptr(gu), _ptr(out[0]), _ptr(out[1]), _ptr(gp))
+        _check(lib, self.ctx.handle, code, "tp_adjoint_backward")
+        shaped = [None if a is None else a.reshape(f.data.shape, order="F") for a, f in zip(out, (self.E, self.B))]
+        return AdjointGrads(gu, shaped[0], shaped[1], gp)
+
+    def backward_device(self, grad_final: int, grad_u0: int, grad_E=None, grad_B=None, grad_param=None,
+                        stream: int = 0) -> None:
+        """Device-buffer backward: every argument is a device pointer (int) or None."""
+        code = self.ctx.lib.tp_adjoint_backward_device(self.handle, grad_final, grad_u0, grad_E, grad_B,
+                                                       grad_param, stream)
+        _check(self.ctx.lib, self.ctx.handle, code, "tp_adjoint_backward_device")
+
+    def rerun_device(self, u0: int, u_final: int, stream: int = 0) -> None:
+        """Re-record the tape for new initial states (device pointers), reusing its memory."""
+        code = self.ctx.lib.tp_tape_rerun_device(self.handle, u0, u_final, stream)
+        _check(self.ctx.lib, self.ctx.handle, code, "tp_tape_rerun_device")
+
+    def info(self) -> tuple[int, int]:
+        """(device bytes held, steps N)."""
+        b, s = C.c_int64(), C.c_int64()
+        self.ctx.lib.tp_tape_info(self.handle, C.byref(b), C.byref(s))
+        return b.value, s.value
+
+    def close(self) -> None:
+        self._fin()

@@ -180,6 +180,41 @@ def plan_gc(prob, ens=None, *, trajectories=1, savestepinterval=1, dt=None, isou
     return GCPlan(desc, as_field(E), as_field(B), y0, pp_q, pp_q2m, pp_mu, dt_arr, tend_arr, alg, ens.device)
 
 
+@dataclass
+class AdjointPlan:
+    desc: _abi.AdjDesc
+    E: object
+    B: object
+    u0: np.ndarray          # (N, 6)
+    device: int
+
+
+def plan_adjoint(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 64,
+                 maxiters=None) -> AdjointPlan:
+    """Descriptor of the discrete adjoint of solve(prob, Boris(); dt) (final save, no saves in between).
+
+    The adjoint runs in the FP32C arithmetic of EnsembleB200(precision="fp32c")
+    with static fields and no termination predicate.
+    """
+    ens = ens if ens is not None else EnsembleB200(precision="fp32c")
+    if ens.precision != "fp32c":
+        raise NotImplementedError("the Boris adjoint runs in precision='fp32c'")
+    p = plan_boris(prob, Boris(), ens, dt=dt, trajectories=trajectories, savestepinterval=1,
+                   save_start=False, save_everystep=False, maxiters=maxiters)
+    d = _abi.AdjDesc()
+    d.run = p.desc
+    d.checkpoint_every = int(checkpoint_every)
+    return AdjointPlan(d, p.E, p.B, p.u0, p.device)
+
+
+def adjoint_solve(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 64, maxiters=None):
+    """(final states (N, 6), Tape): tape.backward(dL/d final states) gives the gradients."""
+    p = plan_adjoint(prob, ens, dt=dt, trajectories=trajectories, checkpoint_every=checkpoint_every,
+                     maxiters=maxiters)
+    ctx = Context.get(p.device)
+    return ctx.adjoint_forward(p.desc, p.E, p.B, p.u0)
+
+
 def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None, isoutside=None,
           save_start: bool = True, save_end: bool = True, save_everystep: bool = True,
           save_fields: bool = False, save_work: bool = False, maxiters=None, alg=None,

@@ -251,3 +251,27 @@ def config4(n: int = 1 << 20) -> GCWorkload:
     y0 = np.concatenate([X, vpar[:, None]], axis=1).T.copy()
     return GCWorkload("config4_gc_dipole", y0, charge, charge / mass, mu, mass, ZeroField(),
                       DipoleField(tuple(mvec)), tau_b)
+
+
+# ------------------------------------------------------------------ config 5
+def config5(n: int = 1 << 18, nt: int = 4096, nx: int = 128) -> FullOrbitWorkload:
+    """Adjoint workload: protons drawn as in config 2 (same field), nt steps.
+
+    extra["target_offset"] (N, 3) holds the seeded N(0, (1e5 m)^2) offsets of
+    the targets x_target = x_N(float64 solve) + offset; the loss is
+    mean_i |x_N,i - x_target,i|^2.
+    """
+    w = config2(n=n, nx=nx, nt=nt, ssi=nt)
+    rng = SplitMix64(SEED0 + 5)
+    w.name = "config5_boris_adjoint_128cube"
+    w.extra["target_offset"] = rng.normal(3 * n, 1.0e5).reshape(n, 3)
+    return w
+
+
+def loss_and_grad(x_final: np.ndarray, x_target: np.ndarray):
+    """L = mean_i |x_i - t_i|^2 and dL/d(final state) (N, 6; zero velocity part)."""
+    d = x_final[:, :3] - x_target
+    n = d.shape[0]
+    g = np.zeros((n, 6))
+    g[:, :3] = 2.0 * d / n
+    return float(np.sum(d * d) / n), g
