@@ -296,7 +296,7 @@ def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, re
     s = stream.cuda_stream
     tape = ctx.adjoint_forward_device(plan.desc, plan.E, plan.B, u0.data_ptr(), n, uf.data_ptr(), s)
     nodes = int(np.prod(w.B.data.shape[1:]))
-    gE = torch.empty(3 * nodes, dtype=torch.float32, device=dev)
+    gE = torch.empty(3 * nodes, dtype=torch.float64, device=dev)
     gB = torch.empty_like(gE)
     gp = torch.empty(6, dtype=torch.float64, device=dev)
     gu = torch.empty_like(u0)

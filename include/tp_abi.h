@@ -313,7 +313,10 @@ int tp_pack_results_device_noalloc(tp_ctx* ctx, const double* t_in,
  * Gradients:
  *   grad_u0      dL/du0, N x 6 (float64)
  *   grad_E/B     for grid fields: dL/d(node values), laid out like the
- *                field's data (component fastest), float32; NULL to skip
+ *                field's data (component fastest), float64; NULL to skip.
+ *                They are accumulated in float32 with a power-of-two scale
+ *                chosen per pass, so they span float64's range; in a chaotic
+ *                field they grow exponentially with the number of steps
  *   grad_param   6 float64: for E then B, dL/dtheta with theta = the dipole
  *                moment for a dipole field, else a uniform offset added to
  *                the field (for a grid: the sum of the node gradients)
@@ -331,15 +334,16 @@ int tp_adjoint_forward(tp_ctx* ctx, const tp_adj_desc* desc, const tp_field* E,
                        const tp_field* B, const double* u0, int64_t n,
                        double* u_final, tp_tape** tape);
 int tp_adjoint_backward(tp_tape* tape, const double* grad_final,
-                        double* grad_u0, float* grad_E, float* grad_B,
+                        double* grad_u0, double* grad_E, double* grad_B,
                         double* grad_param);
-/* device buffers, asynchronous on `stream` (a cudaStream_t) */
+/* device buffers, on `stream` (a cudaStream_t); the backward pass waits for
+ * its stream once, to check the range of the node gradients (see above)    */
 int tp_adjoint_forward_device(tp_ctx* ctx, const tp_adj_desc* desc,
                               const tp_field* E, const tp_field* B,
                               const double* u0, int64_t n, double* u_final,
                               tp_tape** tape, void* stream);
 int tp_adjoint_backward_device(tp_tape* tape, const double* grad_final,
-                               double* grad_u0, float* grad_E, float* grad_B,
+                               double* grad_u0, double* grad_E, double* grad_B,
                                double* grad_param, void* stream);
 /* Re-record an existing tape for new initial states (same N), reusing its
  * device memory; fields updated with tp_field_update since are picked up.

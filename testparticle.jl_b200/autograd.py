@@ -13,7 +13,8 @@ Plain package fields (ZeroField, UniformField, DipoleField,
 FieldInterpolator, ...) are accepted as constants.  The forward pass runs
 tp_adjoint_forward_device (FP32C push, checkpoints every `checkpoint_every`
 steps) on torch's current stream; backward runs tp_adjoint_backward_device.
-Node gradients are computed in float32 and cast to the data's dtype.
+Node gradients are accumulated in float32 with a power-of-two scale per pass,
+returned in float64 by the library, and cast to the data's dtype.
 
 The Julia counterpart is the ChainRulesCore rrule of TestParticleB200.jl.
 """
@@ -161,7 +162,7 @@ class BorisAdjointFunction(torch.autograd.Function):
 
         def node_buf(f):
             if isinstance(f, GridTensor):
-                return torch.empty(3 * int(np.prod(f.data.shape[1:])), dtype=torch.float32, device=dev)
+                return torch.empty(3 * int(np.prod(f.data.shape[1:])), dtype=torch.float64, device=dev)
             return None
 
         gE = node_buf(ctx.E_in) if ctx.needs_input_grad[1] else None

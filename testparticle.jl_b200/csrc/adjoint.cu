@@ -29,6 +29,16 @@
 // lx += sum_c grad w_c(x) (E_c . lE + B_c . lB).
 // Analytic fields contribute J^T l to lx (J the field's Jacobian) and their
 // parameter gradient (uniform offset, or dipole moment) to g_param.
+//
+// Range.  In a chaotic field the cotangents grow exponentially with the
+// number of steps (in the 128^3 turbulent field, |dx_N/dx_0| reaches 1e18 to
+// 1e27 after 4096 steps), beyond float32.  Each particle therefore carries
+// its cotangent as float32 values times 2^e (renormalised by exact powers of
+// two), and the node-gradient tables hold float32 values times 2^G, one G per
+// pass.  A pass whose largest node contribution would not fit reports the
+// exponent it needed (A.need) and the host repeats it with a larger G.
+#include <climits>
+
 #include "fp32c_common.cuh"
 #include "tp_device.cuh"
 #include "tp_launch.h"
@@ -153,15 +163,6 @@ __device__ __forceinline__ void tri_weights(const AxF& ax, const AxF& ay, const 
     w[7] = x1 * a11;
 }
 
-// gradient in x of sum_c w_c(x) g_c
-__device__ __forceinline__ F3 tri_grad(const float* g, const AxF& ax, const AxF& ay, const AxF& az) {
-    const float fx = ax.f, fy = ay.f, fz = az.f;
-    float dx = lerp32(lerp32(g[1] - g[0], g[3] - g[2], fy), lerp32(g[5] - g[4], g[7] - g[6], fy), fz);
-    float dy = lerp32(lerp32(g[2] - g[0], g[3] - g[1], fx), lerp32(g[6] - g[4], g[7] - g[5], fx), fz);
-    float dz = lerp32(lerp32(g[4] - g[0], g[5] - g[1], fx), lerp32(g[6] - g[2], g[7] - g[3], fx), fy);
-    return {dx * ax.ds, dy * ay.ds, dz * az.ds};
-}
-
 __device__ __forceinline__ void red_add3(float4* p, float a, float b, float c) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(0.0f)
                  : "memory");
@@ -237,10 +238,81 @@ __device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w
     }
 }
 
+// ----------------------------------------------------- cotangent frame
+// lambda_true = lambda * 2^e; node contributions are scaled by f = 2^(e - G)
+// (0 when they would underflow the table); mx is the largest exponent of a
+// node contribution seen, e included.
+struct Frame {
+    int e;
+    int mx;
+    float f;
+    double s;  // 2^e, for the float64 parameter accumulators
+};
+
+__device__ __forceinline__ int fexp(float m) { return ((__float_as_int(m) >> 23) & 0xff) - 127; }
+
+__device__ __forceinline__ void frame_set(Frame& fr, int G) {
+    const int d = fr.e - G;
+    fr.f = d < -126 ? 0.0f : __int_as_float((min(d, 127) + 127) << 23);
+    fr.s = ldexp(1.0, fr.e);
+}
+
+// keep max |lambda| near 1: exact rescaling by a power of two
+__device__ __forceinline__ void renorm(F3& lx, F3& lv, Frame& fr, int G) {
+    float m = fmaxf(fmaxf(fmaxf(fabsf(lx.x), fabsf(lx.y)), fmaxf(fabsf(lx.z), fabsf(lv.x))),
+                    fmaxf(fabsf(lv.y), fabsf(lv.z)));
+    int k = fexp(m);
+    if ((k > 40 && k < 128) || (k < -40 && m > 0.0f)) {
+        float sc = __int_as_float((127 - k) << 23);  // 2^-k, k in [-127, 127]
+        lx = sc * lx;
+        lv = sc * lv;
+        fr.e += k;
+        frame_set(fr, G);
+    }
+}
+
+// value and Jacobian (d/dx, d/dy, d/dz of the three components) of the
+// trilinear interpolant; the value uses the forward's lerp order
+__device__ __forceinline__ void tri_val_jac(const float4* q, const AxF& ax, const AxF& ay, const AxF& az, F3& val,
+                                            F3& dx, F3& dy, F3& dz) {
+    val = tri3(xyz(q[0]), xyz(q[1]), xyz(q[2]), xyz(q[3]), xyz(q[4]), xyz(q[5]), xyz(q[6]), xyz(q[7]), ax, ay, az);
+    const float fx = ax.f, fy = ay.f, fz = az.f;
+#define TPB_JAC(c)                                                                                           \
+    dx.c = lerp32(lerp32(q[1].c - q[0].c, q[3].c - q[2].c, fy), lerp32(q[5].c - q[4].c, q[7].c - q[6].c, fy), fz) * \
+           ax.ds;                                                                                            \
+    dy.c = lerp32(lerp32(q[2].c - q[0].c, q[3].c - q[1].c, fx), lerp32(q[6].c - q[4].c, q[7].c - q[5].c, fx), fz) * \
+           ay.ds;                                                                                            \
+    dz.c = lerp32(lerp32(q[4].c - q[0].c, q[5].c - q[1].c, fx), lerp32(q[6].c - q[2].c, q[7].c - q[3].c, fx), fy) * \
+           az.ds;
+    TPB_JAC(x)
+    TPB_JAC(y)
+    TPB_JAC(z)
+#undef TPB_JAC
+}
+
+// J^T l for a Jacobian given by its columns (dx, dy, dz)
+__device__ __forceinline__ F3 jt(const F3& dx, const F3& dy, const F3& dz, F3 l) {
+    return {dot(dx, l), dot(dy, l), dot(dz, l)};
+}
+
+// node contributions: weights times the frame's scale, and the exponent record
+__device__ __forceinline__ bool scale_weights(const AxF& ax, const AxF& ay, const AxF& az, F3 la, F3 lb,
+                                              Frame& fr, float* w) {
+    if (fr.f == 0.0f) return false;
+    float m = fmaxf(fmaxf(fmaxf(fabsf(la.x), fabsf(la.y)), fmaxf(fabsf(la.z), fabsf(lb.x))),
+                    fmaxf(fabsf(lb.y), fabsf(lb.z)));
+    fr.mx = max(fr.mx, fexp(m) + fr.e);
+    tri_weights(ax, ay, az, w);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) w[c] *= fr.f;
+    return true;
+}
+
 // --------------------------------------------- one step, interleaved E/B grid
 // Returns the cotangent of the update's input velocity; adds the position
 // cotangent to lx and scatters the node gradients.
-__device__ __forceinline__ F3 adj_step_eb(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx) {
+__device__ __forceinline__ F3 adj_step_eb(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx,
+                                          Frame& fr) {
     const DevFields& F = A.a.f;
     AxF ax, ay, az;
     if (!axes32(F.B, p, ax, ay, az)) {  // outside a FillExtrap(NaN) grid: NaN, as the forward
@@ -249,22 +321,19 @@ __device__ __forceinline__ F3 adj_step_eb(const AdjArgs& A, const CPos& p, F3 v,
     }
     int nd[8];
     tri_nodes(F.B, ax, ay, az, nd);
-    const float4* T = F.eb32;
-    float4 e[8], b[8];
+    F3 E, B, Ex, Ey, Ez, Bx, By, Bz;
+    {
+        const float4* T = F.eb32;
+        float4 e[8], b[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) ldg_node8(T + 2 * (int64_t)nd[c], e[c], b[c]);
-    F3 E = tri3(xyz(e[0]), xyz(e[1]), xyz(e[2]), xyz(e[3]), xyz(e[4]), xyz(e[5]), xyz(e[6]), xyz(e[7]), ax, ay,
-                az);
-    F3 B = tri3(xyz(b[0]), xyz(b[1]), xyz(b[2]), xyz(b[3]), xyz(b[4]), xyz(b[5]), xyz(b[6]), xyz(b[7]), ax, ay,
-                az);
+        for (int c = 0; c < 8; ++c) ldg_node8(T + 2 * (int64_t)nd[c], e[c], b[c]);
+        tri_val_jac(e, ax, ay, az, E, Ex, Ey, Ez);
+        tri_val_jac(b, ax, ay, az, B, Bx, By, Bz);
+    }
     UAdj u = u_adjoint(v, E, B, h, lo);
-    float g[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) g[c] = dot(xyz(e[c]), u.lE) + dot(xyz(b[c]), u.lB);
-    lx = lx + tri_grad(g, ax, ay, az);
+    lx = lx + jt(Ex, Ey, Ez, u.lE) + jt(Bx, By, Bz, u.lB);
     float w[8];
-    tri_weights(ax, ay, az, w);
-    scatter<2>(A.g_eb, nd, w, u.lE, u.lB);
+    if (scale_weights(ax, ay, az, u.lE, u.lB, fr, w)) scatter<2>(A.g_eb, nd, w, u.lE, u.lB);
     return u.lv;
 }
 
@@ -272,38 +341,36 @@ __device__ __forceinline__ F3 adj_step_eb(const AdjArgs& A, const CPos& p, F3 v,
 struct GridKeep {
     AxF ax, ay, az;
     int nd[8];
-    float4 c[8];
+    F3 dx, dy, dz;
     bool ok;
 };
 
-// the arithmetic of grid_eval32, keeping the stencil
+// the arithmetic of grid_eval32, keeping the stencil and the Jacobian
 __device__ __forceinline__ F3 grid_eval_keep(const DevField& g, const CPos& p, GridKeep& k) {
     k.ok = axes32(g, p, k.ax, k.ay, k.az);
     if (!k.ok) return nanf3_();
     tri_nodes(g, k.ax, k.ay, k.az, k.nd);
+    float4 q[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) k.c[c] = __ldg(g.tab32 + k.nd[c]);
-    return tri3(xyz(k.c[0]), xyz(k.c[1]), xyz(k.c[2]), xyz(k.c[3]), xyz(k.c[4]), xyz(k.c[5]), xyz(k.c[6]),
-                xyz(k.c[7]), k.ax, k.ay, k.az);
+    for (int c = 0; c < 8; ++c) q[c] = __ldg(g.tab32 + k.nd[c]);
+    F3 val;
+    tri_val_jac(q, k.ax, k.ay, k.az, val, k.dx, k.dy, k.dz);
+    return val;
 }
 
 // field f evaluated to lam's cotangent: lx += J^T lam, parameter gradient
 // to th (analytic kinds), node gradients to G (grids)
 __device__ __forceinline__ void field_adj(const DevField& f, const CPos& p, const GridKeep& k, F3 lam, float4* G,
-                                          F3& lx, double* th) {
+                                          F3& lx, double* th, Frame& fr) {
     switch (f.kind) {
         case TP_FIELD_GRID: {
             if (!k.ok) {
                 lx = nanf3_();
                 return;
             }
-            float g[8];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) g[c] = dot(xyz(k.c[c]), lam);
-            lx = lx + tri_grad(g, k.ax, k.ay, k.az);
+            lx = lx + jt(k.dx, k.dy, k.dz, lam);
             float w[8];
-            tri_weights(k.ax, k.ay, k.az, w);
-            scatter<1>(G, k.nd, w, lam, lam);
+            if (scale_weights(k.ax, k.ay, k.az, lam, lam, fr, w)) scatter<1>(G, k.nd, w, lam, lam);
             return;
         }
         case TP_FIELD_AFFINE: {
@@ -311,9 +378,9 @@ __device__ __forceinline__ void field_adj(const DevField& f, const CPos& p, cons
             const float* J = f.Jf;
             lx = lx + F3{J[0] * lam.x + J[3] * lam.y + J[6] * lam.z, J[1] * lam.x + J[4] * lam.y + J[7] * lam.z,
                          J[2] * lam.x + J[5] * lam.y + J[8] * lam.z};
-            th[0] += lam.x;
-            th[1] += lam.y;
-            th[2] += lam.z;
+            th[0] += fr.s * lam.x;
+            th[1] += fr.s * lam.y;
+            th[2] += fr.s * lam.z;
             return;
         }
         case TP_FIELD_DIPOLE: {
@@ -328,23 +395,23 @@ __device__ __forceinline__ void field_adj(const DevField& f, const CPos& p, cons
             float mr = dot(mh, rh), rl = dot(rh, lam), ml = dot(mh, lam);
             float k4 = (f.Kf * ir) * ir * ir * ir;
             lx = lx + k4 * ((3.0f * rl) * mh + (3.0f * mr) * lam + (3.0f * ml - 15.0f * mr * rl) * rh);
-            double k3 = f.coef * (double)ir * (double)ir * (double)ir;
+            double k3 = fr.s * f.coef * (double)ir * (double)ir * (double)ir;
             th[0] += k3 * (3.0 * (double)rl * (double)rh.x - (double)lam.x);
             th[1] += k3 * (3.0 * (double)rl * (double)rh.y - (double)lam.y);
             th[2] += k3 * (3.0 * (double)rl * (double)rh.z - (double)lam.z);
             return;
         }
         default:  // zero / uniform: gradient of a uniform offset
-            th[0] += lam.x;
-            th[1] += lam.y;
-            th[2] += lam.z;
+            th[0] += fr.s * lam.x;
+            th[1] += fr.s * lam.y;
+            th[2] += fr.s * lam.z;
             return;
     }
 }
 
 template <int FK>
 __device__ __forceinline__ F3 adj_step_gen(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx,
-                                           double* thE, double* thB) {
+                                           double* thE, double* thB, Frame& fr) {
     const DevFields& F = A.a.f;
     GridKeep kE, kB;
     kE.ok = kB.ok = true;
@@ -353,16 +420,16 @@ __device__ __forceinline__ F3 adj_step_gen(const AdjArgs& A, const CPos& p, F3 v
     F3 B = (FK == FK_GENERIC && F.B.kind == TP_FIELD_GRID) ? grid_eval_keep(F.B, p, kB)
                                                             : analytic_eval32(F.B, p, A.a.t0);
     UAdj u = u_adjoint(v, E, B, h, lo);
-    field_adj(F.E, p, kE, u.lE, A.g_E, lx, thE);
-    field_adj(F.B, p, kB, u.lB, A.g_B, lx, thB);
+    field_adj(F.E, p, kE, u.lE, A.g_E, lx, thE, fr);
+    field_adj(F.B, p, kB, u.lB, A.g_B, lx, thB, fr);
     return u.lv;
 }
 
 template <int FK>
 __device__ __forceinline__ F3 adj_step(const AdjArgs& A, const CPos& p, F3 v, float h, F3 lo, F3& lx,
-                                       double* thE, double* thB) {
-    if (FK == FK_EBGRID) return adj_step_eb(A, p, v, h, lo, lx);
-    return adj_step_gen<FK>(A, p, v, h, lo, lx, thE, thB);
+                                       double* thE, double* thB, Frame& fr) {
+    if (FK == FK_EBGRID) return adj_step_eb(A, p, v, h, lo, lx, fr);
+    return adj_step_gen<FK>(A, p, v, h, lo, lx, thE, thB, fr);
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -423,12 +490,22 @@ __global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
     const float h = vfac<false>(a, dt);
     const float h_fin = vfac<false>(a, A.dt_final);
     const float h_ini = vfac<false>(a, -0.5 * dt);
+    const int G = A.G;
     double thE[3] = {0.0, 0.0, 0.0}, thB[3] = {0.0, 0.0, 0.0};
+    int mx = INT_MIN;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
          i += (int64_t)gridDim.x * blockDim.x) {
+        // cotangent of the final save, normalised: lambda = g / 2^e
         const double* gf = A.g_final + 6 * i;
-        F3 lx{(float)gf[0], (float)gf[1], (float)gf[2]};
-        F3 lv{(float)gf[3], (float)gf[4], (float)gf[5]};
+        double gm = fmax(fmax(fmax(fabs(gf[0]), fabs(gf[1])), fmax(fabs(gf[2]), fabs(gf[3]))),
+                         fmax(fabs(gf[4]), fabs(gf[5])));
+        Frame fr;
+        fr.e = (gm > 0.0 && gm <= 1.0e300) ? ilogb(gm) : 0;
+        fr.mx = INT_MIN;
+        frame_set(fr, G);
+        const double is = ldexp(1.0, -fr.e);
+        F3 lx{(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
+        F3 lv{(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
         for (int64_t s = A.S - 1; s >= 0; --s) {
             CPos p;
             CV v;
@@ -442,13 +519,25 @@ __global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
                 v = vel32h<false>(v, E, B, a, h);
                 cpos_push_cv(a, p, v, dth, dtl);
             }
-            if (s == A.S - 1) lv = adj_step<FK>(A, p, v.h, h_fin, lv, lx, thE, thB);  // final save
-            for (int j = m - 1; j >= 0; --j) {
+            if (s == A.S - 1) {  // final save
+                lv = adj_step<FK>(A, p, v.h, h_fin, lv, lx, thE, thB, fr);
+                renorm(lx, lv, fr, G);
+            }
+            if (m > 0) {
+                // the record of the next (earlier) step is loaded one step ahead
                 CPos q;
                 F3 vh;
-                load_rec(A, j, i, q, vh);
-                F3 lo = lv + dtf * lx;
-                lv = adj_step<FK>(A, q, vh, h, lo, lx, thE, thB);
+                load_rec(A, m - 1, i, q, vh);
+                for (int j = m - 1; j >= 0; --j) {
+                    CPos qn = q;
+                    F3 vn = vh;
+                    if (j > 0) load_rec(A, j - 1, i, qn, vn);
+                    F3 lo = lv + dtf * lx;
+                    lv = adj_step<FK>(A, q, vh, h, lo, lx, thE, thB, fr);
+                    renorm(lx, lv, fr, G);
+                    q = qn;
+                    vh = vn;
+                }
             }
         }
         // initial half step back
@@ -456,15 +545,18 @@ __global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
         CPos p0;
         cpos_init(a, p0, u0);
         CV v0 = cv_from(u0 + 3);
-        lv = adj_step<FK>(A, p0, v0.h, h_ini, lv, lx, thE, thB);
+        lv = adj_step<FK>(A, p0, v0.h, h_ini, lv, lx, thE, thB, fr);
         double* go = A.g_u0 + 6 * i;
-        go[0] = lx.x;
-        go[1] = lx.y;
-        go[2] = lx.z;
-        go[3] = lv.x;
-        go[4] = lv.y;
-        go[5] = lv.z;
+        go[0] = fr.s * lx.x;
+        go[1] = fr.s * lx.y;
+        go[2] = fr.s * lx.z;
+        go[3] = fr.s * lv.x;
+        go[4] = fr.s * lv.y;
+        go[5] = fr.s * lv.z;
+        mx = max(mx, fr.mx);
     }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0 && mx != INT_MIN) atomicMax(A.need, mx);
     if (FK != FK_EBGRID) {
         bool any = false;
 #pragma unroll
@@ -482,7 +574,188 @@ __global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
     }
 }
 
-__global__ void k_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out) {
+// --------------------------------------------- segmented backward, E/B grid
+// For an interleaved E/B grid the backward pass runs as two kernels per
+// checkpoint segment.  Recompute reads the field table and streams, for every
+// step, the update's inputs and the field's value and Jacobian to the
+// records.  Reverse reads the records and accumulates into the gradient
+// table.  Each kernel's random-access working set is one 32-byte-per-node
+// table, which fits in L2; the records stream through with evict-first hints.
+constexpr int kRecEB = 33;  // cell xyz (int; x = -1 outside the grid), fraction xyz, v, E, B, dE/dx.., dB/dx..
+
+__device__ __forceinline__ void rec_put(float* r, int64_t n, int f, float x) { __stcs(r + f * n, x); }
+__device__ __forceinline__ float rec_get(const float* r, int64_t n, int f) { return __ldcs(r + f * n); }
+
+// field value at p (the forward's arithmetic) with its record for slot j
+__device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, F3 v, int j, int64_t i, F3& E,
+                                               F3& B) {
+    const DevFields& F = A.a.f;
+    const int64_t n = A.a.n;
+    float* r = A.rec + (int64_t)j * kRecEB * n + i;
+    AxF ax, ay, az;
+    if (!axes32(F.B, p, ax, ay, az)) {
+        E = nanf3_();
+        B = E;
+        rec_put(r, n, 0, __int_as_float(-1));
+        return;
+    }
+    int nd[8];
+    tri_nodes(F.B, ax, ay, az, nd);
+    F3 Ex, Ey, Ez, Bx, By, Bz;
+    {
+        float4 e[8], b[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) ldg_node8(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c]);
+        tri_val_jac(e, ax, ay, az, E, Ex, Ey, Ez);
+        tri_val_jac(b, ax, ay, az, B, Bx, By, Bz);
+    }
+    const float q[kRecEB] = {__int_as_float(ax.i0), __int_as_float(ay.i0), __int_as_float(az.i0), ax.f, ay.f, az.f,
+                             v.x, v.y, v.z, E.x, E.y, E.z, B.x, B.y, B.z,
+                             Ex.x, Ex.y, Ex.z, Ey.x, Ey.y, Ey.z, Ez.x, Ez.y, Ez.z,
+                             Bx.x, Bx.y, Bx.z, By.x, By.y, By.z, Bz.x, Bz.y, Bz.z};
+#pragma unroll
+    for (int f = 0; f < kRecEB; ++f) rec_put(r, n, f, q[f]);
+}
+
+// adjoint of one velocity update from its record
+__device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, int j, int64_t i, float h, F3 lo, F3& lx,
+                                              Frame& fr) {
+    const DevField& g = A.a.f.B;
+    const int64_t n = A.a.n;
+    const float* r = A.rec + (int64_t)j * kRecEB * n + i;
+    float q[kRecEB];
+#pragma unroll
+    for (int f = 0; f < kRecEB; ++f) q[f] = rec_get(r, n, f);
+    const int ix = __float_as_int(q[0]);
+    if (ix < 0) {
+        lx = nanf3_();
+        return nanf3_();
+    }
+    F3 v{q[6], q[7], q[8]}, E{q[9], q[10], q[11]}, B{q[12], q[13], q[14]};
+    UAdj u = u_adjoint(v, E, B, h, lo);
+    lx = lx + jt({q[15], q[16], q[17]}, {q[18], q[19], q[20]}, {q[21], q[22], q[23]}, u.lE) +
+         jt({q[24], q[25], q[26]}, {q[27], q[28], q[29]}, {q[30], q[31], q[32]}, u.lB);
+    AxF ax, ay, az;
+    const int i0[3] = {ix, __float_as_int(q[1]), __float_as_int(q[2])};
+    AxF* axs[3] = {&ax, &ay, &az};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        axs[k]->i0 = i0[k];
+        axs[k]->i1 = (g.bc == TP_BC_PERIODIC && i0[k] + 1 == g.n[k]) ? 0 : i0[k] + 1;
+        axs[k]->f = q[3 + k];
+        axs[k]->ds = 0.0f;
+    }
+    float w[8];
+    if (scale_weights(ax, ay, az, u.lE, u.lB, fr, w)) {
+        int nd[8];
+        tri_nodes(g, ax, ay, az, nd);
+        scatter<2>(A.g_eb, nd, w, u.lE, u.lB);
+    }
+    return u.lv;
+}
+
+__device__ __forceinline__ int seg_steps(const AdjArgs& A, int64_t s) {
+    const int64_t k0 = s * A.K;
+    return (int)((A.nt - k0 < A.K) ? A.nt - k0 : A.K);
+}
+
+__global__ void __launch_bounds__(256) k_adj_recompute_eb(AdjArgs A, int64_t s) {
+    const BorisArgs& a = A.a;
+    const double dt = a.dt;
+    const float dth = (float)dt, dtl = (float)(dt - (double)dth);
+    const float h = vfac<false>(a, dt);
+    const int m = seg_steps(A, s);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        CPos p;
+        CV v;
+        load_ck(A, s, i, p, v);
+        for (int j = 0; j < m; ++j) {
+            F3 E, B;
+            record_step_eb(A, p, v.h, j, i, E, B);
+            v = vel32h<false>(v, E, B, a, h);
+            cpos_push_cv(a, p, v, dth, dtl);
+        }
+        if (s == A.S - 1) {  // the final save's update, at (x_N, v_{N-1/2})
+            F3 E, B;
+            record_step_eb(A, p, v.h, m, i, E, B);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
+    const BorisArgs& a = A.a;
+    const double dt = a.dt;
+    const float dtf = (float)dt;
+    const float h = vfac<false>(a, dt);
+    const int G = A.G;
+    const int m = seg_steps(A, s);
+    const int64_t n = a.n;
+    int mx = INT_MIN;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        F3 lx, lv;
+        Frame fr;
+        float* st = A.lam + i;
+        if (s == A.S - 1) {
+            // cotangent of the final save, normalised: lambda = g / 2^e
+            const double* gf = A.g_final + 6 * i;
+            double gm = fmax(fmax(fmax(fabs(gf[0]), fabs(gf[1])), fmax(fabs(gf[2]), fabs(gf[3]))),
+                             fmax(fabs(gf[4]), fabs(gf[5])));
+            fr.e = (gm > 0.0 && gm <= 1.0e300) ? ilogb(gm) : 0;
+            fr.mx = INT_MIN;
+            frame_set(fr, G);
+            const double is = ldexp(1.0, -fr.e);
+            lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
+            lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
+            lv = reverse_step_eb(A, m, i, vfac<false>(a, A.dt_final), lv, lx, fr);
+            renorm(lx, lv, fr, G);
+        } else {
+            lx = {st[0], st[n], st[2 * n]};
+            lv = {st[3 * n], st[4 * n], st[5 * n]};
+            fr.e = __float_as_int(st[6 * n]);
+            fr.mx = __float_as_int(st[7 * n]);
+            frame_set(fr, G);
+        }
+        for (int j = m - 1; j >= 0; --j) {
+            F3 lo = lv + dtf * lx;
+            lv = reverse_step_eb(A, j, i, h, lo, lx, fr);
+            renorm(lx, lv, fr, G);
+        }
+        if (s == 0) {
+            // initial half step back, v_{-1/2} = U(v_0, x_0, -dt/2)
+            const double* u0 = a.u0 + 6 * i;
+            CPos p0;
+            cpos_init(a, p0, u0);
+            CV v0 = cv_from(u0 + 3);
+            lv = adj_step_eb(A, p0, v0.h, vfac<false>(a, -0.5 * dt), lv, lx, fr);
+            double* go = A.g_u0 + 6 * i;
+            go[0] = fr.s * lx.x;
+            go[1] = fr.s * lx.y;
+            go[2] = fr.s * lx.z;
+            go[3] = fr.s * lv.x;
+            go[4] = fr.s * lv.y;
+            go[5] = fr.s * lv.z;
+            mx = max(mx, fr.mx);
+        } else {
+            st[0] = lx.x;
+            st[n] = lx.y;
+            st[2 * n] = lx.z;
+            st[3 * n] = lv.x;
+            st[4 * n] = lv.y;
+            st[5 * n] = lv.z;
+            st[6 * n] = __int_as_float(fr.e);
+            st[7 * n] = __int_as_float(fr.mx);
+        }
+    }
+    if (s == 0) {
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if ((threadIdx.x & 31) == 0 && mx != INT_MIN) atomicMax(A.need, mx);
+    }
+}
+
+// sum of a node-gradient table (stored scaled by 2^-G) into out[0..2]
+__global__ void k_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out) {
     double sx = 0.0, sy = 0.0, sz = 0.0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nodes;
          k += (int64_t)gridDim.x * blockDim.x) {
@@ -503,19 +776,19 @@ __global__ void k_table_sum(const float4* tab, int64_t nodes, int stride, int of
     }
     __syncthreads();
     if (threadIdx.x < 3) {
-        double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += part[threadIdx.x][w];
-        atomicAdd(out + threadIdx.x, s);
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, ldexp(t, G));
     }
 }
 
-__global__ void k_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out) {
+__global__ void k_table_unpack(const float4* tab, int64_t nodes, int stride, int off, int G, double* out) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nodes) return;
     float4 q = tab[k * stride + off];
-    out[3 * k + 0] = q.x;
-    out[3 * k + 1] = q.y;
-    out[3 * k + 2] = q.z;
+    out[3 * k + 0] = ldexp((double)q.x, G);
+    out[3 * k + 1] = ldexp((double)q.y, G);
+    out[3 * k + 2] = ldexp((double)q.z, G);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -534,28 +807,41 @@ cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c,
 }
 
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
-    const void* k = fk == FK_EBGRID    ? (const void*)k_adj_backward<FK_EBGRID>
-                    : fk == FK_ANALYTIC ? (const void*)k_adj_backward<FK_ANALYTIC>
-                                        : (const void*)k_adj_backward<FK_GENERIC>;
+    if (fk == FK_EBGRID) {  // two kernels per segment, last segment first
+        for (int64_t seg = a.S - 1; seg >= 0; --seg) {
+            k_adj_recompute_eb<<<c.grid, c.block, 0, s>>>(a, seg);
+            k_adj_reverse_eb<<<c.grid, c.block, 0, s>>>(a, seg);
+        }
+        return cudaGetLastError();
+    }
+    const void* k = fk == FK_ANALYTIC ? (const void*)k_adj_backward<FK_ANALYTIC>
+                                      : (const void*)k_adj_backward<FK_GENERIC>;
     void* args[] = {const_cast<AdjArgs*>(&a)};
     return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
 }
 
-cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out,
+// float words of the per-step records of one segment and of the cotangent
+// state kept between segments
+int64_t adjoint_record_words(int fk, int64_t K, int64_t n) {
+    return fk == FK_EBGRID ? (K + 1) * kRecEB * n : K * kRec * n;
+}
+int64_t adjoint_state_words(int fk, int64_t n) { return fk == FK_EBGRID ? 8 * n : 0; }
+
+cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,
                              cudaStream_t s) {
     if (nodes <= 0) return cudaSuccess;
     const int block = 256;
     int64_t g = (nodes + block - 1) / block;
     if (g > 148 * 8) g = 148 * 8;
-    k_table_sum<<<(unsigned)g, block, 0, s>>>(tab, nodes, stride, off, out);
+    k_table_sum<<<(unsigned)g, block, 0, s>>>(tab, nodes, stride, off, G, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out,
+cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,
                                 cudaStream_t s) {
     if (nodes <= 0) return cudaSuccess;
     const int block = 256;
-    k_table_unpack<<<(unsigned)((nodes + block - 1) / block), block, 0, s>>>(tab, nodes, stride, off, out);
+    k_table_unpack<<<(unsigned)((nodes + block - 1) / block), block, 0, s>>>(tab, nodes, stride, off, G, out);
     return cudaGetLastError();
 }
 

@@ -1068,10 +1068,13 @@ struct tp_tape {
     float4* d_gE = nullptr;
     float4* d_gB = nullptr;
     double* d_gparam = nullptr;
+    int32_t* d_need = nullptr;
+    float* d_lam = nullptr;
+    int G = 0;  // scale exponent of the node-gradient tables, kept for the next pass
     int64_t bytes = 0;
     ~tp_tape() {
         for (void* q : {(void*)d_ckpt, (void*)d_u0, (void*)d_rec, (void*)d_geb, (void*)d_gE, (void*)d_gB,
-                        (void*)d_gparam})
+                        (void*)d_gparam, (void*)d_need, (void*)d_lam})
             if (q) cudaFree(q);
     }
 };
@@ -1146,6 +1149,7 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
         if (e == cudaSuccess) e = tape_alloc(t, &t->d_u0, (size_t)n * 6 * sizeof(double));
     }
     if (e == cudaSuccess) e = tape_alloc(t, &t->d_gparam, 6 * sizeof(double));
+    if (e == cudaSuccess) e = tape_alloc(t, &t->d_need, sizeof(int32_t));
     if (e != cudaSuccess) {
         delete t;
         return cuda_fail(ctx, e, "adjoint tape");
@@ -1169,16 +1173,19 @@ int adjoint_forward_on(tp_tape* t, const double* u0_dev, double* ufinal_dev, cud
     return TP_OK;
 }
 
-int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, float* gE_dev, float* gB_dev,
+int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, double* gE_dev, double* gB_dev,
                         double* gparam_dev, cudaStream_t s) {
     tp_ctx* ctx = t->ctx;
     AdjArgs& A = t->A;
     if (t->E->id != t->E_id || t->B->id != t->B_id)
-        return fail(ctx, TP_E_ARG, "a field was updated after the tape was recorded");
+        return fail(ctx, TP_E_ARG, "a field was updated after the tape was recorded (rerun the tape)");
     const int64_t n = A.a.n;
     cudaError_t e = cudaSuccess;
     // segment records and node-gradient tables: allocated on first use, kept
-    if (!t->d_rec && n > 0) e = tape_alloc(t, &t->d_rec, (size_t)A.K * 9 * (size_t)n * sizeof(float));
+    if (!t->d_rec && n > 0)
+        e = tape_alloc(t, &t->d_rec, (size_t)adjoint_record_words(t->fk, A.K, n) * sizeof(float));
+    const int64_t sw = adjoint_state_words(t->fk, n);
+    if (e == cudaSuccess && sw > 0 && !t->d_lam) e = tape_alloc(t, &t->d_lam, (size_t)sw * sizeof(float));
     const bool eb = t->fk == FK_EBGRID;
     const bool gridE = !eb && t->E->desc.kind == TP_FIELD_GRID;
     const bool gridB = !eb && t->B->desc.kind == TP_FIELD_GRID;
@@ -1187,31 +1194,51 @@ int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, f
     if (e == cudaSuccess && gridB && !t->d_gB) e = tape_alloc(t, &t->d_gB, (size_t)t->nodes_B * sizeof(float4));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint scratch");
     A.rec = t->d_rec;
+    A.lam = t->d_lam;
     A.g_eb = t->d_geb;
     A.g_E = t->d_gE;
     A.g_B = t->d_gB;
     A.g_final = gfinal_dev;
     A.g_u0 = gu0_dev;
-    if (eb) e = cudaMemsetAsync(t->d_geb, 0, (size_t)t->nodes_B * 2 * sizeof(float4), s);
-    if (e == cudaSuccess && gridE) e = cudaMemsetAsync(t->d_gE, 0, (size_t)t->nodes_E * sizeof(float4), s);
-    if (e == cudaSuccess && gridB) e = cudaMemsetAsync(t->d_gB, 0, (size_t)t->nodes_B * sizeof(float4), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(t->d_gparam, 0, 6 * sizeof(double), s);
-    if (e == cudaSuccess && n > 0) e = launch_adjoint_backward(A, t->fk, t->cfg, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint backward launch");
+    A.need = t->d_need;
+    // A pass whose node contributions reached 2^(G+100) could overflow the
+    // float32 tables (and one far below 2^(G-100) loses their low bits): it
+    // is repeated with G moved to the needed exponent minus 90.  The chosen
+    // G is kept, so repeated passes of one problem run once.
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        A.G = t->G;
+        if (eb) e = cudaMemsetAsync(t->d_geb, 0, (size_t)t->nodes_B * 2 * sizeof(float4), s);
+        if (e == cudaSuccess && gridE) e = cudaMemsetAsync(t->d_gE, 0, (size_t)t->nodes_E * sizeof(float4), s);
+        if (e == cudaSuccess && gridB) e = cudaMemsetAsync(t->d_gB, 0, (size_t)t->nodes_B * sizeof(float4), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(t->d_gparam, 0, 6 * sizeof(double), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(t->d_need, 0x80, sizeof(int32_t), s);  // very negative
+        if (e == cudaSuccess && n > 0) e = launch_adjoint_backward(A, t->fk, t->cfg, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint backward launch");
+        if (!eb && !gridE && !gridB) break;  // no tables
+        int32_t need = 0;
+        e = cudaMemcpyAsync(&need, t->d_need, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint backward");
+        if (need < -(1 << 30)) break;  // no node contribution at all
+        if (need - t->G <= 100 && need - t->G >= -100) break;
+        t->G = need - 90;
+        if (attempt == 2) return fail(ctx, TP_E_OVERFLOW, "node-gradient range could not be fitted");
+    }
+    const int G = t->G;
     // grid parameter (uniform offset) gradients are the node-gradient sums
     if (eb) {
-        e = launch_table_sum(t->d_geb, t->nodes_B, 2, 0, t->d_gparam, s);
-        if (e == cudaSuccess) e = launch_table_sum(t->d_geb, t->nodes_B, 2, 1, t->d_gparam + 3, s);
-        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 0, gE_dev, s);
-        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 1, gB_dev, s);
+        e = launch_table_sum(t->d_geb, t->nodes_B, 2, 0, G, t->d_gparam, s);
+        if (e == cudaSuccess) e = launch_table_sum(t->d_geb, t->nodes_B, 2, 1, G, t->d_gparam + 3, s);
+        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 0, G, gE_dev, s);
+        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_geb, t->nodes_B, 2, 1, G, gB_dev, s);
     }
     if (e == cudaSuccess && gridE) {
-        e = launch_table_sum(t->d_gE, t->nodes_E, 1, 0, t->d_gparam, s);
-        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_gE, t->nodes_E, 1, 0, gE_dev, s);
+        e = launch_table_sum(t->d_gE, t->nodes_E, 1, 0, G, t->d_gparam, s);
+        if (e == cudaSuccess && gE_dev) e = launch_table_unpack(t->d_gE, t->nodes_E, 1, 0, G, gE_dev, s);
     }
     if (e == cudaSuccess && gridB) {
-        e = launch_table_sum(t->d_gB, t->nodes_B, 1, 0, t->d_gparam + 3, s);
-        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_gB, t->nodes_B, 1, 0, gB_dev, s);
+        e = launch_table_sum(t->d_gB, t->nodes_B, 1, 0, G, t->d_gparam + 3, s);
+        if (e == cudaSuccess && gB_dev) e = launch_table_unpack(t->d_gB, t->nodes_B, 1, 0, G, gB_dev, s);
     }
     if (e == cudaSuccess && gparam_dev)
         e = cudaMemcpyAsync(gparam_dev, t->d_gparam, 6 * sizeof(double), cudaMemcpyDefault, s);
@@ -1241,8 +1268,8 @@ int tp_adjoint_forward_device(tp_ctx* ctx, const tp_adj_desc* d, const tp_field*
     return TP_OK;
 }
 
-int tp_adjoint_backward_device(tp_tape* t, const double* grad_final, double* grad_u0, float* grad_E,
-                               float* grad_B, double* grad_param, void* stream) {
+int tp_adjoint_backward_device(tp_tape* t, const double* grad_final, double* grad_u0, double* grad_E,
+                               double* grad_B, double* grad_param, void* stream) {
     if (!t) return TP_E_ARG;
     if (t->A.a.n > 0 && (!grad_final || !grad_u0)) return fail(t->ctx, TP_E_ARG, "null gradient buffer");
     DeviceGuard g(t->ctx->device);
@@ -1278,7 +1305,7 @@ int tp_adjoint_forward(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, con
     return TP_OK;
 }
 
-int tp_adjoint_backward(tp_tape* t, const double* grad_final, double* grad_u0, float* grad_E, float* grad_B,
+int tp_adjoint_backward(tp_tape* t, const double* grad_final, double* grad_u0, double* grad_E, double* grad_B,
                         double* grad_param) {
     if (!t) return TP_E_ARG;
     tp_ctx* ctx = t->ctx;
@@ -1291,20 +1318,20 @@ int tp_adjoint_backward(tp_tape* t, const double* grad_final, double* grad_u0, f
     DBuf gf, gu, ge, gb, gp;
     cudaError_t e = gf.alloc((size_t)n * 6 * sizeof(double));
     if (e == cudaSuccess) e = gu.alloc((size_t)n * 6 * sizeof(double));
-    if (e == cudaSuccess && grad_E && nE) e = ge.alloc((size_t)nE * 3 * sizeof(float));
-    if (e == cudaSuccess && grad_B && nB) e = gb.alloc((size_t)nB * 3 * sizeof(float));
+    if (e == cudaSuccess && grad_E && nE) e = ge.alloc((size_t)nE * 3 * sizeof(double));
+    if (e == cudaSuccess && grad_B && nB) e = gb.alloc((size_t)nB * 3 * sizeof(double));
     if (e == cudaSuccess) e = gp.alloc(6 * sizeof(double));
     if (e == cudaSuccess && n > 0)
         e = cudaMemcpyAsync(gf.p, grad_final, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint buffers");
-    int st = adjoint_backward_on(t, gf.as<double>(), gu.as<double>(), ge.as<float>(), gb.as<float>(),
+    int st = adjoint_backward_on(t, gf.as<double>(), gu.as<double>(), ge.as<double>(), gb.as<double>(),
                                  gp.as<double>(), ctx->stream);
     if (st != TP_OK) return st;
     if (n > 0) e = cudaMemcpyAsync(grad_u0, gu.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && ge.p)
-        e = cudaMemcpyAsync(grad_E, ge.p, (size_t)nE * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpyAsync(grad_E, ge.p, (size_t)nE * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && gb.p)
-        e = cudaMemcpyAsync(grad_B, gb.p, (size_t)nB * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpyAsync(grad_B, gb.p, (size_t)nB * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && grad_param)
         e = cudaMemcpyAsync(grad_param, gp.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

@@ -67,17 +67,24 @@ struct AdjArgs {
     float4* g_E;           // per-field node-gradient tables (1 float4 per node) or null
     float4* g_B;
     double* g_param;       // 6: analytic-field parameter gradients (E then B)
+    int32_t G;             // node-gradient tables hold float32 values times 2^G
+    int32_t pad;
+    int32_t* need;         // device: largest node-contribution exponent of the pass
+    float* lam;            // [8][n] cotangent state between segments (segmented path)
 };
 
 // field configuration of an adjoint run (FK_ANALYTIC / FK_EBGRID / FK_GENERIC)
 int adjoint_field_config(const DevFields& f);
 cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
-// sum of a node-gradient table into out[0..2] (+=), entries k*stride + off
-cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, double* out,
+int64_t adjoint_record_words(int fk, int64_t K, int64_t n);
+int64_t adjoint_state_words(int fk, int64_t n);
+// sum of a node-gradient table (values times 2^-G) into out[0..2] (+=),
+// entries k*stride + off
+cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,
                              cudaStream_t s);
-// node-gradient table -> user layout out[3*k + c] (float32)
-cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, float* out,
+// node-gradient table -> user layout out[3*k + c] (float64, scaled back by 2^G)
+cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,
                                 cudaStream_t s);
 
 cudaError_t launch_boris_fp64(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s);

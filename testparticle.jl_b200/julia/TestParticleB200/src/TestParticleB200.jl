@@ -392,11 +392,11 @@ function ChainRulesCore.rrule(::typeof(boris_final_state), U0::Matrix{Float64}, 
     function boris_final_state_pullback(dUN)
         G = Matrix{Float64}(ChainRulesCore.unthunk(dUN))
         dU0 = Matrix{Float64}(undef, 6, t.n)
-        gE = unwrap(E) isa B200Grid ? Array{Float32}(undef, size(unwrap(E).A)) : nothing
-        gB = unwrap(B) isa B200Grid ? Array{Float32}(undef, size(unwrap(B).A)) : nothing
+        gE = unwrap(E) isa B200Grid ? Array{Float64}(undef, size(unwrap(E).A)) : nothing
+        gB = unwrap(B) isa B200Grid ? Array{Float64}(undef, size(unwrap(B).A)) : nothing
         gp = Vector{Float64}(undef, 6)
         st = ccall((:tp_adjoint_backward, libtpb200), Cint,
-            (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float32}, Ptr{Float32}, Ptr{Float64}),
+            (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
             t.tape, G, dU0, isnothing(gE) ? C_NULL : gE, isnothing(gB) ? C_NULL : gB, gp)
         check(t.ctx, st, "tp_adjoint_backward")
         return (ChainRulesCore.NoTangent(), dU0, field_cotangent(unwrap(E), gE, gp[1:3]),

@@ -228,7 +228,7 @@ def _grid_nodes(f) -> int:
 @dataclass
 class AdjointGrads:
     u0: np.ndarray                 # dL/du0, N x 6
-    E: object                      # dL/d(E node values), (3, nx, ny, nz) float32, or None
+    E: object                      # dL/d(E node values), (3, nx, ny, nz) float64, or None
     B: object
     param: np.ndarray              # 6: (E, B) dipole moment or uniform-offset gradients
 
@@ -250,7 +250,7 @@ class Tape:
         out = []
         for f in (self.E, self.B):
             nodes = _grid_nodes(f) if fields else 0
-            out.append(np.empty(3 * nodes, dtype=np.float32) if nodes else None)
+            out.append(np.empty(3 * nodes, dtype=np.float64) if nodes else None)
         code = lib.tp_adjoint_backward(self.handle, _ptr(g), _ptr(gu), _ptr(out[0]), _ptr(out[1]), _ptr(gp))
         _check(lib, self.ctx.handle, code, "tp_adjoint_backward")
         shaped = [None if a is None else a.reshape(f.data.shape, order="F") for a, f in zip(out, (self.E, self.B))]
