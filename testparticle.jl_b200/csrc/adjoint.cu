@@ -168,6 +168,13 @@ __device__ __forceinline__ void red_add3(float4* p, float a, float b, float c) {
                  : "memory");
 }
 
+// the same with an L2 eviction-priority policy
+__device__ __forceinline__ void red_add3(float4* p, float a, float b, float c, uint64_t pol) {
+    asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(a), "f"(b),
+                 "f"(c), "f"(0.0f), "l"(pol)
+                 : "memory");
+}
+
 // Scatter w_c * la (and w_c * lb when NV == 2) to the 8 corner nodes of a
 // gradient table with NV float4 entries per node.  Warp aggregation: lanes
 // whose particles sit in the same cell update the same 8 nodes, so
@@ -177,8 +184,10 @@ __device__ __forceinline__ void red_add3(float4* p, float a, float b, float c) {
 //  * for groups of 4 or more lanes the group's lowest lane pulls the others'
 //    contributions by shuffles and adds the group sum;
 //  * small groups add individually (the adds are atomic either way).
-template <int NV>
-__device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w, F3 la, F3 lb) {
+#define RED3(p, a, b, c) (POL ? red_add3(p, a, b, c, pol) : red_add3(p, a, b, c))
+template <int NV, bool POL = false>
+__device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w, F3 la, F3 lb,
+                                        uint64_t pol = 0) {
     const unsigned act = __activemask();
     const unsigned me = 1u << (threadIdx.x & 31);
     const unsigned peers = __match_any_sync(act, nd[0]);
@@ -187,8 +196,8 @@ __device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w
     if (gmax == 1) {
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            red_add3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
-            if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
+            RED3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
+            if (NV == 2) RED3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
         }
         return;
     }
@@ -201,8 +210,8 @@ __device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w
 #pragma unroll
                 for (int k = 0; k < 3 * NV; ++k) q[k] += __shfl_xor_sync(0xffffffffu, q[k], o);
             if (me == 1u) {
-                red_add3(G + (int64_t)NV * nd[c], q[0], q[1], q[2]);
-                if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, q[3], q[4], q[5]);
+                RED3(G + (int64_t)NV * nd[c], q[0], q[1], q[2]);
+                if (NV == 2) RED3(G + 2 * (int64_t)nd[c] + 1, q[3], q[4], q[5]);
             }
         }
         return;
@@ -225,18 +234,20 @@ __device__ __forceinline__ void scatter(float4* G, const int* nd, const float* w
                 }
             }
             if (leader) {
-                red_add3(G + (int64_t)NV * nd[c], acc[0], acc[1], acc[2]);
-                if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, acc[3], acc[4], acc[5]);
+                RED3(G + (int64_t)NV * nd[c], acc[0], acc[1], acc[2]);
+                if (NV == 2) RED3(G + 2 * (int64_t)nd[c] + 1, acc[3], acc[4], acc[5]);
             }
         }
         return;
     }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        red_add3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
-        if (NV == 2) red_add3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
+        RED3(G + (int64_t)NV * nd[c], w[c] * la.x, w[c] * la.y, w[c] * la.z);
+        if (NV == 2) RED3(G + 2 * (int64_t)nd[c] + 1, w[c] * lb.x, w[c] * lb.y, w[c] * lb.z);
     }
 }
+
+#undef RED3
 
 // ----------------------------------------------------- cotangent frame
 // lambda_true = lambda * 2^e; node contributions are scaled by f = 2^(e - G)
@@ -582,74 +593,78 @@ __global__ void __launch_bounds__(256) k_adj_backward(AdjArgs A) {
 // table.  Each kernel's random-access working set is one 32-byte-per-node
 // table, which fits in L2; the records stream through with evict-first hints.
 constexpr int kRecEB = 33;  // cell xyz (int; x = -1 outside the grid), fraction xyz, v, E, B, dE/dx.., dB/dx..
+constexpr int kRecEB4 = 9;  // as float4 words (3 floats of padding)
 
-__device__ __forceinline__ void rec_put(float* r, int64_t n, int f, float x) { __stcs(r + f * n, x); }
-__device__ __forceinline__ float rec_get(const float* r, int64_t n, int f) { return __ldcs(r + f * n); }
-
-// field value at p (the forward's arithmetic) with its record for slot j
-__device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, F3 v, int j, int64_t i, F3& E,
-                                               F3& B) {
+// field value at p (the forward's arithmetic) with its record for slot j;
+// the field table is read with an evict-last L2 policy and the record is
+// written with streaming (evict-first) stores
+__device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, F3 v, int j, int64_t i,
+                                               uint64_t pol, F3& E, F3& B) {
     const DevFields& F = A.a.f;
     const int64_t n = A.a.n;
-    float* r = A.rec + (int64_t)j * kRecEB * n + i;
+    float4* r = reinterpret_cast<float4*>(A.rec) + (int64_t)j * kRecEB4 * n + i;
     AxF ax, ay, az;
     if (!axes32(F.B, p, ax, ay, az)) {
         E = nanf3_();
         B = E;
-        rec_put(r, n, 0, __int_as_float(-1));
+        __stcs(r, make_float4(__int_as_float(-1), 0.0f, 0.0f, 0.0f));
         return;
     }
     int nd[8];
     tri_nodes(F.B, ax, ay, az, nd);
-    F3 Ex, Ey, Ez, Bx, By, Bz;
-    {
-        float4 e[8], b[8];
+    float4 e[8], b[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) ldg_node8(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c]);
-        tri_val_jac(e, ax, ay, az, E, Ex, Ey, Ez);
-        tri_val_jac(b, ax, ay, az, B, Bx, By, Bz);
-    }
-    const float q[kRecEB] = {__int_as_float(ax.i0), __int_as_float(ay.i0), __int_as_float(az.i0), ax.f, ay.f, az.f,
-                             v.x, v.y, v.z, E.x, E.y, E.z, B.x, B.y, B.z,
-                             Ex.x, Ex.y, Ex.z, Ey.x, Ey.y, Ey.z, Ez.x, Ez.y, Ez.z,
-                             Bx.x, Bx.y, Bx.z, By.x, By.y, By.z, Bz.x, Bz.y, Bz.z};
-#pragma unroll
-    for (int f = 0; f < kRecEB; ++f) rec_put(r, n, f, q[f]);
+    for (int c = 0; c < 8; ++c) ldg_node8_pol(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c], pol);
+    __stcs(r, make_float4(__int_as_float(ax.i0), __int_as_float(ay.i0), __int_as_float(az.i0), ax.f));
+    __stcs(r + n, make_float4(ay.f, az.f, v.x, v.y));
+    F3 Ex, Ey, Ez;
+    tri_val_jac(e, ax, ay, az, E, Ex, Ey, Ez);
+    __stcs(r + 2 * n, make_float4(v.z, E.x, E.y, E.z));
+    F3 Bx, By, Bz;
+    tri_val_jac(b, ax, ay, az, B, Bx, By, Bz);
+    __stcs(r + 3 * n, make_float4(B.x, B.y, B.z, Ex.x));
+    __stcs(r + 4 * n, make_float4(Ex.y, Ex.z, Ey.x, Ey.y));
+    __stcs(r + 5 * n, make_float4(Ey.z, Ez.x, Ez.y, Ez.z));
+    __stcs(r + 6 * n, make_float4(Bx.x, Bx.y, Bx.z, By.x));
+    __stcs(r + 7 * n, make_float4(By.y, By.z, Bz.x, Bz.y));
+    __stcs(r + 8 * n, make_float4(Bz.z, 0.0f, 0.0f, 0.0f));
 }
 
-// adjoint of one velocity update from its record
+// adjoint of one velocity update from its record; node gradients are added
+// with an evict-last L2 policy
 __device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, int j, int64_t i, float h, F3 lo, F3& lx,
-                                              Frame& fr) {
+                                              Frame& fr, uint64_t pol) {
     const DevField& g = A.a.f.B;
     const int64_t n = A.a.n;
-    const float* r = A.rec + (int64_t)j * kRecEB * n + i;
-    float q[kRecEB];
+    const float4* r = reinterpret_cast<const float4*>(A.rec) + (int64_t)j * kRecEB4 * n + i;
+    float4 q[kRecEB4];
 #pragma unroll
-    for (int f = 0; f < kRecEB; ++f) q[f] = rec_get(r, n, f);
-    const int ix = __float_as_int(q[0]);
+    for (int k = 0; k < kRecEB4; ++k) q[k] = __ldcs(r + k * n);
+    const int ix = __float_as_int(q[0].x);
     if (ix < 0) {
         lx = nanf3_();
         return nanf3_();
     }
-    F3 v{q[6], q[7], q[8]}, E{q[9], q[10], q[11]}, B{q[12], q[13], q[14]};
+    F3 v{q[1].z, q[1].w, q[2].x}, E{q[2].y, q[2].z, q[2].w}, B{q[3].x, q[3].y, q[3].z};
     UAdj u = u_adjoint(v, E, B, h, lo);
-    lx = lx + jt({q[15], q[16], q[17]}, {q[18], q[19], q[20]}, {q[21], q[22], q[23]}, u.lE) +
-         jt({q[24], q[25], q[26]}, {q[27], q[28], q[29]}, {q[30], q[31], q[32]}, u.lB);
+    lx = lx + jt({q[3].w, q[4].x, q[4].y}, {q[4].z, q[4].w, q[5].x}, {q[5].y, q[5].z, q[5].w}, u.lE) +
+         jt({q[6].x, q[6].y, q[6].z}, {q[6].w, q[7].x, q[7].y}, {q[7].z, q[7].w, q[8].x}, u.lB);
     AxF ax, ay, az;
-    const int i0[3] = {ix, __float_as_int(q[1]), __float_as_int(q[2])};
+    const int i0[3] = {ix, __float_as_int(q[0].y), __float_as_int(q[0].z)};
+    const float fr3[3] = {q[0].w, q[1].x, q[1].y};
     AxF* axs[3] = {&ax, &ay, &az};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         axs[k]->i0 = i0[k];
         axs[k]->i1 = (g.bc == TP_BC_PERIODIC && i0[k] + 1 == g.n[k]) ? 0 : i0[k] + 1;
-        axs[k]->f = q[3 + k];
+        axs[k]->f = fr3[k];
         axs[k]->ds = 0.0f;
     }
     float w[8];
     if (scale_weights(ax, ay, az, u.lE, u.lB, fr, w)) {
         int nd[8];
         tri_nodes(g, ax, ay, az, nd);
-        scatter<2>(A.g_eb, nd, w, u.lE, u.lB);
+        scatter<2, true>(A.g_eb, nd, w, u.lE, u.lB, pol);
     }
     return u.lv;
 }
@@ -659,12 +674,13 @@ __device__ __forceinline__ int seg_steps(const AdjArgs& A, int64_t s) {
     return (int)((A.nt - k0 < A.K) ? A.nt - k0 : A.K);
 }
 
-__global__ void __launch_bounds__(256) k_adj_recompute_eb(AdjArgs A, int64_t s) {
+__global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t s) {
     const BorisArgs& a = A.a;
     const double dt = a.dt;
     const float dth = (float)dt, dtl = (float)(dt - (double)dth);
     const float h = vfac<false>(a, dt);
     const int m = seg_steps(A, s);
+    const uint64_t pol = l2_evict_last();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
          i += (int64_t)gridDim.x * blockDim.x) {
         CPos p;
@@ -672,13 +688,13 @@ __global__ void __launch_bounds__(256) k_adj_recompute_eb(AdjArgs A, int64_t s) 
         load_ck(A, s, i, p, v);
         for (int j = 0; j < m; ++j) {
             F3 E, B;
-            record_step_eb(A, p, v.h, j, i, E, B);
+            record_step_eb(A, p, v.h, j, i, pol, E, B);
             v = vel32h<false>(v, E, B, a, h);
             cpos_push_cv(a, p, v, dth, dtl);
         }
         if (s == A.S - 1) {  // the final save's update, at (x_N, v_{N-1/2})
             F3 E, B;
-            record_step_eb(A, p, v.h, m, i, E, B);
+            record_step_eb(A, p, v.h, m, i, pol, E, B);
         }
     }
 }
@@ -691,6 +707,7 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
     const int G = A.G;
     const int m = seg_steps(A, s);
     const int64_t n = a.n;
+    const uint64_t pol = l2_evict_last();
     int mx = INT_MIN;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -708,7 +725,7 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
             const double is = ldexp(1.0, -fr.e);
             lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
             lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
-            lv = reverse_step_eb(A, m, i, vfac<false>(a, A.dt_final), lv, lx, fr);
+            lv = reverse_step_eb(A, m, i, vfac<false>(a, A.dt_final), lv, lx, fr, pol);
             renorm(lx, lv, fr, G);
         } else {
             lx = {st[0], st[n], st[2 * n]};
@@ -719,7 +736,7 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
         }
         for (int j = m - 1; j >= 0; --j) {
             F3 lo = lv + dtf * lx;
-            lv = reverse_step_eb(A, j, i, h, lo, lx, fr);
+            lv = reverse_step_eb(A, j, i, h, lo, lx, fr, pol);
             renorm(lx, lv, fr, G);
         }
         if (s == 0) {
@@ -823,7 +840,7 @@ cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c
 // float words of the per-step records of one segment and of the cotangent
 // state kept between segments
 int64_t adjoint_record_words(int fk, int64_t K, int64_t n) {
-    return fk == FK_EBGRID ? (K + 1) * kRecEB * n : K * kRec * n;
+    return fk == FK_EBGRID ? (K + 1) * kRecEB4 * 4 * n : K * kRec * n;
 }
 int64_t adjoint_state_words(int fk, int64_t n) { return fk == FK_EBGRID ? 8 * n : 0; }
 

@@ -182,6 +182,21 @@ __device__ __forceinline__ void ldg_node8(const float4* p, float4& e, float4& b)
         : "l"(p));
 }
 
+// The same load with an L2 eviction-priority policy (createpolicy), for
+// kernels that stream other data past the table.
+__device__ __forceinline__ void ldg_node8_pol(const float4* p, float4& e, float4& b, uint64_t pol) {
+    asm("ld.global.nc.L2::cache_hint.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p), "l"(pol));
+}
+
+// L2 policy: keep these lines in preference to others
+__device__ __forceinline__ uint64_t l2_evict_last() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 __device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, F3 v101, F3 v011,
                                    F3 v111, const AxF& ax, const AxF& ay, const AxF& az) {
     F3 o;

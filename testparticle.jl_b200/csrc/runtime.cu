@@ -1138,7 +1138,8 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
     t->fk = adjoint_field_config(A.a.f);
     t->nodes_E = E->nodes;
     t->nodes_B = B->nodes;
-    st = pick_launch(ctx, n, r->block, false, 0, t->cfg);
+    // blocks of at most 128 threads (the segment kernels' launch bounds)
+    st = pick_launch(ctx, n, r->block > 0 && r->block < 128 ? r->block : 128, false, 0, t->cfg);
     if (st != TP_OK) {
         delete t;
         return st;
