@@ -630,16 +630,40 @@ __device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, 
     __stcs(r + 8 * n, make_float4(Bz.z, 0.0f, 0.0f, 0.0f));
 }
 
-// adjoint of one velocity update from its record; node gradients are added
-// with an evict-last L2 policy
-__device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, int j, int64_t i, float h, F3 lo, F3& lx,
-                                              Frame& fr, uint64_t pol) {
-    const DevField& g = A.a.f.B;
+// L2 policy for data read once
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// Asynchronous copy of one step's record (kRecEB4 float4 words of particle i)
+// into this thread's shared-memory slot, as one cp.async group.
+__device__ __forceinline__ void rec_prefetch(const AdjArgs& A, int j, int64_t i, float4* slot, int stride,
+                                             uint64_t pol) {
     const int64_t n = A.a.n;
     const float4* r = reinterpret_cast<const float4*>(A.rec) + (int64_t)j * kRecEB4 * n + i;
+#pragma unroll
+    for (int k = 0; k < kRecEB4; ++k) {
+        unsigned d = (unsigned)__cvta_generic_to_shared(slot + k * stride);
+        asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(d), "l"(r + k * n),
+                     "l"(pol)
+                     : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// adjoint of one velocity update from its record (q: kRecEB4 words, `stride`
+// apart); node gradients are added with an evict-last L2 policy
+__device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, const float4* qp, int stride, float h, F3 lo,
+                                              F3& lx, Frame& fr, uint64_t pol) {
+    const DevField& g = A.a.f.B;
     float4 q[kRecEB4];
 #pragma unroll
-    for (int k = 0; k < kRecEB4; ++k) q[k] = __ldcs(r + k * n);
+    for (int k = 0; k < kRecEB4; ++k) q[k] = qp[k * stride];
     const int ix = __float_as_int(q[0].x);
     if (ix < 0) {
         lx = nanf3_();
@@ -699,7 +723,10 @@ __global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t 
     }
 }
 
-__global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
+constexpr int kRevStages = 3;  // records in flight per thread (shared memory ring)
+
+__global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s) {
+    extern __shared__ float4 ring[];  // [kRevStages][kRecEB4][blockDim.x]
     const BorisArgs& a = A.a;
     const double dt = a.dt;
     const float dtf = (float)dt;
@@ -707,10 +734,19 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
     const int G = A.G;
     const int m = seg_steps(A, s);
     const int64_t n = a.n;
-    const uint64_t pol = l2_evict_last();
+    const int stride = blockDim.x;
+    const uint64_t keep = l2_evict_last();
+    const uint64_t once = l2_evict_first();
     int mx = INT_MIN;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
+        // records m-1, m-2, ... stream into the ring ahead of their use
+#pragma unroll
+        for (int d = 0; d < kRevStages; ++d) {
+            const int j = m - 1 - d;
+            if (j >= 0) rec_prefetch(A, j, i, ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
+            cp_async_commit();
+        }
         F3 lx, lv;
         Frame fr;
         float* st = A.lam + i;
@@ -725,7 +761,9 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
             const double is = ldexp(1.0, -fr.e);
             lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
             lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
-            lv = reverse_step_eb(A, m, i, vfac<false>(a, A.dt_final), lv, lx, fr, pol);
+            // the final save's record (slot m) is read directly
+            const float4* r = reinterpret_cast<const float4*>(A.rec) + (int64_t)m * kRecEB4 * n + i;
+            lv = reverse_step_eb(A, r, (int)n, vfac<false>(a, A.dt_final), lv, lx, fr, keep);
             renorm(lx, lv, fr, G);
         } else {
             lx = {st[0], st[n], st[2 * n]};
@@ -735,10 +773,17 @@ __global__ void __launch_bounds__(256) k_adj_reverse_eb(AdjArgs A, int64_t s) {
             frame_set(fr, G);
         }
         for (int j = m - 1; j >= 0; --j) {
+            cp_async_wait<kRevStages - 1>();  // this thread's copy of record j has landed
             F3 lo = lv + dtf * lx;
-            lv = reverse_step_eb(A, j, i, h, lo, lx, fr, pol);
+            lv = reverse_step_eb(A, ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, h, lo, lx,
+                                 fr, keep);
             renorm(lx, lv, fr, G);
+            // refill the slot just consumed with record j - kRevStages
+            const int jn = j - kRevStages;
+            if (jn >= 0) rec_prefetch(A, jn, i, ring + (jn % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
+            cp_async_commit();
         }
+        cp_async_wait<0>();
         if (s == 0) {
             // initial half step back, v_{-1/2} = U(v_0, x_0, -dt/2)
             const double* u0 = a.u0 + 6 * i;
@@ -825,9 +870,12 @@ cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c,
 
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
     if (fk == FK_EBGRID) {  // two kernels per segment, last segment first
+        const size_t ring = (size_t)kRevStages * kRecEB4 * c.block * sizeof(float4);
+        cudaError_t e = cudaFuncSetAttribute(k_adj_reverse_eb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring);
+        if (e != cudaSuccess) return e;
         for (int64_t seg = a.S - 1; seg >= 0; --seg) {
             k_adj_recompute_eb<<<c.grid, c.block, 0, s>>>(a, seg);
-            k_adj_reverse_eb<<<c.grid, c.block, 0, s>>>(a, seg);
+            k_adj_reverse_eb<<<c.grid, c.block, ring, s>>>(a, seg);
         }
         return cudaGetLastError();
     }
