@@ -254,6 +254,8 @@ def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
     out = {"workload": w.name, "particles": n, "time_steps": nt}
     for name, alg, cap in (("multistep4_n2", tp.MultistepBoris4(2), 0), ("adaptive_0.1", tp.AdaptiveBoris(0.1), nt)):
         p32, p64 = _plan(tp, w, alg, "fp32c", ctx.device, cap), _plan(tp, w, alg, "fp64", ctx.device, cap)
+        shapes = {k: ctx.autotune(pl.desc, pl.E, pl.B, pl.u0, max_steps=200) for k, pl in (("fp32c", p32),
+                                                                                          ("fp64", p64))}
         run = DeviceRun(tp, torch, ctx, p32, dev, stream)
         ms32 = timed(torch, dist, dev, run, p32, 1, 1, flush)
         ps32 = run.particle_steps()
@@ -274,7 +276,7 @@ def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
         out[name] = {"fp32c": v32, "fp64": v64, "speedup_fp32c_over_fp64": v32 / v64,
                      "unit": "particle-steps/s", "fp32c_error_vs_fp64": _err_summary(_rel_err(fs32[ok], fs64[ok])),
                      "fp64_vs_fp64_1ulp_start": _err_summary(_rel_err(fs64b[okb], fs64[okb])),
-                     "both_success_fraction": float(ok.mean())}
+                     "both_success_fraction": float(ok.mean()), "autotune": shapes}
     return out
 
 
@@ -423,6 +425,9 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
     p32, p64 = _plan(tp, w, alg, "fp32c", local), _plan(tp, w, alg, "fp64", local)
+    # launch shapes chosen by the autotuner on a sample (untimed)
+    tune = {"fp32c": ctx.autotune(p32.desc, p32.E, p32.B, p32.u0, max_steps=200),
+            "fp64": ctx.autotune(p64.desc, p64.E, p64.B, p64.u0, max_steps=200)}
     run = DeviceRun(tp, torch, ctx, p32, dev, stream)
 
     # ---- FP32C (headline), clocks sampled during the timed region
@@ -524,6 +529,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps,
+            "autotune": tune,
             "clocks": clocks,
             "legs": legs,
         }

@@ -246,6 +246,41 @@ int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* desc,
                         int8_t* retcode, int64_t* nsteps, int32_t* status,
                         void* stream);
 
+/* ---- launch tuning and CUDA graphs ------------------------------------------
+ * No reference counterpart (KernelAbstractions picks its workgroup size).
+ * tp_autotune times every candidate launch shape -- block sizes 64..256 (384
+ * for interleaved E/B grids) with the static and the persistent-queue
+ * schedule -- on a sample of the run (the first min(n, 131072) particles of
+ * u0, host memory, for at most max_steps steps), keeps the fastest in the
+ * context for runs of the same kernel variant whose descriptor leaves block
+ * = 0 / schedule = TP_SCHED_AUTO, and reports it.                          */
+typedef struct tp_tune_result {
+    int32_t block;
+    int32_t schedule;      /* TP_SCHED_STATIC or TP_SCHED_QUEUE */
+    double ms;             /* device time of the chosen shape on the sample */
+    double ms_default;     /* the same sample with the untuned default shape */
+    int32_t candidates;
+    int32_t reserved;
+} tp_tune_result;
+int tp_autotune(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
+                const tp_field* B, const double* u0, int64_t n,
+                int64_t max_steps, tp_tune_result* out);
+
+/* A full-orbit solve with fixed device buffers (the arguments of
+ * tp_boris_run_device) captured once into a CUDA graph; tp_graph_launch
+ * replays it on a stream.  Buffer contents may change between launches
+ * (new initial states); the buffers and fields must outlive the graph.      */
+typedef struct tp_graph tp_graph;
+int tp_boris_graph_create(tp_ctx* ctx, const tp_run_desc* desc,
+                          const tp_field* E, const tp_field* B,
+                          const double* u0, const double* dt_i,
+                          const double* tend_i, int64_t n, int64_t nslots,
+                          double* t_out, double* u_out, int32_t* nsaved,
+                          int8_t* retcode, int64_t* nsteps, int32_t* status,
+                          tp_graph** out);
+int tp_graph_launch(tp_graph* graph, void* stream);
+void tp_graph_destroy(tp_graph* graph);
+
 /* ---- guiding-centre solve -------------------------------------------------
  * Replaces _solve(::EnsembleAlg, ::TraceGCProblem, ...) (gc_solver.jl:104-161)
  * with _rk4! (rk4_gc.jl:27-130) or _rk45! (rk45_gc.jl:52-173).

@@ -151,6 +151,17 @@ class GCDesc(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("block", C.c_int32),
+        ("schedule", C.c_int32),
+        ("ms", C.c_double),
+        ("ms_default", C.c_double),
+        ("candidates", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
 class AdjDesc(C.Structure):
     _fields_ = [
         ("run", RunDesc),
@@ -182,6 +193,11 @@ SIGNATURES = [
     ("tp_pack_results_device_noalloc", C.c_int,
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     ("tp_field_update", C.c_int, [_P, _P]),
+    ("tp_autotune", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(TuneResult)]),
+    ("tp_boris_graph_create", C.c_int,
+     [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    ("tp_graph_launch", C.c_int, [_P, _P]),
+    ("tp_graph_destroy", None, [_P]),
     ("tp_adjoint_forward", C.c_int, [_P, C.POINTER(AdjDesc), _P, _P, _P, C.c_int64, _P, C.POINTER(_P)]),
     ("tp_adjoint_backward", C.c_int, [_P, _P, _P, _P, _P, _P]),
     ("tp_adjoint_forward_device", C.c_int,

@@ -31,8 +31,9 @@ struct tp_ctx {
     int sms = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    // tuned launch shapes keyed by (alg, precision, field kinds, schedule)
-    std::map<std::string, int> tuned_block;
+    // launch shapes chosen by tp_autotune, keyed by the kernel variant
+    // (algorithm, precision, field configuration, termination): block, schedule
+    std::map<std::string, std::pair<int, int>> tuned;
 };
 
 struct tp_field {
@@ -254,8 +255,10 @@ int check_boris_desc(tp_ctx* ctx, const tp_run_desc* d) {
     if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "savestepinterval must be >= 1");
     if (d->precision != TP_PREC_FP64 && d->precision != TP_PREC_FP32C)
         return fail(ctx, TP_E_UNSUPPORTED, "unknown precision");
-    if (d->block < 0 || d->block > 256 || (d->block % 32) != 0)
-        return fail(ctx, TP_E_ARG, "block must be 0 or a multiple of 32 up to 256");
+    if (d->block < 0 || d->block > 384 || (d->block % 32) != 0)
+        return fail(ctx, TP_E_ARG, "block must be 0 or a multiple of 32 up to 384");
+    if (d->schedule < TP_SCHED_AUTO || d->schedule > TP_SCHED_QUEUE)
+        return fail(ctx, TP_E_ARG, "unknown schedule");
     return TP_OK;
 }
 
@@ -510,28 +513,58 @@ int prepare_boris_args(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, tp_
     return TP_OK;
 }
 
-bool use_queue(const tp_run_desc* d) {
-    if (d->schedule == TP_SCHED_QUEUE) return true;
-    if (d->schedule == TP_SCHED_STATIC) return false;
-    // uneven lifetimes: adaptive steps or a termination predicate
-    return d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP || d->term.flags != 0;
+// key of the kernel variant a run selects (what tp_autotune tunes)
+std::string tune_key(const tp_run_desc* d, const BorisArgs& a) {
+    return std::to_string(d->alg) + ":" + std::to_string(d->precision) + ":" +
+           std::to_string(field_config_of(a.f)) + ":" + std::to_string(d->term.flags != 0);
 }
 
-int launch_boris(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, cudaStream_t s,
-                 unsigned long long* d_queue) {
-    bool q = use_queue(d);
-    a.use_queue = q;
-    a.queue = d_queue;
-    int block = d->block;
-    int occ = 0;
-    if (q) {
-        int b = block > 0 ? block : 128;
-        occ = d->precision == TP_PREC_FP32C ? occupancy_boris_fp32c(a, b) : occupancy_boris_fp64(a, b);
+// Effective block size and schedule of a run: the descriptor's, else the
+// tuned ones, else 128 threads and the queue whenever lifetimes can be
+// uneven (adaptive steps or a termination predicate).
+void resolve_launch(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a, int& block, bool& queue) {
+    block = d->block;
+    int sched = d->schedule;
+    if (block == 0 || sched == TP_SCHED_AUTO) {
+        auto it = ctx->tuned.find(tune_key(d, a));
+        if (it != ctx->tuned.end()) {
+            if (block == 0) block = it->second.first;
+            if (sched == TP_SCHED_AUTO) sched = it->second.second;
+        }
     }
-    LaunchCfg cfg;
-    int st = pick_launch(ctx, a.n, block, q, occ, cfg);
-    if (st != TP_OK) return st;
-    if (q) {
+    if (block == 0) block = 128;
+    if (sched == TP_SCHED_AUTO)
+        sched = (d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP || d->term.flags != 0)
+                    ? TP_SCHED_QUEUE
+                    : TP_SCHED_STATIC;
+    queue = sched == TP_SCHED_QUEUE;
+}
+
+bool use_queue(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a) {
+    int block;
+    bool q;
+    resolve_launch(ctx, d, a, block, q);
+    return q;
+}
+
+// launch shape of a run (host-only work: safe before a stream capture)
+int plan_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, LaunchCfg& cfg) {
+    int block;
+    bool q;
+    resolve_launch(ctx, d, a, block, q);
+    if (block > TPB_MAXT(field_config_of(a.f)))
+        return fail(ctx, TP_E_ARG, "block exceeds the kernel's limit for this field configuration");
+    a.use_queue = q;
+    int occ = 0;
+    if (q) occ = d->precision == TP_PREC_FP32C ? occupancy_boris_fp32c(a, block) : occupancy_boris_fp64(a, block);
+    return pick_launch(ctx, a.n, block, q, occ, cfg);
+}
+
+// the stream work of a run: queue reset and the push kernel
+int issue_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, const LaunchCfg& cfg, cudaStream_t s,
+                       unsigned long long* d_queue) {
+    a.queue = d_queue;
+    if (a.use_queue) {
         cudaError_t e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "queue reset");
     }
@@ -539,6 +572,14 @@ int launch_boris(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, cudaStream_t s
                                                   : launch_boris_fp64(a, cfg, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "push kernel launch");
     return TP_OK;
+}
+
+int launch_boris(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, cudaStream_t s,
+                 unsigned long long* d_queue) {
+    LaunchCfg cfg;
+    int st = plan_boris_launch(ctx, d, a, cfg);
+    if (st != TP_OK) return st;
+    return issue_boris_launch(ctx, d, a, cfg, s, d_queue);
 }
 
 int status_to_error(tp_ctx* ctx, int32_t status) {
@@ -644,13 +685,232 @@ int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, co
     a.nsteps = nsteps;
     a.status = status;
     unsigned long long* q = nullptr;
-    if (use_queue(d)) {
+    if (use_queue(ctx, d, a)) {
         e = cudaMallocAsync((void**)&q, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "queue counter");
     }
     st = launch_boris(ctx, d, a, s, q);
     if (q) cudaFreeAsync(q, s);
     return st;
+}
+
+int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B, const double* u0,
+                int64_t n, int64_t max_steps, tp_tune_result* out) {
+    if (!ctx || !out) return TP_E_ARG;
+    int st = check_boris_desc(ctx, d);
+    if (st != TP_OK) return st;
+    if (!E || !B || !u0 || n <= 0) return fail(ctx, TP_E_ARG, "autotune needs fields and initial states");
+    if (max_steps < 1) return fail(ctx, TP_E_ARG, "max_steps must be >= 1");
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (!adaptive && std::fabs(d->dt) < 10.0 * kEps) return fail(ctx, TP_E_ARG, "dt too small");
+    DeviceGuard g(ctx->device);
+    // the sample: first particles, span cut to max_steps
+    tp_run_desc ds = *d;
+    if (adaptive) {
+        ds.step_cap = (ds.step_cap > 0 && ds.step_cap < max_steps) ? ds.step_cap : max_steps;
+    } else {
+        int64_t nt = jl_round_h((d->t1 - d->t0) / d->dt);
+        if (nt < 0) nt = -nt;
+        if (nt > max_steps) ds.t1 = d->t0 + (double)max_steps * d->dt;
+    }
+    const int64_t ns = std::min<int64_t>(n, 131072);
+    int64_t nslots = 0;
+    st = tp_boris_slots(&ds, nullptr, nullptr, ns, &nslots);
+    if (st != TP_OK) return fail(ctx, st, "autotune sample sizing");
+    const int W = ds.save_fields ? 12 : 6;
+    DBuf u0_d, t_d, u_d, ns_d, rc_d, nst_d, st_d, q_d;
+    cudaError_t e = u0_d.alloc((size_t)ns * 6 * sizeof(double));
+    if (e == cudaSuccess) e = t_d.alloc((size_t)std::max<int64_t>(nslots, 1) * ns * sizeof(double));
+    if (e == cudaSuccess) e = u_d.alloc((size_t)std::max<int64_t>(nslots, 1) * W * ns * sizeof(double));
+    if (e == cudaSuccess) e = ns_d.alloc((size_t)ns * sizeof(int32_t));
+    if (e == cudaSuccess) e = rc_d.alloc((size_t)ns * sizeof(int8_t));
+    if (e == cudaSuccess) e = nst_d.alloc((size_t)ns * sizeof(int64_t));
+    if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
+    if (e == cudaSuccess) e = q_d.alloc(sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(u0_d.p, u0, (size_t)ns * 6 * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, std::string("autotune buffers: ") + cudaGetErrorString(e));
+    BorisArgs a;
+    st = prepare_boris_args(ctx, &ds, E, const_cast<tp_field*>(B), a);
+    if (st != TP_OK) return st;
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "field table");
+    a.n = ns;
+    a.nslots = nslots;
+    a.u0 = u0_d.as<double>();
+    a.t_out = t_d.as<double>();
+    a.u_out = u_d.as<double>();
+    a.nsaved = ns_d.as<int32_t>();
+    a.retcode = rc_d.as<int8_t>();
+    a.nsteps = nst_d.as<int64_t>();
+    a.status = st_d.as<int32_t>();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto time_shape = [&](int block, int sched, double& ms) -> int {
+        tp_run_desc dc = ds;
+        dc.block = block;
+        dc.schedule = sched;
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
+            BorisArgs ac = a;
+            cudaEventRecord(e0, ctx->stream);
+            int r = launch_boris(ctx, &dc, ac, ctx->stream, q_d.as<unsigned long long>());
+            if (r != TP_OK) return r;
+            cudaEventRecord(e1, ctx->stream);
+            cudaError_t ee = cudaEventSynchronize(e1);
+            if (ee != cudaSuccess) return cuda_fail(ctx, ee, "autotune run");
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) best = std::min(best, t);
+        }
+        ms = best;
+        return TP_OK;
+    };
+    const std::string key = tune_key(&ds, a);
+    const int maxt = TPB_MAXT(field_config_of(a.f));
+    const int blocks[] = {64, 96, 128, 192, 256, 384};
+    int best_b = 128, best_s = TP_SCHED_STATIC, cands = 0;
+    double best_ms = 1e300, def_ms = 0.0;
+    // the default shape, with any earlier tuning of this variant set aside
+    auto saved = ctx->tuned.find(key);
+    bool had = saved != ctx->tuned.end();
+    std::pair<int, int> old = had ? saved->second : std::make_pair(0, 0);
+    if (had) ctx->tuned.erase(key);
+    st = time_shape(0, TP_SCHED_AUTO, def_ms);
+    for (int b : blocks) {
+        if (st != TP_OK) break;
+        if (b > maxt) continue;
+        for (int sc : {TP_SCHED_STATIC, TP_SCHED_QUEUE}) {
+            double ms = 0.0;
+            st = time_shape(b, sc, ms);
+            if (st != TP_OK) break;
+            ++cands;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_b = b;
+                best_s = sc;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != TP_OK) {
+        if (had) ctx->tuned[key] = old;
+        return st;
+    }
+    int32_t dev_status = 0;
+    e = cudaMemcpy(&dev_status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && dev_status != 0 && dev_status != TP_E_OVERFLOW) {
+        if (had) ctx->tuned[key] = old;
+        return status_to_error(ctx, dev_status);
+    }
+    ctx->tuned[key] = {best_b, best_s};
+    out->block = best_b;
+    out->schedule = best_s;
+    out->ms = best_ms;
+    out->ms_default = def_ms;
+    out->candidates = cands;
+    out->reserved = 0;
+    return TP_OK;
+}
+
+}  // extern "C"
+
+struct tp_graph {
+    tp_ctx* ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long* queue = nullptr;
+    ~tp_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (queue) cudaFree(queue);
+    }
+};
+
+extern "C" {
+
+int tp_boris_graph_create(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B,
+                          const double* u0, const double* dt_i, const double* tend_i, int64_t n, int64_t nslots,
+                          double* t_out, double* u_out, int32_t* nsaved, int8_t* retcode, int64_t* nsteps,
+                          int32_t* status, tp_graph** out) {
+    if (!ctx || !out) return TP_E_ARG;
+    *out = nullptr;
+    int st = check_boris_desc(ctx, d);
+    if (st != TP_OK) return st;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (n <= 0 || nslots < 0) return fail(ctx, TP_E_ARG, "a graph needs n > 0 particles");
+    if (!u0 || !nsaved || !retcode || !nsteps || !status || (nslots > 0 && (!t_out || !u_out)))
+        return fail(ctx, TP_E_ARG, "null device buffer");
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (!adaptive && !dt_i && std::fabs(d->dt) < 10.0 * kEps)
+        return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
+    DeviceGuard g(ctx->device);
+    BorisArgs a;
+    st = prepare_boris_args(ctx, d, E, const_cast<tp_field*>(B), a);
+    if (st != TP_OK) return st;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "field table");
+    a.n = n;
+    a.nslots = nslots;
+    a.u0 = u0;
+    a.dt_i = dt_i;
+    a.tend_i = tend_i;
+    a.t_out = t_out;
+    a.u_out = u_out;
+    a.nsaved = nsaved;
+    a.retcode = retcode;
+    a.nsteps = nsteps;
+    a.status = status;
+    LaunchCfg cfg;
+    st = plan_boris_launch(ctx, d, a, cfg);
+    if (st != TP_OK) return st;
+    auto* gr = new tp_graph();
+    gr->ctx = ctx;
+    if (a.use_queue) {
+        e = cudaMalloc((void**)&gr->queue, sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            delete gr;
+            return cuda_fail(ctx, e, "queue counter");
+        }
+    }
+    cudaStream_t cs = nullptr;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        if (cs) cudaStreamDestroy(cs);
+        delete gr;
+        return cuda_fail(ctx, e, "graph capture");
+    }
+    st = issue_boris_launch(ctx, d, a, cfg, cs, gr->queue);
+    cudaError_t ee = cudaStreamEndCapture(cs, &gr->graph);
+    cudaStreamDestroy(cs);
+    if (st != TP_OK) {
+        delete gr;
+        return st;
+    }
+    if (ee == cudaSuccess) ee = cudaGraphInstantiate(&gr->exec, gr->graph, 0);
+    if (ee != cudaSuccess) {
+        delete gr;
+        return cuda_fail(ctx, ee, "graph instantiate");
+    }
+    *out = gr;
+    return TP_OK;
+}
+
+int tp_graph_launch(tp_graph* gr, void* stream) {
+    if (!gr) return TP_E_ARG;
+    DeviceGuard g(gr->ctx->device);
+    cudaError_t e = cudaGraphLaunch(gr->exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(gr->ctx, e, "graph launch");
+    return TP_OK;
+}
+
+void tp_graph_destroy(tp_graph* gr) {
+    if (!gr) return;
+    DeviceGuard g(gr->ctx->device);
+    cudaDeviceSynchronize();
+    delete gr;
 }
 
 int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B,

@@ -76,6 +76,10 @@ class EnsembleB200:
     schedule:  "auto", "static" (one thread per particle) or "queue"
                (persistent kernel pulling particles from a work queue).
     block:     threads per block (0: library default / tuned).
+    autotune:  time the candidate launch shapes on a sample before the
+               first full-orbit solve of each kernel variant (tp_autotune);
+               later solves with block = 0 and schedule = "auto" use the
+               fastest.
     """
 
     device: int = 0
@@ -83,6 +87,7 @@ class EnsembleB200:
     schedule: str = "auto"
     block: int = 0
     budget_s: float = 0.0
+    autotune: bool = False
 
 
 class EnsembleSerial:  # pragma: no cover - guidance only

@@ -56,6 +56,7 @@ class Context:
         self.handle = h
         self.device = device
         self._fields: dict[int, tuple] = {}
+        self.tuned_keys: set = set()
         weakref.finalize(self, self.lib.tp_ctx_destroy, h)
 
     @classmethod
@@ -151,6 +152,28 @@ class Context:
             f.data = a
             ptr = a.ctypes.data_as(C.c_void_p)
         _check(self.lib, self.handle, self.lib.tp_field_update(h, ptr), "tp_field_update")
+
+    # ------------------------------------------------------------ tuning, graphs
+    def autotune(self, desc: _abi.RunDesc, E, B, u0: np.ndarray, max_steps: int = 200) -> dict:
+        """Time the candidate launch shapes on a sample of the run (tp_autotune); later runs of the
+        same kernel variant with block = 0 / schedule = "auto" use the fastest."""
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        r = _abi.TuneResult()
+        code = self.lib.tp_autotune(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0),
+                                    u0.shape[0], int(max_steps), C.byref(r))
+        _check(self.lib, self.handle, code, "tp_autotune")
+        return {"block": r.block, "schedule": {1: "static", 2: "queue"}.get(r.schedule, "auto"), "ms": r.ms,
+                "ms_default": r.ms_default, "candidates": r.candidates}
+
+    def boris_graph(self, desc: _abi.RunDesc, E, B, u0, dt_i, tend_i, n: int, nslots: int, t_out, u_out, nsaved,
+                    retcode, nsteps, status) -> "Graph":
+        """A solve over fixed device buffers (pointers, as boris_run_device) captured as a CUDA graph."""
+        h = C.c_void_p()
+        code = self.lib.tp_boris_graph_create(self.handle, C.byref(desc), self.field(E), self.field(B), u0, dt_i,
+                                              tend_i, int(n), int(nslots), t_out, u_out, nsaved, retcode, nsteps,
+                                              status, C.byref(h))
+        _check(self.lib, self.handle, code, "tp_boris_graph_create")
+        return Graph(self, h, E, B)
 
     # ------------------------------------------------------------ adjoint
     def adjoint_forward(self, desc: _abi.AdjDesc, E, B, u0: np.ndarray):
@@ -273,6 +296,21 @@ class Tape:
         b, s = C.c_int64(), C.c_int64()
         self.ctx.lib.tp_tape_info(self.handle, C.byref(b), C.byref(s))
         return b.value, s.value
+
+    def close(self) -> None:
+        self._fin()
+
+
+class Graph:
+    """A captured solve (tp_graph); launch(stream) replays it."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, E, B):
+        self.ctx, self.handle = ctx, handle
+        self.E, self.B = E, B  # the fields must outlive the graph
+        self._fin = weakref.finalize(self, ctx.lib.tp_graph_destroy, handle)
+
+    def launch(self, stream: int = 0) -> None:
+        _check(self.ctx.lib, self.ctx.handle, self.ctx.lib.tp_graph_launch(self.handle, stream), "tp_graph_launch")
 
     def close(self) -> None:
         self._fin()

@@ -241,6 +241,11 @@ def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None
                    save_end=save_end, save_everystep=save_everystep, save_fields=save_fields,
                    save_work=save_work, maxiters=maxiters, step_cap=step_cap, tend=tend)
     ctx = Context.get(p.device)
+    if getattr(args[1] if len(args) > 1 else None, "autotune", False):
+        key = (p.desc.alg, p.desc.precision, id(p.E), id(p.B), p.desc.term.flags != 0)
+        if key not in ctx.tuned_keys:
+            ctx.autotune(p.desc, p.E, p.B, p.u0)
+            ctx.tuned_keys.add(key)
     t0 = time.perf_counter()
     r = ctx.boris_run(p.desc, p.E, p.B, p.u0, p.dt_i, p.tend_i)
     wall = time.perf_counter() - t0

@@ -374,3 +374,56 @@ def test_gc_config4_subset(tp, orc):
     err = np.linalg.norm(s32.final_states()[:, :3] - ref.final_states()[:, :3], axis=1) / \
         np.linalg.norm(ref.final_states()[:, :3], axis=1)
     assert np.median(err) <= 1e-4
+
+
+# ---------------------------------------------------------------- tuning and graphs
+def test_autotune_chooses_a_valid_shape_and_keeps_results(tp):
+    w = tp.workloads.config2(n=20000, nt=300, ssi=100)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    base = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=w.dt, savestepinterval=100)
+    plan = tp.plan_boris(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=w.dt, savestepinterval=100)
+    ctx = tp.Context.get(0)
+    r = ctx.autotune(plan.desc, plan.E, plan.B, plan.u0, max_steps=100)
+    assert r["block"] in (64, 96, 128, 192, 256, 384) and r["schedule"] in ("static", "queue")
+    assert r["candidates"] >= 10 and 0 < r["ms"] <= 1.25 * r["ms_default"]
+    tuned = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=w.dt, savestepinterval=100)
+    # per-particle arithmetic does not depend on the launch shape
+    assert np.array_equal(tuned.u_all, base.u_all) and np.array_equal(tuned.t_all, base.t_all)
+    auto = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c", autotune=True), dt=w.dt,
+                    savestepinterval=100)
+    assert np.array_equal(auto.u_all, base.u_all)
+
+
+@pytest.mark.parametrize("term", [False, True])
+def test_graph_replay_equals_direct_run(tp, term):
+    import torch
+    w = tp.workloads.config3(n=4096, nt=500, ssi=100)
+    isout = w.isoutside if term else None
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    plan = tp.plan_boris(prob, tp.MultistepBoris4(2), tp.EnsembleB200(precision="fp32c"), dt=w.dt,
+                         savestepinterval=100, isoutside=isout, tend=w.tend)
+    ctx = tp.Context.get(0)
+    n = plan.u0.shape[0]
+    nslots = ctx.slots(plan.desc, n, plan.dt_i, plan.tend_i)
+    dev = torch.device("cuda", 0)
+    f = lambda a: None if a is None else torch.from_numpy(a).to(dev)  # noqa: E731
+    u0, dt_i, tend_i = f(plan.u0), f(plan.dt_i), f(plan.tend_i)
+
+    def bufs():
+        return (torch.full((nslots, n), np.nan, dtype=torch.float64, device=dev),
+                torch.full((nslots, 6, n), np.nan, dtype=torch.float64, device=dev),
+                torch.zeros(n, dtype=torch.int32, device=dev), torch.zeros(n, dtype=torch.int8, device=dev),
+                torch.zeros(n, dtype=torch.int64, device=dev), torch.zeros(1, dtype=torch.int32, device=dev))
+
+    p = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+    a = bufs()
+    ctx.boris_run_device(plan.desc, plan.E, plan.B, p(u0), p(dt_i), p(tend_i), n, nslots, *[p(x) for x in a],
+                         torch.cuda.current_stream().cuda_stream)
+    b = bufs()
+    g = ctx.boris_graph(plan.desc, plan.E, plan.B, p(u0), p(dt_i), p(tend_i), n, nslots, *[p(x) for x in b])
+    for _ in range(2):  # replays rewrite the same buffers
+        g.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(torch.nan_to_num(x, nan=7.0), torch.nan_to_num(y, nan=7.0))
+    g.close()
