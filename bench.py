@@ -388,7 +388,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3"])
     ap.add_argument("--particles", type=int, default=1_000_000)
-    ap.add_argument("--sample", type=int, default=4000, help="particles of the CPU legs")
+    ap.add_argument("--sample", type=int, default=150_000,
+                    help="particles of the CPU legs (about 10 s of host work at 16 cores)")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")

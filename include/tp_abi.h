@@ -250,8 +250,10 @@ int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* desc,
  * No reference counterpart (KernelAbstractions picks its workgroup size).
  * tp_autotune times every candidate launch shape -- block sizes 64..256 (384
  * for interleaved E/B grids) with the static and the persistent-queue
- * schedule -- on a sample of the run (the first min(n, 131072) particles of
- * u0, host memory, for at most max_steps steps), keeps the fastest in the
+ * schedule (only the queue where lifetimes can be uneven: adaptive steps or
+ * a termination predicate) -- on a sample of the run (the first
+ * min(n, 131072) particles of u0, host memory, for at most max_steps
+ * steps), keeps the fastest in the
  * context for runs of the same kernel variant whose descriptor leaves block
  * = 0 / schedule = TP_SCHED_AUTO, and reports it.                          */
 typedef struct tp_tune_result {

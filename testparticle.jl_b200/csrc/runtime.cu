@@ -777,10 +777,15 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     std::pair<int, int> old = had ? saved->second : std::make_pair(0, 0);
     if (had) ctx->tuned.erase(key);
     st = time_shape(0, TP_SCHED_AUTO, def_ms);
+    // With uneven lifetimes (adaptive steps, termination) a cut sample has
+    // even ones and would favour the static schedule: only the queue is
+    // timed there.
+    const bool uneven = adaptive || ds.term.flags != 0;
     for (int b : blocks) {
         if (st != TP_OK) break;
         if (b > maxt) continue;
         for (int sc : {TP_SCHED_STATIC, TP_SCHED_QUEUE}) {
+            if (uneven && sc == TP_SCHED_STATIC) continue;
             double ms = 0.0;
             st = time_shape(b, sc, ms);
             if (st != TP_OK) break;
