@@ -663,15 +663,24 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// One node-gradient contribution: the cell (x = -1: none), its fractions and
+// the frame-scaled cotangents of E and B.
+struct Contrib {
+    int i0[3];
+    float f[3];
+    F3 lE, lB;
+};
+
 // adjoint of one velocity update from its record (q: kRecEB4 words, `stride`
-// apart); node gradients are added with an evict-last L2 policy
-__device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, const float4* qp, int stride, float h, F3 lo,
-                                              F3& lx, Frame& fr, uint64_t pol) {
-    const DevField& g = A.a.f.B;
+// apart); returns the cotangent of the input velocity, adds to lx and leaves
+// the step's node-gradient contribution in ct
+__device__ __forceinline__ F3 reverse_step_eb(const float4* qp, int stride, float h, F3 lo, F3& lx, Frame& fr,
+                                              Contrib& ct) {
     float4 q[kRecEB4];
 #pragma unroll
     for (int k = 0; k < kRecEB4; ++k) q[k] = qp[k * stride];
     const int ix = __float_as_int(q[0].x);
+    ct.i0[0] = -1;
     if (ix < 0) {
         lx = nanf3_();
         return nanf3_();
@@ -680,44 +689,69 @@ __device__ __forceinline__ F3 reverse_step_eb(const AdjArgs& A, const float4* qp
     UAdj u = u_adjoint(v, E, B, h, lo);
     lx = lx + jt({q[3].w, q[4].x, q[4].y}, {q[4].z, q[4].w, q[5].x}, {q[5].y, q[5].z, q[5].w}, u.lE) +
          jt({q[6].x, q[6].y, q[6].z}, {q[6].w, q[7].x, q[7].y}, {q[7].z, q[7].w, q[8].x}, u.lB);
-    AxF ax, ay, az;
-    const int i0[3] = {ix, __float_as_int(q[0].y), __float_as_int(q[0].z)};
-    const float fr3[3] = {q[0].w, q[1].x, q[1].y};
-    AxF* axs[3] = {&ax, &ay, &az};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        axs[k]->i0 = i0[k];
-        axs[k]->i1 = (g.bc == TP_BC_PERIODIC && i0[k] + 1 == g.n[k]) ? 0 : i0[k] + 1;
-        axs[k]->f = fr3[k];
-        axs[k]->ds = 0.0f;
-    }
     if (fr.f != 0.0f) {
-        if (A.bucket) {
-            // to the bucket of the cell's tile: local cell, fractions and the
-            // scaled cotangents (the deposit kernel forms the weights)
-            float m = fmaxf(fmaxf(fmaxf(fabsf(u.lE.x), fabsf(u.lE.y)), fmaxf(fabsf(u.lE.z), fabsf(u.lB.x))),
-                            fmaxf(fabsf(u.lB.y), fabsf(u.lB.z)));
-            fr.mx = max(fr.mx, fexp(m) + fr.e);
-            const int t = (i0[0] / kAdjTile) + A.tiles[0] * ((i0[1] / kAdjTile) + A.tiles[1] * (i0[2] / kAdjTile));
-            const int slot = atomicAdd(A.cursor + t, 1);
-            if (slot < A.cap) {
-                const int code = (i0[0] % kAdjTile) | ((i0[1] % kAdjTile) << 3) | ((i0[2] % kAdjTile) << 6);
-                float4* b = A.bucket + ((int64_t)t * A.cap + slot) * 3;
-                const float f = fr.f;
-                b[0] = make_float4(__int_as_float(code), fr3[0], fr3[1], fr3[2]);
-                b[1] = make_float4(f * u.lE.x, f * u.lE.y, f * u.lE.z, f * u.lB.x);
-                b[2] = make_float4(f * u.lB.y, f * u.lB.z, 0.0f, 0.0f);
-                return u.lv;
-            }
-        }
-        float w[8];
-        if (scale_weights(ax, ay, az, u.lE, u.lB, fr, w)) {  // full bucket: add directly
-            int nd[8];
-            tri_nodes(g, ax, ay, az, nd);
-            scatter<2, true>(A.g_eb, nd, w, u.lE, u.lB, pol);
-        }
+        float m = fmaxf(fmaxf(fmaxf(fabsf(u.lE.x), fabsf(u.lE.y)), fmaxf(fabsf(u.lE.z), fabsf(u.lB.x))),
+                        fmaxf(fabsf(u.lB.y), fabsf(u.lB.z)));
+        fr.mx = max(fr.mx, fexp(m) + fr.e);
+        ct.i0[0] = ix;
+        ct.i0[1] = __float_as_int(q[0].y);
+        ct.i0[2] = __float_as_int(q[0].z);
+        ct.f[0] = q[0].w;
+        ct.f[1] = q[1].x;
+        ct.f[2] = q[1].y;
+        ct.lE = fr.f * u.lE;
+        ct.lB = fr.f * u.lB;
     }
     return u.lv;
+}
+
+// Warp-transposed scatter of the warp's 32 contributions.  In each of 16
+// rounds the lanes cover two particles x 8 corners x (E, B) half, so one
+// reduction instruction touches the nodes of two particles (about 16
+// sectors, the two halves of a node in one 32-byte sector) instead of 32
+// unrelated ones.  All 32 lanes of the warp must call it (lanes without a
+// contribution pass i0[0] = -1).
+constexpr int kStage = 12;  // staged words per lane
+
+__device__ __forceinline__ void scatter_warp_eb(const AdjArgs& A, float* stage, const Contrib& ct, uint64_t pol) {
+    const int lane = threadIdx.x & 31;
+    float* me = stage + lane * kStage;
+    me[0] = __int_as_float(ct.i0[0]);
+    me[1] = __int_as_float(ct.i0[1]);
+    me[2] = __int_as_float(ct.i0[2]);
+    me[3] = ct.f[0];
+    me[4] = ct.f[1];
+    me[5] = ct.f[2];
+    me[6] = ct.lE.x;
+    me[7] = ct.lE.y;
+    me[8] = ct.lE.z;
+    me[9] = ct.lB.x;
+    me[10] = ct.lB.y;
+    me[11] = ct.lB.z;
+    const unsigned have = __ballot_sync(0xffffffffu, ct.i0[0] >= 0);
+    __syncwarp();
+    if (have) {
+        const DevField& g = A.a.f.B;
+        const int c = (lane & 15) >> 1, h = lane & 1;
+        const int bx = c & 1, by = (c >> 1) & 1, bz = c >> 2;
+        const bool per = g.bc == TP_BC_PERIODIC;
+        for (int r = 0; r < 16; ++r) {
+            const int src = 2 * r + (lane >> 4);
+            if (!((have >> src) & 1u)) continue;
+            const float* q = stage + src * kStage;
+            int gx = __float_as_int(q[0]) + bx, gy = __float_as_int(q[1]) + by, gz = __float_as_int(q[2]) + bz;
+            if (per) {
+                if (gx == g.n[0]) gx = 0;
+                if (gy == g.n[1]) gy = 0;
+                if (gz == g.n[2]) gz = 0;
+            }
+            const float w = (bx ? q[3] : 1.0f - q[3]) * ((by ? q[4] : 1.0f - q[4]) * (bz ? q[5] : 1.0f - q[5]));
+            const float* a = q + 6 + 3 * h;
+            const int64_t node = (int64_t)gx + (int64_t)g.n[0] * (gy + (int64_t)g.n[1] * gz);
+            red_add3(A.g_eb + 2 * node + h, w * a[0], w * a[1], w * a[2], pol);
+        }
+    }
+    __syncwarp();
 }
 
 __device__ __forceinline__ int seg_steps(const AdjArgs& A, int64_t s) {
@@ -751,10 +785,15 @@ __global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t 
     }
 }
 
-constexpr int kRevStages = 3;  // records in flight per thread (shared memory ring)
+constexpr int kRevStages = 2;  // records in flight per thread (shared memory ring)
 
+// The particle loop is uniform over the block (lanes past n run empty) so
+// that whole warps take part in scatter_warp_eb.
 __global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s) {
-    extern __shared__ float4 ring[];  // [kRevStages][kRecEB4][blockDim.x]
+    extern __shared__ float4 smem4[];  // ring [kRevStages][kRecEB4][blockDim.x], then staging
+    float4* ring = smem4;
+    float* stage = reinterpret_cast<float*>(smem4 + kRevStages * kRecEB4 * blockDim.x) +
+                   (threadIdx.x & ~31) * kStage;
     const BorisArgs& a = A.a;
     const double dt = a.dt;
     const float dtf = (float)dt;
@@ -766,34 +805,43 @@ __global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s)
     const uint64_t keep = l2_evict_last();
     const uint64_t once = l2_evict_first();
     int mx = INT_MIN;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t ib = (int64_t)blockIdx.x * blockDim.x; ib < n; ib += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = ib + threadIdx.x;
+        const bool live = i < n;
         // records m-1, m-2, ... stream into the ring ahead of their use
 #pragma unroll
         for (int d = 0; d < kRevStages; ++d) {
             const int j = m - 1 - d;
-            if (j >= 0) rec_prefetch(A, j, i, ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
+            if (live && j >= 0)
+                rec_prefetch(A, j, i, ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
             cp_async_commit();
         }
-        F3 lx, lv;
+        F3 lx{0.0f, 0.0f, 0.0f}, lv{0.0f, 0.0f, 0.0f};
         Frame fr;
+        fr.e = 0;
+        fr.mx = INT_MIN;
+        frame_set(fr, G);
+        Contrib ct;
+        ct.i0[0] = -1;
         float* st = A.lam + i;
         if (s == A.S - 1) {
-            // cotangent of the final save, normalised: lambda = g / 2^e
-            const double* gf = A.g_final + 6 * i;
-            double gm = fmax(fmax(fmax(fabs(gf[0]), fabs(gf[1])), fmax(fabs(gf[2]), fabs(gf[3]))),
-                             fmax(fabs(gf[4]), fabs(gf[5])));
-            fr.e = (gm > 0.0 && gm <= 1.0e300) ? ilogb(gm) : 0;
-            fr.mx = INT_MIN;
-            frame_set(fr, G);
-            const double is = ldexp(1.0, -fr.e);
-            lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
-            lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
-            // the final save's record (slot m) is read directly
-            const float4* r = reinterpret_cast<const float4*>(A.rec) + (int64_t)m * kRecEB4 * n + i;
-            lv = reverse_step_eb(A, r, (int)n, vfac<false>(a, A.dt_final), lv, lx, fr, keep);
-            renorm(lx, lv, fr, G);
-        } else {
+            if (live) {
+                // cotangent of the final save, normalised: lambda = g / 2^e
+                const double* gf = A.g_final + 6 * i;
+                double gm = fmax(fmax(fmax(fabs(gf[0]), fabs(gf[1])), fmax(fabs(gf[2]), fabs(gf[3]))),
+                                 fmax(fabs(gf[4]), fabs(gf[5])));
+                fr.e = (gm > 0.0 && gm <= 1.0e300) ? ilogb(gm) : 0;
+                frame_set(fr, G);
+                const double is = ldexp(1.0, -fr.e);
+                lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
+                lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
+                // the final save's record (slot m) is read directly
+                const float4* r = reinterpret_cast<const float4*>(A.rec) + (int64_t)m * kRecEB4 * n + i;
+                lv = reverse_step_eb(r, (int)n, vfac<false>(a, A.dt_final), lv, lx, fr, ct);
+                renorm(lx, lv, fr, G);
+            }
+            scatter_warp_eb(A, stage, ct, keep);
+        } else if (live) {
             lx = {st[0], st[n], st[2 * n]};
             lv = {st[3 * n], st[4 * n], st[5 * n]};
             fr.e = __float_as_int(st[6 * n]);
@@ -802,16 +850,22 @@ __global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s)
         }
         for (int j = m - 1; j >= 0; --j) {
             cp_async_wait<kRevStages - 1>();  // this thread's copy of record j has landed
-            F3 lo = lv + dtf * lx;
-            lv = reverse_step_eb(A, ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, h, lo, lx,
-                                 fr, keep);
-            renorm(lx, lv, fr, G);
+            ct.i0[0] = -1;
+            if (live) {
+                F3 lo = lv + dtf * lx;
+                lv = reverse_step_eb(ring + (j % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, h, lo, lx, fr,
+                                     ct);
+                renorm(lx, lv, fr, G);
+            }
             // refill the slot just consumed with record j - kRevStages
             const int jn = j - kRevStages;
-            if (jn >= 0) rec_prefetch(A, jn, i, ring + (jn % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
+            if (live && jn >= 0)
+                rec_prefetch(A, jn, i, ring + (jn % kRevStages) * kRecEB4 * stride + threadIdx.x, stride, once);
             cp_async_commit();
+            scatter_warp_eb(A, stage, ct, keep);
         }
         cp_async_wait<0>();
+        if (!live) continue;
         if (s == 0) {
             // initial half step back, v_{-1/2} = U(v_0, x_0, -dt/2)
             const double* u0 = a.u0 + 6 * i;
@@ -841,58 +895,6 @@ __global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s)
     if (s == 0) {
         mx = __reduce_max_sync(0xffffffffu, mx);
         if ((threadIdx.x & 31) == 0 && mx != INT_MIN) atomicMax(A.need, mx);
-    }
-}
-
-// One block per tile of 8^3 cells: the tile's bucket is accumulated into its
-// 9^3 nodes in shared memory, then each touched node is added to the global
-// table with two reductions (E half, B half) -- about 1/60 of the global
-// reductions the per-step scatter needs.  Resets the tile's cursor.
-constexpr int kTileNodes = (kAdjTile + 1) * (kAdjTile + 1) * (kAdjTile + 1);
-
-__global__ void __launch_bounds__(256) k_adj_deposit_eb(AdjArgs A) {
-    __shared__ float acc[kTileNodes][8];  // E xyz, pad, B xyz, pad
-    const int t = blockIdx.x;
-    const int tx = t % A.tiles[0], ty = (t / A.tiles[0]) % A.tiles[1], tz = t / (A.tiles[0] * A.tiles[1]);
-    for (int k = threadIdx.x; k < kTileNodes * 8; k += blockDim.x) (&acc[0][0])[k] = 0.0f;
-    __syncthreads();
-    const int cnt = min(A.cursor[t], A.cap);
-    const float4* b = A.bucket + (int64_t)t * A.cap * 3;
-    for (int c = threadIdx.x; c < cnt; c += blockDim.x) {
-        const float4 q0 = b[3 * c], q1 = b[3 * c + 1], q2 = b[3 * c + 2];
-        const int code = __float_as_int(q0.x);
-        const int lx = code & 7, ly = (code >> 3) & 7, lz = (code >> 6) & 7;
-        AxF ax{0, 1, q0.y, 0.0f}, ay{0, 1, q0.z, 0.0f}, az{0, 1, q0.w, 0.0f};
-        float w[8];
-        tri_weights(ax, ay, az, w);
-        const float v[6] = {q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
-#pragma unroll
-        for (int cn = 0; cn < 8; ++cn) {
-            const int node = ((lz + (cn >> 2)) * (kAdjTile + 1) + (ly + ((cn >> 1) & 1))) * (kAdjTile + 1) + lx + (cn & 1);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                atomicAdd(&acc[node][k], w[cn] * v[k]);
-                atomicAdd(&acc[node][4 + k], w[cn] * v[3 + k]);
-            }
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) A.cursor[t] = 0;
-    const DevField& g = A.a.f.B;
-    const uint64_t keep = l2_evict_last();
-    for (int k = threadIdx.x; k < kTileNodes; k += blockDim.x) {
-        const float* a = acc[k];
-        if (a[0] == 0.0f && a[1] == 0.0f && a[2] == 0.0f && a[4] == 0.0f && a[5] == 0.0f && a[6] == 0.0f) continue;
-        const int lx = k % (kAdjTile + 1), ly = (k / (kAdjTile + 1)) % (kAdjTile + 1), lz = k / ((kAdjTile + 1) * (kAdjTile + 1));
-        int gx = tx * kAdjTile + lx, gy = ty * kAdjTile + ly, gz = tz * kAdjTile + lz;
-        // periodic grids wrap the last node layer to 0; other grids never
-        // reach past n - 1 (their cells stop at n - 2)
-        if (gx >= g.n[0]) gx -= g.n[0];
-        if (gy >= g.n[1]) gy -= g.n[1];
-        if (gz >= g.n[2]) gz -= g.n[2];
-        const int64_t node = (int64_t)gx + (int64_t)g.n[0] * (gy + (int64_t)g.n[1] * gz);
-        red_add3(A.g_eb + 2 * node, a[0], a[1], a[2], keep);
-        red_add3(A.g_eb + 2 * node + 1, a[4], a[5], a[6], keep);
     }
 }
 
@@ -950,14 +952,13 @@ cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c,
 
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
     if (fk == FK_EBGRID) {  // two kernels per segment, last segment first
-        const size_t ring = (size_t)kRevStages * kRecEB4 * c.block * sizeof(float4);
-        cudaError_t e = cudaFuncSetAttribute(k_adj_reverse_eb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring);
+        const size_t smem = (size_t)kRevStages * kRecEB4 * c.block * sizeof(float4) +
+                            (size_t)kStage * c.block * sizeof(float);
+        cudaError_t e = cudaFuncSetAttribute(k_adj_reverse_eb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        const int ntiles = a.tiles[0] * a.tiles[1] * a.tiles[2];
         for (int64_t seg = a.S - 1; seg >= 0; --seg) {
             k_adj_recompute_eb<<<c.grid, c.block, 0, s>>>(a, seg);
-            k_adj_reverse_eb<<<c.grid, c.block, ring, s>>>(a, seg);
-            if (a.bucket) k_adj_deposit_eb<<<ntiles, 256, 0, s>>>(a);
+            k_adj_reverse_eb<<<c.grid, c.block, smem, s>>>(a, seg);
         }
         return cudaGetLastError();
     }

@@ -1335,13 +1335,11 @@ struct tp_tape {
     double* d_gparam = nullptr;
     int32_t* d_need = nullptr;
     float* d_lam = nullptr;
-    int32_t* d_cursor = nullptr;
-    float4* d_bucket = nullptr;
     int G = 0;  // scale exponent of the node-gradient tables, kept for the next pass
     int64_t bytes = 0;
     ~tp_tape() {
         for (void* q : {(void*)d_ckpt, (void*)d_u0, (void*)d_rec, (void*)d_geb, (void*)d_gE, (void*)d_gB,
-                        (void*)d_gparam, (void*)d_need, (void*)d_lam, (void*)d_cursor, (void*)d_bucket})
+                        (void*)d_gparam, (void*)d_need, (void*)d_lam})
             if (q) cudaFree(q);
     }
 };
@@ -1461,29 +1459,6 @@ int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, d
     if (e == cudaSuccess && gridE && !t->d_gE) e = tape_alloc(t, &t->d_gE, (size_t)t->nodes_E * sizeof(float4));
     if (e == cudaSuccess && gridB && !t->d_gB) e = tape_alloc(t, &t->d_gB, (size_t)t->nodes_B * sizeof(float4));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint scratch");
-    // tile buckets of the gradient deposit (interleaved E/B grids): capacity
-    // twice the mean contributions per tile and segment, at most 4 GB
-    if (e == cudaSuccess && eb && !t->d_bucket) {
-        const DevField& gb = A.a.f.B;
-        int64_t ntiles = 1;
-        for (int k = 0; k < 3; ++k) {
-            A.tiles[k] = (gb.n[k] + kAdjTile - 1) / kAdjTile;
-            ntiles *= A.tiles[k];
-        }
-        int64_t per = (n * (A.K + 1) + ntiles - 1) / ntiles;
-        int64_t cap = 2 * per + 256;
-        const int64_t limit = (int64_t)4 << 30;
-        if (ntiles * cap * 48 > limit) cap = limit / (ntiles * 48);
-        if (cap >= 64 && cap < (1 << 30)) {
-            A.cap = (int32_t)cap;
-            e = tape_alloc(t, &t->d_cursor, (size_t)ntiles * sizeof(int32_t));
-            if (e == cudaSuccess) e = tape_alloc(t, &t->d_bucket, (size_t)ntiles * cap * 3 * sizeof(float4));
-            if (e == cudaSuccess) e = cudaMemsetAsync(t->d_cursor, 0, (size_t)ntiles * sizeof(int32_t), s);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint deposit buckets");
-        }
-    }
-    A.cursor = t->d_cursor;
-    A.bucket = t->d_bucket;
     A.rec = t->d_rec;
     A.lam = t->d_lam;
     A.g_eb = t->d_geb;

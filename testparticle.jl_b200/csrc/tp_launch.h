@@ -71,13 +71,6 @@ struct AdjArgs {
     int32_t pad;
     int32_t* need;         // device: largest node-contribution exponent of the pass
     float* lam;            // [8][n] cotangent state between segments (segmented path)
-    // tile-bucketed deposit of node gradients (segmented path): the grid is
-    // cut into tiles of 8^3 cells; a step's contribution goes to its tile's
-    // bucket (48 bytes) unless the bucket is full (then scattered directly)
-    int32_t tiles[3];
-    int32_t cap;           // bucket capacity per tile and segment
-    int32_t* cursor;       // [ntiles] fill counts, reset by the deposit kernel
-    float4* bucket;        // [ntiles][cap][3]
 };
 
 // field configuration of an adjoint run (FK_ANALYTIC / FK_EBGRID / FK_GENERIC)
@@ -85,7 +78,6 @@ int adjoint_field_config(const DevFields& f);
 cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
 int64_t adjoint_record_words(int fk, int64_t K, int64_t n);
-constexpr int kAdjTile = 8;  // cells per tile edge of the gradient deposit
 int64_t adjoint_state_words(int fk, int64_t n);
 // sum of a node-gradient table (values times 2^-G) into out[0..2] (+=),
 // entries k*stride + off
