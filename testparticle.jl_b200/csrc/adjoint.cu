@@ -705,50 +705,52 @@ __device__ __forceinline__ F3 reverse_step_eb(const float4* qp, int stride, floa
     return u.lv;
 }
 
-// Warp-transposed scatter of the warp's 32 contributions.  In each of 16
-// rounds the lanes cover two particles x 8 corners x (E, B) half, so one
-// reduction instruction touches the nodes of two particles (about 16
-// sectors, the two halves of a node in one 32-byte sector) instead of 32
-// unrelated ones.  All 32 lanes of the warp must call it (lanes without a
-// contribution pass i0[0] = -1).
-constexpr int kStage = 12;  // staged words per lane
+// Warp-transposed scatter of the warp's 32 contributions.  Each lane stages
+// its particle's 8 node indices, 8 weights and the two scaled cotangents
+// (24 words); then in each of 16 rounds the lanes cover two particles x 8
+// corners x (E, B) half, so one reduction instruction touches the nodes of
+// two particles (about 16 sectors, the two halves of a node in one 32-byte
+// sector) instead of 32 unrelated ones.  All 32 lanes of the warp must call
+// it (lanes without a contribution pass i0[0] = -1).
+constexpr int kStage = 24;  // staged words per lane: nodes[8], weights[8], lE xyz, pad, lB xyz, pad
 
 __device__ __forceinline__ void scatter_warp_eb(const AdjArgs& A, float* stage, const Contrib& ct, uint64_t pol) {
     const int lane = threadIdx.x & 31;
-    float* me = stage + lane * kStage;
-    me[0] = __int_as_float(ct.i0[0]);
-    me[1] = __int_as_float(ct.i0[1]);
-    me[2] = __int_as_float(ct.i0[2]);
-    me[3] = ct.f[0];
-    me[4] = ct.f[1];
-    me[5] = ct.f[2];
-    me[6] = ct.lE.x;
-    me[7] = ct.lE.y;
-    me[8] = ct.lE.z;
-    me[9] = ct.lB.x;
-    me[10] = ct.lB.y;
-    me[11] = ct.lB.z;
     const unsigned have = __ballot_sync(0xffffffffu, ct.i0[0] >= 0);
-    __syncwarp();
-    if (have) {
+    if (!have) return;  // warp-uniform
+    if (ct.i0[0] >= 0) {
         const DevField& g = A.a.f.B;
-        const int c = (lane & 15) >> 1, h = lane & 1;
-        const int bx = c & 1, by = (c >> 1) & 1, bz = c >> 2;
-        const bool per = g.bc == TP_BC_PERIODIC;
-        for (int r = 0; r < 16; ++r) {
-            const int src = 2 * r + (lane >> 4);
-            if (!((have >> src) & 1u)) continue;
+        AxF ax, ay, az;
+        AxF* axs[3] = {&ax, &ay, &az};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            axs[k]->i0 = ct.i0[k];
+            axs[k]->i1 = (g.bc == TP_BC_PERIODIC && ct.i0[k] + 1 == g.n[k]) ? 0 : ct.i0[k] + 1;
+            axs[k]->f = ct.f[k];
+            axs[k]->ds = 0.0f;
+        }
+        int nd[8];
+        float w[8];
+        tri_nodes(g, ax, ay, az, nd);
+        tri_weights(ax, ay, az, w);
+        float4* me = reinterpret_cast<float4*>(stage + lane * kStage);
+        me[0] = make_float4(__int_as_float(nd[0]), __int_as_float(nd[1]), __int_as_float(nd[2]), __int_as_float(nd[3]));
+        me[1] = make_float4(__int_as_float(nd[4]), __int_as_float(nd[5]), __int_as_float(nd[6]), __int_as_float(nd[7]));
+        me[2] = make_float4(w[0], w[1], w[2], w[3]);
+        me[3] = make_float4(w[4], w[5], w[6], w[7]);
+        me[4] = make_float4(ct.lE.x, ct.lE.y, ct.lE.z, 0.0f);
+        me[5] = make_float4(ct.lB.x, ct.lB.y, ct.lB.z, 0.0f);
+    }
+    __syncwarp();
+    const int c = (lane & 15) >> 1, h = lane & 1;
+    for (int r = 0; r < 16; ++r) {
+        const int src = 2 * r + (lane >> 4);
+        if ((have >> src) & 1u) {
             const float* q = stage + src * kStage;
-            int gx = __float_as_int(q[0]) + bx, gy = __float_as_int(q[1]) + by, gz = __float_as_int(q[2]) + bz;
-            if (per) {
-                if (gx == g.n[0]) gx = 0;
-                if (gy == g.n[1]) gy = 0;
-                if (gz == g.n[2]) gz = 0;
-            }
-            const float w = (bx ? q[3] : 1.0f - q[3]) * ((by ? q[4] : 1.0f - q[4]) * (bz ? q[5] : 1.0f - q[5]));
-            const float* a = q + 6 + 3 * h;
-            const int64_t node = (int64_t)gx + (int64_t)g.n[0] * (gy + (int64_t)g.n[1] * gz);
-            red_add3(A.g_eb + 2 * node + h, w * a[0], w * a[1], w * a[2], pol);
+            const int node = __float_as_int(q[c]);
+            const float w = q[8 + c];
+            const float4 l = *reinterpret_cast<const float4*>(q + 16 + 4 * h);
+            red_add3(A.g_eb + 2 * (int64_t)node + h, w * l.x, w * l.y, w * l.z, pol);
         }
     }
     __syncwarp();
