@@ -610,10 +610,9 @@ __device__ __forceinline__ void st_once(float4* p, float4 v, uint64_t pol) {
 }
 
 // field value at p (the forward's arithmetic) with its record for slot j;
-// the field table is read with an evict-last L2 policy and the record is
-// written with streaming (evict-first) stores
+// the record is written with streaming (evict-first) stores
 __device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, F3 v, int j, int64_t i,
-                                               uint64_t pol, uint64_t once, F3& E, F3& B) {
+                                               uint64_t once, F3& E, F3& B) {
     const DevFields& F = A.a.f;
     const int64_t n = A.a.n;
     float4* r = reinterpret_cast<float4*>(A.rec) + (int64_t)j * kRecEB4 * n + i;
@@ -628,7 +627,7 @@ __device__ __forceinline__ void record_step_eb(const AdjArgs& A, const CPos& p, 
     tri_nodes(F.B, ax, ay, az, nd);
     float4 e[8], b[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) ldg_node8_pol(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c], pol);
+    for (int c = 0; c < 8; ++c) ldg_node8(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c]);
     st_once(r, make_float4(__int_as_float(ax.i0), __int_as_float(ay.i0), __int_as_float(az.i0), ax.f), once);
     st_once(r + n, make_float4(ay.f, az.f, v.x, v.y), once);
     F3 Ex, Ey, Ez;
@@ -767,7 +766,6 @@ __global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t 
     const float dth = (float)dt, dtl = (float)(dt - (double)dth);
     const float h = vfac<false>(a, dt);
     const int m = seg_steps(A, s);
-    const uint64_t pol = l2_evict_last();
     const uint64_t once = l2_evict_first();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -776,13 +774,13 @@ __global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t 
         load_ck(A, s, i, p, v);
         for (int j = 0; j < m; ++j) {
             F3 E, B;
-            record_step_eb(A, p, v.h, j, i, pol, once, E, B);
+            record_step_eb(A, p, v.h, j, i, once, E, B);
             v = vel32h<false>(v, E, B, a, h);
             cpos_push_cv(a, p, v, dth, dtl);
         }
         if (s == A.S - 1) {  // the final save's update, at (x_N, v_{N-1/2})
             F3 E, B;
-            record_step_eb(A, p, v.h, m, i, pol, once, E, B);
+            record_step_eb(A, p, v.h, m, i, once, E, B);
         }
     }
 }

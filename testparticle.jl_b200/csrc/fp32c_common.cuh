@@ -182,14 +182,6 @@ __device__ __forceinline__ void ldg_node8(const float4* p, float4& e, float4& b)
         : "l"(p));
 }
 
-// The same load with an L2 eviction-priority policy (createpolicy), for
-// kernels that stream other data past the table.
-__device__ __forceinline__ void ldg_node8_pol(const float4* p, float4& e, float4& b, uint64_t pol) {
-    asm("ld.global.nc.L2::cache_hint.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
-        : "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
-        : "l"(p), "l"(pol));
-}
-
 // L2 policy: keep these lines in preference to others
 __device__ __forceinline__ uint64_t l2_evict_last() {
     uint64_t pol;
