@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "tp_launch.h"
@@ -34,6 +35,9 @@ struct tp_ctx {
     // launch shapes chosen by tp_autotune, keyed by the kernel variant
     // (algorithm, precision, field configuration, termination): block, schedule
     std::map<std::string, std::pair<int, int>> tuned;
+    // pinned staging for host <-> device transfers of pageable buffers
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
 struct tp_field {
@@ -51,16 +55,24 @@ struct tp_field {
     void* d_eb32 = nullptr;
 };
 
+// Results stay on the device until tp_result_copy moves them into the
+// caller's buffers (one pass through pinned staging).
 struct tp_result {
+    tp_ctx* ctx = nullptr;
     int64_t n = 0;
     int32_t width = 0;
     int64_t total = 0;
-    std::vector<int32_t> nsaved;
-    std::vector<int8_t> retcode;
-    std::vector<int64_t> nsteps;
-    std::vector<double> t;
-    std::vector<double> u;
+    void* nsaved = nullptr;   // device, n x int32
+    void* retcode = nullptr;  // device, n x int8
+    void* nsteps = nullptr;   // device, n x int64
+    void* t = nullptr;        // device, total x double (packed)
+    void* u = nullptr;        // device, total x width x double (packed)
     double elapsed_ms = 0.0;
+    cudaStream_t s = nullptr;  // the stream the buffers are ordered on
+    ~tp_result() {
+        for (void* q : {nsaved, retcode, nsteps, t, u})
+            if (q) cudaFreeAsync(q, s);
+    }
 };
 
 namespace {
@@ -92,22 +104,138 @@ struct DeviceGuard {
 };
 
 // RAII device buffer
+// Stream that DBuf allocations of the calling thread are ordered on: the
+// context stream of the entry point being served (AllocStream sets it).
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
+struct AllocStream {
+    cudaStream_t prev;
+    explicit AllocStream(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+    ~AllocStream() { g_alloc_stream = prev; }
+};
+
+// Device buffer from the device's stream-ordered memory pool (the context
+// raises the pool's release threshold, so freed blocks are reused by the
+// next solve instead of going back to the driver).  Allocation and release
+// are ordered on the context stream, after any work that still uses it.
 struct DBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t s = nullptr;
     ~DBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, s);
     }
     cudaError_t alloc(size_t b) {
         bytes = b;
+        s = g_alloc_stream;
         if (b == 0) return cudaSuccess;
-        return cudaMalloc(&p, b);
+        return cudaMallocAsync(&p, b, s);
     }
     template <class T>
     T* as() const {
         return reinterpret_cast<T*>(p);
     }
 };
+
+// ---------------------------------------------------------------- host transfers
+// Pageable host memory is copied through two pinned 64 MB staging buffers of
+// the context: the DMA of one chunk overlaps the host-side copy of the
+// previous one, and the host-side copy is split over threads, which also
+// spreads the first-touch page faults of freshly allocated destinations.
+constexpr size_t kPinChunk = (size_t)64 << 20;
+
+void host_copy(void* dst, const void* src, size_t bytes) {
+    const size_t per = (size_t)8 << 20;
+    unsigned hw = std::thread::hardware_concurrency();
+    int nt = (int)std::min<size_t>(std::max(1u, std::min(hw, 16u)), (bytes + per - 1) / per);
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t slice = (bytes + nt - 1) / nt;
+    for (int k = 0; k < nt; ++k) {
+        size_t a = (size_t)k * slice, b = std::min(bytes, a + slice);
+        if (a >= b) break;
+        th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+
+cudaError_t ensure_pinned(tp_ctx* ctx) {
+    for (int k = 0; k < 2; ++k) {
+        if (!ctx->pin[k]) {
+            cudaError_t e = cudaHostAlloc(&ctx->pin[k], kPinChunk, cudaHostAllocDefault);
+            if (e != cudaSuccess) return e;
+        }
+        if (!ctx->pin_ev[k]) {
+            cudaError_t e = cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+bool is_pageable(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return at.type == cudaMemoryTypeUnregistered;
+}
+
+// device -> host (dst may be pageable); synchronous on return
+cudaError_t copy_to_host(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    cudaStream_t s = ctx->stream;
+    if (bytes == 0) return cudaSuccess;
+    if (bytes < ((size_t)4 << 20) || !is_pageable(dst)) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
+    cudaError_t e = ensure_pinned(ctx);
+    if (e != cudaSuccess) return e;
+    const size_t nch = (bytes + kPinChunk - 1) / kPinChunk;
+    for (size_t k = 0; k <= nch; ++k) {
+        if (k < nch) {
+            size_t off = k * kPinChunk, len = std::min(kPinChunk, bytes - off);
+            e = cudaMemcpyAsync(ctx->pin[k & 1], (const char*)src + off, len, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->pin_ev[k & 1], s);
+            if (e != cudaSuccess) return e;
+        }
+        if (k > 0) {  // the previous chunk: wait for its DMA, then spread it out
+            size_t j = k - 1, off = j * kPinChunk, len = std::min(kPinChunk, bytes - off);
+            e = cudaEventSynchronize(ctx->pin_ev[j & 1]);
+            if (e != cudaSuccess) return e;
+            host_copy((char*)dst + off, ctx->pin[j & 1], len);
+        }
+    }
+    return cudaSuccess;
+}
+
+// host (possibly pageable) -> device; asynchronous on the context stream
+// after the staging of the last chunk
+cudaError_t copy_to_device(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    cudaStream_t s = ctx->stream;
+    if (bytes == 0) return cudaSuccess;
+    if (bytes < ((size_t)4 << 20) || !is_pageable(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
+    cudaError_t e = ensure_pinned(ctx);
+    if (e != cudaSuccess) return e;
+    const size_t nch = (bytes + kPinChunk - 1) / kPinChunk;
+    for (size_t k = 0; k < nch; ++k) {
+        size_t off = k * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        if (k >= 2) {  // the buffer's previous DMA must be done before refilling it
+            e = cudaEventSynchronize(ctx->pin_ev[k & 1]);
+            if (e != cudaSuccess) return e;
+        }
+        host_copy(ctx->pin[k & 1], (const char*)src + off, len);
+        e = cudaMemcpyAsync((char*)dst + off, ctx->pin[k & 1], len, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->pin_ev[k & 1], s);
+        if (e != cudaSuccess) return e;
+    }
+    // the staging buffers are reused by the next transfer: finish this one
+    return cudaStreamSynchronize(s);
+}
 
 const double kEps = 2.220446049250313e-16;
 
@@ -301,6 +429,15 @@ int tp_ctx_create(int device, tp_ctx** out) {
     c->device = device;
     e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        // keep freed pool memory in this process for the next solve
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     if (e != cudaSuccess) {
         delete c;
         cudaGetLastError();
@@ -313,6 +450,11 @@ int tp_ctx_create(int device, tp_ctx** out) {
 void tp_ctx_destroy(tp_ctx* ctx) {
     if (!ctx) return;
     DeviceGuard g(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->pin[k]) cudaFreeHost(ctx->pin[k]);
+        if (ctx->pin_ev[k]) cudaEventDestroy(ctx->pin_ev[k]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -598,14 +740,16 @@ int status_to_error(tp_ctx* ctx, int32_t status) {
 }
 
 // Copy slot-major device results into a packed host tp_result.
-int pack_to_host(tp_ctx* ctx, int64_t n, int64_t nslots, int W, const DBuf& t_d, const DBuf& u_d,
-                 const DBuf& ns_d, const DBuf& rc_d, const DBuf& st_d, tp_result* r) {
+// Pack slot-major device results into the per-trajectory layout, on the
+// device, into buffers the result owns; the per-particle arrays are moved
+// into the result.
+int pack_results(tp_ctx* ctx, int64_t n, int64_t nslots, int W, const DBuf& t_d, const DBuf& u_d, DBuf& ns_d,
+                 DBuf& rc_d, DBuf& nst_d, tp_result* r) {
     cudaStream_t s = ctx->stream;
+    r->ctx = ctx;
+    r->s = s;
     r->n = n;
     r->width = W;
-    r->nsaved.resize(n);
-    r->retcode.resize(n);
-    r->nsteps.resize(n);
     if (n == 0) return TP_OK;
     DBuf cnt, off, tmp;
     size_t tmp_bytes = 0;
@@ -624,25 +768,17 @@ int pack_to_host(tp_ctx* ctx, int64_t n, int64_t nslots, int W, const DBuf& t_d,
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "result offsets");
     r->total = total;
-    DBuf tp, up;
-    e = tp.alloc((size_t)std::max<int64_t>(total, 1) * sizeof(double));
-    if (e == cudaSuccess) e = up.alloc((size_t)std::max<int64_t>(total, 1) * W * sizeof(double));
+    e = cudaMallocAsync(&r->t, (size_t)std::max<int64_t>(total, 1) * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&r->u, (size_t)std::max<int64_t>(total, 1) * W * sizeof(double), s);
     if (e == cudaSuccess)
         e = launch_pack_results(t_d.as<double>(), u_d.as<double>(), ns_d.as<int32_t>(), off.as<int64_t>(),
-                                n, nslots, W, tp.as<double>(), up.as<double>(), s);
-    r->t.resize(total);
-    r->u.resize((size_t)total * W);
-    if (e == cudaSuccess && total > 0)
-        e = cudaMemcpyAsync(r->t.data(), tp.p, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess && total > 0)
-        e = cudaMemcpyAsync(r->u.data(), up.p, (size_t)total * W * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(r->nsaved.data(), ns_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(r->retcode.data(), rc_d.p, (size_t)n * sizeof(int8_t), cudaMemcpyDeviceToHost, s);
+                                n, nslots, W, (double*)r->t, (double*)r->u, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
-    (void)st_d;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result packing");
+    r->nsaved = ns_d.p;
+    r->retcode = rc_d.p;
+    r->nsteps = nst_d.p;
+    ns_d.p = rc_d.p = nst_d.p = nullptr;
     return TP_OK;
 }
 
@@ -704,6 +840,7 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
     if (!adaptive && std::fabs(d->dt) < 10.0 * kEps) return fail(ctx, TP_E_ARG, "dt too small");
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     // the sample: first particles, span cut to max_steps
     tp_run_desc ds = *d;
     if (adaptive) {
@@ -727,7 +864,8 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     if (e == cudaSuccess) e = nst_d.alloc((size_t)ns * sizeof(int64_t));
     if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
     if (e == cudaSuccess) e = q_d.alloc(sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemcpy(u0_d.p, u0, (size_t)ns * 6 * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = copy_to_device(ctx, u0_d.p, u0, (size_t)ns * 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, std::string("autotune buffers: ") + cudaGetErrorString(e));
     BorisArgs a;
     st = prepare_boris_args(ctx, &ds, E, const_cast<tp_field*>(B), a);
@@ -949,6 +1087,7 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
     if (nslots < 0) nslots = 64;  // adaptive without a cap: grown on overflow below
     const int W = d->save_fields ? 12 : 6;
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     cudaStream_t s = ctx->stream;
     tp_result* r = new tp_result();
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -967,7 +1106,7 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
             delete r;
             return fail(ctx, TP_E_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
         }
-        if (n > 0) e = cudaMemcpyAsync(u0_d.p, u0, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (n > 0) e = copy_to_device(ctx, u0_d.p, u0, (size_t)n * 6 * sizeof(double));
         if (e == cudaSuccess && dt_i)
             e = cudaMemcpyAsync(dt_d.p, dt_i, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && tend_i)
@@ -1037,11 +1176,7 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
             delete r;
             return status_to_error(ctx, status);
         }
-        st = pack_to_host(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, st_d, r);
-        if (st == TP_OK && n > 0) {
-            e = cudaMemcpy(r->nsteps.data(), nst_d.p, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost);
-            if (e != cudaSuccess) st = cuda_fail(ctx, e, "step counts");
-        }
+        st = pack_results(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, nst_d, r);
         if (st != TP_OK) {
             delete r;
             return st;
@@ -1060,6 +1195,7 @@ int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B, const doubl
     if (n < 0 || (n > 0 && (!xv || !y0_out || !mu_out))) return fail(ctx, TP_E_ARG, "bad buffers");
     if (n == 0) return TP_OK;
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     cudaStream_t s = ctx->stream;
     DBuf xv_d, y_d, mu_d;
     cudaError_t e = xv_d.alloc((size_t)n * 6 * sizeof(double));
@@ -1153,6 +1289,7 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
     if (d->alg == TP_GC_RK45 && !d->save_everystep) nslots = 2;
     const int W = d->save_fields ? 10 : 4;
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     cudaStream_t s = ctx->stream;
     tp_result* r = new tp_result();
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -1174,7 +1311,7 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
             delete r;
             return fail(ctx, TP_E_NOMEM, "device allocation");
         }
-        if (n > 0) e = cudaMemcpyAsync(y_d.p, y0, (size_t)n * 4 * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (n > 0) e = copy_to_device(ctx, y_d.p, y0, (size_t)n * 4 * sizeof(double));
         if (e == cudaSuccess && q_i) e = cudaMemcpyAsync(q_d.p, q_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && q2m_i) e = cudaMemcpyAsync(q2m_d.p, q2m_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && mu_i) e = cudaMemcpyAsync(mu_d.p, mu_i, (size_t)n * 8, cudaMemcpyHostToDevice, s);
@@ -1270,11 +1407,7 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
             delete r;
             return status_to_error(ctx, status);
         }
-        st = pack_to_host(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, st_d, r);
-        if (st == TP_OK && n > 0) {
-            e = cudaMemcpy(r->nsteps.data(), nst_d.p, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost);
-            if (e != cudaSuccess) st = cuda_fail(ctx, e, "step counts");
-        }
+        st = pack_results(ctx, n, nslots, W, t_d, u_d, ns_d, rc_d, nst_d, r);
         if (st != TP_OK) {
             delete r;
             return st;
@@ -1298,11 +1431,18 @@ int tp_result_info(const tp_result* r, int64_t* n, int32_t* width, int64_t* tota
 int tp_result_copy(const tp_result* r, int32_t* nsaved, int8_t* retcode, int64_t* nsteps,
                    double* t_packed, double* u_packed) {
     if (!r) return TP_E_ARG;
-    if (nsaved && r->n) std::memcpy(nsaved, r->nsaved.data(), r->n * sizeof(int32_t));
-    if (retcode && r->n) std::memcpy(retcode, r->retcode.data(), r->n * sizeof(int8_t));
-    if (nsteps && r->n) std::memcpy(nsteps, r->nsteps.data(), r->n * sizeof(int64_t));
-    if (t_packed && r->total) std::memcpy(t_packed, r->t.data(), r->total * sizeof(double));
-    if (u_packed && r->total) std::memcpy(u_packed, r->u.data(), (size_t)r->total * r->width * sizeof(double));
+    if (r->n == 0) return TP_OK;
+    tp_ctx* ctx = r->ctx;
+    DeviceGuard g(ctx->device);
+    cudaError_t e = cudaSuccess;
+    if (nsaved) e = copy_to_host(ctx, nsaved, r->nsaved, (size_t)r->n * sizeof(int32_t));
+    if (e == cudaSuccess && retcode) e = copy_to_host(ctx, retcode, r->retcode, (size_t)r->n * sizeof(int8_t));
+    if (e == cudaSuccess && nsteps) e = copy_to_host(ctx, nsteps, r->nsteps, (size_t)r->n * sizeof(int64_t));
+    if (e == cudaSuccess && t_packed && r->total)
+        e = copy_to_host(ctx, t_packed, r->t, (size_t)r->total * sizeof(double));
+    if (e == cudaSuccess && u_packed && r->total)
+        e = copy_to_host(ctx, u_packed, r->u, (size_t)r->total * r->width * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
     return TP_OK;
 }
 
@@ -1312,7 +1452,15 @@ int tp_result_elapsed_ms(const tp_result* r, double* ms) {
     return TP_OK;
 }
 
-void tp_result_destroy(tp_result* r) { delete r; }
+void tp_result_destroy(tp_result* r) {
+    if (!r) return;
+    if (r->ctx) {
+        DeviceGuard g(r->ctx->device);
+        delete r;
+        return;
+    }
+    delete r;
+}
 
 }  // extern "C"
 
@@ -1551,6 +1699,7 @@ int tp_adjoint_forward(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, con
     int st = adjoint_prepare(ctx, d, E, B, n, &t);
     if (st != TP_OK) return st;
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     DBuf uf;
     cudaError_t e = uf.alloc((size_t)n * 6 * sizeof(double));
     if (e != cudaSuccess) {
@@ -1578,6 +1727,7 @@ int tp_adjoint_backward(tp_tape* t, const double* grad_final, double* grad_u0, d
     const int64_t n = t->A.a.n;
     if (n > 0 && (!grad_final || !grad_u0)) return fail(ctx, TP_E_ARG, "null gradient buffer");
     DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
     const bool eb = t->fk == FK_EBGRID;
     const int64_t nE = (eb || t->E->desc.kind == TP_FIELD_GRID) ? t->nodes_E : 0;
     const int64_t nB = (eb || t->B->desc.kind == TP_FIELD_GRID) ? t->nodes_B : 0;
