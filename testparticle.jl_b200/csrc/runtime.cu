@@ -865,6 +865,7 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
     if (e == cudaSuccess) e = q_d.alloc(sizeof(unsigned long long));
     if (e == cudaSuccess) e = copy_to_device(ctx, u0_d.p, u0, (size_t)ns * 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st_d.p, 0, sizeof(int32_t), ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, std::string("autotune buffers: ") + cudaGetErrorString(e));
     BorisArgs a;
@@ -942,7 +943,8 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
         return st;
     }
     int32_t dev_status = 0;
-    e = cudaMemcpy(&dev_status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(&dev_status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess && dev_status != 0 && dev_status != TP_E_OVERFLOW) {
         if (had) ctx->tuned[key] = old;
         return status_to_error(ctx, dev_status);
