@@ -396,6 +396,7 @@ def main():
     ap.add_argument("--no-legs", action="store_true", help="skip the dipole / guiding-centre legs")
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (profiling)")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling)")
     ap.add_argument("--adj-n", type=int, default=1 << 18)
     ap.add_argument("--adj-nt", type=int, default=4096)
     args = ap.parse_args()
@@ -427,8 +428,9 @@ def main():
 
     p32, p64 = _plan(tp, w, alg, "fp32c", local), _plan(tp, w, alg, "fp64", local)
     # launch shapes chosen by the autotuner on a sample (untimed)
-    tune = {"fp32c": ctx.autotune(p32.desc, p32.E, p32.B, p32.u0, max_steps=200),
-            "fp64": ctx.autotune(p64.desc, p64.E, p64.B, p64.u0, max_steps=200)}
+    tune = None if args.no_autotune else {
+        "fp32c": ctx.autotune(p32.desc, p32.E, p32.B, p32.u0, max_steps=200),
+        "fp64": ctx.autotune(p64.desc, p64.E, p64.B, p64.u0, max_steps=200)}
     run = DeviceRun(tp, torch, ctx, p32, dev, stream)
 
     # ---- FP32C (headline), clocks sampled during the timed region
