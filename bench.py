@@ -380,6 +380,23 @@ def leg_gc(tp, n):
     return out
 
 
+def profile_case(tp, case, device):
+    """Small untimed runs of the adaptive and guiding-centre kernels, for ncu captures."""
+    if case == "adaptive":
+        w = tp.workloads.config3(n=262144, nt=200, ssi=200)
+        prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+        for prec in ("fp32c", "fp64"):
+            tp.solve(prob, tp.AdaptiveBoris(0.1), tp.EnsembleB200(device=device, precision=prec),
+                     savestepinterval=200, isoutside=w.isoutside, tend=w.tend, step_cap=200)
+    else:
+        w = tp.workloads.config4(1 << 18)
+        prob = tp.TraceGCProblem(w.y0, (0.0, 1.0), (w.q, w.q2m, w.mu, w.E, w.B))
+        for alg, kw in (("rk4", dict(dt=w.tau_b / 200)), ("rk45", dict(abstol=1e-9, reltol=1e-6))):
+            for prec in ("fp64", "fp32"):
+                tp.solve(prob, tp.EnsembleB200(device=device, precision=prec), alg=alg, tend=w.tau_b,
+                         savestepinterval=100000, maxiters=1_000_000, **kw)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -397,6 +414,10 @@ def main():
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (profiling)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling)")
+    ap.add_argument("--profile-case", choices=["adaptive", "gc"], default=None,
+                    help="run one small untimed case for an ncu capture: AdaptiveBoris(0.1) in the dipole "
+                         "(262144 protons, 200 steps, FP32C then FP64) or guiding centres in the dipole "
+                         "(2^18 particles, one bounce period, RK4 then RK45, FP64 then float32 RHS)")
     ap.add_argument("--adj-n", type=int, default=1 << 18)
     ap.add_argument("--adj-nt", type=int, default=4096)
     args = ap.parse_args()
@@ -413,6 +434,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     tp = ge.load_package()
     ctx = tp.Context.get(local)
+    if args.profile_case:
+        profile_case(tp, args.profile_case, local)
+        return
     if args.adjoint_only:
         dev = torch.device("cuda", local)
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
