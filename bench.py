@@ -362,7 +362,7 @@ def leg_gc(tp, n):
     for prec in ("fp64", "fp32"):
         for alg, kw in (("rk4", dict(dt=w.tau_b / 200)), ("rk45", dict(abstol=1e-9, reltol=1e-6))):
             s = tp.solve(prob, tp.EnsembleB200(precision=prec), alg=alg, tend=5 * w.tau_b, savestepinterval=100000,
-                         maxiters=1_000_000, **kw)
+                         save_everystep=False, maxiters=1_000_000, **kw)
             res[(prec, alg)] = s
             out[f"{alg}_{prec}"] = {"value": s.particle_steps() / s.elapsedTime, "unit": "particle-steps/s",
                                     "device_s": s.elapsedTime}
@@ -394,7 +394,7 @@ def profile_case(tp, case, device):
         for alg, kw in (("rk4", dict(dt=w.tau_b / 200)), ("rk45", dict(abstol=1e-9, reltol=1e-6))):
             for prec in ("fp64", "fp32"):
                 tp.solve(prob, tp.EnsembleB200(device=device, precision=prec), alg=alg, tend=w.tau_b,
-                         savestepinterval=100000, maxiters=1_000_000, **kw)
+                         savestepinterval=100000, save_everystep=False, maxiters=1_000_000, **kw)
 
 
 def main():

@@ -387,8 +387,10 @@ __device__ __forceinline__ void update_dp5(const RHS& f, const DevFields& F, con
                           gscale(e7, k7)));
 }
 
+// Register cap 168 (65536 / 384): three blocks of 128 threads per SM for the
+// float64 right-hand side instead of two, for a few bytes of spill.
 template <class RHS, bool QUEUE>
-__global__ void __launch_bounds__(256) k_rk45(GCArgs a) {
+__global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
     const RHS f;
     const GCSaver<RHS::kGrid> S(a);
     const uint64_t t_start = globaltimer_ns();
