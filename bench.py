@@ -183,7 +183,7 @@ class DeviceRun:
         self.nslots = ctx.slots(plan.desc, n, plan.dt_i, plan.tend_i)
         if self.nslots < 0:
             raise SystemExit("bench runs need a bounded number of saves (set step_cap for adaptive runs)")
-        W = 12 if plan.desc.save_fields else 6
+        W = 6 + 6 * bool(plan.desc.save_fields) + 4 * bool(plan.desc.save_work)
         f = lambda a: None if a is None else torch.from_numpy(a).to(dev)  # noqa: E731
         self.u0, self.dt_i, self.tend_i = f(plan.u0), f(plan.dt_i), f(plan.tend_i)
         self.t_out = torch.empty((self.nslots, n), dtype=torch.float64, device=dev)

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define TP_ABI_VERSION 1
+#define TP_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -167,6 +167,9 @@ typedef struct tp_run_desc {
     int32_t schedule;        /* TP_SCHED_*                                  */
     int32_t block;           /* threads per block, 0 = tuned / default      */
     double budget_s;         /* device wall-clock budget, 0 = default 600 s */
+    int32_t save_work;       /* append (P_par, P_fermi, P_grad, P_betatron)
+                                to every save (boris.jl:405-440)            */
+    int32_t reserved3;
 } tp_run_desc;
 
 /* ---- guiding-centre run ------------------------------------------------- */
@@ -189,6 +192,8 @@ typedef struct tp_gc_desc {
     int32_t block;
     int32_t reserved2;
     double budget_s;
+    int32_t save_work;       /* append the work rates (gc_solver.jl:233-248) */
+    int32_t reserved3;
 } tp_gc_desc;
 
 typedef struct tp_ctx tp_ctx;
@@ -235,7 +240,8 @@ int tp_boris_slots(const tp_run_desc* desc, const double* dt_i,
 /* Device-buffer variant: every pointer is device memory, the call is
  * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
  * Outputs are slot-major structure-of-arrays:
- *   t_out[k*n + i], u_out[(k*width + c)*n + i]  (width 6, or 12 with fields)
+ *   t_out[k*n + i], u_out[(k*width + c)*n + i]  (width 6, + 6 with fields,
+ *   + 4 with work rates)
  * nsaved[i] save count, retcode[i] TP_RET_*, nsteps[i] steps taken.
  * status (device int32) receives a TP_E_* code from the kernel, or 0.      */
 int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* desc,

@@ -185,7 +185,7 @@ def boris_run(desc, E, B, u0: np.ndarray, dt_i=None, tend_i=None, nthreads: int 
     L = lib()
     u0 = np.ascontiguousarray(u0, dtype=np.float64)
     n = u0.shape[0]
-    W = 12 if desc.save_fields else 6
+    W = 6 + 6 * bool(desc.save_fields) + 4 * bool(desc.save_work)
     Ed, Ecb = _field_arg(E)
     Bd, Bcb = _field_arg(B)
     tcb = term_callback(isoutside) if isoutside is not None else None
@@ -258,7 +258,7 @@ def gc_run(desc, E, B, y0: np.ndarray, q_i=None, q2m_i=None, mu_i=None, nthreads
     L = lib()
     y0 = np.ascontiguousarray(y0, dtype=np.float64)
     n = y0.shape[0]
-    W = 10 if desc.save_fields else 4
+    W = 4 + 6 * bool(desc.save_fields) + 4 * bool(desc.save_work)
     Ed, Ecb = _field_arg(E)
     Bd, Bcb = _field_arg(B)
     tcb = term_callback(isoutside) if isoutside is not None else None

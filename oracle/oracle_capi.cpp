@@ -285,7 +285,8 @@ int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_
     if (d->savestepinterval < 1) return TP_E_ARG;
     Term term = make_term(&d->term, tcb);
     Params p{d->q2m, d->m, E.get(), B.get()};
-    const int W = d->save_fields ? 12 : 6;
+    const int W = 6 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
+    const int save_mask = (d->save_fields ? 1 : 0) | (d->save_work ? 2 : 0);
     const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
     const bool multistep = d->alg == TP_ALG_MULTISTEP || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
 
@@ -321,7 +322,7 @@ int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_
             o.save_start = d->save_start != 0;
             o.save_end = d->save_end != 0;
             o.save_everystep = d->save_everystep != 0;
-            o.save_fields = d->save_fields != 0;
+            o.save_fields = save_mask;
             if (multistep)
                 boris_single(MultistepUpdater{d->order, d->nsub}, p, o, term, ui, tr);
             else
@@ -330,10 +331,10 @@ int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_
             if (multistep)
                 adaptive_single(MultistepUpdater{d->order, d->nsub}, p, d->t0, t1, d->safety,
                                 d->savestepinterval, d->save_start, d->save_end,
-                                d->save_everystep, d->save_fields, d->step_cap, term, ui, tr);
+                                d->save_everystep, save_mask, d->step_cap, term, ui, tr);
             else
                 adaptive_single(BorisUpdater{}, p, d->t0, t1, d->safety, d->savestepinterval,
-                                d->save_start, d->save_end, d->save_everystep, d->save_fields,
+                                d->save_start, d->save_end, d->save_everystep, save_mask,
                                 d->step_cap, term, ui, tr);
         }
         if (!store(tr, i, n, W, nslots, t_out, u_out, nsaved, retcode, nsteps)) overflow |= 1;
@@ -350,7 +351,7 @@ int orc_gc_run(const tp_gc_desc* d, const tp_field_desc* Ed, const tp_field_desc
     std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
     if (!E || !B) return TP_E_ARG;
     Term term = make_term(&d->term, tcb);
-    const int W = d->save_fields ? 10 : 4;
+    const int W = 4 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
     // _prepare_gc, src/gc/gc_solver.jl:187-231
     GCOpts o;
     o.t0 = d->t0;
@@ -362,7 +363,7 @@ int orc_gc_run(const tp_gc_desc* d, const tp_field_desc* Ed, const tp_field_desc
     o.save_start = d->save_start != 0;
     o.save_end = d->save_end != 0;
     o.save_everystep = d->save_everystep != 0;
-    o.save_fields = d->save_fields != 0;
+    o.save_fields = (d->save_fields ? 1 : 0) | (d->save_work ? 2 : 0);
     o.abstol = d->abstol;
     o.reltol = d->reltol;
     double ttotal = d->t1 - d->t0;

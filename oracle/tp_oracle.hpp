@@ -80,6 +80,8 @@ struct Field {
     virtual ~Field() {}
     virtual V3d eval(V3d r, double t) const = 0;
     virtual void jac(V3d r, double t, V3d& F, M3& J) const = 0;
+    // dF/dt (derivative_t, src/prepare.jl:64-74): zero for static fields
+    virtual V3d dtime(V3d, double) const { return {0.0, 0.0, 0.0}; }
 };
 
 struct ZeroField : Field {
@@ -116,6 +118,7 @@ struct AffineField : Field {
         F = eval(r, t);
         J = Jm;
     }
+    V3d dtime(V3d, double) const override { return rate; }
 };
 
 // Point dipole B(x) = coef (3 (m.rhat) rhat - m) / d^3, d = |x - c|, evaluated
@@ -276,6 +279,13 @@ struct CallbackField : Field {
         f(x, t, o, user);
         return {o[0], o[1], o[2]};
     }
+    // dF/dt by a central difference (the tests' closures are smooth in t;
+    // ForwardDiff.derivative takes it exactly)
+    V3d dtime(V3d r, double t) const override {
+        double h = 1.0e-6 * std::max(std::fabs(t), 1.0e-12);
+        V3d a = eval(r, t + h), b = eval(r, t - h);
+        return (a - b) / (2.0 * h);
+    }
     void jac(V3d r, double t, V3d& F, M3& J) const override {
         F = eval(r, t);
         if (jf) {
@@ -432,21 +442,77 @@ struct Traj {
     int64_t nsteps = 0;
 };
 
-inline void push_save(Traj& out, const Params& p, bool save_fields, V3d r, V3d v, double t) {
+// get_magnetic_properties, src/utility/utility.jl:409-422, with _get_curvature
+// (:379-384): grad|B| = JB' b, kappa = (JB b + b (-grad|B| . b)) / |B|
+struct MagProps {
+    V3d B, gradB, kappa, bh;
+    double Bmag;
+};
+inline MagProps magnetic_properties(const Field& Bf, V3d r, double t) {
+    MagProps m;
+    M3 J;
+    Bf.jac(r, t, m.B, J);
+    m.Bmag = norm(m.B);
+    if (m.Bmag == 0.0) {
+        m.gradB = m.kappa = m.bh = V3d{0.0, 0.0, 0.0};
+        return m;
+    }
+    V3d b = m.B / m.Bmag;
+    m.bh = b;
+    m.gradB = {(J(0, 0) * b.x + J(1, 0) * b.y) + J(2, 0) * b.z, (J(0, 1) * b.x + J(1, 1) * b.y) + J(2, 1) * b.z,
+               (J(0, 2) * b.x + J(1, 2) * b.y) + J(2, 2) * b.z};
+    V3d Jb{(J(0, 0) * b.x + J(0, 1) * b.y) + J(0, 2) * b.z, (J(1, 0) * b.x + J(1, 1) * b.y) + J(1, 2) * b.z,
+           (J(2, 0) * b.x + J(2, 1) * b.y) + J(2, 2) * b.z};
+    m.kappa = (Jb + b * (-dot(m.gradB, b))) / m.Bmag;
+    return m;
+}
+
+// the four work rates (P_par, P_fermi, P_grad, P_betatron) of
+// get_work_rates (src/equations.jl:394-441) and get_work_rates_gc (:445-480)
+inline void work_terms(const MagProps& mp, V3d E, V3d dBdt, double q, double m, double vpar, double mu,
+                       double* W) {
+    W[0] = q * vpar * dot(E, mp.bh);
+    W[1] = (m * (vpar * vpar) / mp.Bmag) * dot(cross(mp.bh, mp.kappa), E);
+    W[2] = (mu / mp.Bmag) * dot(cross(mp.bh, mp.gradB), E);
+    W[3] = mu * dot(dBdt, mp.bh);
+}
+
+inline void work_rates(const Params& p, V3d r, V3d v, double t, double* W) {
+    double q = p.q2m * p.m;
+    V3d E = p.E->eval(r, t);
+    MagProps mp = magnetic_properties(*p.B, r, t);
+    if (mp.Bmag == 0.0) {
+        W[0] = W[1] = W[2] = W[3] = 0.0;
+        return;
+    }
+    double vpar = dot(v, mp.bh);
+    V3d vperp = v - vpar * mp.bh;
+    double mu = p.m * dot(vperp, vperp) / (2.0 * mp.Bmag);
+    work_terms(mp, E, p.B->dtime(r, t), q, p.m, vpar, mu, W);
+}
+
+// save flags: bit 0 = E and B (save_fields), bit 1 = work rates (save_work)
+inline void push_save(Traj& out, const Params& p, int save_fields, V3d r, V3d v, double t) {
     out.t.push_back(t);
     double s[6] = {r.x, r.y, r.z, v.x, v.y, v.z};
     out.u.insert(out.u.end(), s, s + 6);
-    if (save_fields) {  // _prepare_saved_data, src/boris/boris.jl:405-427
+    if (save_fields & 1) {  // _prepare_saved_data, src/boris/boris.jl:405-427
         V3d E = p.E->eval(r, t), B = p.B->eval(r, t);
         double f[6] = {E.x, E.y, E.z, B.x, B.y, B.z};
         out.u.insert(out.u.end(), f, f + 6);
+    }
+    if (save_fields & 2) {  // boris.jl:429-437
+        double w[4];
+        work_rates(p, r, v, t, w);
+        out.u.insert(out.u.end(), w, w + 4);
     }
 }
 
 struct FixedOpts {
     double t0, t1, dt;
     int64_t nt, nout, ssi;
-    bool save_start, save_end, save_everystep, save_fields;
+    bool save_start, save_end, save_everystep;
+    int save_fields;  // bit 0: E and B, bit 1: work rates
 };
 
 // _boris_single + _boris_loop!, src/boris/boris.jl:445-557
@@ -521,7 +587,7 @@ void boris_single(const Upd& upd, const Params& p, const FixedOpts& o, const Ter
 template <class Upd>
 void adaptive_single(const Upd& upd, const Params& p, double t0, double t1, double safety,
                      int64_t ssi, bool save_start, bool save_end, bool save_everystep,
-                     bool save_fields, int64_t step_cap, const Term& term, const double* u0,
+                     int save_fields, int64_t step_cap, const Term& term, const double* u0,
                      Traj& out) {
     const double twopi = 6.283185307179586;  // Float64(2pi)
     double sgn = (t1 - t0) > 0 ? 1.0 : ((t1 - t0) < 0 ? -1.0 : 0.0);
@@ -639,15 +705,27 @@ inline GCState update_rk4(const GCState& y, const GCParams& p, double dt, double
     return gscale(dt / 6.0, sum);
 }
 
-inline void push_gc_save(Traj& out, const GCParams& p, bool save_fields, const GCState& s,
+// save flags: bit 0 = E and B, bit 1 = work rates (get_work_rates_gc)
+inline void push_gc_save(Traj& out, const GCParams& p, int save_fields, const GCState& s,
                          double t) {
     out.t.push_back(t);
     out.u.insert(out.u.end(), s.y, s.y + 4);
-    if (save_fields) {  // _prepare_saved_data_gc, src/gc/gc_solver.jl:233-248
-        V3d X{s.y[0], s.y[1], s.y[2]};
+    V3d X{s.y[0], s.y[1], s.y[2]};
+    if (save_fields & 1) {  // _prepare_saved_data_gc, src/gc/gc_solver.jl:233-248
         V3d E = p.E->eval(X, t), B = p.B->eval(X, t);
         double f[6] = {E.x, E.y, E.z, B.x, B.y, B.z};
         out.u.insert(out.u.end(), f, f + 6);
+    }
+    if (save_fields & 2) {
+        double w[4];
+        V3d E = p.E->eval(X, t);
+        MagProps mp = magnetic_properties(*p.B, X, t);
+        if (mp.Bmag == 0.0) {
+            w[0] = w[1] = w[2] = w[3] = 0.0;
+        } else {
+            work_terms(mp, E, p.B->dtime(X, t), p.q, p.q / p.q2m, s.y[3], p.mu, w);
+        }
+        out.u.insert(out.u.end(), w, w + 4);
     }
 }
 
@@ -655,7 +733,8 @@ struct GCOpts {
     double t0, t1, dt;
     bool dt_given;
     int64_t nt, nout, ssi, maxiters;
-    bool save_start, save_end, save_everystep, save_fields;
+    bool save_start, save_end, save_everystep;
+    int save_fields;  // bit 0: E and B, bit 1: work rates
     double abstol, reltol;
 };
 

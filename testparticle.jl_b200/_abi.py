@@ -12,7 +12,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libtpb200.so"
 
-TP_ABI_VERSION = 1
+TP_ABI_VERSION = 2
 
 TP_OK = 0
 TP_E_ARG = -1
@@ -121,6 +121,8 @@ class RunDesc(C.Structure):
         ("schedule", C.c_int32),
         ("block", C.c_int32),
         ("budget_s", C.c_double),
+        ("save_work", C.c_int32),
+        ("reserved3", C.c_int32),
     ]
 
 
@@ -148,6 +150,8 @@ class GCDesc(C.Structure):
         ("block", C.c_int32),
         ("reserved2", C.c_int32),
         ("budget_s", C.c_double),
+        ("save_work", C.c_int32),
+        ("reserved3", C.c_int32),
     ]
 
 

@@ -29,8 +29,10 @@ template <int FK>
 struct Saver64 {
     const BorisArgs& a;
     int W;
-    __device__ Saver64(const BorisArgs& a_) : a(a_), W(a_.save_fields ? 12 : 6) {}
-    // slot k of particle i; fields evaluated at (r, t) when save_fields
+    __device__ Saver64(const BorisArgs& a_)
+        : a(a_), W(6 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
+    // slot k of particle i: state, then E and B at (r, t) when save_fields,
+    // then the work rates when save_work (_prepare_saved_data, boris.jl:405-440)
     __device__ __forceinline__ void save(int64_t i, int64_t k, D3 r, D3 v, double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
@@ -45,7 +47,7 @@ struct Saver64 {
         u[3 * n] = v.x;
         u[4 * n] = v.y;
         u[5 * n] = v.z;
-        if (W == 12) {
+        if (a.save_fields) {
             D3 E, B;
             eval_EB64t<FK>(a.f, r, t, E, B);
             u[6 * n] = E.x;
@@ -54,6 +56,12 @@ struct Saver64 {
             u[9 * n] = B.x;
             u[10 * n] = B.y;
             u[11 * n] = B.z;
+        }
+        if (a.save_work) {
+            double w[4];
+            work_rates64<FK != FK_ANALYTIC>(a.f, r, v, t, a.q2m, a.m, w);
+            const int c0 = a.save_fields ? 12 : 6;
+            for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
     }
 };

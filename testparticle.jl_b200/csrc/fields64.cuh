@@ -339,4 +339,170 @@ __device__ __forceinline__ bool outside64(const DevTerm& T, D3 r, D3 v, double t
     return false;
 }
 
+// B and its Jacobian (row-major J[i][j] = dB_i/dx_j), float64, in the order
+// of the CPU restatement (the role of ForwardDiff in _get_B_jacobian,
+// src/utility/utility.jl:386-392)
+template <bool GRID>
+__device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
+    for (int k = 0; k < 9; ++k) J[k] = 0.0;
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            F = {f.v[0], f.v[1], f.v[2]};
+            return;
+        case TP_FIELD_AFFINE:
+            F = analytic_eval64(f, r, t);
+            for (int k = 0; k < 9; ++k) J[k] = f.J[k];
+            return;
+        case TP_FIELD_DIPOLE: {
+            F = analytic_eval64(f, r, t);
+            D3 d = r - D3{f.c[0], f.c[1], f.c[2]};
+            double d2 = abs2sum(d);
+            double dm = sqrt(d2);
+            double inv5 = 1.0 / ((d2 * d2) * dm);
+            double inv7 = inv5 / d2;
+            double md = dot(D3{f.m[0], f.m[1], f.m[2]}, d);
+            double dv[3] = {d.x, d.y, d.z};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double dij = (i == j) ? md : 0.0;
+                    J[3 * i + j] = f.coef * (3.0 * ((f.m[j] * dv[i] + dij) + f.m[i] * dv[j]) * inv5 -
+                                             15.0 * md * dv[i] * dv[j] * inv7);
+                }
+            return;
+        }
+        case TP_FIELD_GRID: {
+            if (!GRID) {
+                F = {0.0, 0.0, 0.0};
+                return;
+            }
+            Ax ax, ay, az;
+            if (!grid_axes64(f, r, ax, ay, az)) {
+                F = nan3();
+                for (int k = 0; k < 9; ++k) J[k] = F.x;
+                return;
+            }
+            F = tri64(f, f.tab, f.f64 != 0, 1, 0, ax, ay, az);
+            double sx = f.inv_dx[0], sy = f.inv_dx[1], sz = f.inv_dx[2];
+            if (f.bc == TP_BC_CLAMP) {
+                double ux = (r.x - f.x0[0]) * f.inv_dx[0], uy = (r.y - f.x0[1]) * f.inv_dx[1],
+                       uz = (r.z - f.x0[2]) * f.inv_dx[2];
+                if (ux < 0.0 || ux > (double)(f.n[0] - 1)) sx = 0.0;
+                if (uy < 0.0 || uy > (double)(f.n[1] - 1)) sy = 0.0;
+                if (uz < 0.0 || uz > (double)(f.n[2] - 1)) sz = 0.0;
+            }
+            const int64_t nx = f.n[0], nxy = (int64_t)f.n[0] * f.n[1];
+            int64_t j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
+            bool f64 = f.f64 != 0;
+            D3 w000 = load_node(f.tab, f64, ax.i0 + j0 + k0), w100 = load_node(f.tab, f64, ax.i1 + j0 + k0);
+            D3 w010 = load_node(f.tab, f64, ax.i0 + j1 + k0), w110 = load_node(f.tab, f64, ax.i1 + j1 + k0);
+            D3 w001 = load_node(f.tab, f64, ax.i0 + j0 + k1), w101 = load_node(f.tab, f64, ax.i1 + j0 + k1);
+            D3 w011 = load_node(f.tab, f64, ax.i0 + j1 + k1), w111 = load_node(f.tab, f64, ax.i1 + j1 + k1);
+            double fx = ax.f, fy = ay.f, fz = az.f;
+#define TPB_GJ(c, row)                                                                  \
+    {                                                                                   \
+        double v000 = w000.c, v100 = w100.c, v010 = w010.c, v110 = w110.c;              \
+        double v001 = w001.c, v101 = w101.c, v011 = w011.c, v111 = w111.c;              \
+        double dx00 = v100 - v000, dx10 = v110 - v010, dx01 = v101 - v001, dx11 = v111 - v011; \
+        double dx0 = lerp64(dx00, dx10, fy), dx1 = lerp64(dx01, dx11, fy);              \
+        J[3 * row + 0] = lerp64(dx0, dx1, fz) * sx;                                     \
+        double c00 = lerp64(v000, v100, fx), c10 = lerp64(v010, v110, fx);              \
+        double c01 = lerp64(v001, v101, fx), c11 = lerp64(v011, v111, fx);              \
+        J[3 * row + 1] = lerp64(c10 - c00, c11 - c01, fz) * sy;                         \
+        double c0 = lerp64(c00, c10, fy), c1 = lerp64(c01, c11, fy);                    \
+        J[3 * row + 2] = (c1 - c0) * sz;                                                \
+    }
+            TPB_GJ(x, 0)
+            TPB_GJ(y, 1)
+            TPB_GJ(z, 2)
+#undef TPB_GJ
+            return;
+        }
+        default:
+            F = {0.0, 0.0, 0.0};
+            return;
+    }
+}
+
+template <bool GRID>
+__device__ __forceinline__ D3 field_val64(const DevField& f, D3 r, double t) {
+    if (GRID) return field_eval64(f, r, t);
+    return analytic_eval64(f, r, t);
+}
+
+// get_magnetic_properties (src/utility/utility.jl:409-422) with
+// _get_curvature (:379-384): B, grad|B| = JB^T b, curvature
+// kappa = (JB b - b (grad|B| . b)) / |B|, b = B / |B|
+struct MagProps {
+    D3 B, gradB, kappa, bh;
+    double Bmag;
+};
+
+template <bool GRID>
+__device__ __forceinline__ MagProps magnetic_properties64(const DevField& f, D3 r, double t) {
+    MagProps m;
+    double J[9];
+    field_jac64<GRID>(f, r, t, m.B, J);
+    m.Bmag = norm(m.B);
+    if (m.Bmag == 0.0) {
+        m.gradB = m.kappa = m.bh = D3{0.0, 0.0, 0.0};
+        return m;
+    }
+    const D3 b = m.B / m.Bmag;
+    m.bh = b;
+    m.gradB = {(J[0] * b.x + J[3] * b.y) + J[6] * b.z, (J[1] * b.x + J[4] * b.y) + J[7] * b.z,
+               (J[2] * b.x + J[5] * b.y) + J[8] * b.z};
+    const D3 Jb{(J[0] * b.x + J[1] * b.y) + J[2] * b.z, (J[3] * b.x + J[4] * b.y) + J[5] * b.z,
+                (J[6] * b.x + J[7] * b.y) + J[8] * b.z};
+    m.kappa = (Jb + b * (-dot(m.gradB, b))) / m.Bmag;
+    return m;
+}
+
+// dB/dt of a field: the rate of a time-dependent affine field, else 0
+// (derivative_t, src/prepare.jl:64-74)
+__device__ __forceinline__ D3 field_dtime64(const DevField& f) {
+    if (f.kind == TP_FIELD_AFFINE) return {f.rate[0], f.rate[1], f.rate[2]};
+    return {0.0, 0.0, 0.0};
+}
+
+// The four work rates of a saved state (P_par, P_fermi, P_grad, P_betatron)
+// from E, the magnetic properties, v_par and mu (get_work_rates,
+// src/equations.jl:394-441; get_work_rates_gc, :445-480)
+__device__ __forceinline__ void work_terms64(const MagProps& mp, D3 E, D3 dBdt, double q, double m, double vpar,
+                                             double mu, double* W) {
+    W[0] = q * vpar * dot(E, mp.bh);
+    W[1] = (m * (vpar * vpar) / mp.Bmag) * dot(cross(mp.bh, mp.kappa), E);
+    W[2] = (mu / mp.Bmag) * dot(cross(mp.bh, mp.gradB), E);
+    W[3] = mu * dot(dBdt, mp.bh);
+}
+
+// full orbit: v_par = v . b, mu = m |v - v_par b|^2 / (2 |B|), q = q2m m
+template <bool GRID>
+__device__ __forceinline__ void work_rates64(const DevFields& F, D3 r, D3 v, double t, double q2m, double m,
+                                             double* W) {
+    const double q = q2m * m;
+    const D3 E = field_val64<GRID>(F.E, r, t);
+    const MagProps mp = magnetic_properties64<GRID>(F.B, r, t);
+    if (mp.Bmag == 0.0) {
+        W[0] = W[1] = W[2] = W[3] = 0.0;
+        return;
+    }
+    const double vpar = dot(v, mp.bh);
+    const D3 vperp = v - vpar * mp.bh;
+    const double mu = m * dot(vperp, vperp) / (2.0 * mp.Bmag);
+    work_terms64(mp, E, field_dtime64(F.B), q, m, vpar, mu, W);
+}
+
+// guiding centre: state (X, v_par), mu given, m = q / q2m
+template <bool GRID>
+__device__ __forceinline__ void work_rates_gc64(const DevFields& F, D3 X, double vpar, double t, double q,
+                                                double q2m, double mu, double* W) {
+    const D3 E = field_val64<GRID>(F.E, X, t);
+    const MagProps mp = magnetic_properties64<GRID>(F.B, X, t);
+    if (mp.Bmag == 0.0) {
+        W[0] = W[1] = W[2] = W[3] = 0.0;
+        return;
+    }
+    work_terms64(mp, E, field_dtime64(F.B), q, q / q2m, vpar, mu, W);
+}
+
 }  // namespace tpb

@@ -27,96 +27,6 @@ struct GCPar {
     double q, q2m, mu;
 };
 
-// B and its Jacobian (row-major J[i][j] = dB_i/dx_j), float64, in the order
-// of the CPU restatement (the role of ForwardDiff in _get_B_jacobian,
-// src/utility/utility.jl:386-392)
-template <bool GRID>
-__device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
-    for (int k = 0; k < 9; ++k) J[k] = 0.0;
-    switch (f.kind) {
-        case TP_FIELD_UNIFORM:
-            F = {f.v[0], f.v[1], f.v[2]};
-            return;
-        case TP_FIELD_AFFINE:
-            F = analytic_eval64(f, r, t);
-            for (int k = 0; k < 9; ++k) J[k] = f.J[k];
-            return;
-        case TP_FIELD_DIPOLE: {
-            F = analytic_eval64(f, r, t);
-            D3 d = r - D3{f.c[0], f.c[1], f.c[2]};
-            double d2 = abs2sum(d);
-            double dm = sqrt(d2);
-            double inv5 = 1.0 / ((d2 * d2) * dm);
-            double inv7 = inv5 / d2;
-            double md = dot(D3{f.m[0], f.m[1], f.m[2]}, d);
-            double dv[3] = {d.x, d.y, d.z};
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    double dij = (i == j) ? md : 0.0;
-                    J[3 * i + j] = f.coef * (3.0 * ((f.m[j] * dv[i] + dij) + f.m[i] * dv[j]) * inv5 -
-                                             15.0 * md * dv[i] * dv[j] * inv7);
-                }
-            return;
-        }
-        case TP_FIELD_GRID: {
-            if (!GRID) {
-                F = {0.0, 0.0, 0.0};
-                return;
-            }
-            Ax ax, ay, az;
-            if (!grid_axes64(f, r, ax, ay, az)) {
-                F = nan3();
-                for (int k = 0; k < 9; ++k) J[k] = F.x;
-                return;
-            }
-            F = tri64(f, f.tab, f.f64 != 0, 1, 0, ax, ay, az);
-            double sx = f.inv_dx[0], sy = f.inv_dx[1], sz = f.inv_dx[2];
-            if (f.bc == TP_BC_CLAMP) {
-                double ux = (r.x - f.x0[0]) * f.inv_dx[0], uy = (r.y - f.x0[1]) * f.inv_dx[1],
-                       uz = (r.z - f.x0[2]) * f.inv_dx[2];
-                if (ux < 0.0 || ux > (double)(f.n[0] - 1)) sx = 0.0;
-                if (uy < 0.0 || uy > (double)(f.n[1] - 1)) sy = 0.0;
-                if (uz < 0.0 || uz > (double)(f.n[2] - 1)) sz = 0.0;
-            }
-            const int64_t nx = f.n[0], nxy = (int64_t)f.n[0] * f.n[1];
-            int64_t j0 = ay.i0 * nx, j1 = ay.i1 * nx, k0 = az.i0 * nxy, k1 = az.i1 * nxy;
-            bool f64 = f.f64 != 0;
-            D3 w000 = load_node(f.tab, f64, ax.i0 + j0 + k0), w100 = load_node(f.tab, f64, ax.i1 + j0 + k0);
-            D3 w010 = load_node(f.tab, f64, ax.i0 + j1 + k0), w110 = load_node(f.tab, f64, ax.i1 + j1 + k0);
-            D3 w001 = load_node(f.tab, f64, ax.i0 + j0 + k1), w101 = load_node(f.tab, f64, ax.i1 + j0 + k1);
-            D3 w011 = load_node(f.tab, f64, ax.i0 + j1 + k1), w111 = load_node(f.tab, f64, ax.i1 + j1 + k1);
-            double fx = ax.f, fy = ay.f, fz = az.f;
-#define TPB_GJ(c, row)                                                                  \
-    {                                                                                   \
-        double v000 = w000.c, v100 = w100.c, v010 = w010.c, v110 = w110.c;              \
-        double v001 = w001.c, v101 = w101.c, v011 = w011.c, v111 = w111.c;              \
-        double dx00 = v100 - v000, dx10 = v110 - v010, dx01 = v101 - v001, dx11 = v111 - v011; \
-        double dx0 = lerp64(dx00, dx10, fy), dx1 = lerp64(dx01, dx11, fy);              \
-        J[3 * row + 0] = lerp64(dx0, dx1, fz) * sx;                                     \
-        double c00 = lerp64(v000, v100, fx), c10 = lerp64(v010, v110, fx);              \
-        double c01 = lerp64(v001, v101, fx), c11 = lerp64(v011, v111, fx);              \
-        J[3 * row + 1] = lerp64(c10 - c00, c11 - c01, fz) * sy;                         \
-        double c0 = lerp64(c00, c10, fy), c1 = lerp64(c01, c11, fy);                    \
-        J[3 * row + 2] = (c1 - c0) * sz;                                                \
-    }
-            TPB_GJ(x, 0)
-            TPB_GJ(y, 1)
-            TPB_GJ(z, 2)
-#undef TPB_GJ
-            return;
-        }
-        default:
-            F = {0.0, 0.0, 0.0};
-            return;
-    }
-}
-
-template <bool GRID>
-__device__ __forceinline__ D3 field_val64(const DevField& f, D3 r, double t) {
-    if (GRID) return field_eval64(f, r, t);
-    return analytic_eval64(f, r, t);
-}
-
 // get_gc_derivatives (src/equations.jl:329-360), float64
 template <bool GRID>
 struct RHS64 {
@@ -160,11 +70,18 @@ __device__ __forceinline__ bool outside_gc(const DevTerm& T, const G4& u, double
     return false;
 }
 
+__device__ __forceinline__ GCPar gc_par(const GCArgs& a, int64_t i) {
+    return {a.q_i ? a.q_i[i] : a.q, a.q2m_i ? a.q2m_i[i] : a.q2m, a.mu_i ? a.mu_i[i] : a.mu};
+}
+
 template <bool GRID>
 struct GCSaver {
     const GCArgs& a;
     int W;
-    __device__ GCSaver(const GCArgs& a_) : a(a_), W(a_.save_fields ? 10 : 4) {}
+    __device__ GCSaver(const GCArgs& a_)
+        : a(a_), W(4 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
+    // slot k: (X, v_par), then E and B when save_fields, then the work rates
+    // when save_work (_prepare_saved_data_gc, src/gc/gc_solver.jl:233-248)
     __device__ __forceinline__ void save(int64_t i, int64_t k, const G4& s, double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
@@ -174,8 +91,8 @@ struct GCSaver {
         a.t_out[k * n + i] = t;
         double* u = a.u_out + (k * W) * n + i;
         for (int c = 0; c < 4; ++c) u[c * n] = s.y[c];
-        if (W == 10) {
-            D3 X{s.y[0], s.y[1], s.y[2]};
+        const D3 X{s.y[0], s.y[1], s.y[2]};
+        if (a.save_fields) {
             D3 E = field_val64<GRID>(a.f.E, X, t), B = field_val64<GRID>(a.f.B, X, t);
             u[4 * n] = E.x;
             u[5 * n] = E.y;
@@ -183,6 +100,13 @@ struct GCSaver {
             u[7 * n] = B.x;
             u[8 * n] = B.y;
             u[9 * n] = B.z;
+        }
+        if (a.save_work) {
+            const GCPar p = gc_par(a, i);
+            double w[4];
+            work_rates_gc64<GRID>(a.f, X, s.y[3], t, p.q, p.q2m, p.mu, w);
+            const int c0 = a.save_fields ? 10 : 4;
+            for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
     }
 };
@@ -197,9 +121,6 @@ __device__ __forceinline__ int64_t gc_next(const GCArgs& a, int64_t& first) {
     return (int64_t)atomicAdd(a.queue, 1ULL);
 }
 
-__device__ __forceinline__ GCPar gc_par(const GCArgs& a, int64_t i) {
-    return {a.q_i ? a.q_i[i] : a.q, a.q2m_i ? a.q2m_i[i] : a.q2m, a.mu_i ? a.mu_i[i] : a.mu};
-}
 
 // update_rk4, src/gc/rk4_gc.jl:7-22
 template <class RHS>

@@ -637,6 +637,7 @@ int prepare_boris_args(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, tp_
     a.order = d->order;
     a.nsub = d->nsub;
     a.save_fields = d->save_fields;
+    a.save_work = d->save_work;
     a.save_start = d->save_start;
     a.save_end = d->save_end;
     a.save_everystep = d->save_everystep;
@@ -854,7 +855,7 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     int64_t nslots = 0;
     st = tp_boris_slots(&ds, nullptr, nullptr, ns, &nslots);
     if (st != TP_OK) return fail(ctx, st, "autotune sample sizing");
-    const int W = ds.save_fields ? 12 : 6;
+    const int W = 6 + (ds.save_fields ? 6 : 0) + (ds.save_work ? 4 : 0);
     DBuf u0_d, t_d, u_d, ns_d, rc_d, nst_d, st_d, q_d;
     cudaError_t e = u0_d.alloc((size_t)ns * 6 * sizeof(double));
     if (e == cudaSuccess) e = t_d.alloc((size_t)std::max<int64_t>(nslots, 1) * ns * sizeof(double));
@@ -1087,7 +1088,7 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
     st = tp_boris_slots(d, dt_i, tend_i, n, &nslots);
     if (st != TP_OK) return fail(ctx, st, "cannot size the output");
     if (nslots < 0) nslots = 64;  // adaptive without a cap: grown on overflow below
-    const int W = d->save_fields ? 12 : 6;
+    const int W = 6 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
     DeviceGuard g(ctx->device);
     AllocStream alloc_stream(ctx->stream);
     cudaStream_t s = ctx->stream;
@@ -1289,7 +1290,7 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
     }
     int64_t nslots = d->alg == TP_GC_RK4 ? std::max<int64_t>(nout, 0) : 64;
     if (d->alg == TP_GC_RK45 && !d->save_everystep) nslots = 2;
-    const int W = d->save_fields ? 10 : 4;
+    const int W = 4 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
     DeviceGuard g(ctx->device);
     AllocStream alloc_stream(ctx->stream);
     cudaStream_t s = ctx->stream;
@@ -1333,6 +1334,7 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
         a.alg = d->alg;
         a.precision = d->precision;
         a.save_fields = d->save_fields;
+        a.save_work = d->save_work;
         a.dt_given = d->dt_given;
         a.save_start = d->save_start;
         a.save_end = d->save_end;

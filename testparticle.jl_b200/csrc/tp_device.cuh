@@ -102,7 +102,7 @@ struct BorisArgs {
     uint64_t budget_ns;
     // FP32C only: per axis, wrap positions into the periodic box
     int32_t wrap[3];
-    int32_t pad2;
+    int32_t save_work;    // work rates appended to every save (width + 4)
     double wrapL[3], wrap0[3];
 };
 

@@ -38,7 +38,7 @@ struct GCArgs {
     int32_t* status;
     unsigned long long* queue;
     int32_t use_queue;
-    int32_t pad2;
+    int32_t save_work;    // work rates appended to every save (width + 4)
     uint64_t budget_ns;
 };
 

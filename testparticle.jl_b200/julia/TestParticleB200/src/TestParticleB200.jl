@@ -161,6 +161,7 @@ struct TpRunDesc
     savestepinterval::Int64; maxiters::Int64
     save_start::Int32; save_end::Int32; save_everystep::Int32; save_fields::Int32
     term::TpTermDesc; step_cap::Int64; schedule::Int32; block::Int32; budget_s::Float64
+    save_work::Int32; reserved3::Int32
 end
 struct TpGCDesc
     alg::Int32; precision::Int32; t0::Float64; t1::Float64; dt::Float64
@@ -168,6 +169,7 @@ struct TpGCDesc
     abstol::Float64; reltol::Float64; savestepinterval::Int64; maxiters::Int64
     save_start::Int32; save_end::Int32; save_everystep::Int32; save_fields::Int32
     term::TpTermDesc; block::Int32; reserved2::Int32; budget_s::Float64
+    save_work::Int32; reserved3::Int32
 end
 
 const Z3 = (0.0, 0.0, 0.0)
@@ -250,7 +252,7 @@ function collect_result(ctx, res, prob, alg_name, T)
 end
 
 function boris_run(ens::EnsembleB200, prob::TraceProblem, alg, adaptive, trajectories, dt, savestepinterval,
-        isoutside, save_start, save_end, save_everystep, save_fields, maxiters, seed, alg_name)
+        isoutside, save_start, save_end, save_everystep, save_fields, save_work, maxiters, seed, alg_name)
     ctx = context(ens.device)
     q2m, m, E, B, _ = prob.p
     hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
@@ -261,7 +263,7 @@ function boris_run(ens::EnsembleB200, prob::TraceProblem, alg, adaptive, traject
             ens.precision === :fp32c ? 1 : 0, alg.safety, prob.tspan[1], prob.tspan[2],
             isnothing(dt) ? 0.0 : dt, q2m, m, savestepinterval, maxiters,
             save_start, save_end, save_everystep, save_fields, termdesc(isoutside), 0,
-            ens.schedule === :static ? 1 : ens.schedule === :queue ? 2 : 0, 0, 0.0))
+            ens.schedule === :static ? 1 : ens.schedule === :queue ? 2 : 0, 0, 0.0, save_work, 0))
         U = initial_table(prob, trajectories, seed)
         res = Ref{Ptr{Cvoid}}(C_NULL)
         st = ccall((:tp_boris_run, libtpb200), Cint,
@@ -278,32 +280,30 @@ end
 function _solve(ens::EnsembleB200, prob::TraceProblem, alg::TestParticle.AbstractBoris, trajectories, dt,
         savestepinterval, isoutside, save_start, save_end, save_everystep,
         ::Val{SaveFields}, ::Val{SaveWork}, maxiters, batch_size, seed) where {SaveFields, SaveWork}
-    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
     name = alg isa MultistepBoris ? :multistep_boris : :boris
     return boris_run(ens, prob, alg, false, trajectories, dt, savestepinterval, isoutside, save_start,
-        save_end, save_everystep, SaveFields, maxiters, seed, name)
+        save_end, save_everystep, SaveFields, SaveWork, maxiters, seed, name)
 end
 
 function _solve_adaptive(ens::EnsembleB200, prob, trajectories, alg::TestParticle.AbstractBoris, savestepinterval,
         isoutside, save_start, save_end, save_everystep, ::Val{SaveFields}, ::Val{SaveWork},
         batch_size) where {SaveFields, SaveWork}
-    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
     name = alg isa Boris ? :adaptive_boris : :adaptive_multistep_boris
     return boris_run(ens, prob, alg, true, trajectories, nothing, savestepinterval, isoutside, save_start,
-        save_end, save_everystep, SaveFields, typemax(Int64), nothing, name)
+        save_end, save_everystep, SaveFields, SaveWork, typemax(Int64), nothing, name)
 end
 
 function _solve(ens::EnsembleB200, prob::TraceGCProblem, trajectories, dt, savestepinterval, isoutside,
         save_start, save_end, save_everystep, alg, abstol, reltol, maxiters,
         ::Val{SaveFields}, ::Val{SaveWork}, seed) where {SaveFields, SaveWork}
-    SaveWork && throw(ArgumentError("save_work is not supported by EnsembleB200"))
     ctx = context(ens.device)
     q, q2m, μ, E, B = prob.p
     hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
     try
         desc = Ref(TpGCDesc(alg == :rk45 ? 1 : 0, ens.precision === :fp64 ? 0 : 1, prob.tspan[1], prob.tspan[2],
             isnothing(dt) ? 0.0 : dt, isnothing(dt) ? 0 : 1, 0, q, q2m, μ, abstol, reltol, savestepinterval,
-            maxiters, save_start, save_end, save_everystep, SaveFields, termdesc(isoutside), 0, 0, 0.0))
+            maxiters, save_start, save_end, save_everystep, SaveFields, termdesc(isoutside), 0, 0, 0.0,
+            SaveWork, 0))
         Y = initial_table(prob, trajectories, seed)
         res = Ref{Ptr{Cvoid}}(C_NULL)
         st = ccall((:tp_gc_run, libtpb200), Cint,
@@ -331,7 +331,7 @@ end
 function adj_desc(q2m, m, dt, tspan, K)
     nt = round(Int, abs((tspan[2] - tspan[1]) / dt))
     TpAdjDesc(TpRunDesc(0, 2, 1, 1, 0.0, tspan[1], tspan[2], dt, q2m, m, 1, max(1_000_000, nt),
-        0, 1, 0, 0, termdesc(TestParticle.ODE_DEFAULT_ISOUTOFDOMAIN), 0, 0, 0, 0.0), K)
+        0, 1, 0, 0, termdesc(TestParticle.ODE_DEFAULT_ISOUTOFDOMAIN), 0, 0, 0, 0.0, 0, 0), K)
 end
 
 # tape and field handles of one recorded forward pass, released by the GC

@@ -86,8 +86,6 @@ def plan_boris(prob, balg, ens=None, *, trajectories=1, savestepinterval=1, dt=N
     ens = ens if ens is not None else EnsembleB200()
     if not isinstance(ens, EnsembleB200):
         raise NotImplementedError("this package runs ensembles on the B200 only: use EnsembleB200()")
-    if save_work:
-        raise NotImplementedError("save_work (work rates at save points) is not implemented on the B200 yet")
     adaptive = getattr(balg, "adaptive", False)
     if not adaptive and dt is None:
         raise TypeError("solve() with a fixed-step Boris algorithm needs dt")
@@ -117,6 +115,7 @@ def plan_boris(prob, balg, ens=None, *, trajectories=1, savestepinterval=1, dt=N
     desc.maxiters = int(1_000_000 if maxiters is None else maxiters)
     desc.save_start, desc.save_end = int(save_start), int(save_end)
     desc.save_everystep, desc.save_fields = int(save_everystep), int(save_fields)
+    desc.save_work = int(save_work)
     desc.term = as_term(isoutside).descriptor()
     desc.step_cap = int(step_cap)
     desc.schedule = _SCHED[ens.schedule]
@@ -136,8 +135,6 @@ def plan_gc(prob, ens=None, *, trajectories=1, savestepinterval=1, dt=None, isou
     ens = ens if ens is not None else EnsembleB200()
     if not isinstance(ens, EnsembleB200):
         raise NotImplementedError("this package runs ensembles on the B200 only: use EnsembleB200()")
-    if save_work:
-        raise NotImplementedError("save_work is not implemented on the B200 yet")
     alg = str(alg).lstrip(":")
     if alg not in ("rk4", "rk45"):
         import warnings
@@ -173,6 +170,7 @@ def plan_gc(prob, ens=None, *, trajectories=1, savestepinterval=1, dt=None, isou
     desc.maxiters = int(maxiters)
     desc.save_start, desc.save_end = int(save_start), int(save_end)
     desc.save_everystep, desc.save_fields = int(save_everystep), int(save_fields)
+    desc.save_work = int(save_work)
     desc.term = as_term(isoutside).descriptor()
     desc.block = int(ens.block)
     desc.budget_s = float(ens.budget_s)

@@ -22,10 +22,11 @@ from conftest import julia_isapprox
 pytestmark = pytest.mark.gpu
 
 
-def _rel(a, b):
+def _rel(a, b, blocks=None):
     """Largest relative difference of saved states, per vector: |dx|/|x| for the
     position (or guiding-centre position) and |dv|/|v| for the velocity block
-    (v_par for guiding centres; saved fields compared as one block each).
+    (v_par for guiding centres; saved fields compared as one block each; work
+    rates as one 4-vector).  `blocks` overrides the column grouping.
     NaN entries must coincide."""
     a = np.asarray(a, float)
     b = np.asarray(b, float)
@@ -41,8 +42,11 @@ def _rel(a, b):
     a = np.where(nan_a, 0.0, a)
     b = np.where(nan_b, 0.0, b)
     W = a.shape[1]
-    blocks = {1: [(0, 1)], 4: [(0, 3), (3, 4)], 6: [(0, 3), (3, 6)], 10: [(0, 3), (3, 4), (4, 7), (7, 10)],
-              12: [(0, 3), (3, 6), (6, 9), (9, 12)]}.get(W, [(c, c + 1) for c in range(W)])
+    if blocks is None:
+        blocks = {1: [(0, 1)], 4: [(0, 3), (3, 4)], 6: [(0, 3), (3, 6)],
+                  10: [(0, 3), (3, 4), (4, 7), (7, 10)], 12: [(0, 3), (3, 6), (6, 9), (9, 12)],
+                  14: [(0, 3), (3, 4), (4, 7), (7, 10), (10, 14)],
+                  16: [(0, 3), (3, 6), (6, 9), (9, 12), (12, 16)]}.get(W, [(c, c + 1) for c in range(W)])
     worst = 0.0
     for lo, hi in blocks:
         d = np.linalg.norm(a[:, lo:hi] - b[:, lo:hi], axis=1)
@@ -136,6 +140,81 @@ def test_save_fields_gpu(tp, orc):
     sols, ref = _both(tp, orc, prob, tp.Boris(), dt=w.dt, savestepinterval=50, save_fields=True)
     assert sols.u_all.shape[1] == 12
     assert _rel(sols.u_all, ref.u) <= 1e-13
+
+
+# ------------------------------------------------------------------ work rates at save points
+_WORK10 = [(0, 3), (3, 6), (6, 10)]   # full orbit: x, v, (P_par, P_fermi, P_grad, P_betatron)
+
+
+def _work_problem(tp, n=64, betatron=False):
+    """test_boris.jl:374-466 fields (constant_E and gradient_B, or the linear
+    betatron B), electrons with spread initial velocities."""
+    rng = np.random.default_rng(5)
+    u0 = np.zeros((6, n))
+    u0[:3] = rng.uniform(-1e-4, 1e-4, (3, n))
+    u0[3:] = rng.normal(0.0, 1.0e5, (3, n))
+    if betatron:
+        E, B = tp.ZeroField(), tp.AffineField((0.0, 0.0, 0.01), rate=(0.0, 0.0, 1.0e5))
+    else:
+        E = tp.UniformField((0.0, 1.0e5, 0.0))
+        B = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    return tp.TraceProblem(u0, (0.0, 1.0e-9), tp.prepare(E, B, species=tp.Electron))
+
+
+@pytest.mark.parametrize("alg", ["boris", "ms2n2", "ms4n2", "adaptive"])
+def test_save_work_matches_oracle(tp, orc, alg):
+    prob = _work_problem(tp)
+    a = {"boris": tp.Boris(), "ms2n2": tp.MultistepBoris(2, 2), "ms4n2": tp.MultistepBoris(4, 2),
+         "adaptive": tp.AdaptiveBoris(0.1)}[alg]
+    kw = dict(savestepinterval=1, save_work=True) if alg == "adaptive" else \
+        dict(dt=1.0e-11, savestepinterval=1, save_work=True)
+    sols, ref = _both(tp, orc, prob, a, **kw)
+    _check_same_layout(sols, ref)
+    assert sols.u_all.shape[1] == 10
+    tol = 1e-10 if alg.startswith("ms") else 1e-13   # CUDA vs glibc atan / sincos
+    assert _rel(sols.u_all, ref.u, _WORK10) <= tol
+    first = sols.u[0].u[0]
+    assert abs(first[6]) <= 1e-10 * 1e5 and abs(first[8]) > 0.0
+    # both flags: 16 columns, work after E and B, equal to the work-only run
+    s16, r16 = _both(tp, orc, prob, a, save_fields=True, **kw)
+    assert s16.u_all.shape[1] == 16
+    assert _rel(s16.u_all, r16.u) <= tol
+    assert np.array_equal(s16.u_all[:, 12:16], sols.u_all[:, 6:10])
+
+
+def test_save_work_betatron_gpu(tp, orc):
+    prob = _work_problem(tp, betatron=True)
+    sols, ref = _both(tp, orc, prob, tp.Boris(), dt=1.0e-11, savestepinterval=10, save_work=True)
+    _check_same_layout(sols, ref)
+    assert _rel(sols.u_all, ref.u, _WORK10) <= 1e-13
+    assert np.all(sols.u_all[:, 9] > 0.0)   # P_betatron = mu dB/dt . b > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_save_work_dipole_and_grid(tp, orc, precision):
+    w, prob, keep = _regular_dipole(tp, 128, 1000, 250)
+    w.dt, w.tend = w.dt[keep], w.tend[keep]
+    # a dawn-dusk electric field makes all three electric work terms nonzero
+    prob = tp.TraceProblem(prob.u0, prob.tspan, tp.prepare(tp.UniformField((0.0, 1.0e-3, 0.0)), w.B,
+                                                           species=tp.Proton))
+    ens = tp.EnsembleB200(precision=precision)
+    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside, save_work=True,
+              save_fields=True)
+    sols = tp.solve(prob, tp.Boris(), ens, **kw)
+    plan = tp.plan_boris(prob, tp.Boris(), **kw)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    _check_same_layout(sols, ref)
+    assert np.all(np.abs(ref.u[:, 12:15]).max(axis=0) > 0.0)
+    if precision == "fp64":
+        assert _rel(sols.u_all, ref.u) <= 1e-13
+    else:
+        # saved fields come from the float32 evaluation, work rates from float64
+        # arithmetic on the compensated state: both follow the state's error
+        assert _rel(sols.u_all[:, 12:16], ref.u[:, 12:16], [(0, 4)]) <= 1e-3
+    gprob, dt, ssi = _small_grid_workload(tp, n=256, nt=1000, ssi=250)
+    sols, ref = _both(tp, orc, gprob, tp.Boris(), dt=dt, savestepinterval=ssi, save_work=True)
+    _check_same_layout(sols, ref)
+    assert _rel(sols.u_all, ref.u, _WORK10) <= 1e-13
 
 
 def test_argument_errors_gpu(tp):
@@ -356,6 +435,21 @@ def test_gc_fp64_matches_oracle(tp, orc, alg):
         # the step controller's pow() (CUDA vs glibc) may differ in the last bit
         assert _rel(sols.t_all, ref.t) <= 1e-10
         assert _rel(sols.u_all, ref.u) <= 1e-10
+
+
+@pytest.mark.parametrize("alg", ["rk4", "rk45"])
+def test_gc_save_fields_and_work(tp, orc, alg):
+    # test_gc.jl:268-304 shape, plus parity of every saved column
+    prob = _gc_dipole(tp, orc)
+    kw = dict(dt=1.0e-4, alg=alg, save_fields=True, save_work=True, maxiters=2000)
+    sols = tp.solve(prob, **kw)
+    plan = tp.plan_gc(prob, **kw)
+    ref = orc.gc_run(plan.desc, plan.E, plan.B, plan.y0)
+    _check_same_layout(sols, ref)
+    assert sols.u_all.shape[1] == 14
+    assert np.linalg.norm(sols.u_all[0, 7:10]) > 0.0 and np.all(sols.u_all[:, 4:7] == 0.0)
+    assert np.all(sols.u_all[:, 10:14] == 0.0)   # E = 0 and static B
+    assert _rel(sols.u_all, ref.u) <= (1e-13 if alg == "rk4" else 1e-10)
 
 
 def test_gc_config4_subset(tp, orc):

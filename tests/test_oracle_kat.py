@@ -174,6 +174,81 @@ def test_saving_flags_multistep_and_fields(tp, orc):
     assert list(u[-1, 6:9]) == [0.0, 0.0, 0.0] and list(u[-1, 9:12]) == [0.0, 0.0, 0.01]
 
 
+def _work_fields(tp, rate=0.0):
+    """constant_E / gradient_B / time_varying_B_linear of test_boris.jl:24-28,419-421."""
+    E = tp.UniformField((0.0, 1.0e5, 0.0))
+    Bgrad = tp.AffineField((0.0, 0.0, 0.01), ((0, 0, 0), (0, 0, 0), (0.01, 0, 0)))
+    Bbeta = tp.AffineField((0.0, 0.0, 0.01), rate=(0.0, 0.0, 0.01 * 1.0e7))
+    return E, Bgrad, Bbeta
+
+
+def test_save_work_kats(tp, orc):
+    # test_boris.jl:374-466
+    E, Bgrad, Bbeta = _work_fields(tp)
+    u0 = [0.0, 0.0, 0.0, 1.0e5, 0.0, 0.0]
+    tspan, dt = (0.0, 1.0e-9), 1.0e-11
+    param = tp.prepare(E, Bgrad, species=tp.Electron)
+    r = _solve(tp, orc, u0, tspan, param, tp.Boris(), dt=dt, savestepinterval=1, save_work=True,
+               save_everystep=True)
+    _, u = r.traj(0)
+    assert u.shape[1] == 10
+    work = u[0, 6:10]
+    assert abs(work[0]) <= 1e-10 and abs(work[1]) <= 1e-10 and abs(work[3]) <= 1e-10
+    assert abs(work[2]) > 0.0
+    # P_grad = mu/|B| (b x grad|B|) . E with mu = m vperp^2 / 2|B| at the start
+    mu = tp.Electron.m * 1.0e10 / (2 * 0.01)
+    assert math.isclose(work[2], mu / 0.01 * 0.01 * 1.0e5, rel_tol=1e-12)
+
+    # betatron: B_z = 0.01 (1 + 1e7 t), E = 0
+    rb = _solve(tp, orc, u0, tspan, tp.prepare(tp.ZeroField(), Bbeta, species=tp.Electron), tp.Boris(), dt=dt,
+                savestepinterval=1, save_work=True)
+    assert rb.traj(0)[1][0, 9] > 0.0
+    # the same field as a Julia-style closure: dB/dt by the oracle's central difference
+    rc = _solve(tp, orc, u0, tspan, tp.prepare(tp.ZeroField(), Bbeta, species=tp.Electron), tp.Boris(),
+                B=lambda x, t: np.array([0.0, 0.0, 0.01 * (1.0 + 1.0e7 * t)]), dt=dt, savestepinterval=1,
+                save_work=True)
+    assert np.allclose(rc.traj(0)[1][:, 9], rb.traj(0)[1][:, 9], rtol=1e-6)
+
+    # both flags: width 16, work after the fields and identical to the work-only run
+    r2 = _solve(tp, orc, u0, tspan, param, tp.Boris(), dt=dt, savestepinterval=1, save_fields=True,
+                save_work=True)
+    _, u2 = r2.traj(0)
+    assert u2.shape[1] == 16
+    assert np.array_equal(u2[0, 12:16], u[0, 6:10])
+    assert np.array_equal(u2[:, 12:16], u[:, 6:10])
+    assert np.array_equal(u2[:, 6:9], np.tile([0.0, 1.0e5, 0.0], (u2.shape[0], 1)))
+
+    # MultistepBoris{2}(n = 2)
+    rm = _solve(tp, orc, u0, tspan, param, tp.MultistepBoris(2, 2), dt=dt, savestepinterval=1, save_work=True)
+    _, um = rm.traj(0)
+    assert um.shape[1] == 10 and abs(um[0, 6]) <= 1e-10 and abs(um[0, 8]) > 0.0
+
+    # AdaptiveBoris(safety = 0.1)
+    ra = _solve(tp, orc, u0, tspan, param, tp.AdaptiveBoris(0.1), save_work=True, save_everystep=True)
+    _, ua = ra.traj(0)
+    assert ua.shape[1] == 10 and abs(ua[0, 6]) <= 1e-10 and abs(ua[0, 8]) > 0.0
+
+
+def test_gc_save_fields_and_work_kat(tp, orc):
+    # test_gc.jl:268-304: fields and work saved by the guiding-centre solver
+    B = tp.DipoleField(tp.BMoment_Earth)
+    r0 = [1.5 * tp.Re, 0.0, 0.0]
+    v0 = [0.0, 1.0e5, 1.0e5]
+    q, m = tp.Proton.q, tp.Proton.m
+    y, mu = orc.gc_prepare(tp.ZeroField(), B, np.array([r0 + v0]), q, m)
+    y0, param = y[0], (q, q / m, float(mu[0]), tp.ZeroField(), B)
+    prob = tp.TraceGCProblem(y0, (0.0, 1.0e-4), param)
+    plan = tp.plan_gc(prob, tp.EnsembleB200(), trajectories=2, dt=1.0e-5, save_fields=True, save_work=True)
+    r = orc.gc_run(plan.desc, plan.E, plan.B, plan.y0)
+    for i in range(2):
+        t, u = r.traj(i)
+        assert u.shape == (t.size, 14)
+        assert np.linalg.norm(u[0, 7:10]) > 0.0
+        assert np.linalg.norm(u[0, 4:7]) == 0.0
+        # E = 0: every electric work term vanishes; static B: no betatron term
+        assert np.all(u[:, 10:14] == 0.0)
+
+
 def test_solver_limits(tp, orc):
     # test_boris.jl:509-532
     E = tp.UniformField((0.0, 1.0e5, 0.0))

@@ -34,7 +34,7 @@ def _problem(tp, kind):
 def _pack_without_alloc(tp, torch, ctx, plan):
     n = plan.u0.shape[0]
     nslots = ctx.slots(plan.desc, n, plan.dt_i, plan.tend_i)
-    W = 12 if plan.desc.save_fields else 6
+    W = 6 + 6 * bool(plan.desc.save_fields) + 4 * bool(plan.desc.save_work)
     dev = torch.device("cuda", 0)
     u0 = torch.from_numpy(plan.u0).to(dev)
     dti = None if plan.dt_i is None else torch.from_numpy(plan.dt_i).to(dev)
