@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define TP_ABI_VERSION 2
+#define TP_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -71,9 +71,12 @@ enum {
  *            linearly time-varying fields of the reference tests)
  *   DIPOLE   F(x) = coef * (3 (m.rhat) rhat - m) / |x - center|^3
  *            (the Magnetostatics.Dipole field of test/test_gc.jl:180)
- *   GRID     trilinear interpolation of a (3, nx, ny, nz) column-major array
- *            on a uniform Cartesian grid: build_interpolator(CartesianGrid,
- *            A, x, y, z, 1, bc) (src/utility/interpolation.jl:217-235)     */
+ *   GRID     interpolation of a (3, nx, ny, nz) column-major array:
+ *            build_interpolator(gridtype, A, grids..., order, bc)
+ *            (src/utility/interpolation.jl:119-311).  The default (a zeroed
+ *            descriptor tail) is trilinear on a uniform Cartesian grid; the
+ *            tail fields below select the order (0 / 1 / 3), rectilinear
+ *            axes, spherical geometry and 1-D / 2-D interpolants.          */
 enum {
     TP_FIELD_ZERO = 0,
     TP_FIELD_UNIFORM = 1,
@@ -83,11 +86,41 @@ enum {
 };
 
 /* grid boundary handling (FastInterpolations FillExtrap(NaN), ClampExtrap(),
- * PeriodicBC(endpoint=:exclusive) / WrapExtrap() with period L = n * dx)   */
+ * PeriodicBC(endpoint=:exclusive) / WrapExtrap() with period L = n * dx,
+ * PeriodicBC(endpoint=:inclusive) with period L = (n - 1) * dx: the last
+ * node repeats the first)                                                   */
 enum {
     TP_BC_FILL_NAN = 0,
     TP_BC_CLAMP = 1,
-    TP_BC_PERIODIC = 2
+    TP_BC_PERIODIC = 2,
+    TP_BC_PERIODIC_INCLUSIVE = 3
+};
+
+/* interpolation order of a grid (build_interpolator's `order`):
+ *   LINEAR    order 1, linear_interp (the default)
+ *   CONSTANT  order 0, constant_interp: the nearest node
+ *   CUBIC     order 3, cardinal_interp: local cubic Hermite (Catmull-Rom)
+ *             on uniform axes                                              */
+enum {
+    TP_ORDER_LINEAR = 0,
+    TP_ORDER_CONSTANT = 1,
+    TP_ORDER_CUBIC = 2
+};
+
+/* grid geometry:
+ *   CARTESIAN  axes x, y, z (CartesianGrid, or RectilinearGrid when node
+ *              coordinates are given per axis)
+ *   SPHERICAL  axes r, theta, phi (StructuredGrid,
+ *              SphericalFieldInterpolator, interpolation.jl:97-117,260-284):
+ *              the point is converted with cart2sph, r and theta fill NaN
+ *              outside the grid, phi is periodic (inclusive), and the
+ *              interpolated (v_r, v_theta, v_phi) is returned in Cartesian
+ *              components (sph2cartvec, src/utility/utility.jl:82-89)      */
+enum {
+    TP_GRID_CARTESIAN = 0,
+    TP_GRID_SPHERICAL = 1,
+    TP_GRID_SPHERICAL_SCALAR = 2 /* spherical grid of a scalar carried in
+                                    component 0: no basis conversion      */
 };
 
 enum { TP_DTYPE_F32 = 0, TP_DTYPE_F64 = 1 };
@@ -109,6 +142,17 @@ typedef struct tp_field_desc {
     const void* data;    /* GRID: host pointer, 3*nx*ny*nz values, (3,nx,ny,nz)
                             column-major: component c of node (i,j,k) is at
                             c + 3*(i + nx*(j + ny*k))                       */
+    /* GRID tail (all zero: trilinear, uniform Cartesian, 3-D)              */
+    int32_t order;       /* TP_ORDER_*                                      */
+    int32_t geometry;    /* TP_GRID_*                                       */
+    int32_t ndim;        /* CARTESIAN: 1, 2 or 3 (0 = 3): FieldInterpolator1D
+                            / 2D / 3D; unused axes have n = 1               */
+    int32_t dir;         /* ndim 1: the coordinate (0, 1, 2) it reads       */
+    const double* axis[3]; /* per-axis node coordinates (n[a] strictly
+                            increasing values, host memory), or NULL for the
+                            uniform axis origin + k * spacing.  Non-uniform
+                            axes take LINEAR or CONSTANT order and FILL_NAN
+                            or CLAMP boundaries.                            */
 } tp_field_desc;
 
 /* ---- termination (the reference's `isoutside(u, p, t)` callback) --------
@@ -218,6 +262,30 @@ void tp_field_destroy(tp_field* field);
  * addition for optimisation loops over gridded fields (the reference rebuilds
  * the interpolator).                                                        */
 int tp_field_update(tp_field* field, const void* data);
+
+/* ---- fields and work rates at given states ------------------------------
+ * get_fields / get_work (src/boris/boris.jl:599-640): E, B and the work rates
+ * of get_work_rates (src/equations.jl:394-441) or get_work_rates_gc
+ * (:445-480) at n states, evaluated on the device.                          */
+enum {
+    TP_POINTS_FULL_ORBIT = 0, /* states (x, v): 6 values                   */
+    TP_POINTS_GC = 1          /* states (X, v_par): 4 values                */
+};
+typedef struct tp_points_desc {
+    int32_t kind;        /* TP_POINTS_*                                     */
+    int32_t want;        /* bit 0: E and B (6 values); bit 1: the four work
+                            rates (P_par, P_fermi, P_grad, P_betatron)     */
+    int32_t stride;      /* doubles per state in `u` (>= 6 or >= 4)         */
+    int32_t reserved;
+    double q2m, m;       /* FULL_ORBIT: charge-to-mass ratio and mass;
+                            GC: q2m                                         */
+    double q, mu;        /* GC: charge and magnetic moment                  */
+} tp_points_desc;
+/* u: n states of `stride` doubles; t: n times; out: n rows of
+ * 6 * (want & 1) + 4 * ((want >> 1) & 1) doubles.  Host or device memory. */
+int tp_eval_points(tp_ctx* ctx, const tp_points_desc* desc, const tp_field* E,
+                   const tp_field* B, const double* u, const double* t, int64_t n,
+                   double* out);
 
 /* ---- full-orbit solve (host buffers) --------------------------------------
  * Replaces _solve(::EnsembleAlg, ::TraceProblem, ::AbstractBoris, ...)

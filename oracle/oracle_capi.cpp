@@ -38,6 +38,35 @@ typedef struct orc_term_cb {
 
 namespace {
 
+template <class D>
+std::unique_ptr<Field> make_general(const tp_field_desc* d) {
+    auto* f = new GeneralGridField<D>();
+    f->order = d->order;
+    f->geom = d->geometry;
+    const bool sph = d->geometry == TP_GRID_SPHERICAL || d->geometry == TP_GRID_SPHERICAL_SCALAR;
+    f->ndim = sph ? 3 : (d->ndim == 0 ? 3 : d->ndim);
+    f->dir = d->dir;
+    for (int a = 0; a < 3; ++a) {
+        f->n[a] = d->n[a];
+        f->abc[a] = d->bc;
+        if (d->axis[a]) {
+            f->coords[a].assign(d->axis[a], d->axis[a] + d->n[a]);
+            f->x0[a] = d->axis[a][0];
+            f->inv_dx[a] = 1.0;
+        } else {
+            f->x0[a] = d->origin[a];
+            f->inv_dx[a] = d->n[a] == 1 ? 1.0 : 1.0 / d->spacing[a];
+        }
+    }
+    if (sph) {
+        f->abc[0] = TP_BC_FILL_NAN;
+        f->abc[1] = TP_BC_FILL_NAN;
+        f->abc[2] = TP_BC_PERIODIC_INCLUSIVE;
+    }
+    f->data = (const D*)d->data;
+    return std::unique_ptr<Field>(f);
+}
+
 std::unique_ptr<Field> make_field(const tp_field_desc* d, const orc_field_cb* cb) {
     if (cb && cb->f) {
         auto* f = new CallbackField();
@@ -65,6 +94,13 @@ std::unique_ptr<Field> make_field(const tp_field_desc* d, const orc_field_cb* cb
             return std::unique_ptr<Field>(f);
         }
         case TP_FIELD_GRID: {
+            const int ndim = d->ndim == 0 ? 3 : d->ndim;
+            const bool general = d->order != TP_ORDER_LINEAR || d->geometry != TP_GRID_CARTESIAN || ndim != 3 ||
+                                 d->bc == TP_BC_PERIODIC_INCLUSIVE || d->axis[0] || d->axis[1] || d->axis[2];
+            if (general) {
+                if (d->dtype == TP_DTYPE_F32) return make_general<float>(d);
+                return make_general<double>(d);
+            }
             if (d->dtype == TP_DTYPE_F32) {
                 auto* f = new GridField<float>();
                 for (int a = 0; a < 3; ++a) {

@@ -267,6 +267,315 @@ struct GridField : Field {
     }
 };
 
+// Gridded fields beyond trilinear-uniform-Cartesian: build_interpolator with
+// order 0 / 1 / 3, RectilinearGrid axes, StructuredGrid (spherical) and the
+// 1-D / 2-D interpolants (src/utility/interpolation.jl:15-311) over
+// FastInterpolations.jl v0.4 (constant_interp, linear_interp,
+// cardinal_interp; a dependency absent here, restated from its documented
+// behaviour and pinned on the reference's interpolation tests).
+//   order 0   nearest node: floor(u + 1/2) on uniform axes, the closer node
+//             on non-uniform ones (ties to the upper node)
+//   order 1   cell i = min(floor(u), n - 2), f = u - i (non-uniform:
+//             f = (x - c_i) / (c_{i+1} - c_i)); lerp a + f (b - a)
+//   order 3   cardinal cubic (Catmull-Rom) Hermite on the same cell with
+//             slopes (f_{i+1} - f_{i-1}) / 2; at the ends of a non-periodic
+//             axis the three-point one-sided slope (-3 f0 + 4 f1 - f2) / 2,
+//             mirrored at the top; two-node axes use the secant at both ends
+//   periodic  exclusive: period n nodes; inclusive: period n - 1 nodes
+//   spherical cart2sph (r = sqrt(x^2 + y^2 + z^2); theta = acos(z / r);
+//             phi = atan(y, x) mapped to [0, 2pi)), r and theta fill NaN, phi
+//             periodic inclusive; the (v_r, v_theta, v_phi) result goes
+//             through sph2cartvec (src/utility/utility.jl:63-89); a scalar
+//             grid (component 0) is returned as interpolated
+// Templated on the scalar: double, or Dl3 (value and d/dx, d/dy, d/dz) for
+// the Jacobian ForwardDiff would take.
+struct Dl3 {
+    double v, d[3];
+};
+inline double sval(double a) { return a; }
+inline double sval(const Dl3& a) { return a.v; }
+template <class S> inline S scst(double c);
+template <> inline double scst<double>(double c) { return c; }
+template <> inline Dl3 scst<Dl3>(double c) { return {c, {0.0, 0.0, 0.0}}; }
+inline Dl3 operator+(const Dl3& a, const Dl3& b) { return {a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}}; }
+inline Dl3 operator-(const Dl3& a, const Dl3& b) { return {a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2]}}; }
+inline Dl3 operator*(const Dl3& a, const Dl3& b) {
+    Dl3 o{a.v * b.v, {0, 0, 0}};
+    for (int k = 0; k < 3; ++k) o.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return o;
+}
+inline Dl3 operator/(const Dl3& a, const Dl3& b) {
+    Dl3 o{a.v / b.v, {0, 0, 0}};
+    for (int k = 0; k < 3; ++k) o.d[k] = (a.d[k] - o.v * b.d[k]) / b.v;
+    return o;
+}
+inline Dl3 operator+(const Dl3& a, double c) { return {a.v + c, {a.d[0], a.d[1], a.d[2]}}; }
+inline Dl3 operator+(double c, const Dl3& a) { return {c + a.v, {a.d[0], a.d[1], a.d[2]}}; }
+inline Dl3 operator-(const Dl3& a, double c) { return {a.v - c, {a.d[0], a.d[1], a.d[2]}}; }
+inline Dl3 operator-(double c, const Dl3& a) { return {c - a.v, {-a.d[0], -a.d[1], -a.d[2]}}; }
+inline Dl3 operator*(const Dl3& a, double c) { return {a.v * c, {a.d[0] * c, a.d[1] * c, a.d[2] * c}}; }
+inline Dl3 operator*(double c, const Dl3& a) { return {c * a.v, {c * a.d[0], c * a.d[1], c * a.d[2]}}; }
+inline Dl3 operator/(const Dl3& a, double c) { return {a.v / c, {a.d[0] / c, a.d[1] / c, a.d[2] / c}}; }
+inline double ssqrt(double a) { return std::sqrt(a); }
+inline Dl3 ssqrt(const Dl3& a) {
+    double r = std::sqrt(a.v), k = 0.5 / r;
+    return {r, {a.d[0] * k, a.d[1] * k, a.d[2] * k}};
+}
+inline double sacos(double a) { return std::acos(a); }
+inline Dl3 sacos(const Dl3& a) {
+    double k = -1.0 / std::sqrt(1.0 - a.v * a.v);
+    return {std::acos(a.v), {a.d[0] * k, a.d[1] * k, a.d[2] * k}};
+}
+inline double satan2(double y, double x) { return std::atan2(y, x); }
+inline Dl3 satan2(const Dl3& y, const Dl3& x) {
+    double den = x.v * x.v + y.v * y.v;
+    Dl3 o{std::atan2(y.v, x.v), {0, 0, 0}};
+    for (int k = 0; k < 3; ++k) o.d[k] = (x.v * y.d[k] - y.v * x.d[k]) / den;
+    return o;
+}
+inline void ssincos(double a, double& s, double& c) {
+    s = std::sin(a);
+    c = std::cos(a);
+}
+inline void ssincos(const Dl3& a, Dl3& s, Dl3& c) {
+    double sv = std::sin(a.v), cv = std::cos(a.v);
+    s = {sv, {a.d[0] * cv, a.d[1] * cv, a.d[2] * cv}};
+    c = {cv, {-(a.d[0] * sv), -(a.d[1] * sv), -(a.d[2] * sv)}};
+}
+
+template <class D>
+struct GeneralGridField : Field {
+    int64_t n[3];
+    double x0[3], inv_dx[3];
+    std::vector<double> coords[3];  // non-uniform axes (empty: uniform)
+    int abc[3];                     // per-axis boundary
+    int order, geom, ndim, dir;
+    const D* data;                  // (3, n0, n1, n2)
+
+    template <class S>
+    struct Axis {
+        int64_t i[4];
+        S w[4];
+        int k;
+    };
+    static int64_t wrap(int64_t i, int64_t m) {
+        int64_t r = i % m;
+        return r < 0 ? r + m : r;
+    }
+
+    template <class S>
+    static void cubic(const S& t, int64_t i, int64_t na, bool periodic, int64_t m, Axis<S>& o) {
+        S t2 = t * t;
+        S t3 = t2 * t;
+        S h00 = (2.0 * t3 - 3.0 * t2) + 1.0;
+        S h10 = (t3 - 2.0 * t2) + t;
+        S h01 = 3.0 * t2 - 2.0 * t3;
+        S h11 = t3 - t2;
+        if (periodic || (i > 0 && i < na - 2)) {
+            o.k = 4;
+            for (int q = 0; q < 4; ++q) o.i[q] = periodic ? wrap(i - 1 + q, m) : i - 1 + q;
+            o.w[0] = -0.5 * h10;
+            o.w[1] = h00 - 0.5 * h11;
+            o.w[2] = h01 + 0.5 * h10;
+            o.w[3] = 0.5 * h11;
+        } else if (na == 2) {
+            o.k = 2;
+            o.i[0] = 0;
+            o.i[1] = 1;
+            o.w[0] = (h00 - h10) - h11;
+            o.w[1] = (h01 + h10) + h11;
+        } else if (i == 0) {
+            o.k = 3;
+            for (int q = 0; q < 3; ++q) o.i[q] = q;
+            o.w[0] = (h00 - 1.5 * h10) - 0.5 * h11;
+            o.w[1] = h01 + 2.0 * h10;
+            o.w[2] = 0.5 * h11 - 0.5 * h10;
+        } else {  // i == na - 2
+            o.k = 3;
+            for (int q = 0; q < 3; ++q) o.i[q] = na - 3 + q;
+            o.w[0] = 0.5 * h11 - 0.5 * h10;
+            o.w[1] = h00 - 2.0 * h11;
+            o.w[2] = (h01 + 0.5 * h10) + 1.5 * h11;
+        }
+    }
+
+    template <class S>
+    bool axis(int a, S x, Axis<S>& o) const {
+        const int64_t na = n[a];
+        if (na == 1) {
+            o.k = 1;
+            o.i[0] = 0;
+            return true;
+        }
+        const int bc = abc[a];
+        if (!coords[a].empty()) {
+            const std::vector<double>& c = coords[a];
+            double xv = sval(x);
+            if (bc == TP_BC_CLAMP) {
+                if (xv < c.front()) x = scst<S>(c.front());
+                else if (xv > c.back()) x = scst<S>(c.back());
+                xv = sval(x);
+            } else if (!(xv >= c.front() && xv <= c.back())) {
+                return false;
+            }
+            // the last node with c_i <= x, at most n - 2
+            int64_t il = std::upper_bound(c.begin(), c.end(), xv) - c.begin() - 1;
+            il = std::max<int64_t>(0, std::min<int64_t>(il, na - 2));
+            if (order == TP_ORDER_CONSTANT) {
+                o.k = 1;
+                o.i[0] = (xv - c[il] < c[il + 1] - xv) ? il : il + 1;
+                return true;
+            }
+            o.k = 2;
+            o.i[0] = il;
+            o.i[1] = il + 1;
+            o.w[0] = (x - c[il]) / (c[il + 1] - c[il]);
+            return true;
+        }
+        S u = (x - x0[a]) * inv_dx[a];
+        const bool periodic = bc == TP_BC_PERIODIC || bc == TP_BC_PERIODIC_INCLUSIVE;
+        const int64_t m = bc == TP_BC_PERIODIC ? na : na - 1;
+        const double umax = (double)(na - 1);
+        if (order == TP_ORDER_CONSTANT) {
+            double uv = sval(u);
+            int64_t i;
+            if (periodic) {
+                i = wrap((int64_t)std::floor(uv + 0.5), m);
+            } else {
+                if (bc == TP_BC_CLAMP) uv = std::min(std::max(uv, 0.0), umax);
+                else if (!(uv >= 0.0 && uv <= umax)) return false;
+                i = (int64_t)std::floor(uv + 0.5);
+            }
+            o.k = 1;
+            o.i[0] = i;
+            return true;
+        }
+        int64_t i;
+        S f;
+        if (periodic) {
+            double fl = std::floor(sval(u));
+            f = u - fl;
+            i = wrap((int64_t)fl, m);
+        } else {
+            double uv = sval(u);
+            if (bc == TP_BC_CLAMP) {
+                if (uv < 0.0) u = scst<S>(0.0);
+                else if (uv > umax) u = scst<S>(umax);
+            } else if (!(uv >= 0.0 && uv <= umax)) {
+                return false;
+            }
+            i = std::min<int64_t>((int64_t)std::floor(sval(u)), na - 2);
+            f = u - (double)i;
+        }
+        if (order == TP_ORDER_CUBIC) {
+            cubic(f, i, na, periodic, m, o);
+            return true;
+        }
+        o.k = 2;
+        o.i[0] = i;
+        o.i[1] = (bc == TP_BC_PERIODIC && i + 1 == na) ? 0 : i + 1;
+        o.w[0] = f;
+        return true;
+    }
+
+    template <class S, class V>
+    S combine(const Axis<S>& a, const V* v) const {
+        if (a.k == 1) return scst<S>(0.0) + v[0];
+        if (order == TP_ORDER_LINEAR) return v[0] + a.w[0] * (v[1] - v[0]);
+        S acc = a.w[0] * v[0] + a.w[1] * v[1];
+        for (int q = 2; q < a.k; ++q) acc = acc + a.w[q] * v[q];
+        return acc;
+    }
+
+    double node(int c, int64_t i, int64_t j, int64_t k) const {
+        return (double)data[c + 3 * (i + n[0] * (j + n[1] * k))];
+    }
+
+    template <class S>
+    bool interp(const S q[3], S out[3]) const {
+        Axis<S> A[3];
+        bool ok = axis(0, q[0], A[0]);
+        ok = axis(1, q[1], A[1]) && ok;
+        ok = axis(2, q[2], A[2]) && ok;
+        if (!ok) return false;
+        for (int c = 0; c < 3; ++c) {
+            S cz[4] = {};
+            for (int kz = 0; kz < A[2].k; ++kz) {
+                S cy[4] = {};
+                for (int ky = 0; ky < A[1].k; ++ky) {
+                    double vx[4] = {0.0, 0.0, 0.0, 0.0};
+                    for (int kx = 0; kx < A[0].k; ++kx) vx[kx] = node(c, A[0].i[kx], A[1].i[ky], A[2].i[kz]);
+                    cy[ky] = combine<S, double>(A[0], vx);
+                }
+                cz[kz] = combine<S, S>(A[1], cy);
+            }
+            out[c] = combine<S, S>(A[2], cz);
+        }
+        return true;
+    }
+
+    template <class S>
+    bool evaluate(const S r[3], S out[3]) const {
+        if (geom == TP_GRID_SPHERICAL || geom == TP_GRID_SPHERICAL_SCALAR) {
+            S rr = ssqrt((r[0] * r[0] + r[1] * r[1]) + r[2] * r[2]);
+            S q[3];
+            if (sval(rr) == 0.0) {
+                q[0] = q[1] = q[2] = scst<S>(0.0);
+            } else {
+                q[0] = rr;
+                q[1] = sacos(r[2] / rr);
+                S ph = satan2(r[1], r[0]);
+                if (sval(ph) < 0.0) ph = ph + 6.283185307179586;
+                q[2] = ph;
+            }
+            S v[3];
+            if (!interp(q, v)) return false;
+            if (geom == TP_GRID_SPHERICAL_SCALAR) {  // a scalar: no basis conversion
+                for (int c = 0; c < 3; ++c) out[c] = v[c];
+                return true;
+            }
+            S st, ct, sp, cp;
+            ssincos(q[1], st, ct);
+            ssincos(q[2], sp, cp);
+            out[0] = ((st * cp) * v[0] + (ct * cp) * v[1]) - sp * v[2];
+            out[1] = ((st * sp) * v[0] + (ct * sp) * v[1]) + cp * v[2];
+            out[2] = ct * v[0] - st * v[1];
+            return true;
+        }
+        S q[3];
+        if (ndim == 1) {
+            q[0] = r[dir];
+            q[1] = q[2] = scst<S>(0.0);
+        } else {
+            q[0] = r[0];
+            q[1] = r[1];
+            q[2] = r[2];
+        }
+        return interp(q, out);
+    }
+
+    V3d eval(V3d r, double) const override {
+        double p[3] = {r.x, r.y, r.z}, o[3];
+        if (!evaluate<double>(p, o)) {
+            double nan = std::numeric_limits<double>::quiet_NaN();
+            return {nan, nan, nan};
+        }
+        return {o[0], o[1], o[2]};
+    }
+    void jac(V3d r, double, V3d& F, M3& J) const override {
+        Dl3 p[3] = {{r.x, {1, 0, 0}}, {r.y, {0, 1, 0}}, {r.z, {0, 0, 1}}}, o[3];
+        if (!evaluate<Dl3>(p, o)) {
+            double nan = std::numeric_limits<double>::quiet_NaN();
+            F = {nan, nan, nan};
+            for (double& a : J.a) a = nan;
+            return;
+        }
+        F = {o[0].v, o[1].v, o[2].v};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) J.a[3 * i + j] = o[i].d[j];
+    }
+};
+
 // A field given by C callbacks (the tests' Julia closures restated in Python).
 typedef void (*field_cb)(const double* x, double t, double* out, void* user);
 typedef void (*jac_cb)(const double* x, double t, double* out9, void* user);

@@ -12,7 +12,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libtpb200.so"
 
-TP_ABI_VERSION = 2
+TP_ABI_VERSION = 3
 
 TP_OK = 0
 TP_E_ARG = -1
@@ -36,6 +36,18 @@ TP_FIELD_GRID = 4
 TP_BC_FILL_NAN = 0
 TP_BC_CLAMP = 1
 TP_BC_PERIODIC = 2
+TP_BC_PERIODIC_INCLUSIVE = 3
+
+TP_ORDER_LINEAR = 0
+TP_ORDER_CONSTANT = 1
+TP_ORDER_CUBIC = 2
+
+TP_GRID_CARTESIAN = 0
+TP_GRID_SPHERICAL = 1
+TP_GRID_SPHERICAL_SCALAR = 2
+
+TP_POINTS_FULL_ORBIT = 0
+TP_POINTS_GC = 1
 
 TP_DTYPE_F32 = 0
 TP_DTYPE_F64 = 1
@@ -83,6 +95,11 @@ class FieldDesc(C.Structure):
         ("origin", _D3),
         ("spacing", _D3),
         ("data", C.c_void_p),
+        ("order", C.c_int32),
+        ("geometry", C.c_int32),
+        ("ndim", C.c_int32),
+        ("dir", C.c_int32),
+        ("axis", C.c_void_p * 3),
     ]
 
 
@@ -166,6 +183,19 @@ class TuneResult(C.Structure):
     ]
 
 
+class PointsDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("want", C.c_int32),
+        ("stride", C.c_int32),
+        ("reserved", C.c_int32),
+        ("q2m", C.c_double),
+        ("m", C.c_double),
+        ("q", C.c_double),
+        ("mu", C.c_double),
+    ]
+
+
 class AdjDesc(C.Structure):
     _fields_ = [
         ("run", RunDesc),
@@ -197,6 +227,7 @@ SIGNATURES = [
     ("tp_pack_results_device_noalloc", C.c_int,
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     ("tp_field_update", C.c_int, [_P, _P]),
+    ("tp_eval_points", C.c_int, [_P, C.POINTER(PointsDesc), _P, _P, _P, _P, C.c_int64, _P]),
     ("tp_autotune", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(TuneResult)]),
     ("tp_boris_graph_create", C.c_int,
      [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),

@@ -76,7 +76,7 @@ struct Saver32 {
         }
         if (a.save_work) {
             double w[4];
-            work_rates64<FK != FK_ANALYTIC>(a.f, D3{x[0], x[1], x[2]}, D3{x[3], x[4], x[5]}, t, a.q2m, a.m, w);
+            work_rates64<GMOf<FK>::value>(a.f, D3{x[0], x[1], x[2]}, D3{x[3], x[4], x[5]}, t, a.q2m, a.m, w);
             const int c0 = a.save_fields ? 12 : 6;
             for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
@@ -355,6 +355,7 @@ template <bool MULTI, bool QUEUE>
 static const void* pick_fk32(bool adaptive, int fk) {
     if (fk == FK_ANALYTIC) return kernel_ptr32<MULTI, QUEUE, FK_ANALYTIC>(adaptive);
     if (fk == FK_EBGRID) return kernel_ptr32<MULTI, QUEUE, FK_EBGRID>(adaptive);
+    if (fk == FK_GENGRID) return kernel_ptr32<MULTI, QUEUE, FK_GENGRID>(adaptive);
     return kernel_ptr32<MULTI, QUEUE, FK_GENERIC>(adaptive);
 }
 

@@ -6,6 +6,7 @@
 // +, -, *, /, sqrt and fma are involved.
 #pragma once
 
+#include "grid_general.cuh"
 #include "tp_device.cuh"
 
 namespace tpb {
@@ -119,7 +120,30 @@ __device__ __forceinline__ bool grid_axes64(const DevField& g, D3 r, Ax& ax, Ax&
     return ok;
 }
 
+// grids off the fast path (grid_general.cuh): value, and value with Jacobian
+static __device__ __noinline__ D3 grid_general64(const DevField& g, D3 r) {
+    double p[3] = {r.x, r.y, r.z}, o[3];
+    if (!grid_general_eval<double>(g, p, o)) return nan3();
+    return {o[0], o[1], o[2]};
+}
+
+static __device__ __noinline__ void grid_general_jac64(const DevField& g, D3 r, D3& F, double J[9]) {
+    Dual3 p[3] = {{r.x, {1.0, 0.0, 0.0}}, {r.y, {0.0, 1.0, 0.0}}, {r.z, {0.0, 0.0, 1.0}}}, o[3];
+    if (!grid_general_eval<Dual3>(g, p, o)) {
+        F = nan3();
+        for (int k = 0; k < 9; ++k) J[k] = F.x;
+        return;
+    }
+    F = {o[0].v, o[1].v, o[2].v};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) J[3 * i + j] = o[i].d[j];
+}
+
+// GEN = false: the caller guarantees no general grid reaches it (kernels
+// specialised for trilinear grids keep the general code out of their body)
+template <bool GEN = true>
 __device__ __forceinline__ D3 grid_eval64(const DevField& g, D3 r) {
+    if (GEN && g.general) return grid_general64(g, r);
     Ax ax, ay, az;
     if (!grid_axes64(g, r, ax, ay, az)) return nan3();
     return tri64(g, g.tab, g.f64 != 0, 1, 0, ax, ay, az);
@@ -152,8 +176,9 @@ __device__ __forceinline__ D3 analytic_eval64(const DevField& f, D3 r, double t)
     }
 }
 
+template <bool GEN = true>
 __device__ __forceinline__ D3 field_eval64(const DevField& f, D3 r, double t) {
-    if (f.kind == TP_FIELD_GRID) return grid_eval64(f, r);
+    if (f.kind == TP_FIELD_GRID) return grid_eval64<GEN>(f, r);
     return analytic_eval64(f, r, t);
 }
 
@@ -233,8 +258,8 @@ __device__ __forceinline__ void eval_EB64t(const DevFields& F, D3 r, double t, D
     } else if (FK == FK_EBGRID) {
         eb_eval64_f32(F, r, E, B);
     } else {
-        E = field_eval64(F.E, r, t);
-        B = field_eval64(F.B, r, t);
+        E = field_eval64<FK == FK_GENGRID>(F.E, r, t);
+        B = field_eval64<FK == FK_GENGRID>(F.B, r, t);
     }
 }
 
@@ -342,8 +367,20 @@ __device__ __forceinline__ bool outside64(const DevTerm& T, D3 r, D3 v, double t
 // B and its Jacobian (row-major J[i][j] = dB_i/dx_j), float64, in the order
 // of the CPU restatement (the role of ForwardDiff in _get_B_jacobian,
 // src/utility/utility.jl:386-392)
-template <bool GRID>
+// Field configurations of the float64 Jacobian and value helpers: GM_ANALYTIC
+// (no grids), GM_GRID (trilinear uniform Cartesian grids only), GM_ANY (also
+// the general grids of grid_general.cuh).
+enum { GM_ANALYTIC = 0, GM_GRID = 1, GM_ANY = 2 };
+
+// the grid mode of a full-orbit kernel's field configuration
+template <int FK>
+struct GMOf {
+    static constexpr int value = FK == FK_ANALYTIC ? GM_ANALYTIC : (FK == FK_GENGRID ? GM_ANY : GM_GRID);
+};
+
+template <int GM>
 __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
+    constexpr bool GRID = GM != GM_ANALYTIC;
     for (int k = 0; k < 9; ++k) J[k] = 0.0;
     switch (f.kind) {
         case TP_FIELD_UNIFORM:
@@ -373,6 +410,10 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
         case TP_FIELD_GRID: {
             if (!GRID) {
                 F = {0.0, 0.0, 0.0};
+                return;
+            }
+            if (GM == GM_ANY && f.general) {
+                grid_general_jac64(f, r, F, J);
                 return;
             }
             Ax ax, ay, az;
@@ -423,9 +464,9 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
     }
 }
 
-template <bool GRID>
+template <int GM>
 __device__ __forceinline__ D3 field_val64(const DevField& f, D3 r, double t) {
-    if (GRID) return field_eval64(f, r, t);
+    if (GM != GM_ANALYTIC) return field_eval64<GM == GM_ANY>(f, r, t);
     return analytic_eval64(f, r, t);
 }
 
@@ -437,11 +478,11 @@ struct MagProps {
     double Bmag;
 };
 
-template <bool GRID>
+template <int GM>
 __device__ __forceinline__ MagProps magnetic_properties64(const DevField& f, D3 r, double t) {
     MagProps m;
     double J[9];
-    field_jac64<GRID>(f, r, t, m.B, J);
+    field_jac64<GM>(f, r, t, m.B, J);
     m.Bmag = norm(m.B);
     if (m.Bmag == 0.0) {
         m.gradB = m.kappa = m.bh = D3{0.0, 0.0, 0.0};
@@ -476,12 +517,12 @@ __device__ __forceinline__ void work_terms64(const MagProps& mp, D3 E, D3 dBdt, 
 }
 
 // full orbit: v_par = v . b, mu = m |v - v_par b|^2 / (2 |B|), q = q2m m
-template <bool GRID>
+template <int GM>
 __device__ __forceinline__ void work_rates64(const DevFields& F, D3 r, D3 v, double t, double q2m, double m,
                                              double* W) {
     const double q = q2m * m;
-    const D3 E = field_val64<GRID>(F.E, r, t);
-    const MagProps mp = magnetic_properties64<GRID>(F.B, r, t);
+    const D3 E = field_val64<GM>(F.E, r, t);
+    const MagProps mp = magnetic_properties64<GM>(F.B, r, t);
     if (mp.Bmag == 0.0) {
         W[0] = W[1] = W[2] = W[3] = 0.0;
         return;
@@ -493,11 +534,11 @@ __device__ __forceinline__ void work_rates64(const DevFields& F, D3 r, D3 v, dou
 }
 
 // guiding centre: state (X, v_par), mu given, m = q / q2m
-template <bool GRID>
+template <int GM>
 __device__ __forceinline__ void work_rates_gc64(const DevFields& F, D3 X, double vpar, double t, double q,
                                                 double q2m, double mu, double* W) {
-    const D3 E = field_val64<GRID>(F.E, X, t);
-    const MagProps mp = magnetic_properties64<GRID>(F.B, X, t);
+    const D3 E = field_val64<GM>(F.E, X, t);
+    const MagProps mp = magnetic_properties64<GM>(F.B, X, t);
     if (mp.Bmag == 0.0) {
         W[0] = W[1] = W[2] = W[3] = 0.0;
         return;

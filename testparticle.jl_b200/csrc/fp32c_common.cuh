@@ -5,6 +5,7 @@
 // Multistep velocity updates in delta form.
 #pragma once
 
+#include "grid_general.cuh"
 #include "tp_device.cuh"
 
 namespace tpb {
@@ -205,7 +206,19 @@ __device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, 
     return o;
 }
 
+static __device__ __noinline__ F3 grid_general32(const DevField& g, const CPos& p) {
+    // grids off the fast path: float64 interpolation of the compensated
+    // position (grid_general.cuh), rounded to float
+    double r[3] = {(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+                   (double)p.hi[2] + (double)p.lo[2]};
+    double o[3];
+    if (!grid_general_eval<double>(g, r, o)) return nanf3();
+    return {(float)o[0], (float)o[1], (float)o[2]};
+}
+
+template <bool GEN = true>
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
+    if (GEN && g.general) return grid_general32(g, p);
     AxF ax, ay, az;
     if (!axes32(g, p, ax, ay, az)) return nanf3();
     const float4* T = g.tab32;
@@ -245,7 +258,7 @@ __device__ __forceinline__ F3 analytic_eval32(const DevField& f, const CPos& p, 
     }
 }
 
-template <bool PACKED_ONLY = false>
+template <bool PACKED_ONLY = false, bool GEN = true>
 __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
     if (PACKED_ONLY || F.eb32) {
         AxF ax, ay, az;
@@ -279,8 +292,8 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
                  xyz(b111), ax, ay, az);
         return;
     }
-    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32(F.E, p) : analytic_eval32(F.E, p, t);
-    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32(F.B, p) : analytic_eval32(F.B, p, t);
+    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p) : analytic_eval32(F.E, p, t);
+    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p) : analytic_eval32(F.B, p, t);
 }
 
 template <int FK>
@@ -291,7 +304,7 @@ __device__ __forceinline__ void eval_EB32t(const DevFields& F, const CPos& p, do
     } else if (FK == FK_EBGRID) {
         eval_EB32<true>(F, p, t, E, B);
     } else {
-        eval_EB32<false>(F, p, t, E, B);
+        eval_EB32<false, FK == FK_GENGRID>(F, p, t, E, B);
     }
 }
 

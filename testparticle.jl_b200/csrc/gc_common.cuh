@@ -28,16 +28,23 @@ struct GCPar {
 };
 
 // get_gc_derivatives (src/equations.jl:329-360), float64
-template <bool GRID>
+// the grid mode a guiding-centre kernel is selected for
+__host__ __device__ __forceinline__ int gc_grid_mode(const DevFields& f) {
+    const bool ge = f.E.kind == TP_FIELD_GRID, gb = f.B.kind == TP_FIELD_GRID;
+    if ((ge && f.E.general) || (gb && f.B.general)) return GM_ANY;
+    return (ge || gb) ? GM_GRID : GM_ANALYTIC;
+}
+
+template <int GM>
 struct RHS64 {
-    static constexpr bool kGrid = GRID;
+    static constexpr int kGM = GM;
     __device__ __forceinline__ G4 operator()(const DevFields& F, const G4& s, const GCPar& p,
                                              double t) const {
         D3 X{s.y[0], s.y[1], s.y[2]};
-        D3 E = field_val64<GRID>(F.E, X, t);
+        D3 E = field_val64<GM>(F.E, X, t);
         D3 B;
         double J[9];
-        field_jac64<GRID>(F.B, X, t, B, J);
+        field_jac64<GM>(F.B, X, t, B, J);
         double Bmag = norm(B);
         D3 bh = B / Bmag;
         D3 gB{(J[0] * bh.x + J[3] * bh.y) + J[6] * bh.z, (J[1] * bh.x + J[4] * bh.y) + J[7] * bh.z,
@@ -74,7 +81,7 @@ __device__ __forceinline__ GCPar gc_par(const GCArgs& a, int64_t i) {
     return {a.q_i ? a.q_i[i] : a.q, a.q2m_i ? a.q2m_i[i] : a.q2m, a.mu_i ? a.mu_i[i] : a.mu};
 }
 
-template <bool GRID>
+template <int GM>
 struct GCSaver {
     const GCArgs& a;
     int W;
@@ -93,7 +100,7 @@ struct GCSaver {
         for (int c = 0; c < 4; ++c) u[c * n] = s.y[c];
         const D3 X{s.y[0], s.y[1], s.y[2]};
         if (a.save_fields) {
-            D3 E = field_val64<GRID>(a.f.E, X, t), B = field_val64<GRID>(a.f.B, X, t);
+            D3 E = field_val64<GM>(a.f.E, X, t), B = field_val64<GM>(a.f.B, X, t);
             u[4 * n] = E.x;
             u[5 * n] = E.y;
             u[6 * n] = E.z;
@@ -104,7 +111,7 @@ struct GCSaver {
         if (a.save_work) {
             const GCPar p = gc_par(a, i);
             double w[4];
-            work_rates_gc64<GRID>(a.f, X, s.y[3], t, p.q, p.q2m, p.mu, w);
+            work_rates_gc64<GM>(a.f, X, s.y[3], t, p.q, p.q2m, p.mu, w);
             const int c0 = a.save_fields ? 10 : 4;
             for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
@@ -140,7 +147,7 @@ __device__ __forceinline__ G4 update_rk4(const RHS& f, const DevFields& F, const
 template <class RHS, bool QUEUE>
 __global__ void __launch_bounds__(256) k_rk4(GCArgs a) {
     const RHS f;
-    const GCSaver<RHS::kGrid> S(a);
+    const GCSaver<RHS::kGM> S(a);
     const uint64_t t_start = globaltimer_ns();
     int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t i = -1, it = 0, iout = 0, nt = 0, nout = 0;
@@ -313,7 +320,7 @@ __device__ __forceinline__ void update_dp5(const RHS& f, const DevFields& F, con
 template <class RHS, bool QUEUE>
 __global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
     const RHS f;
-    const GCSaver<RHS::kGrid> S(a);
+    const GCSaver<RHS::kGM> S(a);
     const uint64_t t_start = globaltimer_ns();
     int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const double safety = 0.9, max_growth = 5.0, min_growth = 0.2;
@@ -335,7 +342,7 @@ __global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
                 dt = a.dt_i[i];
             } else if (!a.dt_given) {
                 D3 R{xv.y[0], xv.y[1], xv.y[2]};
-                double Bmag = norm(field_val64<RHS::kGrid>(a.f.B, R, t));
+                double Bmag = norm(field_val64<RHS::kGM>(a.f.B, R, t));
                 if (Bmag == 0.0 || p.q2m == 0.0) {
                     dt = 1.0e-6;
                 } else {

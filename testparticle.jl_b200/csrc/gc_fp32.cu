@@ -71,21 +71,21 @@ __device__ __forceinline__ void field_jac32(const DevField& f, V3f r, float t, V
     B = field32(f, r, t);
 }
 
-template <bool GRID>
+template <int GM>
 struct RHS32 {
-    static constexpr bool kGrid = GRID;
+    static constexpr int kGM = GM;
     __device__ __forceinline__ G4 operator()(const DevFields& F, const G4& s, const GCPar& p,
                                              double t) const {
         V3f E, B;
         float J[9];
         V3f X{(float)s.y[0], (float)s.y[1], (float)s.y[2]};
         float tf = (float)t;
-        if (GRID) {
+        if (GM != GM_ANALYTIC) {
             // grid fields: value and Jacobian from the float64 interpolant
             D3 Xd{s.y[0], s.y[1], s.y[2]};
-            D3 Ed = field_eval64(F.E, Xd, t), Bd;
+            D3 Ed = field_eval64<GM == GM_ANY>(F.E, Xd, t), Bd;
             double Jd[9];
-            field_jac64<true>(F.B, Xd, t, Bd, Jd);
+            field_jac64<GM>(F.B, Xd, t, Bd, Jd);
             E = {(float)Ed.x, (float)Ed.y, (float)Ed.z};
             B = {(float)Bd.x, (float)Bd.y, (float)Bd.z};
             for (int k = 0; k < 9; ++k) J[k] = (float)Jd[k];
@@ -120,9 +120,10 @@ static const void* gc_kernel32(bool rk4, bool queue) {
 }
 
 const void* select_gc_kernel32(const GCArgs& a, bool queue) {
-    bool grid = a.f.E.kind == TP_FIELD_GRID || a.f.B.kind == TP_FIELD_GRID;
+    const int gm = gc_grid_mode(a.f);
     bool rk4 = a.alg == TP_GC_RK4;
-    return grid ? gc_kernel32<RHS32<true>>(rk4, queue) : gc_kernel32<RHS32<false>>(rk4, queue);
+    if (gm == GM_ANY) return gc_kernel32<RHS32<GM_ANY>>(rk4, queue);
+    return gm == GM_GRID ? gc_kernel32<RHS32<GM_GRID>>(rk4, queue) : gc_kernel32<RHS32<GM_ANALYTIC>>(rk4, queue);
 }
 
 cudaError_t launch_gc_fp32(const GCArgs& a, const LaunchCfg& c, cudaStream_t s) {

@@ -40,6 +40,45 @@ cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// get_fields / get_work (src/boris/boris.jl:599-640) at n states: E and B,
+// then the work rates of get_work_rates (src/equations.jl:394-441) or
+// get_work_rates_gc (:445-480), in the order of the savers.
+__global__ void k_eval_points(PointsArgs a) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double* s = a.u + (int64_t)a.stride * i;
+    const double t = a.t[i];
+    double* o = a.out + (int64_t)a.wout * i;
+    D3 x{s[0], s[1], s[2]};
+    int c = 0;
+    if (a.want & 1) {
+        D3 E = field_eval64(a.f.E, x, t), B = field_eval64(a.f.B, x, t);
+        o[0] = E.x;
+        o[1] = E.y;
+        o[2] = E.z;
+        o[3] = B.x;
+        o[4] = B.y;
+        o[5] = B.z;
+        c = 6;
+    }
+    if (a.want & 2) {
+        double W[4];
+        if (a.kind == TP_POINTS_GC)
+            work_rates_gc64<GM_ANY>(a.f, x, s[3], t, a.q, a.q2m, a.mu, W);
+        else
+            work_rates64<GM_ANY>(a.f, x, D3{s[3], s[4], s[5]}, t, a.q2m, a.m, W);
+        for (int k = 0; k < 4; ++k) o[c + k] = W[k];
+    }
+}
+
+cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    int block = 128;
+    int64_t grid = (a.n + block - 1) / block;
+    k_eval_points<<<(unsigned)grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <class R>
 static const void* gc_kernel(bool rk4, bool queue) {
     if (rk4) return queue ? (const void*)k_rk4<R, true> : (const void*)k_rk4<R, false>;
@@ -47,9 +86,10 @@ static const void* gc_kernel(bool rk4, bool queue) {
 }
 
 const void* select_gc_kernel64(const GCArgs& a, bool queue) {
-    bool grid = a.f.E.kind == TP_FIELD_GRID || a.f.B.kind == TP_FIELD_GRID;
+    const int gm = gc_grid_mode(a.f);
     bool rk4 = a.alg == TP_GC_RK4;
-    return grid ? gc_kernel<RHS64<true>>(rk4, queue) : gc_kernel<RHS64<false>>(rk4, queue);
+    if (gm == GM_ANY) return gc_kernel<RHS64<GM_ANY>>(rk4, queue);
+    return gm == GM_GRID ? gc_kernel<RHS64<GM_GRID>>(rk4, queue) : gc_kernel<RHS64<GM_ANALYTIC>>(rk4, queue);
 }
 
 const void* select_gc_kernel32(const GCArgs& a, bool queue);

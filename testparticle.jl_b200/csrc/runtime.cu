@@ -53,6 +53,7 @@ struct tp_field {
     uint64_t eb_partner = 0;
     void* d_eb = nullptr;
     void* d_eb32 = nullptr;
+    void* d_axis[3] = {nullptr, nullptr, nullptr};  // node coordinates of non-uniform axes
 };
 
 // Results stay on the device until tp_result_copy moves them into the
@@ -273,8 +274,60 @@ void fill_float_copies(DevField& d) {
     d.Kf = (float)(d.coef * mm);
 }
 
+// Validation of a grid descriptor (the reference's build_interpolator
+// errors, src/utility/interpolation.jl:126-311); empty when valid.
+std::string check_grid_desc(const tp_field_desc* d) {
+    if (d->bc < TP_BC_FILL_NAN || d->bc > TP_BC_PERIODIC_INCLUSIVE) return "unknown grid boundary condition";
+    if (d->dtype != TP_DTYPE_F32 && d->dtype != TP_DTYPE_F64) return "grid dtype must be float32 or float64";
+    if (!d->data) return "grid data pointer is null";
+    if (d->order < TP_ORDER_LINEAR || d->order > TP_ORDER_CUBIC)
+        return "Interpolation order is not supported. Supported orders are 0, 1, and 3.";
+    if (d->geometry < TP_GRID_CARTESIAN || d->geometry > TP_GRID_SPHERICAL_SCALAR) return "unknown grid geometry";
+    const bool sph = d->geometry != TP_GRID_CARTESIAN;
+    if (d->ndim < 0 || d->ndim > 3 || (sph && d->ndim != 0 && d->ndim != 3)) return "grid ndim must be 1, 2 or 3";
+    const int ndim = d->ndim == 0 ? 3 : d->ndim;
+    if (ndim == 1 && (d->dir < 0 || d->dir > 2)) return "1-D grid dir must be 0, 1 or 2";
+    int64_t nodes = 1;
+    for (int k = 0; k < 3; ++k) {
+        if (k >= ndim) {
+            if (d->n[k] != 1) return "unused axes of a 1-D / 2-D grid must have n = 1";
+            if (d->axis[k]) return "unused axes of a 1-D / 2-D grid take no node coordinates";
+            continue;
+        }
+        if (d->n[k] < 2 || d->n[k] > (1 << 20)) return "grid needs 2 .. 2^20 nodes per axis";
+        if (d->axis[k]) {
+            const double* c = d->axis[k];
+            for (int64_t i = 0; i < d->n[k]; ++i)
+                if (!std::isfinite(c[i]) || (i > 0 && !(c[i] > c[i - 1])))
+                    return "grid vectors must be finite and strictly increasing";
+            if (d->order == TP_ORDER_CUBIC)
+                return "RectilinearGrid (CartesianNonUniform) only supports order=1 (Linear) interpolation.";
+            const bool periodic_axis =
+                sph ? k == 2 : (d->bc == TP_BC_PERIODIC || d->bc == TP_BC_PERIODIC_INCLUSIVE);
+            if (periodic_axis) return "periodic axes must be uniform";
+        } else if (!(d->spacing[k] > 0.0) || !std::isfinite(d->spacing[k])) {
+            return "grid spacing must be positive and finite";
+        }
+        nodes *= d->n[k];
+    }
+    if (nodes > ((int64_t)1 << 31) / 2) return "grid too large (more than 2^30 nodes)";
+    if (sph) {
+        // build_interpolator(StructuredGrid, ...) assertions (:270-280)
+        double r0 = d->axis[0] ? d->axis[0][0] : d->origin[0];
+        double t0 = d->axis[1] ? d->axis[1][0] : d->origin[1];
+        double t1 = d->axis[1] ? d->axis[1][d->n[1] - 1] : d->origin[1] + (double)(d->n[1] - 1) * d->spacing[1];
+        double p0 = d->origin[2], p1 = d->origin[2] + (double)(d->n[2] - 1) * d->spacing[2];
+        const double pi = 3.141592653589793, eps = 1e-12;
+        if (!(r0 >= 0.0)) return "r must be non-negative.";
+        if (!(t0 >= -eps && t1 <= pi + eps)) return "theta must be within [0, pi].";
+        if (!(p0 >= -eps && p1 <= 2.0 * pi + eps)) return "phi must be within [0, 2pi].";
+    }
+    return std::string();
+}
+
 bool same_geometry(const tp_field* a, const tp_field* b) {
     if (a->desc.kind != TP_FIELD_GRID || b->desc.kind != TP_FIELD_GRID) return false;
+    if (a->dev.general || b->dev.general) return false;
     if (a->desc.bc != b->desc.bc || a->desc.dtype != b->desc.dtype) return false;
     for (int k = 0; k < 3; ++k) {
         if (a->desc.n[k] != b->desc.n[k]) return false;
@@ -352,7 +405,7 @@ void set_wrap(BorisArgs& a, const tp_field* E, const tp_field* B, const tp_term_
                     if (g->desc.jac[3 * r + c] != 0.0) ok = false;
                 continue;
             }
-            if (k != TP_FIELD_GRID || g->desc.bc != TP_BC_PERIODIC) {
+            if (k != TP_FIELD_GRID || g->desc.bc != TP_BC_PERIODIC || g->dev.general) {
                 ok = false;
                 continue;
             }
@@ -492,37 +545,56 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
         case TP_FIELD_DIPOLE:
             break;
         case TP_FIELD_GRID: {
-            if (d->bc != TP_BC_FILL_NAN && d->bc != TP_BC_CLAMP && d->bc != TP_BC_PERIODIC) {
+            std::string why = check_grid_desc(d);
+            if (!why.empty()) {
                 delete f;
-                return fail(ctx, TP_E_ARG, "unknown grid boundary condition");
+                return fail(ctx, TP_E_ARG, why);
             }
-            if (d->dtype != TP_DTYPE_F32 && d->dtype != TP_DTYPE_F64) {
-                delete f;
-                return fail(ctx, TP_E_ARG, "grid dtype must be float32 or float64");
+            const bool sph = d->geometry != TP_GRID_CARTESIAN;
+            const int ndim = sph ? 3 : (d->ndim == 0 ? 3 : d->ndim);
+            dv.order = d->order;
+            dv.geom = d->geometry;
+            dv.ndim = ndim;
+            dv.dir = d->dir;
+            for (int k = 0; k < 3; ++k) dv.abc[k] = d->bc;
+            if (sph) {
+                // SphericalFieldInterpolator: r and theta fill NaN, phi periodic
+                // (interpolation.jl:150-164)
+                dv.abc[0] = TP_BC_FILL_NAN;
+                dv.abc[1] = TP_BC_FILL_NAN;
+                dv.abc[2] = TP_BC_PERIODIC_INCLUSIVE;
             }
-            if (!d->data) {
-                delete f;
-                return fail(ctx, TP_E_ARG, "grid data pointer is null");
-            }
+            bool general = d->order != TP_ORDER_LINEAR || d->geometry != TP_GRID_CARTESIAN || ndim != 3 ||
+                           d->bc == TP_BC_PERIODIC_INCLUSIVE;
             int64_t nodes = 1;
             for (int k = 0; k < 3; ++k) {
-                if (d->n[k] < 2 || d->n[k] > (1 << 20)) {
-                    delete f;
-                    return fail(ctx, TP_E_ARG, "grid needs 2 .. 2^20 nodes per axis");
-                }
-                if (!(d->spacing[k] > 0.0) || !std::isfinite(d->spacing[k])) {
-                    delete f;
-                    return fail(ctx, TP_E_ARG, "grid spacing must be positive and finite");
-                }
                 nodes *= d->n[k];
                 dv.n[k] = (int32_t)d->n[k];
-                dv.x0[k] = d->origin[k];
-                dv.inv_dx[k] = 1.0 / d->spacing[k];
-                dv.L[k] = (double)d->n[k] * d->spacing[k];
+                if (d->axis[k]) {
+                    general = true;
+                    dv.x0[k] = d->axis[k][0];
+                    dv.inv_dx[k] = 1.0;
+                    dv.L[k] = d->axis[k][d->n[k] - 1] - d->axis[k][0];
+                } else {
+                    double sp = d->n[k] == 1 ? 1.0 : d->spacing[k];
+                    dv.x0[k] = d->origin[k];
+                    dv.inv_dx[k] = 1.0 / sp;
+                    dv.L[k] = (double)d->n[k] * sp;
+                }
             }
-            if (nodes > ((int64_t)1 << 31) / 2) {
-                delete f;
-                return fail(ctx, TP_E_ARG, "grid too large (more than 2^30 nodes)");
+            dv.general = general ? 1 : 0;
+            for (int k = 0; k < 3; ++k) {
+                if (!d->axis[k]) continue;
+                cudaError_t e = cudaMalloc(&f->d_axis[k], (size_t)d->n[k] * sizeof(double));
+                if (e == cudaSuccess)
+                    e = cudaMemcpy(f->d_axis[k], d->axis[k], (size_t)d->n[k] * sizeof(double),
+                                   cudaMemcpyDefault);
+                if (e != cudaSuccess) {
+                    int r = cuda_fail(ctx, e, "grid axis upload");
+                    tp_field_destroy(f);
+                    return r;
+                }
+                dv.ax[k] = (const double*)f->d_axis[k];
             }
             f->nodes = nodes;
             bool f64 = d->dtype == TP_DTYPE_F64;
@@ -586,7 +658,7 @@ void tp_field_destroy(tp_field* f) {
     if (!f) return;
     DeviceGuard g(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
-    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32})
+    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_axis[0], f->d_axis[1], f->d_axis[2]})
         if (p) cudaFree(p);
     delete f;
 }
@@ -1227,6 +1299,64 @@ int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B, const doubl
     return TP_OK;
 }
 
+namespace {
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
+int tp_eval_points(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, const tp_field* B,
+                   const double* u, const double* t, int64_t n, double* out) {
+    if (!ctx || !d || !E || !B) return fail(ctx, TP_E_ARG, "null argument");
+    if (d->kind != TP_POINTS_FULL_ORBIT && d->kind != TP_POINTS_GC) return fail(ctx, TP_E_ARG, "unknown state kind");
+    if (d->want < 1 || d->want > 3) return fail(ctx, TP_E_ARG, "want must select fields (1), work (2) or both (3)");
+    const int minw = d->kind == TP_POINTS_GC ? 4 : 6;
+    if (d->stride < minw) return fail(ctx, TP_E_ARG, "stride is shorter than a state");
+    if (n < 0 || (n > 0 && (!u || !t || !out))) return fail(ctx, TP_E_ARG, "bad buffers");
+    if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");
+    if (n == 0) return TP_OK;
+    const int wout = 6 * (d->want & 1) + 4 * ((d->want >> 1) & 1);
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    const size_t ub = (size_t)n * d->stride * sizeof(double), tb = (size_t)n * sizeof(double),
+                 ob = (size_t)n * wout * sizeof(double);
+    // device-resident arguments are used in place
+    const bool u_dev = is_device_ptr(u), t_dev = is_device_ptr(t), o_dev = is_device_ptr(out);
+    DBuf u_d, t_d, o_d;
+    cudaError_t e = cudaSuccess;
+    if (!u_dev) e = u_d.alloc(ub);
+    if (e == cudaSuccess && !t_dev) e = t_d.alloc(tb);
+    if (e == cudaSuccess && !o_dev) e = o_d.alloc(ob);
+    if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, "device allocation");
+    if (!u_dev) e = copy_to_device(ctx, u_d.p, u, ub);
+    if (e == cudaSuccess && !t_dev) e = copy_to_device(ctx, t_d.p, t, tb);
+    PointsArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.f.E = E->dev;
+    a.f.B = B->dev;
+    a.u = u_dev ? u : u_d.as<double>();
+    a.t = t_dev ? t : t_d.as<double>();
+    a.n = n;
+    a.stride = d->stride;
+    a.want = d->want;
+    a.wout = wout;
+    a.kind = d->kind;
+    a.q2m = d->q2m;
+    a.m = d->m;
+    a.q = d->q;
+    a.mu = d->mu;
+    a.out = o_dev ? out : o_d.as<double>();
+    if (e == cudaSuccess) e = launch_eval_points(a, ctx->stream);
+    if (e == cudaSuccess) e = o_dev ? cudaStreamSynchronize(ctx->stream) : copy_to_host(ctx, out, o_d.p, ob);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "eval_points");
+    return TP_OK;
+}
+
 int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_field* B,
               const double* y0, const double* q_i, const double* q2m_i, const double* mu_i,
               const double* dt_i, const double* tend_i, int64_t n, tp_result** out) {
@@ -1524,6 +1654,8 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
     if (r->term.flags != 0) return fail(ctx, TP_E_UNSUPPORTED, "the adjoint takes no termination predicate");
     if (!field_static(E) || !field_static(B))
         return fail(ctx, TP_E_UNSUPPORTED, "the adjoint needs static fields");
+    if (E->dev.general || B->dev.general)
+        return fail(ctx, TP_E_UNSUPPORTED, "the adjoint covers trilinear uniform Cartesian grids");
     if (d->checkpoint_every < 1) return fail(ctx, TP_E_ARG, "checkpoint_every must be >= 1");
     if (n < 0) return fail(ctx, TP_E_ARG, "negative particle count");
     if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");

@@ -49,6 +49,14 @@ struct DevField {
     float Kf;         //   intermediates normal: coef / r^5 alone underflows)
     const void* tab;  // per-node table: float4 / double4 per node (x,y,z,0)
     const float4* tab32;  // float table for the FP32C kernels (same as tab for float data)
+    // grids off the trilinear uniform Cartesian 3-D fast path (grid_general.cuh)
+    int32_t general;  // 1: order, geometry, dimension or axes differ from the fast path
+    int32_t order;    // TP_ORDER_*
+    int32_t geom;     // TP_GRID_*
+    int32_t dir;      // 1-D interpolant: the coordinate axis 0 reads
+    int32_t abc[3];   // per-axis boundary (TP_BC_*)
+    int32_t ndim;
+    const double* ax[3];  // device node coordinates of non-uniform axes, else null
 };
 
 struct DevFields {
@@ -72,9 +80,13 @@ struct DevTerm {
 //   FK_ANALYTIC  E and B analytic (zero / uniform / affine / dipole)
 //   FK_EBGRID    E and B grids on one geometry, interleaved table
 //   FK_GENERIC   anything else (separate grids, grid + analytic)
-enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2 };
+//   FK_GENGRID   at least one grid off the trilinear uniform Cartesian path
+//                (order 0 / 3, rectilinear, spherical, 1-D / 2-D)
+enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2, FK_GENGRID = 3 };
 
 __host__ __device__ __forceinline__ int field_config_of(const DevFields& f) {
+    if ((f.E.kind == TP_FIELD_GRID && f.E.general) || (f.B.kind == TP_FIELD_GRID && f.B.general))
+        return FK_GENGRID;
     if (f.eb && !f.eb_f64) return FK_EBGRID;  // float interleaved table
     if (f.E.kind != TP_FIELD_GRID && f.B.kind != TP_FIELD_GRID) return FK_ANALYTIC;
     return FK_GENERIC;

@@ -51,6 +51,17 @@ struct GCPrepArgs {
     double* mu;
 };
 
+// fields and work rates at given states (tp_eval_points)
+struct PointsArgs {
+    DevFields f;
+    const double* u;   // n states, `stride` doubles each
+    const double* t;   // n times
+    int64_t n;
+    int32_t stride, want, wout, kind;
+    double q2m, m, q, mu;
+    double* out;       // n rows of wout doubles
+};
+
 // discrete adjoint of the fixed-step Boris map (adjoint.cu)
 struct AdjArgs {
     BorisArgs a;           // fields, q2m, t0, dt, FP32C wrap data, n, u0 (device, n x 6)
@@ -96,6 +107,7 @@ cudaError_t launch_gc(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_gc_fp32(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 int occupancy_gc(const GCArgs& a, int block);
 cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
+cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
 
 // context accessors for translation units outside runtime.cu
 int ctx_device(const tp_ctx* ctx);

@@ -8,9 +8,9 @@ field types that cover the reference's tests and workloads:
 * UniformField(value)                          a constant vector
 * AffineField(value, jac, rate)                value + jac @ x + rate * t
 * DipoleField(moment, center, coef)            point dipole (Magnetostatics.Dipole)
-* FieldInterpolator via build_interpolator     src/utility/interpolation.jl:217-235
-  (order 1, uniform Cartesian grid, FillExtrap(NaN) / ClampExtrap() /
-  PeriodicBC(endpoint=:exclusive) == WrapExtrap())
+* FieldInterpolator via build_interpolator     src/utility/interpolation.jl:15-311
+  (orders 0 / 1 / 3; Cartesian, rectilinear and spherical grids; 1-D, 2-D
+  and 3-D interpolants; FillExtrap(NaN) / ClampExtrap() / PeriodicBC)
 
 Any other callable raises NotImplementedError naming these types.
 """
@@ -143,9 +143,23 @@ class WrapExtrap:
 
 @dataclass(frozen=True)
 class PeriodicBC:
-    """PeriodicBC(endpoint='exclusive'), the same as WrapExtrap()."""
+    """PeriodicBC(endpoint='exclusive') (period n * dx, the same as
+    WrapExtrap()) or endpoint='inclusive' (period (n - 1) * dx: the last node
+    repeats the first)."""
 
     endpoint: str = "exclusive"
+
+
+class CartesianGrid:
+    """Grid-type marker of build_interpolator (Meshes.CartesianGrid)."""
+
+
+class RectilinearGrid:
+    """Grid-type marker: axes given by node coordinates (Meshes.RectilinearGrid)."""
+
+
+class StructuredGrid:
+    """Grid-type marker: spherical (r, theta, phi) axes (Meshes.StructuredGrid)."""
 
 
 def _bc_code(bc) -> int:
@@ -158,13 +172,19 @@ def _bc_code(bc) -> int:
     if isinstance(bc, WrapExtrap):
         return _abi.TP_BC_PERIODIC
     if isinstance(bc, PeriodicBC):
-        if bc.endpoint != "exclusive":
-            raise NotImplementedError("PeriodicBC supports endpoint='exclusive' only")
-        return _abi.TP_BC_PERIODIC
+        if bc.endpoint == "exclusive":
+            return _abi.TP_BC_PERIODIC
+        if bc.endpoint == "inclusive":
+            return _abi.TP_BC_PERIODIC_INCLUSIVE
+        raise ValueError(f"unknown PeriodicBC endpoint {bc.endpoint!r}")
     raise TypeError(f"unknown boundary condition {bc!r}")
 
 
-def _uniform_axis(g) -> tuple[float, float, int]:
+_ORDER = {0: _abi.TP_ORDER_CONSTANT, 1: _abi.TP_ORDER_LINEAR, 3: _abi.TP_ORDER_CUBIC}
+
+
+def _axis(g, force_coords: bool = False):
+    """(origin, spacing, n, coords): coords is None for a uniform axis."""
     g = np.asarray(g, dtype=float)
     if g.ndim != 1 or g.size < 2:
         raise ValueError("grid axes must be 1-D with at least 2 nodes")
@@ -172,33 +192,49 @@ def _uniform_axis(g) -> tuple[float, float, int]:
         raise ValueError("grid vectors must be sorted (strictly increasing)")
     n = g.size
     dx = (g[-1] - g[0]) / (n - 1)
-    if not np.allclose(np.diff(g), dx, rtol=1e-9, atol=0.0):
-        raise NotImplementedError("only uniform (Cartesian) grids are supported on the B200")
-    return float(g[0]), float(dx), int(n)
+    if not force_coords and np.allclose(np.diff(g), dx, rtol=1e-9, atol=0.0):
+        return float(g[0]), float(dx), int(n), None
+    return float(g[0]), float(dx), int(n), np.ascontiguousarray(g)
 
 
 @dataclass
 class FieldInterpolator(AbstractField):
-    """Trilinear interpolator of a vector field on a uniform Cartesian grid.
+    """A gridded vector field: the reference's FieldInterpolator /
+    FieldInterpolator2D / FieldInterpolator1D / SphericalFieldInterpolator
+    (src/utility/interpolation.jl:15-117).
 
-    `data[c, i, j, k]` is component c at node (x[i], y[j], z[k]) -- the
-    reference's (3, nx, ny, nz) array.  Stored column-major (Julia's memory
-    order) so the device receives exactly the reference's layout.
+    `data[c, i, j, k]` is component c at node (i, j, k) -- the reference's
+    (3, n1, n2, n3) array -- stored column-major (Julia's memory order) so the
+    device receives exactly the reference's layout.  Unused axes of 1-D / 2-D
+    interpolants have one node.  `axes[a]` holds the node coordinates of a
+    non-uniform axis (None: origin + k * spacing).  Scalar grids are carried
+    as the first component of a vector field.
     """
 
     data: np.ndarray
     origin: tuple
     spacing: tuple
     bc: object = field(default_factory=FillExtrap)
+    order: int = 1
+    geometry: str = "cartesian"      # "spherical", or "spherical_scalar" for a scalar
+    ndim: int = 3
+    dir: int = 0                     # 1-D: the coordinate read (0-based)
+    axes: tuple = (None, None, None)
 
     def __post_init__(self):
         a = np.asarray(self.data)
+        if a.ndim == 4 - (3 - self.ndim) and a.shape[0] == 3 and self.ndim < 3:
+            a = a.reshape(a.shape + (1,) * (4 - a.ndim))
         if a.ndim != 4 or a.shape[0] != 3:
             raise ValueError("Incompatible 3D force field and grid! (expected a (3, nx, ny, nz) array)")
         if a.dtype not in (np.float32, np.float64):
             a = a.astype(np.float64)
         self.data = np.asfortranarray(a)
         self._bc = _bc_code(self.bc)
+        if self.order not in _ORDER:
+            raise ValueError(f"Interpolation order {self.order} is not supported. "
+                             "Supported orders are 0, 1, and 3.")
+        self._axes = tuple(None if c is None else np.ascontiguousarray(c, dtype=np.float64) for c in self.axes)
 
     @property
     def n(self):
@@ -213,31 +249,103 @@ class FieldInterpolator(AbstractField):
             d.n[k] = int(self.data.shape[1 + k])
             d.origin[k] = float(self.origin[k])
             d.spacing[k] = float(self.spacing[k])
+            c = self._axes[k]
+            d.axis[k] = None if c is None else c.ctypes.data
         d.data = self.data.ctypes.data_as(C.c_void_p)
+        d.order = _ORDER[self.order]
+        d.geometry = {"cartesian": _abi.TP_GRID_CARTESIAN, "spherical": _abi.TP_GRID_SPHERICAL,
+                      "spherical_scalar": _abi.TP_GRID_SPHERICAL_SCALAR}[self.geometry]
+        d.ndim = int(self.ndim)
+        d.dir = int(self.dir)
         return d
 
     def keepalive(self):
-        return self.data
+        return (self.data, self._axes)
 
 
-def build_interpolator(A, x, y, z, order: int = 1, bc=None, gridtype="CartesianGrid"):
-    """build_interpolator(CartesianGrid, A, x, y, z, order, bc) of the reference.
-
-    Only order 1 (trilinear) on uniform Cartesian grids is evaluated on the
-    device; other orders and grid types raise NotImplementedError.
-    """
-    if gridtype not in ("CartesianGrid", None):
-        raise NotImplementedError(f"{gridtype} grids are not supported on the B200")
-    if order not in (0, 1, 3):
-        raise ValueError(f"Interpolation order {order} is not supported. Supported orders are 0, 1, and 3.")
-    if order != 1:
-        raise NotImplementedError("only order=1 (trilinear) interpolation runs on the B200")
-    ax = [_uniform_axis(g) for g in (x, y, z)]
+def _vector_data(A, ngrid: int) -> np.ndarray:
+    """(3, n...) vector data, or a scalar (n...) array carried as component 0."""
     A = np.asarray(A)
-    if A.shape[1:] != tuple(a[2] for a in ax):
+    if A.ndim == ngrid + 1 and A.shape[0] == 3:
+        return A
+    if A.ndim == ngrid:
+        V = np.zeros((3,) + A.shape, dtype=A.dtype if A.dtype in (np.float32, np.float64) else np.float64)
+        V[0] = A
+        return V
+    raise ValueError(f"Incompatible {ngrid}D force field and grid!")
+
+
+def build_interpolator(*args, dir: int = 1, coeffs=None):
+    """build_interpolator([gridtype,] A, grids..., order=1, bc=FillExtrap(NaN); dir, coeffs).
+
+    The reference's entry point (src/utility/interpolation.jl:190-311):
+    `gridtype` is CartesianGrid (default; 1, 2 or 3 axes, uniform or given by
+    node coordinates), RectilinearGrid (order 1 only) or StructuredGrid
+    (spherical r, theta, phi: r and theta fill NaN outside, phi periodic).
+    `order` is 0, 1 or 3 (cubic on uniform axes).  `dir` (1-based) selects the
+    coordinate a 1-D interpolant reads.  `coeffs` is accepted for signature
+    compatibility (the cubic is always evaluated on the fly).
+    """
+    args = list(args)
+    gridtype = CartesianGrid
+    if args and isinstance(args[0], type) and args[0] in (CartesianGrid, RectilinearGrid, StructuredGrid):
+        gridtype = args.pop(0)
+    elif args and isinstance(args[0], str):
+        gridtype = {"CartesianGrid": CartesianGrid, "RectilinearGrid": RectilinearGrid,
+                    "StructuredGrid": StructuredGrid}[args.pop(0)]
+    if not args:
+        raise TypeError("build_interpolator needs a field array")
+    A = args.pop(0)
+    grids = []
+    while args and not isinstance(args[0], (int, np.integer)) and not isinstance(
+            args[0], (FillExtrap, ClampExtrap, WrapExtrap, PeriodicBC)) and args[0] is not None:
+        grids.append(args.pop(0))
+    order = int(args.pop(0)) if args and args[0] is not None else 1
+    if args and args[0] is None:
+        args.pop(0)
+    bc = args.pop(0) if args else None
+    if args:
+        raise TypeError("too many arguments to build_interpolator")
+    if order not in _ORDER:
+        raise ValueError(f"Interpolation order {order} is not supported. Supported orders are 0, 1, and 3.")
+    if not 1 <= len(grids) <= 3:
+        raise ValueError("build_interpolator takes 1, 2 or 3 grid axes")
+    bc = bc if bc is not None else FillExtrap()
+    if gridtype is StructuredGrid:
+        if len(grids) != 3:
+            raise ValueError("StructuredGrid needs r, theta and phi axes")
+        ax = [_axis(grids[0]), _axis(grids[1]), _axis(grids[2])]
+        if ax[2][3] is not None:
+            raise NotImplementedError("the phi axis of a spherical grid must be uniform")
+        r0 = ax[0][0]
+        t0, t1 = ax[1][0], ax[1][0] + ax[1][1] * (ax[1][2] - 1)
+        p0, p1 = ax[2][0], ax[2][0] + ax[2][1] * (ax[2][2] - 1)
+        if r0 < 0:
+            raise ValueError("r must be non-negative.")
+        if t0 < -1e-12 or t1 > math.pi + 1e-12:
+            raise ValueError("θ must be within [0, π].")
+        if p0 < -1e-12 or p1 > 2 * math.pi + 1e-12:
+            raise ValueError("ϕ must be within [0, 2π].")
+        data = _vector_data(A, 3)
+        geometry = "spherical" if np.ndim(A) == 4 else "spherical_scalar"
+        ndim = 3
+    else:
+        rect = gridtype is RectilinearGrid
+        if rect and order != 1:
+            raise ValueError("RectilinearGrid (CartesianNonUniform) only supports order=1 (Linear) interpolation.")
+        ax = [_axis(g, force_coords=rect) for g in grids]
+        if order == 3 and any(a[3] is not None for a in ax):
+            raise NotImplementedError("cubic interpolation runs on uniform axes")
+        ndim = len(grids)
+        data = _vector_data(A, ndim)
+        geometry = "cartesian"
+        while len(ax) < 3:
+            ax.append((0.0, 1.0, 1, None))
+    if tuple(data.shape[1:1 + len(grids)]) != tuple(a[2] for a in ax[:len(grids)]):
         raise ValueError("field array shape does not match the grid")
-    return FieldInterpolator(A, tuple(a[0] for a in ax), tuple(a[1] for a in ax),
-                             bc if bc is not None else FillExtrap())
+    return FieldInterpolator(data, tuple(a[0] for a in ax), tuple(a[1] for a in ax), bc, order=order,
+                             geometry=geometry, ndim=ndim, dir=int(dir) - 1 if ndim == 1 else 0,
+                             axes=tuple(a[3] for a in ax))
 
 
 def as_field(f) -> AbstractField:

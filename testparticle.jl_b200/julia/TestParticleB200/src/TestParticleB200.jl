@@ -150,7 +150,14 @@ struct TpFieldDesc
     moment::NTuple{3, Float64}; center::NTuple{3, Float64}; coef::Float64
     n::NTuple{3, Int64}; origin::NTuple{3, Float64}; spacing::NTuple{3, Float64}
     data::Ptr{Cvoid}
+    # grid tail: order, geometry, ndim, dir, per-axis node coordinates (all
+    # zero: trilinear on a uniform Cartesian 3-D grid)
+    order::Int32; geometry::Int32; ndim::Int32; dir::Int32
+    axis::NTuple{3, Ptr{Float64}}
 end
+TpFieldDesc(kind, bc, dtype, reserved, value, jac, rate, moment, center, coef, n, origin, spacing, data) =
+    TpFieldDesc(kind, bc, dtype, reserved, value, jac, rate, moment, center, coef, n, origin, spacing, data,
+        0, 0, 0, 0, (Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL)))
 struct TpTermDesc
     flags::Int32; reserved::Int32; rmin::Float64; rmax::Float64
     lo::NTuple{3, Float64}; hi::NTuple{3, Float64}; tmax::Float64

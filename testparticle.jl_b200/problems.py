@@ -214,11 +214,13 @@ def _species(species, q, m):
 
 
 def prepare(*args, species: Species = Proton, q=None, m=None, order: int = 1, bc=None,
-            E=None, F=None, **kw):
+            E=None, F=None, gridtype=None, **kw):
     """prepare(E, B, F=ZeroField(); species, q, m) -> (q2m, m, E, B, F).
 
-    Also prepare(x, y, z, E, B, F; order, bc) with E, B given as (3, nx, ny, nz)
-    arrays on uniform grids, and prepare(B; E=ZeroField()) (src/prepare.jl:136-170).
+    Also prepare(x, y, z, E, B, F; order, bc, gridtype) with E, B given as
+    (3, n1, n2, n3) arrays on the grid axes (gridtype CartesianGrid,
+    RectilinearGrid or StructuredGrid), and prepare(B; E=ZeroField())
+    (src/prepare.jl:136-170).
     """
     qq, mm = _species(species, q, m)
     if len(args) >= 5:
@@ -228,7 +230,9 @@ def prepare(*args, species: Species = Proton, q=None, m=None, order: int = 1, bc
 
         def grid(a):
             if isinstance(a, np.ndarray) and a.ndim == 4:
-                return build_interpolator(a, x, y, z, order, bc)
+                if gridtype is None:
+                    return build_interpolator(a, x, y, z, order, bc)
+                return build_interpolator(gridtype, a, x, y, z, order, bc)
             return as_field(a)
 
         return (qq / mm, mm, grid(Ea), grid(Ba), as_field(Fa))

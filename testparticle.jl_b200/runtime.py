@@ -56,8 +56,20 @@ class Context:
         self.handle = h
         self.device = device
         self._fields: dict[int, tuple] = {}
+        self._closed = [False]
         self.tuned_keys: set = set()
-        weakref.finalize(self, self.lib.tp_ctx_destroy, h)
+        # at exit the context is released before module teardown frees the
+        # field objects: release their device copies first, and make the
+        # field callbacks that run later do nothing
+        weakref.finalize(self, Context._close, self.lib, h, self._fields, self._closed)
+
+    @staticmethod
+    def _close(lib, handle, fields, closed):
+        closed[0] = True
+        for _ref, fh in list(fields.values()):
+            lib.tp_field_destroy(fh)
+        fields.clear()
+        lib.tp_ctx_destroy(handle)
 
     @classmethod
     def get(cls, device: int = 0) -> "Context":
@@ -82,8 +94,9 @@ class Context:
                "tp_field_create")
         lib = self.lib
 
-        def _drop(k=key, handle=h, fields=self._fields):
-            fields.pop(k, None)
+        def _drop(k=key, handle=h, fields=self._fields, closed=self._closed):
+            if closed[0] or fields.pop(k, None) is None:
+                return
             lib.tp_field_destroy(handle)
 
         try:
@@ -206,6 +219,25 @@ class Context:
                                       float(m), float(t), _ptr(y0), _ptr(mu))
         _check(self.lib, self.handle, code, "tp_gc_prepare")
         return y0, mu
+
+    def eval_points(self, E, B, u: np.ndarray, t: np.ndarray, *, gc: bool, want: int, q2m: float = 0.0,
+                    m: float = 0.0, q: float = 0.0, mu: float = 0.0) -> np.ndarray:
+        """tp_eval_points: E, B (want & 1) and work rates (want & 2) at n states."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64).reshape(-1)
+        if u.ndim != 2 or u.shape[0] != t.size:
+            raise ValueError("u must be (n, width) with one time per state")
+        d = _abi.PointsDesc()
+        d.kind = _abi.TP_POINTS_GC if gc else _abi.TP_POINTS_FULL_ORBIT
+        d.want = int(want)
+        d.stride = int(u.shape[1])
+        d.q2m, d.m, d.q, d.mu = float(q2m), float(m), float(q), float(mu)
+        wout = 6 * (want & 1) + 4 * ((want >> 1) & 1)
+        out = np.empty((t.size, wout))
+        code = self.lib.tp_eval_points(self.handle, C.byref(d), self.field(E), self.field(B), _ptr(u), _ptr(t),
+                                       t.size, _ptr(out))
+        _check(self.lib, self.handle, code, "tp_eval_points")
+        return out
 
     def _collect(self, res: C.c_void_p) -> "RunResult":
         lib = self.lib

@@ -25,14 +25,17 @@ RETCODE_NAMES = {
 
 
 class TraceSolution:
-    __slots__ = ("t", "u", "retcode", "alg", "nsteps")
+    __slots__ = ("t", "u", "retcode", "alg", "nsteps", "prob", "index")
 
-    def __init__(self, t: np.ndarray, u: np.ndarray, retcode: str, alg: str, nsteps: int = 0):
+    def __init__(self, t: np.ndarray, u: np.ndarray, retcode: str, alg: str, nsteps: int = 0, prob=None,
+                 index: int = 0):
         self.t = t
         self.u = u
         self.retcode = retcode
         self.alg = alg
         self.nsteps = nsteps
+        self.prob = prob      # the problem solved (get_fields / get_work read its fields)
+        self.index = index    # trajectory index within its ensemble
 
     def __len__(self):
         return self.t.size
@@ -78,14 +81,15 @@ class _Trajectories(Sequence):
             raise IndexError(i)
         a, b = e.offsets[i], e.offsets[i + 1]
         return TraceSolution(e.t_all[a:b], e.u_all[a:b], RETCODE_NAMES.get(int(e.retcodes[i]), "Default"),
-                             e.alg, int(e.nsteps[i]))
+                             e.alg, int(e.nsteps[i]), e.prob, i)
 
 
 class EnsembleSolution:
     """Ensemble of trajectories over packed buffers (t_all, u_all, offsets)."""
 
     def __init__(self, t_all, u_all, nsaved, retcodes, nsteps, alg: str, elapsed_s: float,
-                 elapsed_e2e_s: float = 0.0):
+                 elapsed_e2e_s: float = 0.0, prob=None):
+        self.prob = prob
         self.t_all = t_all
         self.u_all = u_all
         self.nsaved = nsaved

@@ -229,7 +229,8 @@ def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None
         t0 = time.perf_counter()
         r = ctx.gc_run(p.desc, p.E, p.B, p.y0, p.q_i, p.q2m_i, p.mu_i, p.dt_i, p.tend_i)
         wall = time.perf_counter() - t0
-        return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall)
+        return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall,
+                                prob=prob)
     if not isinstance(prob, TraceProblem):
         raise TypeError("prob must be a TraceProblem or TraceGCProblem")
     if not args:
@@ -247,7 +248,8 @@ def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None
     t0 = time.perf_counter()
     r = ctx.boris_run(p.desc, p.E, p.B, p.u0, p.dt_i, p.tend_i)
     wall = time.perf_counter() - t0
-    return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall)
+    return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, p.alg_name, r.elapsed_ms * 1e-3, wall,
+                            prob=prob)
 
 
 def prepare_gc(xv, E, B, *, species=None, q=None, m=None, t: float = 0.0, device: int = 0):

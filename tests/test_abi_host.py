@@ -111,10 +111,15 @@ def test_unsupported_inputs_raise(tp):
                       tp.Boris(), dt=0.1, isoutside=lambda u, p, t: False)
     with pytest.raises(ValueError):
         tp.MultistepBoris(3)
-    with pytest.raises(NotImplementedError):
-        tp.build_interpolator(np.zeros((3, 4, 4, 4)), np.arange(4.0), np.arange(4.0), np.arange(4.0), 3)
-    with pytest.raises(NotImplementedError):
-        tp.build_interpolator(np.zeros((3, 4, 4, 4)), [0, 1, 3, 4.0], np.arange(4.0), np.arange(4.0))
+    # interpolation.jl:145-146,246-248: unsupported orders and cubic rectilinear grids
+    with pytest.raises(ValueError):
+        tp.build_interpolator(np.zeros((3, 4, 4, 4)), np.arange(4.0), np.arange(4.0), np.arange(4.0), 2)
+    with pytest.raises(ValueError):
+        tp.build_interpolator(tp.RectilinearGrid, np.zeros((3, 4, 4, 4)), [0, 1, 3, 4.0], np.arange(4.0),
+                              np.arange(4.0), 3)
+    with pytest.raises(ValueError):   # StructuredGrid assertions (:270-280)
+        tp.build_interpolator(tp.StructuredGrid, np.zeros((3, 4, 4, 4)), np.arange(4.0),
+                              np.linspace(0, 4.0, 4), np.linspace(0, 6.0, 4))
 
 
 def test_grid_field_layout_is_julia_column_major(tp):

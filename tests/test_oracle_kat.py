@@ -397,15 +397,14 @@ def test_gyro_constants(tp):
     assert math.isclose(tp.get_gyroperiod(5.0e-9), 13.118894973717941, rel_tol=1.5e-8)
 
 
-def _scalar_grid(tp, bc):
+def _scalar_grid(tp, bc, order=1):
     # test_utility.jl:93-110: n[i,j,k] = i + j + k (1-based) on x(4), y(6), z(8) in [-10, 10]
     x = np.linspace(-10, 10, 4)
     y = np.linspace(-10, 10, 6)
     z = np.linspace(-10, 10, 8)
     i, j, k = np.meshgrid(np.arange(1, 5), np.arange(1, 7), np.arange(1, 9), indexing="ij")
-    A = np.zeros((3, 4, 6, 8), dtype=np.float32)
-    A[0] = (i + j + k).astype(np.float32)
-    return tp.build_interpolator(A, x, y, z, 1, bc)
+    A = (i + j + k).astype(np.float32)   # a scalar grid: carried as component 0
+    return tp.build_interpolator(A, x, y, z, order, bc)
 
 
 def test_interpolation_kats(tp, orc):
@@ -416,6 +415,91 @@ def test_interpolation_kats(tp, orc):
     assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 9.5, rel_tol=1e-12)
     f = _scalar_grid(tp, tp.ClampExtrap())
     assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 12.0, rel_tol=1e-12)
+
+
+def test_interpolation_order0_and_cubic_kats(tp, orc):
+    # test_utility.jl:103-120: constant (order 0) and cardinal cubic (order 3)
+    f = _scalar_grid(tp, tp.FillExtrap(), order=0)
+    assert math.isclose(orc.field_eval(f, [-10.0, -10.0, -10.0])[0, 0], 3.0, rel_tol=1e-12)
+    f = _scalar_grid(tp, tp.FillExtrap(), order=3)
+    assert math.isclose(orc.field_eval(f, [9.0, 0.0, 0.0])[0, 0], 11.85, rel_tol=1e-12)
+    f = _scalar_grid(tp, tp.PeriodicBC("exclusive"), order=3)
+    assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 9.25, rel_tol=1e-12)
+    f = _scalar_grid(tp, tp.ClampExtrap(), order=3)
+    assert math.isclose(orc.field_eval(f, [20.0, 0.0, 0.0])[0, 0], 12.0, rel_tol=1e-12)
+    # the cubic passes through the nodes and reproduces quadratics inside
+    x = np.linspace(0.0, 1.0, 9)
+    A = np.zeros((3, 9, 9, 9))
+    A[0] = (x ** 2)[:, None, None] + 0 * x[None, :, None] + 0 * x[None, None, :]
+    g = tp.build_interpolator(A, x, x, x, 3)
+    assert math.isclose(orc.field_eval(g, [0.375, 0.5, 0.5])[0, 0], 0.375 ** 2, rel_tol=1e-12)
+    assert math.isclose(orc.field_eval(g, [0.4, 0.5, 0.5])[0, 0], 0.16, rel_tol=1e-12)
+    assert math.isclose(orc.field_eval(g, [0.05, 0.5, 0.5])[0, 0], 0.0025, rel_tol=1e-12)
+
+
+def _spherical_br(tp, r, order):
+    th = np.linspace(0, math.pi, 11)
+    ph = np.linspace(0, 2 * math.pi, 11)
+    B = np.zeros((3, len(r), 11, 11))
+    B[0] = 1.0
+    return tp.build_interpolator(tp.StructuredGrid, B, r, th, ph, order)
+
+
+def test_spherical_interpolation_kats(tp, orc):
+    # test_utility.jl:123-166: B_r = 1 gives the unit radial vector
+    for r in (np.linspace(0.1, 10, 11), np.geomspace(1.0, 10.0, 11)):
+        for order in (0, 1, 3) if r[0] == 0.1 else (1,):
+            B = _spherical_br(tp, r, order)
+            v = orc.field_eval(B, [1.0, 1.0, 1.0])[0]
+            assert np.allclose(v, [0.57735] * 3, atol=1e-5)
+        A = np.ones((len(r), 11, 11))
+        f = tp.build_interpolator(tp.StructuredGrid, A, r, np.linspace(0, math.pi, 11),
+                                  np.linspace(0, 2 * math.pi, 11))
+        assert orc.field_eval(f, [1.0, 1.0, 1.0])[0, 0] == 1.0
+        assert np.isnan(orc.field_eval(f, [0.0, 0.0, 0.0])[0, 0])
+
+
+def test_rectilinear_interpolation_kats(tp, orc):
+    # test_utility.jl:259-314 (CartesianNonUniform)
+    x = np.linspace(0.0, 10.0, 11)
+    B = np.zeros((3, 11, 11, 11))
+    B[0] = 1.0
+    f = tp.build_interpolator(tp.RectilinearGrid, B, x, x, x)
+    assert np.allclose(orc.field_eval(f, [5.0, 5.0, 5.0])[0], [1.0, 0.0, 0.0])
+    i, j, k = np.meshgrid(x, x, x, indexing="ij")
+    f = tp.build_interpolator(tp.RectilinearGrid, i + j + k, x, x, x)
+    assert math.isclose(orc.field_eval(f, [5.0, 5.0, 5.0])[0, 0], 15.0, rel_tol=1e-12)
+    assert math.isclose(orc.field_eval(f, [5.5, 5.5, 5.5])[0, 0], 16.5, rel_tol=1e-12)
+    xn = np.array([0.0, 1.0, 4.0, 9.0])
+    i, j, k = np.meshgrid(xn, xn, xn, indexing="ij")
+    f = tp.build_interpolator(tp.RectilinearGrid, np.sqrt(i) + np.sqrt(j) + np.sqrt(k), xn, xn, xn)
+    assert math.isclose(orc.field_eval(f, [4.0, 4.0, 4.0])[0, 0], 6.0, rel_tol=1e-12)
+    assert math.isclose(orc.field_eval(f, [1.0, 4.0, 9.0])[0, 0], 6.0, rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("dims", [3, 2, 1])
+def test_grid_jacobians_match_finite_differences(tp, orc, dims):
+    # test_derivatives.jl:6-50 (1-D / 2-D / 3-D), plus the cubic and spherical grids
+    rng = np.random.default_rng(3)
+    x = np.linspace(0.0, 1.0, 5)
+    shape = (3,) + (5,) * dims
+    A = rng.normal(size=shape)
+    fields = [tp.build_interpolator(tp.CartesianGrid, A, *([x] * dims), order) for order in (1, 3)]
+    if dims == 3:
+        r, th, ph = np.linspace(0.5, 2.0, 7), np.linspace(0, math.pi, 9), np.linspace(0, 2 * math.pi, 13)
+        fields += [tp.build_interpolator(tp.StructuredGrid, rng.normal(size=(3, 7, 9, 13)), r, th, ph, o)
+                   for o in (1, 3)]
+    p = np.array([0.43, 0.61, 0.27])
+    for f in fields:
+        _, J = orc.field_eval(f, p, jacobian=True)
+        h = 1e-6
+        for c in range(3):
+            e = np.zeros(3)
+            e[c] = h
+            fd = (orc.field_eval(f, p + e) - orc.field_eval(f, p - e))[0] / (2 * h)
+            assert np.allclose(J[0][:, c], fd, rtol=1e-6, atol=1e-8)
+        if dims < 3:   # unused coordinates have zero derivative
+            assert np.all(J[0][:, dims:] == 0.0)
 
 
 def test_dipole_jacobian_matches_finite_differences(tp, orc):
