@@ -71,6 +71,9 @@ enum {
  *            linearly time-varying fields of the reference tests)
  *   DIPOLE   F(x) = coef * (3 (m.rhat) rhat - m) / |x - center|^3
  *            (the Magnetostatics.Dipole field of test/test_gc.jl:180)
+ *   QUADRATIC  F_i(x,t) = value_i + sum_j jac_ij x_j + sum_jk quad_ijk x_j x_k
+ *            + rate_i t (the quadratic test fields of the reference, e.g.
+ *            the magnetic bottle of test/test_hybrid.jl:61-68)
  *   GRID     interpolation of a (3, nx, ny, nz) column-major array:
  *            build_interpolator(gridtype, A, grids..., order, bc)
  *            (src/utility/interpolation.jl:119-311).  The default (a zeroed
@@ -82,7 +85,8 @@ enum {
     TP_FIELD_UNIFORM = 1,
     TP_FIELD_AFFINE = 2,
     TP_FIELD_DIPOLE = 3,
-    TP_FIELD_GRID = 4
+    TP_FIELD_GRID = 4,
+    TP_FIELD_QUADRATIC = 5
 };
 
 /* grid boundary handling (FastInterpolations FillExtrap(NaN), ClampExtrap(),
@@ -153,6 +157,7 @@ typedef struct tp_field_desc {
                             uniform axis origin + k * spacing.  Non-uniform
                             axes take LINEAR or CONSTANT order and FILL_NAN
                             or CLAMP boundaries.                            */
+    double quad[27];     /* QUADRATIC: quad_ijk at [9 i + 3 j + k]          */
 } tp_field_desc;
 
 /* ---- termination (the reference's `isoutside(u, p, t)` callback) --------
@@ -262,6 +267,45 @@ void tp_field_destroy(tp_field* field);
  * addition for optimisation loops over gridded fields (the reference rebuilds
  * the interpolator).                                                        */
 int tp_field_update(tp_field* field, const void* data);
+
+/* ---- adaptive hybrid guiding-centre / full-orbit solve --------------------
+ * Replaces solve(::TraceHybridProblem, ::AdaptiveHybrid, ensemblealg)
+ * (src/hybrid.jl:123-474): per particle, RK45 guiding-centre steps while the
+ * adiabaticity parameter stays below threshold_gc_to_fo, Boris full-orbit
+ * steps (dt = 2 pi safety_fo / (|q2m| |B|) clamped to [dtmin, dtmax]) until
+ * it drops below threshold_fo_to_gc, checked every check_interval steps.
+ * Saves are full-orbit states (x, v), 6 values.  The adiabaticity value and
+ * mode of every check are returned in a second result of width 2 (value,
+ * mode: 0 = GC, 1 = FO) when `adia` is not NULL.  Return codes follow the
+ * reference: MaxIters when maxiters steps were taken, else Success; a step
+ * whose error norm is NaN ends the trajectory with Terminated (the reference
+ * would retry it forever).                                                  */
+enum {
+    TP_ADIA_CURVATURE = 0, /* epsilon = rho / R_c                            */
+    TP_ADIA_GRADB = 1,     /* epsilon = rho / L_B, L_B = |B| / |grad|B||     */
+    TP_ADIA_BOTH = 2,      /* max of the two                                 */
+    TP_ADIA_JACOBIAN = 3   /* epsilon = rho ||JB||_F / |B|                   */
+};
+
+typedef struct tp_hybrid_desc {
+    double t0, t1;
+    double q2m, m;
+    double threshold_gc_to_fo, threshold_fo_to_gc;
+    double dtmin, dtmax, safety_fo;
+    double abstol, reltol;
+    int64_t maxiters;
+    int64_t check_interval;
+    int64_t savestepinterval;
+    int32_t adiabaticity;     /* TP_ADIA_*                                     */
+    int32_t save_adiabaticity;
+    int32_t save_start, save_end, save_everystep;
+    int32_t block;            /* 0 = automatic                                 */
+    tp_term_desc term;
+    double budget_s;          /* device wall-clock budget, 0 = default 600 s   */
+} tp_hybrid_desc;
+
+int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* desc, const tp_field* E, const tp_field* B,
+                  const double* u0, int64_t n, tp_result** out, tp_result** adia);
 
 /* ---- fields and work rates at given states ------------------------------
  * get_fields / get_work (src/boris/boris.jl:599-640): E, B and the work rates

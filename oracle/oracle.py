@@ -62,6 +62,16 @@ def lib() -> C.CDLL:
         L.orc_gc_run.argtypes = [C.POINTER(from_abi.GCDesc), C.POINTER(from_abi.FieldDesc),
                                  C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), C.POINTER(FieldCB),
                                  C.POINTER(TermCB), P, P, P, P, P, P, C.c_int64, C.c_int, C.c_int64, P, P, P, P, P]
+        L.orc_hybrid_run.restype = C.c_int
+        L.orc_hybrid_run.argtypes = [C.POINTER(from_abi.HybridDesc), C.POINTER(from_abi.FieldDesc),
+                                     C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), C.POINTER(FieldCB),
+                                     C.POINTER(TermCB), P, C.c_int64, C.c_int, C.c_int64, C.c_int64, P, P, P, P,
+                                     P, P, P, P]
+        L.orc_trig.restype = C.c_int
+        L.orc_trig.argtypes = [P, P, C.c_int64, P, P, P]
+        L.orc_gc_roundtrip.restype = C.c_int
+        L.orc_gc_roundtrip.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(from_abi.FieldDesc), P,
+                                       C.c_int64, C.c_double, C.c_double, C.c_double, P]
         L.orc_gc_prepare.restype = C.c_int
         L.orc_gc_prepare.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(from_abi.FieldDesc),
                                      C.POINTER(FieldCB), C.POINTER(FieldCB), P, C.c_int64, C.c_double,
@@ -288,6 +298,74 @@ def gc_run(desc, E, B, y0: np.ndarray, q_i=None, q2m_i=None, mu_i=None, nthreads
         t, u = _pack(t_sm, u_sm, nsaved, W, n)
         return OracleResult(nsaved, rc, nst, t, u)
     raise RuntimeError("oracle: output sizing failed")
+
+
+def hybrid_run(desc, E, B, u0: np.ndarray, nthreads: int = 0, isoutside: Optional[Callable] = None):
+    """Adaptive hybrid ensemble on the CPU -> (OracleResult, adiabaticity OracleResult or None);
+    the adiabaticity rows are (value, mode) with mode 0 = GC, 1 = FO."""
+    L = lib()
+    u0 = np.ascontiguousarray(u0, dtype=np.float64)
+    n = u0.shape[0]
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    tcb = term_callback(isoutside) if isoutside is not None else None
+    if nthreads <= 0 and (Ecb is not None or Bcb is not None or tcb is not None):
+        nthreads = 1
+    want = bool(desc.save_adiabaticity)
+    nslots, aslots = 64, 64
+    for _ in range(3):
+        t_sm = np.empty((nslots, n))
+        u_sm = np.empty((nslots, 6, n))
+        nsaved = np.zeros(n, dtype=np.int32)
+        rc = np.empty(n, dtype=np.int8)
+        nst = np.empty(n, dtype=np.int64)
+        at = np.empty((aslots, n)) if want else None
+        av = np.empty((aslots, 2, n)) if want else None
+        na = np.zeros(n, dtype=np.int32) if want else None
+        code = L.orc_hybrid_run(C.byref(desc), C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None,
+                                C.byref(Ecb) if Ecb else None, C.byref(Bcb) if Bcb else None,
+                                C.byref(tcb) if tcb else None, _ptr(u0), n, int(nthreads), nslots, aslots,
+                                _ptr(t_sm), _ptr(u_sm), _ptr(nsaved), _ptr(rc), _ptr(nst), _ptr(at), _ptr(av),
+                                _ptr(na))
+        if code == -6:
+            nslots = max(nslots, int(nsaved.max()))
+            if want:
+                aslots = max(aslots, int(na.max()))
+            continue
+        if code == -1:
+            raise ValueError("oracle: ArgumentError")
+        if code != 0:
+            raise RuntimeError(f"oracle status {code}")
+        t, u = _pack(t_sm, u_sm, nsaved, 6, n)
+        res = OracleResult(nsaved, rc, nst, t, u)
+        ares = None
+        if want:
+            ta, ua = _pack(at, av, na, 2, n)
+            ares = OracleResult(na, rc, nst, ta, ua)
+        return res, ares
+    raise RuntimeError("oracle: output sizing failed")
+
+
+def trig(x: np.ndarray, y: np.ndarray):
+    """(sin x, cos x, atan2(y, x)) of the hybrid's portable trigonometry."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    s, c, a = np.empty_like(x), np.empty_like(x), np.empty_like(x)
+    lib().orc_trig(_ptr(x), _ptr(y), x.size, _ptr(s), _ptr(c), _ptr(a))
+    return s, c, a
+
+
+def gc_roundtrip(E, B, xv: np.ndarray, q: float, m: float, t: float = 0.0) -> np.ndarray:
+    """Full orbit -> guiding centre -> full orbit, (n, 6) -> (n, 6)."""
+    xv = np.ascontiguousarray(np.atleast_2d(xv), dtype=np.float64)
+    Ed, _ = _field_arg(E)
+    Bd, _ = _field_arg(B)
+    out = np.empty_like(xv)
+    code = lib().orc_gc_roundtrip(C.byref(Ed), C.byref(Bd), _ptr(xv), xv.shape[0], float(q), float(m), float(t),
+                                  _ptr(out))
+    if code != 0:
+        raise RuntimeError(f"oracle status {code}")
+    return out
 
 
 def gc_prepare(E, B, xv: np.ndarray, q: float, m: float, t: float = 0.0):

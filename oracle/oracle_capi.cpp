@@ -86,6 +86,16 @@ std::unique_ptr<Field> make_field(const tp_field_desc* d, const orc_field_cb* cb
             f->rate = {d->rate[0], d->rate[1], d->rate[2]};
             return std::unique_ptr<Field>(f);
         }
+        case TP_FIELD_QUADRATIC: {
+            auto* f = new QuadraticField();
+            for (int k = 0; k < 3; ++k) {
+                f->v[k] = d->value[k];
+                f->rate[k] = d->rate[k];
+            }
+            std::memcpy(f->J, d->jac, sizeof(f->J));
+            std::memcpy(f->Q, d->quad, sizeof(f->Q));
+            return std::unique_ptr<Field>(f);
+        }
         case TP_FIELD_DIPOLE: {
             auto* f = new DipoleField();
             f->m = {d->moment[0], d->moment[1], d->moment[2]};
@@ -374,6 +384,87 @@ int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_
                                 d->step_cap, term, ui, tr);
         }
         if (!store(tr, i, n, W, nslots, t_out, u_out, nsaved, retcode, nsteps)) overflow |= 1;
+    }
+    return overflow ? TP_E_OVERFLOW : TP_OK;
+}
+
+// The hybrid's portable gyrophase trigonometry, for accuracy tests.
+int orc_trig(const double* x, const double* y, int64_t n, double* s, double* c, double* a) {
+    for (int64_t i = 0; i < n; ++i) {
+        psincos(x[i], s[i], c[i]);
+        a[i] = patan2(y[i], x[i]);
+    }
+    return TP_OK;
+}
+
+// Full orbit -> guiding centre -> full orbit (_get_gc_parameters then
+// _gc_to_full, src/gc/gc.jl:13-39,128-154) for n states.
+int orc_gc_roundtrip(const tp_field_desc* Ed, const tp_field_desc* Bd, const double* xv, int64_t n, double q,
+                     double m, double t, double* out) {
+    std::unique_ptr<Field> E = make_field(Ed, nullptr), B = make_field(Bd, nullptr);
+    if (!E || !B) return TP_E_ARG;
+    for (int64_t i = 0; i < n; ++i) {
+        const double* s = xv + 6 * i;
+        V3d X, x, v;
+        double vpar, mu, phase;
+        gc_params_phase({s[0], s[1], s[2]}, {s[3], s[4], s[5]}, *E, *B, q, m, t, X, vpar, mu, phase);
+        GCState g{{X.x, X.y, X.z, vpar}};
+        gc_to_full(g, *E, *B, q, m, mu, t, phase, x, v);
+        double o[6] = {x.x, x.y, x.z, v.x, v.y, v.z};
+        for (int c = 0; c < 6; ++c) out[6 * i + c] = o[c];
+    }
+    return TP_OK;
+}
+
+// Adaptive hybrid GC / full-orbit ensemble (src/hybrid.jl:234-474); the
+// adiabaticity checks go to at_out / av_out when both are given.
+int orc_hybrid_run(const tp_hybrid_desc* d, const tp_field_desc* Ed, const tp_field_desc* Bd,
+                   const orc_field_cb* Ecb, const orc_field_cb* Bcb, const orc_term_cb* tcb, const double* u0,
+                   int64_t n, int nthreads, int64_t nslots, int64_t aslots, double* t_out, double* u_out,
+                   int32_t* nsaved, int8_t* retcode, int64_t* nsteps, double* at_out, double* av_out,
+                   int32_t* nadia) {
+    std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
+    if (!E || !B) return TP_E_ARG;
+    if (d->check_interval <= 0 || !(d->threshold_gc_to_fo >= d->threshold_fo_to_gc)) return TP_E_ARG;
+    if (d->adiabaticity < TP_ADIA_CURVATURE || d->adiabaticity > TP_ADIA_JACOBIAN) return TP_E_ARG;
+    if (d->savestepinterval < 1) return TP_E_ARG;
+    Term term = make_term(&d->term, tcb);
+    Params p{d->q2m, d->m, E.get(), B.get()};
+    HybridOpts o;
+    o.t0 = d->t0;
+    o.t1 = d->t1;
+    o.th_gc_fo = d->threshold_gc_to_fo;
+    o.th_fo_gc = d->threshold_fo_to_gc;
+    o.dtmin = d->dtmin;
+    o.dtmax = d->dtmax;
+    o.safety_fo = d->safety_fo;
+    o.abstol = d->abstol;
+    o.reltol = d->reltol;
+    o.maxiters = d->maxiters;
+    o.check = d->check_interval;
+    o.ssi = d->savestepinterval;
+    o.adia_mode = d->adiabaticity;
+    o.save_start = d->save_start != 0;
+    o.save_end = d->save_end != 0;
+    o.save_everystep = d->save_everystep != 0;
+    const bool want_adia = d->save_adiabaticity && at_out && av_out && nadia;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    int overflow = 0;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads) reduction(| : overflow)
+    for (int64_t i = 0; i < n; ++i) {
+        HybridTraj h;
+        hybrid_single(p, o, term, u0 + 6 * i, want_adia, h);
+        if (!store(h.traj, i, n, 6, nslots, t_out, u_out, nsaved, retcode, nsteps)) overflow |= 1;
+        if (want_adia) {
+            int64_t na = (int64_t)h.at.size();
+            nadia[i] = (int32_t)na;
+            for (int64_t k = 0; k < std::min(na, aslots); ++k) {
+                at_out[k * n + i] = h.at[k];
+                av_out[(k * 2) * n + i] = h.av[2 * k];
+                av_out[(k * 2 + 1) * n + i] = h.av[2 * k + 1];
+            }
+            if (na > aslots) overflow |= 1;
+        }
     }
     return overflow ? TP_E_OVERFLOW : TP_OK;
 }

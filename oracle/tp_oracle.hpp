@@ -121,6 +121,40 @@ struct AffineField : Field {
     V3d dtime(V3d, double) const override { return rate; }
 };
 
+// Quadratic field F_i = value_i + sum_j J_ij x_j + sum_jk Q_ijk x_j x_k + rate_i t,
+// evaluated as ((v_i + ((J_i0 x + J_i1 y) + J_i2 z)) + q_i) + rate_i t with
+// q_i = (x (Q_i0.x) + y (Q_i1.x)) + z (Q_i2.x); the reference's quadratic
+// test fields (the magnetic bottle of test/test_hybrid.jl:61-68).
+struct QuadraticField : Field {
+    double v[3], J[9], Q[27], rate[3];
+    V3d eval(V3d r, double t) const override {
+        double x = r.x, y = r.y, z = r.z, o[3];
+        for (int i = 0; i < 3; ++i) {
+            const double* Ji = J + 3 * i;
+            const double* Qi = Q + 9 * i;
+            double lin = (Ji[0] * x + Ji[1] * y) + Ji[2] * z;
+            double qx = (Qi[0] * x + Qi[1] * y) + Qi[2] * z;
+            double qy = (Qi[3] * x + Qi[4] * y) + Qi[5] * z;
+            double qz = (Qi[6] * x + Qi[7] * y) + Qi[8] * z;
+            double q = (x * qx + y * qy) + z * qz;
+            o[i] = ((v[i] + lin) + q) + rate[i] * t;
+        }
+        return {o[0], o[1], o[2]};
+    }
+    void jac(V3d r, double t, V3d& F, M3& Jm) const override {
+        F = eval(r, t);
+        double x[3] = {r.x, r.y, r.z};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const double* Qi = Q + 9 * i;
+                double acc = J[3 * i + j];
+                for (int k = 0; k < 3; ++k) acc = acc + (Qi[3 * j + k] + Qi[3 * k + j]) * x[k];
+                Jm.a[3 * i + j] = acc;
+            }
+    }
+    V3d dtime(V3d, double) const override { return {rate[0], rate[1], rate[2]}; }
+};
+
 // Point dipole B(x) = coef (3 (m.rhat) rhat - m) / d^3, d = |x - c|, evaluated
 // in the order of the textbook expression coef * (3*(m.rhat)*rhat - m) / d^3.
 struct DipoleField : Field {
@@ -1265,6 +1299,343 @@ inline void gc_parameters(const double* xv, const Field& E, const Field& B, doub
     X_out[2] = X.z;
     *vpar_out = vpar;
     *mu_out = mu;
+}
+
+
+// ---------------------------------------------------------------- hybrid
+// _hybrid_adaptive!, src/hybrid.jl:234-474, one trajectory.  Helpers:
+// _get_gc_parameters with the gyrophase (src/gc/gc.jl:13-39), _gc_to_full
+// (:128-154), adiabaticity_components (src/utility/utility.jl:554-577),
+// _fo_dt (hybrid.jl:226-232), mod2pi with 2 pi carried as two doubles.
+struct HybridOpts {
+    double t0, t1, th_gc_fo, th_fo_gc, dtmin, dtmax, safety_fo, abstol, reltol;
+    int64_t maxiters, check, ssi;
+    int adia_mode;
+    bool save_start, save_end, save_everystep;
+};
+
+struct HybridTraj {
+    Traj traj;
+    std::vector<double> at, av;  // adiabaticity checks: time; (value, mode) pairs
+};
+
+// Portable sin / cos / atan2 for the gyrophase, built from +, -, *, / and
+// sqrt only, so that the kernel and its CPU restatement agree bit for bit
+// (the hybrid's step and mode decisions amplify last-bit differences):
+//   sincos  Cody-Waite reduction by pi/2 (pi/2 split in three parts), then the
+//           Taylor series of sin and cos on [-pi/4, pi/4] to degree 21 / 22
+//   atan    two half-angle reductions tan(a/2) = t / (1 + std::sqrt(1 + t^2)) to
+//           |t| <= tan(pi/16), then the Taylor series to degree 29
+inline void psincos(double x, double& s, double& c) {
+    const double P1 = 1.570796325802803, P2 = 9.920935791635221e-10, P3 = 5.170182981794105e-19;
+    const double kf = std::nearbyint(x * 0.6366197723675814);
+    const double r = ((x - kf * P1) - kf * P2) - kf * P3;
+    const double r2 = r * r;
+    double ps = -1.0 / 51090942171709440000.0;
+    ps = 1.0 / 121645100408832000.0 + r2 * ps;
+    ps = -1.0 / 355687428096000.0 + r2 * ps;
+    ps = 1.0 / 1307674368000.0 + r2 * ps;
+    ps = -1.0 / 6227020800.0 + r2 * ps;
+    ps = 1.0 / 39916800.0 + r2 * ps;
+    ps = -1.0 / 362880.0 + r2 * ps;
+    ps = 1.0 / 5040.0 + r2 * ps;
+    ps = -1.0 / 120.0 + r2 * ps;
+    ps = 1.0 / 6.0 + r2 * ps;
+    const double sr = r - (r * r2) * ps;
+    double pc = 1.0 / 1124000727777607680000.0;
+    pc = -1.0 / 2432902008176640000.0 + r2 * pc;
+    pc = 1.0 / 6402373705728000.0 + r2 * pc;
+    pc = -1.0 / 20922789888000.0 + r2 * pc;
+    pc = 1.0 / 87178291200.0 + r2 * pc;
+    pc = -1.0 / 479001600.0 + r2 * pc;
+    pc = 1.0 / 3628800.0 + r2 * pc;
+    pc = -1.0 / 40320.0 + r2 * pc;
+    pc = 1.0 / 720.0 + r2 * pc;
+    pc = -1.0 / 24.0 + r2 * pc;
+    pc = 0.5 + r2 * pc;
+    const double cr = 1.0 - r2 * pc;
+    const int q = (int)((long long)kf & 3);
+    if (q == 0) {
+        s = sr;
+        c = cr;
+    } else if (q == 1) {
+        s = cr;
+        c = -sr;
+    } else if (q == 2) {
+        s = -sr;
+        c = -cr;
+    } else {
+        s = -cr;
+        c = sr;
+    }
+}
+
+inline double patan01(double t) {
+    double u = t / (1.0 + std::sqrt(1.0 + t * t));
+    u = u / (1.0 + std::sqrt(1.0 + u * u));
+    const double u2 = u * u;
+    double p = -1.0 / 29.0;
+    p = 1.0 / 27.0 + u2 * p;
+    p = -1.0 / 25.0 + u2 * p;
+    p = 1.0 / 23.0 + u2 * p;
+    p = -1.0 / 21.0 + u2 * p;
+    p = 1.0 / 19.0 + u2 * p;
+    p = -1.0 / 17.0 + u2 * p;
+    p = 1.0 / 15.0 + u2 * p;
+    p = -1.0 / 13.0 + u2 * p;
+    p = 1.0 / 11.0 + u2 * p;
+    p = -1.0 / 9.0 + u2 * p;
+    p = 1.0 / 7.0 + u2 * p;
+    p = -1.0 / 5.0 + u2 * p;
+    p = 1.0 / 3.0 + u2 * p;
+    return 4.0 * (u - (u * u2) * p);
+}
+
+inline double patan2(double y, double x) {
+    if (x == 0.0 && y == 0.0) return 0.0;
+    const double ax = std::fabs(x), ay = std::fabs(y);
+    double a = (ay <= ax) ? patan01(ay / ax) : 1.5707963267948966 - patan01(ax / ay);
+    if (x < 0.0) a = 3.141592653589793 - a;
+    return (y < 0.0) ? -a : a;
+}
+
+inline double mod2pi_d(double x) {
+    const double hi = 6.283185307179586, lo = 2.4492935982947064e-16;
+    double k = std::floor(x / hi);
+    double r = std::fma(-k, hi, x);
+    r = std::fma(-k, lo, r);
+    if (r < 0.0) r = (r + hi) + lo;
+    else if (r >= hi) r = (r - hi) - lo;
+    return r;
+}
+
+inline void gc_params_phase(V3d x, V3d v, const Field& E, const Field& B, double q, double m, double t, V3d& X,
+                            double& vpar, double& mu, double& phase) {
+    V3d bp = B.eval(x, t);
+    double Bmp = norm(bp);
+    V3d bhp = bp / Bmp;
+    V3d rho = cross(bhp, v) / (q / m * Bmp);
+    X = x - rho;
+    V3d b = B.eval(X, t);
+    double Bmag = norm(b);
+    V3d bh = b / Bmag;
+    vpar = dot(bh, v);
+    V3d vperp = v - vpar * bh;
+    V3d e = E.eval(X, t);
+    V3d vE = cross(e, bh) / Bmag;
+    V3d w = vperp - vE;
+    mu = m * dot(w, w) / (2.0 * Bmag);
+    V3d e1, e2;
+    get_perp_vector(bh, e1, e2);
+    phase = patan2(dot(w, e2), dot(w, e1));
+}
+
+inline void gc_to_full(const GCState& s, const Field& Ef, const Field& Bf, double q, double m, double mu,
+                       double t, double phase, V3d& x, V3d& v) {
+    V3d R{s.y[0], s.y[1], s.y[2]};
+    V3d E = Ef.eval(R, t), B = Bf.eval(R, t);
+    double Bmag = norm(B);
+    V3d bh = B / Bmag;
+    V3d vE = cross(E, bh) / Bmag;
+    double w = std::sqrt(2.0 * mu * Bmag / m);
+    V3d e1, e2;
+    get_perp_vector(bh, e1, e2);
+    double sp, cp;
+    psincos(phase, sp, cp);
+    V3d vperp = w * (cp * e1 + sp * e2) + vE;
+    v = s.y[3] * bh + vperp;
+    double Om = q * Bmag / m;
+    x = R + cross(bh, vperp) / Om;
+}
+
+inline void adiabaticity_components(const Field& Bf, V3d x, double q, double m, double mu, double t, double c[3]) {
+    V3d B;
+    M3 J;
+    Bf.jac(x, t, B, J);
+    double Bmag = norm(B);
+    const double inf = std::numeric_limits<double>::infinity();
+    if (Bmag == 0.0) {
+        c[0] = c[1] = c[2] = inf;
+        return;
+    }
+    double rho = std::sqrt(2.0 * mu * m / Bmag) / std::fabs(q);
+    V3d bh = B / Bmag;
+    V3d gB{(J(0, 0) * bh.x + J(1, 0) * bh.y) + J(2, 0) * bh.z, (J(0, 1) * bh.x + J(1, 1) * bh.y) + J(2, 1) * bh.z,
+           (J(0, 2) * bh.x + J(1, 2) * bh.y) + J(2, 2) * bh.z};
+    double gBm = norm(gB);
+    double LB = gBm == 0.0 ? inf : Bmag / gBm;
+    c[1] = rho / LB;
+    V3d Jb{(J(0, 0) * bh.x + J(0, 1) * bh.y) + J(0, 2) * bh.z, (J(1, 0) * bh.x + J(1, 1) * bh.y) + J(1, 2) * bh.z,
+           (J(2, 0) * bh.x + J(2, 1) * bh.y) + J(2, 2) * bh.z};
+    V3d kap = (Jb + bh * (-dot(gB, bh))) / Bmag;
+    c[0] = rho * norm(kap);
+    double fro = 0.0;  // sum(abs2, JB), column-major
+    bool first = true;
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            double a = J(i, j) * J(i, j);
+            fro = first ? a : fro + a;
+            first = false;
+        }
+    c[2] = rho * std::sqrt(fro) / Bmag;
+}
+
+inline double adia_select(const double c[3], int mode) {
+    if (mode == TP_ADIA_CURVATURE) return c[0];
+    if (mode == TP_ADIA_GRADB) return c[1];
+    if (mode == TP_ADIA_JACOBIAN) return c[2];
+    if (std::isnan(c[0]) || std::isnan(c[1])) return c[0] + c[1];
+    return c[0] < c[1] ? c[1] : c[0];
+}
+
+inline void hybrid_single(const Params& p, const HybridOpts& o, const Term& term, const double* u0, bool save_adia,
+                          HybridTraj& out) {
+    const double two_pi = 6.283185307179586;
+    const Field& Ef = *p.E;
+    const Field& Bf = *p.B;
+    const double q = p.q2m * p.m;
+    const bool is_td = Ef.dtime({0, 0, 0}, 0.0).x != 0.0 || Ef.dtime({0, 0, 0}, 0.0).y != 0.0 ||
+                       Ef.dtime({0, 0, 0}, 0.0).z != 0.0 || Bf.dtime({0, 0, 0}, 0.0).x != 0.0 ||
+                       Bf.dtime({0, 0, 0}, 0.0).y != 0.0 || Bf.dtime({0, 0, 0}, 0.0).z != 0.0;
+    BorisUpdater upd;
+    auto fo_dt = [&](V3d r, double t) {
+        double Bmag = norm(Bf.eval(r, t));
+        double om = std::fabs(p.q2m) * Bmag;
+        double dt = two_pi * o.safety_fo / om;
+        return dt > o.dtmax ? o.dtmax : (dt < o.dtmin ? o.dtmin : dt);
+    };
+    auto push = [&](V3d x, V3d v, double t) {
+        out.traj.t.push_back(t);
+        double s[6] = {x.x, x.y, x.z, v.x, v.y, v.z};
+        out.traj.u.insert(out.traj.u.end(), s, s + 6);
+    };
+    auto push_adia = [&](double t, double eps, bool gc) {
+        if (!save_adia) return;
+        out.at.push_back(t);
+        out.av.push_back(eps);
+        out.av.push_back(gc ? 0.0 : 1.0);
+    };
+    V3d r{u0[0], u0[1], u0[2]}, v{u0[3], u0[4], u0[5]};
+    double t = o.t0;
+    GCParams pg{q, p.q2m, 0.0, p.E, p.B};
+    V3d X;
+    double vpar, mu, phase;
+    gc_params_phase(r, v, Ef, Bf, q, p.m, t, X, vpar, mu, phase);
+    double c[3];
+    adiabaticity_components(Bf, r, q, p.m, mu, t, c);
+    double eps = adia_select(c, o.adia_mode);
+    bool gc = eps < o.th_gc_fo;
+    GCState xg{{0, 0, 0, 0}};
+    double dt;
+    if (gc) {
+        xg = {{X.x, X.y, X.z, vpar}};
+        pg.mu = mu;
+        double Bmag = norm(Bf.eval(X, t));
+        dt = 0.5 * two_pi / std::fabs(p.q2m * Bmag);
+    } else {
+        dt = fo_dt(r, t);
+        v = upd(v, r, -0.5 * dt, t, p);
+    }
+    push_adia(t, eps, gc);
+    if (o.save_start) push({u0[0], u0[1], u0[2]}, {u0[3], u0[4], u0[5]}, t);
+    int64_t steps = 0, it = 1;
+    int ret = TP_RET_SUCCESS;
+    while (t < o.t1 && steps < o.maxiters) {
+        if (gc) {
+            if (it % o.check == 0) {
+                adiabaticity_components(Bf, {xg.y[0], xg.y[1], xg.y[2]}, q, p.m, mu, t, c);
+                eps = adia_select(c, o.adia_mode);
+                push_adia(t, eps, true);
+                if (eps >= o.th_gc_fo) {
+                    gc = false;
+                    gc_to_full(xg, Ef, Bf, q, p.m, mu, t, phase, r, v);
+                    dt = fo_dt(r, t);
+                    v = upd(v, r, -0.5 * dt, t, p);
+                    continue;
+                }
+            }
+            if (t + dt > o.t1) dt = o.t1 - t;
+            GCState dx, Er;
+            update_dp5(xg, pg, dt, t, dx, Er);
+            GCState yn = gadd(xg, dx);
+            double sum_sq = 0.0;
+            for (int k = 0; k < 4; ++k) {
+                double ax = std::fabs(xg.y[k]), ay = std::fabs(yn.y[k]);
+                double sc = o.abstol + ((ax < ay) ? ay : ax) * o.reltol;
+                double qk = Er.y[k] / sc;
+                sum_sq = sum_sq + qk * qk;
+            }
+            double er = 0.5 * std::sqrt(sum_sq);
+            if (std::isnan(er)) {
+                ret = TP_RET_TERMINATED;
+                break;
+            }
+            if (er <= 1.0) {
+                if (term.any() && term.outside(yn.y, 4, t + dt)) break;
+                t += dt;
+                xg = yn;
+                double Bs = norm(Bf.eval({xg.y[0], xg.y[1], xg.y[2]}, t));
+                phase = mod2pi_d(phase - dt * (p.q2m * Bs));
+                if (o.save_everystep && it % o.ssi == 0) {
+                    V3d xs, vs;
+                    gc_to_full(xg, Ef, Bf, q, p.m, mu, t, phase, xs, vs);
+                    push(xs, vs, t);
+                }
+                steps += 1;
+                it += 1;
+            }
+            double scale = (er == 0.0) ? 5.0 : 0.9 * pow02_rn(1.0 / er);
+            scale = (scale < 5.0) ? scale : 5.0;
+            scale = (0.2 < scale) ? scale : 0.2;
+            dt *= scale;
+            if (dt < 1.0e-14) break;
+        } else {
+            if (it % o.check == 0) {
+                const double t_sync = is_td ? t : 0.0;
+                V3d vs = upd(v, r, 0.5 * dt, t_sync, p);
+                V3d Xf;
+                double vparf, muf, phasef;
+                gc_params_phase(r, vs, Ef, Bf, q, p.m, t, Xf, vparf, muf, phasef);
+                adiabaticity_components(Bf, Xf, q, p.m, muf, t, c);
+                eps = adia_select(c, o.adia_mode);
+                push_adia(t, eps, false);
+                if (eps < o.th_fo_gc) {
+                    gc = true;
+                    xg = {{Xf.x, Xf.y, Xf.z, vparf}};
+                    pg.mu = muf;
+                    mu = muf;
+                    phase = phasef;
+                    double Bmag = norm(Bf.eval(r, t));
+                    dt = 0.5 * two_pi / std::fabs(p.q2m * Bmag);
+                    continue;
+                }
+            }
+            if (t + dt > o.t1) dt = o.t1 - t;
+            V3d vprev = v;
+            v = upd(v, r, dt, t + 0.5 * dt, p);
+            V3d rn = r + v * dt;
+            double tn = t + dt;
+            double xvn[6] = {rn.x, rn.y, rn.z, v.x, v.y, v.z};
+            if (term.any() && term.outside(xvn, 6, tn)) break;
+            if (o.save_everystep && it - 1 > 0 && (it - 1) % o.ssi == 0) push(r, upd(vprev, r, 0.5 * dt, t, p), t);
+            r = rn;
+            t = tn;
+            it += 1;
+            steps += 1;
+        }
+    }
+    if (o.save_end && (out.traj.t.empty() || out.traj.t.back() != t)) {
+        if (gc) {
+            V3d xs, vs;
+            gc_to_full(xg, Ef, Bf, q, p.m, mu, t, phase, xs, vs);
+            push(xs, vs, t);
+        } else {
+            const double t_final = is_td ? t : 0.0;
+            push(r, upd(v, r, 0.5 * dt, t_final, p), t);
+        }
+    }
+    out.traj.retcode = ret != TP_RET_SUCCESS ? ret : (steps >= o.maxiters ? TP_RET_MAXITERS : TP_RET_SUCCESS);
+    out.traj.nsteps = steps;
 }
 
 }  // namespace orc

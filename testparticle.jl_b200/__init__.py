@@ -13,16 +13,17 @@ from . import _abi, workloads
 from .constants import (BMoment_Earth, Electron, Ion, MU0_OVER_4PI, Proton, Re, Species, SpeciesDict,
                         c, eV, kB, me, mi, mu0, qe, qi)
 from .fields import (AffineField, CartesianGrid, ClampExtrap, DipoleField, FieldInterpolator, FillExtrap,
-                     PeriodicBC, RectilinearGrid, StructuredGrid, UniformField, WrapExtrap, ZeroField,
+                     PeriodicBC, QuadraticField, RectilinearGrid, StructuredGrid, UniformField, WrapExtrap, ZeroField,
                      build_interpolator)
-from .problems import (AdaptiveBoris, AdaptiveMultistepBoris, Boris, EnsembleB200, EnsembleContext,
+from .problems import (AdaptiveBoris, AdaptiveHybrid, AdaptiveMultistepBoris, Boris, EnsembleB200, EnsembleContext,
                        MultistepBoris, MultistepBoris2, MultistepBoris4, MultistepBoris6, Terminate,
                        TerminateBox, TerminateNaN, TerminateShell, TerminateTime, TraceGCProblem,
-                       TraceProblem, prepare, remake)
+                       TraceHybridProblem, TraceProblem, prepare, remake)
 from .postprocess import get_fields, get_work
 from .runtime import AdjointGrads, ArgumentError, Context, DeviceError, Tape
 from .solution import EnsembleSolution, TraceSolution
-from .solve import (AdjointPlan, BorisPlan, GCPlan, adjoint_solve, plan_adjoint, plan_boris, plan_gc,
+from .solve import (AdjointPlan, BorisPlan, GCPlan, HybridPlan, adjoint_solve, plan_adjoint, plan_boris, plan_gc,
+                    plan_hybrid,
                     prepare_gc, solve)
 from .utility import energy2velocity, get_gyrofrequency, get_gyroperiod, get_gyroradius, get_perp_vector, sph2cart
 

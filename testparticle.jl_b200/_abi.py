@@ -32,6 +32,7 @@ TP_FIELD_UNIFORM = 1
 TP_FIELD_AFFINE = 2
 TP_FIELD_DIPOLE = 3
 TP_FIELD_GRID = 4
+TP_FIELD_QUADRATIC = 5
 
 TP_BC_FILL_NAN = 0
 TP_BC_CLAMP = 1
@@ -45,6 +46,11 @@ TP_ORDER_CUBIC = 2
 TP_GRID_CARTESIAN = 0
 TP_GRID_SPHERICAL = 1
 TP_GRID_SPHERICAL_SCALAR = 2
+
+TP_ADIA_CURVATURE = 0
+TP_ADIA_GRADB = 1
+TP_ADIA_BOTH = 2
+TP_ADIA_JACOBIAN = 3
 
 TP_POINTS_FULL_ORBIT = 0
 TP_POINTS_GC = 1
@@ -100,6 +106,7 @@ class FieldDesc(C.Structure):
         ("ndim", C.c_int32),
         ("dir", C.c_int32),
         ("axis", C.c_void_p * 3),
+        ("quad", C.c_double * 27),
     ]
 
 
@@ -183,6 +190,33 @@ class TuneResult(C.Structure):
     ]
 
 
+class HybridDesc(C.Structure):
+    _fields_ = [
+        ("t0", C.c_double),
+        ("t1", C.c_double),
+        ("q2m", C.c_double),
+        ("m", C.c_double),
+        ("threshold_gc_to_fo", C.c_double),
+        ("threshold_fo_to_gc", C.c_double),
+        ("dtmin", C.c_double),
+        ("dtmax", C.c_double),
+        ("safety_fo", C.c_double),
+        ("abstol", C.c_double),
+        ("reltol", C.c_double),
+        ("maxiters", C.c_int64),
+        ("check_interval", C.c_int64),
+        ("savestepinterval", C.c_int64),
+        ("adiabaticity", C.c_int32),
+        ("save_adiabaticity", C.c_int32),
+        ("save_start", C.c_int32),
+        ("save_end", C.c_int32),
+        ("save_everystep", C.c_int32),
+        ("block", C.c_int32),
+        ("term", TermDesc),
+        ("budget_s", C.c_double),
+    ]
+
+
 class PointsDesc(C.Structure):
     _fields_ = [
         ("kind", C.c_int32),
@@ -228,6 +262,7 @@ SIGNATURES = [
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     ("tp_field_update", C.c_int, [_P, _P]),
     ("tp_eval_points", C.c_int, [_P, C.POINTER(PointsDesc), _P, _P, _P, _P, C.c_int64, _P]),
+    ("tp_hybrid_run", C.c_int, [_P, C.POINTER(HybridDesc), _P, _P, _P, C.c_int64, C.POINTER(_P), C.POINTER(_P)]),
     ("tp_autotune", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(TuneResult)]),
     ("tp_boris_graph_create", C.c_int,
      [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),

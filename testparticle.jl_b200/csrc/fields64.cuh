@@ -176,9 +176,16 @@ __device__ __forceinline__ D3 analytic_eval64(const DevField& f, D3 r, double t)
     }
 }
 
+__device__ __forceinline__ D3 quad_eval64(const DevField& f, D3 r, double t) {
+    double o[3];
+    quad_eval(f, r.x, r.y, r.z, t, o);
+    return {o[0], o[1], o[2]};
+}
+
 template <bool GEN = true>
 __device__ __forceinline__ D3 field_eval64(const DevField& f, D3 r, double t) {
     if (f.kind == TP_FIELD_GRID) return grid_eval64<GEN>(f, r);
+    if (f.kind == TP_FIELD_QUADRATIC) return quad_eval64(f, r, t);
     return analytic_eval64(f, r, t);
 }
 
@@ -264,9 +271,9 @@ __device__ __forceinline__ void eval_EB64t(const DevFields& F, D3 r, double t, D
 }
 
 __device__ __forceinline__ bool fields_static(const DevFields& F) {
-    bool e = !(F.E.kind == TP_FIELD_AFFINE &&
+    bool e = !((F.E.kind == TP_FIELD_AFFINE || F.E.kind == TP_FIELD_QUADRATIC) &&
                (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
-    bool b = !(F.B.kind == TP_FIELD_AFFINE &&
+    bool b = !((F.B.kind == TP_FIELD_AFFINE || F.B.kind == TP_FIELD_QUADRATIC) &&
                (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
     return e && b;
 }
@@ -390,6 +397,23 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
             F = analytic_eval64(f, r, t);
             for (int k = 0; k < 9; ++k) J[k] = f.J[k];
             return;
+        case TP_FIELD_QUADRATIC: {
+            if (!GRID) {  // never selected: quadratic fields take the generic kernels
+                F = {0.0, 0.0, 0.0};
+                return;
+            }
+            F = quad_eval64(f, r, t);
+            // dF_i/dx_j = J_ij + sum_k (Q_ijk + Q_ikj) x_k
+            const double x[3] = {r.x, r.y, r.z};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double* Q = f.Q + 9 * i;
+                    double acc = f.J[3 * i + j];
+                    for (int k = 0; k < 3; ++k) acc = acc + (Q[3 * j + k] + Q[3 * k + j]) * x[k];
+                    J[3 * i + j] = acc;
+                }
+            return;
+        }
         case TP_FIELD_DIPOLE: {
             F = analytic_eval64(f, r, t);
             D3 d = r - D3{f.c[0], f.c[1], f.c[2]};
@@ -501,7 +525,7 @@ __device__ __forceinline__ MagProps magnetic_properties64(const DevField& f, D3 
 // dB/dt of a field: the rate of a time-dependent affine field, else 0
 // (derivative_t, src/prepare.jl:64-74)
 __device__ __forceinline__ D3 field_dtime64(const DevField& f) {
-    if (f.kind == TP_FIELD_AFFINE) return {f.rate[0], f.rate[1], f.rate[2]};
+    if (f.kind == TP_FIELD_AFFINE || f.kind == TP_FIELD_QUADRATIC) return {f.rate[0], f.rate[1], f.rate[2]};
     return {0.0, 0.0, 0.0};
 }
 

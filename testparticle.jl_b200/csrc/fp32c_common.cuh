@@ -216,6 +216,14 @@ static __device__ __noinline__ F3 grid_general32(const DevField& g, const CPos& 
     return {(float)o[0], (float)o[1], (float)o[2]};
 }
 
+// quadratic fields: float64 evaluation of the compensated position, rounded
+static __device__ __noinline__ F3 quad_eval32(const DevField& f, const CPos& p, double t) {
+    double o[3];
+    quad_eval(f, (double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+              (double)p.hi[2] + (double)p.lo[2], t, o);
+    return {(float)o[0], (float)o[1], (float)o[2]};
+}
+
 template <bool GEN = true>
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
     if (GEN && g.general) return grid_general32(g, p);
@@ -292,8 +300,10 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
                  xyz(b111), ax, ay, az);
         return;
     }
-    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p) : analytic_eval32(F.E, p, t);
-    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p) : analytic_eval32(F.B, p, t);
+    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p)
+        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.E, p, t) : analytic_eval32(F.E, p, t);
+    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p)
+        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.B, p, t) : analytic_eval32(F.B, p, t);
 }
 
 template <int FK>
@@ -309,9 +319,9 @@ __device__ __forceinline__ void eval_EB32t(const DevFields& F, const CPos& p, do
 }
 
 __device__ __forceinline__ bool fields_static32(const DevFields& F) {
-    bool e = !(F.E.kind == TP_FIELD_AFFINE &&
+    bool e = !((F.E.kind == TP_FIELD_AFFINE || F.E.kind == TP_FIELD_QUADRATIC) &&
                (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
-    bool b = !(F.B.kind == TP_FIELD_AFFINE &&
+    bool b = !((F.B.kind == TP_FIELD_AFFINE || F.B.kind == TP_FIELD_QUADRATIC) &&
                (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
     return e && b;
 }

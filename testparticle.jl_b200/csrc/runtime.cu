@@ -544,6 +544,9 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
         case TP_FIELD_AFFINE:
         case TP_FIELD_DIPOLE:
             break;
+        case TP_FIELD_QUADRATIC:
+            for (int k = 0; k < 27; ++k) dv.Q[k] = d->quad[k];
+            break;
         case TP_FIELD_GRID: {
             std::string why = check_grid_desc(d);
             if (!why.empty()) {
@@ -1299,6 +1302,145 @@ int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B, const doubl
     return TP_OK;
 }
 
+int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* d, const tp_field* E, const tp_field* B, const double* u0,
+                  int64_t n, tp_result** out, tp_result** adia) {
+    if (!ctx || !d || !out) return fail(ctx, TP_E_ARG, "null argument");
+    *out = nullptr;
+    if (adia) *adia = nullptr;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");
+    if (n < 0 || (n > 0 && !u0)) return fail(ctx, TP_E_ARG, "bad particle table");
+    // AdaptiveHybrid constructor checks (src/hybrid.jl:58-68)
+    if (d->check_interval <= 0) return fail(ctx, TP_E_ARG, "check_interval must be positive.");
+    if (!(d->threshold_gc_to_fo >= d->threshold_fo_to_gc))
+        return fail(ctx, TP_E_ARG, "threshold_gc_to_fo must be >= threshold_fo_to_gc for hysteresis.");
+    if (d->adiabaticity < TP_ADIA_CURVATURE || d->adiabaticity > TP_ADIA_JACOBIAN)
+        return fail(ctx, TP_E_ARG, "adiabaticity must be one of :curvature, :gradB, :both, :jacobian.");
+    if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "savestepinterval must be >= 1");
+    if (d->maxiters < 0) return fail(ctx, TP_E_ARG, "maxiters must be >= 0");
+    if (d->block < 0 || d->block > 256 || (d->block % 32) != 0)
+        return fail(ctx, TP_E_ARG, "block must be 0 or a multiple of 32 up to 256");
+    const bool want_adia = adia && d->save_adiabaticity;
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    int64_t nslots = 64, aslots = want_adia ? 64 : 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        DBuf u0_d, t_d, u_d, ns_d, rc_d, nst_d, at_d, av_d, na_d, st_d;
+        cudaError_t e = u0_d.alloc((size_t)std::max<int64_t>(n, 1) * 6 * sizeof(double));
+        if (e == cudaSuccess) e = t_d.alloc((size_t)std::max<int64_t>(nslots * n, 1) * sizeof(double));
+        if (e == cudaSuccess) e = u_d.alloc((size_t)std::max<int64_t>(nslots * n, 1) * 6 * sizeof(double));
+        if (e == cudaSuccess) e = ns_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = rc_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int8_t));
+        if (e == cudaSuccess) e = nst_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int64_t));
+        if (e == cudaSuccess && want_adia) e = at_d.alloc((size_t)std::max<int64_t>(aslots * n, 1) * sizeof(double));
+        if (e == cudaSuccess && want_adia)
+            e = av_d.alloc((size_t)std::max<int64_t>(aslots * n, 1) * 2 * sizeof(double));
+        if (e == cudaSuccess && want_adia) e = na_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
+        if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+        if (n > 0) e = copy_to_device(ctx, u0_d.p, u0, (size_t)n * 6 * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemsetAsync(st_d.p, 0, sizeof(int32_t), s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "input upload");
+        HybridArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.f.E = E->dev;
+        a.f.B = B->dev;
+        a.term = dev_term(d->term);
+        a.t0 = d->t0;
+        a.t1 = d->t1;
+        a.q2m = d->q2m;
+        a.m = d->m;
+        a.th_gc_fo = d->threshold_gc_to_fo;
+        a.th_fo_gc = d->threshold_fo_to_gc;
+        a.dtmin = d->dtmin;
+        a.dtmax = d->dtmax;
+        a.safety_fo = d->safety_fo;
+        a.abstol = d->abstol;
+        a.reltol = d->reltol;
+        a.maxiters = d->maxiters;
+        a.check = d->check_interval;
+        a.ssi = d->savestepinterval;
+        a.adia_mode = d->adiabaticity;
+        a.save_adia = want_adia ? 1 : 0;
+        a.save_start = d->save_start;
+        a.save_end = d->save_end;
+        a.save_everystep = d->save_everystep;
+        a.n = n;
+        a.nslots = nslots;
+        a.aslots = aslots;
+        a.u0 = u0_d.as<double>();
+        a.t_out = t_d.as<double>();
+        a.u_out = u_d.as<double>();
+        a.nsaved = ns_d.as<int32_t>();
+        a.retcode = rc_d.as<int8_t>();
+        a.nsteps = nst_d.as<int64_t>();
+        a.at_out = at_d.as<double>();
+        a.av_out = av_d.as<double>();
+        a.nadia = na_d.as<int32_t>();
+        a.status = st_d.as<int32_t>();
+        double budget = d->budget_s > 0 ? d->budget_s : 600.0;
+        a.budget_ns = (uint64_t)(budget * 1e9);
+        cudaEvent_t ev0, ev1;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, s);
+        e = launch_hybrid(a, d->block, s);
+        cudaEventRecord(ev1, s);
+        int32_t status = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "hybrid kernel");
+        if (status == TP_E_OVERFLOW && attempt == 0) {
+            // save and check counts are unknown in advance: size exactly and rerun
+            std::vector<int32_t> ns(n), na(want_adia ? n : 0);
+            e = cudaMemcpy(ns.data(), ns_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess && want_adia)
+                e = cudaMemcpy(na.data(), na_d.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "save counts");
+            for (int32_t v : ns) nslots = std::max<int64_t>(nslots, v);
+            for (int32_t v : na) aslots = std::max<int64_t>(aslots, v);
+            continue;
+        }
+        if (status != 0) return status_to_error(ctx, status);
+        DBuf arc_d, anst_d;
+        if (want_adia) {
+            e = arc_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int8_t));
+            if (e == cudaSuccess) e = anst_d.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(int64_t));
+            if (e == cudaSuccess && n > 0)
+                e = cudaMemcpyAsync(arc_d.p, rc_d.p, (size_t)n * sizeof(int8_t), cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess && n > 0)
+                e = cudaMemcpyAsync(anst_d.p, nst_d.p, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "adiabaticity result");
+        }
+        tp_result* r = new tp_result();
+        int st = pack_results(ctx, n, nslots, 6, t_d, u_d, ns_d, rc_d, nst_d, r);
+        if (st != TP_OK) {
+            delete r;
+            return st;
+        }
+        r->elapsed_ms = ms;
+        if (want_adia) {
+            tp_result* ra = new tp_result();
+            st = pack_results(ctx, n, aslots, 2, at_d, av_d, na_d, arc_d, anst_d, ra);
+            if (st != TP_OK) {
+                delete ra;
+                delete r;
+                return st;
+            }
+            ra->elapsed_ms = ms;
+            *adia = ra;
+        }
+        *out = r;
+        return TP_OK;
+    }
+    return fail(ctx, TP_E_OVERFLOW, "save slots exceeded after resizing");
+}
+
 namespace {
 bool is_device_ptr(const void* p) {
     cudaPointerAttributes at;
@@ -1629,7 +1771,7 @@ struct tp_tape {
 namespace {
 
 bool field_static(const tp_field* f) {
-    if (f->desc.kind != TP_FIELD_AFFINE) return true;
+    if (f->desc.kind != TP_FIELD_AFFINE && f->desc.kind != TP_FIELD_QUADRATIC) return true;
     return f->desc.rate[0] == 0.0 && f->desc.rate[1] == 0.0 && f->desc.rate[2] == 0.0;
 }
 
@@ -1656,6 +1798,8 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
         return fail(ctx, TP_E_UNSUPPORTED, "the adjoint needs static fields");
     if (E->dev.general || B->dev.general)
         return fail(ctx, TP_E_UNSUPPORTED, "the adjoint covers trilinear uniform Cartesian grids");
+    if (E->desc.kind == TP_FIELD_QUADRATIC || B->desc.kind == TP_FIELD_QUADRATIC)
+        return fail(ctx, TP_E_UNSUPPORTED, "the adjoint does not cover quadratic fields");
     if (d->checkpoint_every < 1) return fail(ctx, TP_E_ARG, "checkpoint_every must be >= 1");
     if (n < 0) return fail(ctx, TP_E_ARG, "negative particle count");
     if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");

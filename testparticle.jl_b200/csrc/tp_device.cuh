@@ -57,7 +57,25 @@ struct DevField {
     int32_t abc[3];   // per-axis boundary (TP_BC_*)
     int32_t ndim;
     const double* ax[3];  // device node coordinates of non-uniform axes, else null
+    double Q[27];     // quadratic field: Q[9 i + 3 j + k] x_j x_k
 };
+
+// QUADRATIC field value in float64, in the order of the CPU restatement:
+// F_i = ((v_i + ((J_i0 x + J_i1 y) + J_i2 z)) + q_i) + rate_i t with
+// q_i = (x (Q_i0. x) + y (Q_i1. x)) + z (Q_i2. x), Q_ij. x = (Q_ij0 x + Q_ij1 y) + Q_ij2 z
+__device__ __forceinline__ void quad_eval(const DevField& f, double x, double y, double z, double t,
+                                          double o[3]) {
+    for (int i = 0; i < 3; ++i) {
+        const double* J = f.J + 3 * i;
+        const double* Q = f.Q + 9 * i;
+        double lin = (J[0] * x + J[1] * y) + J[2] * z;
+        double qx = (Q[0] * x + Q[1] * y) + Q[2] * z;
+        double qy = (Q[3] * x + Q[4] * y) + Q[5] * z;
+        double qz = (Q[6] * x + Q[7] * y) + Q[8] * z;
+        double q = (x * qx + y * qy) + z * qz;
+        o[i] = ((f.v[i] + lin) + q) + f.rate[i] * t;
+    }
+}
 
 struct DevFields {
     DevField E, B;
@@ -87,6 +105,7 @@ enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2, FK_GENGRID = 3 };
 __host__ __device__ __forceinline__ int field_config_of(const DevFields& f) {
     if ((f.E.kind == TP_FIELD_GRID && f.E.general) || (f.B.kind == TP_FIELD_GRID && f.B.general))
         return FK_GENGRID;
+    if (f.E.kind == TP_FIELD_QUADRATIC || f.B.kind == TP_FIELD_QUADRATIC) return FK_GENERIC;
     if (f.eb && !f.eb_f64) return FK_EBGRID;  // float interleaved table
     if (f.E.kind != TP_FIELD_GRID && f.B.kind != TP_FIELD_GRID) return FK_ANALYTIC;
     return FK_GENERIC;

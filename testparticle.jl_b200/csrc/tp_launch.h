@@ -51,6 +51,28 @@ struct GCPrepArgs {
     double* mu;
 };
 
+// adaptive hybrid GC / full-orbit solve (hybrid.cu)
+struct HybridArgs {
+    DevFields f;
+    DevTerm term;
+    double t0, t1, q2m, m;
+    double th_gc_fo, th_fo_gc, dtmin, dtmax, safety_fo, abstol, reltol;
+    int64_t maxiters, check, ssi;
+    int32_t adia_mode, save_adia, save_start, save_end, save_everystep, pad;
+    int64_t n, nslots, aslots;
+    const double* u0;      // n x 6
+    double* t_out;         // nslots x n
+    double* u_out;         // nslots x 6 x n
+    int32_t* nsaved;
+    int8_t* retcode;
+    int64_t* nsteps;
+    double* at_out;        // aslots x n: check times
+    double* av_out;        // aslots x 2 x n: (adiabaticity, mode)
+    int32_t* nadia;
+    int32_t* status;
+    uint64_t budget_ns;
+};
+
 // fields and work rates at given states (tp_eval_points)
 struct PointsArgs {
     DevFields f;
@@ -108,6 +130,7 @@ cudaError_t launch_gc_fp32(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 int occupancy_gc(const GCArgs& a, int block);
 cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
+cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s);
 
 // context accessors for translation units outside runtime.cu
 int ctx_device(const tp_ctx* ctx);

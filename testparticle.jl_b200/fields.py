@@ -99,6 +99,54 @@ class AffineField(AbstractField):
 
 
 @dataclass
+class QuadraticField(AbstractField):
+    """F_i(x, t) = value_i + sum_j jac_ij x_j + sum_jk quad_ijk x_j x_k + rate_i t.
+
+    Covers the reference's quadratic test fields, e.g. the magnetic bottle
+    B = B0 (-a x z, -a y z, 1 + a z^2) of test/test_hybrid.jl:61-68
+    (see QuadraticField.bottle).
+    """
+
+    value: tuple
+    jac: tuple = ((0.0, 0.0, 0.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    quad: object = None          # (3, 3, 3): quad[i][j][k] multiplies x_j x_k in F_i
+    rate: tuple = (0.0, 0.0, 0.0)
+
+    @classmethod
+    def bottle(cls, B0: float, alpha: float) -> "QuadraticField":
+        Q = np.zeros((3, 3, 3))
+        Q[0, 0, 2] = -B0 * alpha
+        Q[1, 1, 2] = -B0 * alpha
+        Q[2, 2, 2] = B0 * alpha
+        return cls((0.0, 0.0, B0), quad=Q)
+
+    @property
+    def time_dependent(self):
+        return any(float(r) != 0.0 for r in self.rate)
+
+    def descriptor(self):
+        d = _abi.FieldDesc()
+        d.kind = _abi.TP_FIELD_QUADRATIC
+        J = np.asarray(self.jac, dtype=float).reshape(3, 3)
+        Q = np.zeros(27) if self.quad is None else np.asarray(self.quad, dtype=float).reshape(27)
+        for k in range(3):
+            d.value[k] = float(self.value[k])
+            d.rate[k] = float(self.rate[k])
+        for k in range(9):
+            d.jac[k] = float(J.flat[k])
+        for k in range(27):
+            d.quad[k] = float(Q[k])
+        return d
+
+    def __call__(self, x, t=0.0):
+        x = np.asarray(x, float)
+        J = np.asarray(self.jac, dtype=float).reshape(3, 3)
+        Q = np.zeros((3, 3, 3)) if self.quad is None else np.asarray(self.quad, dtype=float).reshape(3, 3, 3)
+        return (np.asarray(self.value, float) + J @ x + np.einsum("ijk,j,k->i", Q, x, x)
+                + np.asarray(self.rate, float) * t)
+
+
+@dataclass
 class DipoleField(AbstractField):
     """Point dipole B = coef (3 (m.rhat) rhat - m) / |x - center|^3, coef = mu0/4pi."""
 

@@ -200,6 +200,62 @@ class TraceGCProblem:
         return replace(self, **kw)
 
 
+@dataclass
+class TraceHybridProblem:
+    """TraceHybridProblem(u0, tspan, p; prob_func) -- full-orbit u0 (6 values, or a
+    (6, N) table) and p = (q2m, m, E, B, F) (src/hybrid.jl:85-120)."""
+
+    u0: Any
+    tspan: tuple
+    p: tuple
+    prob_func: Optional[Callable] = None
+
+    def remake(self, **kw) -> "TraceHybridProblem":
+        return replace(self, **kw)
+
+
+_ADIA = {"curvature": 0, "gradB": 1, "both": 2, "jacobian": 3}
+
+
+@dataclass(frozen=True)
+class AdaptiveHybrid:
+    """AdaptiveHybrid(; threshold, threshold_gc_to_fo, threshold_fo_to_gc, dtmax, dtmin,
+    safety_fo, abstol, reltol, maxiters, check_interval, adiabaticity, save_adiabaticity)
+    (src/hybrid.jl:41-83): GC (RK45) while adiabatic, Boris full orbit otherwise."""
+
+    threshold_gc_to_fo: float
+    threshold_fo_to_gc: float
+    dtmin: float
+    dtmax: float
+    safety_fo: float = 0.1
+    abstol: float = 1.0e-6
+    reltol: float = 1.0e-6
+    maxiters: int = 10000
+    check_interval: int = 10
+    adiabaticity: str = "curvature"
+    save_adiabaticity: bool = True
+
+    def __init__(self, *, threshold: float = 0.1, threshold_gc_to_fo=None, threshold_fo_to_gc=None, dtmax,
+                 dtmin=None, safety_fo: float = 0.1, abstol: float = 1.0e-6, reltol: float = 1.0e-6,
+                 maxiters: int = 10000, check_interval: int = 10, adiabaticity="curvature",
+                 save_adiabaticity: bool = True):
+        gc_fo = threshold if threshold_gc_to_fo is None else threshold_gc_to_fo
+        fo_gc = threshold if threshold_fo_to_gc is None else threshold_fo_to_gc
+        adia = str(adiabaticity).lstrip(":")
+        if check_interval <= 0:
+            raise ValueError("check_interval must be positive.")
+        if not gc_fo >= fo_gc:
+            raise ValueError("threshold_gc_to_fo must be >= threshold_fo_to_gc for hysteresis.")
+        if adia not in _ADIA:
+            raise ValueError("adiabaticity must be one of :curvature, :gradB, :both, :jacobian.")
+        for k, v in dict(threshold_gc_to_fo=float(gc_fo), threshold_fo_to_gc=float(fo_gc),
+                         dtmin=float(1.0e-2 * dtmax if dtmin is None else dtmin), dtmax=float(dtmax),
+                         safety_fo=float(safety_fo), abstol=float(abstol), reltol=float(reltol),
+                         maxiters=int(maxiters), check_interval=int(check_interval), adiabaticity=adia,
+                         save_adiabaticity=bool(save_adiabaticity)).items():
+            object.__setattr__(self, k, v)
+
+
 def remake(prob, **kw):
     return prob.remake(**kw)
 

@@ -132,6 +132,18 @@ class Context:
         _check(self.lib, self.handle, code, "tp_gc_run")
         return self._collect(res)
 
+    def hybrid_run(self, desc: _abi.HybridDesc, E, B, u0: np.ndarray, adiabaticity: bool = True):
+        """tp_hybrid_run -> (RunResult, RunResult of (value, mode) checks or None)."""
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        n = u0.shape[0]
+        assert u0.shape == (n, 6)
+        res, ares = C.c_void_p(), C.c_void_p()
+        code = self.lib.tp_hybrid_run(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0), n,
+                                      C.byref(res), C.byref(ares) if adiabaticity else None)
+        _check(self.lib, self.handle, code, "tp_hybrid_run")
+        main = self._collect(res)
+        return main, (self._collect(ares) if adiabaticity and ares.value else None)
+
     def slots(self, desc: _abi.RunDesc, n: int, dt_i=None, tend_i=None) -> int:
         """Save slots per trajectory a full-orbit run needs (-1: unknown, adaptive without cap)."""
         dt_i = None if dt_i is None else np.ascontiguousarray(dt_i, dtype=np.float64)

@@ -25,10 +25,10 @@ RETCODE_NAMES = {
 
 
 class TraceSolution:
-    __slots__ = ("t", "u", "retcode", "alg", "nsteps", "prob", "index")
+    __slots__ = ("t", "u", "retcode", "alg", "nsteps", "prob", "index", "stats")
 
     def __init__(self, t: np.ndarray, u: np.ndarray, retcode: str, alg: str, nsteps: int = 0, prob=None,
-                 index: int = 0):
+                 index: int = 0, stats=None):
         self.t = t
         self.u = u
         self.retcode = retcode
@@ -36,6 +36,7 @@ class TraceSolution:
         self.nsteps = nsteps
         self.prob = prob      # the problem solved (get_fields / get_work read its fields)
         self.index = index    # trajectory index within its ensemble
+        self.stats = stats    # hybrid solves: {"adiabaticity": {"t", "components", "mode"}}
 
     def __len__(self):
         return self.t.size
@@ -80,16 +81,27 @@ class _Trajectories(Sequence):
         if not 0 <= i < len(self):
             raise IndexError(i)
         a, b = e.offsets[i], e.offsets[i + 1]
+        stats = None
+        if e.adiabaticity is not None:
+            na, ta, va = e.adiabaticity
+            c, d = e._aoff[i], e._aoff[i + 1]
+            stats = {"adiabaticity": {"t": ta[c:d], "components": va[c:d, 0],
+                                      "mode": ["GC" if m == 0 else "FO" for m in va[c:d, 1]]}}
         return TraceSolution(e.t_all[a:b], e.u_all[a:b], RETCODE_NAMES.get(int(e.retcodes[i]), "Default"),
-                             e.alg, int(e.nsteps[i]), e.prob, i)
+                             e.alg, int(e.nsteps[i]), e.prob, i, stats)
 
 
 class EnsembleSolution:
     """Ensemble of trajectories over packed buffers (t_all, u_all, offsets)."""
 
     def __init__(self, t_all, u_all, nsaved, retcodes, nsteps, alg: str, elapsed_s: float,
-                 elapsed_e2e_s: float = 0.0, prob=None):
+                 elapsed_e2e_s: float = 0.0, prob=None, adiabaticity=None):
         self.prob = prob
+        # hybrid solves: (checks per trajectory, check times, (value, mode) rows)
+        self.adiabaticity = adiabaticity
+        if adiabaticity is not None:
+            self._aoff = np.zeros(adiabaticity[0].size + 1, dtype=np.int64)
+            np.cumsum(adiabaticity[0], out=self._aoff[1:])
         self.t_all = t_all
         self.u_all = u_all
         self.nsaved = nsaved

@@ -19,8 +19,8 @@ import numpy as np
 
 from . import _abi
 from .fields import as_field
-from .problems import (Boris, EnsembleB200, EnsembleContext, MultistepBoris, TraceGCProblem,
-                       TraceProblem, as_term)
+from .problems import (_ADIA, AdaptiveHybrid, Boris, EnsembleB200, EnsembleContext, MultistepBoris,
+                       TraceGCProblem, TraceHybridProblem, TraceProblem, as_term)
 from .runtime import Context
 from .solution import EnsembleSolution
 
@@ -213,12 +213,62 @@ def adjoint_solve(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every
     return ctx.adjoint_forward(p.desc, p.E, p.B, p.u0)
 
 
+@dataclass
+class HybridPlan:
+    desc: _abi.HybridDesc
+    E: object
+    B: object
+    u0: np.ndarray          # (N, 6)
+    device: int
+
+
+def plan_hybrid(prob, alg, ens=None, *, trajectories=1, savestepinterval=1, isoutside=None, save_start=True,
+                save_end=True, save_everystep=True) -> HybridPlan:
+    """Descriptor of solve(::TraceHybridProblem, ::AdaptiveHybrid) (src/hybrid.jl:123-138)."""
+    ens = ens if ens is not None else EnsembleB200()
+    if not isinstance(ens, EnsembleB200):
+        raise NotImplementedError("this package runs ensembles on the B200 only: use EnsembleB200()")
+    if not isinstance(alg, AdaptiveHybrid):
+        raise TypeError("solve(::TraceHybridProblem, ::AdaptiveHybrid)")
+    if ens.precision != "fp64":
+        raise NotImplementedError("the hybrid solver runs in precision='fp64'")
+    q2m, m, E, B, _F = prob.p
+    d = _abi.HybridDesc()
+    d.t0, d.t1 = float(prob.tspan[0]), float(prob.tspan[1])
+    d.q2m, d.m = float(q2m), float(m)
+    d.threshold_gc_to_fo, d.threshold_fo_to_gc = alg.threshold_gc_to_fo, alg.threshold_fo_to_gc
+    d.dtmin, d.dtmax, d.safety_fo = alg.dtmin, alg.dtmax, alg.safety_fo
+    d.abstol, d.reltol = alg.abstol, alg.reltol
+    d.maxiters, d.check_interval = alg.maxiters, alg.check_interval
+    d.savestepinterval = int(savestepinterval)
+    d.adiabaticity = _ADIA[alg.adiabaticity]
+    d.save_adiabaticity = int(alg.save_adiabaticity)
+    d.save_start, d.save_end, d.save_everystep = int(save_start), int(save_end), int(save_everystep)
+    d.block = int(ens.block)
+    d.term = as_term(isoutside).descriptor()
+    d.budget_s = float(ens.budget_s)
+    return HybridPlan(d, as_field(E), as_field(B), _initial_table(prob, trajectories, 6), ens.device)
+
+
 def solve(prob, *args, trajectories: int = 1, savestepinterval: int = 1, dt=None, isoutside=None,
           save_start: bool = True, save_end: bool = True, save_everystep: bool = True,
           save_fields: bool = False, save_work: bool = False, maxiters=None, alg=None,
           abstol: float = 1.0e-6, reltol: float = 1.0e-6, step_cap: int = 0, tend=None,
           batch_size=None, seed=None) -> EnsembleSolution:
     """TestParticle.solve(prob, alg, ensemblealg=EnsembleB200(); kwargs...)."""
+    if isinstance(prob, TraceHybridProblem):
+        if not args:
+            raise TypeError("solve(prob::TraceHybridProblem, alg::AdaptiveHybrid, [ensemblealg]; kwargs...)")
+        p = plan_hybrid(prob, args[0], args[1] if len(args) > 1 else None, trajectories=trajectories,
+                        savestepinterval=savestepinterval, isoutside=isoutside, save_start=save_start,
+                        save_end=save_end, save_everystep=save_everystep)
+        ctx = Context.get(p.device)
+        t0 = time.perf_counter()
+        r, ra = ctx.hybrid_run(p.desc, p.E, p.B, p.u0, adiabaticity=bool(p.desc.save_adiabaticity))
+        wall = time.perf_counter() - t0
+        adia = None if ra is None else (ra.nsaved, ra.t, ra.u)
+        return EnsembleSolution(r.t, r.u, r.nsaved, r.retcode, r.nsteps, "hybrid", r.elapsed_ms * 1e-3, wall,
+                                prob=prob, adiabaticity=adia)
     if isinstance(prob, TraceGCProblem):
         p = plan_gc(prob, args[0] if args else None, trajectories=trajectories,
                     savestepinterval=savestepinterval, dt=dt, isoutside=isoutside, save_start=save_start,

@@ -512,3 +512,127 @@ def test_dipole_jacobian_matches_finite_differences(tp, orc):
         e[jdx] = h
         fd = (orc.field_eval(B, x + e) - orc.field_eval(B, x - e))[0] / (2 * h)
         assert np.allclose(J[0][:, jdx], fd, rtol=1e-6, atol=1e-20)
+
+
+# ------------------------------------------------------------------ test/test_hybrid.jl
+def _hybrid(tp, orc, u0, tspan, E, B, alg, species=None, **kw):
+    q2m, m = tp.qi / tp.mi, tp.mi
+    prob = tp.TraceHybridProblem(u0, tspan, (q2m, m, tp.ZeroField(), tp.ZeroField(), tp.ZeroField()))
+    plan = tp.plan_hybrid(prob, alg, **kw)
+    return orc.hybrid_run(plan.desc, E, B, plan.u0)
+
+
+def test_hybrid_uniform_and_sheared_kats(tp, orc):
+    # test_hybrid.jl:14-53
+    u0 = [0.0, 0.0, 0.0, 1.0e4, 0.0, 1.0e3]
+    alg = tp.AdaptiveHybrid(threshold=0.1, dtmax=1.0e-6)
+    r, a = _hybrid(tp, orc, u0, (0.0, 1.0e-4), tp.ZeroField(), tp.UniformField((0.0, 0.0, 0.01)), alg)
+    assert r.retcode[0] == 1
+    assert set(np.asarray(a.u)[:, 1]) == {0.0}   # uniform field: GC throughout
+    B0, k = 0.01, 100.0
+
+    def sheared(x, t):
+        return (B0 * math.cos(k * x[0]), B0 * math.sin(k * x[0]), 0.0)
+
+    def sheared_jac(x, t):
+        return [[-B0 * k * math.sin(k * x[0]), 0, 0], [B0 * k * math.cos(k * x[0]), 0, 0], [0, 0, 0]]
+
+    r, a = _hybrid(tp, orc, u0, (0.0, 1.0e-5), tp.ZeroField(), (sheared, sheared_jac), alg)
+    assert r.retcode[0] == 1
+
+
+def _bottle_case(tp):
+    B0, alpha = 1.0e-4, 1.0e-2
+    q2m = tp.qi / tp.mi
+    T = 2 * math.pi / (abs(q2m) * B0)
+    return tp.QuadraticField.bottle(B0, alpha), T
+
+
+@pytest.mark.parametrize("buffer", [False, True])
+def test_hybrid_bottle_switching_kat(tp, orc, buffer):
+    # test_hybrid.jl:55-100,177-206
+    B, T = _bottle_case(tp)
+    u0 = [0.0, 0.0, 0.0, 5.0e4, 0.0, 1.0e5]
+    if buffer:
+        alg = tp.AdaptiveHybrid(threshold_gc_to_fo=0.2, threshold_fo_to_gc=0.05, dtmax=T, dtmin=1.0e-4 * T,
+                                check_interval=100)
+    else:
+        alg = tp.AdaptiveHybrid(threshold=0.1, dtmax=T, dtmin=1.0e-4 * T, check_interval=100)
+    r, a = _hybrid(tp, orc, u0, (0.0, 30 * T), tp.ZeroField(), B, alg)
+    t, u = r.traj(0)
+    assert r.retcode[0] == 1 and t.size > 100
+    ke0 = 0.5 * tp.mi * (5.0e4 ** 2 + 1.0e5 ** 2)
+    ke1 = 0.5 * tp.mi * np.sum(u[-1, 3:6] ** 2)
+    assert abs(ke1 - ke0) <= 0.1 * ke0
+    if not buffer:
+        modes = set(np.asarray(a.u)[:, 1])
+        assert modes == {0.0, 1.0}   # both modes visited
+
+
+def test_hybrid_gc_roundtrip_exact_in_uniform_field(tp, orc):
+    # test_hybrid.jl:102-121
+    B = tp.UniformField((0.0, 0.0, 0.01))
+    xv = np.array([[*x0, *v0] for x0 in ([0, 0, 0], [1.0, 0.5, 1.0], [3.0, 0, 2.0])
+                   for v0 in ([5.0e4, 0, 1.0e5], [3.0e4, 4.0e4, 8.0e4])], dtype=float)
+    rec = orc.gc_roundtrip(tp.ZeroField(), B, xv, tp.qi, tp.mi)
+    assert np.all(np.linalg.norm(rec[:, :3] - xv[:, :3], axis=1) < 1.0e-10)
+    assert np.all(np.linalg.norm(rec[:, 3:] - xv[:, 3:], axis=1) < 1.0e-8)
+
+
+def test_hybrid_forced_fo_is_boris(tp, orc):
+    # test_hybrid.jl:123-152: threshold 0 keeps the full orbit; it is Boris with dt_fo
+    B0 = 0.01
+    q2m = tp.qi / tp.mi
+    T = 2 * math.pi / (abs(q2m) * B0)
+    u0 = [0.0, 0.0, 0.0, 5.0e4, 0.0, 1.0e5]
+    alg = tp.AdaptiveHybrid(threshold=0.0, dtmax=10 * T, dtmin=1.0e-6 * T, check_interval=100)
+    r, _ = _hybrid(tp, orc, u0, (0.0, 30 * T), tp.ZeroField(), tp.UniformField((0.0, 0.0, B0)), alg)
+    th, uh = r.traj(0)
+    dt_fo = 2 * math.pi * alg.safety_fo / (abs(q2m) * B0)
+    prob = tp.TraceProblem(u0, (0.0, 30 * T), (q2m, tp.mi, tp.ZeroField(), tp.ZeroField(), tp.ZeroField()))
+    plan = tp.plan_boris(prob, tp.Boris(), dt=dt_fo)
+    rb = orc.boris_run(plan.desc, tp.ZeroField(), tp.UniformField((0.0, 0.0, B0)), plan.u0)
+    tb, ub = rb.traj(0)
+    assert th.size == tb.size
+    sol = tp.TraceSolution(th, uh, "Success", "hybrid")
+    for i in range(tb.size):
+        uu = sol(tb[i])
+        assert np.linalg.norm(uu[:3] - ub[i, :3]) <= 1.0e-8
+        assert np.linalg.norm(uu[3:] - ub[i, 3:]) <= 1.0e-5
+
+
+def test_hybrid_argument_errors(tp):
+    # test_hybrid.jl:154-175
+    assert tp.AdaptiveHybrid(threshold=0.1, dtmax=1.0).threshold_gc_to_fo == 0.1
+    assert tp.AdaptiveHybrid(threshold=0.1, dtmax=1.0).threshold_fo_to_gc == 0.1
+    with pytest.raises(ValueError):
+        tp.AdaptiveHybrid(threshold_gc_to_fo=0.05, threshold_fo_to_gc=0.2, dtmax=1.0)
+    a = tp.AdaptiveHybrid(threshold_gc_to_fo=0.2, threshold_fo_to_gc=0.05, dtmax=1.0)
+    assert a.threshold_gc_to_fo == 0.2 and a.threshold_fo_to_gc == 0.05
+    with pytest.raises(ValueError):
+        tp.AdaptiveHybrid(dtmax=1.0, check_interval=0)
+    with pytest.raises(ValueError):
+        tp.AdaptiveHybrid(dtmax=1.0, adiabaticity="nope")
+
+
+def test_quadratic_field_matches_numpy(tp, orc):
+    B = tp.QuadraticField.bottle(1.0e-4, 1.0e-2)
+    pts = np.random.default_rng(1).normal(size=(50, 3)) * 10
+    v, J = orc.field_eval(B, pts, jacobian=True)
+    for i, x in enumerate(pts):
+        assert np.allclose(v[i], B(x), rtol=1e-14, atol=0)
+        h = 1e-5
+        fd = np.stack([(B(x + h * e) - B(x - h * e)) / (2 * h) for e in np.eye(3)], axis=1)
+        assert np.allclose(J[i], fd, rtol=1e-7, atol=1e-12)
+
+
+def test_portable_gyrophase_trig_accuracy(orc):
+    # the hybrid's sin / cos / atan2 (+, -, *, /, sqrt only, shared by the
+    # kernel and the oracle): within 1 ulp of 1 and 4 ulp of pi of libm
+    rng = np.random.default_rng(0)
+    x = np.concatenate([np.linspace(-8, 8, 100001), rng.uniform(-8, 8, 100000), rng.normal(size=50000)])
+    y = rng.normal(size=x.size)
+    s, c, a = orc.trig(x, y)
+    assert np.max(np.abs(s - np.sin(x))) <= np.spacing(1.0)
+    assert np.max(np.abs(c - np.cos(x))) <= np.spacing(1.0)
+    assert np.max(np.abs(a - np.arctan2(y, x))) <= 4 * np.spacing(np.pi)
