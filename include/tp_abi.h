@@ -307,6 +307,43 @@ typedef struct tp_hybrid_desc {
 int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* desc, const tp_field* E, const tp_field* B,
                   const double* u0, int64_t n, tp_result** out, tp_result** adia);
 
+/* ---- virtual detectors ----------------------------------------------------
+ * get_particle_crossings / get_particle_flux(es) / get_first_crossing of the
+ * Meshes extension (ext/TestParticleMeshesExt.jl:98-491), evaluated on the
+ * device over packed trajectories: t (total saves), u (total x width, the
+ * first 6 values of a row are x, v), nsaved (n; trajectory i owns the next
+ * nsaved[i] rows).  A segment between consecutive saves crosses a surface
+ * when the signed distances s1, s2 of its end points satisfy s1 s2 < 0 or
+ * (s1 != 0 and s2 == 0); the crossing is at f = s1 / (s1 - s2), its state is
+ * the linear interpolation of the saves at t = fma(f, t2 - t1, t1); a disk
+ * crossing counts only inside the radius.  Pointers may be host or device
+ * memory.                                                                    */
+enum { TP_SURF_PLANE = 0, TP_SURF_DISK = 1, TP_SURF_SPHERE = 2 };
+typedef struct tp_surface {
+    int32_t kind;         /* TP_SURF_*                                        */
+    int32_t reserved;
+    double point[3];      /* PLANE / DISK: point of the plane (the disk's
+                             centre); SPHERE: centre                          */
+    double normal[3];     /* PLANE / DISK: unit normal                        */
+    double radius;        /* DISK / SPHERE                                    */
+} tp_surface;
+/* Fluxes through disks and spheres: n_flux[j] = sum of weights / area,
+ * v_flux[3 j + c] = sum of weight * v_c / area over every crossing of
+ * surface j.  weights: n per-trajectory weights, or NULL for `weight`.       */
+int tp_detect_fluxes(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved,
+                     int64_t n, const tp_surface* surfaces, int32_t nsurf, const double* weights,
+                     double weight, double* n_flux, double* v_flux);
+/* Crossing velocities and weights per surface: counts[j] crossings of
+ * surface j; rows (NULL: count only) receives, surface after surface, one
+ * (vx, vy, vz, weight) row per crossing in trajectory and time order.        */
+int tp_detect_crossings(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved,
+                        int64_t n, const tp_surface* surfaces, int32_t nsurf, const double* weights,
+                        double weight, int64_t* counts, double* rows);
+/* The interpolated state (6 values) of each trajectory's first crossing of
+ * one surface, NaN where it never crosses.                                   */
+int tp_detect_first_crossing(tp_ctx* ctx, const double* t, const double* u, int32_t width,
+                             const int32_t* nsaved, int64_t n, const tp_surface* surface, double* out);
+
 /* ---- fields and work rates at given states ------------------------------
  * get_fields / get_work (src/boris/boris.jl:599-640): E, B and the work rates
  * of get_work_rates (src/equations.jl:394-441) or get_work_rates_gc

@@ -67,6 +67,8 @@ def lib() -> C.CDLL:
                                      C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), C.POINTER(FieldCB),
                                      C.POINTER(TermCB), P, C.c_int64, C.c_int, C.c_int64, C.c_int64, P, P, P, P,
                                      P, P, P, P]
+        L.orc_detect.restype = C.c_int
+        L.orc_detect.argtypes = [P, P, C.c_int32, P, C.c_int64, P, C.c_int32, P, C.c_double, P, P, P, P]
         L.orc_trig.restype = C.c_int
         L.orc_trig.argtypes = [P, P, C.c_int64, P, P, P]
         L.orc_gc_roundtrip.restype = C.c_int
@@ -344,6 +346,28 @@ def hybrid_run(desc, E, B, u0: np.ndarray, nthreads: int = 0, isoutside: Optiona
             ares = OracleResult(na, rc, nst, ta, ua)
         return res, ares
     raise RuntimeError("oracle: output sizing failed")
+
+
+def detect(t, u, nsaved, surfaces, weights=None, weight: float = 1.0):
+    """Detector restatement over packed trajectories -> (sums (ns, 4), counts (ns,),
+    rows (total, 4), first (n, 6) for surfaces[0]); surfaces are package Surface objects."""
+    from_abi = _abi()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    ns = np.ascontiguousarray(nsaved, dtype=np.int32)
+    n = ns.size
+    descs = (from_abi.Surface * len(surfaces))(*[sf.descriptor() for sf in surfaces])
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    sums = np.empty((len(surfaces), 4))
+    counts = np.empty(len(surfaces), dtype=np.int64)
+    first = np.empty((n, 6))
+    L = lib()
+    L.orc_detect(_ptr(t), _ptr(u), u.shape[1], _ptr(ns), n, C.cast(descs, C.c_void_p), len(surfaces), _ptr(w),
+                 float(weight), _ptr(sums), _ptr(counts), None, _ptr(first))
+    rows = np.empty((int(counts.sum()), 4))
+    L.orc_detect(_ptr(t), _ptr(u), u.shape[1], _ptr(ns), n, C.cast(descs, C.c_void_p), len(surfaces), _ptr(w),
+                 float(weight), None, None, _ptr(rows), None)
+    return sums, counts, rows, first
 
 
 def trig(x: np.ndarray, y: np.ndarray):

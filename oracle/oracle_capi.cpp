@@ -388,6 +388,63 @@ int orc_boris_run(const tp_run_desc* d, const tp_field_desc* Ed, const tp_field_
     return overflow ? TP_E_OVERFLOW : TP_OK;
 }
 
+// Detectors over packed trajectories (ext/TestParticleMeshesExt.jl:98-491).
+// sums: nsurf x 4 (sum w, sum w v) accumulated trajectory after trajectory as
+// the reference's get_particle_fluxes; counts: nsurf; rows (optional, sized by
+// a counting call): surface-major (vx, vy, vz, w); first: n x 6 for surface 0.
+int orc_detect(const double* t, const double* u, int32_t W, const int32_t* nsaved, int64_t n,
+               const tp_surface* surf, int32_t nsurf, const double* weights, double weight, double* sums,
+               int64_t* counts, double* rows, double* first) {
+    std::vector<int64_t> off(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) off[i + 1] = off[i] + std::max<int32_t>(nsaved[i], 0);
+    if (sums)
+        for (int64_t k = 0; k < (int64_t)nsurf * 4; ++k) sums[k] = 0.0;
+    int64_t row = 0;
+    for (int j = 0; j < nsurf; ++j) {
+        int64_t cj = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const double w = weights ? weights[i] : weight;
+            const double* ti = t + off[i];
+            const double* ui = u + off[i] * W;
+            det_walk(ti, ui, W, nsaved[i], surf[j], [&](const double* st) {
+                cj += 1;
+                if (sums) {
+                    sums[4 * j] = sums[4 * j] + w;
+                    for (int c = 0; c < 3; ++c) sums[4 * j + 1 + c] = sums[4 * j + 1 + c] + st[3 + c] * w;
+                }
+                if (rows) {
+                    for (int c = 0; c < 3; ++c) rows[4 * row + c] = st[3 + c];
+                    rows[4 * row + 3] = w;
+                    row += 1;
+                }
+                return true;
+            });
+        }
+        if (counts) counts[j] = cj;
+    }
+    if (first) {
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        for (int64_t i = 0; i < n; ++i) {
+            const double* ti = t + off[i];
+            const double* ui = u + off[i] * W;
+            double* o = first + 6 * i;
+            for (int c = 0; c < 6; ++c) o[c] = nan;
+            bool zero = false;
+            bool done = false;
+            det_walk(ti, ui, W, nsaved[i], surf[0], [&](const double* st) {
+                if (!done) {
+                    for (int c = 0; c < 6; ++c) o[c] = st[c];
+                    done = true;
+                }
+                return false;
+            }, &zero);
+            if (zero)
+                for (int c = 0; c < 6; ++c) o[c] = ui[c];
+        }
+    }
+    return TP_OK;
+}
+
 // The hybrid's portable gyrophase trigonometry, for accuracy tests.
 int orc_trig(const double* x, const double* y, int64_t n, double* s, double* c, double* a) {
     for (int64_t i = 0; i < n; ++i) {

@@ -1638,4 +1638,64 @@ inline void hybrid_single(const Params& p, const HybridOpts& o, const Term& term
     out.traj.nsteps = steps;
 }
 
+
+// ---------------------------------------------------------------- detectors
+// Virtual detectors of the Meshes extension (ext/TestParticleMeshesExt.jl:
+// 98-491) over packed trajectories.  _signed_distance: (p - p0) . n for a
+// plane or disk, |p - c| - r for a sphere; _is_valid_intersection: a disk
+// crossing lies within the radius.  A segment crosses when s1 s2 < 0 or
+// (s1 != 0 and s2 == 0), at f = s1 / (s1 - s2), t = muladd(f, t2 - t1, t1);
+// the state there is the solution's linear interpolation (searchsortedlast,
+// u_i + theta (u_{i+1} - u_i), as the reference tests' MockSol).
+inline double det_sdist(const tp_surface& S, V3d p) {
+    V3d v = p - V3d{S.point[0], S.point[1], S.point[2]};
+    if (S.kind == TP_SURF_SPHERE) return norm(v) - S.radius;
+    return dot(v, V3d{S.normal[0], S.normal[1], S.normal[2]});
+}
+
+inline bool det_valid(const tp_surface& S, V3d p) {
+    if (S.kind != TP_SURF_DISK) return true;
+    V3d d = p - V3d{S.point[0], S.point[1], S.point[2]};
+    return dot(d, d) <= S.radius * S.radius;
+}
+
+inline void det_interp(const double* t, const double* u, int W, int64_t m, double tc, double s[6]) {
+    int64_t i = std::upper_bound(t, t + m, tc) - t - 1;
+    if (i < 0 || i >= m - 1) {
+        const double* r = u + (i < 0 ? 0 : m - 1) * W;
+        for (int c = 0; c < 6; ++c) s[c] = r[c];
+        return;
+    }
+    double th = (tc - t[i]) / (t[i + 1] - t[i]);
+    for (int c = 0; c < 6; ++c) s[c] = u[i * W + c] + th * (u[(i + 1) * W + c] - u[i * W + c]);
+}
+
+// Calls visit(state) for each valid crossing of trajectory (t, u, m) in time
+// order; returns early when visit returns false.  first_zero: the first
+// save lies on the surface (get_first_crossing returns it).
+template <class Visit>
+inline void det_walk(const double* t, const double* u, int W, int64_t m, const tp_surface& S, Visit visit,
+                     bool* first_zero = nullptr) {
+    if (m < 1) return;
+    V3d p1{u[0], u[1], u[2]};
+    double s1 = det_sdist(S, p1);
+    if (first_zero) *first_zero = (s1 == 0.0);
+    for (int64_t k = 0; k + 1 < m; ++k) {
+        V3d p2{u[(k + 1) * W], u[(k + 1) * W + 1], u[(k + 1) * W + 2]};
+        double s2 = det_sdist(S, p2);
+        if (s1 * s2 < 0.0 || (s1 != 0.0 && s2 == 0.0)) {
+            double f = s1 / (s1 - s2);
+            V3d pc = p1 + f * (p2 - p1);
+            if (det_valid(S, pc)) {
+                double tc = std::fma(f, t[k + 1] - t[k], t[k]);
+                double st[6];
+                det_interp(t, u, W, m, tc, st);
+                if (!visit(st)) return;
+            }
+        }
+        s1 = s2;
+        p1 = p2;
+    }
+}
+
 }  // namespace orc

@@ -19,6 +19,8 @@ from .problems import (AdaptiveBoris, AdaptiveHybrid, AdaptiveMultistepBoris, Bo
                        MultistepBoris, MultistepBoris2, MultistepBoris4, MultistepBoris6, Terminate,
                        TerminateBox, TerminateNaN, TerminateShell, TerminateTime, TraceGCProblem,
                        TraceHybridProblem, TraceProblem, prepare, remake)
+from .detectors import (Disk, Plane, Sphere, get_first_crossing, get_particle_crossings, get_particle_flux,
+                        get_particle_fluxes)
 from .postprocess import get_fields, get_work
 from .runtime import AdjointGrads, ArgumentError, Context, DeviceError, Tape
 from .solution import EnsembleSolution, TraceSolution

@@ -52,6 +52,10 @@ TP_ADIA_GRADB = 1
 TP_ADIA_BOTH = 2
 TP_ADIA_JACOBIAN = 3
 
+TP_SURF_PLANE = 0
+TP_SURF_DISK = 1
+TP_SURF_SPHERE = 2
+
 TP_POINTS_FULL_ORBIT = 0
 TP_POINTS_GC = 1
 
@@ -217,6 +221,16 @@ class HybridDesc(C.Structure):
     ]
 
 
+class Surface(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("reserved", C.c_int32),
+        ("point", _D3),
+        ("normal", _D3),
+        ("radius", C.c_double),
+    ]
+
+
 class PointsDesc(C.Structure):
     _fields_ = [
         ("kind", C.c_int32),
@@ -262,6 +276,11 @@ SIGNATURES = [
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     ("tp_field_update", C.c_int, [_P, _P]),
     ("tp_eval_points", C.c_int, [_P, C.POINTER(PointsDesc), _P, _P, _P, _P, C.c_int64, _P]),
+    ("tp_detect_fluxes", C.c_int,
+     [_P, _P, _P, C.c_int32, _P, C.c_int64, C.POINTER(Surface), C.c_int32, _P, C.c_double, _P, _P]),
+    ("tp_detect_crossings", C.c_int,
+     [_P, _P, _P, C.c_int32, _P, C.c_int64, C.POINTER(Surface), C.c_int32, _P, C.c_double, _P, _P]),
+    ("tp_detect_first_crossing", C.c_int, [_P, _P, _P, C.c_int32, _P, C.c_int64, C.POINTER(Surface), _P]),
     ("tp_hybrid_run", C.c_int, [_P, C.POINTER(HybridDesc), _P, _P, _P, C.c_int64, C.POINTER(_P), C.POINTER(_P)]),
     ("tp_autotune", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(TuneResult)]),
     ("tp_boris_graph_create", C.c_int,

@@ -1,7 +1,7 @@
 """Build libtpb200.so (the CUDA library behind include/tp_abi.h) in-tree.
 
 Every translation unit is compiled for sm_100a only.  The float64 kernels
-(boris_fp64.cu, gc_fp64.cu, hybrid.cu) are compiled with -fmad=false so that their
+(boris_fp64.cu, gc_fp64.cu, hybrid.cu, detect.cu) are compiled with -fmad=false so that their
 arithmetic follows the reference's operation order; the float32 kernels use
 contraction.  Objects are rebuilt only when a source or header is newer.
 """
@@ -22,9 +22,9 @@ INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
-NO_FMAD = {"boris_fp64.cu", "gc_fp64.cu", "hybrid.cu"}
+NO_FMAD = {"boris_fp64.cu", "gc_fp64.cu", "hybrid.cu", "detect.cu"}
 SOURCES = ["runtime.cu", "pack.cu", "boris_fp64.cu", "boris_fp32c.cu", "gc_fp64.cu", "gc_fp32.cu", "adjoint.cu",
-           "noalloc.cu", "hybrid.cu"]
+           "noalloc.cu", "hybrid.cu", "detect.cu"]
 
 
 def _nvcc() -> str:

@@ -1441,6 +1441,7 @@ int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* d, const tp_field* E, const
     return fail(ctx, TP_E_OVERFLOW, "save slots exceeded after resizing");
 }
 
+
 namespace {
 bool is_device_ptr(const void* p) {
     cudaPointerAttributes at;
@@ -1451,6 +1452,142 @@ bool is_device_ptr(const void* p) {
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 }  // namespace
+
+// Inputs of the detector entry points on the device: host arrays are
+// copied (their total number of saves from the host nsaved), device arrays
+// are used in place.
+struct DetInputs {
+    DBuf t_d, u_d, ns_d, w_d, surf_d;
+    const double *t = nullptr, *u = nullptr, *w = nullptr;
+    const int32_t* ns = nullptr;
+    const tp_surface* surf = nullptr;
+};
+
+int det_inputs(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved, int64_t n,
+               const tp_surface* surfaces, int32_t nsurf, const double* weights, bool flux, DetInputs& in) {
+    if (width < 6) return fail(ctx, TP_E_ARG, "width must be >= 6 (x, v first)");
+    if (n < 0 || nsurf < 1 || !surfaces) return fail(ctx, TP_E_ARG, "need n >= 0 trajectories and a surface");
+    if (n > 0 && (!t || !u || !nsaved)) return fail(ctx, TP_E_ARG, "null trajectory buffer");
+    for (int j = 0; j < nsurf; ++j) {
+        const tp_surface& S = surfaces[j];
+        if (S.kind < TP_SURF_PLANE || S.kind > TP_SURF_SPHERE) return fail(ctx, TP_E_ARG, "unknown surface kind");
+        if (flux && S.kind == TP_SURF_PLANE) return fail(ctx, TP_E_ARG, "fluxes need a disk or a sphere (an area)");
+    }
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = in.surf_d.alloc((size_t)nsurf * sizeof(tp_surface));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in.surf_d.p, surfaces, (size_t)nsurf * sizeof(tp_surface),
+                                              cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "surfaces");
+    in.surf = in.surf_d.as<tp_surface>();
+    if (n == 0) return TP_OK;
+    if (is_device_ptr(u)) {
+        in.t = t;
+        in.u = u;
+        in.ns = nsaved;
+        if (weights && !is_device_ptr(weights)) {
+            e = in.w_d.alloc((size_t)n * sizeof(double));
+            if (e == cudaSuccess) e = copy_to_device(ctx, in.w_d.p, weights, (size_t)n * sizeof(double));
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "weights");
+            in.w = in.w_d.as<double>();
+        } else {
+            in.w = weights;
+        }
+        return TP_OK;
+    }
+    int64_t total = 0;
+    for (int64_t i = 0; i < n; ++i) total += nsaved[i] > 0 ? nsaved[i] : 0;
+    e = in.t_d.alloc((size_t)std::max<int64_t>(total, 1) * sizeof(double));
+    if (e == cudaSuccess) e = in.u_d.alloc((size_t)std::max<int64_t>(total, 1) * width * sizeof(double));
+    if (e == cudaSuccess) e = in.ns_d.alloc((size_t)n * sizeof(int32_t));
+    if (e == cudaSuccess && weights) e = in.w_d.alloc((size_t)n * sizeof(double));
+    if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, "device allocation");
+    e = copy_to_device(ctx, in.t_d.p, t, (size_t)total * sizeof(double));
+    if (e == cudaSuccess) e = copy_to_device(ctx, in.u_d.p, u, (size_t)total * width * sizeof(double));
+    if (e == cudaSuccess) e = copy_to_device(ctx, in.ns_d.p, nsaved, (size_t)n * sizeof(int32_t));
+    if (e == cudaSuccess && weights) e = copy_to_device(ctx, in.w_d.p, weights, (size_t)n * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trajectory upload");
+    in.t = in.t_d.as<double>();
+    in.u = in.u_d.as<double>();
+    in.ns = in.ns_d.as<int32_t>();
+    in.w = weights ? in.w_d.as<double>() : nullptr;
+    return TP_OK;
+}
+
+int tp_detect_fluxes(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved, int64_t n,
+                     const tp_surface* surfaces, int32_t nsurf, const double* weights, double weight,
+                     double* n_flux, double* v_flux) {
+    if (!ctx || !n_flux || !v_flux) return fail(ctx, TP_E_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    DetInputs in;
+    int st = det_inputs(ctx, t, u, width, nsaved, n, surfaces, nsurf, weights, true, in);
+    if (st != TP_OK) return st;
+    std::vector<double> tot((size_t)nsurf * 4, 0.0);
+    if (n > 0) {
+        DBuf tot_d;
+        cudaError_t e = tot_d.alloc((size_t)nsurf * 4 * sizeof(double));
+        if (e == cudaSuccess)
+            e = launch_detect(0, in.t, in.u, width, in.ns, n, in.surf, nsurf, in.w, weight, tot_d.as<double>(),
+                              nullptr, nullptr, nullptr, ctx->stream);
+        if (e == cudaSuccess) e = copy_to_host(ctx, tot.data(), tot_d.p, tot.size() * sizeof(double));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "detector fluxes");
+    }
+    // get_particle_flux(es): sums times inv(area) (Meshes: pi r^2, 4 pi r^2)
+    const double pi = 3.141592653589793;
+    for (int j = 0; j < nsurf; ++j) {
+        const double r = surfaces[j].radius;
+        const double area = surfaces[j].kind == TP_SURF_SPHERE ? (4.0 * pi) * (r * r) : pi * (r * r);
+        const double inv_area = 1.0 / area;
+        n_flux[j] = tot[4 * j] * inv_area;
+        for (int c = 0; c < 3; ++c) v_flux[3 * j + c] = tot[4 * j + 1 + c] * inv_area;
+    }
+    return TP_OK;
+}
+
+int tp_detect_crossings(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved,
+                        int64_t n, const tp_surface* surfaces, int32_t nsurf, const double* weights, double weight,
+                        int64_t* counts, double* rows) {
+    if (!ctx || !counts) return fail(ctx, TP_E_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    DetInputs in;
+    int st = det_inputs(ctx, t, u, width, nsaved, n, surfaces, nsurf, weights, false, in);
+    if (st != TP_OK) return st;
+    for (int j = 0; j < nsurf; ++j) counts[j] = 0;
+    if (n == 0) return TP_OK;
+    double* rows_d = nullptr;
+    cudaError_t e = launch_detect(1, in.t, in.u, width, in.ns, n, in.surf, nsurf, in.w, weight, nullptr, counts,
+                                  rows ? &rows_d : nullptr, nullptr, ctx->stream);
+    if (e == cudaSuccess && rows) {
+        int64_t total = 0;
+        for (int j = 0; j < nsurf; ++j) total += counts[j];
+        e = copy_to_host(ctx, rows, rows_d, (size_t)total * 4 * sizeof(double));
+    }
+    if (rows_d) cudaFreeAsync(rows_d, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "detector crossings");
+    return TP_OK;
+}
+
+int tp_detect_first_crossing(tp_ctx* ctx, const double* t, const double* u, int32_t width, const int32_t* nsaved,
+                             int64_t n, const tp_surface* surface, double* out) {
+    if (!ctx || !out) return fail(ctx, TP_E_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    DetInputs in;
+    int st = det_inputs(ctx, t, u, width, nsaved, n, surface, 1, nullptr, false, in);
+    if (st != TP_OK) return st;
+    if (n == 0) return TP_OK;
+    const bool o_dev = is_device_ptr(out);
+    DBuf o_d;
+    cudaError_t e = o_dev ? cudaSuccess : o_d.alloc((size_t)n * 6 * sizeof(double));
+    if (e == cudaSuccess)
+        e = launch_detect(2, in.t, in.u, width, in.ns, n, in.surf, 1, nullptr, 0.0, nullptr, nullptr, nullptr,
+                          o_dev ? out : o_d.as<double>(), ctx->stream);
+    if (e == cudaSuccess)
+        e = o_dev ? cudaStreamSynchronize(ctx->stream) : copy_to_host(ctx, out, o_d.p, (size_t)n * 6 * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "first crossing");
+    return TP_OK;
+}
 
 int tp_eval_points(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, const tp_field* B,
                    const double* u, const double* t, int64_t n, double* out) {

@@ -131,6 +131,13 @@ int occupancy_gc(const GCArgs& a, int block);
 cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
 cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s);
+// virtual detectors (detect.cu): mode 0 fluxes (tot: nsurf x 4 sums on the
+// device), 1 crossings (counts on the host; *rows_d_out: device rows the
+// caller frees with cudaFreeAsync), 2 first crossing (first: n x 6, device)
+cudaError_t launch_detect(int mode, const double* t, const double* u, int32_t width, const int32_t* nsaved,
+                          int64_t n, const tp_surface* surf_d, int32_t nsurf, const double* weights,
+                          double weight, double* tot, int64_t* counts_h, double** rows_d_out, double* first,
+                          cudaStream_t s);
 
 // context accessors for translation units outside runtime.cu
 int ctx_device(const tp_ctx* ctx);

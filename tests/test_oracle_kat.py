@@ -636,3 +636,57 @@ def test_portable_gyrophase_trig_accuracy(orc):
     assert np.max(np.abs(s - np.sin(x))) <= np.spacing(1.0)
     assert np.max(np.abs(c - np.cos(x))) <= np.spacing(1.0)
     assert np.max(np.abs(a - np.arctan2(y, x))) <= 4 * np.spacing(np.pi)
+
+
+# ------------------------------------------------------------------ virtual detectors (test_utility.jl:768-960)
+def _line(x0, y0, vx, vy, z0=0.0, vz=0.0, n=21):
+    t = np.arange(float(n))
+    u = np.stack([x0 + vx * t, y0 + vy * t, z0 + vz * t, np.full(n, vx), np.full(n, vy), np.full(n, vz)], axis=1)
+    return t, u
+
+
+def _pack_lines(*lines):
+    t = np.concatenate([a for a, _ in lines])
+    u = np.concatenate([b for _, b in lines])
+    return t, u, np.array([len(a) for a, _ in lines], dtype=np.int32)
+
+
+def test_detector_kats(tp, orc):
+    disk = tp.Disk(tp.Plane((0.0, 0.0, 0.0), (1.0, 0.0, 0.0)), 5.0)
+    area = math.pi * 25.0
+    l1 = _line(-10.0, 0.0, 1.0, 0.0)
+    l2 = _line(-10.0, 10.0, 1.0, 0.0)      # misses the disk
+    l3 = _line(5.0, -10.0, 0.0, 1.0)       # parallel to the plane
+    sums, counts, rows, _ = orc.detect(*_pack_lines(l1), [disk])
+    assert counts[0] == 1 and np.allclose(rows[0], [1.0, 0.0, 0.0, 1.0])
+    assert math.isclose(sums[0, 0] / area, 1.0 / area) and np.allclose(sums[0, 1:] / area, [1.0 / area, 0, 0])
+    for l in (l2, l3):
+        sums, counts, _, _ = orc.detect(*_pack_lines(l), [disk])
+        assert counts[0] == 0 and np.all(sums == 0.0)
+    sums, counts, _, _ = orc.detect(*_pack_lines(l1, l2, l3), [disk], weights=[1.0, 2.0, 3.0])
+    assert sums[0, 0] == 1.0
+    sums, _, _, _ = orc.detect(*_pack_lines(l1, l1, l2), [disk], weights=[1.0, 2.0, 3.0])
+    assert sums[0, 0] == 3.0 and np.allclose(sums[0, 1:], [3.0, 0.0, 0.0])
+    _, counts, rows, _ = orc.detect(*_pack_lines(l1), [tp.Plane((0.0, 0.0, 0.0), (1.0, 0.0, 0.0))], weight=3.0)
+    assert counts[0] == 1 and rows[0, 3] == 3.0 and np.allclose(rows[0, :3], [1.0, 0.0, 0.0])
+    sums, counts, _, _ = orc.detect(*_pack_lines(l1), [tp.Sphere((0.0, 0.0, 0.0), 5.0)])
+    assert counts[0] == 2 and np.allclose(sums[0], [2.0, 2.0, 0.0, 0.0])
+    # equivalence: weight 2 at v = 1 and weight 1 at v = 2 (exact values)
+    la, lb = _line(-10.0, 0.0, 1.0, 0.0), _line(-10.0, 0.0, 2.0, 0.0)
+    _, _, ra, _ = orc.detect(*_pack_lines(la), [disk], weight=2.0)
+    _, _, rb, _ = orc.detect(*_pack_lines(lb), [disk], weight=1.0)
+    assert ra[0, 0] == 1.0 and ra[0, 3] == 2.0 and rb[0, 0] == 2.0 and rb[0, 3] == 1.0
+    # two detectors on one segment (test_utility.jl:853-868)
+    t = np.array([0.0, 2.0])
+    u = np.array([[0.0, 0, 0, 1, 0, 0], [2.0, 0, 0, 1, 0, 0]])
+    d1 = tp.Disk(tp.Plane((0.5, 0.0, 0.0), (1.0, 0.0, 0.0)), 5.0)
+    d2 = tp.Disk(tp.Plane((1.5, 0.0, 0.0), (1.0, 0.0, 0.0)), 5.0)
+    sums, counts, _, _ = orc.detect(t, u, [2], [d1, d2])
+    assert list(counts) == [1, 1] and np.allclose(sums[:, :2], [[1.0, 1.0], [1.0, 1.0]])
+    # first crossing (test_utility.jl:900-918)
+    lz = _line(0.0, 0.0, 0.0, 0.0, z0=-10.0, vz=1.0)
+    plane = tp.Plane((0.0, 0.0, 0.0), (0.0, 0.0, 1.0))
+    _, _, _, first = orc.detect(*_pack_lines(lz), [plane])
+    assert np.allclose(first[0], [0, 0, 0, 0, 0, 1.0])
+    _, _, _, first = orc.detect(*_pack_lines(lz), [tp.Plane((0.0, 0.0, 20.0), (0.0, 0.0, 1.0))])
+    assert np.all(np.isnan(first[0]))
