@@ -74,6 +74,11 @@ enum {
  *   QUADRATIC  F_i(x,t) = value_i + sum_j jac_ij x_j + sum_jk quad_ijk x_j x_k
  *            + rate_i t (the quadratic test fields of the reference, e.g.
  *            the magnetic bottle of test/test_hybrid.jl:61-68)
+ *   SERIES   LazyTimeInterpolator(times, loader) (src/utility/interpolation.jl:
+ *            337-430): snapshot fields at sorted times, blended linearly in
+ *            time, (1 - w) F_k(x) + w F_{k+1}(x), and clamped to the first /
+ *            last snapshot outside [times[0], times[n-1]].  Every snapshot
+ *            is uploaded and stays resident on the device.
  *   GRID     interpolation of a (3, nx, ny, nz) column-major array:
  *            build_interpolator(gridtype, A, grids..., order, bc)
  *            (src/utility/interpolation.jl:119-311).  The default (a zeroed
@@ -86,7 +91,8 @@ enum {
     TP_FIELD_AFFINE = 2,
     TP_FIELD_DIPOLE = 3,
     TP_FIELD_GRID = 4,
-    TP_FIELD_QUADRATIC = 5
+    TP_FIELD_QUADRATIC = 5,
+    TP_FIELD_SERIES = 6
 };
 
 /* grid boundary handling (FastInterpolations FillExtrap(NaN), ClampExtrap(),
@@ -158,6 +164,10 @@ typedef struct tp_field_desc {
                             axes take LINEAR or CONSTANT order and FILL_NAN
                             or CLAMP boundaries.                            */
     double quad[27];     /* QUADRATIC: quad_ijk at [9 i + 3 j + k]          */
+    int64_t nseries;     /* SERIES: number of snapshots (>= 1)              */
+    const double* series_times;          /* SERIES: nseries sorted times    */
+    const struct tp_field_desc* series;  /* SERIES: nseries snapshot
+                            descriptors (any kind but SERIES)               */
 } tp_field_desc;
 
 /* ---- termination (the reference's `isoutside(u, p, t)` callback) --------

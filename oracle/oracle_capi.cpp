@@ -86,6 +86,23 @@ std::unique_ptr<Field> make_field(const tp_field_desc* d, const orc_field_cb* cb
             f->rate = {d->rate[0], d->rate[1], d->rate[2]};
             return std::unique_ptr<Field>(f);
         }
+        case TP_FIELD_SERIES: {
+            if (d->nseries < 1 || !d->series || !d->series_times) return nullptr;
+            auto* f = new SeriesField();
+            for (int64_t k = 0; k < d->nseries; ++k) {
+                if (d->series[k].kind == TP_FIELD_SERIES) {
+                    delete f;
+                    return nullptr;
+                }
+                f->times.push_back(d->series_times[k]);
+                f->snaps.push_back(make_field(&d->series[k], nullptr));
+                if (!f->snaps.back()) {
+                    delete f;
+                    return nullptr;
+                }
+            }
+            return std::unique_ptr<Field>(f);
+        }
         case TP_FIELD_QUADRATIC: {
             auto* f = new QuadraticField();
             for (int k = 0; k < 3; ++k) {

@@ -610,6 +610,45 @@ struct GeneralGridField : Field {
     }
 };
 
+// LazyTimeInterpolator (src/utility/interpolation.jl:337-430): snapshots at
+// sorted times; k = searchsortedlast(times, t); k == 0 or k == n clamp to the
+// first / last snapshot, otherwise (1 - w) F_k + w F_{k+1}, w = (t - t_k) /
+// (t_{k+1} - t_k); the Jacobian blends the snapshot Jacobians, derivative_t
+// is (F_{k+1} - F_k) / (t_{k+1} - t_k) inside and zero outside.
+struct SeriesField : Field {
+    std::vector<double> times;
+    std::vector<std::unique_ptr<Field>> snaps;
+    int64_t index(double t) const { return std::upper_bound(times.begin(), times.end(), t) - times.begin(); }
+    V3d eval(V3d r, double t) const override {
+        int64_t k = index(t), n = (int64_t)times.size();
+        if (k == 0) return snaps[0]->eval(r, t);
+        if (k >= n) return snaps[n - 1]->eval(r, t);
+        double w = (t - times[k - 1]) / (times[k] - times[k - 1]);
+        V3d a = snaps[k - 1]->eval(r, t), b = snaps[k]->eval(r, t);
+        return (1.0 - w) * a + w * b;
+    }
+    void jac(V3d r, double t, V3d& F, M3& J) const override {
+        int64_t k = index(t), n = (int64_t)times.size();
+        if (k == 0 || k >= n) {
+            snaps[k == 0 ? 0 : n - 1]->jac(r, t, F, J);
+            return;
+        }
+        double w = (t - times[k - 1]) / (times[k] - times[k - 1]);
+        V3d Fa, Fb;
+        M3 Ja, Jb;
+        snaps[k - 1]->jac(r, t, Fa, Ja);
+        snaps[k]->jac(r, t, Fb, Jb);
+        F = (1.0 - w) * Fa + w * Fb;
+        for (int q = 0; q < 9; ++q) J.a[q] = (1.0 - w) * Ja.a[q] + w * Jb.a[q];
+    }
+    V3d dtime(V3d r, double t) const override {
+        int64_t k = index(t), n = (int64_t)times.size();
+        if (k == 0 || k >= n) return {0.0, 0.0, 0.0};
+        V3d a = snaps[k - 1]->eval(r, t), b = snaps[k]->eval(r, t);
+        return (b - a) / (times[k] - times[k - 1]);
+    }
+};
+
 // A field given by C callbacks (the tests' Julia closures restated in Python).
 typedef void (*field_cb)(const double* x, double t, double* out, void* user);
 typedef void (*jac_cb)(const double* x, double t, double* out9, void* user);

@@ -13,7 +13,7 @@ from . import _abi, workloads
 from .constants import (BMoment_Earth, Electron, Ion, MU0_OVER_4PI, Proton, Re, Species, SpeciesDict,
                         c, eV, kB, me, mi, mu0, qe, qi)
 from .fields import (AffineField, CartesianGrid, ClampExtrap, DipoleField, FieldInterpolator, FillExtrap,
-                     PeriodicBC, QuadraticField, RectilinearGrid, StructuredGrid, UniformField, WrapExtrap, ZeroField,
+                     LazyTimeInterpolator, PeriodicBC, QuadraticField, RectilinearGrid, StructuredGrid, UniformField, WrapExtrap, ZeroField,
                      build_interpolator)
 from .problems import (AdaptiveBoris, AdaptiveHybrid, AdaptiveMultistepBoris, Boris, EnsembleB200, EnsembleContext,
                        MultistepBoris, MultistepBoris2, MultistepBoris4, MultistepBoris6, Terminate,

@@ -33,6 +33,7 @@ TP_FIELD_AFFINE = 2
 TP_FIELD_DIPOLE = 3
 TP_FIELD_GRID = 4
 TP_FIELD_QUADRATIC = 5
+TP_FIELD_SERIES = 6
 
 TP_BC_FILL_NAN = 0
 TP_BC_CLAMP = 1
@@ -111,6 +112,9 @@ class FieldDesc(C.Structure):
         ("dir", C.c_int32),
         ("axis", C.c_void_p * 3),
         ("quad", C.c_double * 27),
+        ("nseries", C.c_int64),
+        ("series_times", C.c_void_p),
+        ("series", C.c_void_p),
     ]
 
 

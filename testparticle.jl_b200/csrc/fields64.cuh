@@ -182,10 +182,51 @@ __device__ __forceinline__ D3 quad_eval64(const DevField& f, D3 r, double t) {
     return {o[0], o[1], o[2]};
 }
 
+// ---------------------------------------------------------------- time series
+// LazyTimeInterpolator (src/utility/interpolation.jl:337-430): k = the
+// number of snapshot times <= t (searchsortedlast); k == 0 or k == n clamp
+// to the first / last snapshot, otherwise w = (t - t_k) / (t_{k+1} - t_k)
+// and the value is (1 - w) F_k + w F_{k+1}.  Snapshots are never series.
+__device__ __forceinline__ D3 snapshot_eval64(const DevField& f, D3 r, double t) {
+    if (f.kind == TP_FIELD_GRID) return grid_eval64<true>(f, r);
+    if (f.kind == TP_FIELD_QUADRATIC) return quad_eval64(f, r, t);
+    return analytic_eval64(f, r, t);
+}
+
+__device__ __forceinline__ int series_index(const DevField& f, double t) {
+    int lo = 0, hi = f.nts;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(f.ts + mid) <= t) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static __device__ __noinline__ D3 series_eval64(const DevField& f, D3 r, double t) {
+    const int k = series_index(f, t);
+    if (k == 0) return snapshot_eval64(f.snaps[0], r, t);
+    if (k >= f.nts) return snapshot_eval64(f.snaps[f.nts - 1], r, t);
+    const double t1 = __ldg(f.ts + k - 1), t2 = __ldg(f.ts + k);
+    const double w = (t - t1) / (t2 - t1);
+    D3 a = snapshot_eval64(f.snaps[k - 1], r, t), b = snapshot_eval64(f.snaps[k], r, t);
+    return (1.0 - w) * a + w * b;
+}
+
+// derivative_t: (F_{k+1} - F_k) / (t_{k+1} - t_k) inside, zero outside
+static __device__ __noinline__ D3 series_dtime64(const DevField& f, D3 r, double t) {
+    const int k = series_index(f, t);
+    if (k == 0 || k >= f.nts) return {0.0, 0.0, 0.0};
+    const double t1 = __ldg(f.ts + k - 1), t2 = __ldg(f.ts + k);
+    D3 a = snapshot_eval64(f.snaps[k - 1], r, t), b = snapshot_eval64(f.snaps[k], r, t);
+    return (b - a) / (t2 - t1);
+}
+
 template <bool GEN = true>
 __device__ __forceinline__ D3 field_eval64(const DevField& f, D3 r, double t) {
     if (f.kind == TP_FIELD_GRID) return grid_eval64<GEN>(f, r);
     if (f.kind == TP_FIELD_QUADRATIC) return quad_eval64(f, r, t);
+    if (GEN && f.kind == TP_FIELD_SERIES) return series_eval64(f, r, t);
     return analytic_eval64(f, r, t);
 }
 
@@ -275,7 +316,7 @@ __device__ __forceinline__ bool fields_static(const DevFields& F) {
                (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
     bool b = !((F.B.kind == TP_FIELD_AFFINE || F.B.kind == TP_FIELD_QUADRATIC) &&
                (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
-    return e && b;
+    return e && b && F.E.kind != TP_FIELD_SERIES && F.B.kind != TP_FIELD_SERIES;
 }
 
 // ---------------------------------------------------------------- updates
@@ -377,13 +418,15 @@ __device__ __forceinline__ bool outside64(const DevTerm& T, D3 r, D3 v, double t
 // Field configurations of the float64 Jacobian and value helpers: GM_ANALYTIC
 // (no grids), GM_GRID (trilinear uniform Cartesian grids only), GM_ANY (also
 // the general grids of grid_general.cuh).
-enum { GM_ANALYTIC = 0, GM_GRID = 1, GM_ANY = 2 };
+enum { GM_ANALYTIC = 0, GM_GRID = 1, GM_ANY = 2, GM_LEAF = 3 };  // GM_LEAF: GM_ANY but no series
 
 // the grid mode of a full-orbit kernel's field configuration
 template <int FK>
 struct GMOf {
     static constexpr int value = FK == FK_ANALYTIC ? GM_ANALYTIC : (FK == FK_GENGRID ? GM_ANY : GM_GRID);
 };
+
+static __device__ __noinline__ void series_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]);
 
 template <int GM>
 __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
@@ -436,7 +479,7 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
                 F = {0.0, 0.0, 0.0};
                 return;
             }
-            if (GM == GM_ANY && f.general) {
+            if ((GM == GM_ANY || GM == GM_LEAF) && f.general) {
                 grid_general_jac64(f, r, F, J);
                 return;
             }
@@ -482,15 +525,39 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
 #undef TPB_GJ
             return;
         }
+        case TP_FIELD_SERIES:
+            if (GM == GM_ANY) {
+                series_jac64(f, r, t, F, J);
+                return;
+            }
+            F = {0.0, 0.0, 0.0};
+            return;
         default:
             F = {0.0, 0.0, 0.0};
             return;
     }
 }
 
+// Jacobian of a series: (1 - w) J_k + w J_{k+1} (clamped outside)
+static __device__ __noinline__ void series_jac64(const DevField& f, D3 r, double t, D3& F, double J[9]) {
+    const int k = series_index(f, t);
+    if (k == 0 || k >= f.nts) {
+        field_jac64<GM_LEAF>(f.snaps[k == 0 ? 0 : f.nts - 1], r, t, F, J);
+        return;
+    }
+    const double t1 = __ldg(f.ts + k - 1), t2 = __ldg(f.ts + k);
+    const double w = (t - t1) / (t2 - t1);
+    D3 Fa, Fb;
+    double Ja[9], Jb[9];
+    field_jac64<GM_LEAF>(f.snaps[k - 1], r, t, Fa, Ja);
+    field_jac64<GM_LEAF>(f.snaps[k], r, t, Fb, Jb);
+    F = (1.0 - w) * Fa + w * Fb;
+    for (int q = 0; q < 9; ++q) J[q] = (1.0 - w) * Ja[q] + w * Jb[q];
+}
+
 template <int GM>
 __device__ __forceinline__ D3 field_val64(const DevField& f, D3 r, double t) {
-    if (GM != GM_ANALYTIC) return field_eval64<GM == GM_ANY>(f, r, t);
+    if (GM != GM_ANALYTIC) return field_eval64<GM == GM_ANY || GM == GM_LEAF>(f, r, t);
     return analytic_eval64(f, r, t);
 }
 
@@ -524,8 +591,10 @@ __device__ __forceinline__ MagProps magnetic_properties64(const DevField& f, D3 
 
 // dB/dt of a field: the rate of a time-dependent affine field, else 0
 // (derivative_t, src/prepare.jl:64-74)
-__device__ __forceinline__ D3 field_dtime64(const DevField& f) {
+template <int GM>
+__device__ __forceinline__ D3 field_dtime64(const DevField& f, D3 r, double t) {
     if (f.kind == TP_FIELD_AFFINE || f.kind == TP_FIELD_QUADRATIC) return {f.rate[0], f.rate[1], f.rate[2]};
+    if (GM == GM_ANY && f.kind == TP_FIELD_SERIES) return series_dtime64(f, r, t);
     return {0.0, 0.0, 0.0};
 }
 
@@ -554,7 +623,7 @@ __device__ __forceinline__ void work_rates64(const DevFields& F, D3 r, D3 v, dou
     const double vpar = dot(v, mp.bh);
     const D3 vperp = v - vpar * mp.bh;
     const double mu = m * dot(vperp, vperp) / (2.0 * mp.Bmag);
-    work_terms64(mp, E, field_dtime64(F.B), q, m, vpar, mu, W);
+    work_terms64(mp, E, field_dtime64<GM>(F.B, r, t), q, m, vpar, mu, W);
 }
 
 // guiding centre: state (X, v_par), mu given, m = q / q2m
@@ -567,7 +636,7 @@ __device__ __forceinline__ void work_rates_gc64(const DevFields& F, D3 X, double
         W[0] = W[1] = W[2] = W[3] = 0.0;
         return;
     }
-    work_terms64(mp, E, field_dtime64(F.B), q, q / q2m, vpar, mu, W);
+    work_terms64(mp, E, field_dtime64<GM>(F.B, X, t), q, q / q2m, vpar, mu, W);
 }
 
 }  // namespace tpb

@@ -5,6 +5,7 @@
 // Multistep velocity updates in delta form.
 #pragma once
 
+#include "fields64.cuh"
 #include "grid_general.cuh"
 #include "tp_device.cuh"
 
@@ -224,6 +225,13 @@ static __device__ __noinline__ F3 quad_eval32(const DevField& f, const CPos& p, 
     return {(float)o[0], (float)o[1], (float)o[2]};
 }
 
+// time series: the float64 blend of the compensated position, rounded
+static __device__ __noinline__ F3 series_eval32(const DevField& f, const CPos& p, double t) {
+    D3 r{(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1], (double)p.hi[2] + (double)p.lo[2]};
+    D3 o = series_eval64(f, r, t);
+    return {(float)o.x, (float)o.y, (float)o.z};
+}
+
 template <bool GEN = true>
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
     if (GEN && g.general) return grid_general32(g, p);
@@ -301,9 +309,11 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
         return;
     }
     E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p)
-        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.E, p, t) : analytic_eval32(F.E, p, t);
+        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.E, p, t)
+        : (GEN && F.E.kind == TP_FIELD_SERIES) ? series_eval32(F.E, p, t) : analytic_eval32(F.E, p, t);
     B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p)
-        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.B, p, t) : analytic_eval32(F.B, p, t);
+        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.B, p, t)
+        : (GEN && F.B.kind == TP_FIELD_SERIES) ? series_eval32(F.B, p, t) : analytic_eval32(F.B, p, t);
 }
 
 template <int FK>
@@ -323,7 +333,7 @@ __device__ __forceinline__ bool fields_static32(const DevFields& F) {
                (F.E.rate[0] != 0.0 || F.E.rate[1] != 0.0 || F.E.rate[2] != 0.0));
     bool b = !((F.B.kind == TP_FIELD_AFFINE || F.B.kind == TP_FIELD_QUADRATIC) &&
                (F.B.rate[0] != 0.0 || F.B.rate[1] != 0.0 || F.B.rate[2] != 0.0));
-    return e && b;
+    return e && b && F.E.kind != TP_FIELD_SERIES && F.B.kind != TP_FIELD_SERIES;
 }
 
 // ---------------------------------------------------------------- updates

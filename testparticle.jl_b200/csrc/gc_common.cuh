@@ -32,6 +32,7 @@ struct GCPar {
 __host__ __device__ __forceinline__ int gc_grid_mode(const DevFields& f) {
     const bool ge = f.E.kind == TP_FIELD_GRID, gb = f.B.kind == TP_FIELD_GRID;
     if ((ge && f.E.general) || (gb && f.B.general)) return GM_ANY;
+    if (f.E.kind == TP_FIELD_SERIES || f.B.kind == TP_FIELD_SERIES) return GM_ANY;
     const bool quad = f.E.kind == TP_FIELD_QUADRATIC || f.B.kind == TP_FIELD_QUADRATIC;
     return (ge || gb || quad) ? GM_GRID : GM_ANALYTIC;
 }

@@ -54,6 +54,10 @@ struct tp_field {
     void* d_eb = nullptr;
     void* d_eb32 = nullptr;
     void* d_axis[3] = {nullptr, nullptr, nullptr};  // node coordinates of non-uniform axes
+    // SERIES: owned snapshot fields, their device descriptors and times
+    std::vector<tp_field*> snaps;
+    void* d_snaps = nullptr;
+    void* d_times = nullptr;
 };
 
 // Results stay on the device until tp_result_copy moves them into the
@@ -547,6 +551,52 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
         case TP_FIELD_QUADRATIC:
             for (int k = 0; k < 27; ++k) dv.Q[k] = d->quad[k];
             break;
+        case TP_FIELD_SERIES: {
+            // LazyTimeInterpolator: every snapshot uploaded once, resident
+            const int64_t ns = d->nseries;
+            if (ns < 1 || ns > (1 << 20) || !d->series || !d->series_times) {
+                delete f;
+                return fail(ctx, TP_E_ARG, "a series needs 1 .. 2^20 snapshots with times");
+            }
+            for (int64_t k = 0; k < ns; ++k) {
+                if (!std::isfinite(d->series_times[k]) || (k > 0 && d->series_times[k] < d->series_times[k - 1])) {
+                    delete f;
+                    return fail(ctx, TP_E_ARG, "series times must be finite and sorted");
+                }
+                if (d->series[k].kind == TP_FIELD_SERIES) {
+                    delete f;
+                    return fail(ctx, TP_E_ARG, "a series snapshot cannot be a series");
+                }
+            }
+            f->desc.series = nullptr;
+            f->desc.series_times = nullptr;
+            std::vector<DevField> devs((size_t)ns);
+            for (int64_t k = 0; k < ns; ++k) {
+                tp_field* c = nullptr;
+                int st = tp_field_create(ctx, &d->series[k], &c);
+                if (st != TP_OK) {
+                    tp_field_destroy(f);
+                    return st;
+                }
+                f->snaps.push_back(c);
+                devs[(size_t)k] = c->dev;
+            }
+            cudaError_t e = cudaMalloc(&f->d_snaps, (size_t)ns * sizeof(DevField));
+            if (e == cudaSuccess) e = cudaMalloc(&f->d_times, (size_t)ns * sizeof(double));
+            if (e == cudaSuccess)
+                e = cudaMemcpy(f->d_snaps, devs.data(), (size_t)ns * sizeof(DevField), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess)
+                e = cudaMemcpy(f->d_times, d->series_times, (size_t)ns * sizeof(double), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                int r = cuda_fail(ctx, e, "series upload");
+                tp_field_destroy(f);
+                return r;
+            }
+            dv.snaps = (const DevField*)f->d_snaps;
+            dv.ts = (const double*)f->d_times;
+            dv.nts = (int32_t)ns;
+            break;
+        }
         case TP_FIELD_GRID: {
             std::string why = check_grid_desc(d);
             if (!why.empty()) {
@@ -661,8 +711,10 @@ void tp_field_destroy(tp_field* f) {
     if (!f) return;
     DeviceGuard g(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
-    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_axis[0], f->d_axis[1], f->d_axis[2]})
+    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_axis[0], f->d_axis[1], f->d_axis[2],
+                    f->d_snaps, f->d_times})
         if (p) cudaFree(p);
+    for (tp_field* c : f->snaps) tp_field_destroy(c);
     delete f;
 }
 
@@ -1908,6 +1960,7 @@ struct tp_tape {
 namespace {
 
 bool field_static(const tp_field* f) {
+    if (f->desc.kind == TP_FIELD_SERIES) return false;
     if (f->desc.kind != TP_FIELD_AFFINE && f->desc.kind != TP_FIELD_QUADRATIC) return true;
     return f->desc.rate[0] == 0.0 && f->desc.rate[1] == 0.0 && f->desc.rate[2] == 0.0;
 }

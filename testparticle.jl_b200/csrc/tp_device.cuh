@@ -58,6 +58,11 @@ struct DevField {
     int32_t ndim;
     const double* ax[3];  // device node coordinates of non-uniform axes, else null
     double Q[27];     // quadratic field: Q[9 i + 3 j + k] x_j x_k
+    // time series (LazyTimeInterpolator): snapshots at sorted times
+    const DevField* snaps;
+    const double* ts;
+    int32_t nts;
+    int32_t pad2;
 };
 
 // QUADRATIC field value in float64, in the order of the CPU restatement:
@@ -103,7 +108,8 @@ struct DevTerm {
 enum { FK_ANALYTIC = 0, FK_EBGRID = 1, FK_GENERIC = 2, FK_GENGRID = 3 };
 
 __host__ __device__ __forceinline__ int field_config_of(const DevFields& f) {
-    if ((f.E.kind == TP_FIELD_GRID && f.E.general) || (f.B.kind == TP_FIELD_GRID && f.B.general))
+    if ((f.E.kind == TP_FIELD_GRID && f.E.general) || (f.B.kind == TP_FIELD_GRID && f.B.general) ||
+        f.E.kind == TP_FIELD_SERIES || f.B.kind == TP_FIELD_SERIES)
         return FK_GENGRID;
     if (f.E.kind == TP_FIELD_QUADRATIC || f.B.kind == TP_FIELD_QUADRATIC) return FK_GENERIC;
     if (f.eb && !f.eb_f64) return FK_EBGRID;  // float interleaved table

@@ -396,6 +396,43 @@ def build_interpolator(*args, dir: int = 1, coeffs=None):
                              axes=tuple(a[3] for a in ax))
 
 
+class LazyTimeInterpolator(AbstractField):
+    """LazyTimeInterpolator(times, loader) (src/utility/interpolation.jl:337-430).
+
+    `loader(i)` (1-based, as in the reference) returns the field at times[i];
+    the field at time t blends the two snapshots around t linearly and is
+    clamped to the first / last snapshot outside the times.  The reference
+    loads snapshots on demand and keeps two; here every snapshot is loaded
+    once and stays resident on the device (HBM holds hundreds of 128^3 grids).
+    """
+
+    time_dependent = True
+
+    def __init__(self, times, loader):
+        self.times = np.ascontiguousarray(np.asarray(times, dtype=np.float64).reshape(-1))
+        if self.times.size < 1:
+            raise ValueError("LazyTimeInterpolator needs at least one time")
+        if np.any(np.diff(self.times) < 0):
+            raise ValueError("times must be sorted")
+        self.snapshots = [as_field(loader(i + 1)) for i in range(self.times.size)]
+        if any(isinstance(f, LazyTimeInterpolator) for f in self.snapshots):
+            raise ValueError("a snapshot cannot be a LazyTimeInterpolator")
+
+    def descriptor(self):
+        descs = [f.descriptor() for f in self.snapshots]
+        arr = (_abi.FieldDesc * len(descs))(*descs)
+        self._arr = arr  # the descriptor array must outlive the upload
+        d = _abi.FieldDesc()
+        d.kind = _abi.TP_FIELD_SERIES
+        d.nseries = len(descs)
+        d.series_times = self.times.ctypes.data
+        d.series = C.cast(arr, C.c_void_p).value
+        return d
+
+    def keepalive(self):
+        return (self.times, getattr(self, "_arr", None), [f.keepalive() for f in self.snapshots])
+
+
 def as_field(f) -> AbstractField:
     """Normalise a user field argument to a device-evaluable field."""
     if isinstance(f, AbstractField):

@@ -155,10 +155,14 @@ struct TpFieldDesc
     order::Int32; geometry::Int32; ndim::Int32; dir::Int32
     axis::NTuple{3, Ptr{Float64}}
     quad::NTuple{27, Float64}   # QUADRATIC: quad_ijk at 9i + 3j + k (0-based)
+    nseries::Int64              # SERIES: snapshots, their times and descriptors
+    series_times::Ptr{Float64}
+    series::Ptr{Cvoid}
 end
 TpFieldDesc(kind, bc, dtype, reserved, value, jac, rate, moment, center, coef, n, origin, spacing, data) =
     TpFieldDesc(kind, bc, dtype, reserved, value, jac, rate, moment, center, coef, n, origin, spacing, data,
-        0, 0, 0, 0, (Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL)), ntuple(_ -> 0.0, 27))
+        0, 0, 0, 0, (Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL), Ptr{Float64}(C_NULL)), ntuple(_ -> 0.0, 27),
+        0, Ptr{Float64}(C_NULL), C_NULL)
 struct TpTermDesc
     flags::Int32; reserved::Int32; rmin::Float64; rmax::Float64
     lo::NTuple{3, Float64}; hi::NTuple{3, Float64}; tmax::Float64

@@ -242,3 +242,70 @@ def test_gc_cubic_grid_rk45(tp, orc):
         r = orc.gc_run(p.desc, p.E, p.B, p.y0, p.q_i, p.q2m_i, p.mu_i)
         assert np.array_equal(s.nsaved, r.nsaved)
         assert _rel_rows(s.u_all[:, :3], r.u[:, :3]) <= (1e-12 if alg == "rk4" else 1e-9)
+
+
+# ------------------------------------------------------------------ time series (LazyTimeInterpolator)
+def _series(tp, nsnap=5, n=16, order=1):
+    """Snapshots of the turbulent box whose fluctuation amplitude grows in time."""
+    dx = 1.0e5
+    Ea, Ba, L = tp.workloads.turbulent_grid(n, dx, 5.0e-9, nmodes=8)
+    x = np.arange(n) * dx
+    B0 = np.zeros_like(Ba)
+    B0[2] = 5.0e-9
+    times = np.linspace(0.0, 40.0, nsnap)
+
+    def loader(i):
+        a = (i - 1) / max(nsnap - 1, 1)
+        return tp.build_interpolator((B0 + a * (Ba - B0)).astype(np.float64), x, x, x, order,
+                                     tp.PeriodicBC("exclusive"))
+
+    return tp.LazyTimeInterpolator(times, loader), L
+
+
+def test_series_eval_points_and_work_match_oracle(tp, orc):
+    B, L = _series(tp)
+    rng = np.random.default_rng(1)
+    n = 4096
+    u = np.concatenate([rng.uniform(0, L, (n, 3)), rng.normal(0, 1e5, (n, 3))], axis=1)
+    t = rng.uniform(-5.0, 45.0, n)   # before, inside and after the snapshot times
+    ctx = tp.Context.get(0)
+    E = tp.UniformField((0.0, 1.0e-4, 0.0))
+    out = ctx.eval_points(E, B, u, t, gc=False, want=3, q2m=tp.qi / tp.mi, m=tp.mi)
+    for k in range(0, n, 97):
+        ref, J = orc.field_eval(B, u[k, :3], t[k], jacobian=True)
+        assert _rel_rows(out[k:k + 1, 3:6], ref) <= 1e-13
+    # the betatron term follows dB/dt of the series: nonzero inside, zero outside
+    inside = (t > 0.0) & (t < 40.0)
+    assert np.any(out[inside, 9] != 0.0) and np.all(out[~inside, 9] == 0.0)
+
+
+def test_series_boris_and_gc_match_oracle(tp, orc):
+    B, L = _series(tp)
+    rng = np.random.default_rng(6)
+    n = 256
+    u0 = np.empty((6, n))
+    u0[:3] = rng.uniform(0.0, L, (3, n))
+    u0[3:] = rng.normal(0.0, 1.0e5, (3, n))
+    dt = tp.get_gyroperiod(5.0e-9) / 40
+    prob = tp.TraceProblem(u0, (0.0, 120 * dt), tp.prepare(tp.ZeroField(), B))
+    kw = dict(dt=dt, savestepinterval=30, save_work=True)
+    sols = tp.solve(prob, tp.Boris(), **kw)
+    plan = tp.plan_boris(prob, tp.Boris(), **kw)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0)
+    assert np.array_equal(sols.nsaved, ref.nsaved)
+    assert _rel_rows(sols.u_all[:, :3], ref.u[:, :3]) <= 1e-13
+    assert _rel_rows(sols.u_all[:, 3:6], ref.u[:, 3:6]) <= 1e-13
+    d = np.linalg.norm(sols.u_all[:, 6:10] - ref.u[:, 6:10], axis=1)
+    assert np.all(d <= 1e-12 * np.linalg.norm(ref.u[:, 6:10], axis=1) + 1e-30)
+    s32 = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=dt, savestepinterval=30)
+    e = np.linalg.norm(s32.final_states()[:, :3] - ref.final_states()[:, :3], axis=1)
+    assert np.median(e) <= 1e-5 * L
+    xv = np.concatenate([u0[:3].T, u0[3:].T], axis=1)
+    y0, mu = orc.gc_prepare(tp.ZeroField(), B, xv, tp.qi, tp.mi)
+    gprob = tp.TraceGCProblem(y0.T.copy(), (0.0, 30.0), (tp.qi, tp.qi / tp.mi, mu, tp.ZeroField(), B))
+    gkw = dict(dt=0.05, alg="rk4", savestepinterval=100)
+    gs = tp.solve(gprob, **gkw)
+    gp = tp.plan_gc(gprob, **gkw)
+    gr = orc.gc_run(gp.desc, gp.E, gp.B, gp.y0, gp.q_i, gp.q2m_i, gp.mu_i)
+    assert np.array_equal(gs.nsaved, gr.nsaved)
+    assert _rel_rows(gs.u_all[:, :3], gr.u[:, :3]) <= 1e-12

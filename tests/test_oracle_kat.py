@@ -690,3 +690,49 @@ def test_detector_kats(tp, orc):
     assert np.allclose(first[0], [0, 0, 0, 0, 0, 1.0])
     _, _, _, first = orc.detect(*_pack_lines(lz), [tp.Plane((0.0, 0.0, 20.0), (0.0, 0.0, 1.0))])
     assert np.all(np.isnan(first[0]))
+
+
+# ------------------------------------------------------------------ LazyTimeInterpolator
+def test_lazy_time_interpolator_kats(tp, orc):
+    # test_utility.jl:316-405: E = t * x snapshots at t = 0, 1, 2
+    times = [0.0, 1.0, 2.0]
+    itp = tp.LazyTimeInterpolator(times, lambda i: tp.AffineField((0.0, 0.0, 0.0), np.eye(3) * times[i - 1]))
+    x = [1.0, 2.0, 3.0]
+    for t, ref in [(0.0, [0, 0, 0]), (1.0, [1, 2, 3]), (0.5, [0.5, 1.0, 1.5]), (1.5, [1.5, 3.0, 4.5])]:
+        assert np.allclose(orc.field_eval(itp, x, t)[0], ref, rtol=1e-14, atol=0)
+    assert np.array_equal(orc.field_eval(itp, x, 3.0), orc.field_eval(itp, x, 2.0))
+    assert np.array_equal(orc.field_eval(itp, x, -1.0), orc.field_eval(itp, x, 0.0))
+    # numerical snapshots: B = (1, 0, 0) at t = 0, (0, 2, 0) at t = 1
+    g = np.linspace(0.0, 1.0, 4)
+    B0 = np.zeros((3, 4, 4, 4))
+    B0[0] = 1.0
+    B1 = np.zeros((3, 4, 4, 4))
+    B1[1] = 2.0
+    itp = tp.LazyTimeInterpolator([0.0, 1.0], lambda i: tp.build_interpolator(B0 if i == 1 else B1, g, g, g))
+    pt = [0.5, 0.5, 0.5]
+    for t, ref in [(0.0, [1, 0, 0]), (1.0, [0, 2, 0]), (0.5, [0.5, 1.0, 0]), (0.25, [0.75, 0.5, 0])]:
+        assert np.allclose(orc.field_eval(itp, pt, t)[0], ref, rtol=1e-14, atol=1e-15)
+
+
+def test_lazy_time_interpolator_derivatives(tp, orc):
+    # test_derivatives.jl:57-90: Jacobian and d/dt against finite differences,
+    # clamped Jacobians and zero d/dt outside the times
+    times = [0.0, 1.0, 2.0]
+    itp = tp.LazyTimeInterpolator(times, lambda i: tp.AffineField((0.0, 0.0, 0.0), np.eye(3) * times[i - 1]))
+    pos = np.array([1.0, 2.0, 3.0])
+    _, J = orc.field_eval(itp, pos, 0.5, jacobian=True)
+    assert np.allclose(J[0], 0.5 * np.eye(3))
+    _, Jm = orc.field_eval(itp, pos, -1.0, jacobian=True)
+    _, J0 = orc.field_eval(itp, pos, 0.0, jacobian=True)
+    _, J3 = orc.field_eval(itp, pos, 3.0, jacobian=True)
+    _, J2 = orc.field_eval(itp, pos, 2.0, jacobian=True)
+    assert np.array_equal(Jm, J0) and np.array_equal(J3, J2)
+    # betatron work uses d|B|/dt: B(t) = t x along a unit x -> dB/dt = x inside, 0 outside
+    B = tp.LazyTimeInterpolator(times, lambda i: tp.UniformField((0.0, 0.0, 1.0 + times[i - 1])))
+    prob = tp.TraceProblem([0.0, 0.0, 0.0, 1.0, 0.0, 0.0], (0.0, 0.5),
+                           (1.0, 1.0, tp.ZeroField(), tp.ZeroField(), tp.ZeroField()))
+    plan = tp.plan_boris(prob, tp.Boris(), dt=0.1, save_work=True)
+    r = orc.boris_run(plan.desc, tp.ZeroField(), B, plan.u0)
+    _, u = r.traj(0)
+    # P_betatron = mu dB/dt . b with mu = |v_perp|^2 / (2 |B|), dB/dt = (0, 0, 1)
+    assert np.all(u[:, 9] > 0.0)
