@@ -19,7 +19,6 @@
 //    of the cancellation the Taylor branch (multistep_boris.jl:99-108) guards;
 //  * time t, the adaptive step dt = C/|B| and the end-of-span clipping in
 //    float64 so that step decisions follow the float64 controller.
-#include "fields64.cuh"
 #include "fp32c_common.cuh"
 #include "tp_device.cuh"
 #include "tp_launch.h"
@@ -57,13 +56,26 @@ template <int FK>
 struct Saver32 {
     const BorisArgs& a;
     int W;
+    // slot width: the state, E and B (float evaluation, as the push sees
+    // them) when save_fields, and four work-rate columns when save_work that
+    // a post-pass over the saved states fills (keeps that float64 code out
+    // of this kernel's registers)
     __device__ Saver32(const BorisArgs& a_)
         : a(a_), W(6 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
-    // columns after the state: E and B (float evaluation, as the push sees
-    // them) when save_fields, then the work rates (float64, from the state
-    // rounded to float64) when save_work
-    __device__ __forceinline__ void extras(double* u, const CPos& p, const double* x, double t) const {
+    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, const CV& v, double t) const {
+        if (k >= a.nslots) {
+            set_status(a.status, TP_E_OVERFLOW);
+            return;
+        }
         const int64_t n = a.n;
+        a.t_out[k * n + i] = t;
+        double* u = a.u_out + (k * W) * n + i;
+        u[0 * n] = cpos_value(a, p, 0);
+        u[1 * n] = cpos_value(a, p, 1);
+        u[2 * n] = cpos_value(a, p, 2);
+        u[3 * n] = (double)v.h.x + (double)v.l.x;
+        u[4 * n] = (double)v.h.y + (double)v.l.y;
+        u[5 * n] = (double)v.h.z + (double)v.l.z;
         if (a.save_fields) {
             F3 E, B;
             eval_EB32t<FK>(a.f, p, t, E, B);
@@ -74,26 +86,6 @@ struct Saver32 {
             u[10 * n] = B.y;
             u[11 * n] = B.z;
         }
-        if (a.save_work) {
-            double w[4];
-            work_rates64<GMOf<FK>::value>(a.f, D3{x[0], x[1], x[2]}, D3{x[3], x[4], x[5]}, t, a.q2m, a.m, w);
-            const int c0 = a.save_fields ? 12 : 6;
-            for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
-        }
-    }
-    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, const CV& v, double t) const {
-        if (k >= a.nslots) {
-            set_status(a.status, TP_E_OVERFLOW);
-            return;
-        }
-        const int64_t n = a.n;
-        a.t_out[k * n + i] = t;
-        double* u = a.u_out + (k * W) * n + i;
-        const double x[6] = {cpos_value(a, p, 0), cpos_value(a, p, 1), cpos_value(a, p, 2),
-                             (double)v.h.x + (double)v.l.x, (double)v.h.y + (double)v.l.y,
-                             (double)v.h.z + (double)v.l.z};
-        for (int c = 0; c < 6; ++c) u[c * n] = x[c];
-        extras(u, p, x, t);
     }
 };
 
@@ -154,7 +146,12 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
                 if (a.nslots > 0) {
                     double* u = a.u_out + i;
                     for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
-                    S.extras(u, p, u0, a.t0);
+                    if (a.save_fields) {
+                        F3 E, B;
+                        eval_EB32t<FK>(a.f, p, a.t0, E, B);
+                        u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                        u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                    }
                 } else {
                     set_status(a.status, TP_E_OVERFLOW);
                 }
@@ -266,7 +263,10 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
                     a.t_out[i] = t;
                     double* u = a.u_out + i;
                     for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
-                    S.extras(u, p, u0, t);
+                    if (a.save_fields) {
+                        u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                        u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                    }
                 } else {
                     set_status(a.status, TP_E_OVERFLOW);
                 }

@@ -31,8 +31,9 @@ struct Saver64 {
     int W;
     __device__ Saver64(const BorisArgs& a_)
         : a(a_), W(6 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
-    // slot k of particle i: state, then E and B at (r, t) when save_fields,
-    // then the work rates when save_work (_prepare_saved_data, boris.jl:405-440)
+    // slot k of particle i: state, then E and B at (r, t) when save_fields
+    // (_prepare_saved_data, boris.jl:405-440); the four work-rate columns of
+    // save_work are filled by a post-pass over the saved states
     __device__ __forceinline__ void save(int64_t i, int64_t k, D3 r, D3 v, double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
@@ -56,12 +57,6 @@ struct Saver64 {
             u[9 * n] = B.x;
             u[10 * n] = B.y;
             u[11 * n] = B.z;
-        }
-        if (a.save_work) {
-            double w[4];
-            work_rates64<GMOf<FK>::value>(a.f, r, v, t, a.q2m, a.m, w);
-            const int c0 = a.save_fields ? 12 : 6;
-            for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
     }
 };

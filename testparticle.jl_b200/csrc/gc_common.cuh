@@ -89,8 +89,9 @@ struct GCSaver {
     int W;
     __device__ GCSaver(const GCArgs& a_)
         : a(a_), W(4 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
-    // slot k: (X, v_par), then E and B when save_fields, then the work rates
-    // when save_work (_prepare_saved_data_gc, src/gc/gc_solver.jl:233-248)
+    // slot k: (X, v_par), then E and B when save_fields
+    // (_prepare_saved_data_gc, src/gc/gc_solver.jl:233-248); the four
+    // work-rate columns of save_work are filled by a post-pass
     __device__ __forceinline__ void save(int64_t i, int64_t k, const G4& s, double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
@@ -109,13 +110,6 @@ struct GCSaver {
             u[7 * n] = B.x;
             u[8 * n] = B.y;
             u[9 * n] = B.z;
-        }
-        if (a.save_work) {
-            const GCPar p = gc_par(a, i);
-            double w[4];
-            work_rates_gc64<GM>(a.f, X, s.y[3], t, p.q, p.q2m, p.mu, w);
-            const int c0 = a.save_fields ? 10 : 4;
-            for (int c = 0; c < 4; ++c) u[(c0 + c) * n] = w[c];
         }
     }
 };

@@ -71,6 +71,39 @@ __global__ void k_eval_points(PointsArgs a) {
     }
 }
 
+// save_work columns (_prepare_saved_data, src/boris/boris.jl:429-437;
+// gc_solver.jl:233-248): the work rates of every saved state, one thread per
+// (slot, particle), written after the push so the push kernels carry no
+// Jacobian code
+__global__ void k_fill_work(WorkFillArgs a) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.nslots * a.n) return;
+    const int64_t k = idx / a.n, i = idx - k * a.n;
+    if (k >= a.nsaved[i]) return;
+    const int64_t n = a.n;
+    double* u = a.u_out + (k * a.W) * n + i;
+    const double t = a.t_out[k * n + i];
+    const D3 x{u[0], u[n], u[2 * n]};
+    double W[4];
+    if (a.gc) {
+        const double q = a.q_i ? a.q_i[i] : a.q;
+        const double q2m = a.q2m_i ? a.q2m_i[i] : a.q2m;
+        const double mu = a.mu_i ? a.mu_i[i] : a.mu;
+        work_rates_gc64<GM_ANY>(a.f, x, u[3 * n], t, q, q2m, mu, W);
+    } else {
+        work_rates64<GM_ANY>(a.f, x, D3{u[3 * n], u[4 * n], u[5 * n]}, t, a.q2m, a.m, W);
+    }
+    for (int c = 0; c < 4; ++c) u[(int64_t)(a.c0 + c) * n] = W[c];
+}
+
+cudaError_t launch_fill_work(const WorkFillArgs& a, cudaStream_t s) {
+    const int64_t total = a.nslots * a.n;
+    if (total <= 0) return cudaSuccess;
+    const int block = 128;
+    k_fill_work<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
     int block = 128;

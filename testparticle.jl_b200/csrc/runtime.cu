@@ -841,6 +841,22 @@ int issue_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, const La
     cudaError_t e = d->precision == TP_PREC_FP32C ? launch_boris_fp32c(a, cfg, s)
                                                   : launch_boris_fp64(a, cfg, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "push kernel launch");
+    if (a.save_work && a.nslots > 0) {
+        WorkFillArgs w;
+        std::memset(&w, 0, sizeof(w));
+        w.f = a.f;
+        w.t_out = a.t_out;
+        w.u_out = a.u_out;
+        w.nsaved = a.nsaved;
+        w.n = a.n;
+        w.nslots = a.nslots;
+        w.c0 = a.save_fields ? 12 : 6;
+        w.W = w.c0 + 4;
+        w.q2m = a.q2m;
+        w.m = a.m;
+        e = launch_fill_work(w, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "work-rate pass");
+    }
     return TP_OK;
 }
 
@@ -1843,6 +1859,26 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, s);
         if (n > 0) e = launch_gc(a, cfg, s);
+        if (e == cudaSuccess && n > 0 && a.save_work && a.nslots > 0) {
+            WorkFillArgs w;
+            std::memset(&w, 0, sizeof(w));
+            w.f = a.f;
+            w.t_out = a.t_out;
+            w.u_out = a.u_out;
+            w.nsaved = a.nsaved;
+            w.n = a.n;
+            w.nslots = a.nslots;
+            w.c0 = a.save_fields ? 10 : 4;
+            w.W = w.c0 + 4;
+            w.gc = 1;
+            w.q = a.q;
+            w.q2m = a.q2m;
+            w.mu = a.mu;
+            w.q_i = a.q_i;
+            w.q2m_i = a.q2m_i;
+            w.mu_i = a.mu_i;
+            e = launch_fill_work(w, s);
+        }
         cudaEventRecord(ev1, s);
         int32_t status = 0;
         if (e == cudaSuccess) e = cudaMemcpyAsync(&status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);

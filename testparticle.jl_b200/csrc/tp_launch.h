@@ -51,6 +51,22 @@ struct GCPrepArgs {
     double* mu;
 };
 
+// the work-rate columns of save_work, filled after a push over its saved
+// states (slot-major: t[k n + i], u[(k W + c) n + i]) (gc_fp64.cu)
+struct WorkFillArgs {
+    DevFields f;
+    const double* t_out;
+    double* u_out;
+    const int32_t* nsaved;
+    int64_t n, nslots;
+    int32_t W, c0, gc, pad;
+    double q2m, m;           // full orbit
+    double q, mu;            // guiding centre (scalars)
+    const double* q_i;       // guiding centre, per particle (optional)
+    const double* q2m_i;
+    const double* mu_i;
+};
+
 // adaptive hybrid GC / full-orbit solve (hybrid.cu)
 struct HybridArgs {
     DevFields f;
@@ -130,6 +146,7 @@ cudaError_t launch_gc_fp32(const GCArgs& a, const LaunchCfg& c, cudaStream_t s);
 int occupancy_gc(const GCArgs& a, int block);
 cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
+cudaError_t launch_fill_work(const WorkFillArgs& a, cudaStream_t s);
 cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s);
 // virtual detectors (detect.cu): mode 0 fluxes (tot: nsurf x 4 sums on the
 // device), 1 crossings (counts on the host; *rows_d_out: device rows the
