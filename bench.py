@@ -380,6 +380,88 @@ def leg_gc(tp, n):
     return out
 
 
+def leg_next_rows(tp, n=1 << 20, nt=1000):
+    """Throughput of the rows beyond the drop-in path (device time of solve()):
+    cubic and nearest-node grids and a field time series on the config-2 box,
+    the dipole sampled on a spherical grid, the adaptive hybrid in a magnetic
+    bottle, and the virtual detectors over saved trajectories."""
+    import math
+    out = {}
+    w = tp.workloads.config2(n=n, nt=nt, ssi=nt)
+    dx = 1.0e5
+    g = np.arange(128) * dx
+    Ea, Ba, _L = tp.workloads.turbulent_grid(128, dx, 5.0e-9)
+
+    def rate(sol):
+        return sol.particle_steps() / sol.elapsedTime
+
+    for order in (3, 0):
+        E = tp.build_interpolator(Ea, g, g, g, order, tp.PeriodicBC("exclusive"))
+        B = tp.build_interpolator(Ba, g, g, g, order, tp.PeriodicBC("exclusive"))
+        prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(E, B))
+        r = {}
+        for prec in ("fp32c", "fp64"):
+            r[prec] = rate(tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision=prec), dt=w.dt,
+                                    savestepinterval=nt))
+        out[f"config2_order{order}"] = {**r, "unit": "particle-steps/s", "particles": n, "time_steps": nt}
+    # a 4-snapshot time series of the config-2 fields (linear in time)
+    times = np.linspace(0.0, float(w.tspan[1]), 4)
+
+    def loader(Af):
+        return lambda i: tp.build_interpolator(Af * (0.7 + 0.1 * i), g, g, g, 1, tp.PeriodicBC("exclusive"))
+
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(tp.LazyTimeInterpolator(times, loader(Ea)),
+                                                     tp.LazyTimeInterpolator(times, loader(Ba))))
+    out["config2_series4"] = {prec: rate(tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision=prec), dt=w.dt,
+                                                  savestepinterval=nt)) for prec in ("fp32c", "fp64")}
+    out["config2_series4"]["unit"] = "particle-steps/s"
+    # the Earth dipole on a 64 x 64 x 96 spherical grid (linear), config-3 particles
+    w3 = tp.workloads.config3(n=n, nt=nt, ssi=nt)
+    r_ = np.geomspace(0.8 * tp.Re, 20.0 * tp.Re, 64)
+    th = np.linspace(0.0, math.pi, 64)
+    ph = np.linspace(0.0, 2 * math.pi, 96)
+    R, T, _P = np.meshgrid(r_, th, ph, indexing="ij")
+    k = tp.MU0_OVER_4PI * 8.0e22 / R ** 3
+    A = np.zeros((3,) + R.shape)
+    A[0] = -2.0 * k * np.cos(T)
+    A[1] = -k * np.sin(T)
+    Bs = tp.build_interpolator(tp.StructuredGrid, A.astype(np.float32), r_, th, ph)
+    prob = tp.TraceProblem(w3.u0, w3.tspan, tp.prepare(tp.ZeroField(), Bs))
+    out["config3_spherical_grid"] = {
+        prec: rate(tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision=prec), dt=w3.dt, tend=w3.tend,
+                            savestepinterval=nt, isoutside=w3.isoutside)) for prec in ("fp32c", "fp64")}
+    out["config3_spherical_grid"]["unit"] = "particle-steps/s"
+    # adaptive hybrid in the bottle of test_hybrid.jl, 2^18 protons, 30 gyroperiods
+    B0, alpha = 1.0e-4, 1.0e-2
+    Tg = 2 * math.pi / (tp.qi / tp.mi * B0)
+    rng = np.random.default_rng(3)
+    nh = 1 << 18
+    u0 = np.zeros((6, nh))
+    u0[:3] = rng.normal(0.0, 0.5, (3, nh))
+    vp = rng.uniform(2.0e4, 8.0e4, nh)
+    phs = rng.uniform(0, 2 * math.pi, nh)
+    u0[3], u0[4], u0[5] = vp * np.cos(phs), vp * np.sin(phs), rng.uniform(-1.2e5, 1.2e5, nh)
+    prob = tp.TraceHybridProblem(u0, (0.0, 30 * Tg), tp.prepare(tp.ZeroField(), tp.QuadraticField.bottle(B0, alpha)))
+    sh = tp.solve(prob, tp.AdaptiveHybrid(threshold=0.1, dtmax=Tg, dtmin=1e-4 * Tg, check_interval=100),
+                  savestepinterval=1000)
+    out["hybrid_bottle"] = {"value": rate(sh), "unit": "particle-steps/s", "particles": nh,
+                            "steps_mean": float(sh.nsteps.mean())}
+    # detectors over the saves of a config-2 FP64 run (1e6 x 11 saves)
+    ws = tp.workloads.config2(n=n, nt=nt, ssi=nt // 10)
+    sol = tp.solve(tp.TraceProblem(ws.u0, ws.tspan, tp.prepare(ws.E, ws.B)), tp.Boris(), dt=ws.dt,
+                   savestepinterval=nt // 10)
+    L = 128 * dx
+    surfs = [tp.Disk(tp.Plane((L / 2, L / 2, L / 2), (1.0, 0.0, 0.0)), L / 4), tp.Sphere((L / 2, L / 2, L / 2), L / 3)]
+    t0 = time.perf_counter()
+    nf, _vf = tp.get_particle_fluxes(sol, surfs, 1.0)
+    el = time.perf_counter() - t0
+    segs = float(np.maximum(sol.nsaved - 1, 0).sum()) * len(surfs)
+    out["detectors_config2_saves"] = {"segment_surface_checks_per_s": segs / el, "wall_s": el,
+                                      "includes": "host -> device copy of the saved trajectories",
+                                      "n_flux": [float(x) for x in nf]}
+    return out
+
+
 def profile_case(tp, case, device):
     """Small untimed runs of the adaptive and guiding-centre kernels, for ncu captures."""
     if case == "adaptive":
@@ -413,6 +495,8 @@ def main():
     ap.add_argument("--no-legs", action="store_true", help="skip the dipole / guiding-centre legs")
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (profiling)")
+    ap.add_argument("--next-rows", action="store_true",
+                    help="also time the general grids, field series, hybrid and detectors")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling)")
     ap.add_argument("--profile-case", choices=["adaptive", "gc"], default=None,
                     help="run one small untimed case for an ncu capture: AdaptiveBoris(0.1) in the dipole "
@@ -522,6 +606,8 @@ def main():
         if rank == 0:
             legs["guiding_centre_config4"] = leg_gc(tp, 1 << 20)
         legs["adjoint_config5"] = leg_adjoint(tp, torch, ctx, dev, stream, flush)
+    if args.next_rows and rank == 0:
+        legs["next_rows"] = leg_next_rows(tp)
 
     if rank == 0:
         cpu = None
