@@ -138,9 +138,11 @@ class BorisAdjointFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, u0, e_val, b_val, spec):
         E_in, B_in, desc, device = spec
-        torch.cuda.current_stream(device).synchronize()  # field uploads run on the library's stream
         E = _proxy(E_in, e_val)
         B = _proxy(B_in, b_val)
+        # the proxies' device copies are made on torch's stream and the field
+        # uploads read them on the library's stream
+        torch.cuda.current_stream(device).synchronize()
         lib_ctx = Context.get(device)
         u0c = u0.detach().to(torch.float64).contiguous()
         n = u0c.shape[0]

@@ -143,7 +143,7 @@ static __device__ __noinline__ void grid_general_jac64(const DevField& g, D3 r, 
 // specialised for trilinear grids keep the general code out of their body)
 template <bool GEN = true>
 __device__ __forceinline__ D3 grid_eval64(const DevField& g, D3 r) {
-    if (GEN && g.general) return grid_general64(g, r);
+    if (GEN && g.general) return grid_general64(*g.self, r);
     Ax ax, ay, az;
     if (!grid_axes64(g, r, ax, ay, az)) return nan3();
     return tri64(g, g.tab, g.f64 != 0, 1, 0, ax, ay, az);
@@ -226,7 +226,7 @@ template <bool GEN = true>
 __device__ __forceinline__ D3 field_eval64(const DevField& f, D3 r, double t) {
     if (f.kind == TP_FIELD_GRID) return grid_eval64<GEN>(f, r);
     if (f.kind == TP_FIELD_QUADRATIC) return quad_eval64(f, r, t);
-    if (GEN && f.kind == TP_FIELD_SERIES) return series_eval64(f, r, t);
+    if (GEN && f.kind == TP_FIELD_SERIES) return series_eval64(*f.self, r, t);
     return analytic_eval64(f, r, t);
 }
 
@@ -480,7 +480,7 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
                 return;
             }
             if ((GM == GM_ANY || GM == GM_LEAF) && f.general) {
-                grid_general_jac64(f, r, F, J);
+                grid_general_jac64(*f.self, r, F, J);
                 return;
             }
             Ax ax, ay, az;
@@ -527,7 +527,7 @@ __device__ __forceinline__ void field_jac64(const DevField& f, D3 r, double t, D
         }
         case TP_FIELD_SERIES:
             if (GM == GM_ANY) {
-                series_jac64(f, r, t, F, J);
+                series_jac64(*f.self, r, t, F, J);
                 return;
             }
             F = {0.0, 0.0, 0.0};
@@ -594,7 +594,7 @@ __device__ __forceinline__ MagProps magnetic_properties64(const DevField& f, D3 
 template <int GM>
 __device__ __forceinline__ D3 field_dtime64(const DevField& f, D3 r, double t) {
     if (f.kind == TP_FIELD_AFFINE || f.kind == TP_FIELD_QUADRATIC) return {f.rate[0], f.rate[1], f.rate[2]};
-    if (GM == GM_ANY && f.kind == TP_FIELD_SERIES) return series_dtime64(f, r, t);
+    if (GM == GM_ANY && f.kind == TP_FIELD_SERIES) return series_dtime64(*f.self, r, t);
     return {0.0, 0.0, 0.0};
 }
 

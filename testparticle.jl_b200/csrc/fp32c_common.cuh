@@ -234,7 +234,7 @@ static __device__ __noinline__ F3 series_eval32(const DevField& f, const CPos& p
 
 template <bool GEN = true>
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
-    if (GEN && g.general) return grid_general32(g, p);
+    if (GEN && g.general) return grid_general32(*g.self, p);
     AxF ax, ay, az;
     if (!axes32(g, p, ax, ay, az)) return nanf3();
     const float4* T = g.tab32;
@@ -309,11 +309,11 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
         return;
     }
     E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p)
-        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.E, p, t)
-        : (GEN && F.E.kind == TP_FIELD_SERIES) ? series_eval32(F.E, p, t) : analytic_eval32(F.E, p, t);
+        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.E.self, p, t)
+        : (GEN && F.E.kind == TP_FIELD_SERIES) ? series_eval32(*F.E.self, p, t) : analytic_eval32(F.E, p, t);
     B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p)
-        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(F.B, p, t)
-        : (GEN && F.B.kind == TP_FIELD_SERIES) ? series_eval32(F.B, p, t) : analytic_eval32(F.B, p, t);
+        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.B.self, p, t)
+        : (GEN && F.B.kind == TP_FIELD_SERIES) ? series_eval32(*F.B.self, p, t) : analytic_eval32(F.B, p, t);
 }
 
 template <int FK>

@@ -58,6 +58,7 @@ struct tp_field {
     std::vector<tp_field*> snaps;
     void* d_snaps = nullptr;
     void* d_times = nullptr;
+    void* d_self = nullptr;  // the DevField in device memory (DevField::self)
 };
 
 // Results stay on the device until tp_result_copy moves them into the
@@ -378,6 +379,9 @@ int make_dev_fields(tp_ctx* ctx, const tp_field* E, tp_field* B, DevFields& F) {
                 if (e == cudaSuccess)
                     e = launch_pack_node_table(B->d_raw, 1, B->nodes, B->d_eb32, 0, 2, 1, ctx->stream);
             }
+            // the table is complete before any launch reads it: the entries
+            // that take the caller's stream are not ordered after this one
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
             if (e != cudaSuccess) return cuda_fail(ctx, e, "interleaved field table");
             B->eb_partner = E->id;
         }
@@ -680,6 +684,18 @@ int tp_field_create(tp_ctx* ctx, const tp_field_desc* d, tp_field** out) {
             return fail(ctx, TP_E_UNSUPPORTED, "field kind not supported by the B200 library");
     }
     fill_float_copies(dv);
+    {
+        cudaError_t e = cudaMalloc(&f->d_self, sizeof(DevField));
+        if (e == cudaSuccess) {
+            dv.self = (const DevField*)f->d_self;
+            e = cudaMemcpy(f->d_self, &dv, sizeof(DevField), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            int r = cuda_fail(ctx, e, "field descriptor upload");
+            tp_field_destroy(f);
+            return r;
+        }
+    }
     *out = f;
     return TP_OK;
 }
@@ -712,7 +728,7 @@ void tp_field_destroy(tp_field* f) {
     DeviceGuard g(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
     for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_axis[0], f->d_axis[1], f->d_axis[2],
-                    f->d_snaps, f->d_times})
+                    f->d_snaps, f->d_times, f->d_self})
         if (p) cudaFree(p);
     for (tp_field* c : f->snaps) tp_field_destroy(c);
     delete f;

@@ -63,6 +63,11 @@ struct DevField {
     const double* ts;
     int32_t nts;
     int32_t pad2;
+    // a copy of this descriptor in device memory: the out-of-line evaluators
+    // of the general grids, quadratic fields and series take it, so a call
+    // passes a global pointer instead of copying the kernel-parameter struct
+    // to local memory
+    const DevField* self;
 };
 
 // QUADRATIC field value in float64, in the order of the CPU restatement:
