@@ -463,13 +463,25 @@ def leg_next_rows(tp, n=1 << 20, nt=1000):
 
 
 def profile_case(tp, case, device):
-    """Small untimed runs of the adaptive and guiding-centre kernels, for ncu captures."""
+    """Small untimed runs of the adaptive, guiding-centre and general-grid kernels, for ncu captures."""
     if case == "adaptive":
         w = tp.workloads.config3(n=262144, nt=200, ssi=200)
         prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
         for prec in ("fp32c", "fp64"):
             tp.solve(prob, tp.AdaptiveBoris(0.1), tp.EnsembleB200(device=device, precision=prec),
                      savestepinterval=200, isoutside=w.isoutside, tend=w.tend, step_cap=200)
+    elif case == "grids":
+        w = tp.workloads.config2(n=262144, nt=100, ssi=100)
+        dx = 1.0e5
+        g = np.arange(128) * dx
+        Ea, Ba, _L = tp.workloads.turbulent_grid(128, dx, 5.0e-9)
+        for order in (3, 0):
+            E = tp.build_interpolator(Ea, g, g, g, order, tp.PeriodicBC("exclusive"))
+            B = tp.build_interpolator(Ba, g, g, g, order, tp.PeriodicBC("exclusive"))
+            prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(E, B))
+            for prec in ("fp32c", "fp64"):
+                tp.solve(prob, tp.Boris(), tp.EnsembleB200(device=device, precision=prec), dt=w.dt,
+                         savestepinterval=100)
     else:
         w = tp.workloads.config4(1 << 18)
         prob = tp.TraceGCProblem(w.y0, (0.0, 1.0), (w.q, w.q2m, w.mu, w.E, w.B))
@@ -498,10 +510,12 @@ def main():
     ap.add_argument("--next-rows", action="store_true",
                     help="also time the general grids, field series, hybrid and detectors")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling)")
-    ap.add_argument("--profile-case", choices=["adaptive", "gc"], default=None,
+    ap.add_argument("--profile-case", choices=["adaptive", "gc", "grids"], default=None,
                     help="run one small untimed case for an ncu capture: AdaptiveBoris(0.1) in the dipole "
                          "(262144 protons, 200 steps, FP32C then FP64) or guiding centres in the dipole "
-                         "(2^18 particles, one bounce period, RK4 then RK45, FP64 then float32 RHS)")
+                         "(2^18 particles, one bounce period, RK4 then RK45, FP64 then float32 RHS) or the "
+                         "config-2 field on cubic then nearest-node grids (262144 protons, 100 steps, FP32C "
+                         "then FP64)")
     ap.add_argument("--adj-n", type=int, default=1 << 18)
     ap.add_argument("--adj-nt", type=int, default=4096)
     args = ap.parse_args()

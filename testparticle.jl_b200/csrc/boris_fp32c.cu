@@ -373,6 +373,11 @@ cudaError_t launch_boris_fp32c(const BorisArgs& a, const LaunchCfg& c, cudaStrea
     return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
 }
 
+cudaError_t prime_boris_fp32c(const BorisArgs& a) {
+    cudaFuncAttributes at;
+    return cudaFuncGetAttributes(&at, select_kernel32(a, a.use_queue != 0));
+}
+
 int occupancy_boris_fp32c(const BorisArgs& a, int block) {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, select_kernel32(a, true), block, 0);

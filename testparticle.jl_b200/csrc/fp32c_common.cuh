@@ -207,16 +207,6 @@ __device__ __forceinline__ F3 tri3(F3 v000, F3 v100, F3 v010, F3 v110, F3 v001, 
     return o;
 }
 
-static __device__ __noinline__ F3 grid_general32(const DevField& g, const CPos& p) {
-    // grids off the fast path: float64 interpolation of the compensated
-    // position (grid_general.cuh), rounded to float
-    double r[3] = {(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
-                   (double)p.hi[2] + (double)p.lo[2]};
-    double o[3];
-    if (!grid_general_eval<double>(g, r, o)) return nanf3();
-    return {(float)o[0], (float)o[1], (float)o[2]};
-}
-
 // quadratic fields: float64 evaluation of the compensated position, rounded
 static __device__ __noinline__ F3 quad_eval32(const DevField& f, const CPos& p, double t) {
     double o[3];
@@ -232,9 +222,8 @@ static __device__ __noinline__ F3 series_eval32(const DevField& f, const CPos& p
     return {(float)o.x, (float)o.y, (float)o.z};
 }
 
-template <bool GEN = true>
+// trilinear uniform-Cartesian grid (general grids: field_any32)
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
-    if (GEN && g.general) return grid_general32(*g.self, p);
     AxF ax, ay, az;
     if (!axes32(g, p, ax, ay, az)) return nanf3();
     const float4* T = g.tab32;
@@ -274,7 +263,7 @@ __device__ __forceinline__ F3 analytic_eval32(const DevField& f, const CPos& p, 
     }
 }
 
-template <bool PACKED_ONLY = false, bool GEN = true>
+template <bool PACKED_ONLY = false>
 __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, double t, F3& E, F3& B) {
     if (PACKED_ONLY || F.eb32) {
         AxF ax, ay, az;
@@ -308,12 +297,47 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
                  xyz(b111), ax, ay, az);
         return;
     }
-    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.E, p)
-        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.E.self, p, t)
-        : (GEN && F.E.kind == TP_FIELD_SERIES) ? series_eval32(*F.E.self, p, t) : analytic_eval32(F.E, p, t);
-    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32<GEN>(F.B, p)
-        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.B.self, p, t)
-        : (GEN && F.B.kind == TP_FIELD_SERIES) ? series_eval32(*F.B.self, p, t) : analytic_eval32(F.B, p, t);
+    E = (F.E.kind == TP_FIELD_GRID) ? grid_eval32(F.E, p)
+        : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.E.self, p, t) : analytic_eval32(F.E, p, t);
+    B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32(F.B, p)
+        : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.B.self, p, t) : analytic_eval32(F.B, p, t);
+}
+
+// E and B of the FP32C kernels for general grids and series (any field
+// kind), out of line: one call evaluates both fields from their descriptors'
+// device copies.  Measured on the config-2 field on a cubic grid, this is
+// 1.3x the rate of one call per field; the float64 kernels keep one call per
+// field (grid_general64), which measured 1.5x the rate of a combined call.
+struct EB32 {
+    F3 E, B;
+};
+
+__device__ __forceinline__ F3 field_any32(const DevField& f, const CPos& p, double t) {
+    if (f.kind == TP_FIELD_GRID) {
+        if (f.general) {
+            double r[3] = {(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+                           (double)p.hi[2] + (double)p.lo[2]};
+            double o[3];
+            if (!grid_general_eval<double, true>(f, r, o)) return nanf3();
+            return {(float)o[0], (float)o[1], (float)o[2]};
+        }
+        return grid_eval32(f, p);
+    }
+    if (f.kind == TP_FIELD_QUADRATIC) {
+        double o[3];
+        quad_eval(f, (double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+                  (double)p.hi[2] + (double)p.lo[2], t, o);
+        return {(float)o[0], (float)o[1], (float)o[2]};
+    }
+    if (f.kind == TP_FIELD_SERIES) return series_eval32(f, p, t);
+    return analytic_eval32(f, p, t);
+}
+
+static __device__ __noinline__ EB32 eval_EB_any32(const DevField& Ef, const DevField& Bf, CPos p, double t) {
+    EB32 o;
+    o.E = field_any32(Ef, p, t);
+    o.B = field_any32(Bf, p, t);
+    return o;
 }
 
 template <int FK>
@@ -323,8 +347,12 @@ __device__ __forceinline__ void eval_EB32t(const DevFields& F, const CPos& p, do
         B = analytic_eval32(F.B, p, t);
     } else if (FK == FK_EBGRID) {
         eval_EB32<true>(F, p, t, E, B);
+    } else if (FK == FK_GENGRID) {
+        EB32 o = eval_EB_any32(*F.E.self, *F.B.self, p, t);
+        E = o.E;
+        B = o.B;
     } else {
-        eval_EB32<false, FK == FK_GENGRID>(F, p, t, E, B);
+        eval_EB32<false>(F, p, t, E, B);
     }
 }
 

@@ -127,6 +127,18 @@ const void* select_gc_kernel64(const GCArgs& a, bool queue) {
 
 const void* select_gc_kernel32(const GCArgs& a, bool queue);
 
+cudaError_t prime_gc(const GCArgs& a) {
+    const bool q = a.use_queue != 0;
+    cudaFuncAttributes at;
+    return cudaFuncGetAttributes(&at, a.precision == TP_GC_PREC_FP32RHS ? select_gc_kernel32(a, q)
+                                                                         : select_gc_kernel64(a, q));
+}
+
+cudaError_t prime_fill_work() {
+    cudaFuncAttributes at;
+    return cudaFuncGetAttributes(&at, (const void*)k_fill_work);
+}
+
 int occupancy_gc(const GCArgs& a, int block) {
     int nb = 0;
     const void* f = a.precision == TP_GC_PREC_FP32RHS ? select_gc_kernel32(a, true) : select_gc_kernel64(a, true);

@@ -264,9 +264,16 @@ __device__ __forceinline__ bool gaxis(const DevField& g, int a, S x, GAx<S>& o) 
     return true;
 }
 
-// one node (3 components) of the per-node table as doubles
+// one node (3 components) of the per-node table as doubles; T32 reads the
+// float table (the FP32C kernels' copy, half the bytes of a float64 table)
+template <bool T32>
 __device__ __forceinline__ void gnode(const DevField& g, int64_t idx, double v[3]) {
-    if (g.f64) {
+    if (T32) {
+        float4 q = __ldg(g.tab32 + idx);
+        v[0] = (double)q.x;
+        v[1] = (double)q.y;
+        v[2] = (double)q.z;
+    } else if (g.f64) {
         const double2* p = reinterpret_cast<const double2*>(g.tab) + 2 * idx;
         double2 a = __ldg(p), b = __ldg(p + 1);
         v[0] = a.x;
@@ -290,8 +297,90 @@ __device__ __forceinline__ S gcombine(const GAx<S>& a, bool linear, const V* v) 
     return acc;
 }
 
+// Value-only interpolation when every axis of the cell takes the same
+// number of nodes: 64 nodes of an interior cubic cell, 8 of a linear cell, 1
+// nearest node.  Unrolled with the partial sums accumulated as the nodes
+// arrive, so nothing is indexed at run time and the sums stay in registers;
+// the operations and their order are those of the general loop below.
+template <bool T32>
+__device__ __forceinline__ void ginterp_cubic4(const DevField& g, const GAx<double> A[3], double out[3]) {
+    const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
+    double oz[3];
+#pragma unroll
+    for (int kz = 0; kz < 4; ++kz) {
+        double oy[3];
+#pragma unroll
+        for (int ky = 0; ky < 4; ++ky) {
+            const int64_t base = (int64_t)A[1].i[ky] * nx + (int64_t)A[2].i[kz] * nxy;
+            double ox[3];
+#pragma unroll
+            for (int kx = 0; kx < 4; ++kx) {
+                double v[3];
+                gnode<T32>(g, base + A[0].i[kx], v);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ox[c] = kx == 0 ? A[0].w[0] * v[c] : ox[c] + A[0].w[kx] * v[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) oy[c] = ky == 0 ? A[1].w[0] * ox[c] : oy[c] + A[1].w[ky] * ox[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) oz[c] = kz == 0 ? A[2].w[0] * oy[c] : oz[c] + A[2].w[kz] * oy[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = oz[c];
+}
+
+template <bool T32>
+__device__ __forceinline__ void ginterp_linear2(const DevField& g, const GAx<double> A[3], double out[3]) {
+    const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
+    double cz[2][3];
+#pragma unroll
+    for (int kz = 0; kz < 2; ++kz) {
+        double cy[2][3];
+#pragma unroll
+        for (int ky = 0; ky < 2; ++ky) {
+            const int64_t base = (int64_t)A[1].i[ky] * nx + (int64_t)A[2].i[kz] * nxy;
+            double v0[3], v1[3];
+            gnode<T32>(g, base + A[0].i[0], v0);
+            gnode<T32>(g, base + A[0].i[1], v1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) cy[ky][c] = v0[c] + A[0].w[0] * (v1[c] - v0[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) cz[kz][c] = cy[0][c] + A[1].w[0] * (cy[1][c] - cy[0][c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = cz[0][c] + A[2].w[0] * (cz[1][c] - cz[0][c]);
+}
+
+template <bool T32>
+__device__ __forceinline__ bool ginterp_fixed(const DevField&, const GAx<Dual3>*, bool, Dual3*) {
+    return false;
+}
+template <bool T32>
+__device__ __forceinline__ bool ginterp_fixed(const DevField& g, const GAx<double>* A, bool lin, double* out) {
+    const int k = A[0].k;
+    if (A[1].k != k || A[2].k != k) return false;
+    if (k == 4) {
+        ginterp_cubic4<T32>(g, A, out);
+        return true;
+    }
+    if (k == 2 && lin) {
+        ginterp_linear2<T32>(g, A, out);
+        return true;
+    }
+    if (k == 1) {
+        double v[3];
+        gnode<T32>(g, (int64_t)A[0].i[0] + (int64_t)A[1].i[0] * g.n[0] + (int64_t)A[2].i[0] * ((int64_t)g.n[0] * g.n[1]),
+              v);
+        for (int c = 0; c < 3; ++c) out[c] = 0.0 + (0.0 + (0.0 + v[c]));
+        return true;
+    }
+    return false;
+}
+
 // interpolate the three components at grid coordinates (q0, q1, q2)
-template <class S>
+template <class S, bool T32>
 __device__ __forceinline__ bool ginterp(const DevField& g, const S q[3], S out[3]) {
     GAx<S> A[3];
     bool ok = gaxis(g, 0, q[0], A[0]);
@@ -299,6 +388,7 @@ __device__ __forceinline__ bool ginterp(const DevField& g, const S q[3], S out[3
     ok = gaxis(g, 2, q[2], A[2]) && ok;
     if (!ok) return false;
     const bool lin = g.order == TP_ORDER_LINEAR;
+    if (ginterp_fixed<T32>(g, A, lin, out)) return true;
     const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
     S cz[4][3];
     for (int kz = 0; kz < A[2].k; ++kz) {
@@ -306,7 +396,7 @@ __device__ __forceinline__ bool ginterp(const DevField& g, const S q[3], S out[3
         for (int ky = 0; ky < A[1].k; ++ky) {
             double vx[4][3];
             const int64_t base = (int64_t)A[1].i[ky] * nx + (int64_t)A[2].i[kz] * nxy;
-            for (int kx = 0; kx < A[0].k; ++kx) gnode(g, base + A[0].i[kx], vx[kx]);
+            for (int kx = 0; kx < A[0].k; ++kx) gnode<T32>(g, base + A[0].i[kx], vx[kx]);
             for (int c = 0; c < 3; ++c) {
                 double col[4];
                 for (int kx = 0; kx < A[0].k; ++kx) col[kx] = vx[kx][c];
@@ -328,8 +418,9 @@ __device__ __forceinline__ bool ginterp(const DevField& g, const S q[3], S out[3
 }
 
 // Field value (and, for S = Dual3, its partial derivatives) at the
-// Cartesian point r; false where the field is NaN.
-template <class S>
+// Cartesian point r; false where the field is NaN.  T32: node values from
+// the float table.
+template <class S, bool T32 = false>
 __device__ __forceinline__ bool grid_general_eval(const DevField& g, const S r[3], S out[3]) {
     if (g.geom == TP_GRID_SPHERICAL || g.geom == TP_GRID_SPHERICAL_SCALAR) {
         // cart2sph (src/utility/utility.jl:63-71)
@@ -345,7 +436,7 @@ __device__ __forceinline__ bool grid_general_eval(const DevField& g, const S r[3
             q[2] = ph;
         }
         S v[3];
-        if (!ginterp(g, q, v)) return false;
+        if (!ginterp<S, T32>(g, q, v)) return false;
         if (g.geom == TP_GRID_SPHERICAL_SCALAR) {
             out[0] = v[0];
             out[1] = v[1];
@@ -370,7 +461,7 @@ __device__ __forceinline__ bool grid_general_eval(const DevField& g, const S r[3
         q[1] = r[1];
         q[2] = r[2];
     }
-    return ginterp(g, q, out);
+    return ginterp<S, T32>(g, q, out);
 }
 
 }  // namespace tpb

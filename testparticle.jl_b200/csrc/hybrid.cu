@@ -401,15 +401,23 @@ __global__ void __launch_bounds__(256, 1) k_hybrid(HybridArgs a) {
     }
 }
 
+static const void* hybrid_kernel(const HybridArgs& a) {
+    const int gm = gc_grid_mode(a.f);
+    return gm == GM_ANY ? (const void*)k_hybrid<GM_ANY>
+                        : (gm == GM_GRID ? (const void*)k_hybrid<GM_GRID> : (const void*)k_hybrid<GM_ANALYTIC>);
+}
+
+cudaError_t prime_hybrid(const HybridArgs& a) {
+    cudaFuncAttributes at;
+    return cudaFuncGetAttributes(&at, hybrid_kernel(a));
+}
+
 cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
     if (block <= 0) block = 128;
     int64_t grid = (a.n + block - 1) / block;
-    const int gm = gc_grid_mode(a.f);
     void* args[] = {const_cast<HybridArgs*>(&a)};
-    const void* k = gm == GM_ANY ? (const void*)k_hybrid<GM_ANY>
-                                 : (gm == GM_GRID ? (const void*)k_hybrid<GM_GRID> : (const void*)k_hybrid<GM_ANALYTIC>);
-    return cudaLaunchKernel(k, dim3((unsigned)grid), dim3(block), args, 0, s);
+    return cudaLaunchKernel(hybrid_kernel(a), dim3((unsigned)grid), dim3(block), args, 0, s);
 }
 
 }  // namespace tpb

@@ -841,6 +841,9 @@ int plan_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, LaunchCfg
     if (block > TPB_MAXT(field_config_of(a.f)))
         return fail(ctx, TP_E_ARG, "block exceeds the kernel's limit for this field configuration");
     a.use_queue = q;
+    cudaError_t e = d->precision == TP_PREC_FP32C ? prime_boris_fp32c(a) : prime_boris_fp64(a);
+    if (e == cudaSuccess && a.save_work) e = prime_fill_work();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel load");
     int occ = 0;
     if (q) occ = d->precision == TP_PREC_FP32C ? occupancy_boris_fp32c(a, block) : occupancy_boris_fp64(a, block);
     return pick_launch(ctx, a.n, block, q, occ, cfg);
@@ -1465,6 +1468,8 @@ int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* d, const tp_field* E, const
         a.status = st_d.as<int32_t>();
         double budget = d->budget_s > 0 ? d->budget_s : 600.0;
         a.budget_ns = (uint64_t)(budget * 1e9);
+        e = prime_hybrid(a);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel load");
         cudaEvent_t ev0, ev1;
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
@@ -1869,6 +1874,12 @@ int tp_gc_run(tp_ctx* ctx, const tp_gc_desc* d, const tp_field* E, const tp_fiel
         if (st != TP_OK) {
             delete r;
             return st;
+        }
+        e = prime_gc(a);
+        if (e == cudaSuccess && a.save_work) e = prime_fill_work();
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "kernel load");
         }
         cudaEvent_t ev0, ev1;
         cudaEventCreate(&ev0);

@@ -148,6 +148,13 @@ cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
 cudaError_t launch_fill_work(const WorkFillArgs& a, cudaStream_t s);
 cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s);
+// Load the kernel a launch will use (cudaFuncGetAttributes), so that lazy
+// module loading happens before a timed region instead of at the first launch
+cudaError_t prime_boris_fp64(const BorisArgs& a);
+cudaError_t prime_boris_fp32c(const BorisArgs& a);
+cudaError_t prime_gc(const GCArgs& a);
+cudaError_t prime_fill_work();
+cudaError_t prime_hybrid(const HybridArgs& a);
 // virtual detectors (detect.cu): mode 0 fluxes (tot: nsurf x 4 sums on the
 // device), 1 crossings (counts on the host; *rows_d_out: device rows the
 // caller frees with cudaFreeAsync), 2 first crossing (first: n x 6, device)
