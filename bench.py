@@ -112,6 +112,23 @@ def _dist():
     return world, rank, local
 
 
+def max_over_ranks(dist, value: float, device) -> float:
+    """The job's time is its slowest rank's: the maximum of `value` over ranks
+    (every rank calls this at the same point; identity without a process group)."""
+    if not dist:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units, the slowest finishing after `seconds`."""
+    return world * float(units_per_rank) / float(seconds)
+
+
 def _workload(tp, name: str, n: int, nt: int = 10_000):
     if name == "config2":
         return tp.workloads.config2(n=n, nt=nt, ssi=min(1000, nt))
@@ -235,11 +252,9 @@ def timed(torch, dist, dev, run, plan, k, warm, flush):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    tot = torch.tensor([sum(a.elapsed_time(b) for a, b in evs)], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    tot = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in evs), dev)
     run.check()
-    return float(tot.item())
+    return tot
 
 
 def _plan(tp, w, alg, prec, device, step_cap=0):
@@ -272,7 +287,7 @@ def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
         run.u0.copy_(u0_saved)
         ok = (rc32 == 1) & (rc64 == 1)
         okb = (rc64b == 1) & (rc64 == 1)
-        v32, v64 = world * ps32 / (ms32 * 1e-3), world * ps64 / (ms64 * 1e-3)
+        v32, v64 = whole_job_rate(world, ps32, ms32 * 1e-3), whole_job_rate(world, ps64, ms64 * 1e-3)
         out[name] = {"fp32c": v32, "fp64": v64, "speedup_fp32c_over_fp64": v32 / v64,
                      "unit": "particle-steps/s", "fp32c_error_vs_fp64": _err_summary(_rel_err(fs32[ok], fs64[ok])),
                      "fp64_vs_fp64_1ulp_start": _err_summary(_rel_err(fs64b[okb], fs64[okb])),
@@ -580,8 +595,8 @@ def main():
     chaos = _rel_err(run.final_states(), fs64)
     run.u0.copy_(u0_saved)
 
-    value = world * ps_step * args.steps / (tot32 * 1e-3)
-    value64 = world * ps64 * k64 / (tot64 * 1e-3)
+    value = whole_job_rate(world, ps_step * args.steps, tot32 * 1e-3)
+    value64 = whole_job_rate(world, ps64 * k64, tot64 * 1e-3)
     kernel_s = tot32 * 1e-3 / args.steps
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_PARTICLE_STEP * ps_step / kernel_s / 1e9
@@ -606,12 +621,8 @@ def main():
         d2h = sol.t_all.nbytes + sol.u_all.nbytes + sol.nsaved.nbytes + sol.retcodes.nbytes + sol.nsteps.nbytes
     e2e_value = None
     if e2e_t:
-        e2e_time = max(e2e_t)
-        if dist:
-            tt = torch.tensor([e2e_time], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_time = float(tt.item())
-        e2e_value = world * float(sol.nsteps.sum()) / e2e_time
+        e2e_time = max_over_ranks(dist, max(e2e_t), dev)
+        e2e_value = whole_job_rate(world, float(sol.nsteps.sum()), e2e_time)
     del sol
 
     legs = {}
