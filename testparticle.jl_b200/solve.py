@@ -11,6 +11,8 @@ instead.  Only EnsembleB200 runs here: there is no CPU fallback.
 """
 from __future__ import annotations
 
+import os
+import threading
 import time
 from dataclasses import dataclass
 from typing import Optional
@@ -30,6 +32,28 @@ _GC_PREC = {"fp64": _abi.TP_GC_PREC_FP64, "fp32": _abi.TP_GC_PREC_FP32RHS, "fp32
             "fp32c": _abi.TP_GC_PREC_FP32RHS}
 
 
+def _rows_of(table: np.ndarray) -> np.ndarray:
+    """(N, width) C-contiguous copy of a (width, N) table: particle-major, the
+    library's layout.  Large tables are transposed by several host threads
+    (numpy's copy releases the GIL)."""
+    n = table.shape[1]
+    if n < (1 << 18) or table.flags["F_CONTIGUOUS"]:
+        return np.ascontiguousarray(table.T)
+    out = np.empty((n, table.shape[0]))
+    k = max(1, min(8, os.cpu_count() or 1))
+    step = (n + k - 1) // k
+
+    def part(a):
+        np.copyto(out[a:a + step], table[:, a:a + step].T)
+
+    threads = [threading.Thread(target=part, args=(a,)) for a in range(0, n, step)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    return out
+
+
 def _initial_table(prob, trajectories: int, width: int) -> np.ndarray:
     u0 = np.asarray(prob.u0, dtype=np.float64)
     if u0.ndim == 2:
@@ -39,7 +63,7 @@ def _initial_table(prob, trajectories: int, width: int) -> np.ndarray:
             raise ValueError("pass either a (width, N) u0 table or a prob_func, not both")
         if trajectories not in (1, u0.shape[1]):
             raise ValueError("trajectories must equal the number of u0 columns")
-        return np.ascontiguousarray(u0.T)
+        return _rows_of(u0)
     if u0.shape != (width,):
         raise ValueError(f"u0 must have {width} components")
     if prob.prob_func is None:
