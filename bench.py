@@ -381,6 +381,22 @@ def leg_gc(tp, n):
             res[(prec, alg)] = s
             out[f"{alg}_{prec}"] = {"value": s.particle_steps() / s.elapsedTime, "unit": "particle-steps/s",
                                     "device_s": s.elapsedTime}
+    # mu through gc_to_full then full_to_gc (prepare_gc) at the final states:
+    # mu is a constant parameter of the guiding-centre equations, so this is
+    # the drift the conversion pair reports at the end of the run
+    half = n // 2
+
+    def mu_roundtrip(final):
+        rel = np.empty(n)
+        for lo, hi, sp in ((0, half, tp.Electron), (half, n, tp.Proton)):
+            pd = tp.prepare(w.E, w.B, species=sp)
+            xv = tp.gc_to_full(final[lo:hi].T, pd, w.mu[lo:hi])
+            _, mu2 = tp.full_to_gc(xv, pd)
+            rel[lo:hi] = np.abs(mu2 - w.mu[lo:hi]) / w.mu[lo:hi]
+        return float(np.median(rel))
+
+    for prec in ("fp64", "fp32"):
+        out[f"rk4_{prec}"]["mu_roundtrip_rel_median"] = mu_roundtrip(res[(prec, "rk4")].final_states())
     # energy 1/2 m v_par^2 + mu |B| at the end, float32 RHS against float64 (same algorithm)
     for alg in ("rk4", "rk45"):
         a, b = res[("fp32", alg)].final_states(), res[("fp64", alg)].final_states()

@@ -467,6 +467,15 @@ int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B,
                   const double* xv, int64_t n, double q, double m, double t,
                   double* y0_out, double* mu_out);
 
+/* gc_to_full (src/gc/gc.jl:106-154) for N guiding-centre states y (4 x N,
+ * (X, v_par)) with magnetic moments mu (N) at time t: xv_out (6 x N) is the
+ * full-orbit state at gyrophase phase_i[i] (phase when phase_i is null).  q,
+ * m shared by all particles; host buffers.  With tp_gc_prepare it is the
+ * reference's full_to_gc / gc_to_full pair.                                */
+int tp_gc_to_full(tp_ctx* ctx, const tp_field* E, const tp_field* B,
+                  const double* y, const double* mu, int64_t n, double q, double m,
+                  double phase, const double* phase_i, double t, double* xv_out);
+
 /* ---- results ---------------------------------------------------------------
  * Packed, per-trajectory layout of the reference solutions: trajectory i owns
  * saves offset_i .. offset_i + nsaved_i - 1 with offset_i = sum_{j<i} nsaved_j;

@@ -78,6 +78,10 @@ def lib() -> C.CDLL:
         L.orc_gc_prepare.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(from_abi.FieldDesc),
                                      C.POINTER(FieldCB), C.POINTER(FieldCB), P, C.c_int64, C.c_double,
                                      C.c_double, C.c_double, P, P]
+        L.orc_gc_to_full.restype = C.c_int
+        L.orc_gc_to_full.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(from_abi.FieldDesc),
+                                     C.POINTER(FieldCB), C.POINTER(FieldCB), P, P, C.c_int64, C.c_double,
+                                     C.c_double, C.c_double, P, C.c_double, P]
         L.orc_field_eval.restype = C.c_int
         L.orc_field_eval.argtypes = [C.POINTER(from_abi.FieldDesc), C.POINTER(FieldCB), P, C.c_int64,
                                      C.c_double, P, P]
@@ -406,6 +410,26 @@ def gc_prepare(E, B, xv: np.ndarray, q: float, m: float, t: float = 0.0):
     if code != 0:
         raise RuntimeError(f"oracle status {code}")
     return y0, mu
+
+
+def gc_to_full(E, B, y: np.ndarray, mu, q: float, m: float, phase=0.0, t: float = 0.0):
+    """gc_to_full restatement at rows of y (N, 4) -> (N, 6); phase scalar or (N,)."""
+    L = lib()
+    y = np.ascontiguousarray(np.atleast_2d(y), dtype=np.float64)
+    n = y.shape[0]
+    mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (n,)))
+    ph = np.asarray(phase, dtype=np.float64)
+    ph_i = np.ascontiguousarray(np.broadcast_to(ph, (n,))) if ph.ndim else None
+    Ed, Ecb = _field_arg(E)
+    Bd, Bcb = _field_arg(B)
+    out = np.empty((n, 6))
+    code = L.orc_gc_to_full(C.byref(Ed) if Ed else None, C.byref(Bd) if Bd else None,
+                            C.byref(Ecb) if Ecb else None, C.byref(Bcb) if Bcb else None, _ptr(y), _ptr(mu), n,
+                            float(q), float(m), float(ph) if ph_i is None else 0.0, _ptr(ph_i), float(t),
+                            _ptr(out))
+    if code != 0:
+        raise RuntimeError(f"oracle status {code}")
+    return out
 
 
 def field_eval(F, x: np.ndarray, t: float = 0.0, jacobian: bool = False):

@@ -642,6 +642,28 @@ int orc_gc_prepare(const tp_field_desc* Ed, const tp_field_desc* Bd, const orc_f
     return TP_OK;
 }
 
+// gc_to_full (src/gc/gc.jl:106-154) at n guiding-centre states y (n x 4)
+// with moments mu (n): xv_out (n x 6) at gyrophase phase_i[i] (or phase).
+int orc_gc_to_full(const tp_field_desc* Ed, const tp_field_desc* Bd, const orc_field_cb* Ecb,
+                   const orc_field_cb* Bcb, const double* y, const double* mu, int64_t n, double q,
+                   double m, double phase, const double* phase_i, double t, double* xv_out) {
+    std::unique_ptr<Field> E = make_field(Ed, Ecb), B = make_field(Bd, Bcb);
+    if (!E || !B) return TP_E_ARG;
+    for (int64_t i = 0; i < n; ++i) {
+        GCState s{{y[4 * i], y[4 * i + 1], y[4 * i + 2], y[4 * i + 3]}};
+        V3d x, v;
+        gc_to_full(s, *E, *B, q, m, mu[i], t, phase_i ? phase_i[i] : phase, x, v);
+        double* o = xv_out + 6 * i;
+        o[0] = x.x;
+        o[1] = x.y;
+        o[2] = x.z;
+        o[3] = v.x;
+        o[4] = v.y;
+        o[5] = v.z;
+    }
+    return TP_OK;
+}
+
 // Field values (and optionally Jacobians, row-major 9 per point) at n points.
 int orc_field_eval(const tp_field_desc* d, const orc_field_cb* cb, const double* x, int64_t n,
                    double t, double* out, double* jac_out) {

@@ -24,9 +24,8 @@ from .detectors import (Disk, Plane, Sphere, get_first_crossing, get_particle_cr
 from .postprocess import get_fields, get_work
 from .runtime import AdjointGrads, ArgumentError, Context, DeviceError, Tape
 from .solution import EnsembleSolution, TraceSolution
-from .solve import (AdjointPlan, BorisPlan, GCPlan, HybridPlan, adjoint_solve, plan_adjoint, plan_boris, plan_gc,
-                    plan_hybrid,
-                    prepare_gc, solve)
+from .solve import (AdjointPlan, BorisPlan, GCPlan, HybridPlan, adjoint_solve, full_to_gc, gc_to_full, plan_adjoint,
+                    plan_boris, plan_gc, plan_hybrid, prepare_gc, solve)
 from .utility import energy2velocity, get_gyrofrequency, get_gyroperiod, get_gyroradius, get_perp_vector, sph2cart
 
 __version__ = "0.1.0"

@@ -272,6 +272,8 @@ SIGNATURES = [
      [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
     ("tp_gc_run", C.c_int, [_P, C.POINTER(GCDesc), _P, _P, _P, _P, _P, _P, _P, _P, C.c_int64, C.POINTER(_P)]),
     ("tp_gc_prepare", C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_double, C.c_double, C.c_double, _P, _P]),
+    ("tp_gc_to_full", C.c_int, [_P, _P, _P, _P, _P, C.c_int64, C.c_double, C.c_double, C.c_double, _P, C.c_double,
+                                _P]),
     ("tp_result_info", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("tp_result_copy", C.c_int, [_P, _P, _P, _P, _P, _P]),
     ("tp_result_elapsed_ms", C.c_int, [_P, _DP]),

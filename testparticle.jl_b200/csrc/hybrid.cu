@@ -401,6 +401,36 @@ __global__ void __launch_bounds__(256, 1) k_hybrid(HybridArgs a) {
     }
 }
 
+// gc_to_full (src/gc/gc.jl:106-154) at n guiding-centre states: the
+// conversion of the hybrid solver, with the same portable sin / cos
+template <int GM>
+__global__ void k_gc_to_full(GCFullArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double* y = a.y + 4 * i;
+    G4 s{{y[0], y[1], y[2], y[3]}};
+    D3 x, v;
+    gc_full<GM>(a.f, s, a.q, a.m, a.mu[i], a.t, a.phase_i ? a.phase_i[i] : a.phase, x, v);
+    double* o = a.xv + 6 * i;
+    o[0] = x.x;
+    o[1] = x.y;
+    o[2] = x.z;
+    o[3] = v.x;
+    o[4] = v.y;
+    o[5] = v.z;
+}
+
+cudaError_t launch_gc_to_full(const GCFullArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    const int gm = gc_grid_mode(a.f);
+    const void* k = gm == GM_ANY    ? (const void*)k_gc_to_full<GM_ANY>
+                    : gm == GM_GRID ? (const void*)k_gc_to_full<GM_GRID>
+                                    : (const void*)k_gc_to_full<GM_ANALYTIC>;
+    const int block = 128;
+    void* args[] = {const_cast<GCFullArgs*>(&a)};
+    return cudaLaunchKernel(k, dim3((unsigned)((a.n + block - 1) / block)), dim3(block), args, 0, s);
+}
+
 static const void* hybrid_kernel(const HybridArgs& a) {
     const int gm = gc_grid_mode(a.f);
     return gm == GM_ANY ? (const void*)k_hybrid<GM_ANY>

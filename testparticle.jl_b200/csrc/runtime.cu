@@ -1389,6 +1389,46 @@ int tp_gc_prepare(tp_ctx* ctx, const tp_field* E, const tp_field* B, const doubl
     return TP_OK;
 }
 
+int tp_gc_to_full(tp_ctx* ctx, const tp_field* E, const tp_field* B, const double* y, const double* mu, int64_t n,
+                  double q, double m, double phase, const double* phase_i, double t, double* xv_out) {
+    if (!ctx || !E || !B) return fail(ctx, TP_E_ARG, "null argument");
+    if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");
+    if (n < 0 || (n > 0 && (!y || !mu || !xv_out))) return fail(ctx, TP_E_ARG, "bad buffers");
+    if (n == 0) return TP_OK;
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    DBuf y_d, mu_d, ph_d, xv_d;
+    cudaError_t e = y_d.alloc((size_t)n * 4 * sizeof(double));
+    if (e == cudaSuccess) e = mu_d.alloc((size_t)n * sizeof(double));
+    if (e == cudaSuccess && phase_i) e = ph_d.alloc((size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = xv_d.alloc((size_t)n * 6 * sizeof(double));
+    if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, "device allocation");
+    e = cudaMemcpyAsync(y_d.p, y, (size_t)n * 4 * sizeof(double), cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mu_d.p, mu, (size_t)n * sizeof(double), cudaMemcpyDefault, s);
+    if (e == cudaSuccess && phase_i)
+        e = cudaMemcpyAsync(ph_d.p, phase_i, (size_t)n * sizeof(double), cudaMemcpyDefault, s);
+    GCFullArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.f.E = E->dev;
+    a.f.B = B->dev;
+    a.y = y_d.as<double>();
+    a.mu = mu_d.as<double>();
+    a.phase_i = phase_i ? ph_d.as<double>() : nullptr;
+    a.n = n;
+    a.q = q;
+    a.m = m;
+    a.t = t;
+    a.phase = phase;
+    a.xv = xv_d.as<double>();
+    if (e == cudaSuccess) e = launch_gc_to_full(a, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(xv_out, xv_d.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "gc_to_full");
+    return TP_OK;
+}
+
 int tp_hybrid_run(tp_ctx* ctx, const tp_hybrid_desc* d, const tp_field* E, const tp_field* B, const double* u0,
                   int64_t n, tp_result** out, tp_result** adia) {
     if (!ctx || !d || !out) return fail(ctx, TP_E_ARG, "null argument");

@@ -51,6 +51,18 @@ struct GCPrepArgs {
     double* mu;
 };
 
+// gc_to_full at n guiding-centre states (y: n x 4, mu: n, phase_i: n or
+// null for the shared phase) into xv (n x 6) (hybrid.cu)
+struct GCFullArgs {
+    DevFields f;
+    const double* y;
+    const double* mu;
+    const double* phase_i;
+    int64_t n;
+    double q, m, t, phase;
+    double* xv;
+};
+
 // the work-rate columns of save_work, filled after a push over its saved
 // states (slot-major: t[k n + i], u[(k W + c) n + i]) (gc_fp64.cu)
 struct WorkFillArgs {
@@ -148,6 +160,7 @@ cudaError_t launch_gc_prepare(const GCPrepArgs& a, cudaStream_t s);
 cudaError_t launch_eval_points(const PointsArgs& a, cudaStream_t s);
 cudaError_t launch_fill_work(const WorkFillArgs& a, cudaStream_t s);
 cudaError_t launch_hybrid(const HybridArgs& a, int block, cudaStream_t s);
+cudaError_t launch_gc_to_full(const GCFullArgs& a, cudaStream_t s);
 // Load the kernel a launch will use (cudaFuncGetAttributes), so that lazy
 // module loading happens before a timed region instead of at the first launch
 cudaError_t prime_boris_fp64(const BorisArgs& a);

@@ -283,6 +283,19 @@ class Context:
         _check(self.lib, self.handle, code, "tp_gc_prepare")
         return y0, mu
 
+    def gc_to_full(self, E, B, y: np.ndarray, mu, q: float, m: float, phase=0.0, t: float = 0.0) -> np.ndarray:
+        """tp_gc_to_full: full-orbit states (N, 6) of guiding-centre rows y (N, 4)."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        n = y.shape[0]
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (n,)))
+        ph = np.asarray(phase, dtype=np.float64)
+        ph_i = np.ascontiguousarray(np.broadcast_to(ph, (n,))) if ph.ndim else None
+        xv = np.empty((n, 6))
+        code = self.lib.tp_gc_to_full(self.handle, self.field(E), self.field(B), _ptr(y), _ptr(mu), n, float(q),
+                                      float(m), float(ph) if ph_i is None else 0.0, _ptr(ph_i), float(t), _ptr(xv))
+        _check(self.lib, self.handle, code, "tp_gc_to_full")
+        return xv
+
     def eval_points(self, E, B, u: np.ndarray, t: np.ndarray, *, gc: bool, want: int, q2m: float = 0.0,
                     m: float = 0.0, q: float = 0.0, mu: float = 0.0) -> np.ndarray:
         """tp_eval_points: E, B (want & 1) and work rates (want & 2) at n states."""

@@ -343,3 +343,35 @@ def prepare_gc(xv, E, B, *, species=None, q=None, m=None, t: float = 0.0, device
     if table:
         return y0.T.copy(), (qq, qq / mm, mu, E, B)
     return y0[0], (qq, qq / mm, float(mu[0]), E, B)
+
+
+def full_to_gc(xu, param, t: float = 0.0, device: int = 0):
+    """full_to_gc(xu, param, t) -> (state_gc, mu) (src/gc/gc.jl:86-102), on the device.
+
+    param is the full-orbit parameter tuple of prepare(): (q2m, m, E, B, F).
+    Extension: xu may be a (6, N) table; the result is then a (4, N) table
+    and an array of mu.
+    """
+    q2m, m, E, B = param[0], param[1], as_field(param[2]), as_field(param[3])
+    xu = np.asarray(xu, dtype=np.float64)
+    table = xu.ndim == 2
+    xs = xu.T if table else xu.reshape(1, 6)
+    y, mu = Context.get(device).gc_prepare(E, B, xs, q2m * m, m, t)
+    if table:
+        return y.T.copy(), mu
+    return y[0], float(mu[0])
+
+
+def gc_to_full(state_gc, param, mu, phase=0.0, *, t: float = 0.0, device: int = 0) -> np.ndarray:
+    """gc_to_full(state_gc, param, mu, phase=0; t=0) -> xu (src/gc/gc.jl:104-154), on the device.
+
+    param is the full-orbit parameter tuple of prepare(): (q2m, m, E, B, F).
+    Extension: state_gc may be a (4, N) table with mu (and phase) scalars or
+    arrays of N; the result is then a (6, N) table.
+    """
+    q2m, m, E, B = param[0], param[1], as_field(param[2]), as_field(param[3])
+    y = np.asarray(state_gc, dtype=np.float64)
+    table = y.ndim == 2
+    ys = y.T if table else y.reshape(1, 4)
+    xv = Context.get(device).gc_to_full(E, B, ys, mu, q2m * m, m, phase, t)
+    return xv.T.copy() if table else xv[0]

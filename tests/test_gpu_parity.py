@@ -407,6 +407,39 @@ def _gc_dipole(tp, orc):
     return tp.TraceGCProblem(y0, (0.0, 1.0), p)
 
 
+def test_gc_full_conversion_gpu(tp, orc):
+    # test_gc.jl:62-160 through the device (full_to_gc = tp_gc_prepare, gc_to_full = tp_gc_to_full)
+    param = tp.prepare(tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0)), species=tp.Proton)
+    R, vpar, mu = np.array([1.0, 0.0, 0.0]), 1.0e5, 1.0e-15
+    xu = tp.gc_to_full(np.r_[R, vpar], param, mu, np.pi / 3)
+    assert xu.shape == (6,)
+    y, mu_new = tp.full_to_gc(xu, param)
+    assert np.allclose(y[:3], R, rtol=1e-5) and np.isclose(y[3], vpar, rtol=1e-5) and np.isclose(mu_new, mu, rtol=1e-5)
+    param2 = tp.prepare(tp.UniformField((0.0, 1.0e3, 0.0)), tp.UniformField((0.0, 0.0, 1.0)), species=tp.Proton)
+    xu = tp.gc_to_full(np.zeros(4), param2, 0.0)
+    assert np.allclose(xu[3:], [1000.0, 0.0, 0.0], atol=1e-5)
+    y, mu_new = tp.full_to_gc(xu, param2)
+    assert np.allclose(y, 0.0, atol=1e-5) and abs(mu_new) <= 1e-10
+    v0 = tp.gc_to_full(np.zeros(4), param, 1.0e-15, 0.0)[3:]
+    v90 = tp.gc_to_full(np.zeros(4), param, 1.0e-15, np.pi / 2)[3:]
+    assert np.allclose(v0 / np.linalg.norm(v0), [1, 0, 0], atol=1e-5)
+    assert np.allclose(v90 / np.linalg.norm(v90), [0, 1, 0], atol=1e-5)
+    # parity with the oracle on guiding centres in the dipole, per-particle phase
+    w = tp.workloads.config4(256)
+    keep = slice(128, 256)  # the protons
+    y = w.y0[:, keep]
+    rng = np.random.default_rng(11)
+    ph = rng.uniform(0.0, 2 * np.pi, y.shape[1])
+    pd = tp.prepare(w.E, w.B, species=tp.Proton)
+    xv = tp.gc_to_full(y, pd, w.mu[keep], ph)
+    ref = orc.gc_to_full(w.E, w.B, y.T, w.mu[keep], tp.Proton.q, tp.Proton.m, ph)
+    assert xv.shape == (6, 128)
+    assert _rel(xv.T, ref) <= 1e-13
+    yb, mub = tp.full_to_gc(xv, pd)
+    yr, mur = orc.gc_prepare(w.E, w.B, ref, tp.Proton.q, tp.Proton.m)
+    assert _rel(yb.T, yr) <= 1e-13 and np.max(np.abs(mub - mur) / mur) <= 1e-13
+
+
 def test_gc_reference_counts_gpu(tp, orc):
     # test_gc.jl:190-251 through the B200 path
     prob = _gc_dipole(tp, orc)

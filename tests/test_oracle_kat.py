@@ -390,6 +390,30 @@ def test_gc_rk45_dipole_counts(tp, orc):
     assert auto.nsaved[0] == 58 and auto.retcode[0] == 1
 
 
+def test_gc_full_conversion_kats(tp, orc):
+    """test_gc.jl:62-160: GC -> full -> GC reversibility, the E x B drift and the gyrophase."""
+    q, m = tp.Proton.q, tp.Proton.m
+    Z, B1 = tp.ZeroField(), tp.UniformField((0.0, 0.0, 1.0))
+    R, vpar, mu = np.array([1.0, 0.0, 0.0]), 1.0e5, 1.0e-15
+    xu = orc.gc_to_full(Z, B1, np.r_[R, vpar], mu, q, m, np.pi / 3)[0]
+    assert xu.shape == (6,)
+    y, mu_new = orc.gc_prepare(Z, B1, xu, q, m)
+    assert np.allclose(y[0, :3], R, rtol=1e-5) and np.isclose(y[0, 3], vpar, rtol=1e-5)
+    assert np.isclose(mu_new[0], mu, rtol=1e-5)
+    # E in y, B in z: the drift (E x B) / B^2 = (1000, 0, 0)
+    E2 = tp.UniformField((0.0, 1.0e3, 0.0))
+    xu = orc.gc_to_full(E2, B1, np.zeros(4), 0.0, q, m)[0]
+    assert np.allclose(xu[3:], [1000.0, 0.0, 0.0], atol=1e-5)
+    y, mu_new = orc.gc_prepare(E2, B1, xu, q, m)
+    assert np.allclose(y[0], 0.0, atol=1e-5) and abs(mu_new[0]) <= 1e-10
+    # phase 0 along e1 = x, phase pi/2 along e2 = y (get_perp_vector of z)
+    v0 = orc.gc_to_full(Z, B1, np.zeros(4), 1.0e-15, q, m, 0.0)[0, 3:]
+    v90 = orc.gc_to_full(Z, B1, np.zeros(4), 1.0e-15, q, m, np.pi / 2)[0, 3:]
+    n0, n90 = v0 / np.linalg.norm(v0), v90 / np.linalg.norm(v90)
+    assert abs(n0 @ n90) <= 1e-5
+    assert np.allclose(n0, [1.0, 0.0, 0.0], atol=1e-5) and np.allclose(n90, [0.0, 1.0, 0.0], atol=1e-5)
+
+
 # ------------------------------------------------------------------ test/test_utility.jl
 def test_gyro_constants(tp):
     # test_utility.jl:28-33
