@@ -125,18 +125,21 @@ __device__ __forceinline__ int64_t gc_next(const GCArgs& a, int64_t& first) {
 }
 
 
-// update_rk4, src/gc/rk4_gc.jl:7-22
+// update_rk4, src/gc/rk4_gc.jl:7-22.  The stages run as a loop that is not
+// unrolled (the right-hand side inlined once, as in update_dp5); the sum
+// ((k1 + 2 k2) + 2 k3) + k4 is accumulated in the reference's order.
 template <class RHS>
 __device__ __forceinline__ G4 update_rk4(const RHS& f, const DevFields& F, const G4& y,
                                          const GCPar& p, double dt, double t) {
-    G4 k1 = f(F, y, p, t);
-    G4 yt = gadd(y, gscale(0.5 * dt, k1));
-    G4 k2 = f(F, yt, p, t + 0.5 * dt);
-    yt = gadd(y, gscale(0.5 * dt, k2));
-    G4 k3 = f(F, yt, p, t + 0.5 * dt);
-    yt = gadd(y, gscale(dt, k3));
-    G4 k4 = f(F, yt, p, t + dt);
-    G4 sum = gadd(gadd(gadd(k1, gscale(2.0, k2)), gscale(2.0, k3)), k4);
+    G4 k = f(F, y, p, t);
+    G4 sum = k;
+#pragma unroll 1
+    for (int st = 1; st < 4; ++st) {
+        const double h = st < 3 ? 0.5 * dt : dt;
+        G4 yt = gadd(y, gscale(h, k));
+        k = f(F, yt, p, t + h);
+        sum = st < 3 ? gadd(sum, gscale(2.0, k)) : gadd(sum, k);
+    }
     return gscale(dt / 6.0, sum);
 }
 
@@ -265,50 +268,54 @@ __device__ __forceinline__ double pow02_rn(double x) {
     return __dadd_rn(z0, __dadd_rn(corr, __dmul_rn(z0, t)));
 }
 
-// update_dp5, src/gc/rk45_gc.jl:7-47 (tableau of rk45_gc.jl:9-20)
+// update_dp5, src/gc/rk45_gc.jl:7-47 (tableau of rk45_gc.jl:9-20), with k1 =
+// f(y, t) given by the caller; returns the seventh stage's input y7 and k7
+// = f(y7, t + dt).  The stages run as a loop that is not unrolled, so the
+// right-hand side is inlined once: seven inlined copies overflowed the
+// instruction cache (the kernel stalled on instruction fetch).  Each stage's
+// sum adds a_s1 k1 + a_s2 k2 + ... left to right, the reference's order, and
+// its time is fma(c_s, dt, t) (c6 = c7 = 1: t + dt exactly).
+struct DP5Tableau {
+    double a[7][6];
+    double c[7];
+};
+__constant__ const DP5Tableau kDP5 = {
+    {{0, 0, 0, 0, 0, 0},
+     {1.0 / 5, 0, 0, 0, 0, 0},
+     {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+     {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+     {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+     {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+     {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}},
+    {0.0, 1.0 / 5, 3.0 / 10, 4.0 / 5, 8.0 / 9, 1.0, 1.0}};
+
 template <class RHS>
 __device__ __forceinline__ void update_dp5(const RHS& f, const DevFields& F, const G4& y,
-                                           const GCPar& p, double dt, double t, G4& dy, G4& err) {
-    const double c2 = 1.0 / 5, c3 = 3.0 / 10, c4 = 4.0 / 5, c5 = 8.0 / 9;
-    const double a21 = 1.0 / 5;
-    const double a31 = 3.0 / 40, a32 = 9.0 / 40;
-    const double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
-    const double a51 = 19372.0 / 6561, a52 = -25360.0 / 2187, a53 = 64448.0 / 6561, a54 = -212.0 / 729;
-    const double a61 = 9017.0 / 3168, a62 = -355.0 / 33, a63 = 46732.0 / 5247, a64 = 49.0 / 176,
-                 a65 = -5103.0 / 18656;
-    const double a71 = 35.0 / 384, a72 = 0.0, a73 = 500.0 / 1113, a74 = 125.0 / 192,
-                 a75 = -2187.0 / 6784, a76 = 11.0 / 84;
+                                           const GCPar& p, double dt, double t, const G4& k1, G4& dy, G4& err,
+                                           G4& y7, G4& k7) {
     const double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192, b5 = -2187.0 / 6784,
                  b6 = 11.0 / 84;
     const double e1 = 71.0 / 57600, e3 = -71.0 / 16695, e4 = 71.0 / 1920, e5 = -17253.0 / 339200,
                  e6 = 22.0 / 525, e7 = -1.0 / 40;
-    G4 k1 = f(F, y, p, t);
-    G4 yt = gadd(y, gscale(dt, gscale(a21, k1)));
-    G4 k2 = f(F, yt, p, fma(c2, dt, t));
-    yt = gadd(y, gscale(dt, gadd(gscale(a31, k1), gscale(a32, k2))));
-    G4 k3 = f(F, yt, p, fma(c3, dt, t));
-    yt = gadd(y, gscale(dt, gadd(gadd(gscale(a41, k1), gscale(a42, k2)), gscale(a43, k3))));
-    G4 k4 = f(F, yt, p, fma(c4, dt, t));
-    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gscale(a51, k1), gscale(a52, k2)), gscale(a53, k3)),
-                                 gscale(a54, k4))));
-    G4 k5 = f(F, yt, p, fma(c5, dt, t));
-    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gscale(a61, k1), gscale(a62, k2)), gscale(a63, k3)),
-                                      gscale(a64, k4)),
-                                 gscale(a65, k5))));
-    G4 k6 = f(F, yt, p, fma(1.0, dt, t));
-    yt = gadd(y, gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(a71, k1), gscale(a72, k2)),
-                                                gscale(a73, k3)),
-                                           gscale(a74, k4)),
-                                      gscale(a75, k5)),
-                                 gscale(a76, k6))));
-    G4 k7 = f(F, yt, p, t + dt);
-    dy = gscale(dt, gadd(gadd(gadd(gadd(gscale(b1, k1), gscale(b3, k3)), gscale(b4, k4)),
-                              gscale(b5, k5)),
-                         gscale(b6, k6)));
-    err = gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(e1, k1), gscale(e3, k3)), gscale(e4, k4)),
-                                    gscale(e5, k5)),
-                               gscale(e6, k6)),
-                          gscale(e7, k7)));
+    G4 k[7];
+    k[0] = k1;
+    G4 yt;
+#pragma unroll 1
+    for (int st = 1; st < 7; ++st) {
+        G4 acc = gscale(kDP5.a[st][0], k[0]);
+        for (int j = 1; j < st; ++j) acc = gadd(acc, gscale(kDP5.a[st][j], k[j]));
+        yt = gadd(y, gscale(dt, acc));
+        k[st] = f(F, yt, p, fma(kDP5.c[st], dt, t));
+    }
+    y7 = yt;
+    k7 = k[6];
+    dy = gscale(dt, gadd(gadd(gadd(gadd(gscale(b1, k[0]), gscale(b3, k[2])), gscale(b4, k[3])),
+                              gscale(b5, k[4])),
+                         gscale(b6, k[5])));
+    err = gscale(dt, gadd(gadd(gadd(gadd(gadd(gscale(e1, k[0]), gscale(e3, k[2])), gscale(e4, k[3])),
+                                    gscale(e5, k[4])),
+                               gscale(e6, k[5])),
+                          gscale(e7, k[6])));
 }
 
 // Register cap 168 (65536 / 384): three blocks of 128 threads per SM for the
@@ -321,7 +328,8 @@ __global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
     int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const double safety = 0.9, max_growth = 5.0, min_growth = 0.2;
     int64_t i = -1, iout = 0, steps = 0, attempts = 0;
-    G4 xv;
+    G4 xv, k1;
+    bool have_k1 = false;
     GCPar p{0, 0, 0};
     double t = 0, dt = 0, t_last = 0, t1 = 0;
     int ret = TP_RET_SUCCESS;
@@ -357,13 +365,20 @@ __global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
             steps = 0;
             attempts = 0;
             ret = TP_RET_SUCCESS;
+            have_k1 = false;
         }
         bool done = !(t < t1 && steps < a.maxiters);
         if (!done) {
             if (t + dt > t1) dt = t1 - t;
-            G4 dx, E;
-            update_dp5(f, a.f, xv, p, dt, t, dx, E);
+            // k1 = f(x, t) is the last attempt's k1 after a rejection (same x
+            // and t) and its k7 after an acceptance whose seventh-stage input
+            // equals the new state bit for bit (k7 is then f(x_new, t + dt)):
+            // the same value the reference recomputes, one evaluation fewer
+            if (!have_k1) k1 = f(a.f, xv, p, t);
+            G4 dx, E, y7, k7;
+            update_dp5(f, a.f, xv, p, dt, t, k1, dx, E, y7, k7);
             G4 yn = gadd(xv, dx);
+            have_k1 = true;
             double sum_sq = 0.0;
             for (int k = 0; k < 4; ++k) {
                 double ax_ = fabs(xv.y[k]), ay_ = fabs(yn.y[k]);
@@ -382,6 +397,12 @@ __global__ void __launch_bounds__(384, 1) k_rk45(GCArgs a) {
                     stop = true;
                 } else {
                     t += dt;
+                    bool same = true;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        same = same && __double_as_longlong(y7.y[k]) == __double_as_longlong(yn.y[k]);
+                    if (same) k1 = k7;
+                    have_k1 = same;
                     xv = yn;
                     if (a.save_everystep) {
                         S.save(i, iout, xv, t);

@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(256, 1) k_hybrid(HybridArgs a) {
                     }
                 }
                 if (t + dt > a.t1) dt = a.t1 - t;
-                G4 dx, Er;
-                update_dp5(f, a.f, xg, p, dt, t, dx, Er);
+                G4 dx, Er, y7, k7;
+                update_dp5(f, a.f, xg, p, dt, t, f(a.f, xg, p, t), dx, Er, y7, k7);
                 G4 yn = gadd(xg, dx);
                 double sum_sq = 0.0;
                 for (int k = 0; k < 4; ++k) {
