@@ -215,13 +215,6 @@ static __device__ __noinline__ F3 quad_eval32(const DevField& f, const CPos& p, 
     return {(float)o[0], (float)o[1], (float)o[2]};
 }
 
-// time series: the float64 blend of the compensated position, rounded
-static __device__ __noinline__ F3 series_eval32(const DevField& f, const CPos& p, double t) {
-    D3 r{(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1], (double)p.hi[2] + (double)p.lo[2]};
-    D3 o = series_eval64(f, r, t);
-    return {(float)o.x, (float)o.y, (float)o.z};
-}
-
 // trilinear uniform-Cartesian grid (general grids: field_any32)
 __device__ __forceinline__ F3 grid_eval32(const DevField& g, const CPos& p) {
     AxF ax, ay, az;
@@ -301,6 +294,44 @@ __device__ __forceinline__ void eval_EB32(const DevFields& F, const CPos& p, dou
         : (F.E.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.E.self, p, t) : analytic_eval32(F.E, p, t);
     B = (F.B.kind == TP_FIELD_GRID) ? grid_eval32(F.B, p)
         : (F.B.kind == TP_FIELD_QUADRATIC) ? quad_eval32(*F.B.self, p, t) : analytic_eval32(F.B, p, t);
+}
+
+// a series snapshot (never a series) in the FP32C arithmetic: trilinear
+// grids through the float table as in grid_eval32, general grids through
+// grid_general.cuh over the float table (out of line), quadratic and
+// analytic fields as elsewhere
+static __device__ __noinline__ F3 snapshot_general32(const DevField& g, const CPos& p) {
+    double r[3] = {(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+                   (double)p.hi[2] + (double)p.lo[2]};
+    double o[3];
+    if (!grid_general_eval<double, true>(g, r, o)) return nanf3();
+    return {(float)o[0], (float)o[1], (float)o[2]};
+}
+
+__device__ __forceinline__ F3 snapshot_eval32(const DevField& g, const CPos& p, double t) {
+    if (g.kind == TP_FIELD_GRID) return g.general ? snapshot_general32(g, p) : grid_eval32(g, p);
+    if (g.kind == TP_FIELD_QUADRATIC) {
+        double o[3];
+        quad_eval(g, (double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+                  (double)p.hi[2] + (double)p.lo[2], t, o);
+        return {(float)o[0], (float)o[1], (float)o[2]};
+    }
+    return analytic_eval32(g, p, t);
+}
+
+// time series (LazyTimeInterpolator, src/utility/interpolation.jl:337-430)
+// in the FP32C arithmetic: the snapshot index and the weight w from the
+// float64 times, the snapshots evaluated over their float tables (half the
+// bytes of the float64 tables the FP64 kernels read) and blended in float,
+// (1 - w) F_k + w F_{k+1}
+static __device__ __noinline__ F3 series_eval32(const DevField& f, const CPos& p, double t) {
+    const int k = series_index(f, t);
+    if (k == 0) return snapshot_eval32(f.snaps[0], p, t);
+    if (k >= f.nts) return snapshot_eval32(f.snaps[f.nts - 1], p, t);
+    const double t1 = __ldg(f.ts + k - 1), t2 = __ldg(f.ts + k);
+    const float w = (float)((t - t1) / (t2 - t1)), u = 1.0f - w;
+    const F3 a = snapshot_eval32(f.snaps[k - 1], p, t), b = snapshot_eval32(f.snaps[k], p, t);
+    return {u * a.x + w * b.x, u * a.y + w * b.y, u * a.z + w * b.z};
 }
 
 // E and B of the FP32C kernels for general grids and series (any field
