@@ -182,7 +182,10 @@ __device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, b
 // Largest block a push kernel is compiled for, per field configuration: it
 // caps the register allocation at 65536 / TPB_MAXT(FK) per thread.  The
 // interleaved-grid kernels are gather-latency bound, so they take 384 (<= 170
-// registers: three 128-thread blocks per SM).  The analytic-field kernels
+// registers: three 128-thread blocks per SM); at 512 the float64 one spills
+// 340 bytes per thread and measured 7 % slower on the 128^3 gridded
+// workload (1.93e10 against 2.07e10 particle-steps/s, four blocks per SM
+// instead of three), and the FP32C one would spill.  The analytic-field kernels
 // are latency bound on float64 dependency chains and take 512 (<= 128
 // registers, no spills): the float64 multistep and adaptive pushes in the
 // dipole measured 15 % faster than at 256.  The others take 256.
