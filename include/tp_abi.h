@@ -492,15 +492,19 @@ void tp_result_destroy(tp_result* res);
  * No counterpart in the reference: an addition of this library for callers
  * that must not let a library allocate device memory (their own memory pool
  * owns every buffer, or allocation is off-limits on their latency path).
- * Packs the slot-major output of tp_boris_run_device (or a guiding-centre run
- * written the same way) into the per-trajectory layout of tp_result_copy, on
- * `stream`, using a static device scratch array instead of cudaMalloc:
+ * Packs the slot-major output of tp_boris_run_device into the
+ * per-trajectory layout of tp_result_copy, on `stream`, using a static
+ * device scratch array instead of cudaMalloc:
  *   t_in[k*n + i], u_in[(k*width + c)*n + i], nsaved[i]  (device, as written)
  *   t_out, u_out  device buffers of at least total saves (n * nslots is safe)
  *   total_out     device int64 receiving the number of packed saves
  * n may not exceed TP_NOALLOC_MAX_TRAJECTORIES (else TP_E_ARG).  Calls share
  * the scratch: calls that overlap on the GPU race.  The first call on a
- * device performs a one-time set-up; make it before any stream capture.    */
+ * device performs a one-time set-up (it looks up the scratch's device
+ * address); make it before any stream capture.  The address is kept for the
+ * life of the process: after cudaDeviceReset on that device the library
+ * must not be called again in the same process.  Negative nsaved entries
+ * count as 0, entries above nslots as nslots, as in tp_boris_run.          */
 #define TP_NOALLOC_MAX_TRAJECTORIES 1048576
 int tp_pack_results_device_noalloc(tp_ctx* ctx, const double* t_in,
                                    const double* u_in, const int32_t* nsaved,

@@ -19,7 +19,10 @@
 // on two streams, or from two host threads -- race on it and must not be
 // issued.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture begins.
+// before any stream capture begins.  The address is cached per device for the
+// life of the process: it is valid until the device's primary context is
+// destroyed (cudaDeviceReset), after which the library must not be called.
+// Counts are clamped to [0, nslots], as the allocating path does (pack.cu).
 #include <cub/block/block_scan.cuh>
 
 #include <cstring>

@@ -43,7 +43,7 @@ __global__ void k_pack_results(const double* t_in, const double* u_in, const int
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t ns = nsaved[i];
-    if (ns > nslots) ns = nslots;
+    ns = ns < 0 ? 0 : (ns > nslots ? nslots : ns);
     int64_t o = offsets[i];
     for (int64_t k = 0; k < ns; ++k) {
         t_out[o + k] = t_in[k * n + i];
@@ -61,7 +61,7 @@ cudaError_t launch_pack_results(const double* t_in, const double* u_in, const in
     return cudaGetLastError();
 }
 
-// nsaved (clamped to nslots) -> exclusive offsets, plus the total in offsets[n]
+// nsaved (clamped to [0, nslots]) -> exclusive offsets, plus the total in offsets[n]
 __global__ void k_clamp_counts(const int32_t* nsaved, int64_t n, int64_t nslots, int64_t* cnt) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
@@ -70,7 +70,7 @@ __global__ void k_clamp_counts(const int32_t* nsaved, int64_t n, int64_t nslots,
         return;
     }
     int64_t v = nsaved[i];
-    cnt[i] = v > nslots ? nslots : v;
+    cnt[i] = v < 0 ? 0 : (v > nslots ? nslots : v);
 }
 
 cudaError_t scan_offsets(const int32_t* nsaved, int64_t n, int64_t nslots, int64_t* cnt,

@@ -20,15 +20,18 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _problem(tp, kind):
+def _problem(tp, kind, n=None):
     if kind == "fixed":
-        w = tp.workloads.config1(300)
+        w = tp.workloads.config1(n or 300)
         prob = tp.TraceProblem(w.u0, (0.0, 2000 * w.dt), tp.prepare(w.E, w.B))
         return tp.plan_boris(prob, tp.Boris(), dt=w.dt, savestepinterval=100)
-    w = tp.workloads.config3(200, nt=500, ssi=40)
+    # adaptive steps in the dipole: the save counts differ from particle to
+    # particle, so every trajectory's packed offset depends on all before it
+    nt, ssi = (500, 40) if n is None else (120, 10)
+    w = tp.workloads.config3(n or 200, nt=nt, ssi=ssi)
     prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
-    return tp.plan_boris(prob, tp.AdaptiveBoris(0.1), tend=w.tend, savestepinterval=40, isoutside=w.isoutside,
-                         step_cap=500)
+    return tp.plan_boris(prob, tp.AdaptiveBoris(0.1), tend=w.tend, savestepinterval=ssi, isoutside=w.isoutside,
+                         step_cap=nt)
 
 
 def _pack_without_alloc(tp, torch, ctx, plan):
@@ -59,21 +62,40 @@ def _pack_without_alloc(tp, torch, ctx, plan):
     torch.cuda.synchronize()
     assert int(status.item()) == 0
     tot = int(total.item())
-    return nsaved.cpu().numpy(), t_pk[:tot].cpu().numpy(), u_pk[:tot].cpu().numpy(), t_pk[tot:].cpu().numpy()
+    ns = nsaved.cpu().numpy()
+    # the reported total is the sum of the clamped save counts
+    assert tot == int(np.minimum(np.maximum(ns.astype(np.int64), 0), nslots).sum())
+    return ns, t_pk[:tot].cpu().numpy(), u_pk[:tot].cpu().numpy(), t_pk[tot:].cpu().numpy()
+
+
+def _check_against_allocating_path(tp, torch, ctx, plan):
+    ref = ctx.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    nsaved, t, u, rest = _pack_without_alloc(tp, torch, ctx, plan)
+    assert np.array_equal(nsaved, ref.nsaved)
+    assert t.shape == ref.t.shape and u.shape == ref.u.shape
+    assert np.array_equal(t, ref.t)
+    assert np.array_equal(u, ref.u, equal_nan=True)
+    assert np.all(np.isnan(rest))  # nothing written past the packed total
+    return nsaved
 
 
 def test_noalloc_pack_matches_allocating_entry_point(tp):
     torch = pytest.importorskip("torch")
     ctx = tp.Context.get(0)
     for kind in ("fixed", "adaptive"):  # two calls in a row share the static scratch
-        plan = _problem(tp, kind)
-        ref = ctx.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
-        nsaved, t, u, rest = _pack_without_alloc(tp, torch, ctx, plan)
-        assert np.array_equal(nsaved, ref.nsaved)
-        assert t.shape == ref.t.shape and u.shape == ref.u.shape
-        assert np.array_equal(t, ref.t)
-        assert np.array_equal(u, ref.u, equal_nan=True)
-        assert np.all(np.isnan(rest))  # nothing written past the packed total
+        _check_against_allocating_path(tp, torch, ctx, _problem(tp, kind))
+
+
+@pytest.mark.parametrize("n", [5000, 1048576])
+def test_noalloc_pack_across_scan_blocks(tp, n):
+    """Several 1024-trajectory scan blocks, uneven save counts, and the largest n
+    the static scratch takes: every block's offset comes from the scan of the
+    block totals, so a wrong block prefix shows up as a mismatch."""
+    torch = pytest.importorskip("torch")
+    assert n <= tp._abi.TP_NOALLOC_MAX_TRAJECTORIES
+    ctx = tp.Context.get(0)
+    nsaved = _check_against_allocating_path(tp, torch, ctx, _problem(tp, "adaptive", n))
+    assert len(np.unique(nsaved)) > 1  # uneven: offsets are not a multiple of one count
 
 
 def test_noalloc_pack_rejects_more_than_the_static_limit(tp):
