@@ -13,10 +13,12 @@ It adds methods to the reference's own dispatch points
 `_solve_adaptive(::EnsembleAlg, ...)`, src/boris/adaptive_boris.jl:40-139;
 `_solve(::EnsembleAlg, ::TraceGCProblem, ...)`, src/gc/gc_solver.jl:104-161).
 
-Fields must be one of the device-evaluable types below (closures cannot run on
-the device); they are ordinary callables, so the reference CPU solver runs on
-the same objects for a like-for-like comparison.  `isoutside` must be a
-`Terminate` predicate.
+Fields must be the reference's `ZeroField`, a trilinear `FieldInterpolator` on
+uniform axes (what `prepare(x, y, z, E, B)` and `build_interpolator(CartesianGrid,
+A, x, y, z, 1, bc)` build), or one of the device-evaluable types below
+(closures cannot run on the device); these are ordinary callables, so the
+reference CPU solver runs on the same objects for a like-for-like comparison.
+`isoutside` must be a `Terminate` predicate.
 """
 module TestParticleB200
 
@@ -28,7 +30,7 @@ using SciMLBase: BasicEnsembleAlgorithm, EnsembleSolution, EnsembleContext, Retu
 using StaticArrays: SVector
 import ChainRulesCore
 
-export EnsembleB200, UniformField, AffineField, DipoleField, B200Grid, Terminate, boris_final_state
+export EnsembleB200, UniformField, AffineField, DipoleField, B200Grid, Terminate, boris_final_state, grid_of
 
 const libtpb200 = get(ENV, "TPB200_LIB", joinpath(@__DIR__, "..", "..", "..", "libtpb200.so"))
 
@@ -85,7 +87,10 @@ end
     B200Grid(A, x, y, z; bc = :fill_nan | :clamp | :periodic)
 
 Trilinear interpolator of a (3, nx, ny, nz) Float32/Float64 array on uniform
-ranges, evaluated identically on the CPU (this callable) and on the device.
+ranges.  This callable evaluates in Float64 with the operation order of the
+device's FP64 path (`u = (x - x0) * (1/dx)`, then `a + f * (b - a)` along x,
+then y, then z), so the two agree bit for bit; the device's FP32C path
+evaluates the same formula in Float32 arithmetic and differs in the last bits.
 """
 struct B200Grid{T} <: Function
     A::Array{T, 4}
@@ -196,7 +201,123 @@ fdesc(f::DipoleField) = TpFieldDesc(3, 0, 0, 0, Z3, Z9, Z3, Tuple(f.m), Tuple(f.
 fdesc(g::B200Grid{T}) where {T} = TpFieldDesc(4, g.bc, T === Float32 ? 0 : 1, 0, Z3, Z9, Z3, Z3, Z3, 0.0,
     Int64.(size(g.A)[2:4]), g.origin, g.spacing, pointer(g.A))
 fdesc(f) = throw(ArgumentError("field not supported by EnsembleB200: $(typeof(f)); use ZeroField, " *
-    "UniformField, AffineField, DipoleField or B200Grid"))
+    "UniformField, AffineField, DipoleField, B200Grid or a trilinear FieldInterpolator"))
+
+# ------------------------------------------------------------------ the reference's gridded field
+# A user's gridded problem holds `Field(FieldInterpolator(itp))` with `itp` the
+# FastInterpolations interpolant that build_interpolator(CartesianGrid, A, x, y, z,
+# 1, bc) made (src/utility/interpolation.jl:15-36,119-148,217-235).  The device
+# needs its node array, uniform axes and boundary condition.  They are found by
+# type among the interpolant's properties (FastInterpolations is a dependency of
+# the reference, so its field names are not relied on): the axes are a tuple of
+# three vectors, the nodes an array of SVector{3} (the reinterpreted (3, nx, ny,
+# nz) array, whose parent is used when it is one), and the boundary condition a
+# PeriodicBC / WrapExtrap / ClampExtrap / FillExtrap(NaN) value.  The result is
+# then checked against the interpolant itself at a few interior points, so a
+# cubic or nearest-node interpolant, or a non-uniform axis, is an ArgumentError
+# rather than a silently different field.
+function _walk(f, x, depth)
+    f(x) && return x
+    depth == 0 && return nothing
+    isstructtype(typeof(x)) || return nothing
+    for name in propertynames(x)
+        v = try
+            getproperty(x, name)
+        catch
+            continue
+        end
+        r = _walk(f, v, depth - 1)
+        isnothing(r) || return r
+    end
+    if x isa Tuple
+        for v in x
+            r = _walk(f, v, depth - 1)
+            isnothing(r) || return r
+        end
+    end
+    return nothing
+end
+
+_is_axes(v) = v isa Tuple && length(v) == 3 && all(a -> a isa AbstractVector{<:Real} && length(a) >= 2, v)
+_is_nodes(v) = v isa AbstractArray{<:SVector{3, <:AbstractFloat}, 3}
+_is_bc(v) = v isa TestParticle.PeriodicBC || v isa TestParticle.WrapExtrap || v isa TestParticle.ClampExtrap ||
+    v isa TestParticle.FillExtrap
+
+function _uniform_axis(a::AbstractVector{<:Real})
+    a isa AbstractRange && return Float64(first(a)), Float64(step(a))
+    n = length(a)
+    x0 = Float64(a[1])
+    h = (Float64(a[end]) - x0) / (n - 1)
+    for k in 1:n
+        abs(Float64(a[k]) - (x0 + (k - 1) * h)) <= 1e-12 * abs(h) ||
+            throw(ArgumentError("EnsembleB200: grid axis is not uniform (node $k); only uniform CartesianGrid " *
+                "axes are supported on the device"))
+    end
+    return x0, h
+end
+
+function _bc_code(bc)
+    if bc isa TestParticle.WrapExtrap
+        return Int32(2)
+    elseif bc isa TestParticle.PeriodicBC
+        ep = hasproperty(bc, :endpoint) ? getproperty(bc, :endpoint) : :exclusive
+        return ep === :inclusive ? Int32(3) : Int32(2)
+    elseif bc isa TestParticle.ClampExtrap
+        return Int32(1)
+    else  # FillExtrap: the device fills with NaN only
+        fv = hasproperty(bc, :fill_value) ? getproperty(bc, :fill_value) : NaN
+        all(isnan, fv) || throw(ArgumentError("EnsembleB200: FillExtrap supports NaN fill values only"))
+        return Int32(0)
+    end
+end
+
+"""
+    grid_of(fi::TestParticle.FieldInterpolator) -> B200Grid
+
+The device form of the reference's trilinear `FieldInterpolator`, sharing its
+node memory (no copy when the interpolant keeps the caller's array or an
+`Array{SVector{3}}`).  Used by `EnsembleB200` for every `FieldInterpolator` it
+meets; throws `ArgumentError` for interpolants the device cannot reproduce.
+"""
+function grid_of(fi::TestParticle.FieldInterpolator)
+    itp = fi.itp
+    axes = _walk(_is_axes, itp, 3)
+    V = _walk(_is_nodes, itp, 3)
+    bc = _walk(_is_bc, itp, 3)
+    (isnothing(axes) || isnothing(V)) &&
+        throw(ArgumentError("EnsembleB200: cannot find the axes and node array of $(typeof(itp))"))
+    isnothing(bc) && throw(ArgumentError("EnsembleB200: boundary condition of $(typeof(itp)) is not one of " *
+        "PeriodicBC, WrapExtrap, ClampExtrap or FillExtrap(NaN)"))
+    T = eltype(eltype(V))
+    nx, ny, nz = size(V)
+    P = parent(V)
+    A = if P isa Array{T, 4} && size(P) == (3, nx, ny, nz)
+        P                                    # the (3, nx, ny, nz) array itself
+    elseif V isa Array
+        unsafe_wrap(Array, Ptr{T}(pointer(V)), (3, nx, ny, nz))  # same bytes, V kept alive by fi
+    else
+        reshape(collect(reinterpret(T, vec(collect(V)))), 3, nx, ny, nz)
+    end
+    (x0, hx), (y0, hy), (z0, hz) = map(_uniform_axis, axes)
+    code = _bc_code(bc)
+    code == 3 && throw(ArgumentError("EnsembleB200: PeriodicBC(endpoint = :inclusive) needs the general-grid " *
+        "descriptor; use endpoint = :exclusive"))
+    g = B200Grid{T}(A, (x0, y0, z0), (hx, hy, hz), code)
+    # the interpolant itself is the reference: it must agree with the trilinear form
+    for (a, b, c) in ((0.37, 0.61, 0.23), (0.5, 0.5, 0.5), (0.91, 0.13, 0.77))
+        x = SVector(x0 + (a * (nx - 1)) * hx, y0 + (b * (ny - 1)) * hy, z0 + (c * (nz - 1)) * hz)
+        ref = fi(x)
+        dev = g(x)
+        tol = 64 * eps(float(promote_type(T, eltype(ref)))) * (1 + maximum(abs, ref))
+        maximum(abs, ref - dev) <= tol || throw(ArgumentError("EnsembleB200: $(typeof(itp)) is not a trilinear " *
+            "interpolant on uniform axes (order 1); the device supports order 1 here"))
+    end
+    return g
+end
+
+fdesc(fi::TestParticle.FieldInterpolator) = fdesc(grid_of(fi))
+device_view(f) = f
+device_view(fi::TestParticle.FieldInterpolator) = grid_of(fi)
 
 termdesc(::typeof(TestParticle.ODE_DEFAULT_ISOUTOFDOMAIN)) = TpTermDesc(0, 0, -Inf, Inf, (-Inf, -Inf, -Inf), (Inf, Inf, Inf), Inf)
 termdesc(T::Terminate) = TpTermDesc(T.flags, 0, T.rmin, T.rmax, T.lo, T.hi, T.tmax)
@@ -218,9 +339,10 @@ function check(ctx, st, what)
     st == -1 ? throw(ArgumentError("$what: $msg")) : error("$what: $msg (status $st)")
 end
 function field_handle(ctx, f)
-    d = Ref(fdesc(f))
+    g = device_view(f)   # grids are copied to the device inside tp_field_create
+    d = Ref(fdesc(g))
     h = Ref{Ptr{Cvoid}}(C_NULL)
-    GC.@preserve f check(ctx, ccall((:tp_field_create, libtpb200), Cint,
+    GC.@preserve f g check(ctx, ccall((:tp_field_create, libtpb200), Cint,
         (Ptr{Cvoid}, Ref{TpFieldDesc}, Ref{Ptr{Cvoid}}), ctx, d, h), "tp_field_create")
     return h[]
 end
@@ -395,6 +517,8 @@ function boris_final_state(U0::Matrix{Float64}, E, B; kw...)
 end
 
 field_cotangent(f::B200Grid, g, _) = ChainRulesCore.Tangent{typeof(f)}(; A = g)
+# the reference's FieldInterpolator: the node gradient, shaped like the (3, nx, ny, nz) array
+field_cotangent(f::TestParticle.FieldInterpolator, g, _) = g
 field_cotangent(f::UniformField, _, p) = ChainRulesCore.Tangent{typeof(f)}(; v = SVector{3}(p))
 field_cotangent(f::DipoleField, _, p) = ChainRulesCore.Tangent{typeof(f)}(; m = SVector{3}(p))
 field_cotangent(f, _, _) = ChainRulesCore.NoTangent()
@@ -404,8 +528,9 @@ function ChainRulesCore.rrule(::typeof(boris_final_state), U0::Matrix{Float64}, 
     function boris_final_state_pullback(dUN)
         G = Matrix{Float64}(ChainRulesCore.unthunk(dUN))
         dU0 = Matrix{Float64}(undef, 6, t.n)
-        gE = unwrap(E) isa B200Grid ? Array{Float64}(undef, size(unwrap(E).A)) : nothing
-        gB = unwrap(B) isa B200Grid ? Array{Float64}(undef, size(unwrap(B).A)) : nothing
+        vE, vB = device_view(unwrap(E)), device_view(unwrap(B))
+        gE = vE isa B200Grid ? Array{Float64}(undef, size(vE.A)) : nothing
+        gB = vB isa B200Grid ? Array{Float64}(undef, size(vB.A)) : nothing
         gp = Vector{Float64}(undef, 6)
         st = ccall((:tp_adjoint_backward, libtpb200), Cint,
             (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
