@@ -375,7 +375,7 @@ def detect(t, u, nsaved, surfaces, weights=None, weight: float = 1.0):
 
 
 def trig(x: np.ndarray, y: np.ndarray):
-    """(sin x, cos x, atan2(y, x)) of the hybrid's portable trigonometry."""
+    """(sin x, cos x, atan2(y, x)) of the portable trigonometry (hybrid gyrophase, Multistep rotation)."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.ascontiguousarray(y, dtype=np.float64)
     s, c, a = np.empty_like(x), np.empty_like(x), np.empty_like(x)

@@ -7,6 +7,7 @@
 #pragma once
 
 #include "grid_general.cuh"
+#include "ptrig.cuh"
 #include "tp_device.cuh"
 
 namespace tpb {
@@ -365,9 +366,11 @@ __device__ __forceinline__ D3 multistep_rot64(D3 v, D3 E, D3 B, double q2m, doub
         c3 = fma(-((4.0 * nd * nd + 2.0 * nd * nd * nd * nd) / 3.0), t_n_mag2, 2.0 * nd * nd);
         c6 = (n_term1 + n_term3) / 3.0;
     } else {
-        double alpha = atan(t_n_mag);
+        // atan and sincos of the reference, as the portable routines the
+        // oracle shares (ptrig.cuh): the same bits on the device and the CPU
+        double alpha = patan2(t_n_mag, 1.0);
         double s, c;
-        sincos(nd * alpha, &s, &c);
+        psincos(nd * alpha, s, c);
         double s2 = 2.0 * s * c;
         c1 = fma(c, c, -(s * s));
         c2 = s2 / t_n_mag;

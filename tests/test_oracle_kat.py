@@ -662,6 +662,27 @@ def test_portable_gyrophase_trig_accuracy(orc):
     assert np.max(np.abs(a - np.arctan2(y, x))) <= 4 * np.spacing(np.pi)
 
 
+def test_portable_trig_relative_accuracy_on_the_multistep_range(orc):
+    # The closed-form MultistepBoris rotation (multistep_boris.jl:110-119)
+    # calls atan(|t_n|) for |t_n| >= 1e-4 and sincos(n * alpha); the float64
+    # kernel and the oracle both use the portable routines there.  Relative
+    # error against libm: atan within 2 ulp up to tan(pi/16) (no half-angle
+    # reduction: the typical |t_n| of a step), 4 ulp above; sin and cos
+    # within 2 ulp of the larger of the value and 1e-3 (n * alpha lies in
+    # (0, n * pi / 2)).
+    rng = np.random.default_rng(1)
+    t = np.exp(rng.uniform(np.log(1e-4), np.log(1e4), 200000))
+    _, _, a = orc.trig(np.ones_like(t), t)  # atan2(t, 1)
+    ulps = np.abs(a - np.arctan(t)) / np.spacing(np.arctan(t))
+    assert np.max(ulps[t <= 0.1989]) <= 2
+    assert np.max(ulps) <= 4
+    for n in (1, 2, 4, 6):
+        x = n * np.arctan(t)
+        s, c, _ = orc.trig(x, np.ones_like(x))
+        assert np.max(np.abs(s - np.sin(x)) / np.spacing(np.maximum(np.abs(np.sin(x)), 1e-3))) <= 2
+        assert np.max(np.abs(c - np.cos(x)) / np.spacing(np.maximum(np.abs(np.cos(x)), 1e-3))) <= 2
+
+
 # ------------------------------------------------------------------ virtual detectors (test_utility.jl:768-960)
 def _line(x0, y0, vx, vy, z0=0.0, vz=0.0, n=21):
     t = np.arange(float(n))
