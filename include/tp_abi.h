@@ -377,6 +377,17 @@ typedef struct tp_points_desc {
 int tp_eval_points(tp_ctx* ctx, const tp_points_desc* desc, const tp_field* E,
                    const tp_field* B, const double* u, const double* t, int64_t n,
                    double* out);
+/* The same with per-point parameters, each optional (NULL: the desc's
+ * scalar): q2m_i and m_i (full orbit), q2m_i, q_i and mu_i (guiding
+ * centres), n values each, host or device memory.  An ensemble whose
+ * particles carry their own q, q/m and mu (the per-particle extension of
+ * tp_gc_run) is evaluated in one launch: the reference's get_work /
+ * get_fields (boris.jl:594-640) see one p per solve.                      */
+int tp_eval_points_params(tp_ctx* ctx, const tp_points_desc* desc,
+                          const tp_field* E, const tp_field* B, const double* u,
+                          const double* t, const double* q2m_i,
+                          const double* m_i, const double* q_i,
+                          const double* mu_i, int64_t n, double* out);
 
 /* ---- full-orbit solve (host buffers) --------------------------------------
  * Replaces _solve(::EnsembleAlg, ::TraceProblem, ::AbstractBoris, ...)

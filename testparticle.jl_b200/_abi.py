@@ -282,6 +282,7 @@ SIGNATURES = [
      [_P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     ("tp_field_update", C.c_int, [_P, _P]),
     ("tp_eval_points", C.c_int, [_P, C.POINTER(PointsDesc), _P, _P, _P, _P, C.c_int64, _P]),
+    ("tp_eval_points_params", C.c_int, [_P, C.POINTER(PointsDesc), _P, _P, _P, _P, _P, _P, _P, _P, C.c_int64, _P]),
     ("tp_detect_fluxes", C.c_int,
      [_P, _P, _P, C.c_int32, _P, C.c_int64, C.POINTER(Surface), C.c_int32, _P, C.c_double, _P, _P]),
     ("tp_detect_crossings", C.c_int,

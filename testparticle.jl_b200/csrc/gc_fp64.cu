@@ -63,10 +63,11 @@ __global__ void k_eval_points(PointsArgs a) {
     }
     if (a.want & 2) {
         double W[4];
+        const double q2m = a.q2m_i ? a.q2m_i[i] : a.q2m;
         if (a.kind == TP_POINTS_GC)
-            work_rates_gc64<GM_ANY>(a.f, x, s[3], t, a.q, a.q2m, a.mu, W);
+            work_rates_gc64<GM_ANY>(a.f, x, s[3], t, a.q_i ? a.q_i[i] : a.q, q2m, a.mu_i ? a.mu_i[i] : a.mu, W);
         else
-            work_rates64<GM_ANY>(a.f, x, D3{s[3], s[4], s[5]}, t, a.q2m, a.m, W);
+            work_rates64<GM_ANY>(a.f, x, D3{s[3], s[4], s[5]}, t, q2m, a.m_i ? a.m_i[i] : a.m, W);
         for (int k = 0; k < 4; ++k) o[c + k] = W[k];
     }
 }

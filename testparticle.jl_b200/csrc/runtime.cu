@@ -1720,6 +1720,12 @@ int tp_detect_first_crossing(tp_ctx* ctx, const double* t, const double* u, int3
 
 int tp_eval_points(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, const tp_field* B,
                    const double* u, const double* t, int64_t n, double* out) {
+    return tp_eval_points_params(ctx, d, E, B, u, t, nullptr, nullptr, nullptr, nullptr, n, out);
+}
+
+int tp_eval_points_params(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, const tp_field* B,
+                          const double* u, const double* t, const double* q2m_i, const double* m_i,
+                          const double* q_i, const double* mu_i, int64_t n, double* out) {
     if (!ctx || !d || !E || !B) return fail(ctx, TP_E_ARG, "null argument");
     if (d->kind != TP_POINTS_FULL_ORBIT && d->kind != TP_POINTS_GC) return fail(ctx, TP_E_ARG, "unknown state kind");
     if (d->want < 1 || d->want > 3) return fail(ctx, TP_E_ARG, "want must select fields (1), work (2) or both (3)");
@@ -1740,6 +1746,20 @@ int tp_eval_points(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, cons
     if (!u_dev) e = u_d.alloc(ub);
     if (e == cudaSuccess && !t_dev) e = t_d.alloc(tb);
     if (e == cudaSuccess && !o_dev) e = o_d.alloc(ob);
+    // per-point parameters: used in place when already on the device
+    const double* par[4] = {q2m_i, m_i, q_i, mu_i};
+    const double* par_d[4] = {nullptr, nullptr, nullptr, nullptr};
+    DBuf par_buf[4];
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        if (!par[k]) continue;
+        if (is_device_ptr(par[k])) {
+            par_d[k] = par[k];
+            continue;
+        }
+        e = par_buf[k].alloc(tb);
+        if (e == cudaSuccess) e = copy_to_device(ctx, par_buf[k].p, par[k], tb);
+        par_d[k] = par_buf[k].as<double>();
+    }
     if (e != cudaSuccess) return fail(ctx, TP_E_NOMEM, "device allocation");
     if (!u_dev) e = copy_to_device(ctx, u_d.p, u, ub);
     if (e == cudaSuccess && !t_dev) e = copy_to_device(ctx, t_d.p, t, tb);
@@ -1758,6 +1778,10 @@ int tp_eval_points(tp_ctx* ctx, const tp_points_desc* d, const tp_field* E, cons
     a.m = d->m;
     a.q = d->q;
     a.mu = d->mu;
+    a.q2m_i = par_d[0];
+    a.m_i = par_d[1];
+    a.q_i = par_d[2];
+    a.mu_i = par_d[3];
     a.out = o_dev ? out : o_d.as<double>();
     if (e == cudaSuccess) e = launch_eval_points(a, ctx->stream);
     if (e == cudaSuccess) e = o_dev ? cudaStreamSynchronize(ctx->stream) : copy_to_host(ctx, out, o_d.p, ob);

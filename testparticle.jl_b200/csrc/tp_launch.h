@@ -109,6 +109,11 @@ struct PointsArgs {
     int64_t n;
     int32_t stride, want, wout, kind;
     double q2m, m, q, mu;
+    // optional per-point parameters (null: the scalar above)
+    const double* q2m_i;
+    const double* m_i;
+    const double* q_i;
+    const double* mu_i;
     double* out;       // n rows of wout doubles
 };
 

@@ -33,17 +33,13 @@ def _eval(sol, want: int, device: int = 0):
     if isinstance(prob, TraceGCProblem):
         q, q2m, mu, E, B = prob.p[:5]
         E, B = as_field(E), as_field(B)
-        per = any(np.ndim(a) > 0 for a in (q, q2m, mu))
-        if not per:
-            return ctx.eval_points(E, B, u, t, gc=True, want=want, q2m=q2m, q=q, mu=mu)
-        out = np.empty((t.size, 6 * (want & 1) + 4 * ((want >> 1) & 1)))
+        # per-particle q, q2m, mu (an extension) become one value per saved
+        # state, so the whole ensemble is still one launch
         idx = np.asarray(idx)
-        for i in np.unique(idx):   # per-particle q, q2m, mu (an extension): one call per trajectory
-            sel = idx == i
-            pick = (lambda a: float(np.asarray(a).reshape(-1)[i]) if np.ndim(a) > 0 else float(a))  # noqa: E731
-            out[sel] = ctx.eval_points(E, B, u[sel], t[sel], gc=True, want=want, q2m=pick(q2m), q=pick(q),
-                                       mu=pick(mu))
-        return out
+        per_state = (lambda a: np.asarray(a, dtype=np.float64).reshape(-1)[idx]  # noqa: E731
+                     if np.ndim(a) > 0 else float(a))
+        return ctx.eval_points(E, B, u, t, gc=True, want=want, q2m=per_state(q2m), q=per_state(q),
+                               mu=per_state(mu))
     q2m, m, E, B = prob.p[:4]
     return ctx.eval_points(as_field(E), as_field(B), u, t, gc=False, want=want, q2m=q2m, m=m)
 

@@ -296,9 +296,10 @@ class Context:
         _check(self.lib, self.handle, code, "tp_gc_to_full")
         return xv
 
-    def eval_points(self, E, B, u: np.ndarray, t: np.ndarray, *, gc: bool, want: int, q2m: float = 0.0,
-                    m: float = 0.0, q: float = 0.0, mu: float = 0.0) -> np.ndarray:
-        """tp_eval_points: E, B (want & 1) and work rates (want & 2) at n states."""
+    def eval_points(self, E, B, u: np.ndarray, t: np.ndarray, *, gc: bool, want: int, q2m=0.0, m=0.0, q=0.0,
+                    mu=0.0) -> np.ndarray:
+        """tp_eval_points: E, B (want & 1) and work rates (want & 2) at n states.  q2m, m, q and mu are
+        scalars or arrays of one value per state (tp_eval_points_params: still one launch)."""
         u = np.ascontiguousarray(u, dtype=np.float64)
         t = np.ascontiguousarray(t, dtype=np.float64).reshape(-1)
         if u.ndim != 2 or u.shape[0] != t.size:
@@ -307,11 +308,24 @@ class Context:
         d.kind = _abi.TP_POINTS_GC if gc else _abi.TP_POINTS_FULL_ORBIT
         d.want = int(want)
         d.stride = int(u.shape[1])
-        d.q2m, d.m, d.q, d.mu = float(q2m), float(m), float(q), float(mu)
+        per = {}
+        for name, val in (("q2m", q2m), ("m", m), ("q", q), ("mu", mu)):
+            if np.ndim(val) == 0:
+                setattr(d, name, float(val))
+            else:
+                a = np.ascontiguousarray(val, dtype=np.float64).reshape(-1)
+                if a.size != t.size:
+                    raise ValueError(f"{name} must be a scalar or one value per state")
+                per[name] = a
         wout = 6 * (want & 1) + 4 * ((want >> 1) & 1)
         out = np.empty((t.size, wout))
-        code = self.lib.tp_eval_points(self.handle, C.byref(d), self.field(E), self.field(B), _ptr(u), _ptr(t),
-                                       t.size, _ptr(out))
+        if per:
+            code = self.lib.tp_eval_points_params(self.handle, C.byref(d), self.field(E), self.field(B), _ptr(u),
+                                                  _ptr(t), _ptr(per.get("q2m")), _ptr(per.get("m")),
+                                                  _ptr(per.get("q")), _ptr(per.get("mu")), t.size, _ptr(out))
+        else:
+            code = self.lib.tp_eval_points(self.handle, C.byref(d), self.field(E), self.field(B), _ptr(u),
+                                           _ptr(t), t.size, _ptr(out))
         _check(self.lib, self.handle, code, "tp_eval_points")
         return out
 

@@ -194,3 +194,29 @@ def test_config5_adjoint_full_size(tp):
             a = np.asarray(table, np.float64).reshape(3, -1)
             s = a.sum(axis=1)
             assert np.all(np.abs(g.param[k:k + 3] - s) <= 1e-12 * np.abs(a).sum(axis=1))
+
+
+def test_config4_get_work_is_one_launch(tp):
+    """get_work / get_fields of 2^20 guiding centres that carry their own q, q/m
+    and mu: one tp_eval_points_params call for the whole ensemble, equal to the
+    save_work columns the solve wrote (same kernel code, same states)."""
+    w = tp.workloads.config4()
+    prob = tp.TraceGCProblem(w.y0, (0.0, 1.0), (w.q, w.q2m, w.mu, w.E, w.B))
+    sols = tp.solve(prob, tp.EnsembleB200(), alg="rk4", dt=w.tau_b / 200, tend=0.05 * w.tau_b, savestepinterval=5,
+                    save_work=True)
+    ctx = tp.Context.get(0)
+    calls = []
+    orig = ctx.eval_points
+
+    def counted(*a, **k):
+        calls.append(1)
+        return orig(*a, **k)
+
+    ctx.eval_points = counted
+    try:
+        work = tp.get_work(sols)
+    finally:
+        del ctx.eval_points
+    assert len(calls) == 1
+    assert work.shape == (sols.t_all.size, 4)
+    assert np.array_equal(work, sols.u_all[:, 4:8])
