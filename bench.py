@@ -1,14 +1,22 @@
 #!/usr/bin/env python
 """Benchmark of the particle-push hot path on B200 (one JSON line on rank 0).
 
-Workload (default): the gridded-Boris configuration -- 1e6 protons in a 128^3
-periodic turbulent E/B field (float32 nodes, trilinear), dt = T_gyro(B0)/50,
-1e4 time steps, saves every 1000 steps.  One bench step is one complete solve
-of that workload (1e10 particle-steps) with the initial states already in HBM;
-`value` is particle-steps/s of the FP32-compensated push, the FP64 drop-in
-path and the FP32C error against it are reported beside it.  `e2e` is the
-same solve through the public API (solve() with host arrays: the upload of the
-initial states and the download of every saved state are inside the timing).
+Workload (default): the Earth-dipole ensemble -- 1e6 protons, kinetic energy
+log-uniform 10 keV - 10 MeV, isotropic pitch angles, L uniform in [3, 7],
+MultistepBoris4(n=2) at dt_i = 0.02 T_gyro(|B(r0)|), 1e4 steps, termination
+at 1 and 15 R_E, saves every 1000 steps.  One bench step is one complete
+solve of that workload (up to 1e10 particle-steps) with the initial states
+already in HBM; `value` is particle-steps/s of the FP32-compensated push
+(float rotation factors, compensated float positions, float64 field and
+velocity).  Beside it: the plain FP64 drop-in path on the same workload, the
+FP32C final-position error against it, and how far float64 runs started a
+float32 ulp (and a float64 ulp) away separate -- the orbits' own
+sensitivity, which classifies them into regular and chaotic ones.  `e2e` is
+the same solve through the public API (solve() with host arrays: the upload
+of the initial states, dt and tspan, and the download of every saved state
+are inside the timing).  `--workload config2` makes the gridded turbulent
+field (128^3, 1e6 protons, 1e4 Boris steps) the headline instead; by default
+it is a leg.
 
 --impl reference times the CPU restatement of the reference's EnsembleThreads
 path (oracle/, OpenMP on all host cores) on a bounded sample of the same
@@ -36,12 +44,23 @@ sys.path.insert(0, str(ROOT))
 
 import __graft_entry__ as ge  # noqa: E402
 
-BYTES_PER_PARTICLE_STEP = 192  # 8 trilinear corners x (E, B) x 3 float32
-# DRAM bytes per particle-step of k_fixed32c on this workload, from an ncu
-# capture (profiles/k_fixed32c_config2_gridded.md): 1.683 GB / 2e8 particle-steps
+# gridded workload (config 2): algorithmic bytes of one particle-step, 8
+# trilinear corners x (E, B) x 3 float32, and the DRAM bytes per particle-step
+# of k_fixed32c measured by ncu (1.683 GB over 2e8 particle-steps; the 67 MB
+# field table is L2-resident)
+BYTES_PER_PARTICLE_STEP = 192
 TRAFFIC_PER_PARTICLE_STEP = 8.4
+# dipole workload (config 3, MultistepBoris4(2)): algorithmic flops of one
+# particle-step (the rotation 121, the dipole 29), and the warp instructions
+# one warp-step of k_fixed32c<MULTI, queue, analytic> issues and the DRAM
+# bytes per particle-step, both measured by ncu on 262144 protons x 200 steps
+FLOPS_PER_PARTICLE_STEP_DIPOLE = 150
+INST_PER_WARP_STEP_DIPOLE = 348.5
+TRAFFIC_PER_PARTICLE_STEP_DIPOLE = 0.32
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+SMS = 148
+ISSUE_PER_SM_CLOCK = 4  # one warp instruction per clock on each of the four SM sub-partitions
 
 
 def _peaks():
@@ -263,11 +282,15 @@ def _plan(tp, w, alg, prec, device, step_cap=0):
                          savestepinterval=w.savestepinterval, isoutside=w.isoutside, step_cap=step_cap)
 
 
-def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt):
-    """Dipole ensemble (config 3): MultistepBoris4(n=2) and AdaptiveBoris(0.1), FP32C vs FP64."""
+def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt, multistep=True):
+    """Dipole ensemble (config 3): AdaptiveBoris(0.1) (and MultistepBoris4(n=2)
+    when it is not the headline), FP32C vs FP64."""
     w = tp.workloads.config3(n=n, nt=nt, ssi=min(1000, nt))
     out = {"workload": w.name, "particles": n, "time_steps": nt}
-    for name, alg, cap in (("multistep4_n2", tp.MultistepBoris4(2), 0), ("adaptive_0.1", tp.AdaptiveBoris(0.1), nt)):
+    cases = [("adaptive_0.1", tp.AdaptiveBoris(0.1), nt)]
+    if multistep:
+        cases.insert(0, ("multistep4_n2", tp.MultistepBoris4(2), 0))
+    for name, alg, cap in cases:
         p32, p64 = _plan(tp, w, alg, "fp32c", ctx.device, cap), _plan(tp, w, alg, "fp64", ctx.device, cap)
         shapes = {k: ctx.autotune(pl.desc, pl.E, pl.B, pl.u0, max_steps=200) for k, pl in (("fp32c", p32),
                                                                                           ("fp64", p64))}
@@ -522,20 +545,175 @@ def profile_case(tp, case, device):
                          savestepinterval=100000, save_everystep=False, maxiters=1_000_000, **kw)
 
 
+def _device_err(a, b, torch):
+    """|x_a - x_b| / |x_b| per save slot and particle (slots, n), on the device."""
+    return (torch.linalg.vector_norm(a - b, dim=1) / torch.linalg.vector_norm(b, dim=1))
+
+
+def _quantiles(e):
+    e = e[np.isfinite(e)]
+    if e.size == 0:
+        return None
+    q = np.quantile(e, [0.5, 0.9, 0.99, 0.999])
+    return {"p50": float(q[0]), "p90": float(q[1]), "p99": float(q[2]), "p999": float(q[3]), "max": float(e.max()),
+            "orbits": int(e.size)}
+
+
+def orbit_errors(torch, run, p32, p64):
+    """FP32C against FP64 on the same workload, and the orbits' own sensitivity.
+
+    Runs FP32C, FP64 and FP64 from three perturbed starts (each component
+    rounded to float32; all scaled by 1 + 2^-23, one float32 ulp; scaled by
+    1 + 2^-52, one float64 ulp) into the same device buffers, and compares the
+    saved positions.  An orbit is "regular" when the float32-ulp starts stay
+    within 1e-6 (round) and 1e-5 (scale) of the float64 orbit at every save:
+    there the float32 arithmetic itself is what the error measures.
+    """
+    def saves(plan):
+        run.launch(plan)
+        torch.cuda.synchronize()
+        run.check()
+        return run.u_out[:, :3, :].clone(), run.retc.clone()
+
+    x32, rc32 = saves(p32)
+    x64, rc64 = saves(p64)
+    ok = (rc32 == 1) & (rc64 == 1)
+    e32 = _device_err(x32, x64, torch)
+    del x32
+    u0 = run.u0.clone()
+    seps = {}
+    for name, pert in (("f32ulp_round", lambda u: u.float().double()), ("f32ulp_scale", lambda u: u * (1.0 + 2.0 ** -23)),
+                       ("f64ulp_scale", lambda u: u * (1.0 + 2.0 ** -52))):
+        run.u0.copy_(pert(u0))
+        xp, rcp = saves(p64)
+        ok &= rcp == 1
+        seps[name] = _device_err(xp, x64, torch)
+        del xp
+    run.u0.copy_(u0)
+    okc = ok.cpu().numpy()
+    fin = e32[-1].cpu().numpy()[okc]
+    out = {"fp32c_error_vs_fp64": _quantiles(fin), "orbits_compared": int(okc.sum()),
+           "fp64_vs_fp64": {k: _quantiles(v[-1].cpu().numpy()[okc]) for k, v in seps.items()}}
+    r_max = seps["f32ulp_round"].amax(dim=0).cpu().numpy()[okc]
+    s_max = seps["f32ulp_scale"].amax(dim=0).cpu().numpy()[okc]
+    reg = (r_max < 1e-6) & (s_max < 1e-5)
+    out["regular_orbits"] = {"classifier": "float64 runs started a float32 ulp away stay within 1e-6 (components "
+                                           "rounded) and 1e-5 (scaled by 1 + 2^-23) at every save",
+                             "fraction": float(reg.mean()), "fp32c_error": _quantiles(fin[reg])}
+    reg1 = r_max < 1e-6
+    out["regular_orbits_round_only"] = {"classifier": "components rounded to float32: within 1e-6 at every save",
+                                        "fraction": float(reg1.mean()), "fp32c_error": _quantiles(fin[reg1])}
+    sep = seps["f32ulp_scale"][-1].cpu().numpy()[okc]
+    ratio = fin / np.maximum(sep, 1e-300)
+    out["fp32c_error_over_f32ulp_scale_separation"] = {k: float(v) for k, v in zip(
+        ("p50", "p90", "p99"), np.quantile(ratio, [0.5, 0.9, 0.99]))}
+    return out
+
+
+def headline_run(tp, torch, ctx, dist, dev, stream, flush, world, local, args, w, alg):
+    """Timed FP32C and FP64 solves of workload w, errors, and the end-to-end solve."""
+    p32, p64 = _plan(tp, w, alg, "fp32c", local), _plan(tp, w, alg, "fp64", local)
+    tune = None if args.no_autotune else {
+        "fp32c": ctx.autotune(p32.desc, p32.E, p32.B, p32.u0, max_steps=200),
+        "fp64": ctx.autotune(p64.desc, p64.E, p64.B, p64.u0, max_steps=200)}
+    run = DeviceRun(tp, torch, ctx, p32, dev, stream)
+    sampler = ClockSampler(local)
+    run.launch(p32)  # first call builds any field tables
+    torch.cuda.synchronize()
+    sampler.start()
+    tot32 = timed(torch, dist, dev, run, p32, args.steps, args.warmup, flush)
+    clocks = sampler.stop()
+    ps_step = run.particle_steps()
+    k64 = max(args.fp64_steps, 1)
+    tot64 = timed(torch, dist, dev, run, p64, k64, 1, flush)
+    ps64 = run.particle_steps()
+    errs = orbit_errors(torch, run, p32, p64)
+    value = whole_job_rate(world, ps_step * args.steps, tot32 * 1e-3)
+    value64 = whole_job_rate(world, ps64 * k64, tot64 * 1e-3)
+
+    # end to end through the public API (host arrays in, packed host results out)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    e2e_t = []
+    h2d = d2h = 0
+    sol = None
+    for k in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol = tp.solve(prob, alg, tp.EnsembleB200(device=local, precision="fp32c"), dt=w.dt, tend=w.tend,
+                       savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+        el = time.perf_counter() - t0
+        if k > 0:
+            e2e_t.append(el)
+        h2d = w.u0.nbytes + (0 if w.tend is None else np.asarray(w.tend).nbytes) + \
+            (0 if np.ndim(w.dt) == 0 else np.asarray(w.dt).nbytes)
+        d2h = sol.t_all.nbytes + sol.u_all.nbytes + sol.nsaved.nbytes + sol.retcodes.nbytes + sol.nsteps.nbytes
+    e2e_value = None
+    if e2e_t:
+        e2e_time = max_over_ranks(dist, max(e2e_t), dev)
+        e2e_value = whole_job_rate(world, float(sol.nsteps.sum()), e2e_time)
+    del sol
+    return {"value": value, "value64": value64, "tot32": tot32, "tot64": tot64, "k64": k64, "ps_step": ps_step,
+            "clocks": clocks, "tune": tune, "errors": errs, "e2e": e2e_value, "h2d": h2d, "d2h": d2h, "n": run.n}
+
+
+def gridded_roofline(r, world, args, peak, peak_kind):
+    kernel_s = r["tot32"] * 1e-3 / args.steps
+    achieved = BYTES_PER_PARTICLE_STEP * r["ps_step"] / kernel_s / 1e9
+    sm_clock = (r["clocks"].get("sm_mhz") or 1965.0) * 1e6
+    l1_ceiling = SMS * sm_clock / 8  # one L1 wavefront per SM clock, 8 corner lines per particle-step
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": TRAFFIC_PER_PARTICLE_STEP * r["ps_step"],
+            "note": f"{BYTES_PER_PARTICLE_STEP} algorithmic B/particle-step; peak {peak_kind}; the field table is "
+                    f"L2-resident (DRAM {TRAFFIC_PER_PARTICLE_STEP} B/particle-step by ncu), so the binding "
+                    "ceiling is the L1 wavefront one beside this"}
+    l1 = {"value": l1_ceiling, "unit": "particle-steps/s", "frac": r["value"] / world / l1_ceiling,
+          "note": "148 SMs x SM clock / 8 corner lines per particle-step"}
+    return roof, l1
+
+
+def dipole_roofline(r, world, args):
+    """Instruction-issue ceiling of the dipole push: no field memory and no
+    contraction, so neither HBM nor the tensor cores bound it."""
+    kernel_s = r["tot32"] * 1e-3 / args.steps
+    sm_clock = (r["clocks"].get("sm_mhz") or 1965.0) * 1e6
+    peak = SMS * ISSUE_PER_SM_CLOCK * sm_clock
+    warp_steps = r["ps_step"] / 32.0
+    achieved = INST_PER_WARP_STEP_DIPOLE * warp_steps / kernel_s
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp-instructions/s",
+            "frac": achieved / peak, "traffic": TRAFFIC_PER_PARTICLE_STEP_DIPOLE * r["ps_step"],
+            "flops": {"per_particle_step": FLOPS_PER_PARTICLE_STEP_DIPOLE,
+                      "achieved_tflops": FLOPS_PER_PARTICLE_STEP_DIPOLE * r["ps_step"] / kernel_s / 1e12},
+            "note": f"{INST_PER_WARP_STEP_DIPOLE:.0f} warp instructions per warp-step (ncu, 262144 x 200 steps) x "
+                    "warp-steps / kernel time, against 148 SMs x 4 issue slots x the sampled SM clock; "
+                    "MEASURED_PEAKS.json holds no FP32 or FP64 peak, so the flop rate is stated without a "
+                    "fraction; DRAM traffic (inputs and saves only) by ncu"}
+
+
+def leg_gridded(tp, torch, ctx, dist, dev, stream, flush, world, local, args, peak, peak_kind):
+    """The gridded turbulent field (config 2): FP32C and FP64 Boris, 1e6 x 1e4."""
+    w = _workload(tp, "config2", args.particles, args.nt)
+    r = headline_run(tp, torch, ctx, dist, dev, stream, flush, world, local, args, w, tp.Boris())
+    roof, l1 = gridded_roofline(r, world, args, peak, peak_kind)
+    return {"workload": w.name, "particles": r["n"], "time_steps": w.nt,
+            "fp32c": r["value"], "fp64": r["value64"], "unit": "particle-steps/s",
+            "speedup_fp32c_over_fp64": r["value"] / r["value64"], "errors": r["errors"],
+            "roofline": roof, "l1_wavefront_ceiling": l1, "e2e": r["e2e"], "autotune": r["tune"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3"])
+    ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3"])
     ap.add_argument("--particles", type=int, default=1_000_000)
-    ap.add_argument("--sample", type=int, default=150_000,
-                    help="particles of the CPU legs (about 10 s of host work at 16 cores)")
+    ap.add_argument("--sample", type=int, default=0,
+                    help="particles of the CPU legs (default: about 10-20 s of host work at 16 cores)")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-legs", action="store_true", help="skip the dipole / guiding-centre legs")
+    ap.add_argument("--no-legs", action="store_true", help="skip the gridded / adaptive / guiding-centre / adjoint legs")
     ap.add_argument("--nt", type=int, default=10_000, help="time steps (reduced only for profiling)")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (profiling)")
     ap.add_argument("--next-rows", action="store_true",
@@ -550,6 +728,10 @@ def main():
     ap.add_argument("--adj-n", type=int, default=1 << 18)
     ap.add_argument("--adj-nt", type=int, default=4096)
     args = ap.parse_args()
+    if args.sample <= 0:
+        # oracle rates at 16 threads: ~1.5e8 (gridded Boris) and ~1.3e8
+        # (dipole Multistep) particle-steps/s: about 10 s of host work
+        args.sample = {"config2": 150_000, "config3": 150_000}.get(args.workload, 1000)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -578,72 +760,23 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
-
-    p32, p64 = _plan(tp, w, alg, "fp32c", local), _plan(tp, w, alg, "fp64", local)
-    # launch shapes chosen by the autotuner on a sample (untimed)
-    tune = None if args.no_autotune else {
-        "fp32c": ctx.autotune(p32.desc, p32.E, p32.B, p32.u0, max_steps=200),
-        "fp64": ctx.autotune(p64.desc, p64.E, p64.B, p64.u0, max_steps=200)}
-    run = DeviceRun(tp, torch, ctx, p32, dev, stream)
-
-    # ---- FP32C (headline), clocks sampled during the timed region
-    sampler = ClockSampler(local)
-    run.launch(p32)  # first call builds the interleaved field table
-    torch.cuda.synchronize()
-    sampler.start()
-    tot32 = timed(torch, dist, dev, run, p32, args.steps, args.warmup, flush)
-    clocks = sampler.stop()
-    ps_step = run.particle_steps()
-    fs32 = run.final_states()
-
-    # ---- FP64 drop-in path on the same workload
-    k64 = max(args.fp64_steps, 1)
-    tot64 = timed(torch, dist, dev, run, p64, k64, 1, flush)
-    ps64 = run.particle_steps()
-    fs64 = run.final_states()
-    err = _rel_err(fs32, fs64)
-    # the same float64 solve started 1 ulp away: how fast neighbouring orbits
-    # separate in this field (chaotic flows separate at any precision)
-    u0_saved = run.u0.clone()
-    run.u0.mul_(1.0 + 2.0 ** -52)
-    run.launch(p64)
-    torch.cuda.synchronize()
-    chaos = _rel_err(run.final_states(), fs64)
-    run.u0.copy_(u0_saved)
-
-    value = whole_job_rate(world, ps_step * args.steps, tot32 * 1e-3)
-    value64 = whole_job_rate(world, ps64 * k64, tot64 * 1e-3)
-    kernel_s = tot32 * 1e-3 / args.steps
     peak, peak_kind = _peaks()
-    achieved = BYTES_PER_PARTICLE_STEP * ps_step / kernel_s / 1e9
-    sm_clock = (clocks.get("sm_mhz") or 1965.0) * 1e6
-    l1_ceiling = 148 * sm_clock / 8  # one L1 wavefront per SM clock, 8 corner lines per particle-step
 
-    # ---- end to end through the public API (host arrays in, packed host results out)
-    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
-    e2e_t = []
-    h2d = d2h = 0
-    sol = None
-    for k in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        sol = tp.solve(prob, alg, tp.EnsembleB200(device=local, precision="fp32c"), dt=w.dt, tend=w.tend,
-                       savestepinterval=w.savestepinterval, isoutside=w.isoutside)
-        el = time.perf_counter() - t0
-        if k > 0:
-            e2e_t.append(el)
-        h2d = w.u0.nbytes + (0 if w.tend is None else np.asarray(w.tend).nbytes) + \
-            (0 if np.ndim(w.dt) == 0 else np.asarray(w.dt).nbytes)
-        d2h = sol.t_all.nbytes + sol.u_all.nbytes + sol.nsaved.nbytes + sol.retcodes.nbytes + sol.nsteps.nbytes
-    e2e_value = None
-    if e2e_t:
-        e2e_time = max_over_ranks(dist, max(e2e_t), dev)
-        e2e_value = whole_job_rate(world, float(sol.nsteps.sum()), e2e_time)
-    del sol
+    r = headline_run(tp, torch, ctx, dist, dev, stream, flush, world, local, args, w, alg)
+    value, value64 = r["value"], r["value64"]
+    if args.workload == "config2":
+        roof, l1 = gridded_roofline(r, world, args, peak, peak_kind)
+        extra_roof = {"l1_wavefront_ceiling": l1}
+    else:
+        roof, extra_roof = dipole_roofline(r, world, args), {}
 
     legs = {}
     if not args.no_legs:
-        legs["dipole_config3"] = leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, 1_000_000, args.nt)
+        if args.workload != "config2":
+            legs["gridded_config2"] = leg_gridded(tp, torch, ctx, dist, dev, stream, flush, world, local, args,
+                                                  peak, peak_kind)
+        legs["dipole_config3"] = leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, 1_000_000, args.nt,
+                                            multistep=args.workload != "config3")
         if rank == 0:
             legs["guiding_centre_config4"] = leg_gc(tp, 1 << 20)
         legs["adjoint_config5"] = leg_adjoint(tp, torch, ctx, dev, stream, flush)
@@ -658,33 +791,26 @@ def main():
             cpu = {"value": rate, "unit": "particle-steps/s", "cores": orc.max_threads(), "kind": "port",
                    "sample": f"{args.sample} particles x {w.nt} steps of the same workload, FP64 reference "
                              f"order, {el:.1f} s (C++ restatement of the reference EnsembleThreads path)"}
+        alg_name = "MultistepBoris4(n=2)" if args.workload == "config3" else "Boris()"
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot32 / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["tot32"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+compensated",
             "data": "synthetic (seeded SplitMix64)",
-            "config": {"workload": w.name, "particles": run.n, "time_steps": w.nt,
+            "config": {"workload": w.name, "algorithm": alg_name, "particles": r["n"], "time_steps": w.nt,
                        "savestepinterval": w.savestepinterval, "precision": "fp32c",
                        "inputs_in_hbm": True, "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}"},
-            "fp64": {"value": value64, "unit": "particle-steps/s", "ms_per_step": tot64 / k64,
+            "fp64": {"value": value64, "unit": "particle-steps/s", "ms_per_step": r["tot64"] / r["k64"],
                      "speedup_fp32c_over_fp64": value / value64},
-            "fp32c_error_vs_fp64": _err_summary(err),
-            "fp64_vs_fp64_1ulp_start": _err_summary(chaos),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": TRAFFIC_PER_PARTICLE_STEP * ps_step,
-                         "note": f"{BYTES_PER_PARTICLE_STEP} algorithmic B/particle-step; peak {peak_kind}; "
-                                 "the field table is L2-resident (DRAM traffic from an ncu capture, "
-                                 f"{TRAFFIC_PER_PARTICLE_STEP} B/particle-step), so frac > 1 is possible"},
-            "l1_wavefront_ceiling": {"value": l1_ceiling, "unit": "particle-steps/s",
-                                     "frac": value / world / l1_ceiling,
-                                     "note": "148 SMs x SM clock / 8 corner lines per particle-step"},
+            **r["errors"],
+            "roofline": roof, **extra_roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": r["e2e"], "unit": "particle-steps/s", "h2d_bytes_per_step": int(r["h2d"]),
+                    "d2h_bytes_per_step": int(r["d2h"])},
             "gpu_launches": args.steps,
-            "autotune": tune,
-            "clocks": clocks,
+            "autotune": r["tune"],
+            "clocks": r["clocks"],
             "legs": legs,
         }
         print(json.dumps(line), flush=True)

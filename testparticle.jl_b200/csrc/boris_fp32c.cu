@@ -27,23 +27,27 @@ namespace tpb {
 
 namespace {
 
-__device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, const CV& vc, double t) {
-    const F3 v = vc.h;
+template <int FK>
+__device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, const typename Vel32<FK>::V& v,
+                                          double t) {
     const DevTerm& T = a.term;
     int f = T.flags;
     if (f & TP_TERM_NAN)
-        if (isnan(p.hi[0]) || isnan(p.hi[1]) || isnan(p.hi[2]) || isnan(v.x) || isnan(v.y) ||
-            isnan(v.z))
-            return true;
+        if (isnan(p.hi[0]) || isnan(p.hi[1]) || isnan(p.hi[2]) || Vel32<FK>::has_nan(v)) return true;
     if (f & (TP_TERM_SHELL | TP_TERM_BOX)) {
-        double x = cpos_value(a, p, 0), y = cpos_value(a, p, 1), z = cpos_value(a, p, 2);
+        // in float on hi + lo: no axis wraps when a spatial predicate is set,
+        // and the float-side position already differs from the float64 one
+        // by more than the float rounding of the test (no float64 sqrt)
+        const float x = p.hi[0] + p.lo[0], y = p.hi[1] + p.lo[1], z = p.hi[2] + p.lo[2];
         if (f & TP_TERM_SHELL) {
-            double rr = sqrt((x * x + y * y) + z * z);
-            if (rr < T.rmin || rr > T.rmax) return true;
+            const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+            const float rmin2 = T.rmin > 0.0 ? (float)(T.rmin * T.rmin) : -1.0f;
+            const float rmax2 = T.rmax >= 0.0 ? (float)(T.rmax * T.rmax) : -1.0f;
+            if (r2 < rmin2 || r2 > rmax2) return true;
         }
         if (f & TP_TERM_BOX) {
-            if (x < T.lo[0] || x > T.hi[0] || y < T.lo[1] || y > T.hi[1] || z < T.lo[2] ||
-                z > T.hi[2])
+            if (x < (float)T.lo[0] || x > (float)T.hi[0] || y < (float)T.lo[1] || y > (float)T.hi[1] ||
+                z < (float)T.lo[2] || z > (float)T.hi[2])
                 return true;
         }
     }
@@ -54,6 +58,7 @@ __device__ __forceinline__ bool outside32(const BorisArgs& a, const CPos& p, con
 
 template <int FK>
 struct Saver32 {
+    using P = Vel32<FK>;
     const BorisArgs& a;
     int W;
     // slot width: the state, E and B (float evaluation, as the push sees
@@ -62,7 +67,8 @@ struct Saver32 {
     // of this kernel's registers)
     __device__ Saver32(const BorisArgs& a_)
         : a(a_), W(6 + (a_.save_fields ? 6 : 0) + (a_.save_work ? 4 : 0)) {}
-    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, const CV& v, double t) const {
+    __device__ __forceinline__ void save(int64_t i, int64_t k, const CPos& p, const typename P::V& v,
+                                         double t) const {
         if (k >= a.nslots) {
             set_status(a.status, TP_E_OVERFLOW);
             return;
@@ -73,12 +79,12 @@ struct Saver32 {
         u[0 * n] = cpos_value(a, p, 0);
         u[1 * n] = cpos_value(a, p, 1);
         u[2 * n] = cpos_value(a, p, 2);
-        u[3 * n] = (double)v.h.x + (double)v.l.x;
-        u[4 * n] = (double)v.h.y + (double)v.l.y;
-        u[5 * n] = (double)v.h.z + (double)v.l.z;
+        u[3 * n] = P::comp(v, 0);
+        u[4 * n] = P::comp(v, 1);
+        u[5 * n] = P::comp(v, 2);
         if (a.save_fields) {
-            F3 E, B;
-            eval_EB32t<FK>(a.f, p, t, E, B);
+            typename P::Fv E, B;
+            P::fields(a.f, p, t, E, B);
             u[6 * n] = E.x;
             u[7 * n] = E.y;
             u[8 * n] = E.z;
@@ -104,6 +110,9 @@ __device__ __forceinline__ int64_t next_particle32(const BorisArgs& a, int64_t& 
 // ---------------------------------------------------------------- fixed step
 template <bool MULTI, bool QUEUE, int FK>
 __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
+    using P = Vel32<FK>;
+    using V = typename P::V;
+    using Fv = typename P::Fv;
     const Saver32<FK> S(a);
     const bool stat = fields_static32(a.f);
     const uint64_t t_start = globaltimer_ns();
@@ -111,9 +120,10 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
 
     int64_t i = -1;
     CPos p;
-    CV v{};
+    V v{};
     double dt = 0, t = 0, t1 = 0, t_last = 0;
-    float dth = 0, dtl = 0, hstep = 0;
+    float dth = 0, dtl = 0;
+    typename P::H hstep = 0;
     int64_t it = 0, nt = 0;
     int32_t nout = 0, iout = 0, csave = 0;
 
@@ -135,11 +145,11 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
             }
             dth = (float)dt;
             dtl = (float)(dt - (double)dth);
-            hstep = vfac<MULTI>(a, dt);
+            hstep = P::template fac<MULTI>(a, dt);
             nout = (int32_t)calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
             const double* u0 = a.u0 + 6 * i;
             cpos_init(a, p, u0);
-            v = cv_from(u0 + 3);
+            v = P::init(u0 + 3);
             iout = 0;
             if (a.save_start) {
                 a.t_out[i] = a.t0;  // save_start writes u0 exactly (slot 0)
@@ -147,8 +157,8 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
                     double* u = a.u_out + i;
                     for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
                     if (a.save_fields) {
-                        F3 E, B;
-                        eval_EB32t<FK>(a.f, p, a.t0, E, B);
+                        Fv E, B;
+                        P::fields(a.f, p, a.t0, E, B);
                         u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
                         u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
                     }
@@ -158,9 +168,9 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
                 t_last = a.t0;
                 iout = 1;
             }
-            F3 E, B;
-            eval_EB32t<FK>(a.f, p, a.t0, E, B);
-            v = vel32<MULTI>(v, E, B, a, -0.5 * dt);
+            Fv E, B;
+            P::fields(a.f, p, a.t0, E, B);
+            v = P::template step<MULTI>(v, E, B, a, -0.5 * dt);
             it = 1;
             t = a.t0 - 0.5 * dt;
             csave = 0;
@@ -172,20 +182,20 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
             // and the termination rollback (the reference returns v_prev,
             // boris.jl:460) both use it, so no copy of it is kept
             t += dt;
-            F3 E, B;
-            eval_EB32t<FK>(a.f, p, t, E, B);
-            CV vn = vel32h<MULTI>(v, E, B, a, hstep);
+            Fv E, B;
+            P::fields(a.f, p, t, E, B);
+            V vn = P::template step_h<MULTI>(v, E, B, a, hstep);
             CPos pn = p;
-            cpos_push_cv(a, pn, vn, dth, dtl);
-            if (a.term.flags && outside32(a, pn, vn, t + 0.5 * dt)) {
+            P::push(a, pn, vn, dth, dtl, dt);
+            if (a.term.flags && outside32<FK>(a, pn, vn, t + 0.5 * dt)) {
                 done = true;
             } else {
                 if (a.save_everystep && it > 1 && csave == 0) {
                     iout += 1;
                     if (iout <= nout) {
                         double t_cur = t - 0.5 * dt;
-                        if (!stat) eval_EB32t<FK>(a.f, p, t_cur, E, B);
-                        CV vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                        if (!stat) P::fields(a.f, p, t_cur, E, B);
+                        V vs = P::template step<MULTI>(v, E, B, a, 0.5 * dt);
                         S.save(i, iout - 1, p, vs, t_cur);
                         t_last = t_cur;
                     }
@@ -210,9 +220,9 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
                 double t_final = (final_step == nt) ? t1 : fma((double)final_step, dt, a.t0);
                 if (iout == 0 || t_last < t_final) {
                     double dt_final = t_final - fma((double)final_step - 0.5, dt, a.t0);
-                    F3 E, B;
-                    eval_EB32t<FK>(a.f, p, t_final, E, B);
-                    CV vf = vel32<MULTI>(v, E, B, a, dt_final);
+                    Fv E, B;
+                    P::fields(a.f, p, t_final, E, B);
+                    V vf = P::template step<MULTI>(v, E, B, a, dt_final);
                     S.save(i, iout, p, vf, t_final);
                     iout += 1;
                 }
@@ -228,6 +238,9 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
 __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
+    using P = Vel32<FK>;
+    using V = typename P::V;
+    using Fv = typename P::Fv;
     const Saver32<FK> S(a);
     const bool stat = fields_static32(a.f);
     const uint64_t t_start = globaltimer_ns();
@@ -236,8 +249,8 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
 
     int64_t i = -1;
     CPos p;
-    CV v{};
-    F3 E{0, 0, 0}, B{0, 0, 0};
+    V v{};
+    Fv E{0, 0, 0}, B{0, 0, 0};
     double t = 0, t1 = 0, dt = 0, C = 0, ttotal = 0, t_last = 0;
     int64_t it = 0, iout = 0, steps = 0;
     bool ssf = false;
@@ -253,11 +266,11 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
             C = (twopi * a.safety * sgn) / fabs(a.q2m);
             const double* u0 = a.u0 + 6 * i;
             cpos_init(a, p, u0);
-            v = cv_from(u0 + 3);
+            v = P::init(u0 + 3);
             t = a.t0;
             ttotal = dtt;
             iout = 0;
-            eval_EB32t<FK>(a.f, p, t, E, B);
+            P::fields(a.f, p, t, E, B);
             if (a.save_start) {
                 if (a.nslots > 0) {
                     a.t_out[i] = t;
@@ -273,8 +286,8 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
                 t_last = t;
                 iout = 1;
             }
-            dt = C / sqrt((double)dot(B, B));
-            v = vel32<MULTI>(v, E, B, a, -0.5 * dt);
+            dt = C / sqrt(P::bmag2(B));
+            v = P::template step<MULTI>(v, E, B, a, -0.5 * dt);
             it = 1;
             steps = 0;
             ssf = a.save_end;
@@ -287,27 +300,27 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
             done = true;
         }
         if (!done) {
-            if (!stat) eval_EB32t<FK>(a.f, p, t, E, B);
+            if (!stat) P::fields(a.f, p, t, E, B);
             if (fabs(t + dt - a.t0) > fabs(ttotal)) {
                 double dt_step = t1 - t;
-                v = vel32<MULTI>(v, E, B, a, 0.5 * dt);
-                v = vel32<MULTI>(v, E, B, a, -0.5 * dt_step);
+                v = P::template step<MULTI>(v, E, B, a, 0.5 * dt);
+                v = P::template step<MULTI>(v, E, B, a, -0.5 * dt_step);
                 dt = dt_step;
             }
             if (a.save_everystep && (it - 1) > 0 && (it - 1) % a.ssi == 0) {
-                CV vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                V vs = P::template step<MULTI>(v, E, B, a, 0.5 * dt);
                 S.save(i, iout, p, vs, t);
                 t_last = t;
                 iout += 1;
             }
-            F3 Em = E, Bm = B;
-            if (!stat) eval_EB32t<FK>(a.f, p, t + 0.5 * dt, Em, Bm);
-            CV v_new = vel32<MULTI>(v, Em, Bm, a, dt);
+            Fv Em = E, Bm = B;
+            if (!stat) P::fields(a.f, p, t + 0.5 * dt, Em, Bm);
+            V v_new = P::template step<MULTI>(v, Em, Bm, a, dt);
             CPos pn = p;
             float dh = (float)dt;
-            cpos_push_cv(a, pn, v_new, dh, (float)(dt - (double)dh));
+            P::push(a, pn, v_new, dh, (float)(dt - (double)dh), dt);
             double t_next = t + dt;
-            if (a.term.flags && outside32(a, pn, v_new, t_next)) {
+            if (a.term.flags && outside32<FK>(a, pn, v_new, t_next)) {
                 ssf = true;
                 ret = TP_RET_TERMINATED;
                 done = true;
@@ -316,10 +329,10 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
                 t = t_next;
                 v = v_new;
                 steps += 1;
-                eval_EB32t<FK>(a.f, p, t, E, B);
-                double dt_new = C / sqrt((double)dot(B, B));
-                v = vel32<MULTI>(v, E, B, a, 0.5 * dt);
-                v = vel32<MULTI>(v, E, B, a, -0.5 * dt_new);
+                P::fields(a.f, p, t, E, B);
+                double dt_new = C / sqrt(P::bmag2(B));
+                v = P::template step<MULTI>(v, E, B, a, 0.5 * dt);
+                v = P::template step<MULTI>(v, E, B, a, -0.5 * dt_new);
                 dt = dt_new;
                 it += 1;
                 if (a.save_everystep && (it - 1) % a.ssi == 0) ssf = true;
@@ -332,8 +345,8 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
         }
         if (done) {
             if (ssf && (iout == 0 || t_last != t)) {
-                if (!stat) eval_EB32t<FK>(a.f, p, t, E, B);
-                CV vf = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                if (!stat) P::fields(a.f, p, t, E, B);
+                V vf = P::template step<MULTI>(v, E, B, a, 0.5 * dt);
                 S.save(i, iout, p, vf, t);
                 iout += 1;
             }

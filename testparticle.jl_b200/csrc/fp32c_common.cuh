@@ -61,12 +61,14 @@ __device__ __forceinline__ void cpos_init(const BorisArgs& a, CPos& p, const dou
     }
 }
 
+// WRAP = false: the caller knows no axis wraps (analytic fields never do)
+template <bool WRAP = true>
 __device__ __forceinline__ void cpos_push(const BorisArgs& a, CPos& p, F3 v, float dt) {
     float d[3] = {v.x * dt, v.y * dt, v.z * dt};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         cadd(p.hi[c], p.lo[c], d[c]);
-        if (a.wrap[c]) {
+        if (WRAP && a.wrap[c]) {
             float x0 = (float)a.wrap0[c];
             float L = (float)a.wrapL[c];
             if (p.hi[c] >= x0 + L) {
@@ -499,6 +501,196 @@ __device__ __forceinline__ void cpos_push_cv(const BorisArgs& a, CPos& p, const 
          fmaf(v.h.z, dth, fmaf(v.h.z, dtl, v.l.z * dth))};
     cpos_push(a, p, d, 1.0f);
 }
+
+// ---------------------------------------------------------------- analytic fields: invariant-preserving update
+// With analytic fields (FK_ANALYTIC) the FP32C kernels keep the rotation
+// factors of the closed form in float, but the rotation axis, the velocity
+// and the field in float64.  The float delta form above leaves two random
+// walks that dominate the final-position error of long orbits in a dipole:
+//   |v|       the float rounding of each increment (~eps_f * angle per step)
+//             walks the energy, which shifts bounce and drift phases;
+//   pitch     the float field's direction error (~6e-8 rad per evaluation)
+//             tilts every rotation axis, which walks v . b and with it the
+//             magnetic moment and the mirror points.
+// Rotation factors rounded in float only misplace the gyrophase, but their
+// mutual consistency is what conserves |v| and v . t: one float64 step
+// restores (1 + c1)^2 + c2^2 |t|^2 = 1 (a common scale of 1 + c1 and c2) and
+// c1 + c3 |t|^2 = 0 (c3 alone), after which the update is orthogonal on
+// float64's scale.  The field costs about thirty float64 operations: 1/r from
+// a float rsqrt and one float64 Newton step (no sqrt, no division).
+
+// position of a compensated pair in float64 (analytic fields: no wrapping)
+__device__ __forceinline__ D3 cpos_d3(const CPos& p) {
+    return {(double)p.hi[0] + (double)p.lo[0], (double)p.hi[1] + (double)p.lo[1],
+            (double)p.hi[2] + (double)p.lo[2]};
+}
+
+// analytic field in float64 at a compensated position
+__device__ __forceinline__ D3 analytic_eval_mixed(const DevField& f, const CPos& p, double t) {
+    switch (f.kind) {
+        case TP_FIELD_UNIFORM:
+            return {f.v[0], f.v[1], f.v[2]};
+        case TP_FIELD_AFFINE: {
+            const D3 r = cpos_d3(p);
+            return {f.v[0] + f.J[0] * r.x + f.J[1] * r.y + f.J[2] * r.z + f.rate[0] * t,
+                    f.v[1] + f.J[3] * r.x + f.J[4] * r.y + f.J[5] * r.z + f.rate[1] * t,
+                    f.v[2] + f.J[6] * r.x + f.J[7] * r.y + f.J[8] * r.z + f.rate[2] * t};
+        }
+        case TP_FIELD_DIPOLE: {
+            // B = coef (3 (m.d) d / r^5 - m / r^3), 1/r = y (1.5 - r^2 y^2 / 2)
+            // from the float estimate y (relative error ~1e-13 after the step)
+            const D3 d = cpos_d3(p) - D3{f.c[0], f.c[1], f.c[2]};
+            const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+            double y = (double)rsqrtf((float)r2);
+            y = y * fma(-0.5 * r2, y * y, 1.5);
+            const double ir2 = y * y;
+            const double k3 = f.coef * (ir2 * y);
+            const double k5 = 3.0 * (k3 * ir2) * (f.m[0] * d.x + f.m[1] * d.y + f.m[2] * d.z);
+            return {k5 * d.x - k3 * f.m[0], k5 * d.y - k3 * f.m[1], k5 * d.z - k3 * f.m[2]};
+        }
+        default:
+            return {0.0, 0.0, 0.0};
+    }
+}
+
+// Multistep / Hyper Boris (multistep_boris.jl:65-142) -- and Boris itself,
+// which is its n = 1, N = 2 case (c1 + 1 = c2 = c3 = c6 = 2 / (1 + |t|^2)) --
+// with fac = q2m dt / (2n): float rotation factors from the float copy of
+// the axis, refined as above, applied in float64.
+__device__ __forceinline__ D3 rot_mixed(D3 v, D3 E, D3 B, double fac, int N, int n, bool hasE) {
+    D3 t = fac * B;
+    D3 e = hasE ? fac * E : D3{0.0, 0.0, 0.0};
+    double sd = dot(t, t);
+    float s = (float)sd;
+    if (N != 2) {
+        float f_N, e_corr;
+        if (N == 4) {
+            f_N = 1.0f + s * (1.0f / 3.0f);
+            e_corr = -1.0f / 3.0f;
+        } else {
+            f_N = 1.0f + s * (1.0f / 3.0f) + 2.0f * s * s * (1.0f / 15.0f);
+            e_corr = -1.0f / 3.0f - 2.0f * s * (1.0f / 15.0f);
+        }
+        const double fd = f_N;
+        if (hasE) e = fd * e + ((double)e_corr * dot(e, t)) * t;
+        t = fd * t;
+        sd = (fd * fd) * sd;
+        s = (float)sd;
+    }
+    float zr = 1.0f, q = 0.0f, A = 1.0f, R = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        R = R + (float)(k + 1) * A + 2.0f * q * q + zr * q;
+        float nzr = zr - s * q;
+        q = zr + q;
+        zr = nzr;
+        A = A * (1.0f + s);
+    }
+    // 1/A: the float estimate and one float64 Newton step
+    double invA = (double)__fdividef(1.0f, A);
+    invA = invA * fma(-(double)A, invA, 2.0);
+    double C2 = (2.0 * zr) * q * invA;
+    double C3 = (2.0 * q) * q * invA;
+    double C1 = -(double)s * C3;
+    // consistency in float64: scale (1 + C1, C2) onto the unit circle, then
+    // C3 from C1 + C3 |t|^2 = 0
+    const double hg = 0.5 * fma(C1, 2.0 + C1, C2 * C2 * sd);
+    C1 = C1 - hg * (1.0 + C1);
+    C2 = C2 - hg * C2;
+    const float rs = s > 0.0f ? __fdividef(1.0f, s) : 0.0f;
+    C3 = C3 - fma(C3, sd, C1) * (double)rs;
+    const D3 vxt = cross(v, t);
+    D3 dv = C1 * v + C2 * vxt + (C3 * dot(v, t)) * t;
+    if (hasE) {
+        const double c6 = (2.0 * R) * invA;
+        dv = dv + C2 * e + C3 * cross(e, t) + (c6 * dot(e, t)) * t;
+    }
+    return v + dv;
+}
+
+// velocity update of length dt, fields (E, B) in float64
+template <bool MULTI>
+__device__ __forceinline__ D3 vel_mixed(D3 v, D3 E, D3 B, const BorisArgs& a, double dt) {
+    const bool hasE = a.f.E.kind != TP_FIELD_ZERO;
+    if (MULTI) return rot_mixed(v, E, B, a.q2m * dt / (double)(2 * a.nsub), a.order, a.nsub, hasE);
+    return rot_mixed(v, E, B, a.q2m * 0.5 * dt, 2, 1, hasE);
+}
+
+// position push x += v dt from a float64 velocity
+__device__ __forceinline__ void cpos_push_d(const BorisArgs& a, CPos& p, const D3& v, double dt) {
+    const F3 d{(float)(v.x * dt), (float)(v.y * dt), (float)(v.z * dt)};
+    cpos_push<false>(a, p, d, 1.0f);
+}
+
+// ---------------------------------------------------------------- velocity representation per field kind
+// Grids: compensated float velocity, float fields, delta form.  Analytic
+// fields: float64 velocity and fields, invariant-preserving update.
+template <int FK>
+struct Vel32 {
+    using V = CV;
+    using Fv = F3;
+    static __device__ __forceinline__ V init(const double* u) { return cv_from(u); }
+    static __device__ __forceinline__ double comp(const V& v, int c) {
+        return c == 0 ? (double)v.h.x + (double)v.l.x : (c == 1 ? (double)v.h.y + (double)v.l.y
+                                                                 : (double)v.h.z + (double)v.l.z);
+    }
+    static __device__ __forceinline__ bool has_nan(const V& v) {
+        return isnan(v.h.x) || isnan(v.h.y) || isnan(v.h.z);
+    }
+    static __device__ __forceinline__ void fields(const DevFields& F, const CPos& p, double t, Fv& E, Fv& B) {
+        eval_EB32t<FK>(F, p, t, E, B);
+    }
+    using H = float;  // factor of one velocity update
+    template <bool MULTI>
+    static __device__ __forceinline__ H fac(const BorisArgs& a, double dt) {
+        return vfac<MULTI>(a, dt);
+    }
+    template <bool MULTI>
+    static __device__ __forceinline__ V step_h(const V& v, const Fv& E, const Fv& B, const BorisArgs& a, H h) {
+        return vel32h<MULTI>(v, E, B, a, h);
+    }
+    template <bool MULTI>
+    static __device__ __forceinline__ V step(const V& v, const Fv& E, const Fv& B, const BorisArgs& a, double dt) {
+        return vel32<MULTI>(v, E, B, a, dt);
+    }
+    static __device__ __forceinline__ void push(const BorisArgs& a, CPos& p, const V& v, float dth, float dtl,
+                                                double) {
+        cpos_push_cv(a, p, v, dth, dtl);
+    }
+    static __device__ __forceinline__ double bmag2(const Fv& B) { return (double)dot(B, B); }
+    static __device__ __forceinline__ double fcomp(const Fv& f, int c) { return c == 0 ? f.x : (c == 1 ? f.y : f.z); }
+};
+
+template <>
+struct Vel32<FK_ANALYTIC> {
+    using V = D3;
+    using Fv = D3;
+    static __device__ __forceinline__ V init(const double* u) { return {u[0], u[1], u[2]}; }
+    static __device__ __forceinline__ double comp(const V& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+    static __device__ __forceinline__ bool has_nan(const V& v) { return isnan(v.x) || isnan(v.y) || isnan(v.z); }
+    static __device__ __forceinline__ void fields(const DevFields& F, const CPos& p, double t, Fv& E, Fv& B) {
+        E = analytic_eval_mixed(F.E, p, t);
+        B = analytic_eval_mixed(F.B, p, t);
+    }
+    using H = double;
+    template <bool MULTI>
+    static __device__ __forceinline__ H fac(const BorisArgs& a, double dt) {
+        return MULTI ? a.q2m * dt / (double)(2 * a.nsub) : a.q2m * 0.5 * dt;
+    }
+    template <bool MULTI>
+    static __device__ __forceinline__ V step_h(const V& v, const Fv& E, const Fv& B, const BorisArgs& a, H h) {
+        const bool hasE = a.f.E.kind != TP_FIELD_ZERO;
+        return MULTI ? rot_mixed(v, E, B, h, a.order, a.nsub, hasE) : rot_mixed(v, E, B, h, 2, 1, hasE);
+    }
+    template <bool MULTI>
+    static __device__ __forceinline__ V step(const V& v, const Fv& E, const Fv& B, const BorisArgs& a, double dt) {
+        return vel_mixed<MULTI>(v, E, B, a, dt);
+    }
+    static __device__ __forceinline__ void push(const BorisArgs& a, CPos& p, const V& v, float, float, double dt) {
+        cpos_push_d(a, p, v, dt);
+    }
+    static __device__ __forceinline__ double bmag2(const Fv& B) { return dot(B, B); }
+    static __device__ __forceinline__ double fcomp(const Fv& f, int c) { return c == 0 ? f.x : (c == 1 ? f.y : f.z); }
+};
 
 }  // namespace
 

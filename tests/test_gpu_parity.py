@@ -371,7 +371,7 @@ def test_grid_fp32c_error_stated(tp, orc):
 
 
 # ------------------------------------------------------------------ FP32C in analytic fields
-def test_fp32c_uniform_and_dipole(tp, orc):
+def test_fp32c_uniform(tp, orc):
     w = tp.workloads.config1(1000)
     prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
     sols = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c"), dt=w.dt,
@@ -383,21 +383,59 @@ def test_fp32c_uniform_and_dipole(tp, orc):
     d = np.abs(sols.u_all[:, :3] - ref.u[:, :3]).max()
     assert d <= 1e-5 * np.abs(ref.u[:, :3]).max()
 
-    w = tp.workloads.config3(1024, nt=10_000, ssi=1000)
-    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
-    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside)
-    sols = tp.solve(prob, tp.MultistepBoris(4, 2), tp.EnsembleB200(precision="fp32c"), **kw)
-    plan = tp.plan_boris(prob, tp.MultistepBoris(4, 2), **kw)
-    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
-    both = (sols.retcodes == 1) & (ref.retcode == 1)
-    assert both.mean() > 0.9
-    fs, fr = sols.final_states()[both], ref.final_states()[both]
-    err = np.linalg.norm(fs[:, :3] - fr[:, :3], axis=1) / np.linalg.norm(fr[:, :3], axis=1)
-    # <= 1e-5 relative position error after 1e4 steps
-    assert np.median(err) <= 1e-5
-    # the tail is the non-adiabatic (10 MeV, large-L) orbits, where float64
-    # runs started a float32 ulp apart separate just as far; bench.py states it
-    assert np.quantile(err, 0.9) <= 1e-4
+
+def _saves_by_particle(sols, nslots):
+    """(n, nslots, 3) saved positions of particles that made every save, and that mask."""
+    full = sols.nsaved == nslots
+    off = np.concatenate([[0], np.cumsum(sols.nsaved.astype(np.int64))])
+    rows = off[:-1][full][:, None] + np.arange(nslots)[None, :]
+    return sols.u_all[rows, :3], full
+
+
+def test_fp32c_dipole_multistep_error_bar(tp):
+    """The FP32C bar on the dipole ensemble: MultistepBoris4(2), 1e4 steps, a
+    fixed 4096-particle sample of the 1e6-proton workload (every 4th particle).
+    The float64 runs started a float32 ulp away (components rounded to
+    float32; all scaled by 1 + 2^-23) measure each orbit's own sensitivity:
+      p90 of the final-position error over all orbits <= 1e-5;
+      every regular orbit (both float32-ulp starts within 1e-6 / 1e-5 of the
+      float64 orbit at every save) <= 1e-5."""
+    w = tp.workloads.config3()
+    idx = np.arange(0, 4 * 4096, 4)
+    u0, dt, tend = w.u0[:, idx].copy(), w.dt[idx].copy(), w.tend[idx].copy()
+    param = tp.prepare(w.E, w.B, species=tp.Proton)
+    kw = dict(dt=dt, tend=tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+    nslots = w.nt // w.savestepinterval + 1
+
+    def run(u, prec):
+        return tp.solve(tp.TraceProblem(u, w.tspan, param), tp.MultistepBoris4(2), tp.EnsembleB200(precision=prec),
+                        **kw)
+
+    x32, f32 = _saves_by_particle(run(u0, "fp32c"), nslots)
+    s64 = run(u0, "fp64")
+    x64, f64 = _saves_by_particle(s64, nslots)
+    xr, fr = _saves_by_particle(run(u0.astype(np.float32).astype(np.float64), "fp64"), nslots)
+    xs, fs = _saves_by_particle(run(u0 * (1.0 + 2.0 ** -23), "fp64"), nslots)
+    both = f32 & f64 & fr & fs
+    assert both.mean() > 0.95
+
+    def sel(x, f):  # rows of the particles in `both`
+        pos = np.cumsum(f) - 1
+        return x[pos[both]]
+
+    a64 = sel(x64, f64)
+
+    def err(x, f):
+        return np.linalg.norm(sel(x, f) - a64, axis=2) / np.linalg.norm(a64, axis=2)
+
+    e32 = err(x32, f32)[:, -1]
+    sr, ss = err(xr, fr).max(axis=1), err(xs, fs).max(axis=1)
+    regular = (sr < 1e-6) & (ss < 1e-5)
+    print(f"FP32C error: p50 {np.median(e32):.2e} p90 {np.quantile(e32, 0.9):.2e}; regular orbits "
+          f"{regular.mean():.2f}, max {e32[regular].max():.2e}")
+    assert np.quantile(e32, 0.9) <= 1e-5
+    assert regular.mean() > 0.4
+    assert e32[regular].max() <= 1e-5
 
 
 # ------------------------------------------------------------------ guiding centre
