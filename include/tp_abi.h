@@ -228,7 +228,9 @@ typedef struct tp_run_desc {
     double budget_s;         /* device wall-clock budget, 0 = default 600 s */
     int32_t save_work;       /* append (P_par, P_fermi, P_grad, P_betatron)
                                 to every save (boris.jl:405-440)            */
-    int32_t reserved3;
+    int32_t particles_per_thread; /* fixed step, analytic fields: 1 or 2
+                                particles advanced in lock step by each
+                                thread; 0 = tuned / default (1)             */
 } tp_run_desc;
 
 /* ---- guiding-centre run ------------------------------------------------- */
@@ -427,18 +429,20 @@ int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* desc,
  * tp_autotune times every candidate launch shape -- block sizes 64..256 (384
  * for interleaved E/B grids) with the static and the persistent-queue
  * schedule (only the queue where lifetimes can be uneven: adaptive steps or
- * a termination predicate) -- on a sample of the run (the first
+ * a termination predicate), and for fixed steps in analytic fields one or
+ * two particles per thread -- on a sample of the run (the first
  * min(n, 131072) particles of u0, host memory, for at most max_steps
  * steps), keeps the fastest in the
  * context for runs of the same kernel variant whose descriptor leaves block
- * = 0 / schedule = TP_SCHED_AUTO, and reports it.                          */
+ * = 0 / schedule = TP_SCHED_AUTO / particles_per_thread = 0, and reports
+ * it.                                                                      */
 typedef struct tp_tune_result {
     int32_t block;
     int32_t schedule;      /* TP_SCHED_STATIC or TP_SCHED_QUEUE */
     double ms;             /* device time of the chosen shape on the sample */
     double ms_default;     /* the same sample with the untuned default shape */
     int32_t candidates;
-    int32_t reserved;
+    int32_t particles_per_thread;  /* the chosen particles per thread      */
 } tp_tune_result;
 int tp_autotune(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
                 const tp_field* B, const double* u0, int64_t n,

@@ -154,7 +154,7 @@ class RunDesc(C.Structure):
         ("block", C.c_int32),
         ("budget_s", C.c_double),
         ("save_work", C.c_int32),
-        ("reserved3", C.c_int32),
+        ("particles_per_thread", C.c_int32),
     ]
 
 
@@ -194,7 +194,7 @@ class TuneResult(C.Structure):
         ("ms", C.c_double),
         ("ms_default", C.c_double),
         ("candidates", C.c_int32),
-        ("reserved", C.c_int32),
+        ("particles_per_thread", C.c_int32),
     ]
 
 

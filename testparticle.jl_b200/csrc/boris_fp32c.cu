@@ -235,6 +235,184 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
     }
 }
 
+// ---------------------------------------------------------------- fixed step, several particles per thread
+// PPT particles per thread ("slots"), advanced in lock step: each loop
+// iteration first refills idle slots, then computes every slot's step (field,
+// velocity update, push) as one straight-line block -- independent work the
+// scheduler can interleave -- and then commits each slot (termination, saves,
+// end of trajectory).  A slot without a particle computes on its stale state
+// and commits nothing.  Static schedule: slot k of global thread g owns
+// particle g + k * (threads in the grid).
+template <bool MULTI, bool QUEUE, int FK, int PPT>
+__global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed32c_slots(BorisArgs a) {
+    using P = Vel32<FK>;
+    using V = typename P::V;
+    using Fv = typename P::Fv;
+    const Saver32<FK> S(a);
+    const uint64_t t_start = globaltimer_ns();
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+
+    int64_t first[PPT], i[PPT];
+    CPos p[PPT];
+    V v[PPT];
+    double dt[PPT], t[PPT], t1[PPT], t_last[PPT];
+    float dth[PPT], dtl[PPT];
+    typename P::H hstep[PPT];
+    int64_t it[PPT], nt[PPT];
+    int32_t nout[PPT], iout[PPT], csave[PPT];
+    bool dead[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        first[k] = g + k * gstride;
+        i[k] = -1;
+        dead[k] = false;
+        v[k] = V{};
+        dt[k] = t[k] = t1[k] = t_last[k] = 0.0;
+        dth[k] = dtl[k] = 0.0f;
+        hstep[k] = 0;
+        it[k] = nt[k] = 0;
+        nout[k] = iout[k] = csave[k] = 0;
+        for (int c = 0; c < 3; ++c) {
+            p[k].hi[c] = p[k].lo[c] = 0.0f;
+            p[k].w[c] = 0;
+        }
+    }
+
+    for (;;) {
+        // ---- refill idle slots (_boris_single set-up, boris.jl:480-514)
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            while (!dead[k] && i[k] < 0) {
+                i[k] = next_particle32<QUEUE>(a, first[k]);
+                if (i[k] >= a.n) {
+                    dead[k] = true;
+                    break;
+                }
+                const int64_t ii = i[k];
+                dt[k] = a.dt_i ? a.dt_i[ii] : a.dt;
+                t1[k] = a.tend_i ? a.tend_i[ii] : a.t1;
+                nt[k] = (fabs(dt[k]) < 10.0 * 2.220446049250313e-16) ? -1 : jl_round((t1[k] - a.t0) / dt[k]);
+                if (nt[k] < 0 && fabs(dt[k]) >= 10.0 * 2.220446049250313e-16) nt[k] = -nt[k];
+                if (nt[k] < 0 || nt[k] > a.maxiters) {
+                    set_status(a.status, TP_E_ARG);
+                    a.nsaved[ii] = 0;
+                    a.retcode[ii] = TP_RET_DEFAULT;
+                    a.nsteps[ii] = 0;
+                    i[k] = -1;
+                    continue;
+                }
+                dth[k] = (float)dt[k];
+                dtl[k] = (float)(dt[k] - (double)dth[k]);
+                hstep[k] = P::template fac<MULTI>(a, dt[k]);
+                nout[k] = (int32_t)calc_nout(nt[k], a.ssi, a.save_start, a.save_end, a.save_everystep);
+                const double* u0 = a.u0 + 6 * ii;
+                cpos_init(a, p[k], u0);
+                v[k] = P::init(u0 + 3);
+                iout[k] = 0;
+                if (a.save_start) {
+                    a.t_out[ii] = a.t0;  // save_start writes u0 exactly (slot 0)
+                    if (a.nslots > 0) {
+                        double* u = a.u_out + ii;
+                        for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
+                        if (a.save_fields) {
+                            Fv E, B;
+                            P::fields(a.f, p[k], a.t0, E, B);
+                            u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                            u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                        }
+                    } else {
+                        set_status(a.status, TP_E_OVERFLOW);
+                    }
+                    t_last[k] = a.t0;
+                    iout[k] = 1;
+                }
+                Fv E, B;
+                P::fields(a.f, p[k], a.t0, E, B);
+                v[k] = P::template step<MULTI>(v[k], E, B, a, -0.5 * dt[k]);
+                it[k] = 1;
+                t[k] = a.t0 - 0.5 * dt[k];
+                csave[k] = 0;
+            }
+        }
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) any = any || !dead[k];
+        if (!any) break;
+
+        // ---- one step of every slot: field, velocity update, push.  v stays
+        // v_{it-1/2} until the step is accepted: the save of r_{it-1} and the
+        // termination rollback (the reference returns v_prev, boris.jl:460)
+        // both use it
+        V vn[PPT];
+        CPos pn[PPT];
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            Fv E, B;
+            P::fields(a.f, p[k], t[k] + dt[k], E, B);
+            vn[k] = P::template step_h<MULTI>(v[k], E, B, a, hstep[k]);
+            pn[k] = p[k];
+            P::push(a, pn[k], vn[k], dth[k], dtl[k], dt[k]);
+        }
+
+        // ---- commit (_boris_loop!, boris.jl:452-476), end of trajectory (:522-551)
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            if (dead[k]) continue;
+            const int64_t ii = i[k];
+            bool done = it[k] > nt[k];
+            if (!done) {
+                t[k] += dt[k];
+                if (a.term.flags && outside32<FK>(a, pn[k], vn[k], t[k] + 0.5 * dt[k])) {
+                    done = true;
+                } else {
+                    if (a.save_everystep && it[k] > 1 && csave[k] == 0) {
+                        iout[k] += 1;
+                        if (iout[k] <= nout[k]) {
+                            const double t_cur = t[k] - 0.5 * dt[k];
+                            Fv E, B;
+                            P::fields(a.f, p[k], t_cur, E, B);
+                            V vs = P::template step<MULTI>(v[k], E, B, a, 0.5 * dt[k]);
+                            S.save(ii, iout[k] - 1, p[k], vs, t_cur);
+                            t_last[k] = t_cur;
+                        }
+                    }
+                    p[k] = pn[k];
+                    v[k] = vn[k];
+                    it[k] += 1;
+                    csave[k] += 1;
+                    if (csave[k] == a.ssi) csave[k] = 0;
+                    done = it[k] > nt[k];
+                    if ((it[k] & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                        set_status(a.status, TP_E_TIMEOUT);
+                        done = true;
+                    }
+                }
+            }
+            if (done) {
+                const int64_t final_step = it[k] - 1;
+                const bool save_final = a.save_end ||
+                                        (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
+                if (iout[k] < nout[k] && save_final) {
+                    const double t_final = (final_step == nt[k]) ? t1[k] : fma((double)final_step, dt[k], a.t0);
+                    if (iout[k] == 0 || t_last[k] < t_final) {
+                        const double dt_final = t_final - fma((double)final_step - 0.5, dt[k], a.t0);
+                        Fv E, B;
+                        P::fields(a.f, p[k], t_final, E, B);
+                        V vf = P::template step<MULTI>(v[k], E, B, a, dt_final);
+                        S.save(ii, iout[k], p[k], vf, t_final);
+                        iout[k] += 1;
+                    }
+                }
+                a.nsaved[ii] = (int32_t)iout[k];
+                a.retcode[ii] = (int8_t)((iout[k] < nout[k]) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
+                a.nsteps[ii] = final_step;
+                i[k] = -1;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
 __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
@@ -359,25 +537,31 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
 }
 
 // ---------------------------------------------------------------- launchers
+// Two particles per thread are compiled for the analytic-field fixed-step
+// kernels (no field memory: a slot without a particle computes without
+// touching memory); everything else runs one particle per thread.
 template <bool MULTI, bool QUEUE, int FK>
-static const void* kernel_ptr32(bool adaptive) {
-    return adaptive ? (const void*)k_adaptive32c<MULTI, QUEUE, FK> : (const void*)k_fixed32c<MULTI, QUEUE, FK>;
+static const void* kernel_ptr32(bool adaptive, int ppt) {
+    if (adaptive) return (const void*)k_adaptive32c<MULTI, QUEUE, FK>;
+    if (FK == FK_ANALYTIC && ppt == 2) return (const void*)k_fixed32c_slots<MULTI, QUEUE, FK, 2>;
+    return (const void*)k_fixed32c<MULTI, QUEUE, FK>;
 }
 
 template <bool MULTI, bool QUEUE>
-static const void* pick_fk32(bool adaptive, int fk) {
-    if (fk == FK_ANALYTIC) return kernel_ptr32<MULTI, QUEUE, FK_ANALYTIC>(adaptive);
-    if (fk == FK_EBGRID) return kernel_ptr32<MULTI, QUEUE, FK_EBGRID>(adaptive);
-    if (fk == FK_GENGRID) return kernel_ptr32<MULTI, QUEUE, FK_GENGRID>(adaptive);
-    return kernel_ptr32<MULTI, QUEUE, FK_GENERIC>(adaptive);
+static const void* pick_fk32(bool adaptive, int fk, int ppt) {
+    if (fk == FK_ANALYTIC) return kernel_ptr32<MULTI, QUEUE, FK_ANALYTIC>(adaptive, ppt);
+    if (fk == FK_EBGRID) return kernel_ptr32<MULTI, QUEUE, FK_EBGRID>(adaptive, 1);
+    if (fk == FK_GENGRID) return kernel_ptr32<MULTI, QUEUE, FK_GENGRID>(adaptive, 1);
+    return kernel_ptr32<MULTI, QUEUE, FK_GENERIC>(adaptive, 1);
 }
 
 static const void* select_kernel32(const BorisArgs& a, bool queue) {
     const bool multi = a.alg == TP_ALG_MULTISTEP || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
     const bool adaptive = a.alg == TP_ALG_ADAPTIVE || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
-    int fk = field_config_of(a.f);
-    if (multi) return queue ? pick_fk32<true, true>(adaptive, fk) : pick_fk32<true, false>(adaptive, fk);
-    return queue ? pick_fk32<false, true>(adaptive, fk) : pick_fk32<false, false>(adaptive, fk);
+    const int fk = field_config_of(a.f);
+    const int ppt = a.ppt;
+    if (multi) return queue ? pick_fk32<true, true>(adaptive, fk, ppt) : pick_fk32<true, false>(adaptive, fk, ppt);
+    return queue ? pick_fk32<false, true>(adaptive, fk, ppt) : pick_fk32<false, false>(adaptive, fk, ppt);
 }
 
 cudaError_t launch_boris_fp32c(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s) {

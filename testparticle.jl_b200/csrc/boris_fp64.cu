@@ -14,7 +14,7 @@
 //
 // Kernels (MULTI: Multistep update; QUEUE: schedule; FK: field configuration,
 // see tp_device.cuh):
-//   k_fixed64<MULTI, QUEUE, FK>    _boris_single + _boris_loop!  (boris.jl:445-557)
+//   k_fixed64<MULTI, QUEUE, FK, PPT>  _boris_single + _boris_loop!  (boris.jl:445-557)
 //                                  with Boris (boris.jl:19-45) or
 //                                  Multistep (multistep_boris.jl:65-142) updates
 //   k_adaptive64<MULTI, QUEUE, FK> _adaptive_boris_single (adaptive_boris.jl:145-266)
@@ -191,6 +191,163 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
     }
 }
 
+// ---------------------------------------------------------------- fixed step, several particles per thread
+// PPT particles per thread ("slots") in lock step, as in boris_fp32c.cu: each
+// iteration refills idle slots, computes every slot's step as one
+// straight-line block (independent float64 chains the scheduler can
+// interleave), then commits each slot.  The arithmetic of a slot is that of
+// one particle per thread, so the results do not depend on PPT.  Static
+// schedule: slot k of global thread g owns particle g + k * (threads in the grid).
+template <bool MULTI, bool QUEUE, int FK, int PPT>
+__global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed64_slots(BorisArgs a) {
+    const Saver64<FK> S(a);
+    const uint64_t t_start = globaltimer_ns();
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+
+    // per-slot particle state
+    int64_t first[PPT], i[PPT];
+    D3 r[PPT], v[PPT];
+    double dt[PPT], t[PPT], t1[PPT], t_last[PPT];
+    int64_t it[PPT], nt[PPT];
+    int32_t nout[PPT], iout[PPT], csave[PPT];
+    bool dead[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        first[k] = g + k * gstride;
+        i[k] = -1;
+        dead[k] = false;
+        r[k] = v[k] = D3{0.0, 0.0, 0.0};
+        dt[k] = t[k] = t1[k] = t_last[k] = 0.0;
+        it[k] = nt[k] = 0;
+        nout[k] = iout[k] = csave[k] = 0;
+    }
+
+    for (;;) {
+        // ---- refill idle slots: _boris_single (boris.jl:480-514)
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            while (!dead[k] && i[k] < 0) {
+                i[k] = next_particle<QUEUE>(a, first[k]);
+                if (i[k] >= a.n) {
+                    dead[k] = true;
+                    break;
+                }
+                const int64_t ii = i[k];
+                dt[k] = a.dt_i ? a.dt_i[ii] : a.dt;
+                t1[k] = a.tend_i ? a.tend_i[ii] : a.t1;
+                if (fabs(dt[k]) < 10.0 * 2.220446049250313e-16) {
+                    set_status(a.status, TP_E_ARG);
+                    a.nsaved[ii] = 0;
+                    a.retcode[ii] = TP_RET_DEFAULT;
+                    a.nsteps[ii] = 0;
+                    i[k] = -1;
+                    continue;
+                }
+                nt[k] = jl_round((t1[k] - a.t0) / dt[k]);
+                if (nt[k] < 0) nt[k] = -nt[k];
+                if (nt[k] > a.maxiters) {
+                    set_status(a.status, TP_E_ARG);
+                    a.nsaved[ii] = 0;
+                    a.retcode[ii] = TP_RET_DEFAULT;
+                    a.nsteps[ii] = 0;
+                    i[k] = -1;
+                    continue;
+                }
+                nout[k] = (int32_t)calc_nout(nt[k], a.ssi, a.save_start, a.save_end, a.save_everystep);
+                const double* u0 = a.u0 + 6 * ii;
+                r[k] = {u0[0], u0[1], u0[2]};
+                v[k] = {u0[3], u0[4], u0[5]};
+                iout[k] = 0;
+                if (a.save_start) {
+                    S.save(ii, 0, r[k], v[k], a.t0);
+                    t_last[k] = a.t0;
+                    iout[k] = 1;
+                }
+                D3 E, B;
+                eval_EB64t<FK>(a.f, r[k], a.t0, E, B);
+                v[k] = vel_update64<MULTI>(v[k], E, B, a.q2m, -0.5 * dt[k], a.order, a.nsub);
+                it[k] = 1;
+                t[k] = a.t0 - 0.5 * dt[k];
+                csave[k] = 0;  // (it - 1) % ssi
+            }
+        }
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) any = any || !dead[k];
+        if (!any) break;
+
+        // ---- one step of _boris_loop! (boris.jl:452-476) for every slot; v
+        // stays the pre-step velocity (the reference's v_prev) until the step
+        // is accepted, which serves both the save and the termination rollback
+        D3 vn[PPT], r_next[PPT];
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            D3 E, B;
+            eval_EB64t<FK>(a.f, r[k], t[k] + dt[k], E, B);
+            vn[k] = vel_update64<MULTI>(v[k], E, B, a.q2m, dt[k], a.order, a.nsub);
+            r_next[k] = r[k] + vn[k] * dt[k];
+        }
+
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            if (dead[k]) continue;
+            const int64_t ii = i[k];
+            bool done = it[k] > nt[k];
+            if (!done) {
+                t[k] += dt[k];
+                const double t_next = t[k] + 0.5 * dt[k];
+                if (a.term.flags && outside64(a.term, r_next[k], vn[k], t_next)) {
+                    done = true;
+                } else {
+                    if (a.save_everystep && it[k] > 1 && csave[k] == 0) {
+                        iout[k] += 1;
+                        if (iout[k] <= nout[k]) {
+                            const double t_cur = t[k] - 0.5 * dt[k];
+                            D3 E, B;
+                            eval_EB64t<FK>(a.f, r[k], t_cur, E, B);
+                            D3 v_save = vel_update64<MULTI>(v[k], E, B, a.q2m, 0.5 * dt[k], a.order, a.nsub);
+                            S.save(ii, iout[k] - 1, r[k], v_save, t_cur);
+                            t_last[k] = t_cur;
+                        }
+                    }
+                    r[k] = r_next[k];
+                    v[k] = vn[k];
+                    it[k] += 1;
+                    csave[k] += 1;
+                    if (csave[k] == a.ssi) csave[k] = 0;
+                    done = it[k] > nt[k];
+                    if ((it[k] & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                        set_status(a.status, TP_E_TIMEOUT);
+                        done = true;
+                    }
+                }
+            }
+            if (done) {
+                // ---- final save and retcode (boris.jl:522-551)
+                const int64_t final_step = it[k] - 1;
+                const bool save_final = a.save_end ||
+                                        (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
+                if (iout[k] < nout[k] && save_final) {
+                    const double t_final = (final_step == nt[k]) ? t1[k] : fma((double)final_step, dt[k], a.t0);
+                    if (iout[k] == 0 || t_last[k] < t_final) {
+                        const double dt_final = t_final - fma((double)final_step - 0.5, dt[k], a.t0);
+                        D3 E, B;
+                        eval_EB64t<FK>(a.f, r[k], t_final, E, B);
+                        D3 vf = vel_update64<MULTI>(v[k], E, B, a.q2m, dt_final, a.order, a.nsub);
+                        S.save(ii, iout[k], r[k], vf, t_final);
+                        iout[k] += 1;
+                    }
+                }
+                a.nsaved[ii] = (int32_t)iout[k];
+                a.retcode[ii] = (int8_t)((iout[k] < nout[k]) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
+                a.nsteps[ii] = final_step;
+                i[k] = -1;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
 __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive64(BorisArgs a) {
@@ -303,25 +460,30 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive64(BorisArgs a) {
 }
 
 // ---------------------------------------------------------------- launchers
+// Two particles per thread are compiled for the analytic-field fixed-step
+// kernels only (see boris_fp32c.cu).
 template <bool MULTI, bool QUEUE, int FK>
-static const void* kernel_ptr64(bool adaptive) {
-    return adaptive ? (const void*)k_adaptive64<MULTI, QUEUE, FK> : (const void*)k_fixed64<MULTI, QUEUE, FK>;
+static const void* kernel_ptr64(bool adaptive, int ppt) {
+    if (adaptive) return (const void*)k_adaptive64<MULTI, QUEUE, FK>;
+    if (FK == FK_ANALYTIC && ppt == 2) return (const void*)k_fixed64_slots<MULTI, QUEUE, FK, 2>;
+    return (const void*)k_fixed64<MULTI, QUEUE, FK>;
 }
 
 template <bool MULTI, bool QUEUE>
-static const void* pick_fk64(bool adaptive, int fk) {
-    if (fk == FK_ANALYTIC) return kernel_ptr64<MULTI, QUEUE, FK_ANALYTIC>(adaptive);
-    if (fk == FK_EBGRID) return kernel_ptr64<MULTI, QUEUE, FK_EBGRID>(adaptive);
-    if (fk == FK_GENGRID) return kernel_ptr64<MULTI, QUEUE, FK_GENGRID>(adaptive);
-    return kernel_ptr64<MULTI, QUEUE, FK_GENERIC>(adaptive);
+static const void* pick_fk64(bool adaptive, int fk, int ppt) {
+    if (fk == FK_ANALYTIC) return kernel_ptr64<MULTI, QUEUE, FK_ANALYTIC>(adaptive, ppt);
+    if (fk == FK_EBGRID) return kernel_ptr64<MULTI, QUEUE, FK_EBGRID>(adaptive, 1);
+    if (fk == FK_GENGRID) return kernel_ptr64<MULTI, QUEUE, FK_GENGRID>(adaptive, 1);
+    return kernel_ptr64<MULTI, QUEUE, FK_GENERIC>(adaptive, 1);
 }
 
 static const void* select_kernel64(const BorisArgs& a, bool queue) {
     const bool multi = a.alg == TP_ALG_MULTISTEP || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
     const bool adaptive = a.alg == TP_ALG_ADAPTIVE || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
-    int fk = field_config_of(a.f);
-    if (multi) return queue ? pick_fk64<true, true>(adaptive, fk) : pick_fk64<true, false>(adaptive, fk);
-    return queue ? pick_fk64<false, true>(adaptive, fk) : pick_fk64<false, false>(adaptive, fk);
+    const int fk = field_config_of(a.f);
+    const int ppt = a.ppt;
+    if (multi) return queue ? pick_fk64<true, true>(adaptive, fk, ppt) : pick_fk64<true, false>(adaptive, fk, ppt);
+    return queue ? pick_fk64<false, true>(adaptive, fk, ppt) : pick_fk64<false, false>(adaptive, fk, ppt);
 }
 
 cudaError_t launch_boris_fp64(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s) {

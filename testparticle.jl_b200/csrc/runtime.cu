@@ -34,7 +34,10 @@ struct tp_ctx {
     std::string err;
     // launch shapes chosen by tp_autotune, keyed by the kernel variant
     // (algorithm, precision, field configuration, termination): block, schedule
-    std::map<std::string, std::pair<int, int>> tuned;
+    struct Shape {
+        int block, sched, ppt;
+    };
+    std::map<std::string, Shape> tuned;
     // pinned staging for host <-> device transfers of pageable buffers
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
@@ -805,20 +808,24 @@ std::string tune_key(const tp_run_desc* d, const BorisArgs& a) {
            std::to_string(field_config_of(a.f)) + ":" + std::to_string(d->term.flags != 0);
 }
 
-// Effective block size and schedule of a run: the descriptor's, else the
-// tuned ones, else 128 threads and the queue whenever lifetimes can be
-// uneven (adaptive steps or a termination predicate).
-void resolve_launch(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a, int& block, bool& queue) {
+// Effective block size, schedule and particles per thread of a run: the
+// descriptor's, else the tuned ones, else 128 threads, one particle per
+// thread and the queue whenever lifetimes can be uneven (adaptive steps or a
+// termination predicate).
+void resolve_launch(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a, int& block, bool& queue, int& ppt) {
     block = d->block;
     int sched = d->schedule;
-    if (block == 0 || sched == TP_SCHED_AUTO) {
+    ppt = d->particles_per_thread;
+    if (block == 0 || sched == TP_SCHED_AUTO || ppt == 0) {
         auto it = ctx->tuned.find(tune_key(d, a));
         if (it != ctx->tuned.end()) {
-            if (block == 0) block = it->second.first;
-            if (sched == TP_SCHED_AUTO) sched = it->second.second;
+            if (block == 0) block = it->second.block;
+            if (sched == TP_SCHED_AUTO) sched = it->second.sched;
+            if (ppt == 0) ppt = it->second.ppt;
         }
     }
     if (block == 0) block = 128;
+    if (ppt == 0) ppt = 1;
     if (sched == TP_SCHED_AUTO)
         sched = (d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP || d->term.flags != 0)
                     ? TP_SCHED_QUEUE
@@ -827,26 +834,34 @@ void resolve_launch(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a, int& 
 }
 
 bool use_queue(tp_ctx* ctx, const tp_run_desc* d, const BorisArgs& a) {
-    int block;
+    int block, ppt;
     bool q;
-    resolve_launch(ctx, d, a, block, q);
+    resolve_launch(ctx, d, a, block, q, ppt);
     return q;
+}
+
+// two particles per thread exist for the fixed-step analytic-field kernels
+bool ppt2_available(const tp_run_desc* d, const BorisArgs& a) {
+    return (d->alg == TP_ALG_BORIS || d->alg == TP_ALG_MULTISTEP) && field_config_of(a.f) == FK_ANALYTIC;
 }
 
 // launch shape of a run (host-only work: safe before a stream capture)
 int plan_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, LaunchCfg& cfg) {
-    int block;
+    int block, ppt;
     bool q;
-    resolve_launch(ctx, d, a, block, q);
-    if (block > TPB_MAXT(field_config_of(a.f)))
+    resolve_launch(ctx, d, a, block, q, ppt);
+    if (ppt != 1 && ppt != 2) return fail(ctx, TP_E_ARG, "particles_per_thread must be 0, 1 or 2");
+    if (ppt == 2 && !ppt2_available(d, a)) ppt = 1;
+    if (block > TPB_MAXT(field_config_of(a.f)) / ppt)
         return fail(ctx, TP_E_ARG, "block exceeds the kernel's limit for this field configuration");
     a.use_queue = q;
+    a.ppt = ppt;
     cudaError_t e = d->precision == TP_PREC_FP32C ? prime_boris_fp32c(a) : prime_boris_fp64(a);
     if (e == cudaSuccess && a.save_work) e = prime_fill_work();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel load");
     int occ = 0;
     if (q) occ = d->precision == TP_PREC_FP32C ? occupancy_boris_fp32c(a, block) : occupancy_boris_fp64(a, block);
-    return pick_launch(ctx, a.n, block, q, occ, cfg);
+    return pick_launch(ctx, (a.n + ppt - 1) / ppt, block, q, occ, cfg);
 }
 
 // the stream work of a run: queue reset and the push kernel
@@ -1048,10 +1063,11 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    auto time_shape = [&](int block, int sched, double& ms) -> int {
+    auto time_shape = [&](int block, int sched, int ppt, double& ms) -> int {
         tp_run_desc dc = ds;
         dc.block = block;
         dc.schedule = sched;
+        dc.particles_per_thread = ppt;
         float best = 1e30f;
         for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
             BorisArgs ac = a;
@@ -1071,31 +1087,35 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
     const std::string key = tune_key(&ds, a);
     const int maxt = TPB_MAXT(field_config_of(a.f));
     const int blocks[] = {64, 96, 128, 192, 256, 384};
-    int best_b = 128, best_s = TP_SCHED_STATIC, cands = 0;
+    int best_b = 128, best_s = TP_SCHED_STATIC, best_p = 1, cands = 0;
     double best_ms = 1e300, def_ms = 0.0;
     // the default shape, with any earlier tuning of this variant set aside
     auto saved = ctx->tuned.find(key);
     bool had = saved != ctx->tuned.end();
-    std::pair<int, int> old = had ? saved->second : std::make_pair(0, 0);
+    tp_ctx::Shape old = had ? saved->second : tp_ctx::Shape{0, 0, 0};
     if (had) ctx->tuned.erase(key);
-    st = time_shape(0, TP_SCHED_AUTO, def_ms);
+    st = time_shape(0, TP_SCHED_AUTO, 1, def_ms);
     // With uneven lifetimes (adaptive steps, termination) a cut sample has
     // even ones and would favour the static schedule: only the queue is
     // timed there.
     const bool uneven = adaptive || ds.term.flags != 0;
-    for (int b : blocks) {
-        if (st != TP_OK) break;
-        if (b > maxt) continue;
-        for (int sc : {TP_SCHED_STATIC, TP_SCHED_QUEUE}) {
-            if (uneven && sc == TP_SCHED_STATIC) continue;
-            double ms = 0.0;
-            st = time_shape(b, sc, ms);
+    const int max_ppt = ppt2_available(&ds, a) ? 2 : 1;
+    for (int pp = 1; pp <= max_ppt; ++pp) {
+        for (int b : blocks) {
             if (st != TP_OK) break;
-            ++cands;
-            if (ms < best_ms) {
-                best_ms = ms;
-                best_b = b;
-                best_s = sc;
+            if (b > maxt / pp) continue;
+            for (int sc : {TP_SCHED_STATIC, TP_SCHED_QUEUE}) {
+                if (uneven && sc == TP_SCHED_STATIC) continue;
+                double ms = 0.0;
+                st = time_shape(b, sc, pp, ms);
+                if (st != TP_OK) break;
+                ++cands;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_b = b;
+                    best_s = sc;
+                    best_p = pp;
+                }
             }
         }
     }
@@ -1112,13 +1132,13 @@ int tp_autotune(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_f
         if (had) ctx->tuned[key] = old;
         return status_to_error(ctx, dev_status);
     }
-    ctx->tuned[key] = {best_b, best_s};
+    ctx->tuned[key] = {best_b, best_s, best_p};
     out->block = best_b;
     out->schedule = best_s;
     out->ms = best_ms;
     out->ms_default = def_ms;
     out->candidates = cands;
-    out->reserved = 0;
+    out->particles_per_thread = best_p;
     return TP_OK;
 }
 

@@ -146,6 +146,8 @@ struct BorisArgs {
     int32_t wrap[3];
     int32_t save_work;    // work rates appended to every save (width + 4)
     double wrapL[3], wrap0[3];
+    int32_t ppt;          // particles per thread of the fixed-step kernels (1 or 2)
+    int32_t pad_ppt;
 };
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {

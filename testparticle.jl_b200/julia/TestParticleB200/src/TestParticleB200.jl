@@ -178,7 +178,7 @@ struct TpRunDesc
     savestepinterval::Int64; maxiters::Int64
     save_start::Int32; save_end::Int32; save_everystep::Int32; save_fields::Int32
     term::TpTermDesc; step_cap::Int64; schedule::Int32; block::Int32; budget_s::Float64
-    save_work::Int32; reserved3::Int32
+    save_work::Int32; particles_per_thread::Int32
 end
 struct TpGCDesc
     alg::Int32; precision::Int32; t0::Float64; t1::Float64; dt::Float64

@@ -76,10 +76,13 @@ class EnsembleB200:
     schedule:  "auto", "static" (one thread per particle) or "queue"
                (persistent kernel pulling particles from a work queue).
     block:     threads per block (0: library default / tuned).
+    particles_per_thread:
+               fixed-step solves in analytic fields: 1 or 2 particles advanced
+               in lock step by each thread (0: library default / tuned).
     autotune:  time the candidate launch shapes on a sample before the
                first full-orbit solve of each kernel variant (tp_autotune);
-               later solves with block = 0 and schedule = "auto" use the
-               fastest.
+               later solves with block = 0, schedule = "auto" and
+               particles_per_thread = 0 use the fastest.
     """
 
     device: int = 0
@@ -88,6 +91,7 @@ class EnsembleB200:
     block: int = 0
     budget_s: float = 0.0
     autotune: bool = False
+    particles_per_thread: int = 0
 
 
 class EnsembleSerial:  # pragma: no cover - guidance only

@@ -238,8 +238,9 @@ class Context:
         code = self.lib.tp_autotune(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0),
                                     u0.shape[0], int(max_steps), C.byref(r))
         _check(self.lib, self.handle, code, "tp_autotune")
-        return {"block": r.block, "schedule": {1: "static", 2: "queue"}.get(r.schedule, "auto"), "ms": r.ms,
-                "ms_default": r.ms_default, "candidates": r.candidates}
+        return {"block": r.block, "schedule": {1: "static", 2: "queue"}.get(r.schedule, "auto"),
+                "particles_per_thread": r.particles_per_thread, "ms": r.ms, "ms_default": r.ms_default,
+                "candidates": r.candidates}
 
     def boris_graph(self, desc: _abi.RunDesc, E, B, u0, dt_i, tend_i, n: int, nslots: int, t_out, u_out, nsaved,
                     retcode, nsteps, status) -> "Graph":

@@ -144,6 +144,7 @@ def plan_boris(prob, balg, ens=None, *, trajectories=1, savestepinterval=1, dt=N
     desc.step_cap = int(step_cap)
     desc.schedule = _SCHED[ens.schedule]
     desc.block = int(ens.block)
+    desc.particles_per_thread = int(ens.particles_per_thread)
     desc.budget_s = float(ens.budget_s)
     u0 = _initial_table(prob, trajectories, 6)
     tend_arr = None if tend is None else np.ascontiguousarray(tend, dtype=np.float64)

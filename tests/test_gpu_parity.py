@@ -314,6 +314,25 @@ def test_queue_and_static_schedules_agree(tp):
     assert np.array_equal(a.nsaved, b.nsaved) and np.array_equal(a.u_all, b.u_all)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_two_particles_per_thread_is_the_same_solve(tp, precision):
+    # particles advanced two per thread in lock step take the same arithmetic
+    # as one per thread: identical saves, step counts and return codes, with
+    # either schedule and for a particle count that leaves a slot empty
+    w = tp.workloads.config3(1001, nt=1500, ssi=250)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B))
+    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=w.savestepinterval, isoutside=w.isoutside)
+    for alg in (tp.MultistepBoris(4, 2), tp.Boris()):
+        ref = tp.solve(prob, alg, tp.EnsembleB200(precision=precision, particles_per_thread=1, schedule="static"),
+                       **kw)
+        for sched in ("static", "queue"):
+            s = tp.solve(prob, alg, tp.EnsembleB200(precision=precision, particles_per_thread=2, schedule=sched),
+                         **kw)
+            assert np.array_equal(s.nsaved, ref.nsaved) and np.array_equal(s.retcodes, ref.retcodes)
+            assert np.array_equal(s.nsteps, ref.nsteps)
+            assert np.array_equal(s.t_all, ref.t_all) and np.array_equal(s.u_all, ref.u_all)
+
+
 # ------------------------------------------------------------------ gridded fields
 def _small_grid_workload(tp, n=512, nx=32, nt=2000, ssi=500):
     dx = 1.0e5
@@ -562,6 +581,23 @@ def test_autotune_chooses_a_valid_shape_and_keeps_results(tp):
     auto = tp.solve(prob, tp.Boris(), tp.EnsembleB200(precision="fp32c", autotune=True), dt=w.dt,
                     savestepinterval=100)
     assert np.array_equal(auto.u_all, base.u_all)
+    assert r["particles_per_thread"] == 1  # grids: one particle per thread only
+
+
+def test_autotune_times_particles_per_thread_in_analytic_fields(tp):
+    w = tp.workloads.config3(n=60000, nt=300, ssi=100)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    kw = dict(dt=w.dt, tend=w.tend, savestepinterval=100)
+    ctx = tp.Context.get(0)
+    for prec in ("fp32c", "fp64"):
+        plan = tp.plan_boris(prob, tp.MultistepBoris4(2), tp.EnsembleB200(precision=prec), **kw)
+        base = tp.solve(prob, tp.MultistepBoris4(2), tp.EnsembleB200(precision=prec, particles_per_thread=1),
+                        **kw)
+        r = ctx.autotune(plan.desc, plan.E, plan.B, plan.u0, max_steps=100)
+        assert r["particles_per_thread"] in (1, 2)
+        assert r["candidates"] >= 18  # (block sizes x schedules) for one and for two particles per thread
+        tuned = tp.solve(prob, tp.MultistepBoris4(2), tp.EnsembleB200(precision=prec), **kw)
+        assert np.array_equal(tuned.u_all, base.u_all)
 
 
 @pytest.mark.parametrize("term", [False, True])
