@@ -100,9 +100,9 @@ __device__ __forceinline__ int64_t next_particle32(const BorisArgs& a, int64_t& 
     if (!QUEUE) {
         int64_t g = first;
         first = a.n;
-        return g;
+        return take_particle(a, g);
     }
-    return (int64_t)atomicAdd(a.queue, 1ULL);
+    return take_particle(a, (int64_t)atomicAdd(a.queue, 1ULL));
 }
 
 }  // namespace
@@ -413,6 +413,276 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed32c_slots(BorisA
     }
 }
 
+// ---------------------------------------------------------------- cubic grids, warp-cooperative
+// E and B on one periodic, uniform, Cartesian 3-D grid interpolated at order
+// 3 (cardinal_interp, src/utility/interpolation.jl:142; the local cubic
+// Hermite with Catmull-Rom slopes of grid_general.cuh), from the interleaved
+// float table (E xyz0, B xyz0 per node, 32 bytes).  A particle's stencil is
+// 4 x 4 x 4 nodes; a row of 4 nodes along x is 128 contiguous bytes.  Instead
+// of each lane gathering its own 64 nodes (64 scattered lines per lane), the
+// warp gathers the stencils of its particles two at a time: for each, lane l
+// loads nodes (l & 3, (l >> 2) & 3, l >> 4) and (.., .., (l >> 4) + 2) -- 8
+// rows of 128 bytes per load instruction -- weights them, and a butterfly sum
+// over the warp leaves E and B with the owning lane (the two particles' loads
+// and sums interleave).  All 32 lanes of the warp must call it together;
+// lanes with want = false only help.
+// The weight of node d (0..3) of the 4-node stencil at fraction t of the
+// middle cell, w_d(t) = h-basis combination of the Catmull-Rom Hermite cubic
+// (grid_general.cuh), as the polynomial c0 + c1 t + c2 t^2 + c3 t^3:
+//   w0 = -t/2 + t^2 - t^3/2        w1 = 1 - 5t^2/2 + 3t^3/2
+//   w2 =  t/2 + 2t^2 - 3t^3/2      w3 = -t^2/2 + t^3/2
+// A lane always takes the same node of every stencil, so its coefficients
+// are fixed for the whole kernel and a weight costs three FMAs.
+struct CubicW {
+    float c0, c1, c2, c3;
+};
+__device__ __forceinline__ CubicW cubic_coef(int d) {
+    return d == 0 ? CubicW{0.0f, -0.5f, 1.0f, -0.5f}
+                  : (d == 1 ? CubicW{1.0f, 0.0f, -2.5f, 1.5f}
+                            : (d == 2 ? CubicW{0.0f, 0.5f, 2.0f, -1.5f} : CubicW{0.0f, 0.0f, -0.5f, 0.5f}));
+}
+__device__ __forceinline__ float cubic_w(const CubicW& c, float t) {
+    return fmaf(fmaf(fmaf(c.c3, t, c.c2), t, c.c1), t, c.c0);
+}
+
+// cell index in [0, n) and fraction in [0, 1) on a periodic axis, from the
+// compensated coordinate (positions are wrapped into the box)
+__device__ __forceinline__ void cubic_cell(const DevField& g, int a, float hi, float lo, int& i, float& f) {
+    AxF o;
+    axis32(g, a, hi, lo, o);  // periodic: always in range
+    i = o.i0;
+    f = o.f;
+}
+
+// this lane's weighted share of the stencil of the particle at cell (qi, qj,
+// qk), fractions (fx, fy, fz): E in s[0..2], B in s[3..5]
+__device__ __forceinline__ void cubic_share(const DevField& g, const float4* tab, int qi, int qj, int qk, float fx,
+                                            float fy, float fz, float s[6]) {
+    const int lane = threadIdx.x & 31;
+    const int dx = lane & 3, dy = (lane >> 2) & 3, dz = lane >> 4;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const float wxy = cubic_w(cubic_coef(dx), fx) * cubic_w(cubic_coef(dy), fy);
+    const float w0 = wxy * cubic_w(cubic_coef(dz), fz), w1 = wxy * cubic_w(cubic_coef(dz + 2), fz);
+    int ix = qi - 1 + dx, iy = qj - 1 + dy, iz0 = qk - 1 + dz, iz1 = qk + 1 + dz;
+    ix += ix < 0 ? nx : 0;
+    ix -= ix >= nx ? nx : 0;
+    iy += iy < 0 ? ny : 0;
+    iy -= iy >= ny ? ny : 0;
+    iz0 += iz0 < 0 ? nz : 0;
+    iz1 -= iz1 >= nz ? nz : 0;
+    const int64_t row = (int64_t)ix + (int64_t)nx * iy;
+    const int64_t nxy = (int64_t)nx * ny;
+    float4 e0, b0, e1, b1;
+    ldg_node8(tab + 2 * (row + nxy * iz0), e0, b0);
+    ldg_node8(tab + 2 * (row + nxy * iz1), e1, b1);
+    s[0] = fmaf(w0, e0.x, w1 * e1.x);
+    s[1] = fmaf(w0, e0.y, w1 * e1.y);
+    s[2] = fmaf(w0, e0.z, w1 * e1.z);
+    s[3] = fmaf(w0, b0.x, w1 * b1.x);
+    s[4] = fmaf(w0, b0.y, w1 * b1.y);
+    s[5] = fmaf(w0, b0.z, w1 * b1.z);
+}
+
+__device__ __forceinline__ void coop_cubic_eval(const DevField& g, const float4* tab, bool want, const CPos& p,
+                                                F3& E, F3& B) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int ci[3] = {0, 0, 0};
+    float cf[3] = {0.0f, 0.0f, 0.0f};
+    if (want) {
+        cubic_cell(g, 0, p.hi[0], p.lo[0], ci[0], cf[0]);
+        cubic_cell(g, 1, p.hi[1], p.lo[1], ci[1], cf[1]);
+        cubic_cell(g, 2, p.hi[2], p.lo[2], ci[2], cf[2]);
+    }
+    unsigned mask = __ballot_sync(full, want);
+    // two particles per round: their loads and reductions interleave
+    while (mask) {
+        const int qa = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const bool two = mask != 0;
+        const int qb = two ? __ffs(mask) - 1 : qa;
+        if (two) mask &= mask - 1;
+        float sa[6], sb[6];
+        cubic_share(g, tab, __shfl_sync(full, ci[0], qa), __shfl_sync(full, ci[1], qa), __shfl_sync(full, ci[2], qa),
+                    __shfl_sync(full, cf[0], qa), __shfl_sync(full, cf[1], qa), __shfl_sync(full, cf[2], qa), sa);
+        cubic_share(g, tab, __shfl_sync(full, ci[0], qb), __shfl_sync(full, ci[1], qb), __shfl_sync(full, ci[2], qb),
+                    __shfl_sync(full, cf[0], qb), __shfl_sync(full, cf[1], qb), __shfl_sync(full, cf[2], qb), sb);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                sa[c] += __shfl_xor_sync(full, sa[c], o);
+                sb[c] += __shfl_xor_sync(full, sb[c], o);
+            }
+        }
+        if (lane == qa) {
+            E = {sa[0], sa[1], sa[2]};
+            B = {sa[3], sa[4], sa[5]};
+        }
+        if (two && lane == qb) {
+            E = {sb[0], sb[1], sb[2]};
+            B = {sb[3], sb[4], sb[5]};
+        }
+    }
+}
+
+// Fixed-step Boris / Multistep in the cubic field, FP32C (compensated float
+// positions and velocities, float delta-form rotation), one particle per
+// lane, static schedule.  Every lane runs the loop until all lanes of its
+// warp are done, so that the cooperative gathers see the whole warp; a lane
+// whose particle is done (or that has none) only helps.  The fields are
+// static, so the save of r_{k-1} reuses the step's evaluation at r_{k-1}.
+// slot k of particle i: state, then the given E and B when save_fields
+__device__ __forceinline__ void save_row32(const BorisArgs& a, int W, int64_t i, int64_t k, const CPos& p,
+                                           const CV& v, double t, const F3& E, const F3& B) {
+    if (k >= a.nslots) {
+        set_status(a.status, TP_E_OVERFLOW);
+        return;
+    }
+    const int64_t n = a.n;
+    a.t_out[k * n + i] = t;
+    double* u = a.u_out + (k * W) * n + i;
+    u[0 * n] = cpos_value(a, p, 0);
+    u[1 * n] = cpos_value(a, p, 1);
+    u[2 * n] = cpos_value(a, p, 2);
+    u[3 * n] = (double)v.h.x + (double)v.l.x;
+    u[4 * n] = (double)v.h.y + (double)v.l.y;
+    u[5 * n] = (double)v.h.z + (double)v.l.z;
+    if (a.save_fields) {
+        u[6 * n] = E.x;
+        u[7 * n] = E.y;
+        u[8 * n] = E.z;
+        u[9 * n] = B.x;
+        u[10 * n] = B.y;
+        u[11 * n] = B.z;
+    }
+}
+
+template <bool MULTI>
+__global__ void __launch_bounds__(128, 5) k_cubic32c(BorisArgs a) {
+    const int W = 6 + (a.save_fields ? 6 : 0) + (a.save_work ? 4 : 0);
+    const uint64_t t_start = globaltimer_ns();
+    const int64_t i = take_particle(a, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+    const DevField& g = a.f.B;
+    const float4* tab = a.f.ebc32;
+
+    bool active = i < a.n;
+    CPos p;
+    CV v{};
+    for (int c = 0; c < 3; ++c) {
+        p.hi[c] = p.lo[c] = 0.0f;
+        p.w[c] = 0;
+    }
+    double dt = 0, t = 0, t1 = 0, t_last = 0;
+    float dth = 0, dtl = 0, hstep = 0;
+    int64_t it = 1, nt = 0;
+    int32_t nout = 0, iout = 0, csave = 0;
+    if (active) {
+        dt = a.dt_i ? a.dt_i[i] : a.dt;
+        t1 = a.tend_i ? a.tend_i[i] : a.t1;
+        nt = (fabs(dt) < 10.0 * 2.220446049250313e-16) ? -1 : jl_round((t1 - a.t0) / dt);
+        if (nt < 0 && fabs(dt) >= 10.0 * 2.220446049250313e-16) nt = -nt;
+        if (nt < 0 || nt > a.maxiters) {
+            set_status(a.status, TP_E_ARG);
+            a.nsaved[i] = 0;
+            a.retcode[i] = TP_RET_DEFAULT;
+            a.nsteps[i] = 0;
+            active = false;
+        }
+    }
+    if (active) {
+        dth = (float)dt;
+        dtl = (float)(dt - (double)dth);
+        hstep = vfac<MULTI>(a, dt);
+        nout = (int32_t)calc_nout(nt, a.ssi, a.save_start, a.save_end, a.save_everystep);
+        const double* u0 = a.u0 + 6 * i;
+        cpos_init(a, p, u0);
+        v = cv_from(u0 + 3);
+    }
+    // v_{-1/2} (and the save of u0 with its fields)
+    F3 E{0.0f, 0.0f, 0.0f}, B{0.0f, 0.0f, 0.0f};
+    coop_cubic_eval(g, tab, active, p, E, B);
+    if (active) {
+        if (a.save_start) {
+            a.t_out[i] = a.t0;
+            if (a.nslots > 0) {
+                double* u = a.u_out + i;
+                const double* u0 = a.u0 + 6 * i;
+                for (int c = 0; c < 6; ++c) u[c * a.n] = u0[c];
+                if (a.save_fields) {
+                    u[6 * a.n] = E.x; u[7 * a.n] = E.y; u[8 * a.n] = E.z;
+                    u[9 * a.n] = B.x; u[10 * a.n] = B.y; u[11 * a.n] = B.z;
+                }
+            } else {
+                set_status(a.status, TP_E_OVERFLOW);
+            }
+            t_last = a.t0;
+            iout = 1;
+        }
+        v = vel32<MULTI>(v, E, B, a, -0.5 * dt);
+        t = a.t0 - 0.5 * dt;
+    }
+    bool stepping = active && it <= nt;
+    bool finishing = active && !stepping;
+    for (;;) {
+        // ---- one step of _boris_loop! (boris.jl:452-476) for the stepping lanes
+        coop_cubic_eval(g, tab, stepping, p, E, B);
+        if (stepping) {
+            t += dt;
+            CV vn = vel32h<MULTI>(v, E, B, a, hstep);
+            CPos pn = p;
+            cpos_push_cv(a, pn, vn, dth, dtl);
+            if (a.term.flags && outside32<FK_GENGRID>(a, pn, vn, t + 0.5 * dt)) {
+                finishing = true;
+            } else {
+                if (a.save_everystep && it > 1 && csave == 0) {
+                    iout += 1;
+                    if (iout <= nout) {
+                        const double t_cur = t - 0.5 * dt;
+                        CV vs = vel32<MULTI>(v, E, B, a, 0.5 * dt);
+                        save_row32(a, W, i, iout - 1, p, vs, t_cur, E, B);
+                        t_last = t_cur;
+                    }
+                }
+                p = pn;
+                v = vn;
+                it += 1;
+                csave += 1;
+                if (csave == a.ssi) csave = 0;
+                if (it > nt) finishing = true;
+                if ((it & 1023) == 0 && globaltimer_ns() - t_start > a.budget_ns) {
+                    set_status(a.status, TP_E_TIMEOUT);
+                    finishing = true;
+                }
+            }
+            if (finishing) stepping = false;
+        }
+        // ---- final save and retcode (boris.jl:522-551) for the lanes that finished
+        int64_t final_step = it - 1;
+        bool save_final = false;
+        double t_final = 0.0;
+        if (finishing) {
+            save_final = a.save_end || (a.save_everystep && final_step > 0 && final_step % a.ssi == 0);
+            t_final = (final_step == nt) ? t1 : fma((double)final_step, dt, a.t0);
+            save_final = save_final && iout < nout && (iout == 0 || t_last < t_final);
+        }
+        coop_cubic_eval(g, tab, save_final, p, E, B);
+        if (finishing) {
+            if (save_final) {
+                const double dt_final = t_final - fma((double)final_step - 0.5, dt, a.t0);
+                CV vf = vel32<MULTI>(v, E, B, a, dt_final);
+                save_row32(a, W, i, iout, p, vf, t_final, E, B);
+                iout += 1;
+            }
+            a.nsaved[i] = (int32_t)iout;
+            a.retcode[i] = (int8_t)((iout < nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
+            a.nsteps[i] = final_step;
+            finishing = false;
+        }
+        if (!__any_sync(0xffffffffu, stepping)) break;
+    }
+}
+
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
 __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
@@ -555,9 +825,17 @@ static const void* pick_fk32(bool adaptive, int fk, int ppt) {
     return kernel_ptr32<MULTI, QUEUE, FK_GENERIC>(adaptive, 1);
 }
 
+// fixed steps in static cubic grids with the interleaved table
+static bool cubic_coop_kernel(const BorisArgs& a) {
+    return a.f.ebc32 != nullptr && (a.alg == TP_ALG_BORIS || a.alg == TP_ALG_MULTISTEP);
+}
+
+bool fp32c_cubic_coop(const BorisArgs& a) { return cubic_coop_kernel(a); }
+
 static const void* select_kernel32(const BorisArgs& a, bool queue) {
     const bool multi = a.alg == TP_ALG_MULTISTEP || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
     const bool adaptive = a.alg == TP_ALG_ADAPTIVE || a.alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    if (cubic_coop_kernel(a)) return multi ? (const void*)k_cubic32c<true> : (const void*)k_cubic32c<false>;
     const int fk = field_config_of(a.f);
     const int ppt = a.ppt;
     if (multi) return queue ? pick_fk32<true, true>(adaptive, fk, ppt) : pick_fk32<true, false>(adaptive, fk, ppt);

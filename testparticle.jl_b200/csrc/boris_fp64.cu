@@ -66,9 +66,9 @@ __device__ __forceinline__ int64_t next_particle(const BorisArgs& a, int64_t& fi
     if (!QUEUE) {
         int64_t g = first;
         first = a.n;  // static: one particle per thread
-        return g;
+        return take_particle(a, g);
     }
-    return (int64_t)atomicAdd(a.queue, 1ULL);
+    return take_particle(a, (int64_t)atomicAdd(a.queue, 1ULL));
 }
 
 }  // namespace

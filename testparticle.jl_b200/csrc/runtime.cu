@@ -56,6 +56,9 @@ struct tp_field {
     uint64_t eb_partner = 0;
     void* d_eb = nullptr;
     void* d_eb32 = nullptr;
+    // the same for two cubic periodic grids (k_cubic32c)
+    uint64_t ebc_partner = 0;
+    void* d_ebc32 = nullptr;
     void* d_axis[3] = {nullptr, nullptr, nullptr};  // node coordinates of non-uniform axes
     // SERIES: owned snapshot fields, their device descriptors and times
     std::vector<tp_field*> snaps;
@@ -345,6 +348,25 @@ bool same_geometry(const tp_field* a, const tp_field* b) {
     return true;
 }
 
+// E and B both periodic (exclusive), uniform, Cartesian 3-D grids of order 3
+// on one geometry with at least 4 nodes per axis: the interleaved float table
+// of the warp-cooperative FP32C kernel
+bool same_geometry_cubic(const tp_field* a, const tp_field* b) {
+    for (const tp_field* f : {a, b}) {
+        const tp_field_desc& d = f->desc;
+        if (d.kind != TP_FIELD_GRID || d.order != TP_ORDER_CUBIC || d.geometry != TP_GRID_CARTESIAN) return false;
+        if (!(d.ndim == 0 || d.ndim == 3) || d.bc != TP_BC_PERIODIC) return false;
+        for (int k = 0; k < 3; ++k)
+            if (d.axis[k] || d.n[k] < 4 || d.n[k] > (1 << 20)) return false;
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (a->desc.n[k] != b->desc.n[k]) return false;
+        if (a->desc.origin[k] != b->desc.origin[k]) return false;
+        if (a->desc.spacing[k] != b->desc.spacing[k]) return false;
+    }
+    return a->nodes <= ((int64_t)1 << 31) / 2;
+}
+
 DevTerm dev_term(const tp_term_desc& t) {
     DevTerm d{};
     d.flags = t.flags;
@@ -391,6 +413,19 @@ int make_dev_fields(tp_ctx* ctx, const tp_field* E, tp_field* B, DevFields& F) {
         F.eb = B->d_eb;
         F.eb_f64 = B->desc.dtype == TP_DTYPE_F64;
         F.eb32 = (const float4*)(B->d_eb32 ? B->d_eb32 : B->d_eb);
+    } else if (same_geometry_cubic(E, B)) {
+        if (B->ebc_partner != E->id) {
+            if (B->d_ebc32) cudaFree(B->d_ebc32);
+            B->d_ebc32 = nullptr;
+            const int f64e = E->desc.dtype == TP_DTYPE_F64, f64b = B->desc.dtype == TP_DTYPE_F64;
+            cudaError_t e = cudaMalloc(&B->d_ebc32, (size_t)B->nodes * 8 * sizeof(float));
+            if (e == cudaSuccess) e = launch_pack_node_table(E->d_raw, f64e, E->nodes, B->d_ebc32, 0, 2, 0, ctx->stream);
+            if (e == cudaSuccess) e = launch_pack_node_table(B->d_raw, f64b, B->nodes, B->d_ebc32, 0, 2, 1, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "interleaved cubic field table");
+            B->ebc_partner = E->id;
+        }
+        F.ebc32 = (const float4*)B->d_ebc32;
     }
     return TP_OK;
 }
@@ -416,7 +451,12 @@ void set_wrap(BorisArgs& a, const tp_field* E, const tp_field* B, const tp_term_
                     if (g->desc.jac[3 * r + c] != 0.0) ok = false;
                 continue;
             }
-            if (k != TP_FIELD_GRID || g->desc.bc != TP_BC_PERIODIC || g->dev.general) {
+            // trilinear grids, and cubic ones on uniform Cartesian 3-D axes:
+            // exclusive-periodic with period n dx on every axis
+            const bool cubic_uniform = g->desc.order == TP_ORDER_CUBIC && g->desc.geometry == TP_GRID_CARTESIAN &&
+                                       (g->desc.ndim == 0 || g->desc.ndim == 3) && !g->desc.axis[0] &&
+                                       !g->desc.axis[1] && !g->desc.axis[2];
+            if (k != TP_FIELD_GRID || g->desc.bc != TP_BC_PERIODIC || (g->dev.general && !cubic_uniform)) {
                 ok = false;
                 continue;
             }
@@ -730,7 +770,7 @@ void tp_field_destroy(tp_field* f) {
     if (!f) return;
     DeviceGuard g(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
-    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_axis[0], f->d_axis[1], f->d_axis[2],
+    for (void* p : {f->d_raw, f->d_tab, f->d_tab32, f->d_eb, f->d_eb32, f->d_ebc32, f->d_axis[0], f->d_axis[1], f->d_axis[2],
                     f->d_snaps, f->d_times, f->d_self})
         if (p) cudaFree(p);
     for (tp_field* c : f->snaps) tp_field_destroy(c);
@@ -852,6 +892,10 @@ int plan_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, LaunchCfg
     resolve_launch(ctx, d, a, block, q, ppt);
     if (ppt != 1 && ppt != 2) return fail(ctx, TP_E_ARG, "particles_per_thread must be 0, 1 or 2");
     if (ppt == 2 && !ppt2_available(d, a)) ppt = 1;
+    if (d->precision == TP_PREC_FP32C && fp32c_cubic_coop(a)) {
+        q = false;  // the warp-cooperative kernel walks one particle per lane, static
+        if (block > 128) block = 128;
+    }
     if (block > TPB_MAXT(field_config_of(a.f)) / ppt)
         return fail(ctx, TP_E_ARG, "block exceeds the kernel's limit for this field configuration");
     a.use_queue = q;
@@ -891,6 +935,33 @@ int issue_boris_launch(tp_ctx* ctx, const tp_run_desc* d, BorisArgs& a, const La
         e = launch_fill_work(w, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "work-rate pass");
     }
+    return TP_OK;
+}
+
+// Processing order of a solve in gridded fields (Cartesian geometry, n >=
+// 65536): the particles sorted by the Morton key of their initial cell, so
+// that the lanes of a warp gather neighbouring nodes (one radix sort of n
+// keys, in the solve's device time).  Results do not depend on the order.
+// The scratch comes from the pool on stream s; the caller releases *buf
+// there after the push.
+int order_particles(tp_ctx* ctx, BorisArgs& a, cudaStream_t s, void** buf) {
+    *buf = nullptr;
+    a.perm = nullptr;
+    const DevField* g = nullptr;
+    if (a.f.B.kind == TP_FIELD_GRID && a.f.B.geom == TP_GRID_CARTESIAN) g = &a.f.B;
+    else if (a.f.E.kind == TP_FIELD_GRID && a.f.E.geom == TP_GRID_CARTESIAN) g = &a.f.E;
+    if (!g || a.n < 65536 || a.n > 0x7fffffffLL) return TP_OK;
+    size_t bytes = 0;
+    cudaError_t e = cell_order(a.u0, a.n, *g, nullptr, &bytes, nullptr, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(buf, bytes, s);
+    int32_t* perm = nullptr;
+    if (e == cudaSuccess) e = cell_order(a.u0, a.n, *g, *buf, &bytes, &perm, s);
+    if (e != cudaSuccess) {
+        if (*buf) cudaFreeAsync(*buf, s);
+        *buf = nullptr;
+        return cuda_fail(ctx, e, "particle cell ordering");
+    }
+    a.perm = perm;
     return TP_OK;
 }
 
@@ -1003,7 +1074,10 @@ int tp_boris_run_device(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, co
         e = cudaMallocAsync((void**)&q, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "queue counter");
     }
-    st = launch_boris(ctx, d, a, s, q);
+    void* obuf = nullptr;
+    st = order_particles(ctx, a, s, &obuf);
+    if (st == TP_OK) st = launch_boris(ctx, d, a, s, q);
+    if (obuf) cudaFreeAsync(obuf, s);
     if (q) cudaFreeAsync(q, s);
     return st;
 }
@@ -1323,7 +1397,10 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, s);
         if (n > 0) {
-            st = launch_boris(ctx, d, a, s, q_d.as<unsigned long long>());
+            void* obuf = nullptr;
+            st = order_particles(ctx, a, s, &obuf);
+            if (st == TP_OK) st = launch_boris(ctx, d, a, s, q_d.as<unsigned long long>());
+            if (obuf) cudaFreeAsync(obuf, s);
             if (st != TP_OK) {
                 cudaEventDestroy(ev0);
                 cudaEventDestroy(ev1);

@@ -93,6 +93,9 @@ struct DevFields {
     const float4* eb32;   // float interleaved table for the FP32C kernels
     int32_t eb_f64;
     int32_t pad;
+    // E and B on one periodic, uniform, Cartesian 3-D grid of order 3: their
+    // float interleaved table (the warp-cooperative FP32C kernel), else null
+    const float4* ebc32;
 };
 
 // Termination predicate (the reference's isoutside, as flags).
@@ -148,7 +151,16 @@ struct BorisArgs {
     double wrapL[3], wrap0[3];
     int32_t ppt;          // particles per thread of the fixed-step kernels (1 or 2)
     int32_t pad_ppt;
+    // optional processing order: the k-th particle a kernel takes is perm[k]
+    // (a cell ordering of the initial positions in gridded fields, so that
+    // the lanes of a warp gather neighbouring nodes); null = 0, 1, 2, ...
+    const int32_t* perm;
 };
+
+// the particle taken k-th under the run's processing order (k < n)
+__device__ __forceinline__ int64_t take_particle(const BorisArgs& a, int64_t k) {
+    return (a.perm && k < a.n) ? (int64_t)__ldg(a.perm + k) : k;
+}
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {
     uint64_t t;

@@ -155,6 +155,8 @@ cudaError_t launch_table_unpack(const float4* tab, int64_t nodes, int stride, in
 
 cudaError_t launch_boris_fp64(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_boris_fp32c(const BorisArgs& a, const LaunchCfg& c, cudaStream_t s);
+// the FP32C run takes the warp-cooperative cubic-grid kernel (static schedule only)
+bool fp32c_cubic_coop(const BorisArgs& a);
 int occupancy_boris_fp64(const BorisArgs& a, int block);
 int occupancy_boris_fp32c(const BorisArgs& a, int block);
 
@@ -192,6 +194,10 @@ cudaError_t launch_noalloc_pack(int64_t* scratch, const double* t_in, const doub
                                 double* t_out, double* u_out, int64_t* total_out, cudaStream_t s);
 
 // packing helpers (pack.cu)
+// processing order of the particles by the Morton key of their initial cell
+// on grid g (pack.cu); tmp = null sizes the scratch
+cudaError_t cell_order(const double* u0, int64_t n, const DevField& g, void* tmp, size_t* tmp_bytes,
+                       int32_t** perm, cudaStream_t s);
 cudaError_t launch_pack_node_table(const void* src, int src_f64, int64_t nodes, void* dst,
                                    int dst_f64, int stride, int off, cudaStream_t s);
 cudaError_t launch_pack_results(const double* t_in, const double* u_in, const int32_t* nsaved,

@@ -309,3 +309,38 @@ def test_series_boris_and_gc_match_oracle(tp, orc):
     gr = orc.gc_run(gp.desc, gp.E, gp.B, gp.y0, gp.q_i, gp.q2m_i, gp.mu_i)
     assert np.array_equal(gs.nsaved, gr.nsaved)
     assert _rel_rows(gs.u_all[:, :3], gr.u[:, :3]) <= 1e-12
+
+
+@pytest.mark.parametrize("alg", ["boris", "multistep"])
+def test_cubic_grid_fp32c_warp_cooperative_kernel(tp, orc, alg):
+    """E and B on one periodic cubic grid take the warp-cooperative FP32C
+    kernel (one particle's 64-node stencil gathered by the whole warp).  Uneven
+    lifetimes (per-particle dt, a box that stops some orbits), a partial last
+    warp and saved fields, against the float64 oracle over ~1.5 gyroperiods."""
+    E, B, L = _turb(tp, 20, 3, tp.PeriodicBC("exclusive"))
+    rng = np.random.default_rng(11)
+    n = 1000
+    u0 = np.empty((6, n))
+    u0[:3] = rng.uniform(0.3 * L, 0.7 * L, (3, n))
+    u0[3:] = rng.normal(0.0, 1.0e5, (3, n))
+    T = tp.get_gyroperiod(5.0e-9)
+    dt = (T / 40) * rng.uniform(0.9, 1.1, n)
+    a = tp.Boris() if alg == "boris" else tp.MultistepBoris4(2)
+    prob = tp.TraceProblem(u0, (0.0, 1.5 * T), tp.prepare(E, B))
+    # orbits stream along B (z) and drift across x and y by about L within the
+    # span: a box of [-L/2, 3L/2] in y stops about a fifth of them (oracle)
+    box = tp.TerminateBox((-np.inf, -0.5 * L, -np.inf), (np.inf, 1.5 * L, np.inf))
+    kw = dict(dt=dt, savestepinterval=20, save_fields=True, isoutside=box)
+    s32 = tp.solve(prob, a, tp.EnsembleB200(precision="fp32c"), **kw)
+    plan = tp.plan_boris(prob, a, **kw)
+    ref = orc.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    assert np.array_equal(s32.nsaved, ref.nsaved) and np.array_equal(s32.retcodes, ref.retcode)
+    assert 0 < np.sum(ref.retcode == 2) < n  # some orbits stop at the box, some do not
+    assert np.array_equal(s32.t_all, ref.t)
+    d = np.abs(s32.u_all[:, :3] - ref.u[:, :3]).max(axis=1)
+    assert np.max(d) <= 1e-5 * L
+    assert _rel_rows(s32.u_all[:, 3:6], ref.u[:, 3:6]) <= 1e-4
+    # the saved fields are the kernel's float evaluation at the saved positions:
+    # against the float64 evaluation at those same positions
+    Eg, Bg = tp.get_fields(s32)
+    assert _rel_rows(s32.u_all[:, 9:12], Bg) <= 1e-5 and _rel_rows(s32.u_all[:, 6:9], Eg) <= 1e-5
