@@ -420,12 +420,12 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed32c_slots(BorisA
 // float table (E xyz0, B xyz0 per node, 32 bytes).  A particle's stencil is
 // 4 x 4 x 4 nodes; a row of 4 nodes along x is 128 contiguous bytes.  Instead
 // of each lane gathering its own 64 nodes (64 scattered lines per lane), the
-// warp gathers the stencils of its particles two at a time: for each, lane l
-// loads nodes (l & 3, (l >> 2) & 3, l >> 4) and (.., .., (l >> 4) + 2) -- 8
-// rows of 128 bytes per load instruction -- weights them, and a butterfly sum
-// over the warp leaves E and B with the owning lane (the two particles' loads
-// and sums interleave).  All 32 lanes of the warp must call it together;
-// lanes with want = false only help.
+// warp gathers the stencils of its particles four at a time: for each, lane
+// l loads nodes (l & 3, (l >> 2) & 3, l >> 4) and (.., .., (l >> 4) + 2) -- 8
+// rows of 128 bytes per load instruction -- and weights them; one
+// reduce-scatter over the warp sums the four particles' E and B (reduce4x6)
+// and the owning lanes fetch theirs.  All 32 lanes of the warp must call it
+// together; lanes with want = false only help.
 // The weight of node d (0..3) of the 4-node stencil at fraction t of the
 // middle cell, w_d(t) = h-basis combination of the Catmull-Rom Hermite cubic
 // (grid_general.cuh), as the polynomial c0 + c1 t + c2 t^2 + c3 t^3:
@@ -483,6 +483,47 @@ __device__ __forceinline__ void cubic_share(const DevField& g, const float4* tab
     s[5] = fmaf(w0, b0.z, w1 * b1.z);
 }
 
+// Sum s[k][c] (particle k = 0..3, component c = 0..5: E xyz, B xyz) over the
+// 32 lanes of the warp by halving (a reduce-scatter): after the exchanges with
+// lanes 16, 8 and 4 apart each lane holds three components of one particle
+// summed over 8 lanes -- particle 2 b4 + b3, components 3 b2 .. 3 b2 + 2 for
+// lane bits b4 b3 b2 -- and two butterfly levels complete the sums: 27
+// shuffles for four particles instead of 120.  Returns the three sums.
+__device__ __forceinline__ void reduce4x6(const float s[4][6], float out[3]) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
+    // lanes 16 apart: keep particles {0, 1} (b4 = 0) or {2, 3}
+    float t[2][6];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const float keep = b4 ? s[2 + k][c] : s[k][c];
+            const float send = b4 ? s[k][c] : s[2 + k][c];
+            t[k][c] = keep + __shfl_xor_sync(full, send, 16);
+        }
+    // lanes 8 apart: keep particle b3 of the pair
+    float u[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const float keep = b3 ? t[1][c] : t[0][c];
+        const float send = b3 ? t[0][c] : t[1][c];
+        u[c] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    // lanes 4 apart: keep E (b2 = 0) or B
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float keep = b2 ? u[3 + c] : u[c];
+        const float send = b2 ? u[c] : u[3 + c];
+        out[c] = keep + __shfl_xor_sync(full, send, 4);
+    }
+#pragma unroll
+    for (int o = 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[c] += __shfl_xor_sync(full, out[c], o);
+}
+
 __device__ __forceinline__ void coop_cubic_eval(const DevField& g, const float4* tab, bool want, const CPos& p,
                                                 F3& E, F3& B) {
     const unsigned full = 0xffffffffu;
@@ -495,33 +536,38 @@ __device__ __forceinline__ void coop_cubic_eval(const DevField& g, const float4*
         cubic_cell(g, 2, p.hi[2], p.lo[2], ci[2], cf[2]);
     }
     unsigned mask = __ballot_sync(full, want);
-    // two particles per round: their loads and reductions interleave
+    // four particles per round (the last round repeats its final particle)
     while (mask) {
-        const int qa = __ffs(mask) - 1;
+        int q[4];
+        q[0] = __ffs(mask) - 1;
         mask &= mask - 1;
-        const bool two = mask != 0;
-        const int qb = two ? __ffs(mask) - 1 : qa;
-        if (two) mask &= mask - 1;
-        float sa[6], sb[6];
-        cubic_share(g, tab, __shfl_sync(full, ci[0], qa), __shfl_sync(full, ci[1], qa), __shfl_sync(full, ci[2], qa),
-                    __shfl_sync(full, cf[0], qa), __shfl_sync(full, cf[1], qa), __shfl_sync(full, cf[2], qa), sa);
-        cubic_share(g, tab, __shfl_sync(full, ci[0], qb), __shfl_sync(full, ci[1], qb), __shfl_sync(full, ci[2], qb),
-                    __shfl_sync(full, cf[0], qb), __shfl_sync(full, cf[1], qb), __shfl_sync(full, cf[2], qb), sb);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int k = 1; k < 4; ++k) {
+            q[k] = mask ? __ffs(mask) - 1 : q[k - 1];
+            mask &= mask - 1;
+        }
+        float sk[4][6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                sa[c] += __shfl_xor_sync(full, sa[c], o);
-                sb[c] += __shfl_xor_sync(full, sb[c], o);
-            }
-        }
-        if (lane == qa) {
-            E = {sa[0], sa[1], sa[2]};
-            B = {sa[3], sa[4], sa[5]};
-        }
-        if (two && lane == qb) {
-            E = {sb[0], sb[1], sb[2]};
-            B = {sb[3], sb[4], sb[5]};
+        for (int k = 0; k < 4; ++k)
+            cubic_share(g, tab, __shfl_sync(full, ci[0], q[k]), __shfl_sync(full, ci[1], q[k]),
+                        __shfl_sync(full, ci[2], q[k]), __shfl_sync(full, cf[0], q[k]),
+                        __shfl_sync(full, cf[1], q[k]), __shfl_sync(full, cf[2], q[k]), sk[k]);
+        float r[3];
+        reduce4x6(sk, r);
+        // the owner of particle k takes E from lane (k >> 1) << 4 | (k & 1) << 3
+        // and B from that lane + 4
+        int mine = -1;
+#pragma unroll
+        for (int k = 3; k >= 0; --k)
+            if (lane == q[k]) mine = k;
+        const int src = mine < 0 ? 0 : (((mine >> 1) << 4) | ((mine & 1) << 3));
+        const float ex = __shfl_sync(full, r[0], src), ey = __shfl_sync(full, r[1], src),
+                    ez = __shfl_sync(full, r[2], src);
+        const float bx = __shfl_sync(full, r[0], src + 4), by = __shfl_sync(full, r[1], src + 4),
+                    bz = __shfl_sync(full, r[2], src + 4);
+        if (mine >= 0) {
+            E = {ex, ey, ez};
+            B = {bx, by, bz};
         }
     }
 }
