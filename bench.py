@@ -318,10 +318,12 @@ def leg_dipole(tp, torch, ctx, dist, dev, stream, flush, world, n, nt, multistep
     return out
 
 
-def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, reps=3):
+def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=0, reps=3, compare_k=64):
     """Discrete adjoint of Boris in the gridded field (config 5): forward with
-    checkpoints, backward (recompute + reverse + node scatter), and the plain
-    FP32C push of the same workload, each timed on the device."""
+    checkpoints, backward, and the plain FP32C push of the same workload, each
+    timed on the device.  K = 0 takes the library's automatic segment length
+    (2 steps: the one-kernel backward); the same problem with `compare_k`-step
+    segments (two kernels per segment) is timed beside it."""
     w = tp.workloads.config5(n=n, nt=nt)
     prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
     # targets: the float64 endpoints (library FP64 path) plus seeded offsets
@@ -329,28 +331,11 @@ def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, re
                      savestepinterval=10 ** 9, save_start=False)
     x_target = torch.from_numpy(sol64.final_states()[:, :3] + w.extra["target_offset"]).to(dev)
     del sol64
-    plan = tp.plan_adjoint(prob, tp.EnsembleB200(device=ctx.device, precision="fp32c"), dt=w.dt,
-                           checkpoint_every=K)
-    u0 = torch.from_numpy(plan.u0).to(dev)
-    uf = torch.empty_like(u0)
     s = stream.cuda_stream
-    tape = ctx.adjoint_forward_device(plan.desc, plan.E, plan.B, u0.data_ptr(), n, uf.data_ptr(), s)
     nodes = int(np.prod(w.B.data.shape[1:]))
     gE = torch.empty(3 * nodes, dtype=torch.float64, device=dev)
     gB = torch.empty_like(gE)
     gp = torch.empty(6, dtype=torch.float64, device=dev)
-    gu = torch.empty_like(u0)
-
-    def grad_final():
-        g = torch.zeros_like(uf)
-        g[:, :3] = 2.0 * (uf[:, :3] - x_target) / n
-        return g
-
-    def fwd():
-        tape.rerun_device(u0.data_ptr(), uf.data_ptr(), s)
-
-    def bwd(g):
-        tape.backward_device(g.data_ptr(), gu.data_ptr(), gE.data_ptr(), gB.data_ptr(), gp.data_ptr(), s)
 
     def device_ms(fn, *args):
         fn(*args)  # warm-up (first backward allocates the records and tables)
@@ -367,11 +352,29 @@ def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, re
             tot += a.elapsed_time(b)
         return tot / reps
 
-    torch.cuda.synchronize()
-    ms_f = device_ms(fwd)
-    g = grad_final()
-    loss = float(((uf[:, :3] - x_target) ** 2).sum().item() / n)
-    ms_b = device_ms(bwd, g)
+    def run_tape(k):
+        plan = tp.plan_adjoint(prob, tp.EnsembleB200(device=ctx.device, precision="fp32c"), dt=w.dt,
+                               checkpoint_every=k)
+        u0 = torch.from_numpy(plan.u0).to(dev)
+        uf = torch.empty_like(u0)
+        gu = torch.empty_like(u0)
+        tape = ctx.adjoint_forward_device(plan.desc, plan.E, plan.B, u0.data_ptr(), n, uf.data_ptr(), s)
+        torch.cuda.synchronize()
+        ms_f = device_ms(lambda: tape.rerun_device(u0.data_ptr(), uf.data_ptr(), s))
+        g = torch.zeros_like(uf)
+        g[:, :3] = 2.0 * (uf[:, :3] - x_target) / n
+        loss = float(((uf[:, :3] - x_target) ** 2).sum().item() / n)
+        ms_b = device_ms(lambda: tape.backward_device(g.data_ptr(), gu.data_ptr(), gE.data_ptr(), gB.data_ptr(),
+                                                      gp.data_ptr(), s))
+        out = {"checkpoint_every": tape.segments()[0], "forward_ms": ms_f, "backward_ms": ms_b,
+               "tape_device_bytes": tape.info()[0], "loss": loss,
+               "grad_x0_norm": float(torch.linalg.vector_norm(gu[:, :3]).item()),
+               "dL_dB0": 4.0e5 * float(gp[1].item()) + float(gp[5].item())}
+        tape.close()
+        return out
+
+    main = run_tape(K)
+    other = run_tape(compare_k)
     # the plain FP32C push of the same workload (no checkpoints, final save only)
     pp = tp.plan_boris(prob, tp.Boris(), tp.EnsembleB200(device=ctx.device, precision="fp32c"), dt=w.dt,
                        savestepinterval=10 ** 9, save_start=False)
@@ -379,16 +382,14 @@ def leg_adjoint(tp, torch, ctx, dev, stream, flush, n=1 << 18, nt=4096, K=64, re
     ms_p = device_ms(run.launch, pp)
     run.check()
     ps = float(n) * nt
-    gnorm = float(torch.linalg.vector_norm(gu[:, :3]).item())
-    dLdB0 = 4.0e5 * float(gp[1].item()) + float(gp[5].item())
-    bytes_, _ = tape.info()
-    tape.close()
-    return {"workload": w.name, "particles": n, "time_steps": nt, "checkpoint_every": K,
-            "forward_ms": ms_f, "backward_ms": ms_b, "plain_fp32c_push_ms": ms_p,
+    ms_f, ms_b = main["forward_ms"], main["backward_ms"]
+    return {"workload": w.name, "particles": n, "time_steps": nt, **main, "plain_fp32c_push_ms": ms_p,
             "forward": {"value": ps / (ms_f * 1e-3), "unit": "particle-steps/s"},
             "backward": {"value": ps / (ms_b * 1e-3), "unit": "particle-steps/s"},
             "adjoint_over_forward": ms_b / ms_f, "adjoint_over_plain_push": ms_b / ms_p,
-            "tape_device_bytes": bytes_, "loss": loss, "grad_x0_norm": gnorm, "dL_dB0": dLdB0}
+            "forward_plus_backward_ms": ms_f + ms_b,
+            f"segments_of_{compare_k}": {k: other[k] for k in ("checkpoint_every", "forward_ms", "backward_ms",
+                                                             "tape_device_bytes", "loss")}}
 
 
 def leg_gc(tp, n):
@@ -727,6 +728,7 @@ def main():
                          "then FP64)")
     ap.add_argument("--adj-n", type=int, default=1 << 18)
     ap.add_argument("--adj-nt", type=int, default=4096)
+    ap.add_argument("--adj-k", type=int, default=0, help="checkpoint interval of the adjoint leg (0: automatic)")
     args = ap.parse_args()
     if args.sample <= 0:
         # oracle rates at 16 threads: ~1.5e8 (gridded Boris) and ~1.3e8
@@ -751,7 +753,8 @@ def main():
     if args.adjoint_only:
         dev = torch.device("cuda", local)
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-        leg = leg_adjoint(tp, torch, ctx, dev, torch.cuda.current_stream(), flush, n=args.adj_n, nt=args.adj_nt)
+        leg = leg_adjoint(tp, torch, ctx, dev, torch.cuda.current_stream(), flush, n=args.adj_n, nt=args.adj_nt,
+                          K=args.adj_k)
         if rank == 0:
             print(json.dumps({"adjoint_only": leg}), flush=True)
         return

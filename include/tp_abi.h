@@ -554,7 +554,14 @@ int tp_pack_results_device_noalloc(tp_ctx* ctx, const double* t_in,
 typedef struct tp_adj_desc {
     tp_run_desc run;           /* alg TP_ALG_BORIS, precision TP_PREC_FP32C,
                                   term.flags 0; t0, t1, dt, q2m, block     */
-    int64_t checkpoint_every;  /* K >= 1 steps per checkpoint segment     */
+    int64_t checkpoint_every;  /* K >= 1 steps per checkpoint segment, or
+                                  0: automatic (2 for an interleaved E/B
+                                  grid when the tape fits in half of the
+                                  free device memory, else 64).  The tape
+                                  holds 48 bytes per particle per segment;
+                                  E/B-grid segments of <= 8 steps run the
+                                  one-kernel backward, longer ones two
+                                  kernels per segment                     */
 } tp_adj_desc;
 
 typedef struct tp_tape tp_tape;
@@ -583,6 +590,9 @@ int tp_tape_rerun_device(tp_tape* tape, const double* u0, double* u_final,
 /* device bytes a tape holds (checkpoints, and after the first backward pass
  * the segment records and gradient tables), and its step count N */
 int tp_tape_info(const tp_tape* tape, int64_t* device_bytes, int64_t* nsteps);
+/* Steps per checkpoint segment the tape uses (the automatic choice resolved)
+ * and the number of segments; either pointer may be null. */
+int tp_tape_segments(const tp_tape* tape, int64_t* checkpoint_every, int64_t* segments);
 void tp_tape_destroy(tp_tape* tape);
 
 #ifdef __cplusplus

@@ -301,6 +301,7 @@ SIGNATURES = [
     ("tp_adjoint_backward_device", C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     ("tp_tape_rerun_device", C.c_int, [_P, _P, _P, _P]),
     ("tp_tape_info", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("tp_tape_segments", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("tp_tape_destroy", None, [_P]),
 ]
 

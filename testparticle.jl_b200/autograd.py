@@ -189,7 +189,7 @@ class BorisAdjointFunction(torch.autograd.Function):
 
 
 def boris_final_state(u0: torch.Tensor, E, B, *, q2m: float, dt: float, tspan, m: float = 1.0,
-                      checkpoint_every: int = 64, block: int = 0) -> torch.Tensor:
+                      checkpoint_every: int = 0, block: int = 0) -> torch.Tensor:
     """Differentiable final save (x_N, v_N), (N, 6) float64, of the fixed-step Boris solve.
 
     The forward is the FP32C push of EnsembleB200(precision="fp32c") without

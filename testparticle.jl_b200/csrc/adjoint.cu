@@ -47,39 +47,42 @@ namespace tpb {
 
 namespace {
 
-constexpr int kCk = 15;   // checkpoint words per particle
 constexpr int kRec = 9;   // record words per particle-step
 
 __device__ __forceinline__ F3 nanf3_() { return nanf3(); }
 
+// Checkpoint: position hi xyz, lo xyz, velocity hi xyz, lo xyz.  The wrap
+// counts are left out: the backward evaluates fields only, and wrapped axes
+// are periodic in every field.  Written and read once, with streaming
+// (evict-first) hints so that the tape does not displace the field table
+// from L2.
 __device__ __forceinline__ void store_ck(const AdjArgs& A, int64_t s, int64_t i, const CPos& p, const CV& v) {
     const int64_t n = A.a.n;
-    float* c = A.ckpt + s * kCk * n + i;
+    float* c = A.ckpt + s * kAdjCkWords * n + i;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        c[(0 + k) * n] = p.hi[k];
-        c[(3 + k) * n] = p.lo[k];
-        c[(6 + k) * n] = __int_as_float(p.w[k]);
+        __stcs(c + (0 + k) * n, p.hi[k]);
+        __stcs(c + (3 + k) * n, p.lo[k]);
     }
-    c[9 * n] = v.h.x;
-    c[10 * n] = v.h.y;
-    c[11 * n] = v.h.z;
-    c[12 * n] = v.l.x;
-    c[13 * n] = v.l.y;
-    c[14 * n] = v.l.z;
+    __stcs(c + 6 * n, v.h.x);
+    __stcs(c + 7 * n, v.h.y);
+    __stcs(c + 8 * n, v.h.z);
+    __stcs(c + 9 * n, v.l.x);
+    __stcs(c + 10 * n, v.l.y);
+    __stcs(c + 11 * n, v.l.z);
 }
 
 __device__ __forceinline__ void load_ck(const AdjArgs& A, int64_t s, int64_t i, CPos& p, CV& v) {
     const int64_t n = A.a.n;
-    const float* c = A.ckpt + s * kCk * n + i;
+    const float* c = A.ckpt + s * kAdjCkWords * n + i;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        p.hi[k] = c[(0 + k) * n];
-        p.lo[k] = c[(3 + k) * n];
-        p.w[k] = __float_as_int(c[(6 + k) * n]);
+        p.hi[k] = __ldcs(c + (0 + k) * n);
+        p.lo[k] = __ldcs(c + (3 + k) * n);
+        p.w[k] = 0;
     }
-    v.h = {c[9 * n], c[10 * n], c[11 * n]};
-    v.l = {c[12 * n], c[13 * n], c[14 * n]};
+    v.h = {__ldcs(c + 6 * n), __ldcs(c + 7 * n), __ldcs(c + 8 * n)};
+    v.l = {__ldcs(c + 9 * n), __ldcs(c + 10 * n), __ldcs(c + 11 * n)};
 }
 
 __device__ __forceinline__ void store_rec(const AdjArgs& A, int j, int64_t i, const CPos& p, F3 v) {
@@ -116,11 +119,17 @@ struct UAdj {
     F3 lv, lE, lB;
 };
 
-__device__ __forceinline__ UAdj u_adjoint(F3 v, F3 E, F3 B, float h, F3 lo) {
+// vm = v + hE, the update's half-accelerated velocity
+__device__ __forceinline__ F3 vminus(F3 v, F3 E, float h) {
+    F3 he = h * E;
+    return v + he;
+}
+
+// The adjoint depends on v and E only through vm (lE = h (2 lo + lvm) holds
+// for any E), so records of the fused backward keep vm instead of both.
+__device__ __forceinline__ UAdj u_adjoint_vm(F3 vm, F3 B, float h, F3 lo) {
     F3 t = h * B;
     float sc = 2.0f * __frcp_rn(1.0f + dot(t, t));
-    F3 he = h * E;
-    F3 vm = v + he;
     F3 vp = vm + cross(vm, t);
     F3 s = sc * t;
     F3 ls = cross(lo, vp);
@@ -132,6 +141,10 @@ __device__ __forceinline__ UAdj u_adjoint(F3 v, F3 E, F3 B, float h, F3 lo) {
     r.lE = h * ((2.0f * lo) + lvm);
     r.lB = h * lt;
     return r;
+}
+
+__device__ __forceinline__ UAdj u_adjoint(F3 v, F3 E, F3 B, float h, F3 lo) {
+    return u_adjoint_vm(vminus(v, E, h), B, h, lo);
 }
 
 // ------------------------------------------------------- trilinear stencil
@@ -760,7 +773,7 @@ __device__ __forceinline__ int seg_steps(const AdjArgs& A, int64_t s) {
     return (int)((A.nt - k0 < A.K) ? A.nt - k0 : A.K);
 }
 
-__global__ void __launch_bounds__(128, 5) k_adj_recompute_eb(AdjArgs A, int64_t s) {
+__global__ void __launch_bounds__(128, 4) k_adj_recompute_eb(AdjArgs A, int64_t s) {
     const BorisArgs& a = A.a;
     const double dt = a.dt;
     const float dth = (float)dt, dtl = (float)(dt - (double)dth);
@@ -898,6 +911,179 @@ __global__ void __launch_bounds__(128, 4) k_adj_reverse_eb(AdjArgs A, int64_t s)
     }
 }
 
+// ------------------------------------- fused backward, E/B grid, short segments
+// With checkpoint segments of at most kFusedMaxK steps the whole backward
+// pass is one kernel.  Each thread walks its particle's segments from last to
+// first: it recomputes the segment from its checkpoint into its own records
+// in shared memory, then runs them backwards through the adjoint step and
+// the warp-transposed scatter.  Records never reach global memory and the
+// cotangent stays in registers from the final save to x_0, so per
+// particle-step the pass moves the field gather (8 sectors), the node
+// reductions (about 8.1 sectors) and 1/K of a 48-byte checkpoint, against
+// the two-kernel pass's additional record write and read (4.5 sectors each).
+// The records take K x 120 bytes of shared memory per thread, which the SM
+// takes from its L1 cache: K = 2 (3 blocks of 128 threads, L1 left at about
+// half) is the fastest; at K = 4 the L1 cache shrinks to 28 KB and the pass
+// is slower than the two kernels per segment.
+//
+// Record of one step, 15 float2 words, [slot][word][thread] in shared memory:
+//   0: cell x, y (int; x = -1 outside the grid)   1: cell z, fraction x
+//   2: fraction y, z   3: vm x, y   4: vm z, B x   5: B y, z
+//   6-14: dE/dx, dE/dy, dE/dz, dB/dx, dB/dy, dB/dz (9 + 9 floats in order)
+// (vm = v + hE; the adjoint needs no more)
+constexpr int kRecF2 = 15;
+
+__device__ __forceinline__ void record_step_f(const DevFields& F, const CPos& p, F3 v, float h, float2* r,
+                                              int stride, F3& E, F3& B) {
+    AxF ax, ay, az;
+    if (!axes32(F.B, p, ax, ay, az)) {
+        E = nanf3_();
+        B = E;
+        r[0] = make_float2(__int_as_float(-1), 0.0f);
+        return;
+    }
+    int nd[8];
+    tri_nodes(F.B, ax, ay, az, nd);
+    float4 e[8], b[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ldg_node8(F.eb32 + 2 * (int64_t)nd[c], e[c], b[c]);
+    F3 Ex, Ey, Ez, Bx, By, Bz;
+    tri_val_jac(e, ax, ay, az, E, Ex, Ey, Ez);
+    tri_val_jac(b, ax, ay, az, B, Bx, By, Bz);
+    const F3 vm = vminus(v, E, h);
+    r[0] = make_float2(__int_as_float(ax.i0), __int_as_float(ay.i0));
+    r[stride] = make_float2(__int_as_float(az.i0), ax.f);
+    r[2 * stride] = make_float2(ay.f, az.f);
+    r[3 * stride] = make_float2(vm.x, vm.y);
+    r[4 * stride] = make_float2(vm.z, B.x);
+    r[5 * stride] = make_float2(B.y, B.z);
+    r[6 * stride] = make_float2(Ex.x, Ex.y);
+    r[7 * stride] = make_float2(Ex.z, Ey.x);
+    r[8 * stride] = make_float2(Ey.y, Ey.z);
+    r[9 * stride] = make_float2(Ez.x, Ez.y);
+    r[10 * stride] = make_float2(Ez.z, Bx.x);
+    r[11 * stride] = make_float2(Bx.y, Bx.z);
+    r[12 * stride] = make_float2(By.x, By.y);
+    r[13 * stride] = make_float2(By.z, Bz.x);
+    r[14 * stride] = make_float2(Bz.y, Bz.z);
+}
+
+// reverse_step_eb for a shared-memory record of record_step_f
+__device__ __forceinline__ F3 reverse_step_f(const float2* r, int stride, float h, F3 lo, F3& lx, Frame& fr,
+                                             Contrib& ct) {
+    ct.i0[0] = -1;
+    float2 q[kRecF2];
+#pragma unroll
+    for (int k = 0; k < kRecF2; ++k) q[k] = r[k * stride];
+    const float2 q0 = q[0];
+    if (__float_as_int(q0.x) < 0) {
+        lx = nanf3_();
+        return nanf3_();
+    }
+    const F3 vm{q[3].x, q[3].y, q[4].x}, B{q[4].y, q[5].x, q[5].y};
+    UAdj u = u_adjoint_vm(vm, B, h, lo);
+    lx = lx + jt({q[6].x, q[6].y, q[7].x}, {q[7].y, q[8].x, q[8].y}, {q[9].x, q[9].y, q[10].x}, u.lE) +
+         jt({q[10].y, q[11].x, q[11].y}, {q[12].x, q[12].y, q[13].x}, {q[13].y, q[14].x, q[14].y}, u.lB);
+    if (fr.f != 0.0f) {
+        float m = fmaxf(fmaxf(fmaxf(fabsf(u.lE.x), fabsf(u.lE.y)), fmaxf(fabsf(u.lE.z), fabsf(u.lB.x))),
+                        fmaxf(fabsf(u.lB.y), fabsf(u.lB.z)));
+        fr.mx = max(fr.mx, fexp(m) + fr.e);
+        ct.i0[0] = __float_as_int(q0.x);
+        ct.i0[1] = __float_as_int(q0.y);
+        ct.i0[2] = __float_as_int(q[1].x);
+        ct.f[0] = q[1].y;
+        ct.f[1] = q[2].x;
+        ct.f[2] = q[2].y;
+        ct.lE = fr.f * u.lE;
+        ct.lB = fr.f * u.lB;
+    }
+    return u.lv;
+}
+
+// The particle loop is uniform over the block (lanes past n run empty, with
+// the same segment and step counts) so that whole warps take part in
+// scatter_warp_eb.  No block-level synchronisation: each thread reads only
+// the records it wrote.
+__global__ void __launch_bounds__(128, 3) k_adj_fused_eb(AdjArgs A) {
+    extern __shared__ float4 smem4[];  // records [K][kRecF2][blockDim.x] (float2), then staging
+    float2* mine = reinterpret_cast<float2*>(smem4) + threadIdx.x;
+    const int stride = blockDim.x;
+    float* stage = reinterpret_cast<float*>(reinterpret_cast<float2*>(smem4) + (int64_t)A.K * kRecF2 * stride) +
+                   (threadIdx.x & ~31) * kStage;
+    const BorisArgs& a = A.a;
+    const double dt = a.dt;
+    const float dtf = (float)dt, dth = dtf, dtl = (float)(dt - (double)dth);
+    const float h = vfac<false>(a, dt);
+    const int G = A.G;
+    const int64_t n = a.n;
+    const uint64_t keep = l2_evict_last();
+    int mx = INT_MIN;
+    for (int64_t ib = (int64_t)blockIdx.x * blockDim.x; ib < n; ib += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = ib + threadIdx.x;
+        const bool live = i < n;
+        F3 lx{0.0f, 0.0f, 0.0f}, lv{0.0f, 0.0f, 0.0f};
+        Frame fr;
+        fr.e = 0;
+        fr.mx = INT_MIN;
+        if (live) {
+            // cotangent of the final save, normalised: lambda = g / 2^e
+            const double* gf = A.g_final + 6 * i;
+            double gm = fmax(fmax(fmax(fabs(gf[0]), fabs(gf[1])), fmax(fabs(gf[2]), fabs(gf[3]))),
+                             fmax(fabs(gf[4]), fabs(gf[5])));
+            fr.e = (gm > 0.0 && gm <= 1.0e300) ? ilogb(gm) : 0;
+            const double is = ldexp(1.0, -fr.e);
+            lx = {(float)(gf[0] * is), (float)(gf[1] * is), (float)(gf[2] * is)};
+            lv = {(float)(gf[3] * is), (float)(gf[4] * is), (float)(gf[5] * is)};
+        }
+        frame_set(fr, G);
+        for (int64_t s = A.S - 1; s >= 0; --s) {
+            const int m = seg_steps(A, s);
+            if (live) {
+                CPos p;
+                CV v;
+                load_ck(A, s, i, p, v);
+                for (int j = 0; j < m; ++j) {
+                    F3 E, B;
+                    record_step_f(a.f, p, v.h, h, mine + j * kRecF2 * stride, stride, E, B);
+                    v = vel32h<false>(v, E, B, a, h);
+                    cpos_push_cv(a, p, v, dth, dtl);
+                }
+                if (s == A.S - 1) {  // the final save's update, at (x_N, v_{N-1/2})
+                    lv = adj_step_eb(A, p, v.h, vfac<false>(a, A.dt_final), lv, lx, fr);
+                    renorm(lx, lv, fr, G);
+                }
+            }
+            for (int j = m - 1; j >= 0; --j) {
+                Contrib ct;
+                ct.i0[0] = -1;
+                if (live) {
+                    F3 lo = lv + dtf * lx;
+                    lv = reverse_step_f(mine + j * kRecF2 * stride, stride, h, lo, lx, fr, ct);
+                    renorm(lx, lv, fr, G);
+                }
+                scatter_warp_eb(A, stage, ct, keep);
+            }
+        }
+        if (!live) continue;
+        // initial half step back, v_{-1/2} = U(v_0, x_0, -dt/2)
+        const double* u0 = a.u0 + 6 * i;
+        CPos p0;
+        cpos_init(a, p0, u0);
+        CV v0 = cv_from(u0 + 3);
+        lv = adj_step_eb(A, p0, v0.h, vfac<false>(a, -0.5 * dt), lv, lx, fr);
+        double* go = A.g_u0 + 6 * i;
+        go[0] = fr.s * lx.x;
+        go[1] = fr.s * lx.y;
+        go[2] = fr.s * lx.z;
+        go[3] = fr.s * lv.x;
+        go[4] = fr.s * lv.y;
+        go[5] = fr.s * lv.z;
+        mx = max(mx, fr.mx);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0 && mx != INT_MIN) atomicMax(A.need, mx);
+}
+
 // sum of a node-gradient table (stored scaled by 2^-G) into out[0..2]
 __global__ void k_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out) {
     double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -950,7 +1136,21 @@ cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c,
     return cudaLaunchKernel(k, dim3(c.grid), dim3(c.block), args, 0, s);
 }
 
+// shared memory of k_adj_fused_eb for a block of `block` threads
+size_t fused_smem(int64_t K, int block) {
+    return (size_t)K * kRecF2 * block * sizeof(float2) + (size_t)kStage * block * sizeof(float);
+}
+
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s) {
+    if (fk == FK_EBGRID && adjoint_fused(fk, a.K)) {  // one kernel for the whole pass
+        const int block = c.block < 128 ? (c.block < 32 ? 32 : c.block & ~31) : 128;
+        const size_t smem = fused_smem(a.K, block);
+        cudaError_t e = cudaFuncSetAttribute(k_adj_fused_eb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int64_t g = (a.a.n + block - 1) / block;
+        k_adj_fused_eb<<<(unsigned)(g < 0x7fffffff ? g : 0x7fffffff), block, smem, s>>>(a);
+        return cudaGetLastError();
+    }
     if (fk == FK_EBGRID) {  // two kernels per segment, last segment first
         const size_t smem = (size_t)kRevStages * kRecEB4 * c.block * sizeof(float4) +
                             (size_t)kStage * c.block * sizeof(float);
@@ -971,9 +1171,13 @@ cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c
 // float words of the per-step records of one segment and of the cotangent
 // state kept between segments
 int64_t adjoint_record_words(int fk, int64_t K, int64_t n) {
+    if (adjoint_fused(fk, K)) return 0;
     return fk == FK_EBGRID ? (K + 1) * kRecEB4 * 4 * n : K * kRec * n;
 }
-int64_t adjoint_state_words(int fk, int64_t n) { return fk == FK_EBGRID ? 8 * n : 0; }
+int64_t adjoint_state_words(int fk, int64_t K, int64_t n) {
+    return fk == FK_EBGRID && !adjoint_fused(fk, K) ? 8 * n : 0;
+}
+bool adjoint_fused(int fk, int64_t K) { return fk == FK_EBGRID && K <= kFusedMaxK; }
 
 cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,
                              cudaStream_t s) {

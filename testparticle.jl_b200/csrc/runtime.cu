@@ -2214,7 +2214,7 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
         return fail(ctx, TP_E_UNSUPPORTED, "the adjoint covers trilinear uniform Cartesian grids");
     if (E->desc.kind == TP_FIELD_QUADRATIC || B->desc.kind == TP_FIELD_QUADRATIC)
         return fail(ctx, TP_E_UNSUPPORTED, "the adjoint does not cover quadratic fields");
-    if (d->checkpoint_every < 1) return fail(ctx, TP_E_ARG, "checkpoint_every must be >= 1");
+    if (d->checkpoint_every < 0) return fail(ctx, TP_E_ARG, "checkpoint_every must be >= 0 (0: automatic)");
     if (n < 0) return fail(ctx, TP_E_ARG, "negative particle count");
     if (E->ctx != ctx || B->ctx != ctx) return fail(ctx, TP_E_ARG, "fields belong to another context");
     double dt = r->dt;
@@ -2238,11 +2238,22 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
     }
     A.a.n = n;
     A.nt = nt;
-    A.K = d->checkpoint_every < nt ? d->checkpoint_every : (nt > 0 ? nt : 1);
+    t->fk = adjoint_field_config(A.a.f);
+    int64_t K = d->checkpoint_every;
+    if (K == 0) {
+        // Automatic: an interleaved E/B grid takes 2-step segments (the
+        // one-kernel backward) when their checkpoints fit in half of the free
+        // device memory, else 64-step segments; other fields take 64.
+        K = 64;
+        size_t free_b = 0, total_b = 0;
+        if (t->fk == FK_EBGRID && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+            (double)((nt + 1) / 2 + 1) * kAdjCkWords * 4.0 * (double)n <= 0.5 * (double)free_b)
+            K = 2;
+    }
+    A.K = K < nt ? K : (nt > 0 ? nt : 1);
     A.S = nt > 0 ? (nt + A.K - 1) / A.K : 1;
     // final save of _boris_loop! at it = nt: t_final = t1, dt_final = t1 - (t0 + (nt - 1/2) dt)
     A.dt_final = r->t1 - std::fma((double)nt - 0.5, dt, r->t0);
-    t->fk = adjoint_field_config(A.a.f);
     t->nodes_E = E->nodes;
     t->nodes_B = B->nodes;
     // blocks of at most 128 threads (the segment kernels' launch bounds)
@@ -2253,7 +2264,7 @@ int adjoint_prepare(tp_ctx* ctx, const tp_adj_desc* d, const tp_field* E, const 
     }
     cudaError_t e = cudaSuccess;
     if (n > 0) {
-        e = tape_alloc(t, &t->d_ckpt, (size_t)A.S * 15 * (size_t)n * sizeof(float));
+        e = tape_alloc(t, &t->d_ckpt, (size_t)A.S * kAdjCkWords * (size_t)n * sizeof(float));
         if (e == cudaSuccess) e = tape_alloc(t, &t->d_u0, (size_t)n * 6 * sizeof(double));
     }
     if (e == cudaSuccess) e = tape_alloc(t, &t->d_gparam, 6 * sizeof(double));
@@ -2290,9 +2301,9 @@ int adjoint_backward_on(tp_tape* t, const double* gfinal_dev, double* gu0_dev, d
     const int64_t n = A.a.n;
     cudaError_t e = cudaSuccess;
     // segment records and node-gradient tables: allocated on first use, kept
-    if (!t->d_rec && n > 0)
-        e = tape_alloc(t, &t->d_rec, (size_t)adjoint_record_words(t->fk, A.K, n) * sizeof(float));
-    const int64_t sw = adjoint_state_words(t->fk, n);
+    const int64_t rw = adjoint_record_words(t->fk, A.K, n);
+    if (!t->d_rec && rw > 0) e = tape_alloc(t, &t->d_rec, (size_t)rw * sizeof(float));
+    const int64_t sw = adjoint_state_words(t->fk, A.K, n);
     if (e == cudaSuccess && sw > 0 && !t->d_lam) e = tape_alloc(t, &t->d_lam, (size_t)sw * sizeof(float));
     const bool eb = t->fk == FK_EBGRID;
     const bool gridE = !eb && t->E->desc.kind == TP_FIELD_GRID;
@@ -2468,6 +2479,13 @@ int tp_tape_info(const tp_tape* t, int64_t* device_bytes, int64_t* nsteps) {
     if (!t) return TP_E_ARG;
     if (device_bytes) *device_bytes = t->bytes;
     if (nsteps) *nsteps = t->A.nt;
+    return TP_OK;
+}
+
+int tp_tape_segments(const tp_tape* t, int64_t* checkpoint_every, int64_t* segments) {
+    if (!t) return TP_E_ARG;
+    if (checkpoint_every) *checkpoint_every = t->A.K;
+    if (segments) *segments = t->A.S;
     return TP_OK;
 }
 

@@ -118,13 +118,15 @@ struct PointsArgs {
 };
 
 // discrete adjoint of the fixed-step Boris map (adjoint.cu)
+constexpr int kAdjCkWords = 12;  // checkpoint words per particle
+
 struct AdjArgs {
     BorisArgs a;           // fields, q2m, t0, dt, FP32C wrap data, n, u0 (device, n x 6)
     int64_t nt;            // steps N
     int64_t K;             // steps per checkpoint segment
     int64_t S;             // checkpoints: max(1, ceil(N / K))
     double dt_final;       // dt of the final save's half update
-    float* ckpt;           // [S][15][n]: hi xyz, lo xyz, wrap xyz (int bits), v.h xyz, v.l xyz
+    float* ckpt;           // [S][kAdjCkWords][n]: hi xyz, lo xyz, v.h xyz, v.l xyz
     double* u_final;       // n x 6
     const double* g_final; // n x 6: dL/d(x_N, v_N)
     double* g_u0;          // n x 6
@@ -144,7 +146,11 @@ int adjoint_field_config(const DevFields& f);
 cudaError_t launch_adjoint_forward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_adjoint_backward(const AdjArgs& a, int fk, const LaunchCfg& c, cudaStream_t s);
 int64_t adjoint_record_words(int fk, int64_t K, int64_t n);
-int64_t adjoint_state_words(int fk, int64_t n);
+int64_t adjoint_state_words(int fk, int64_t K, int64_t n);
+// E/B-grid segments of at most kFusedMaxK steps run the one-kernel backward
+// (records in shared memory); longer ones the two kernels per segment
+constexpr int64_t kFusedMaxK = 8;
+bool adjoint_fused(int fk, int64_t K);
 // sum of a node-gradient table (values times 2^-G) into out[0..2] (+=),
 // entries k*stride + off
 cudaError_t launch_table_sum(const float4* tab, int64_t nodes, int stride, int off, int G, double* out,

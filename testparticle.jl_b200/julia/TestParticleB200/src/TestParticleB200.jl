@@ -484,7 +484,7 @@ function release!(t::AdjointTape)
     return nothing
 end
 
-function adjoint_forward(U0::Matrix{Float64}, E, B; q2m, m = 1.0, dt, tspan, checkpoint_every = 64, device = 0)
+function adjoint_forward(U0::Matrix{Float64}, E, B; q2m, m = 1.0, dt, tspan, checkpoint_every = 0, device = 0)
     size(U0, 1) == 6 || throw(ArgumentError("U0 must be a (6, N) matrix"))
     ctx = context(device)
     hE = field_handle(ctx, unwrap(E)); hB = field_handle(ctx, unwrap(B))
@@ -504,7 +504,7 @@ function adjoint_forward(U0::Matrix{Float64}, E, B; q2m, m = 1.0, dt, tspan, che
 end
 
 """
-    boris_final_state(U0, E, B; q2m, m, dt, tspan, checkpoint_every = 64, device = 0)
+    boris_final_state(U0, E, B; q2m, m, dt, tspan, checkpoint_every = 0, device = 0)
 
 (6, N) final saves of `solve(TraceProblem(u0, tspan, (q2m, m, E, B, ...)), Boris(); dt)` for the
 columns of `U0`, in the FP32C arithmetic of `EnsembleB200(; precision = :fp32c)`.  Differentiable

@@ -424,6 +424,12 @@ class Tape:
         self.ctx.lib.tp_tape_info(self.handle, C.byref(b), C.byref(s))
         return b.value, s.value
 
+    def segments(self) -> tuple[int, int]:
+        """(steps per checkpoint segment, segments): the automatic choice resolved."""
+        k, s = C.c_int64(), C.c_int64()
+        self.ctx.lib.tp_tape_segments(self.handle, C.byref(k), C.byref(s))
+        return k.value, s.value
+
     def close(self) -> None:
         self._fin()
 

@@ -212,12 +212,15 @@ class AdjointPlan:
     device: int
 
 
-def plan_adjoint(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 64,
+def plan_adjoint(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 0,
                  maxiters=None) -> AdjointPlan:
     """Descriptor of the discrete adjoint of solve(prob, Boris(); dt) (final save, no saves in between).
 
     The adjoint runs in the FP32C arithmetic of EnsembleB200(precision="fp32c")
-    with static fields and no termination predicate.
+    with static fields and no termination predicate.  checkpoint_every = 0
+    lets the library choose the segment length: 2 steps for an interleaved
+    E/B grid when the tape (48 bytes per particle per segment) fits in half
+    of the free device memory, else 64.
     """
     ens = ens if ens is not None else EnsembleB200(precision="fp32c")
     if ens.precision != "fp32c":
@@ -230,7 +233,7 @@ def plan_adjoint(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every:
     return AdjointPlan(d, p.E, p.B, p.u0, p.device)
 
 
-def adjoint_solve(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 64, maxiters=None):
+def adjoint_solve(prob, ens=None, *, dt, trajectories: int = 1, checkpoint_every: int = 0, maxiters=None):
     """(final states (N, 6), Tape): tape.backward(dL/d final states) gives the gradients."""
     p = plan_adjoint(prob, ens, dt=dt, trajectories=trajectories, checkpoint_every=checkpoint_every,
                      maxiters=maxiters)

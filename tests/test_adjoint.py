@@ -216,17 +216,34 @@ def test_adjoint_smooth_fields_vs_central_differences(tp, orc):
 
 @pytest.mark.gpu
 def test_adjoint_independent_of_checkpoint_interval(tp):
-    w, prob = _grid_case(tp, n=64, nt=100)
+    """K <= 8 runs the one-kernel backward (records in shared memory), larger
+    K the two kernels per segment; 200 particles leave a partial warp and a
+    partial block."""
+    w, prob = _grid_case(tp, n=200, nt=100)
     rng = np.random.default_rng(6)
-    c = rng.normal(size=(64, 6)) * np.array([1e-7] * 3 + [1e-6] * 3)
+    c = rng.normal(size=(200, 6)) * np.array([1e-7] * 3 + [1e-6] * 3)
     res = []
-    for K in (1, 7, 64, 100, 1000):
+    for K in (1, 3, 4, 7, 8, 9, 64, 100, 1000):
         uf, tape = tp.adjoint_solve(prob, dt=w.dt, checkpoint_every=K)
         res.append((uf, tape.backward(c)))
     for uf, g in res[1:]:
         assert np.array_equal(uf, res[0][0])
         assert np.array_equal(g.u0, res[0][1].u0)  # recomputation is exact
         assert np.allclose(g.B, res[0][1].B, rtol=1e-5, atol=1e-6 * np.abs(res[0][1].B).max())
+
+
+@pytest.mark.gpu
+def test_adjoint_automatic_segments(tp):
+    """checkpoint_every = 0: 2-step segments (one-kernel backward) on the
+    interleaved E/B grid, 64 for analytic fields; explicit K is kept."""
+    w, prob = _grid_case(tp, n=64, nt=100)
+    _, tape = tp.adjoint_solve(prob, dt=w.dt)
+    assert tape.segments() == (2, 50)
+    _, tape = tp.adjoint_solve(prob, dt=w.dt, checkpoint_every=7)
+    assert tape.segments() == (7, 15)
+    sprob, _, _, dt = _smooth_case(tp, n=16, nt=200)
+    _, tape = tp.adjoint_solve(sprob, dt=dt)
+    assert tape.segments() == (64, 4)
 
 
 @pytest.mark.gpu
@@ -259,7 +276,7 @@ def test_adjoint_argument_errors(tp):
     with pytest.raises(NotImplementedError):
         ctx.adjoint_forward(p.desc, p.E, p.B, p.u0)
     p = tp.plan_adjoint(prob, dt=w.dt)
-    p.desc.checkpoint_every = 0
+    p.desc.checkpoint_every = -1
     with pytest.raises(tp.ArgumentError):
         ctx.adjoint_forward(p.desc, p.E, p.B, p.u0)
 
@@ -306,12 +323,13 @@ def test_adjoint_chaotic_range(tp):
     rng = np.random.default_rng(8)
     c = rng.normal(size=(64, 6)) * np.array([1e-7] * 3 + [1e-6] * 3)
     out = []
-    for K in (64, 512):
+    for K in (4, 64, 512):
         _, tape = tp.adjoint_solve(prob, dt=w.dt, checkpoint_every=K)
         out.append(tape.backward(c))
     g = out[0]
     for a in (g.u0, g.E, g.B, g.param):
         assert np.all(np.isfinite(a))
     assert np.abs(g.u0[:, :3]).max() > 1e10  # the growth is real
-    assert np.array_equal(g.u0, out[1].u0)
-    assert np.allclose(g.B, out[1].B, rtol=1e-4, atol=1e-6 * np.abs(g.B).max())
+    for o in out[1:]:
+        assert np.array_equal(g.u0, o.u0)
+        assert np.allclose(g.B, o.B, rtol=1e-4, atol=1e-6 * np.abs(g.B).max())
