@@ -268,6 +268,70 @@ int64_t nout_h(int64_t nt, int64_t ssi, bool ss, bool se, bool sev) {
     return nout;
 }
 
+// Per-particle step counts of a fixed-step solve: the save slots needed (the
+// largest nout over particles) and the first particle that breaks the
+// reference's argument checks (boris.jl:349-356), in index order: dt below
+// 10 eps (bad = 1) or |nt| above maxiters (bad = 2, nt reported).  Large
+// ensembles are scanned by several host threads; the result is the serial
+// loop's.
+struct StepScan {
+    int64_t nslots = 0;
+    int64_t bad_index = -1;
+    int bad = 0;
+    int64_t bad_nt = 0;
+};
+
+StepScan scan_steps(const tp_run_desc* d, const double* dt_i, const double* tend_i, int64_t n) {
+    const bool per = (dt_i || tend_i) && n > 0;
+    const int64_t m = per ? n : 1;
+    auto part = [&](int64_t a, int64_t b, StepScan& r) {
+        for (int64_t i = a; i < b; ++i) {
+            const double dt = (dt_i && n > 0) ? dt_i[i] : d->dt;
+            const double t1 = (tend_i && n > 0) ? tend_i[i] : d->t1;
+            if (std::fabs(dt) < 10.0 * kEps) {
+                r.bad_index = i;
+                r.bad = 1;
+                return;
+            }
+            int64_t nt = jl_round_h((t1 - d->t0) / dt);
+            if (nt < 0) nt = -nt;
+            if (nt > d->maxiters) {
+                r.bad_index = i;
+                r.bad = 2;
+                r.bad_nt = nt;
+                return;
+            }
+            r.nslots = std::max(r.nslots, nout_h(nt, d->savestepinterval, d->save_start, d->save_end,
+                                                 d->save_everystep));
+        }
+    };
+    const int64_t per_thread = 1 << 16;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nth = (int)std::min<int64_t>(std::max(1u, std::min(hw, 32u)), (m + per_thread - 1) / per_thread);
+    if (nth <= 1) {
+        StepScan r;
+        part(0, m, r);
+        return r;
+    }
+    std::vector<StepScan> rs(nth);
+    std::vector<std::thread> th;
+    const int64_t slice = (m + nth - 1) / nth;
+    for (int k = 0; k < nth; ++k)
+        th.emplace_back(part, std::min(m, k * slice), std::min(m, (k + 1) * slice), std::ref(rs[k]));
+    for (auto& t : th) t.join();
+    StepScan r;
+    for (const StepScan& q : rs) {  // slices in index order: the first bad one is the serial loop's
+        if (q.bad) {
+            r.bad_index = q.bad_index;
+            r.bad = q.bad;
+            r.bad_nt = q.bad_nt;
+            return r;
+        }
+        r.nslots = std::max(r.nslots, q.nslots);
+    }
+    return r;
+}
+
 void fill_float_copies(DevField& d) {
     for (int a = 0; a < 3; ++a) {
         d.vf[a] = (float)d.v[a];
@@ -792,19 +856,9 @@ int tp_boris_slots(const tp_run_desc* d, const double* dt_i, const double* tend_
         *nslots = s;
         return TP_OK;
     }
-    int64_t best = 0;
-    for (int64_t i = 0; i < std::max<int64_t>(n, 1); ++i) {
-        double dt = (dt_i && n > 0) ? dt_i[i] : d->dt;
-        double t1 = (tend_i && n > 0) ? tend_i[i] : d->t1;
-        if (std::fabs(dt) < 10.0 * kEps) return TP_E_ARG;
-        int64_t nt = jl_round_h((t1 - d->t0) / dt);
-        if (nt < 0) nt = -nt;
-        if (nt > d->maxiters) return TP_E_ARG;
-        best = std::max(best, nout_h(nt, d->savestepinterval, d->save_start, d->save_end,
-                                     d->save_everystep));
-        if (!dt_i && !tend_i) break;
-    }
-    *nslots = best;
+    const StepScan sc = scan_steps(d, dt_i, tend_i, n);
+    if (sc.bad) return TP_E_ARG;
+    *nslots = sc.nslots;
     return TP_OK;
 }
 
@@ -1325,24 +1379,22 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
     if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
     if (n < 0 || (n > 0 && !u0)) return fail(ctx, TP_E_ARG, "bad particle table");
     const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
-    // the reference's ArgumentErrors (boris.jl:349-356) before any tracing
-    if (!adaptive) {
-        for (int64_t i = 0; i < std::max<int64_t>(n, 1); ++i) {
-            double dt = (dt_i && n > 0) ? dt_i[i] : d->dt;
-            double t1 = (tend_i && n > 0) ? tend_i[i] : d->t1;
-            if (std::fabs(dt) < 10.0 * kEps)
-                return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
-            int64_t nt = jl_round_h((t1 - d->t0) / dt);
-            if (nt < 0) nt = -nt;
-            if (nt > d->maxiters)
-                return fail(ctx, TP_E_ARG, "number of iterations nt (" + std::to_string(nt) +
-                                               ") exceeds maxiters (" + std::to_string(d->maxiters) + ")");
-            if (!dt_i && !tend_i) break;
-        }
-    }
     int64_t nslots = 0;
-    st = tp_boris_slots(d, dt_i, tend_i, n, &nslots);
-    if (st != TP_OK) return fail(ctx, st, "cannot size the output");
+    if (!adaptive) {
+        // the reference's ArgumentErrors (boris.jl:349-356) before any tracing,
+        // in the same pass as the output sizing
+        if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "cannot size the output");
+        const StepScan sc = scan_steps(d, dt_i, tend_i, n);
+        if (sc.bad == 1)
+            return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
+        if (sc.bad == 2)
+            return fail(ctx, TP_E_ARG, "number of iterations nt (" + std::to_string(sc.bad_nt) +
+                                           ") exceeds maxiters (" + std::to_string(d->maxiters) + ")");
+        nslots = sc.nslots;
+    } else {
+        st = tp_boris_slots(d, dt_i, tend_i, n, &nslots);
+        if (st != TP_OK) return fail(ctx, st, "cannot size the output");
+    }
     if (nslots < 0) nslots = 64;  // adaptive without a cap: grown on overflow below
     const int W = 6 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
     DeviceGuard g(ctx->device);
