@@ -405,6 +405,30 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
                  const tp_field* B, const double* u0, const double* dt_i,
                  const double* tend_i, int64_t n, tp_result** out);
 
+/* The same solve from host arrays into host arrays in one call: the results
+ * of tp_boris_run followed by tp_result_copy, bit for bit.  One kernel runs
+ * the ensemble and counts finished particles per chunk of consecutive
+ * indices (up to 32 chunks of at least 32768 particles); the queue schedule
+ * hands particles out in index order, so chunks finish while the kernel
+ * still runs, and each finished chunk is copied to pinned memory and packed
+ * into the caller's buffers by host threads meanwhile.  The context keeps
+ * the pinned staging (one chunk, at most 256 MB) between calls.
+ *   cap_rows        rows t_packed and u_packed can hold (n * slots from
+ *                   tp_boris_slots always suffices; fewer fails with
+ *                   TP_E_ARG once the saves exceed them)
+ *   nsaved, retcode, nsteps   n values each
+ *   t_packed, u_packed        packed saves as tp_result_copy writes them
+ *   total           rows written;  elapsed_ms  device time of the push
+ *                   (may be NULL)
+ * Runs whose save count is unknown in advance (adaptive without step_cap)
+ * return TP_E_UNSUPPORTED: use tp_boris_run.                                */
+int tp_boris_run_host(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
+                      const tp_field* B, const double* u0, const double* dt_i,
+                      const double* tend_i, int64_t n, int64_t cap_rows,
+                      int32_t* nsaved, int8_t* retcode, int64_t* nsteps,
+                      double* t_packed, double* u_packed, int64_t* total,
+                      double* elapsed_ms);
+
 /* Number of save slots per particle that a run needs (host arrays). */
 int tp_boris_slots(const tp_run_desc* desc, const double* dt_i,
                    const double* tend_i, int64_t n, int64_t* nslots);

@@ -268,6 +268,9 @@ SIGNATURES = [
     ("tp_field_destroy", None, [_P]),
     ("tp_boris_run", C.c_int, [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.POINTER(_P)]),
     ("tp_boris_slots", C.c_int, [C.POINTER(RunDesc), _P, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    ("tp_boris_run_host", C.c_int,
+     [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P,
+      C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     ("tp_boris_run_device", C.c_int,
      [_P, C.POINTER(RunDesc), _P, _P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
     ("tp_gc_run", C.c_int, [_P, C.POINTER(GCDesc), _P, _P, _P, _P, _P, _P, _P, _P, C.c_int64, C.POINTER(_P)]),

@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
                 a.nsaved[i] = 0;
                 a.retcode[i] = TP_RET_DEFAULT;
                 a.nsteps[i] = 0;
+                particle_done(a, i);
                 i = -1;
                 continue;
             }
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
             a.nsaved[i] = (int32_t)iout;
             a.retcode[i] = (int8_t)((iout < nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
             a.nsteps[i] = final_step;
+            particle_done(a, i);
             i = -1;
         }
     }
@@ -299,6 +301,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed32c_slots(BorisA
                     a.nsaved[ii] = 0;
                     a.retcode[ii] = TP_RET_DEFAULT;
                     a.nsteps[ii] = 0;
+                    particle_done(a, ii);
                     i[k] = -1;
                     continue;
                 }
@@ -407,6 +410,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed32c_slots(BorisA
                 a.nsaved[ii] = (int32_t)iout[k];
                 a.retcode[ii] = (int8_t)((iout[k] < nout[k]) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
                 a.nsteps[ii] = final_step;
+                particle_done(a, ii);
                 i[k] = -1;
             }
         }
@@ -633,6 +637,7 @@ __global__ void __launch_bounds__(128, 5) k_cubic32c(BorisArgs a) {
             a.nsaved[i] = 0;
             a.retcode[i] = TP_RET_DEFAULT;
             a.nsteps[i] = 0;
+            particle_done(a, i);
             active = false;
         }
     }
@@ -723,6 +728,7 @@ __global__ void __launch_bounds__(128, 5) k_cubic32c(BorisArgs a) {
             a.nsaved[i] = (int32_t)iout;
             a.retcode[i] = (int8_t)((iout < nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
             a.nsteps[i] = final_step;
+            particle_done(a, i);
             finishing = false;
         }
         if (!__any_sync(0xffffffffu, stepping)) break;
@@ -847,6 +853,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
             a.nsaved[i] = (int32_t)iout;
             a.retcode[i] = (int8_t)ret;
             a.nsteps[i] = steps;
+            particle_done(a, i);
             i = -1;
         }
     }

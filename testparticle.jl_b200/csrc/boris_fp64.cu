@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
                 a.nsaved[i] = 0;
                 a.retcode[i] = TP_RET_DEFAULT;
                 a.nsteps[i] = 0;
+                particle_done(a, i);
                 i = -1;
                 continue;
             }
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
                 a.nsaved[i] = 0;
                 a.retcode[i] = TP_RET_DEFAULT;
                 a.nsteps[i] = 0;
+                particle_done(a, i);
                 i = -1;
                 continue;
             }
@@ -186,6 +188,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
             a.nsaved[i] = (int32_t)iout;
             a.retcode[i] = (int8_t)((iout < nout) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
             a.nsteps[i] = final_step;
+            particle_done(a, i);
             i = -1;
         }
     }
@@ -241,6 +244,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed64_slots(BorisAr
                     a.nsaved[ii] = 0;
                     a.retcode[ii] = TP_RET_DEFAULT;
                     a.nsteps[ii] = 0;
+                    particle_done(a, ii);
                     i[k] = -1;
                     continue;
                 }
@@ -251,6 +255,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed64_slots(BorisAr
                     a.nsaved[ii] = 0;
                     a.retcode[ii] = TP_RET_DEFAULT;
                     a.nsteps[ii] = 0;
+                    particle_done(a, ii);
                     i[k] = -1;
                     continue;
                 }
@@ -342,6 +347,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed64_slots(BorisAr
                 a.nsaved[ii] = (int32_t)iout[k];
                 a.retcode[ii] = (int8_t)((iout[k] < nout[k]) ? TP_RET_TERMINATED : TP_RET_SUCCESS);
                 a.nsteps[ii] = final_step;
+                particle_done(a, ii);
                 i[k] = -1;
             }
         }
@@ -454,6 +460,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive64(BorisArgs a) {
             a.nsaved[i] = (int32_t)iout;
             a.retcode[i] = (int8_t)ret;
             a.nsteps[i] = steps;
+            particle_done(a, i);
             i = -1;
         }
     }

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -41,6 +42,15 @@ struct tp_ctx {
     // pinned staging for host <-> device transfers of pageable buffers
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+    // tp_boris_run_host, created on first use and kept: pinned staging of
+    // one chunk's slot-major results, the chunk counts' pinned mirror, the
+    // copy stream and the two timing events
+    void* chunk_pin = nullptr;
+    size_t chunk_pin_bytes = 0;
+    int32_t* done_pin = nullptr;
+    int64_t done_cap = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t run_ev[2] = {nullptr, nullptr};
 };
 
 struct tp_field {
@@ -197,9 +207,8 @@ bool is_pageable(const void* p) {
     return at.type == cudaMemoryTypeUnregistered;
 }
 
-// device -> host (dst may be pageable); synchronous on return
-cudaError_t copy_to_host(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
-    cudaStream_t s = ctx->stream;
+// device -> host (dst may be pageable) on stream s; synchronous on return
+cudaError_t copy_to_host_on(tp_ctx* ctx, cudaStream_t s, void* dst, const void* src, size_t bytes) {
     if (bytes == 0) return cudaSuccess;
     if (bytes < ((size_t)4 << 20) || !is_pageable(dst)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
@@ -225,10 +234,14 @@ cudaError_t copy_to_host(tp_ctx* ctx, void* dst, const void* src, size_t bytes) 
     return cudaSuccess;
 }
 
-// host (possibly pageable) -> device; asynchronous on the context stream
-// after the staging of the last chunk
-cudaError_t copy_to_device(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
-    cudaStream_t s = ctx->stream;
+cudaError_t copy_to_host(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    return copy_to_host_on(ctx, ctx->stream, dst, src, bytes);
+}
+
+// host (possibly pageable) -> device on stream s; the call returns once the
+// staging buffers are free again (the stream is synchronised when they were
+// used)
+cudaError_t copy_to_device_on(tp_ctx* ctx, cudaStream_t s, void* dst, const void* src, size_t bytes) {
     if (bytes == 0) return cudaSuccess;
     if (bytes < ((size_t)4 << 20) || !is_pageable(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
     cudaError_t e = ensure_pinned(ctx);
@@ -247,6 +260,10 @@ cudaError_t copy_to_device(tp_ctx* ctx, void* dst, const void* src, size_t bytes
     }
     // the staging buffers are reused by the next transfer: finish this one
     return cudaStreamSynchronize(s);
+}
+
+cudaError_t copy_to_device(tp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    return copy_to_device_on(ctx, ctx->stream, dst, src, bytes);
 }
 
 const double kEps = 2.220446049250313e-16;
@@ -623,6 +640,11 @@ void tp_ctx_destroy(tp_ctx* ctx) {
         if (ctx->pin[k]) cudaFreeHost(ctx->pin[k]);
         if (ctx->pin_ev[k]) cudaEventDestroy(ctx->pin_ev[k]);
     }
+    if (ctx->chunk_pin) cudaFreeHost(ctx->chunk_pin);
+    if (ctx->done_pin) cudaFreeHost(ctx->done_pin);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    for (cudaEvent_t ev : ctx->run_ev)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1500,6 +1522,271 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_
     }
     delete r;
     return fail(ctx, TP_E_OVERFLOW, "save slots exceeded after resizing");
+}
+
+}  // extern "C"
+
+namespace {
+
+// One chunk's saves, slot-major in pinned memory (t: [nslots][m], u:
+// [nslots * W][m]), into the packed per-trajectory layout of tp_result_copy
+// starting at row 0 of t_dst / u_dst; counts clamped to [0, nslots] as the
+// device packing does.  Returns the rows written.  Host threads split the
+// particles; each walks blocks of 8 particles so that the strided reads
+// use whole cache lines.
+int64_t pack_chunk_host(const double* t_st, const double* u_st, const int32_t* ns, int64_t m, int64_t nslots,
+                        int W, double* t_dst, double* u_dst) {
+    std::vector<int64_t> off((size_t)m + 1);
+    off[0] = 0;
+    for (int64_t i = 0; i < m; ++i)
+        off[i + 1] = off[i] + std::min<int64_t>(std::max<int32_t>(ns[i], 0), nslots);
+    auto part = [&](int64_t a, int64_t b) {
+        for (int64_t i0 = a; i0 < b; i0 += 8) {
+            const int64_t i1 = std::min(b, i0 + 8);
+            for (int64_t s = 0; s < nslots; ++s) {
+                for (int64_t i = i0; i < i1; ++i)
+                    if (s < off[i + 1] - off[i]) t_dst[off[i] + s] = t_st[s * m + i];
+                for (int c = 0; c < W; ++c) {
+                    const double* src = u_st + (s * W + c) * m;
+                    for (int64_t i = i0; i < i1; ++i)
+                        if (s < off[i + 1] - off[i]) u_dst[(off[i] + s) * W + c] = src[i];
+                }
+            }
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nth = (int)std::min<int64_t>(std::max(1u, std::min(hw, 16u)), (m + 8191) / 8192);
+    if (nth <= 1) {
+        part(0, m);
+    } else {
+        std::vector<std::thread> th;
+        const int64_t slice = ((m + nth - 1) / nth + 7) & ~(int64_t)7;
+        for (int k = 0; k < nth; ++k) {
+            const int64_t a = std::min(m, k * slice), b = std::min(m, (k + 1) * slice);
+            if (a < b) th.emplace_back(part, a, b);
+        }
+        for (auto& t : th) t.join();
+    }
+    return off[m];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Host-to-host solve with the copy-out overlapped with the push.  One kernel
+// runs the whole ensemble; each particle, once its outputs are written,
+// counts itself in its chunk (BorisArgs::done).  The queue schedule hands out
+// particles in index order, so chunks finish one after another while the
+// kernel runs: the host polls the counts and copies each finished chunk's
+// slot-major results (two strided copies into pinned staging), then packs
+// them into the caller's arrays on host threads.
+int tp_boris_run_host(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, const tp_field* B,
+                      const double* u0, const double* dt_i, const double* tend_i, int64_t n, int64_t cap_rows,
+                      int32_t* nsaved, int8_t* retcode, int64_t* nsteps, double* t_packed, double* u_packed,
+                      int64_t* total, double* elapsed_ms) {
+    if (!ctx || !total) return TP_E_ARG;
+    *total = 0;
+    if (elapsed_ms) *elapsed_ms = 0.0;
+    int st = check_boris_desc(ctx, d);
+    if (st != TP_OK) return st;
+    if (!E || !B) return fail(ctx, TP_E_ARG, "null field");
+    if (n < 0 || (n > 0 && (!u0 || !nsaved || !retcode || !nsteps))) return fail(ctx, TP_E_ARG, "bad particle table");
+    if (cap_rows < 0 || (cap_rows > 0 && (!t_packed || !u_packed))) return fail(ctx, TP_E_ARG, "bad result buffers");
+    const bool adaptive = d->alg == TP_ALG_ADAPTIVE || d->alg == TP_ALG_ADAPTIVE_MULTISTEP;
+    int64_t nslots = 0;
+    if (!adaptive) {
+        // the reference's ArgumentErrors (boris.jl:349-356) before any tracing
+        if (d->savestepinterval < 1) return fail(ctx, TP_E_ARG, "cannot size the output");
+        const StepScan sc = scan_steps(d, dt_i, tend_i, n);
+        if (sc.bad == 1)
+            return fail(ctx, TP_E_ARG, "time step dt is too small, violating min_dt = 10 * eps(typeof(dt))");
+        if (sc.bad == 2)
+            return fail(ctx, TP_E_ARG, "number of iterations nt (" + std::to_string(sc.bad_nt) +
+                                           ") exceeds maxiters (" + std::to_string(d->maxiters) + ")");
+        nslots = sc.nslots;
+    } else {
+        st = tp_boris_slots(d, dt_i, tend_i, n, &nslots);
+        if (st != TP_OK) return fail(ctx, st, "cannot size the output");
+        if (nslots < 0)
+            return fail(ctx, TP_E_UNSUPPORTED, "adaptive run without step_cap: the save count is unknown (tp_boris_run)");
+    }
+    if (n == 0) return TP_OK;
+    const int W = 6 + (d->save_fields ? 6 : 0) + (d->save_work ? 4 : 0);
+    // chunks of at least 32768 particles, at most 32 of them unless a
+    // chunk's staging would exceed 256 MB (the last chunk's copy and packing
+    // are what remains after the kernel)
+    const int64_t row_bytes = (int64_t)nslots * (W + 1) * 8 + 13;
+    int64_t C = std::max<int64_t>(1, std::min<int64_t>(32, n / 32768));
+    C = std::max<int64_t>(C, (n * row_bytes + ((int64_t)256 << 20) - 1) / ((int64_t)256 << 20));
+    C = std::min<int64_t>(C, n);
+    const int64_t cn = (n + C - 1) / C;
+    const size_t stage_bytes = (size_t)cn * row_bytes + 64;
+    DeviceGuard g(ctx->device);
+    AllocStream alloc_stream(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->copy_stream) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+        if (!ctx->run_ev[k]) e = cudaEventCreate(&ctx->run_ev[k]);
+    if (e == cudaSuccess && ctx->done_cap < C) {
+        if (ctx->done_pin) cudaFreeHost(ctx->done_pin);
+        ctx->done_pin = nullptr;
+        ctx->done_cap = 0;
+        e = cudaHostAlloc((void**)&ctx->done_pin, (size_t)std::max<int64_t>(C, 64) * sizeof(int32_t),
+                          cudaHostAllocDefault);
+        if (e == cudaSuccess) ctx->done_cap = std::max<int64_t>(C, 64);
+    }
+    cudaStream_t s_cp = ctx->copy_stream;
+    cudaEvent_t ev0 = ctx->run_ev[0], ev1 = ctx->run_ev[1];
+    int32_t* hdone = ctx->done_pin;
+    if (e == cudaSuccess && ctx->chunk_pin_bytes < stage_bytes) {
+        if (ctx->chunk_pin) cudaFreeHost(ctx->chunk_pin);
+        ctx->chunk_pin = nullptr;
+        ctx->chunk_pin_bytes = 0;
+        e = cudaHostAlloc(&ctx->chunk_pin, stage_bytes, cudaHostAllocDefault);
+        if (e == cudaSuccess) ctx->chunk_pin_bytes = stage_bytes;
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(ctx, e, "pipeline set-up");
+    }
+    int rc = TP_OK;
+    {
+        DBuf u0_d, dt_d, te_d, t_d, u_d, ns_d, rc_d, nst_d, st_d, q_d, done_d;
+        e = u0_d.alloc((size_t)n * 6 * sizeof(double));
+        if (e == cudaSuccess && dt_i) e = dt_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess && tend_i) e = te_d.alloc((size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = t_d.alloc((size_t)nslots * n * sizeof(double));
+        if (e == cudaSuccess) e = u_d.alloc((size_t)nslots * W * n * sizeof(double));
+        if (e == cudaSuccess) e = ns_d.alloc((size_t)n * sizeof(int32_t));
+        if (e == cudaSuccess) e = rc_d.alloc((size_t)n * sizeof(int8_t));
+        if (e == cudaSuccess) e = nst_d.alloc((size_t)n * sizeof(int64_t));
+        if (e == cudaSuccess) e = st_d.alloc(sizeof(int32_t));
+        if (e == cudaSuccess) e = q_d.alloc(sizeof(unsigned long long));
+        if (e == cudaSuccess) e = done_d.alloc((size_t)C * sizeof(int32_t));
+        if (e != cudaSuccess) {
+            return fail(ctx, TP_E_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+        }
+        e = copy_to_device(ctx, u0_d.p, u0, (size_t)n * 6 * sizeof(double));
+        if (e == cudaSuccess && dt_i) e = copy_to_device(ctx, dt_d.p, dt_i, (size_t)n * sizeof(double));
+        if (e == cudaSuccess && tend_i) e = copy_to_device(ctx, te_d.p, tend_i, (size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemsetAsync(st_d.p, 0, sizeof(int32_t), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(done_d.p, 0, (size_t)C * sizeof(int32_t), s);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(s);
+            return cuda_fail(ctx, e, "input upload");
+        }
+        BorisArgs a;
+        st = prepare_boris_args(ctx, d, E, const_cast<tp_field*>(B), a);
+        if (st != TP_OK) {
+            cudaStreamSynchronize(s);
+            return st;
+        }
+        a.n = n;
+        a.nslots = nslots;
+        a.u0 = u0_d.as<double>();
+        a.dt_i = dt_i ? dt_d.as<double>() : nullptr;
+        a.tend_i = tend_i ? te_d.as<double>() : nullptr;
+        a.t_out = t_d.as<double>();
+        a.u_out = u_d.as<double>();
+        a.nsaved = ns_d.as<int32_t>();
+        a.retcode = rc_d.as<int8_t>();
+        a.nsteps = nst_d.as<int64_t>();
+        a.status = st_d.as<int32_t>();
+        // with work rates a post-pass completes the saves: chunks are final
+        // only when the whole launch is
+        const bool progressive = !a.save_work;
+        a.done = progressive ? done_d.as<int32_t>() : nullptr;
+        a.done_chunk = cn;
+        e = cudaEventRecord(ev0, s);
+        // the copy stream's polls and copies come after the counters' reset
+        // (pool memory may hold a previous call's counts)
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s_cp, ev0, 0);
+        void* obuf = nullptr;
+        if (e == cudaSuccess) st = order_particles(ctx, a, s, &obuf);
+        if (e == cudaSuccess && st == TP_OK) st = launch_boris(ctx, d, a, s, q_d.as<unsigned long long>());
+        if (obuf) cudaFreeAsync(obuf, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ev1, s);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "push kernel launch");
+        else if (st != TP_OK) rc = st;
+        // copy each chunk out once all its particles are done
+        char* stage = (char*)ctx->chunk_pin;
+        int64_t row = 0;
+        for (int64_t k = 0; k < C && rc == TP_OK; ++k) {
+            const int64_t a0 = k * cn, m = std::min(cn, n - a0);
+            for (;;) {
+                cudaError_t q = cudaEventQuery(ev1);
+                if (q == cudaSuccess) break;  // the whole launch is done
+                if (q != cudaErrorNotReady) {
+                    rc = cuda_fail(ctx, q, "push kernel");
+                    break;
+                }
+                if (progressive) {
+                    e = cudaMemcpyAsync(hdone, done_d.p, (size_t)C * sizeof(int32_t), cudaMemcpyDeviceToHost, s_cp);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(s_cp);
+                    if (e != cudaSuccess) {
+                        rc = cuda_fail(ctx, e, "chunk progress");
+                        break;
+                    }
+                    if (hdone[k] >= m) break;
+                }
+                std::this_thread::sleep_for(std::chrono::microseconds(250));
+            }
+            if (rc != TP_OK) break;
+            double* t_st = (double*)stage;
+            double* u_st = t_st + nslots * m;
+            int32_t* ns_st = (int32_t*)(u_st + nslots * W * m);
+            int64_t* nst_st = (int64_t*)(ns_st + ((m + 1) & ~(int64_t)1));
+            int8_t* rc_st = (int8_t*)(nst_st + m);
+            e = cudaSuccess;
+            if (nslots > 0) {
+                e = cudaMemcpy2DAsync(t_st, m * sizeof(double), t_d.as<double>() + a0, n * sizeof(double),
+                                      m * sizeof(double), nslots, cudaMemcpyDeviceToHost, s_cp);
+                if (e == cudaSuccess)
+                    e = cudaMemcpy2DAsync(u_st, m * sizeof(double), u_d.as<double>() + a0, n * sizeof(double),
+                                          m * sizeof(double), nslots * W, cudaMemcpyDeviceToHost, s_cp);
+            }
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ns_st, ns_d.as<int32_t>() + a0, m * sizeof(int32_t), cudaMemcpyDeviceToHost, s_cp);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(nst_st, nst_d.as<int64_t>() + a0, m * sizeof(int64_t), cudaMemcpyDeviceToHost, s_cp);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(rc_st, rc_d.as<int8_t>() + a0, m, cudaMemcpyDeviceToHost, s_cp);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s_cp);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(ctx, e, "result copy");
+                break;
+            }
+            int64_t rows = 0;
+            for (int64_t i = 0; i < m; ++i) rows += std::min<int64_t>(std::max<int32_t>(ns_st[i], 0), nslots);
+            if (row + rows > cap_rows) {
+                rc = fail(ctx, TP_E_ARG, "cap_rows is smaller than the number of saves");
+                break;
+            }
+            pack_chunk_host(t_st, u_st, ns_st, m, nslots, W, t_packed + row, u_packed + row * W);
+            std::memcpy(nsaved + a0, ns_st, m * sizeof(int32_t));
+            std::memcpy(nsteps + a0, nst_st, m * sizeof(int64_t));
+            std::memcpy(retcode + a0, rc_st, m);
+            row += rows;
+        }
+        e = cudaStreamSynchronize(s);
+        if (rc == TP_OK && e != cudaSuccess) rc = cuda_fail(ctx, e, "push kernel");
+        if (rc == TP_OK) {
+            int32_t status = 0;
+            e = cudaMemcpy(&status, st_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "push status");
+            else if (status != 0) rc = status_to_error(ctx, status);
+        }
+        if (rc == TP_OK) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            if (elapsed_ms) *elapsed_ms = ms;
+            *total = row;
+        }
+        cudaStreamSynchronize(s_cp);
+    }
+    cudaStreamSynchronize(s);
+    return rc;
 }
 
 // ---------------------------------------------------------------- guiding centre

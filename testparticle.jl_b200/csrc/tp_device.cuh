@@ -155,7 +155,20 @@ struct BorisArgs {
     // (a cell ordering of the initial positions in gridded fields, so that
     // the lanes of a warp gather neighbouring nodes); null = 0, 1, 2, ...
     const int32_t* perm;
+    // optional completion counts: once particle i's outputs are written it
+    // adds 1 to done[i / done_chunk], so a host can copy out finished index
+    // ranges while the kernel runs; null = off
+    int32_t* done;
+    int64_t done_chunk;
 };
+
+// particle i's outputs are final: publish them, then count the particle
+__device__ __forceinline__ void particle_done(const BorisArgs& a, int64_t i) {
+    if (a.done) {
+        __threadfence_system();
+        atomicAdd(a.done + i / a.done_chunk, 1);
+    }
+}
 
 // the particle taken k-th under the run's processing order (k < n)
 __device__ __forceinline__ int64_t take_particle(const BorisArgs& a, int64_t k) {

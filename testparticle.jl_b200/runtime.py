@@ -8,7 +8,6 @@ ArgumentError; the others -> RuntimeError).
 from __future__ import annotations
 
 import ctypes as C
-import os
 import threading
 import weakref
 from dataclasses import dataclass
@@ -24,50 +23,6 @@ class ArgumentError(ValueError):
 
 class DeviceError(RuntimeError):
     """A CUDA, timeout or capacity failure reported by the library."""
-
-
-class _ResultBuffers:
-    """Host arrays for a run's packed results, allocated at their upper bound
-    (n trajectories x slots) and first-touched by host threads while the run's
-    kernels execute (the C call releases the GIL).  Copying the results then
-    writes into pages that already exist: a first touch of fresh pages costs
-    the kernel's page zeroing, about twice the copy itself."""
-
-    MIN_BYTES = 64 << 20
-
-    def __init__(self, rows: int, width: int):
-        self.rows, self.width = rows, width
-        self.t = self.u = None
-        # one coordinator thread allocates and starts the fillers, so the
-        # caller only pays for one thread start before its C call
-        self.thread = threading.Thread(target=self._fill, daemon=True)
-        self.thread.start()
-
-    def _fill(self):
-        t = np.empty(self.rows, dtype=np.float64)
-        u = np.empty((self.rows, self.width), dtype=np.float64)
-        k = max(1, min(8, os.cpu_count() or 1))
-        parts = []
-        for a in (t, u.reshape(-1)):
-            step = (a.size + k - 1) // k
-            parts += [a[j:j + step] for j in range(0, a.size, step)]
-        workers = [threading.Thread(target=part.fill, args=(0.0,), daemon=True) for part in parts]
-        for th in workers:
-            th.start()
-        for th in workers:
-            th.join()
-        self.t, self.u = t, u
-
-    @classmethod
-    def maybe(cls, rows: int, width: int):
-        return cls(rows, width) if rows > 0 and rows * (width + 1) * 8 >= cls.MIN_BYTES else None
-
-    def take(self, total: int, width: int):
-        """(t, u) of `total` rows, or None when they would waste the buffers."""
-        self.thread.join()
-        if self.u is None or width != self.width or total > self.rows or total < 0.9 * self.rows:
-            return None
-        return self.t[:total], self.u[:total]
 
 
 def _check(lib, ctx, code: int, what: str):
@@ -152,7 +107,11 @@ class Context:
         return h
 
     # ------------------------------------------------------------ runs
-    def boris_run(self, desc: _abi.RunDesc, E, B, u0: np.ndarray, dt_i=None, tend_i=None):
+    def boris_run(self, desc: _abi.RunDesc, E, B, u0: np.ndarray, dt_i=None, tend_i=None, pipelined=True):
+        """Full-orbit solve of host arrays.  With a known save count it runs
+        through tp_boris_run_host (chunks, results copied while later chunks
+        compute); otherwise, or with pipelined=False, through tp_boris_run and
+        tp_result_copy.  Both give the same results bit for bit."""
         u0 = np.ascontiguousarray(u0, dtype=np.float64)
         n = u0.shape[0]
         assert u0.shape == (n, 6)
@@ -164,11 +123,32 @@ class Context:
         # slots per trajectory (an invalid descriptor is reported by the run itself)
         if n > 0 and self.lib.tp_boris_slots(C.byref(desc), _ptr(dt_i), _ptr(tend_i), n, C.byref(ns)) != _abi.TP_OK:
             ns.value = -1
-        bufs = _ResultBuffers.maybe(n * ns.value, width) if ns.value > 0 else None
+        if pipelined and ns.value >= 0 and n > 0:
+            return self.boris_run_host(desc, E, B, u0, dt_i, tend_i, n * ns.value)
         code = self.lib.tp_boris_run(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0),
                                      _ptr(dt_i), _ptr(tend_i), n, C.byref(res))
         _check(self.lib, self.handle, code, "tp_boris_run")
-        return self._collect(res, bufs)
+        return self._collect(res)
+
+    def boris_run_host(self, desc: _abi.RunDesc, E, B, u0: np.ndarray, dt_i, tend_i, cap_rows: int):
+        """tp_boris_run_host: one kernel, with each finished chunk of particles
+        copied and packed into the returned arrays while the kernel runs.  The
+        row arrays are allocated at cap_rows and not touched beforehand: the
+        library's packing threads fault their pages in while the GPU is busy."""
+        n = u0.shape[0]
+        width = 6 + 6 * bool(desc.save_fields) + 4 * bool(desc.save_work)
+        nsaved = np.empty(n, dtype=np.int32)
+        retcode = np.empty(n, dtype=np.int8)
+        nsteps = np.empty(n, dtype=np.int64)
+        t = np.empty(max(cap_rows, 1), dtype=np.float64)
+        u = np.empty((max(cap_rows, 1), width), dtype=np.float64)
+        tot = C.c_int64()
+        ms = C.c_double()
+        code = self.lib.tp_boris_run_host(self.handle, C.byref(desc), self.field(E), self.field(B), _ptr(u0),
+                                          _ptr(dt_i), _ptr(tend_i), n, cap_rows, _ptr(nsaved), _ptr(retcode),
+                                          _ptr(nsteps), _ptr(t), _ptr(u), C.byref(tot), C.byref(ms))
+        _check(self.lib, self.handle, code, "tp_boris_run_host")
+        return RunResult(nsaved, retcode, nsteps, t[:tot.value], u[:tot.value], ms.value)
 
     def gc_run(self, desc: _abi.GCDesc, E, B, y0: np.ndarray, q_i=None, q2m_i=None, mu_i=None,
                dt_i=None, tend_i=None):
@@ -330,7 +310,7 @@ class Context:
         _check(self.lib, self.handle, code, "tp_eval_points")
         return out
 
-    def _collect(self, res: C.c_void_p, bufs: "_ResultBuffers | None" = None) -> "RunResult":
+    def _collect(self, res: C.c_void_p) -> "RunResult":
         lib = self.lib
         try:
             n = C.c_int64()
@@ -340,12 +320,8 @@ class Context:
             nsaved = np.empty(n.value, dtype=np.int32)
             retcode = np.empty(n.value, dtype=np.int8)
             nsteps = np.empty(n.value, dtype=np.int64)
-            pre = bufs.take(tot.value, w.value) if bufs is not None else None
-            if pre is not None:
-                t, u = pre
-            else:
-                t = np.empty(tot.value, dtype=np.float64)
-                u = np.empty((tot.value, w.value), dtype=np.float64)
+            t = np.empty(tot.value, dtype=np.float64)
+            u = np.empty((tot.value, w.value), dtype=np.float64)
             lib.tp_result_copy(res, _ptr(nsaved), _ptr(retcode), _ptr(nsteps), _ptr(t), _ptr(u))
             ms = C.c_double()
             lib.tp_result_elapsed_ms(res, C.byref(ms))

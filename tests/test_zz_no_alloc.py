@@ -69,7 +69,7 @@ def _pack_without_alloc(tp, torch, ctx, plan):
 
 
 def _check_against_allocating_path(tp, torch, ctx, plan):
-    ref = ctx.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i)
+    ref = ctx.boris_run(plan.desc, plan.E, plan.B, plan.u0, plan.dt_i, plan.tend_i, pipelined=False)
     nsaved, t, u, rest = _pack_without_alloc(tp, torch, ctx, plan)
     assert np.array_equal(nsaved, ref.nsaved)
     assert t.shape == ref.t.shape and u.shape == ref.u.shape
