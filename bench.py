@@ -55,7 +55,7 @@ TRAFFIC_PER_PARTICLE_STEP = 8.4
 # one warp-step of k_fixed32c<MULTI, queue, analytic> issues and the DRAM
 # bytes per particle-step, both measured by ncu on 262144 protons x 200 steps
 FLOPS_PER_PARTICLE_STEP_DIPOLE = 150
-INST_PER_WARP_STEP_DIPOLE = 348.5
+INST_PER_WARP_STEP_DIPOLE = 340.8
 TRAFFIC_PER_PARTICLE_STEP_DIPOLE = 0.32
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0

@@ -109,7 +109,7 @@ __device__ __forceinline__ int64_t next_particle32(const BorisArgs& a, int64_t& 
 
 // ---------------------------------------------------------------- fixed step
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed32c(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_FIXED_BOUND(FK), 1) k_fixed32c(BorisArgs a) {
     using P = Vel32<FK>;
     using V = typename P::V;
     using Fv = typename P::Fv;

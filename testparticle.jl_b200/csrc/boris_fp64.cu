@@ -75,7 +75,7 @@ __device__ __forceinline__ int64_t next_particle(const BorisArgs& a, int64_t& fi
 
 // ---------------------------------------------------------------- fixed step
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_fixed64(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_FIXED_BOUND(FK), 1) k_fixed64(BorisArgs a) {
     const Saver64<FK> S(a);
     const bool stat = fields_static(a.f);
     const uint64_t t_start = globaltimer_ns();

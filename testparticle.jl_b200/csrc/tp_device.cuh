@@ -217,3 +217,14 @@ __device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, b
 // registers, no spills): the float64 multistep and adaptive pushes in the
 // dipole measured 15 % faster than at 256.  The others take 256.
 #define TPB_MAXT(FK) ((FK) == FK_EBGRID ? 384 : ((FK) == FK_ANALYTIC ? 512 : 256))
+
+// Register cap of the one-particle-per-thread fixed-step kernels (k_fixed32c,
+// k_fixed64).  In analytic fields they are compiled for blocks of up to 768
+// threads (<= 80 registers per thread, six 128-thread blocks per SM) although
+// launches stay at or below TPB_MAXT: the extra resident warps hide the
+// float64 dependency latency that bounds them, and outweigh the 40-150 bytes
+// of spills this costs.  On the dipole ensemble (MultistepBoris4(2), 1e6 x 1e4)
+// the FP32C push measured 7.50e10 -> 7.93e10 particle-steps/s (caps of 640,
+// 896 and 1024 threads: 7.69e10, 7.64e10, 7.58e10) and the float64 push
+// 2.71e10 -> 2.88e10 (640: 2.80e10).
+#define TPB_FIXED_BOUND(FK) ((FK) == FK_ANALYTIC ? 768 : TPB_MAXT(FK))
