@@ -412,7 +412,11 @@ int tp_boris_run(tp_ctx* ctx, const tp_run_desc* desc, const tp_field* E,
  * hands particles out in index order, so chunks finish while the kernel
  * still runs, and each finished chunk is copied to pinned memory and packed
  * into the caller's buffers by host threads meanwhile.  The context keeps
- * the pinned staging (one chunk, at most 256 MB) between calls.
+ * the pinned staging (one chunk, at most 256 MB) between calls.  Where
+ * chunks cannot finish early (gridded solves processed in cell order, or
+ * work rates completed by a post-pass), host threads first-touch the
+ * caller's arrays while the kernel runs and the saves are packed on the
+ * device afterwards.
  *   cap_rows        rows t_packed and u_packed can hold (n * slots from
  *                   tp_boris_slots always suffices; fewer fails with
  *                   TP_E_ARG once the saves exceed them)

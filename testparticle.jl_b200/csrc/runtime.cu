@@ -1534,6 +1534,21 @@ namespace {
 // device packing does.  Returns the rows written.  Host threads split the
 // particles; each walks blocks of 8 particles so that the strided reads
 // use whole cache lines.
+// Write zeros over n doubles with host threads: the first touch of fresh
+// pages (the kernel's page zeroing) happens here, off the copy's path.
+void touch_pages(double* p, int64_t n) {
+    if (!p || n <= 0) return;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nth = (int)std::min<int64_t>(std::max(1u, std::min(hw, 8u)), (n + (1 << 20) - 1) >> 20);
+    std::vector<std::thread> th;
+    const int64_t slice = (n + nth - 1) / nth;
+    for (int k = 0; k < nth; ++k) {
+        const int64_t a = std::min(n, k * slice), b = std::min(n, (k + 1) * slice);
+        if (a < b) th.emplace_back([=]() { std::memset(p + a, 0, (size_t)(b - a) * sizeof(double)); });
+    }
+    for (auto& t : th) t.join();
+}
+
 int64_t pack_chunk_host(const double* t_st, const double* u_st, const int32_t* ns, int64_t m, int64_t nslots,
                         int W, double* t_dst, double* u_dst) {
     std::vector<int64_t> off((size_t)m + 1);
@@ -1709,10 +1724,55 @@ int tp_boris_run_host(tp_ctx* ctx, const tp_run_desc* d, const tp_field* E, cons
         if (e == cudaSuccess) e = cudaEventRecord(ev1, s);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "push kernel launch");
         else if (st != TP_OK) rc = st;
-        // copy each chunk out once all its particles are done
-        char* stage = (char*)ctx->chunk_pin;
+        // Particles processed in cell order (gridded solves) or saves completed
+        // by a post-pass: chunks are final only at the end.  Then the caller's
+        // arrays are first touched by host threads while the kernel runs, and
+        // the saves are packed on the device and copied through the pinned
+        // staging buffers afterwards.
+        const bool in_order = progressive && !a.perm;
         int64_t row = 0;
-        for (int64_t k = 0; k < C && rc == TP_OK; ++k) {
+        if (!in_order && rc == TP_OK) {
+            std::thread toucher([&]() {
+                touch_pages(t_packed, cap_rows);
+                touch_pages(u_packed, cap_rows * W);
+            });
+            e = cudaEventSynchronize(ev1);
+            toucher.join();
+            DBuf cnt_d, off_d, tmp_d, tp_d, up_d;
+            size_t tb = 0;
+            if (e == cudaSuccess) e = cnt_d.alloc((size_t)(n + 1) * sizeof(int64_t));
+            if (e == cudaSuccess) e = off_d.alloc((size_t)(n + 1) * sizeof(int64_t));
+            if (e == cudaSuccess)
+                e = scan_offsets(ns_d.as<int32_t>(), n, nslots, cnt_d.as<int64_t>(), off_d.as<int64_t>(), nullptr, &tb, s);
+            if (e == cudaSuccess) e = tmp_d.alloc(tb);
+            if (e == cudaSuccess)
+                e = scan_offsets(ns_d.as<int32_t>(), n, nslots, cnt_d.as<int64_t>(), off_d.as<int64_t>(), tmp_d.p, &tb, s);
+            int64_t tot = 0;
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&tot, off_d.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(ctx, e, "result offsets");
+            } else if (tot > cap_rows) {
+                rc = fail(ctx, TP_E_ARG, "cap_rows is smaller than the number of saves");
+            } else {
+                e = tp_d.alloc((size_t)std::max<int64_t>(tot, 1) * sizeof(double));
+                if (e == cudaSuccess) e = up_d.alloc((size_t)std::max<int64_t>(tot, 1) * W * sizeof(double));
+                if (e == cudaSuccess)
+                    e = launch_pack_results(t_d.as<double>(), u_d.as<double>(), ns_d.as<int32_t>(),
+                                            off_d.as<int64_t>(), n, nslots, W, tp_d.as<double>(), up_d.as<double>(), s);
+                if (e == cudaSuccess) e = copy_to_host_on(ctx, s, t_packed, tp_d.p, (size_t)tot * sizeof(double));
+                if (e == cudaSuccess) e = copy_to_host_on(ctx, s, u_packed, up_d.p, (size_t)tot * W * sizeof(double));
+                if (e == cudaSuccess) e = copy_to_host_on(ctx, s, nsaved, ns_d.p, (size_t)n * sizeof(int32_t));
+                if (e == cudaSuccess) e = copy_to_host_on(ctx, s, retcode, rc_d.p, (size_t)n);
+                if (e == cudaSuccess) e = copy_to_host_on(ctx, s, nsteps, nst_d.p, (size_t)n * sizeof(int64_t));
+                if (e != cudaSuccess) rc = cuda_fail(ctx, e, "result packing");
+                else row = tot;
+            }
+        }
+        // otherwise copy each chunk out once all its particles are done
+        char* stage = (char*)ctx->chunk_pin;
+        for (int64_t k = 0; k < C && rc == TP_OK && in_order; ++k) {
             const int64_t a0 = k * cn, m = std::min(cn, n - a0);
             for (;;) {
                 cudaError_t q = cudaEventQuery(ev1);

@@ -67,6 +67,20 @@ def test_pipelined_gridded_with_fields_and_work(tp):
     _same(a, b)
 
 
+def test_pipelined_gridded_cell_order(tp):
+    """Cell-ordered processing without a post-pass: the device-packing branch."""
+    n = 150_000
+    w = tp.workloads.config2(n, nx=32, nt=100, ssi=20)
+    prob = tp.TraceProblem(w.u0, w.tspan, tp.prepare(w.E, w.B, species=w.species))
+    plan = tp.plan_boris(prob, tp.Boris(), tp.EnsembleB200(precision="fp64"), dt=w.dt,
+                         savestepinterval=w.savestepinterval)
+    ctx = tp.Context.get(0)
+    a, b = _both(ctx, plan)
+    _same(a, b)
+    again, _ = _both(ctx, plan)
+    _same(again, b)
+
+
 def test_pipelined_static_schedule(tp):
     n = 100_000
     w = tp.workloads.config3(n, nt=200, ssi=25)
