@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(128, 5) k_cubic32c(BorisArgs a) {
 
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive32c(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_ADAPTIVE32_BOUND(FK), 1) k_adaptive32c(BorisArgs a) {
     using P = Vel32<FK>;
     using V = typename P::V;
     using Fv = typename P::Fv;

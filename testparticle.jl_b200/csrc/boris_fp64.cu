@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(TPB_MAXT(FK) / PPT, 1) k_fixed64_slots(BorisAr
 
 // ---------------------------------------------------------------- adaptive
 template <bool MULTI, bool QUEUE, int FK>
-__global__ void __launch_bounds__(TPB_MAXT(FK), 1) k_adaptive64(BorisArgs a) {
+__global__ void __launch_bounds__(TPB_ADAPTIVE64_BOUND(FK), 1) k_adaptive64(BorisArgs a) {
     const Saver64<FK> S(a);
     const bool stat = fields_static(a.f);
     const uint64_t t_start = globaltimer_ns();

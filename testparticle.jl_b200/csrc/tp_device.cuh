@@ -228,3 +228,10 @@ __device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, b
 // 896 and 1024 threads: 7.69e10, 7.64e10, 7.58e10) and the float64 push
 // 2.71e10 -> 2.88e10 (640: 2.80e10).
 #define TPB_FIXED_BOUND(FK) ((FK) == FK_ANALYTIC ? 768 : TPB_MAXT(FK))
+
+// The same for the adaptive kernels in analytic fields (AdaptiveBoris(0.1)
+// on the dipole ensemble, 1e6 particles, cap 1e4 steps): FP32C at 640
+// threads (<= 96 registers) 3.39e10 -> 3.57e10 particle-steps/s (768:
+// 3.54e10), float64 at 768 (<= 80) 2.32e10 -> 2.44e10 (640: 2.42e10).
+#define TPB_ADAPTIVE32_BOUND(FK) ((FK) == FK_ANALYTIC ? 640 : TPB_MAXT(FK))
+#define TPB_ADAPTIVE64_BOUND(FK) ((FK) == FK_ANALYTIC ? 768 : TPB_MAXT(FK))
