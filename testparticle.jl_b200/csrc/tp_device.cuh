@@ -214,10 +214,11 @@ __device__ __forceinline__ int64_t calc_nout(int64_t nt, int64_t ssi, bool ss, b
 // workload (1.93e10 against 2.07e10 particle-steps/s, four blocks per SM
 // instead of three), and the FP32C one spills 70-110 bytes and measured
 // 8 % slower at 448 or 512 (2.77e10 against 3.02e10): spills add traffic to
-// the L1 path that bounds it.  The analytic-field kernels
-// are latency bound on float64 dependency chains and take 512 (<= 128
-// registers, no spills): the float64 multistep and adaptive pushes in the
-// dipole measured 15 % faster than at 256.  The others take 256.
+// the L1 path that bounds it.  The analytic-field kernels are latency bound
+// on float64 dependency chains and launch up to 512 threads: the float64
+// multistep and adaptive pushes in the dipole measured 15 % faster than at
+// 256 (the fixed-step and adaptive ones are compiled for larger blocks
+// still, below).  The others take 256.
 #define TPB_MAXT(FK) ((FK) == FK_EBGRID ? 384 : ((FK) == FK_ANALYTIC ? 512 : 256))
 
 // Register cap of the one-particle-per-thread fixed-step kernels (k_fixed32c,
