@@ -110,9 +110,18 @@ class EnsembleSolution:
         self.alg = alg
         self.elapsedTime = elapsed_s
         self.elapsed_e2e = elapsed_e2e_s
-        self.offsets = np.zeros(nsaved.size + 1, dtype=np.int64)
-        np.cumsum(nsaved, out=self.offsets[1:])
+        self._offsets = None
         self.u = _Trajectories(self)
+
+    @property
+    def offsets(self) -> np.ndarray:
+        """Row of each trajectory's first save in t_all / u_all (n + 1 values),
+        computed on first use."""
+        if self._offsets is None:
+            off = np.zeros(self.nsaved.size + 1, dtype=np.int64)
+            np.cumsum(self.nsaved, out=off[1:])
+            self._offsets = off
+        return self._offsets
 
     def __len__(self):
         return self.nsaved.size
